@@ -1,0 +1,195 @@
+"""Python host interface over the C ABI (device memory and streams come from PyTorch).
+
+``Context`` owns an ar_ctx; ``GpuScene`` is a resident scene stepped with the fused
+pipeline; ``Batch`` steps many resident scenes with one launch per stage.  The stage entry
+points of include/arsim.h are reachable through ``diploma_thesis_b200._lib.call``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import (AR_BROADPHASE_BVH, AR_BROADPHASE_GRID, SceneDesc, SceneInit, SceneView,
+                   SimParams, StepView, call, lib)
+from .scenes import Scene
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> C.c_void_p:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def ptr(t: torch.Tensor | None) -> C.c_void_p:
+    if t is None:
+        return C.c_void_p(None)
+    assert t.is_cuda and t.is_contiguous(), "device tensors must be contiguous CUDA tensors"
+    return C.c_void_p(t.data_ptr())
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        torch.cuda.set_device(device)
+        torch.cuda.init()
+        self.handle = C.c_void_p()
+        call("ar_ctx_create", device, C.byref(self.handle))
+
+    def status(self, stream=None) -> int:
+        return lib.ar_ctx_status(self.handle, stream_handle(stream))
+
+    def check(self, stream=None) -> None:
+        _lib.check(self.status(stream), "ar_ctx_status")
+
+    def close(self) -> None:
+        if self.handle:
+            lib.ar_ctx_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):  # pragma: no cover - best effort
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def make_desc(scene: Scene, broadphase: int = AR_BROADPHASE_GRID, block_size: int = 0,
+              cell_size: float | None = None, grid_log2=None) -> SceneDesc:
+    d = SceneDesc()
+    d.num_bodies = scene.num_bodies
+    d.num_particles = scene.num_particles
+    d.radius = scene.radius
+    for a in range(3):
+        d.box_min[a] = float(scene.box_min[a])
+        d.box_max[a] = float(scene.box_max[a])
+        d.gravity[a] = float(scene.gravity[a])
+    d.dt = scene.dt
+    d.spring = scene.spring
+    d.damping = scene.damping
+    d.shear = scene.shear
+    d.attraction = scene.attraction
+    d.broadphase = broadphase
+    d.cell_size = scene.cell_size if cell_size is None else cell_size
+    g = scene.grid_log2 if grid_log2 is None else grid_log2
+    for a in range(3):
+        d.grid_log2[a] = int(g[a])
+    d.block_size = block_size
+    return d
+
+
+def _np_ptr(a: np.ndarray) -> C.c_void_p:
+    return C.c_void_p(a.ctypes.data)
+
+
+class GpuScene:
+    """A scene resident on the device, advanced by ar_step."""
+
+    def __init__(self, ctx: Context, scene: Scene, block_size: int = 0,
+                 cell_size: float | None = None, grid_log2=None):
+        self.ctx = ctx
+        self.scene = scene
+        self.desc = make_desc(scene, AR_BROADPHASE_GRID, block_size, cell_size, grid_log2)
+        self._keep = [np.ascontiguousarray(a) for a in (
+            scene.body_pos, scene.body_quat, scene.body_vel, scene.body_angvel,
+            scene.body_mass.astype(np.float32), scene.body_inv_inertia.astype(np.float32),
+            scene.body_offsets.astype(np.int32), scene.particle_rel)]
+        init = SceneInit(*[_np_ptr(a) for a in self._keep])
+        self.handle = C.c_void_p()
+        call("ar_scene_create", ctx.handle, C.byref(self.desc), C.byref(init),
+             stream_handle(), C.byref(self.handle))
+        self.num_bodies = scene.num_bodies
+        self.num_particles = scene.num_particles
+
+    def step(self, n: int = 1, use_graph: bool = True, stream=None) -> None:
+        call("ar_step", self.ctx.handle, self.handle, int(n), int(use_graph),
+             stream_handle(stream))
+
+    def download(self) -> dict[str, np.ndarray]:
+        nb = self.num_bodies
+        out = {k: np.zeros((nb, 4), np.float32) for k in ("pos", "quat", "vel", "angvel")}
+        call("ar_scene_download", self.handle, _np_ptr(out["pos"]), _np_ptr(out["quat"]),
+             _np_ptr(out["vel"]), _np_ptr(out["angvel"]), stream_handle())
+        return out
+
+    def view(self) -> SceneView:
+        v = SceneView()
+        call("ar_scene_get_view", self.handle, C.byref(v))
+        return v
+
+    def step_view(self) -> StepView:
+        v = StepView()
+        call("ar_scene_step_view", self.handle, C.byref(v))
+        return v
+
+    def grid_info(self):
+        o = (C.c_float * 3)()
+        c = (C.c_float * 3)()
+        d = (C.c_uint32 * 3)()
+        call("ar_scene_grid_info", self.handle, o, c, d)
+        return list(o), list(c), list(d)
+
+    def launches_per_step(self) -> int:
+        return int(lib.ar_scene_launches_per_step(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            lib.ar_scene_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+
+class Batch:
+    """Many resident scenes advanced together (one launch per stage, CUDA graph)."""
+
+    def __init__(self, ctx: Context, scenes: list[GpuScene] | None = None):
+        self.ctx = ctx
+        self.handle = C.c_void_p()
+        call("ar_batch_create", ctx.handle, C.byref(self.handle))
+        self.scenes: list[GpuScene] = []
+        if scenes:
+            self.set_scenes(scenes)
+
+    def set_scenes(self, scenes: list[GpuScene]) -> None:
+        self.scenes = list(scenes)
+        arr = (C.c_void_p * max(1, len(scenes)))(*[s.handle for s in scenes])
+        call("ar_batch_set_scenes", self.handle, arr, len(scenes))
+
+    def step(self, n: int = 1, use_graph: bool = True, stream=None) -> None:
+        call("ar_batch_step", self.ctx.handle, self.handle, int(n), int(use_graph),
+             stream_handle(stream))
+
+    def launches_per_step(self) -> int:
+        return int(lib.ar_batch_launches_per_step(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            lib.ar_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+
+def device_view(addr: int, count: int, dtype: torch.dtype, device: int = 0) -> torch.Tensor:
+    """Copy `count` elements starting at a raw device address into a new tensor."""
+    elem = torch.empty((), dtype=dtype).element_size()
+    out = torch.empty(count, dtype=dtype, device=f"cuda:{device}")
+    if count:
+        torch.cuda.synchronize()
+        cudart = torch.cuda.cudart()
+        cudart.cudaMemcpy(out.data_ptr(), addr, count * elem, 3)  # device to device
+    return out
+
+
+def sim_params(radius: float, grid_origin, cell, grid_dims, spring=0.5, damping=0.02,
+               shear=0.1, attraction=0.0, gravity=(0.0, -9.81, 0.0), w_damping=1.0) -> SimParams:
+    p = SimParams()
+    p.particle_radius = radius
+    for a in range(3):
+        p.world_origin[a] = grid_origin[a]
+        p.cell_size[a] = cell[a] if np.ndim(cell) else cell
+        p.grid_size[a] = int(grid_dims[a])
+        p.gravity[a] = gravity[a]
+    p.num_cells = int(np.prod(grid_dims))
+    p.spring, p.damping, p.shear, p.attraction = spring, damping, shear, attraction
+    p.w_damping = w_damping
+    p.global_damping = 1.0
+    p.boundary_damping = -0.5
+    return p

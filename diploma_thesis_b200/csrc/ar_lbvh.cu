@@ -1,0 +1,410 @@
+// (a9) Karras LBVH hierarchy, (a10) leaves, (a11) bottom-up refit, (a12) traversal.
+//
+// Node numbering is the reference's SoA layout (BVHSource/BVHSoAKernels.cu): leaf i at index
+// i, internal node i at n + i, root at n.  Boxes are the reference's 32-byte AABB
+// {min.xyz, max.xyz, pad, pad}, read as two float4.
+//
+// Traversal is stackless: the tree's parent links replace the reference's int[64] stack.
+// The visit order is the reference's (RB_BVHKernels.cu:145-214): at an internal node, its
+// overlapping leaf children are handled left then right, then the walk descends into the
+// left internal child if it overlaps, and on the way back up into the right one.  Handling
+// contacts in the same order keeps the float sums identical to the reference's.
+#include "ar_internal.cuh"
+#include "ar_dem.cuh"
+
+namespace {
+
+// ---- longest common prefix (BVHSource/BVHAuxiliary.cuh:31-43) ------------------------------
+__device__ __forceinline__ int lcp(const uint32_t* __restrict__ c, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t a = __ldg(c + i), b = __ldg(c + j);
+  return a != b ? __clz(a ^ b) : __clz(i ^ j) + 32;
+}
+__device__ __forceinline__ int lcp(const uint64_t* __restrict__ c, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  uint64_t a = __ldg((const unsigned long long*)c + i), b = __ldg((const unsigned long long*)c + j);
+  return a != b ? __clzll(a ^ b) : __clz(i ^ j) + 64;
+}
+
+// ---- Karras 2012 internal nodes (kernelConstructRadixTreeSoA, BVHSoAKernels.cu:7-99) -------
+template <class K>
+__global__ void __launch_bounds__(256) build_kernel(const K* __restrict__ codes, int n,
+                                                    uint8_t* __restrict__ is_leaf,
+                                                    int32_t* __restrict__ left,
+                                                    int32_t* __restrict__ right,
+                                                    int32_t* __restrict__ parent,
+                                                    int32_t* __restrict__ min_r,
+                                                    int32_t* __restrict__ max_r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) parent[n] = -1;  // root: no parent (the reference leaves it unset)
+  if (i >= n - 1) return;
+  const int d = (lcp(codes, n, i, i + 1) - lcp(codes, n, i, i - 1)) > 0 ? 1 : -1;
+  const int sig_min = lcp(codes, n, i, i - d);
+  int lmax = 2;
+  while (lcp(codes, n, i, i + lmax * d) > sig_min) lmax *= 2;
+  int l = 0;
+  for (int t = lmax / 2; t >= 1; t /= 2) {
+    if (lcp(codes, n, i, i + (l + t) * d) > sig_min) l += t;
+    if (t == 1) break;
+  }
+  const int j = i + l * d;
+  const int sig_node = lcp(codes, n, i, j);
+  // split search: t = ceil(l / 2^k), k = 1, 2, ... (the reference's double division by a
+  // power of two is exact, so the integer ceiling is the same value)
+  int s = 0;
+  for (int k = 1;; ++k) {
+    int t = (int)(((long long)l + (1ll << k) - 1) >> k);
+    if (lcp(codes, n, i, i + (s + t) * d) > sig_node) s += t;
+    if (t <= 1) break;
+  }
+  const int gamma = i + s * d + min(d, 0);
+  const int node = n + i;
+  const int lo = min(i, j), hi = max(i, j);
+  is_leaf[node] = 0;
+  const int lc = (lo == gamma) ? gamma : gamma + n;
+  const int rc = (hi == gamma + 1) ? gamma + 1 : gamma + 1 + n;
+  left[node] = lc;
+  right[node] = rc;
+  parent[lc] = node;
+  parent[rc] = node;
+  min_r[node] = lo;
+  max_r[node] = hi;
+}
+
+// ---- leaves (kernelConstructLeafNodesSoA + initializeRadii, BVHSoAKernels.cu:108-138) ------
+__global__ void __launch_bounds__(256) leaves_kernel(int n, const int32_t* __restrict__ sorted_idx,
+                                                     const float4* __restrict__ pos, float r,
+                                                     uint8_t* __restrict__ is_leaf,
+                                                     int32_t* __restrict__ min_r,
+                                                     int32_t* __restrict__ max_r,
+                                                     float4* __restrict__ cms,
+                                                     float4* __restrict__ bounds,
+                                                     float* __restrict__ radii) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 c = __ldg(pos + __ldg(sorted_idx + i));
+  is_leaf[i] = 1;
+  min_r[i] = i;
+  max_r[i] = i;
+  cms[i] = c;
+  bounds[2 * i] = make_float4(c.x - r, c.y - r, c.z - r, c.x + r);
+  bounds[2 * i + 1] = make_float4(c.y + r, c.z + r, 0.f, 0.f);
+  radii[i] = r;
+}
+
+// ---- refit (kernelConstructInternalNodesSoA, BVHSoAKernels.cu:148-176) ----------------------
+// Release (fence before the counter) / acquire (fence after it, L2 loads of the children).
+__global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t* __restrict__ left,
+                                                    const int32_t* __restrict__ right,
+                                                    const int32_t* __restrict__ parent,
+                                                    float4* bounds, int* __restrict__ counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int node = __ldg(parent + i);
+  while (true) {
+    __threadfence();
+    if (atomicAdd(counters + (node - n), 1) == 0) return;
+    __threadfence();
+    const int a = __ldg(left + node), b = __ldg(right + node);
+    float4 a0 = __ldcg(bounds + 2 * a), a1 = __ldcg(bounds + 2 * a + 1);
+    float4 b0 = __ldcg(bounds + 2 * b), b1 = __ldcg(bounds + 2 * b + 1);
+    // mergeBounds (BVHAuxiliary.cuh:83-94): min via `a < b ? a : b`, max via `a > b ? a : b`
+    float4 m0, m1;
+    m0.x = a0.x < b0.x ? a0.x : b0.x;
+    m0.y = a0.y < b0.y ? a0.y : b0.y;
+    m0.z = a0.z < b0.z ? a0.z : b0.z;
+    m0.w = a0.w > b0.w ? a0.w : b0.w;  // max.x
+    m1.x = a1.x > b1.x ? a1.x : b1.x;  // max.y
+    m1.y = a1.y > b1.y ? a1.y : b1.y;  // max.z
+    m1.z = 0.f;
+    m1.w = 0.f;
+    __stcg(bounds + 2 * node, m0);
+    __stcg(bounds + 2 * node + 1, m1);
+    if (node == n) return;
+    node = __ldg(parent + node);
+  }
+}
+
+// ---- traversal helpers -------------------------------------------------------------------------
+struct Box {
+  float lx, ly, lz, hx, hy, hz;
+};
+__device__ __forceinline__ Box load_box(const float4* __restrict__ b, int node) {
+  float4 p = __ldg(b + 2 * node), q = __ldg(b + 2 * node + 1);
+  return Box{p.x, p.y, p.z, p.w, q.x, q.y};
+}
+// checkOverlap(AABB, AABB) (BVHAuxiliary.cuh:139-152)
+__device__ __forceinline__ bool overlap(const Box& a, const Box& b) {
+  return (a.lx <= b.hx && a.hx >= b.lx) && (a.ly <= b.hy && a.hy >= b.ly) &&
+         (a.lz <= b.hz && a.hz >= b.lz);
+}
+
+// Walk the tree in the reference's order, calling visit_leaf(leaf, is_left_child) for every
+// leaf child that `accept(child)` admits, and descending into internal children it admits.
+template <class Accept, class Visit>
+__device__ __forceinline__ void walk(int n, const uint8_t* __restrict__ is_leaf,
+                                     const int32_t* __restrict__ left,
+                                     const int32_t* __restrict__ right,
+                                     const int32_t* __restrict__ parent, Accept accept,
+                                     Visit visit_leaf) {
+  // The root (index n) is never left through its parent link, so parent[n] is not read.
+  int node = n;
+  bool descending = true;
+  int from = -1;
+  while (true) {
+    if (descending) {
+      const int lc = __ldg(left + node), rc = __ldg(right + node);
+      const bool ll = __ldg(is_leaf + lc), rl = __ldg(is_leaf + rc);
+      const bool ol = accept(lc), orr = accept(rc);
+      if (ol && ll) visit_leaf(lc, true);
+      if (orr && rl) visit_leaf(rc, false);
+      if (ol && !ll) { node = lc; continue; }
+      if (orr && !rl) { node = rc; continue; }
+      descending = false;
+    } else {
+      const int rc = __ldg(right + node);
+      if (from == __ldg(left + node) && !__ldg(is_leaf + rc) && accept(rc)) {
+        node = rc;
+        descending = true;
+        continue;
+      }
+    }
+    if (node == n) return;
+    from = node;
+    node = __ldg(parent + node);
+  }
+}
+
+// ---- collideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:100-244) ------------------------------
+__global__ void __launch_bounds__(128) collide_bvh_kernel(
+    ar_sim_params prm, const int32_t* __restrict__ rb_idx, const float4* __restrict__ rel,
+    const float4* __restrict__ vel, const uint8_t* __restrict__ is_leaf,
+    const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+    const int32_t* __restrict__ parent, const float4* __restrict__ cms,
+    const float4* __restrict__ bounds, const int32_t* __restrict__ sorted_idx,
+    const float* __restrict__ radii, int n, float4* __restrict__ p_force,
+    float4* __restrict__ p_torque, float4* __restrict__ p_positions) {
+  const int index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= n) return;
+  const int q = __ldg(sorted_idx + index);
+  const float3 qvel = ar::xyz(__ldg(vel + q));
+  const float4 qpos = __ldg(cms + index);
+  const float qrad = __ldg(radii + index);
+  const int qbody = __ldg(rb_idx + q);
+  const Box qbox = load_box(bounds, index);
+  const float4 qrel = __ldg(rel + q);
+  const float4 rbcm = make_float4(qpos.x - qrel.x, qpos.y - qrel.y, qpos.z - qrel.z, qpos.w - qrel.w);
+  float3 force = ar::mk3(0.f, 0.f, 0.f), torque = ar::mk3(0.f, 0.f, 0.f);
+  float4 corr = make_float4(0.f, 0.f, 0.f, 0.f);
+  const float3 r3 = ar::xyz(qrel);
+  if (n >= 2) {
+    walk(n, is_leaf, left, right, parent,
+         [&](int c) { return c != index && overlap(qbox, load_box(bounds, c)); },
+         [&](int c, bool is_left) {
+           const int oc = __ldg(sorted_idx + c);
+           const int ob = __ldg(rb_idx + oc);
+           if (!(qbody != ob || qbody == -1)) return;
+           float4 lc = make_float4(0.f, 0.f, 0.f, 0.f);
+           float3 f = ar_dem::static_pair(qpos, __ldg(cms + c), rbcm, qvel,
+                                          ar::xyz(__ldg(vel + oc)), qrad, __ldg(radii + c), prm,
+                                          &lc);
+           if (!is_left) {  // the right-leaf branch also takes maxOpF4(local, corr) first (:191)
+             corr.x = corr.x > lc.x ? corr.x : lc.x;
+             corr.y = corr.y > lc.y ? corr.y : lc.y;
+             corr.z = corr.z > lc.z ? corr.z : lc.z;
+             corr.w = corr.w > lc.w ? corr.w : lc.w;
+           }
+           corr = make_float4(corr.x + lc.x, corr.y + lc.y, corr.z + lc.z, corr.w + lc.w);
+           force = ar::add(force, f);
+           torque = ar::add(torque, ar::cross(r3, f));
+         });
+  }
+  if (qbody == -1) return;  // free particles: the reference updates vel in place (not on this path)
+  p_force[q] = make_float4(force.x, force.y, force.z, 0.f);
+  p_torque[q] = make_float4(torque.x, torque.y, torque.z, 0.f);
+  if (p_positions) p_positions[q] = corr;
+}
+
+// ---- FindRigidBodyCollisionsBVHKernel (Kernels/RB_BVHKernels.cu:760-876) ---------------------
+__global__ void __launch_bounds__(128) find_contacts_kernel(
+    const int32_t* __restrict__ rb_idx, const uint8_t* __restrict__ is_leaf,
+    const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+    const int32_t* __restrict__ parent, const int32_t* __restrict__ max_r,
+    const float4* __restrict__ cms, const float4* __restrict__ bounds,
+    const int32_t* __restrict__ sorted_idx, const float* __restrict__ radii, int n,
+    float* __restrict__ contact_distance, int32_t* __restrict__ colliding_particle,
+    int32_t* __restrict__ colliding_body) {
+  const int index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= n || n < 2) return;
+  const int q = __ldg(sorted_idx + index);
+  const float4 qpos = __ldg(cms + index);
+  const Box qbox = load_box(bounds, index);
+  const float qrad = __ldg(radii + q);
+  const int qbody = __ldg(rb_idx + q);
+  float best = contact_distance[q];
+  int best_p = 0, best_b = 0;
+  bool found = false;
+  walk(n, is_leaf, left, right, parent,
+       [&](int c) {
+         return c != index && __ldg(max_r + c) >= index && overlap(qbox, load_box(bounds, c));
+       },
+       [&](int c, bool) {
+         const int oc = __ldg(sorted_idx + c);
+         const int ob = __ldg(rb_idx + oc);
+         if (qbody == ob) return;
+         const float4 cp = __ldg(cms + c);
+         const float4 dd = make_float4(cp.x - qpos.x, cp.y - qpos.y, cp.z - qpos.z, cp.w - qpos.w);
+         const float dist = sqrtf(dd.x * dd.x + dd.y * dd.y + dd.z * dd.z + dd.w * dd.w);
+         const float thr = qrad + __ldg(radii + oc);
+         if (thr - dist > best) {
+           best = thr - dist;
+           best_p = oc;
+           best_b = ob;
+           found = true;
+         }
+       });
+  if (found) {
+    contact_distance[q] = best;
+    colliding_particle[q] = best_p;
+    colliding_body[q] = best_b;
+  }
+}
+
+// ---- contact pairs through the BVH ------------------------------------------------------------
+__global__ void __launch_bounds__(128) pairs_bvh_kernel(
+    float two_r, const int32_t* __restrict__ rb_idx, const uint8_t* __restrict__ is_leaf,
+    const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+    const int32_t* __restrict__ parent, const float4* __restrict__ cms,
+    const float4* __restrict__ bounds, const int32_t* __restrict__ sorted_idx, int n,
+    int2* __restrict__ pairs, int capacity, int* __restrict__ count, int* __restrict__ err) {
+  const int index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= n || n < 2) return;
+  const int q = __ldg(sorted_idx + index);
+  const float4 qpos = __ldg(cms + index);
+  const Box qbox = load_box(bounds, index);
+  const int qbody = __ldg(rb_idx + q);
+  walk(n, is_leaf, left, right, parent,
+       [&](int c) { return c != index && overlap(qbox, load_box(bounds, c)); },
+       [&](int c, bool) {
+         if (c < index) return;  // each unordered pair once (from its lower sorted leaf)
+         const int oc = __ldg(sorted_idx + c);
+         if (__ldg(rb_idx + oc) == qbody) return;
+         if (!ar_dem::touching(ar::xyz(qpos), ar::xyz(__ldg(cms + c)), two_r)) return;
+         int slot = atomicAdd(count, 1);
+         if (slot < capacity)
+           pairs[slot] = make_int2(min(q, oc), max(q, oc));
+         else
+           ar::raise_error(err, ar::kErrOverflow);
+       });
+}
+
+}  // namespace
+
+extern "C" {
+
+ar_status ar_lbvh_build(ar_ctx* ctx, const uint32_t* sorted_codes, int n, uint8_t* is_leaf,
+                        int32_t* left, int32_t* right, int32_t* parent, int32_t* min_r,
+                        int32_t* max_r, ar_stream_t stream) {
+  if (!ctx || n < 0 || (n > 0 && (!sorted_codes || !is_leaf || !left || !right || !parent ||
+                                  !min_r || !max_r)))
+    return AR_ERR_INVALID_ARG;
+  if (n < 2) return AR_OK;
+  build_kernel<uint32_t><<<arh::grid_for(n - 1, 256), 256, 0, arh::stream(stream)>>>(
+      sorted_codes, n, is_leaf, left, right, parent, min_r, max_r);
+  return arh::check_launch("ar_lbvh_build");
+}
+
+ar_status ar_lbvh_build64(ar_ctx* ctx, const uint64_t* sorted_codes, int n, uint8_t* is_leaf,
+                          int32_t* left, int32_t* right, int32_t* parent, int32_t* min_r,
+                          int32_t* max_r, ar_stream_t stream) {
+  if (!ctx || n < 0 || (n > 0 && (!sorted_codes || !is_leaf || !left || !right || !parent ||
+                                  !min_r || !max_r)))
+    return AR_ERR_INVALID_ARG;
+  if (n < 2) return AR_OK;
+  build_kernel<uint64_t><<<arh::grid_for(n - 1, 256), 256, 0, arh::stream(stream)>>>(
+      sorted_codes, n, is_leaf, left, right, parent, min_r, max_r);
+  return arh::check_launch("ar_lbvh_build64");
+}
+
+ar_status ar_lbvh_leaves(ar_ctx* ctx, int n, const int32_t* sorted_idx, const float* pos4,
+                         float radius, uint8_t* is_leaf, int32_t* min_r, int32_t* max_r,
+                         float* cms4, float* bounds8, float* radii, ar_stream_t stream) {
+  if (!ctx || n < 0 ||
+      (n > 0 && (!sorted_idx || !pos4 || !is_leaf || !min_r || !max_r || !cms4 || !bounds8 ||
+                 !radii)))
+    return AR_ERR_INVALID_ARG;
+  if (n == 0) return AR_OK;
+  leaves_kernel<<<arh::grid_for(n, 256), 256, 0, arh::stream(stream)>>>(
+      n, sorted_idx, (const float4*)pos4, radius, is_leaf, min_r, max_r, (float4*)cms4,
+      (float4*)bounds8, radii);
+  return arh::check_launch("ar_lbvh_leaves");
+}
+
+ar_status ar_lbvh_refit(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
+                        const int32_t* parent, float* bounds8, ar_stream_t stream) {
+  if (!ctx || n < 0 || (n > 0 && (!left || !right || !parent || !bounds8)))
+    return AR_ERR_INVALID_ARG;
+  if (n < 2) return AR_OK;
+  int* counters = (int*)arh::scratch(ctx, (size_t)(n - 1) * sizeof(int));
+  if (!counters) return AR_ERR_OOM;
+  cudaStream_t st = arh::stream(stream);
+  cudaMemsetAsync(counters, 0, (size_t)(n - 1) * sizeof(int), st);
+  refit_kernel<<<arh::grid_for(n, 256), 256, 0, st>>>(n, left, right, parent, (float4*)bounds8,
+                                                      counters);
+  return arh::check_launch("ar_lbvh_refit");
+}
+
+ar_status ar_collide_bvh_dem(ar_ctx* ctx, const ar_sim_params* params, const int32_t* rb_idx,
+                             const float* rel4, const float* vel4, const uint8_t* is_leaf,
+                             const int32_t* left, const int32_t* right, const int32_t* parent,
+                             const float* cms4, const float* bounds8, const int32_t* sorted_idx,
+                             const float* radii, int n, float* p_force4, float* p_torque4,
+                             float* p_positions4, ar_stream_t stream) {
+  if (!ctx || !params || n < 0 ||
+      (n > 0 && (!rb_idx || !rel4 || !vel4 || !is_leaf || !left || !right || !parent ||
+                 !cms4 || !bounds8 || !sorted_idx || !radii || !p_force4 || !p_torque4)))
+    return AR_ERR_INVALID_ARG;
+  if (n == 0) return AR_OK;
+  collide_bvh_kernel<<<arh::grid_for(n, 128), 128, 0, arh::stream(stream)>>>(
+      *params, rb_idx, (const float4*)rel4, (const float4*)vel4, is_leaf, left, right, parent,
+      (const float4*)cms4, (const float4*)bounds8, sorted_idx, radii, n, (float4*)p_force4,
+      (float4*)p_torque4, (float4*)p_positions4);
+  return arh::check_launch("ar_collide_bvh_dem");
+}
+
+ar_status ar_find_contacts_bvh(ar_ctx* ctx, const int32_t* rb_idx, const uint8_t* is_leaf,
+                               const int32_t* left, const int32_t* right, const int32_t* parent,
+                               const int32_t* max_r, const float* cms4, const float* bounds8,
+                               const int32_t* sorted_idx, const float* radii, int n,
+                               float* contact_distance, int32_t* colliding_particle,
+                               int32_t* colliding_body, ar_stream_t stream) {
+  if (!ctx || n < 0 ||
+      (n > 0 && (!rb_idx || !is_leaf || !left || !right || !parent || !max_r || !cms4 ||
+                 !bounds8 || !sorted_idx || !radii || !contact_distance ||
+                 !colliding_particle || !colliding_body)))
+    return AR_ERR_INVALID_ARG;
+  if (n < 2) return AR_OK;
+  find_contacts_kernel<<<arh::grid_for(n, 128), 128, 0, arh::stream(stream)>>>(
+      rb_idx, is_leaf, left, right, parent, max_r, (const float4*)cms4, (const float4*)bounds8,
+      sorted_idx, radii, n, contact_distance, colliding_particle, colliding_body);
+  return arh::check_launch("ar_find_contacts_bvh");
+}
+
+ar_status ar_pairs_bvh(ar_ctx* ctx, float radius, const int32_t* rb_idx, const uint8_t* is_leaf,
+                       const int32_t* left, const int32_t* right, const int32_t* parent,
+                       const float* cms4, const float* bounds8, const int32_t* sorted_idx, int n,
+                       int32_t* pairs2, int capacity, int32_t* d_count, ar_stream_t stream) {
+  if (!ctx || n < 0 || capacity < 0 || !d_count ||
+      (n > 0 && (!rb_idx || !is_leaf || !left || !right || !parent || !cms4 || !bounds8 ||
+                 !sorted_idx || (capacity > 0 && !pairs2))))
+    return AR_ERR_INVALID_ARG;
+  cudaStream_t st = arh::stream(stream);
+  cudaMemsetAsync(d_count, 0, sizeof(int32_t), st);
+  if (n < 2) return arh::check_launch("ar_pairs_bvh");
+  pairs_bvh_kernel<<<arh::grid_for(n, 128), 128, 0, st>>>(
+      2.0f * radius, rb_idx, is_leaf, left, right, parent, (const float4*)cms4,
+      (const float4*)bounds8, sorted_idx, n, (int2*)pairs2, capacity, d_count, ctx->d_err);
+  return arh::check_launch("ar_pairs_bvh");
+}
+
+}  // extern "C"

@@ -1,0 +1,712 @@
+// Fused PHYSICAL-mode step over a table of resident scenes.
+//
+// Per step (one launch per stage, whatever the number of scenes):
+//   memset   clear the sort's histogram / look-back head
+//   K1       re-pose + hash: key = scene cell base + wrapped cell of the particle's world
+//            position; the sort histogram is accumulated on the fly; cells touched by the
+//            previous step are reset to empty (no full-table clear)
+//   sort     onesweep passes over the global keys (values = global particle index)
+//   K3       scatter + cell ranges: sorted position (w = global body id) and velocity,
+//            recomputed from the body state; start/end of every occupied cell
+//   K4       DEM gather over the 27 neighbour cells + box walls -> per-particle force at the
+//            particle's original index (no atomics)
+//   K5       one warp per body: fixed-order sum of F and r x F, then integration
+// A scene's keys live in its own cell range, so sorting all scenes together orders them by
+// scene and within a scene exactly as a solo sort would: batched and solo steps are
+// bit-identical.  The sequence is captured once into a CUDA graph and replayed.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "ar_internal.cuh"
+#include "ar_dem.cuh"
+#include "ar_pipeline.cuh"
+#include "ar_sort.cuh"
+
+using ar_pipe::SceneDev;
+
+namespace {
+
+constexpr int kK1Threads = 256;
+
+__device__ __forceinline__ int find_range(const int* __restrict__ off, int count, int g) {
+  int lo = 0, hi = count;  // off[lo] <= g < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(off + mid) <= g) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// ---- K0: reset the cells a previous layout touched -------------------------------------------
+__global__ void __launch_bounds__(256) clear_cells_kernel(const uint32_t* __restrict__ skeys,
+                                                          int prev_n, uint2* __restrict__ cells) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < prev_n; g += gridDim.x * blockDim.x) {
+    const uint32_t k0 = skeys[g];
+    if (g == 0 || k0 != skeys[g - 1]) cells[k0].x = ar::kEmpty;
+  }
+}
+
+// ---- K1: re-pose + hash + sort histogram -----------------------------------------------------
+__global__ void __launch_bounds__(kK1Threads) repose_hash_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    int* __restrict__ d_prev_n, const uint32_t* __restrict__ prev_skeys, uint2* __restrict__ cells,
+    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits) {
+  __shared__ uint32_t s_hist[4][256];
+  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
+  __syncthreads();
+  const int prev_n = *d_prev_n;
+  const int lim = nt > prev_n ? nt : prev_n;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < lim; g += gridDim.x * blockDim.x) {
+    if (g < prev_n) {
+      const uint32_t k0 = __ldg(prev_skeys + g);
+      if (g == 0 || k0 != __ldg(prev_skeys + g - 1)) cells[k0].x = ar::kEmpty;
+    }
+    if (g < nt) {
+      const SceneDev& S = table[find_range(poff, ns, g)];
+      const int i = g - S.poff;
+      const float4 r4 = __ldg(S.rel + i);
+      const int b = __float_as_int(r4.w);
+      float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
+      float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
+      const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
+      keys[g] = key;
+      ar_sort::hist_count(s_hist, key, 0, passes, last_bits);
+    }
+  }
+  __syncthreads();
+  ar_sort::hist_flush(s_hist, ws_hist, passes);
+}
+
+// ---- K3: scatter + cell ranges ------------------------------------------------------------
+__global__ void __launch_bounds__(256) scatter_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
+    uint2* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
+    int* __restrict__ d_prev_n) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_prev_n = nt;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+    const uint32_t key = __ldg(skeys + k);
+    if (k == 0 || key != __ldg(skeys + k - 1)) {
+      cells[key].x = (uint32_t)k;
+      if (k > 0) cells[__ldg(skeys + k - 1)].y = (uint32_t)k;
+    }
+    if (k == nt - 1) cells[key].y = (uint32_t)nt;
+    const int g = (int)__ldg(svals + k);
+    const SceneDev& S = table[find_range(poff, ns, g)];
+    const int i = g - S.poff;
+    const float4 r4 = __ldg(S.rel + i);
+    const int b = __float_as_int(r4.w);
+    float3 r, p, v;
+    ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
+                    ar::mk3(r4.x, r4.y, r4.z), &r, &p, &v);
+    spos[k] = make_float4(p.x, p.y, p.z, __int_as_float(S.boff + b));
+    svel[k] = make_float4(v.x, v.y, v.z, 0.f);
+  }
+}
+
+// ---- K4: DEM gather + walls ----------------------------------------------------------------
+// Per sorted particle: the 27 neighbour cells in z, y, x order, occupants in sorted order,
+// skipping itself and its own body; per-cell partial sums added to the total (the order of
+// FindAndHandleRigidBodyCollisionsUniformGridKernel, RigidBodies/UniformGridDEM.cu:166-193).
+__global__ void __launch_bounds__(128) collide_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const uint32_t* __restrict__ svals, const uint2* __restrict__ cells,
+    const float4* __restrict__ spos, const float4* __restrict__ svel,
+    float4* __restrict__ pforce) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  const int g = (int)__ldg(svals + k);
+  const SceneDev& S = table[find_range(poff, ns, g)];
+  const float4 p4 = __ldg(spos + k);
+  const float3 pos = ar::xyz(p4);
+  const int body = __float_as_int(p4.w);
+  const float3 vel = ar::xyz(__ldg(svel + k));
+  const float thr = 2.0f * S.r;
+  const float kk = S.k, dmp = S.damping, shr = S.shear, att = S.attraction;
+  const int3 gp = ar_pipe::cell_of(S, pos);
+  float3 lin = ar::mk3(0.f, 0.f, 0.f);
+  for (int z = -1; z <= 1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x) {
+        float3 cell_f = ar::mk3(0.f, 0.f, 0.f);
+        const uint2 se = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x + x, gp.y + y, gp.z + z)));
+        if (se.x != ar::kEmpty) {
+          for (uint32_t j = se.x; j < se.y; ++j) {
+            const float4 q4 = __ldg(spos + j);
+            if (j == (uint32_t)k || __float_as_int(q4.w) == body) continue;
+            const float3 rp = ar::sub(ar::xyz(q4), pos);
+            const float dist = sqrtf(ar::dot(rp, rp));
+            if (dist < thr) {
+              const float3 v2 = ar::xyz(__ldg(svel + j));
+              cell_f = ar::add(cell_f, ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att));
+            }
+          }
+        }
+        lin = ar::add(lin, cell_f);
+      }
+  lin = ar::add(lin, ar_pipe::wall_force(S, pos, vel));
+  pforce[g] = make_float4(lin.x, lin.y, lin.z, 0.f);
+}
+
+// ---- K5: fixed-order body sums + integration ---------------------------------------------------
+__global__ void __launch_bounds__(256) reduce_integrate_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ boff, int ns, int bt,
+    const float4* __restrict__ pforce, int* __restrict__ err) {
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  const int lane = ar::lane_id();
+  for (int gb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gb < bt; gb += warps) {
+    const SceneDev& S = table[find_range(boff, ns, gb)];
+    const int b = gb - S.boff;
+    const int s0 = __ldg(S.offsets + b), s1 = __ldg(S.offsets + b + 1);
+    const float4 q = S.quat[b];
+    float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
+    for (int i = s0 + lane; i < s1; i += 32) {
+      const float4 f4 = __ldcs(pforce + S.poff + i);
+      const float4 r4 = __ldg(S.rel + i);
+      const float3 f = ar::xyz(f4);
+      const float3 t = ar::cross(ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z)), f);
+      fx += f.x; fy += f.y; fz += f.z;
+      tx += t.x; ty += t.y; tz += t.z;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, o);
+      fy += __shfl_xor_sync(0xffffffffu, fy, o);
+      fz += __shfl_xor_sync(0xffffffffu, fz, o);
+      tx += __shfl_xor_sync(0xffffffffu, tx, o);
+      ty += __shfl_xor_sync(0xffffffffu, ty, o);
+      tz += __shfl_xor_sync(0xffffffffu, tz, o);
+    }
+    if (lane == 0) {
+      float ib[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) ib[k] = __ldg(S.inv_inertia + 9 * b + k);
+      float4 pos = S.pos[b], quat = q, vel = S.vel[b], ang = S.ang[b];
+      const float3 F = ar::mk3(fx, fy, fz), T = ar::mk3(tx, ty, tz);
+      if (!ar_pipe::integrate_body(S, F, T, __ldg(S.mass + b), ib, &pos, &quat, &vel, &ang))
+        ar::raise_error(err, ar::kErrNaN);
+      S.pos[b] = pos;
+      S.quat[b] = quat;
+      S.vel[b] = vel;
+      S.ang[b] = ang;
+      S.bforce[b] = make_float4(fx, fy, fz, 0.f);
+      S.btorque[b] = make_float4(tx, ty, tz, 0.f);
+    }
+  }
+}
+
+int ceil_log2(uint64_t v) {
+  int b = 0;
+  while ((1ull << b) < v) ++b;
+  return b;
+}
+
+}  // namespace
+
+// --------------------------------------------------------------------------------------------
+struct ar_scene {
+  ar_ctx* ctx = nullptr;
+  ar_scene_desc desc{};
+  int n = 0, nb = 0;
+  float4 *pos = nullptr, *quat = nullptr, *vel = nullptr, *ang = nullptr;
+  float4 *bforce = nullptr, *btorque = nullptr, *rel = nullptr;
+  float *mass = nullptr, *inv_inertia = nullptr;
+  int32_t* offsets = nullptr;
+  float origin[3], cell[3];
+  uint32_t gdim[3];
+  ar_batch* solo = nullptr;
+};
+
+struct ar_batch {
+  ar_ctx* ctx = nullptr;
+  std::vector<ar_scene*> scenes;
+  bool table_dirty = true;
+  // capacities
+  long cap_n = 0, cap_b = 0, cap_s = 0;
+  uint64_t cap_cells = 0;
+  size_t cap_sort = 0;
+  // buffers
+  uint32_t *keys = nullptr, *skeys = nullptr, *svals = nullptr;
+  float4 *spos = nullptr, *svel = nullptr, *pforce = nullptr;
+  uint2* cells = nullptr;
+  char* sort_ws = nullptr;
+  SceneDev* d_table = nullptr;
+  int *d_poff = nullptr, *d_boff = nullptr, *d_prev_n = nullptr;
+  // layout
+  long nt = 0, bt = 0;
+  uint64_t total_cells = 0;
+  int key_bits = 1, passes = 1, last_bits = 1;
+  int host_prev_n = 0;  // particles whose cells are marked in skeys (0 after a clear)
+  // graph
+  cudaGraphExec_t graph = nullptr;
+  cudaStream_t cap_stream = nullptr;
+};
+
+namespace {
+
+void free_batch_buffers(ar_batch* B) {
+  cudaFree(B->keys); cudaFree(B->skeys); cudaFree(B->svals);
+  cudaFree(B->spos); cudaFree(B->svel); cudaFree(B->pforce);
+  cudaFree(B->cells); cudaFree(B->sort_ws);
+  cudaFree(B->d_table); cudaFree(B->d_poff); cudaFree(B->d_boff); cudaFree(B->d_prev_n);
+  B->keys = B->skeys = B->svals = nullptr;
+  B->spos = B->svel = B->pforce = nullptr;
+  B->cells = nullptr; B->sort_ws = nullptr; B->d_table = nullptr;
+  B->d_poff = B->d_boff = B->d_prev_n = nullptr;
+  B->cap_n = B->cap_b = B->cap_s = 0;
+  B->cap_cells = 0;
+  B->cap_sort = 0;
+}
+
+void drop_graph(ar_batch* B) {
+  if (B->graph) cudaGraphExecDestroy(B->graph);
+  B->graph = nullptr;
+}
+
+template <class T>
+bool alloc(T** p, size_t count) {
+  if (cudaMalloc((void**)p, count * sizeof(T) + 16) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return false;
+  }
+  return true;
+}
+
+uint64_t scene_cells(const ar_scene* s) {
+  return (uint64_t)s->gdim[0] * s->gdim[1] * s->gdim[2];
+}
+
+// Clear the cells the last step marked (so the table is all-empty before a layout change).
+void clear_marked(ar_batch* B, cudaStream_t st) {
+  if (B->host_prev_n > 0 && B->cells) {
+    clear_cells_kernel<<<arh::grid_for(B->host_prev_n, 256) > 4096 ? 4096
+                                                                   : arh::grid_for(B->host_prev_n, 256),
+                         256, 0, st>>>(B->skeys, B->host_prev_n, B->cells);
+    cudaMemsetAsync(B->d_prev_n, 0, sizeof(int), st);
+  }
+  B->host_prev_n = 0;
+}
+
+// (Re)build the scene table and make sure every buffer is large enough.
+ar_status prepare(ar_batch* B, cudaStream_t st) {
+  if (!B->table_dirty) return AR_OK;
+  clear_marked(B, st);
+  drop_graph(B);
+  long nt = 0, bt = 0;
+  uint64_t cells = 0;
+  std::vector<SceneDev> tab;
+  std::vector<int> poff, boff;
+  for (ar_scene* s : B->scenes) {
+    SceneDev d{};
+    const ar_scene_desc& D = s->desc;
+    for (int a = 0; a < 3; ++a) {
+      d.bmin[a] = D.box_min[a];
+      d.bmax[a] = D.box_max[a];
+      d.g[a] = D.gravity[a];
+      d.origin[a] = s->origin[a];
+      d.cell[a] = s->cell[a];
+    }
+    d.r = D.radius; d.dt = D.dt; d.k = D.spring; d.damping = D.damping; d.shear = D.shear;
+    d.attraction = D.attraction;
+    d.gx = s->gdim[0]; d.gy = s->gdim[1]; d.gz = s->gdim[2];
+    d.cell_base = (uint32_t)cells;
+    d.poff = (int)nt; d.boff = (int)bt; d.n = s->n; d.nb = s->nb;
+    d.pos = s->pos; d.quat = s->quat; d.vel = s->vel; d.ang = s->ang;
+    d.mass = s->mass; d.inv_inertia = s->inv_inertia; d.offsets = s->offsets; d.rel = s->rel;
+    d.bforce = s->bforce; d.btorque = s->btorque;
+    tab.push_back(d);
+    poff.push_back((int)nt);
+    boff.push_back((int)bt);
+    nt += s->n;
+    bt += s->nb;
+    cells += scene_cells(s);
+  }
+  poff.push_back((int)nt);
+  boff.push_back((int)bt);
+  if (cells >= (1ull << 32) || nt >= (1l << 30)) {
+    arh::set_error("batch too large: %llu cells, %ld particles", (unsigned long long)cells, nt);
+    return AR_ERR_INVALID_ARG;
+  }
+  const int key_bits = std::max(1, ceil_log2(cells));
+  const int passes = (key_bits + 7) / 8;
+  const size_t sort_bytes = ar_sort::layout(std::max(nt, 1l), 4, passes).total;
+  const long ns = (long)B->scenes.size();
+  bool realloc_needed = nt > B->cap_n || bt > B->cap_b || ns + 1 > B->cap_s ||
+                        cells > B->cap_cells || sort_bytes > B->cap_sort;
+  if (realloc_needed) {
+    cudaStreamSynchronize(st);
+    free_batch_buffers(B);
+    long cn = std::max(nt, 1l) + std::max(nt, 1l) / 8, cb = std::max(bt, 1l) + 8,
+         cs = ns + 8;
+    uint64_t cc = std::max<uint64_t>(cells, 1);
+    size_t csort = ar_sort::layout(cn, 4, passes).total;
+    bool ok = alloc(&B->keys, cn) && alloc(&B->skeys, cn) && alloc(&B->svals, cn) &&
+              alloc(&B->spos, cn) && alloc(&B->svel, cn) && alloc(&B->pforce, cn) &&
+              alloc(&B->cells, cc) && alloc(&B->sort_ws, csort) && alloc(&B->d_table, cs) &&
+              alloc(&B->d_poff, cs + 1) && alloc(&B->d_boff, cs + 1) && alloc(&B->d_prev_n, 1);
+    if (!ok) {
+      free_batch_buffers(B);
+      arh::set_error("batch workspace allocation failed (%ld particles, %llu cells)", nt,
+                     (unsigned long long)cells);
+      return AR_ERR_OOM;
+    }
+    B->cap_n = cn; B->cap_b = cb; B->cap_s = cs; B->cap_cells = cc; B->cap_sort = csort;
+    cudaMemsetAsync(B->cells, 0xff, cc * sizeof(uint2), st);
+    cudaMemsetAsync(B->d_prev_n, 0, sizeof(int), st);
+  }
+  if (ns > 0) {
+    cudaMemcpyAsync(B->d_table, tab.data(), tab.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(B->d_poff, poff.data(), poff.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(B->d_boff, boff.data(), boff.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+  }
+  cudaStreamSynchronize(st);  // host vectors go out of scope
+  B->nt = nt;
+  B->bt = bt;
+  B->total_cells = cells;
+  B->key_bits = key_bits;
+  B->passes = passes;
+  B->last_bits = key_bits - 8 * (passes - 1);
+  B->table_dirty = false;
+  return arh::check_launch("batch prepare");
+}
+
+ar_status enqueue_step(ar_batch* B, cudaStream_t st) {
+  if (B->nt == 0) return AR_OK;
+  ar_ctx* ctx = B->ctx;
+  const int ns = (int)B->scenes.size();
+  const int nt = (int)B->nt, bt = (int)B->bt;
+  cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
+  unsigned g1 = arh::grid_for(nt, kK1Threads);
+  unsigned cap1 = (unsigned)ctx->num_sms * 4;
+  repose_hash_kernel<<<g1 > cap1 ? cap1 : g1, kK1Threads, 0, st>>>(
+      B->d_table, B->d_poff, ns, nt, B->d_prev_n, B->skeys, B->cells, B->keys,
+      (uint32_t*)B->sort_ws, B->passes, B->last_bits);
+  ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
+                                  st, B->sort_ws, B->cap_sort, true);
+  if (s != AR_OK) return s;
+  unsigned g3 = arh::grid_for(nt, 256);
+  unsigned cap3 = (unsigned)ctx->num_sms * 8;
+  scatter_kernel<<<g3 > cap3 ? cap3 : g3, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->skeys,
+                                                        B->svals, B->cells, B->spos, B->svel,
+                                                        B->d_prev_n);
+  int bs = 128;
+  if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
+  collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals,
+                                                       B->cells, B->spos, B->svel, B->pforce);
+  reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
+      B->d_table, B->d_boff, ns, bt, B->pforce, ctx->d_err);
+  B->host_prev_n = nt;
+  return arh::check_launch("step");
+}
+
+ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaStream_t st) {
+  ar_status s = prepare(B, st);
+  if (s != AR_OK) return s;
+  if (B->nt == 0 || n_steps <= 0) return AR_OK;
+  if (!use_graph) {
+    for (int i = 0; i < n_steps; ++i)
+      if ((s = enqueue_step(B, st)) != AR_OK) return s;
+    return AR_OK;
+  }
+  if (!B->graph) {
+    if (!B->cap_stream &&
+        cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      arh::set_error("capture stream creation failed");
+      return AR_ERR_CUDA;
+    }
+    // work already queued on `st` (table uploads, clears) must precede the graph
+    cudaStreamSynchronize(st);
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      arh::set_error("cudaStreamBeginCapture failed");
+      return AR_ERR_CUDA;
+    }
+    ar_status es = enqueue_step(B, B->cap_stream);
+    cudaError_t ce = cudaStreamEndCapture(B->cap_stream, &g);
+    if (es != AR_OK || ce != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      arh::set_error("step capture failed (%s)", cudaGetErrorString(ce));
+      return es != AR_OK ? es : AR_ERR_CUDA;
+    }
+    ce = cudaGraphInstantiate(&B->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) {
+      B->graph = nullptr;
+      arh::set_error("cudaGraphInstantiate failed (%s)", cudaGetErrorString(ce));
+      return AR_ERR_CUDA;
+    }
+  }
+  for (int i = 0; i < n_steps; ++i)
+    if (cudaGraphLaunch(B->graph, st) != cudaSuccess) return arh::check_launch("graph launch");
+  B->host_prev_n = (int)B->nt;
+  return arh::check_launch("graph launch");
+}
+
+uint32_t next_pow2(uint64_t v) {
+  uint32_t p = 1;
+  while (p < v && p < (1u << 31)) p <<= 1;
+  return p;
+}
+
+// Grid of a scene: cell edge (default 2r), origin at the box minimum, cells per axis the next
+// power of two covering the box (or the given log2), then halved on the largest axis while the
+// total exceeds max(2^12, next_pow2(8 N)) -- the wrap keeps any size correct.
+void scene_grid(const ar_scene_desc& D, float origin[3], float cell[3], uint32_t g[3]) {
+  const float c = D.cell_size > 0.f ? D.cell_size : 2.f * D.radius;
+  for (int a = 0; a < 3; ++a) {
+    origin[a] = D.box_min[a];
+    cell[a] = c;
+    if (D.grid_log2[a] > 0) {
+      g[a] = 1u << D.grid_log2[a];
+    } else {
+      double ext = (double)D.box_max[a] - (double)D.box_min[a];
+      uint64_t cells = (uint64_t)std::ceil(ext / c);
+      g[a] = std::max<uint32_t>(4, next_pow2(std::max<uint64_t>(cells, 1)));
+    }
+  }
+  if (D.grid_log2[0] > 0 || D.grid_log2[1] > 0 || D.grid_log2[2] > 0) return;
+  const uint64_t cap = std::max<uint64_t>(1ull << 12, next_pow2(8ull * std::max(D.num_particles, 1)));
+  while ((uint64_t)g[0] * g[1] * g[2] > cap) {
+    int a = 0;
+    for (int k = 1; k < 3; ++k) if (g[k] > g[a]) a = k;
+    if (g[a] <= 4) break;
+    g[a] >>= 1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t ar_scene_footprint(const ar_scene_desc* d) {
+  if (!d) return 0;
+  float o[3], c[3];
+  uint32_t g[3];
+  scene_grid(*d, o, c, g);
+  const size_t n = (size_t)std::max(d->num_particles, 0), b = (size_t)std::max(d->num_bodies, 0);
+  const size_t per_particle = 16 /*rel*/ + 4 * 3 /*keys*/ + 16 * 3 /*spos svel pforce*/ + 8 /*sort tmp*/ + 1;
+  const size_t per_body = 16 * 6 + 4 + 36 + 4;
+  return n * per_particle + b * per_body + (size_t)g[0] * g[1] * g[2] * 8 + 4096;
+}
+
+ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene_init* init,
+                          ar_stream_t stream, ar_scene** out) {
+  if (!ctx || !desc || !init || !out) return AR_ERR_INVALID_ARG;
+  *out = nullptr;
+  const ar_scene_desc& D = *desc;
+  if (D.num_bodies <= 0 || D.num_particles <= 0 || !(D.radius > 0.f) || !(D.dt > 0.f)) {
+    arh::set_error("ar_scene_create: need bodies, particles, radius > 0 and dt > 0");
+    return AR_ERR_INVALID_ARG;
+  }
+  if (D.broadphase != AR_BROADPHASE_GRID && D.broadphase != AR_BROADPHASE_BVH) {
+    arh::set_error("ar_scene_create: unknown broadphase %d", D.broadphase);
+    return AR_ERR_INVALID_ARG;
+  }
+  for (int a = 0; a < 3; ++a)
+    if (D.grid_log2[a] < 0 || D.grid_log2[a] > 20) return AR_ERR_INVALID_ARG;
+  if (D.block_size != 0 && (D.block_size < 32 || D.block_size > 1024 || D.block_size % 32)) {
+    arh::set_error("ar_scene_create: block_size must be a multiple of 32 in [32, 1024]");
+    return AR_ERR_INVALID_ARG;
+  }
+  if (!init->body_pos4 || !init->body_quat4 || !init->body_vel4 || !init->body_angvel4 ||
+      !init->body_mass || !init->body_inv_inertia9 || !init->body_offsets || !init->particle_rel4)
+    return AR_ERR_INVALID_ARG;
+  const int nb = D.num_bodies, n = D.num_particles;
+  if (init->body_offsets[0] != 0 || init->body_offsets[nb] != n) {
+    arh::set_error("ar_scene_create: body_offsets must run from 0 to num_particles");
+    return AR_ERR_INVALID_ARG;
+  }
+  for (int b = 0; b < nb; ++b)
+    if (init->body_offsets[b + 1] < init->body_offsets[b]) {
+      arh::set_error("ar_scene_create: body_offsets must be non-decreasing");
+      return AR_ERR_INVALID_ARG;
+    }
+  ar_scene* s = new ar_scene();
+  s->ctx = ctx;
+  s->desc = D;
+  s->n = n;
+  s->nb = nb;
+  scene_grid(D, s->origin, s->cell, s->gdim);
+  bool ok = alloc(&s->pos, nb) && alloc(&s->quat, nb) && alloc(&s->vel, nb) &&
+            alloc(&s->ang, nb) && alloc(&s->bforce, nb) && alloc(&s->btorque, nb) &&
+            alloc(&s->mass, nb) && alloc(&s->inv_inertia, 9 * (size_t)nb) &&
+            alloc(&s->offsets, nb + 1) && alloc(&s->rel, n);
+  if (!ok) {
+    ar_scene_destroy(s);
+    arh::set_error("ar_scene_create: out of device memory");
+    return AR_ERR_OOM;
+  }
+  // particle rel with the body index in w
+  std::vector<float4> rel(n);
+  for (int b = 0; b < nb; ++b)
+    for (int i = init->body_offsets[b]; i < init->body_offsets[b + 1]; ++i) {
+      const float* r = init->particle_rel4 + 4 * (size_t)i;
+      float w;
+      std::memcpy(&w, &b, 4);
+      rel[i] = make_float4(r[0], r[1], r[2], w);
+    }
+  cudaStream_t st = arh::stream(stream);
+  cudaMemcpyAsync(s->pos, init->body_pos4, 16 * (size_t)nb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->quat, init->body_quat4, 16 * (size_t)nb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->vel, init->body_vel4, 16 * (size_t)nb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->ang, init->body_angvel4, 16 * (size_t)nb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->mass, init->body_mass, 4 * (size_t)nb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->inv_inertia, init->body_inv_inertia9, 36 * (size_t)nb, cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->offsets, init->body_offsets, 4 * (size_t)(nb + 1), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(s->rel, rel.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, st);
+  cudaMemsetAsync(s->bforce, 0, 16 * (size_t)nb, st);
+  cudaMemsetAsync(s->btorque, 0, 16 * (size_t)nb, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    arh::set_error("ar_scene_create: %s", cudaGetErrorString(e));
+    ar_scene_destroy(s);
+    return AR_ERR_CUDA;
+  }
+  *out = s;
+  return AR_OK;
+}
+
+ar_status ar_scene_destroy(ar_scene* s) {
+  if (!s) return AR_ERR_INVALID_ARG;
+  if (s->solo) ar_batch_destroy(s->solo);
+  cudaFree(s->pos); cudaFree(s->quat); cudaFree(s->vel); cudaFree(s->ang);
+  cudaFree(s->bforce); cudaFree(s->btorque); cudaFree(s->mass); cudaFree(s->inv_inertia);
+  cudaFree(s->offsets); cudaFree(s->rel);
+  delete s;
+  return AR_OK;
+}
+
+ar_status ar_scene_download(ar_scene* s, float* h_pos4, float* h_quat4, float* h_vel4,
+                            float* h_ang4, ar_stream_t stream) {
+  if (!s) return AR_ERR_INVALID_ARG;
+  cudaStream_t st = arh::stream(stream);
+  const size_t bytes = 16 * (size_t)s->nb;
+  if (h_pos4) cudaMemcpyAsync(h_pos4, s->pos, bytes, cudaMemcpyDeviceToHost, st);
+  if (h_quat4) cudaMemcpyAsync(h_quat4, s->quat, bytes, cudaMemcpyDeviceToHost, st);
+  if (h_vel4) cudaMemcpyAsync(h_vel4, s->vel, bytes, cudaMemcpyDeviceToHost, st);
+  if (h_ang4) cudaMemcpyAsync(h_ang4, s->ang, bytes, cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    arh::set_error("ar_scene_download: %s", cudaGetErrorString(e));
+    return AR_ERR_CUDA;
+  }
+  return AR_OK;
+}
+
+ar_status ar_scene_get_view(ar_scene* s, ar_scene_view* v) {
+  if (!s || !v) return AR_ERR_INVALID_ARG;
+  v->num_bodies = s->nb;
+  v->num_particles = s->n;
+  v->body_pos4 = (float*)s->pos; v->body_quat4 = (float*)s->quat;
+  v->body_vel4 = (float*)s->vel; v->body_angvel4 = (float*)s->ang;
+  v->body_mass = s->mass; v->body_inv_inertia9 = s->inv_inertia; v->body_offsets = s->offsets;
+  v->particle_rel4 = (float*)s->rel;
+  v->body_force4 = (float*)s->bforce; v->body_torque4 = (float*)s->btorque;
+  return AR_OK;
+}
+
+ar_status ar_scene_grid_info(ar_scene* s, float origin[3], float cell[3], uint32_t dims[3]) {
+  if (!s) return AR_ERR_INVALID_ARG;
+  for (int a = 0; a < 3; ++a) {
+    if (origin) origin[a] = s->origin[a];
+    if (cell) cell[a] = s->cell[a];
+    if (dims) dims[a] = s->gdim[a];
+  }
+  return AR_OK;
+}
+
+static ar_status ensure_solo(ar_scene* s) {
+  if (s->solo) return AR_OK;
+  ar_status st = ar_batch_create(s->ctx, &s->solo);
+  if (st != AR_OK) return st;
+  return ar_batch_set_scenes(s->solo, &s, 1);
+}
+
+ar_status ar_step(ar_ctx* ctx, ar_scene* s, int n_steps, int use_graph, ar_stream_t stream) {
+  if (!ctx || !s || n_steps < 0) return AR_ERR_INVALID_ARG;
+  if (s->desc.broadphase != AR_BROADPHASE_GRID) {
+    arh::set_error("ar_step: the fused step implements the grid broad phase");
+    return AR_ERR_UNSUPPORTED;
+  }
+  ar_status st = ensure_solo(s);
+  if (st != AR_OK) return st;
+  return batch_step(ctx, s->solo, n_steps, use_graph, arh::stream(stream));
+}
+
+ar_status ar_scene_particle_forces(ar_scene* s, float* p_force4, float* p_torque4,
+                                   ar_stream_t stream) {
+  (void)p_torque4;
+  if (!s || !p_force4 || !s->solo || !s->solo->pforce) return AR_ERR_INVALID_ARG;
+  cudaMemcpyAsync(p_force4, s->solo->pforce, 16 * (size_t)s->n, cudaMemcpyDeviceToDevice,
+                  arh::stream(stream));
+  return arh::check_launch("ar_scene_particle_forces");
+}
+
+ar_status ar_scene_step_view(ar_scene* s, ar_step_view* v) {
+  if (!s || !v || !s->solo) return AR_ERR_INVALID_ARG;
+  ar_batch* B = s->solo;
+  v->num_particles = (int)B->nt;
+  v->num_cells = B->total_cells;
+  v->key_bits = B->key_bits;
+  v->sorted_keys = B->skeys;
+  v->sorted_idx = B->svals;
+  v->sorted_pos4 = (float*)B->spos;
+  v->sorted_vel4 = (float*)B->svel;
+  v->particle_force4 = (float*)B->pforce;
+  v->cells2 = (uint32_t*)B->cells;
+  return AR_OK;
+}
+
+ar_status ar_batch_create(ar_ctx* ctx, ar_batch** out) {
+  if (!ctx || !out) return AR_ERR_INVALID_ARG;
+  ar_batch* B = new ar_batch();
+  B->ctx = ctx;
+  *out = B;
+  return AR_OK;
+}
+
+ar_status ar_batch_destroy(ar_batch* B) {
+  if (!B) return AR_ERR_INVALID_ARG;
+  cudaDeviceSynchronize();
+  drop_graph(B);
+  if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
+  free_batch_buffers(B);
+  delete B;
+  return AR_OK;
+}
+
+ar_status ar_batch_set_scenes(ar_batch* B, ar_scene* const* scenes, int n_scenes) {
+  if (!B || n_scenes < 0 || (n_scenes > 0 && !scenes)) return AR_ERR_INVALID_ARG;
+  for (int i = 0; i < n_scenes; ++i) {
+    if (!scenes[i]) return AR_ERR_INVALID_ARG;
+    if (scenes[i]->desc.broadphase != AR_BROADPHASE_GRID) {
+      arh::set_error("ar_batch_set_scenes: the fused step implements the grid broad phase");
+      return AR_ERR_UNSUPPORTED;
+    }
+  }
+  B->scenes.assign(scenes, scenes + n_scenes);
+  B->table_dirty = true;
+  return AR_OK;
+}
+
+ar_status ar_batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph,
+                        ar_stream_t stream) {
+  if (!ctx || !B || n_steps < 0) return AR_ERR_INVALID_ARG;
+  return batch_step(ctx, B, n_steps, use_graph, arh::stream(stream));
+}
+
+int ar_batch_launches_per_step(ar_batch* B) {
+  if (!B) return 0;
+  return 1 /*memset*/ + 1 /*K1*/ + ar_sort::launches(0, B->key_bits, true) + 3;
+}
+
+int ar_scene_launches_per_step(ar_scene* s) {
+  if (!s || !s->solo) return 0;
+  return ar_batch_launches_per_step(s->solo);
+}
+
+}  // extern "C"

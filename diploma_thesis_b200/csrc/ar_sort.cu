@@ -1,0 +1,383 @@
+// (a8) Stable LSD radix sort, onesweep style (one histogram pass + one pass per digit with
+// decoupled look-back).  Replaces cub::DeviceRadixSort::SortPairs on the reference's path
+// (Kernels/particleKernelWrappers.cu:419-534, BVHSource/createMortonCodes.cu:183-218).
+//
+// Pass structure (per 8-bit digit):
+//   * each CTA takes the next tile index from an atomic counter, so every earlier tile is
+//     already running or finished (look-back always makes progress);
+//   * warps rank their items stably with a ballot multi-split (items are visited in input
+//     order: warp w owns a contiguous sub-range, item j of lane l is element j*32 + l);
+//   * per digit, the tile count is published, earlier tiles are looked back through until an
+//     inclusive prefix is found, and the tile's own inclusive prefix is published;
+//   * items are staged in shared memory in (digit, rank) order and written out with
+//     consecutive threads, so each digit run is a coalesced write.
+// Spin waits are bounded; on timeout the kernel raises kErrTimeout and finishes the pass
+// with whatever prefix it has (the result is then garbage, but nothing hangs).
+#include <cuda/atomic>
+
+#include "ar_internal.cuh"
+#include "ar_sort.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kItems = 16;
+constexpr int kTile = kThreads * kItems;  // 4096
+constexpr int kRadix = 256;
+constexpr uint32_t kFlagAgg = 1u << 30;
+constexpr uint32_t kFlagPrefix = 2u << 30;
+constexpr uint32_t kValueMask = (1u << 30) - 1;
+constexpr long kSpinLimit = 1l << 24;
+
+template <class K>
+__device__ __forceinline__ uint32_t digit_of(K key, int shift, uint32_t mask) {
+  return (uint32_t)(key >> shift) & mask;
+}
+
+// ---- histogram of every pass, one read of the keys -----------------------------------------
+template <class K>
+__global__ void __launch_bounds__(kThreads) hist_kernel(const K* __restrict__ keys, int n,
+                                                       int begin_bit, int passes, int last_bits,
+                                                       uint32_t* __restrict__ hist) {
+  __shared__ uint32_t s_hist[ar_sort::kMaxPasses][kRadix];
+  for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) (&s_hist[0][0])[i] = 0;
+  __syncthreads();
+  for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+    K k = keys[i];
+    for (int p = 0; p < passes; ++p) {
+      uint32_t mask = (p == passes - 1) ? ((1u << last_bits) - 1) : 0xffu;
+      atomicAdd(&s_hist[p][digit_of(k, begin_bit + 8 * p, mask)], 1u);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) {
+    uint32_t v = (&s_hist[0][0])[i];
+    if (v) atomicAdd(hist + i, v);
+  }
+}
+
+// Exclusive scan of each pass's 256-bin histogram (one warp per pass).
+__global__ void hist_scan_kernel(uint32_t* __restrict__ hist, int passes) {
+  int p = threadIdx.x >> 5;
+  if (p >= passes) return;
+  uint32_t* h = hist + p * kRadix;
+  int lane = ar::lane_id();
+  uint32_t carry = 0;
+  for (int c = 0; c < kRadix; c += 32) {
+    uint32_t v = h[c + lane], x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    h[c + lane] = carry + x - v;
+    carry += __shfl_sync(0xffffffffu, x, 31);
+  }
+}
+
+// ---- one digit pass ---------------------------------------------------------------------------
+template <class K>
+struct PassSmem {
+  K keys[kTile];
+  uint32_t vals[kTile];
+  uint32_t warp_hist[kWarps][kRadix];
+  uint32_t digit_start[kRadix];  // tile-local exclusive start of each digit
+  uint32_t gofs[kRadix];         // global destination of the digit's first tile element
+  uint32_t tile_id;
+};
+
+template <class K>
+__global__ void __launch_bounds__(kThreads) onesweep_kernel(
+    const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
+    uint32_t* __restrict__ vals_out, int n, int shift, int bits,
+    const uint32_t* __restrict__ digit_base, uint32_t* __restrict__ status,
+    uint32_t* __restrict__ tile_counter, int* __restrict__ err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PassSmem<K>& sm = *reinterpret_cast<PassSmem<K>*>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t mask = (1u << bits) - 1;
+
+  if (tid == 0) sm.tile_id = atomicAdd(tile_counter, 1u);
+  for (int i = tid; i < kWarps * kRadix; i += kThreads) (&sm.warp_hist[0][0])[i] = 0;
+  __syncthreads();
+  const uint32_t tile = sm.tile_id;
+  const long tile_base = (long)tile * kTile;
+
+  // load (coalesced: item j of lane l in warp w is element base + w*kItems*32 + j*32 + l)
+  K key[kItems];
+  uint32_t val[kItems];
+  uint32_t dig[kItems];
+  uint32_t rank[kItems];
+  const long wbase = tile_base + (long)warp * kItems * 32;
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    long g = wbase + j * 32 + lane;
+    if (g < n) {
+      key[j] = keys_in[g];
+      val[j] = vals_in ? vals_in[g] : (uint32_t)g;
+      dig[j] = digit_of(key[j], shift, mask);
+    } else {
+      key[j] = (K)~(K)0;
+      val[j] = 0;
+      dig[j] = kRadix - 1;  // after every valid item of the tile; never written
+    }
+  }
+
+  // stable warp multi-split: peers = lanes holding the same digit
+  const uint32_t lt = (1u << lane) - 1;
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    uint32_t peers = 0xffffffffu;
+    for (int b = 0; b < 8; ++b) {
+      uint32_t bit = (dig[j] >> b) & 1u;
+      uint32_t m = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? m : ~m;
+    }
+    uint32_t before = __popc(peers & lt);
+    int leader = __ffs(peers) - 1;
+    __syncwarp();
+    uint32_t old = sm.warp_hist[warp][dig[j]];
+    __syncwarp();
+    if (lane == leader) sm.warp_hist[warp][dig[j]] = old + __popc(peers);
+    rank[j] = old + before;
+  }
+  __syncthreads();
+
+  // per digit: exclusive over warps, tile count
+  const int d = tid;  // kThreads == kRadix
+  uint32_t tile_count = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    uint32_t c = sm.warp_hist[w][d];
+    sm.warp_hist[w][d] = tile_count;
+    tile_count += c;
+  }
+
+  // publish aggregate / look back / publish inclusive prefix
+  {
+    cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(long)tile * kRadix + d]);
+    uint32_t excl = 0;
+    if (tile == 0) {
+      mine.store(kFlagPrefix | tile_count, cuda::memory_order_relaxed);
+    } else {
+      mine.store(kFlagAgg | tile_count, cuda::memory_order_relaxed);
+      long k = (long)tile - 1;
+      long spins = 0;
+      while (k >= 0) {
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> other(status[k * kRadix + d]);
+        uint32_t v = other.load(cuda::memory_order_relaxed);
+        uint32_t flag = v & ~kValueMask;
+        if (flag == 0) {
+          if (++spins > kSpinLimit) {
+            ar::raise_error(err, ar::kErrTimeout);
+            break;
+          }
+          if (spins > 64) __nanosleep(64);
+          continue;
+        }
+        excl += v & kValueMask;
+        if (flag == kFlagPrefix) break;
+        --k;
+      }
+      mine.store(kFlagPrefix | ((excl + tile_count) & kValueMask), cuda::memory_order_relaxed);
+    }
+    sm.gofs[d] = digit_base[d] + excl;
+  }
+
+  // tile-local exclusive scan over digits (block scan of one value per thread)
+  {
+    uint32_t x = tile_count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    __shared__ uint32_t s_wsum[kWarps];
+    if (lane == 31) s_wsum[warp] = x;
+    __syncthreads();
+    uint32_t add = 0;
+    for (int w = 0; w < warp; ++w) add += s_wsum[w];
+    sm.digit_start[d] = add + x - tile_count;
+  }
+  __syncthreads();
+
+  // stage in (digit, rank) order
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    long g = wbase + j * 32 + lane;
+    if (g < n) {
+      uint32_t pos = sm.digit_start[dig[j]] + sm.warp_hist[warp][dig[j]] + rank[j];
+      sm.keys[pos] = key[j];
+      sm.vals[pos] = val[j];
+    }
+  }
+  __syncthreads();
+
+  // coalesced write-out
+  long valid = n - tile_base;
+  int count = valid < kTile ? (int)valid : kTile;
+  for (int i = tid; i < count; i += kThreads) {
+    K k = sm.keys[i];
+    uint32_t dd = digit_of(k, shift, mask);
+    uint32_t dst = sm.gofs[dd] + (uint32_t)i - sm.digit_start[dd];
+    keys_out[dst] = k;
+    vals_out[dst] = sm.vals[i];
+  }
+}
+
+// external_hist: the caller already cleared the workspace head (ar_sort::clear) and
+// accumulated the per-pass histograms into it (ar_sort::hist_accumulate), e.g. fused into the
+// kernel that produced the keys.
+template <class K>
+ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* keys_out,
+                    uint32_t* vals_out, int n, int begin_bit, int end_bit, cudaStream_t st,
+                    void* ws, size_t ws_bytes, bool external_hist = false) {
+  const int total_bits = end_bit - begin_bit;
+  const int passes = (total_bits + 7) / 8;
+  const int last_bits = total_bits - 8 * (passes - 1);
+  const long tiles = ((long)n + kTile - 1) / kTile;
+  ar_sort::Layout L = ar_sort::layout(n, sizeof(K), passes);
+  if (ws_bytes < L.total) {
+    arh::set_error("radix sort: workspace too small");
+    return AR_ERR_INVALID_ARG;
+  }
+  char* base = (char*)ws;
+  uint32_t* hist = (uint32_t*)(base + L.hist);
+  uint32_t* counters = (uint32_t*)(base + L.counters);
+  uint32_t* status = (uint32_t*)(base + L.status);
+  K* tmp_keys = (K*)(base + L.tmp_keys);
+  uint32_t* tmp_vals = (uint32_t*)(base + L.tmp_vals);
+  int* err = ctx ? ctx->d_err : nullptr;
+
+  if (!external_hist) {
+  cudaMemsetAsync(base, 0, L.status + (size_t)passes * tiles * kRadix * sizeof(uint32_t), st);
+  unsigned hgrid = (unsigned)((n + kThreads * 8 - 1) / (kThreads * 8));
+  unsigned cap = (unsigned)(ctx ? ctx->num_sms : 148) * 4;
+  if (hgrid > cap) hgrid = cap;
+  if (hgrid < 1) hgrid = 1;
+  hist_kernel<K><<<hgrid, kThreads, 0, st>>>(keys_in, n, begin_bit, passes, last_bits, hist);
+  }
+  hist_scan_kernel<<<1, 32 * ar_sort::kMaxPasses, 0, st>>>(hist, passes);
+
+  const size_t smem = sizeof(PassSmem<K>);
+  // ping-pong so that the last pass lands in keys_out
+  const K* src_k = keys_in;
+  const uint32_t* src_v = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    bool to_out = ((passes - 1 - p) % 2) == 0;
+    K* dk = to_out ? keys_out : tmp_keys;
+    uint32_t* dv = to_out ? vals_out : tmp_vals;
+    int bits = (p == passes - 1) ? last_bits : 8;
+    onesweep_kernel<K><<<(unsigned)tiles, kThreads, smem, st>>>(
+        src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
+        status + (size_t)p * tiles * kRadix, counters + p, err);
+    src_k = dk;
+    src_v = dv;
+  }
+  return arh::check_launch("radix sort");
+}
+
+template <class K>
+ar_status sort_entry(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* keys_out,
+                     uint32_t* vals_out, int n, int begin_bit, int end_bit, ar_stream_t stream) {
+  const int kbits = 8 * (int)sizeof(K);
+  if (!ctx || n < 0 || begin_bit < 0 || end_bit > kbits || begin_bit > end_bit)
+    return AR_ERR_INVALID_ARG;
+  if (n > 0 && (!keys_in || !keys_out || !vals_out)) return AR_ERR_INVALID_ARG;
+  if (n > 0 && ((const void*)keys_in == (const void*)keys_out ||
+                (vals_in && (const void*)vals_in == (const void*)vals_out))) {
+    arh::set_error("radix sort: outputs must not alias inputs");
+    return AR_ERR_INVALID_ARG;
+  }
+  if (n >= (1 << 30)) {
+    arh::set_error("radix sort: n must be < 2^30");
+    return AR_ERR_INVALID_ARG;
+  }
+  cudaStream_t st = arh::stream(stream);
+  if (n == 0) return AR_OK;
+  if (begin_bit == end_bit) {  // nothing to sort: copy through
+    cudaMemcpyAsync(keys_out, keys_in, (size_t)n * sizeof(K), cudaMemcpyDeviceToDevice, st);
+    if (vals_in)
+      cudaMemcpyAsync(vals_out, vals_in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+    else
+      ar_sort::iota(vals_out, n, st);
+    return arh::check_launch("radix sort copy");
+  }
+  const int passes = (end_bit - begin_bit + 7) / 8;
+  ar_sort::Layout L = ar_sort::layout(n, sizeof(K), passes);
+  void* ws = arh::scratch(ctx, L.total);
+  if (!ws) return AR_ERR_OOM;
+  return sort_impl<K>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit, st, ws,
+                      L.total);
+}
+
+__global__ void iota_kernel(uint32_t* v, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+}  // namespace
+
+namespace ar_sort {
+
+void init() {
+  cudaFuncSetAttribute(onesweep_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PassSmem<uint32_t>));
+  cudaFuncSetAttribute(onesweep_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PassSmem<uint64_t>));
+}
+
+Layout layout(long n, size_t key_bytes, int passes) {
+  const long tiles = (n + kTile - 1) / kTile;
+  auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  Layout L;
+  L.hist = 0;
+  L.counters = up(L.hist + (size_t)kMaxPasses * kRadix * 4);
+  L.status = up(L.counters + kMaxPasses * 4);
+  L.tmp_keys = up(L.status + (size_t)passes * tiles * kRadix * 4);
+  L.tmp_vals = up(L.tmp_keys + (size_t)n * key_bytes);
+  L.total = up(L.tmp_vals + (size_t)n * 4);
+  return L;
+}
+
+void iota(uint32_t* v, int n, cudaStream_t st) {
+  iota_kernel<<<arh::grid_for(n, 256) > 4096 ? 4096 : arh::grid_for(n, 256), 256, 0, st>>>(v, n);
+}
+
+ar_status sort_u32(ar_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in,
+                   uint32_t* keys_out, uint32_t* vals_out, int n, int begin_bit, int end_bit,
+                   cudaStream_t st, void* ws, size_t ws_bytes, bool external_hist) {
+  if (n == 0) return AR_OK;
+  return sort_impl<uint32_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
+                             st, ws, ws_bytes, external_hist);
+}
+
+size_t clear_bytes(long n, int passes) {
+  const long tiles = (n + kTile - 1) / kTile;
+  Layout L = layout(n, 4, passes);
+  return L.status + (size_t)passes * tiles * kRadix * sizeof(uint32_t);
+}
+
+int launches(int begin_bit, int end_bit, bool external_hist) {
+  return (external_hist ? 1 : 3) + (end_bit - begin_bit + 7) / 8;
+}
+
+}  // namespace ar_sort
+
+extern "C" {
+
+ar_status ar_radix_sort_pairs_u32(ar_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in,
+                                  uint32_t* keys_out, uint32_t* vals_out, int n, int begin_bit,
+                                  int end_bit, ar_stream_t stream) {
+  return sort_entry<uint32_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
+                              stream);
+}
+
+ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in,
+                                  uint64_t* keys_out, uint32_t* vals_out, int n, int begin_bit,
+                                  int end_bit, ar_stream_t stream) {
+  return sort_entry<uint64_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
+                              stream);
+}
+
+}  // extern "C"

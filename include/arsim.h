@@ -1,0 +1,412 @@
+/*
+ * arsim.h -- C ABI of libarsim.so, a B200 (sm_100a) implementation of AR_Sim's per-step
+ * rigid-body pipeline (ATriantafyllopoulos/Diploma_Thesis).
+ *
+ * Conventions
+ *  - Every entry point returns ar_status; none exits or aborts.  ar_last_error() gives the
+ *    message of the last failure on the calling thread.
+ *  - Array arguments are DEVICE pointers unless the name starts with `h_`.  Layouts are the
+ *    reference's: "4" suffix = float4 per element (x, y, z, w) with w ignored on input,
+ *    "9" = 3x3 matrix stored as glm::mat3 (column-major, 9 floats), quaternions are glm::quat
+ *    memory order (x, y, z, w), AABB = 8 floats {min.x, min.y, min.z, max.x, max.y, max.z,
+ *    pad, pad} (the reference's 16-byte aligned `struct AABB`, BVHSource/BVHcreation.h:33-37).
+ *  - Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and is
+ *    asynchronous.  Nothing allocates or synchronises in steady state: temporaries come from
+ *    the context's grow-only scratch arena, sized on first use.
+ *  - Device-side failures (a bounded spin wait giving up, NaN state) set a word in the
+ *    context that ar_ctx_status() reads back.
+ *
+ * Each declaration names the reference function it replaces (file:line within AR_Sim/).
+ */
+#ifndef ARSIM_H
+#define ARSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AR_API __attribute__((visibility("default")))
+
+typedef enum ar_status {
+  AR_OK = 0,
+  AR_ERR_INVALID_ARG = 1,
+  AR_ERR_OOM = 2,
+  AR_ERR_TIMEOUT = 3,     /* a device-side bounded wait gave up */
+  AR_ERR_NAN = 4,         /* non-finite body state detected */
+  AR_ERR_CUDA = 5,
+  AR_ERR_UNSUPPORTED = 6,
+  AR_ERR_OVERFLOW = 7     /* an output buffer (pair list) was too small */
+} ar_status;
+
+typedef void* ar_stream_t; /* cudaStream_t */
+
+/* Simulation parameters.  Byte-for-byte the reference's `struct SimParams`
+ * (Kernels/particleSystem.cuh:27-55), 128 bytes, so a SimParams* may be passed directly. */
+typedef struct ar_sim_params {
+  float collider_pos[3];
+  float collider_radius;
+  float gravity[3];
+  float global_damping;
+  float particle_radius;
+  uint32_t grid_size[3];
+  uint32_t num_cells;
+  float world_origin[3];
+  float cell_size[3];
+  uint32_t num_bodies;
+  uint32_t max_particles_per_cell;
+  float spring;
+  float damping;
+  float shear;
+  float attraction;
+  float boundary_damping;
+  float ar_restitution;
+  float rb_restitution;
+  float ar_friction;
+  float rb_friction;
+  float w_damping;
+  float v_damping;
+} ar_sim_params;
+
+/* ---- context ------------------------------------------------------------------------- */
+typedef struct ar_ctx ar_ctx;
+
+/* Replaces the reference's implicit global CUDA state (cudaInit, Particles/
+ * ParticleAuxiliaryFunctions.h:3) and its __constant__ SimParams (Kernels/particleKernels.cu:42).
+ * Selects `device` and creates the per-device error word. */
+AR_API ar_status ar_ctx_create(int device, ar_ctx** out);
+AR_API ar_status ar_ctx_destroy(ar_ctx* ctx);
+/* Synchronises `stream`, returns (and clears) any device-side error raised since the last
+ * call: AR_ERR_TIMEOUT, AR_ERR_NAN, AR_ERR_OVERFLOW or AR_OK.  Replaces checkCudaErrors'
+ * exit() (Libs/common/inc/helper_cuda.h:967-981). */
+AR_API ar_status ar_ctx_status(ar_ctx* ctx, ar_stream_t stream);
+/* Pre-size the scratch arena (so later calls inside a CUDA graph capture never grow it). */
+AR_API ar_status ar_ctx_reserve(ar_ctx* ctx, size_t bytes);
+AR_API const char* ar_last_error(void);
+AR_API const char* ar_version(void);
+
+/* ---- (a6) scene bounding box -------------------------------------------------------------
+ * findAABBCub (BVHSource/createMortonCodes.cu:65-107): min and max over all four lanes of
+ * pos4[0..n), starting from +/-2139095040.0f (the reference's int `inf` macro, :10).
+ * Writes one float4 each to d_min4 / d_max4 (device). */
+AR_API ar_status ar_scene_aabb(ar_ctx* ctx, const float* pos4, int n, float* d_min4,
+                               float* d_max4, ar_stream_t stream);
+
+/* ---- (a7) Morton codes ---------------------------------------------------------------------
+ * generateMortonCodes (BVHSource/BVHkernels.cu:646-716): normalise each position to the box,
+ * 10 bits per axis, code = x*4 + y*2 + z interleave; idx[i] = i.  The box comes from device
+ * memory (the createMortonCodes path, createMortonCodes.cu:109-251) ... */
+AR_API ar_status ar_morton30(ar_ctx* ctx, const float* pos4, int n, const float* d_min4,
+                             const float* d_max4, uint32_t* codes, int32_t* idx,
+                             ar_stream_t stream);
+/* ... or by value from the host (createMortonCodesPreallocated, createMortonCodes.cu:255-347). */
+AR_API ar_status ar_morton30_box(ar_ctx* ctx, const float* pos4, int n, const float h_min4[4],
+                                 const float h_max4[4], uint32_t* codes, int32_t* idx,
+                                 ar_stream_t stream);
+/* 63-bit variant (21 bits per axis), new: the reference only reserves CODE_LENGTH 21
+ * (BVHSource/BVHkernels.cu:4-5).  Same normalisation, scale 2^21, clamp [0, 2^21-1]. */
+AR_API ar_status ar_morton63(ar_ctx* ctx, const float* pos4, int n, const float* d_min4,
+                             const float* d_max4, uint64_t* codes, int32_t* idx,
+                             ar_stream_t stream);
+
+/* ---- (a8) stable LSD radix sort ------------------------------------------------------------
+ * Replaces cub::DeviceRadixSort::SortPairs (Kernels/particleKernelWrappers.cu:419-534,
+ * BVHSource/createMortonCodes.cu:183-218).  Sorts (key, value) pairs by key bits
+ * [begin_bit, end_bit) -- the reference always sorts all 32 bits; passing the number of
+ * significant bits gives the same order with fewer passes.  Stable: equal keys keep input
+ * order.  Inputs are left intact; results go to keys_out/vals_out (vals_in may be NULL to
+ * mean the identity 0..n-1).  Onesweep: one histogram pass plus one pass per 8-bit digit
+ * with decoupled look-back. */
+AR_API ar_status ar_radix_sort_pairs_u32(ar_ctx* ctx, const uint32_t* keys_in,
+                                         const uint32_t* vals_in, uint32_t* keys_out,
+                                         uint32_t* vals_out, int n, int begin_bit, int end_bit,
+                                         ar_stream_t stream);
+AR_API ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in,
+                                         const uint32_t* vals_in, uint64_t* keys_out,
+                                         uint32_t* vals_out, int n, int begin_bit, int end_bit,
+                                         ar_stream_t stream);
+
+/* ---- (a9) Karras LBVH hierarchy --------------------------------------------------------------
+ * kernelConstructRadixTreeSoA (BVHSource/BVHSoAKernels.cu:7-99) with longestCommonPrefix
+ * (BVHSource/BVHAuxiliary.cuh:31-43): leaves at [0, n), internal node i at n + i, root at n;
+ * duplicate codes are tie-broken by the index prefix (clz(i ^ j) + 32).  Arrays have 2n-1
+ * entries.  Writes is_leaf, left, right, parent, min_r, max_r of the internal nodes and the
+ * parent of every node. */
+AR_API ar_status ar_lbvh_build(ar_ctx* ctx, const uint32_t* sorted_codes, int n,
+                               uint8_t* is_leaf, int32_t* left, int32_t* right,
+                               int32_t* parent, int32_t* min_r, int32_t* max_r,
+                               ar_stream_t stream);
+/* 63-bit codes: same algorithm, prefix over 64 bits, ties broken by clz(i ^ j) + 64. */
+AR_API ar_status ar_lbvh_build64(ar_ctx* ctx, const uint64_t* sorted_codes, int n,
+                                 uint8_t* is_leaf, int32_t* left, int32_t* right,
+                                 int32_t* parent, int32_t* min_r, int32_t* max_r,
+                                 ar_stream_t stream);
+
+/* ---- (a10) leaves ---------------------------------------------------------------------------
+ * kernelConstructLeafNodesSoA + initializeRadii (BVHSoAKernels.cu:108-138,
+ * Kernels/particleKernels.cu:694-708): leaf i gets is_leaf = 1, min_r = max_r = i,
+ * cms4[i] = pos4[sorted_idx[i]], bounds[i] = cms +/- radius, radii[i] = radius. */
+AR_API ar_status ar_lbvh_leaves(ar_ctx* ctx, int n, const int32_t* sorted_idx,
+                                const float* pos4, float radius, uint8_t* is_leaf,
+                                int32_t* min_r, int32_t* max_r, float* cms4, float* bounds8,
+                                float* radii, ar_stream_t stream);
+
+/* ---- (a11) bottom-up AABB refit --------------------------------------------------------------
+ * kernelConstructInternalNodesSoA (BVHSoAKernels.cu:148-176): one thread per leaf climbs to
+ * the root; the second thread to reach a node merges its children's boxes.  Unlike the
+ * reference, the arrival counter is ordered by release/acquire fences, so the merge always
+ * sees both children's final boxes. */
+AR_API ar_status ar_lbvh_refit(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
+                               const int32_t* parent, float* bounds8, ar_stream_t stream);
+
+/* ---- (a12) BVH traversal ---------------------------------------------------------------------
+ * collideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:100-244) with collideStaticSpheresBVH
+ * (:24-98): per sorted leaf, DEM force against every overlapping leaf of another body;
+ * p_force4 / p_torque4 / p_positions4 are written at the particle's original index
+ * (sorted_idx[leaf]); vel4 is the unsorted particle velocity.  Traversal is stackless
+ * (parent links), so no per-thread stack limits the tree depth. */
+AR_API ar_status ar_collide_bvh_dem(ar_ctx* ctx, const ar_sim_params* params,
+                                    const int32_t* rb_idx, const float* rel4,
+                                    const float* vel4, const uint8_t* is_leaf,
+                                    const int32_t* left, const int32_t* right,
+                                    const int32_t* parent, const float* cms4,
+                                    const float* bounds8, const int32_t* sorted_idx,
+                                    const float* radii, int n, float* p_force4,
+                                    float* p_torque4, float* p_positions4, ar_stream_t stream);
+/* FindRigidBodyCollisionsBVHKernel (Kernels/RB_BVHKernels.cu:760-876): per particle the
+ * deepest contact with a later leaf (max_r >= leaf) of another body.  contact_distance is
+ * read as the starting threshold and updated, like the reference. */
+AR_API ar_status ar_find_contacts_bvh(ar_ctx* ctx, const int32_t* rb_idx,
+                                      const uint8_t* is_leaf, const int32_t* left,
+                                      const int32_t* right, const int32_t* parent,
+                                      const int32_t* max_r, const float* cms4,
+                                      const float* bounds8, const int32_t* sorted_idx,
+                                      const float* radii, int n, float* contact_distance,
+                                      int32_t* colliding_particle, int32_t* colliding_body,
+                                      ar_stream_t stream);
+
+/* Contact-pair sets (new; used to prove broad-phase equality).  Emits each unordered pair
+ * {i, j} (original particle indices, i < j) with |p_i - p_j| < 2r and rb_idx[i] != rb_idx[j],
+ * in unspecified order.  pairs2 holds capacity (i, j) int pairs; *d_count (device) receives
+ * the number found; AR_ERR_OVERFLOW is raised through ar_ctx_status if it exceeds capacity. */
+AR_API ar_status ar_pairs_bvh(ar_ctx* ctx, float radius, const int32_t* rb_idx,
+                              const uint8_t* is_leaf, const int32_t* left,
+                              const int32_t* right, const int32_t* parent, const float* cms4,
+                              const float* bounds8, const int32_t* sorted_idx, int n,
+                              int32_t* pairs2, int capacity, int32_t* d_count,
+                              ar_stream_t stream);
+AR_API ar_status ar_pairs_grid(ar_ctx* ctx, const ar_sim_params* params,
+                               const int32_t* rb_idx, const float* sorted_pos4,
+                               const uint32_t* grid_idx, const uint32_t* cell_start,
+                               const uint32_t* cell_end, int n, int32_t* pairs2, int capacity,
+                               int32_t* d_count, ar_stream_t stream);
+
+/* ---- (a13) uniform-grid hash -----------------------------------------------------------------
+ * calcHash / calcHashD (Kernels/particleKernelWrappers.cu:195-211, Kernels/particleKernels.cu:
+ * 150-189): cell = floor((p - world_origin) / cell_size), wrapped with & (grid_size - 1)
+ * (grid sizes must be powers of two), hash = z*Gy*Gx + y*Gx + x; idx[i] = i. */
+AR_API ar_status ar_calc_hash(ar_ctx* ctx, const ar_sim_params* params, const float* pos4,
+                              int n, uint32_t* hash, uint32_t* idx, ar_stream_t stream);
+
+/* ---- (a14) reorder + cell ranges ---------------------------------------------------------------
+ * reorderDataAndFindCellStart (Kernels/particleKernelWrappers.cu:213-254, kernel
+ * Kernels/particleKernels.cu:193-258): clears cell_start[0..num_cells) to 0xffffffff, then
+ * records the first/one-past-last sorted slot of every occupied cell and gathers
+ * sorted_pos4/sorted_vel4 = pos4/vel4[sorted_idx].  cell_end is left stale for empty cells,
+ * like the reference. */
+AR_API ar_status ar_reorder_cells(ar_ctx* ctx, const uint32_t* sorted_hash,
+                                  const uint32_t* sorted_idx, const float* pos4,
+                                  const float* vel4, int n, uint32_t num_cells,
+                                  uint32_t* cell_start, uint32_t* cell_end, float* sorted_pos4,
+                                  float* sorted_vel4, ar_stream_t stream);
+
+/* ---- (a15) DEM contact forces on the grid ------------------------------------------------------
+ * FindAndHandleRigidBodyCollisionsUniformGridKernel (RigidBodies/UniformGridDEM.cu:57-241):
+ * per sorted particle, the 27 neighbour cells in z, y, x order (-1..1), occupants in sorted
+ * order, skipping itself and particles of its own body; for d < 2r:
+ *   F += -spring (2r - d) n + damping v_rel + shear v_t + attraction p_rel
+ * summed per cell then across cells; then p_force4[orig] += F and
+ * p_torque4[orig] += rel4[orig] x F (accumulating, like the reference).  No atomics. */
+AR_API ar_status ar_collide_grid_dem(ar_ctx* ctx, const ar_sim_params* params,
+                                     const int32_t* rb_idx, const float* sorted_pos4,
+                                     const float* sorted_vel4, const float* rel4,
+                                     const uint32_t* grid_idx, const uint32_t* cell_start,
+                                     const uint32_t* cell_end, int n, float* p_force4,
+                                     float* p_torque4, ar_stream_t stream);
+
+/* ---- (a16/a17) per-body reduction --------------------------------------------------------------
+ * Replaces ReducePerParticleImpulses + CombineReducedImpulses (RigidBodies/UniformGridDEM.cu:
+ * 421-666) and ReduceRigidBodyVariables (Kernels/rigidBodyKernels.cu:861-1043): a fixed-order
+ * segmented sum of p_force4 / p_torque4 over each body's particles [offsets[b], offsets[b+1])
+ * (one warp per body: lane l sums elements l, l+32, ... in order, then a xor-shuffle tree
+ * 16, 8, 4, 2, 1), written to body_force4 / body_torque4.  Deterministic and independent of
+ * the other bodies.  The reference instead differences a global float prefix sum and reads
+ * the segment start one element late (:440-441); this entry point sums each segment exactly
+ * once. */
+AR_API ar_status ar_reduce_bodies(ar_ctx* ctx, const float* p_force4, const float* p_torque4,
+                                  const int32_t* offsets, int num_bodies, float* body_force4,
+                                  float* body_torque4, ar_stream_t stream);
+/* ReducePerParticleImpulses semantics on top of ar_reduce_bodies: rb_vel4 += F / mass,
+ * rb_ang4 += inv_inertia9 * tau (CombineReducedImpulses, UniformGridDEM.cu:421-460). */
+AR_API ar_status ar_reduce_impulses(ar_ctx* ctx, const float* p_force4, const float* p_torque4,
+                                    const int32_t* offsets, int num_bodies, float* rb_vel4,
+                                    float* rb_ang4, const float* rb_mass,
+                                    const float* rb_inv_inertia9, ar_stream_t stream);
+
+/* ---- (a2) body integration, reference semantics --------------------------------------------------
+ * GPUintegratorKernel (Kernels/rigidBodyKernels.cu:262-348): x += v dt; q = axis-angle
+ * rotation of omega*dt (identity below 1e-5 rad); current inverse inertia R I^-1 R^T;
+ * cumulative quaternion and 4x4 model matrix; v += gravity (per step, no dt, as the
+ * reference does); omega *= w_damping.  model16 / cum_quat4 may be NULL. */
+AR_API ar_status ar_integrate_reference(ar_ctx* ctx, const ar_sim_params* params, float dt,
+                                        int num_bodies, float* cms4, float* vel4, float* ang4,
+                                        float* quat4, const float* inv_inertia9,
+                                        float* cur_inv_inertia9, float* model16,
+                                        float* cum_quat4, const float* mass,
+                                        ar_stream_t stream);
+
+/* ---- (a4) particle re-posing, reference semantics -------------------------------------------------
+ * computeGlobalAttributes + resetQuaternionKernel (Kernels/rigidBodyKernels.cu:386-456):
+ * rel4 <- R(q) rel4 (in place), pos4 = rel + cm, vel4 = v + omega x rel; then q <- identity. */
+AR_API ar_status ar_global_attributes(ar_ctx* ctx, int n, int num_bodies, const float* cms4,
+                                      const float* rb_vel4, const float* rb_ang4, float* quat4,
+                                      const int32_t* rb_idx, float* rel4, float* pos4,
+                                      float* vel4, ar_stream_t stream);
+
+/* ---- (a18) wall collisions, reference semantics ---------------------------------------------------
+ * WallCollisionWrapper (WallCollisions.cu:338-597): per particle the deepest of the six box
+ * walls it penetrates while its body moves toward that wall (walls tested +x, +y, +z, -x, -y,
+ * -z; a later wall must be strictly deeper); per body the deepest such contact (ties -> the
+ * larger particle index); then a Baraff e = 1 impulse on the body's linear and angular
+ * velocity (HandleWallCollisionKernelUnmapped, :201-276).  One gather per body, no sorts.
+ * offsets[b]..offsets[b+1] are the body's particles. */
+AR_API ar_status ar_walls_reference(ar_ctx* ctx, float radius, const float* particle_pos4,
+                                    const float* rb_pos4, const float h_min_pos3[3],
+                                    const float h_max_pos3[3], float* rb_vel4, float* rb_ang4,
+                                    const float* inv_inertia9, const float* rb_mass,
+                                    const int32_t* rb_idx, const int32_t* offsets,
+                                    int num_bodies, int n, ar_stream_t stream);
+
+/* ==== fused step: scenes and batches ================================================================
+ * A scene is one independent rigid-body world resident on the device.  ar_step advances it
+ * with the fused pipeline (re-pose + hash, onesweep sort, scatter + cell ranges, DEM
+ * gather + walls, fixed-order body reduction + integration), PHYSICAL semantics:
+ *   v += (g + F/m) dt,  omega += I_w^-1 tau dt,  x += v dt,
+ *   q += dt/2 (omega, 0) q, normalised;  I_w^-1 = R I_b^-1 R^T,
+ * with box walls as DEM springs (the wall is a static sphere surface at the plane).
+ * Body-frame particle offsets stay constant (no incremental re-rotation drift).
+ * Replaces ParticleSystem::updateUniformGridDEM (RigidBodies/UniformGridUpdate.cpp:939-999)
+ * and updateRigidBodies (RigidBodies/BVHUpdate.cpp:5-438). */
+
+enum { AR_BROADPHASE_GRID = 0, AR_BROADPHASE_BVH = 1 };
+
+typedef struct ar_scene_desc {
+  int num_bodies;
+  int num_particles;
+  float radius;          /* particle radius r; contact distance 2r */
+  float box_min[3];      /* walls */
+  float box_max[3];
+  float gravity[3];
+  float dt;
+  float spring;          /* k */
+  float damping;         /* dashpot coefficient on relative velocity */
+  float shear;           /* coefficient on tangential relative velocity */
+  float attraction;
+  int broadphase;        /* AR_BROADPHASE_GRID or AR_BROADPHASE_BVH */
+  float cell_size;       /* grid cell edge; 0 -> 2r */
+  int grid_log2[3];      /* log2 grid cells per axis (wrapped); 0 -> derived from the box */
+  int block_size;        /* threads per CTA for the per-particle kernels; 0 -> 128 */
+} ar_scene_desc;
+
+typedef struct ar_scene ar_scene;
+
+/* Host-side initial state, all arrays host memory:
+ *  body_pos4[B], body_quat4[B] (x,y,z,w), body_vel4[B], body_angvel4[B], body_mass[B],
+ *  body_inv_inertia9[B] (body frame, glm::mat3 layout), body_offsets[B+1] (particles of body
+ *  b are [off[b], off[b+1]), particle_rel4[N] (body-frame offsets from the body centre). */
+typedef struct ar_scene_init {
+  const float* body_pos4;
+  const float* body_quat4;
+  const float* body_vel4;
+  const float* body_angvel4;
+  const float* body_mass;
+  const float* body_inv_inertia9;
+  const int32_t* body_offsets;
+  const float* particle_rel4;
+} ar_scene_init;
+
+AR_API ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc,
+                                 const ar_scene_init* init, ar_stream_t stream,
+                                 ar_scene** out);
+AR_API ar_status ar_scene_destroy(ar_scene* scene);
+/* Device bytes a scene with this description keeps resident (state + its share of the
+ * step workspace); used for HBM-budget admission. */
+AR_API size_t ar_scene_footprint(const ar_scene_desc* desc);
+/* Copy body state to host arrays (any may be NULL). */
+AR_API ar_status ar_scene_download(ar_scene* scene, float* h_body_pos4, float* h_body_quat4,
+                                   float* h_body_vel4, float* h_body_angvel4,
+                                   ar_stream_t stream);
+/* Device pointers of the scene's resident arrays (for tests / zero-copy consumers). */
+typedef struct ar_scene_view {
+  int num_bodies, num_particles;
+  float* body_pos4; float* body_quat4; float* body_vel4; float* body_angvel4;
+  float* body_mass; float* body_inv_inertia9; int32_t* body_offsets;
+  float* particle_rel4;           /* w holds the body index (int bits) */
+  float* body_force4; float* body_torque4;   /* last step's per-body totals */
+} ar_scene_view;
+AR_API ar_status ar_scene_get_view(ar_scene* scene, ar_scene_view* out);
+
+/* Grid the scene was given: origin, cell edge and cells per axis (powers of two). */
+AR_API ar_status ar_scene_grid_info(ar_scene* scene, float origin[3], float cell[3],
+                                    uint32_t dims[3]);
+
+/* Device pointers into the workspace of the scene's last ar_step (for parity tests and
+ * consumers that want the sorted state): the sorted cell keys and the particle index of each
+ * sorted slot, sorted positions (w = body index, int bits) and velocities, the per-particle
+ * DEM + wall force at the original index, and the cell table as (start, end) pairs
+ * (start = 0xffffffff for an empty cell). */
+typedef struct ar_step_view {
+  int num_particles;
+  uint64_t num_cells;
+  int key_bits;
+  uint32_t* sorted_keys;
+  uint32_t* sorted_idx;
+  float* sorted_pos4;
+  float* sorted_vel4;
+  float* particle_force4;
+  uint32_t* cells2;
+} ar_step_view;
+AR_API ar_status ar_scene_step_view(ar_scene* scene, ar_step_view* out);
+
+/* Advance one scene by n_steps (one launch sequence per step; captured into a CUDA graph on
+ * first use when use_graph != 0). */
+AR_API ar_status ar_step(ar_ctx* ctx, ar_scene* scene, int n_steps, int use_graph,
+                         ar_stream_t stream);
+
+/* Per-particle DEM + wall force of the last step (original particle order): copies N float4
+ * to a device buffer.  p_torque4 is reserved and may be NULL (torques are summed per body
+ * from the forces, see ar_scene_view.body_torque4). */
+AR_API ar_status ar_scene_particle_forces(ar_scene* scene, float* p_force4, float* p_torque4,
+                                          ar_stream_t stream);
+
+/* A batch advances many scenes with one launch per stage: keys of all scenes are sorted
+ * together in a global cell space (scene cell base + local cell), every per-particle kernel
+ * is a grid-stride loop over the concatenation, and the step is a CUDA graph.  Each scene's
+ * result is bit-identical to stepping it alone. */
+typedef struct ar_batch ar_batch;
+AR_API ar_status ar_batch_create(ar_ctx* ctx, ar_batch** out);
+AR_API ar_status ar_batch_destroy(ar_batch* batch);
+/* Replace the batch's member list (scenes stay resident and owned by the caller). */
+AR_API ar_status ar_batch_set_scenes(ar_batch* batch, ar_scene* const* scenes, int n_scenes);
+AR_API ar_status ar_batch_step(ar_ctx* ctx, ar_batch* batch, int n_steps, int use_graph,
+                               ar_stream_t stream);
+/* Number of kernel launches one step of this batch issues (for launch accounting). */
+AR_API int ar_batch_launches_per_step(ar_batch* batch);
+AR_API int ar_scene_launches_per_step(ar_scene* scene);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ARSIM_H */

@@ -1,0 +1,315 @@
+"""numpy wrappers over oracle/liboracle.so -- the CPU restatement used as the checker.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, bench.py (cpu_baseline and reference arm) and
+__graft_entry__.smoke(); never by the product package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from pathlib import Path
+
+import numpy as np
+
+from . import build as _build
+
+_SO = Path(__file__).resolve().parent / "liboracle.so"
+if not _SO.exists():
+    _build.build()
+_L = C.CDLL(str(_SO))
+
+
+def _p(a: np.ndarray | None):
+    # data_as keeps a reference to the array, so temporaries live through the call
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+for _name in ["or_aabb", "or_morton30", "or_morton63", "or_sort_pairs_u32", "or_sort_pairs_u64",
+              "or_radix_tree_u32", "or_radix_tree_u64", "or_leaves", "or_refit",
+              "or_collide_bvh_dem", "or_find_contacts_bvh", "or_calc_hash", "or_reorder",
+              "or_collide_grid_dem", "or_reduce_bodies", "or_reduce_impulses",
+              "or_integrate_reference", "or_global_attributes", "or_walls_reference"]:
+    getattr(_L, _name).restype = None
+_L.or_pairs_brute.restype = C.c_long
+_L.or_step.restype = C.c_int
+_L.or_step_f64.restype = C.c_int
+for _name in ["or_aabb", "or_morton30", "or_morton63", "or_sort_pairs_u32", "or_sort_pairs_u64",
+              "or_calc_hash", "or_reorder", "or_collide_grid_dem", "or_pairs_brute"]:
+    pass  # argument conversion is explicit at each call (longs passed via C.c_long)
+
+
+# ---- stages -------------------------------------------------------------------------------------
+def aabb(pos4):
+    pos4 = _f32(pos4)
+    mn, mx = np.zeros(4, np.float32), np.zeros(4, np.float32)
+    _L.or_aabb(_p(pos4), C.c_long(len(pos4)), _p(mn), _p(mx))
+    return mn, mx
+
+
+def morton30(pos4, mn4, mx4) -> np.ndarray:
+    pos4, mn4, mx4 = _f32(pos4), _f32(mn4), _f32(mx4)
+    out = np.zeros(len(pos4), np.uint32)
+    _L.or_morton30(_p(pos4), C.c_long(len(pos4)), _p(mn4), _p(mx4), _p(out))
+    return out
+
+
+def morton63(pos4, mn4, mx4) -> np.ndarray:
+    pos4, mn4, mx4 = _f32(pos4), _f32(mn4), _f32(mx4)
+    out = np.zeros(len(pos4), np.uint64)
+    _L.or_morton63(_p(pos4), C.c_long(len(pos4)), _p(mn4), _p(mx4), _p(out))
+    return out
+
+
+def sort_pairs(keys, vals=None, begin_bit=0, end_bit=None):
+    """Stable sort by key bits [begin, end) -- cub::DeviceRadixSort::SortPairs order."""
+    keys = np.ascontiguousarray(keys)
+    n = len(keys)
+    vin = None if vals is None else _u32(vals)
+    vout = np.zeros(n, np.uint32)
+    if keys.dtype == np.uint64:
+        kout = np.zeros(n, np.uint64)
+        _L.or_sort_pairs_u64(_p(keys), _p(vin), _p(kout), _p(vout), C.c_long(n), begin_bit,
+                             64 if end_bit is None else end_bit)
+    else:
+        keys = _u32(keys)
+        kout = np.zeros(n, np.uint32)
+        _L.or_sort_pairs_u32(_p(keys), _p(vin), _p(kout), _p(vout), C.c_long(n), begin_bit,
+                             32 if end_bit is None else end_bit)
+    return kout, vout
+
+
+def radix_tree(sorted_codes) -> dict[str, np.ndarray]:
+    codes = np.ascontiguousarray(sorted_codes)
+    n = len(codes)
+    m = max(2 * n - 1, 1)
+    t = {"is_leaf": np.zeros(m, np.uint8), "left": np.full(m, -1, np.int32),
+         "right": np.full(m, -1, np.int32), "parent": np.full(m, -1, np.int32),
+         "min_r": np.full(m, -1, np.int32), "max_r": np.full(m, -1, np.int32)}
+    fn = _L.or_radix_tree_u64 if codes.dtype == np.uint64 else _L.or_radix_tree_u32
+    if codes.dtype != np.uint64:
+        codes = _u32(codes)
+    fn(_p(codes), n, _p(t["is_leaf"]), _p(t["left"]), _p(t["right"]), _p(t["parent"]),
+       _p(t["min_r"]), _p(t["max_r"]))
+    return t
+
+
+def leaves(tree: dict, sorted_idx, pos4, r: float):
+    n = len(sorted_idx)
+    sorted_idx, pos4 = _i32(sorted_idx), _f32(pos4)
+    cms = np.zeros((n, 4), np.float32)
+    bounds = np.zeros((max(2 * n - 1, 1), 8), np.float32)
+    _L.or_leaves(n, _p(sorted_idx), _p(pos4), C.c_float(r), _p(tree["is_leaf"]),
+                 _p(tree["min_r"]), _p(tree["max_r"]), _p(cms), _p(bounds))
+    return cms, bounds
+
+
+def refit(tree: dict, bounds: np.ndarray) -> np.ndarray:
+    n = (len(tree["left"]) + 1) // 2
+    b = _f32(bounds).copy()
+    _L.or_refit(n, _p(tree["left"]), _p(tree["right"]), _p(b))
+    return b
+
+
+def collide_bvh_dem(prm4, rb_idx, rel4, vel4, tree, cms4, bounds8, sorted_idx, radii):
+    n = len(sorted_idx)
+    pf = np.zeros((n, 4), np.float32)
+    pt = np.zeros((n, 4), np.float32)
+    pp = np.zeros((n, 4), np.float32)
+    args = [_f32(prm4), _i32(rb_idx), _f32(rel4), _f32(vel4), tree["is_leaf"], tree["left"],
+            tree["right"], _f32(cms4), _f32(bounds8), _i32(sorted_idx), _f32(radii)]
+    _L.or_collide_bvh_dem(*[_p(a) for a in args], n, _p(pf), _p(pt), _p(pp))
+    return pf, pt, pp
+
+
+def find_contacts_bvh(rb_idx, tree, cms4, bounds8, sorted_idx, radii, contact_distance):
+    n = len(sorted_idx)
+    cd = _f32(contact_distance).copy()
+    cp = np.zeros(n, np.int32)
+    cb = np.zeros(n, np.int32)
+    args = [_i32(rb_idx), tree["is_leaf"], tree["left"], tree["right"], tree["max_r"],
+            _f32(cms4), _f32(bounds8), _i32(sorted_idx), _f32(radii)]
+    _L.or_find_contacts_bvh(*[_p(a) for a in args], n, _p(cd), _p(cp), _p(cb))
+    return cd, cp, cb
+
+
+def pairs_brute(pos4, rb_idx, two_r: float) -> np.ndarray:
+    pos4, rb_idx = _f32(pos4), _i32(rb_idx)
+    n = len(pos4)
+    cnt = _L.or_pairs_brute(_p(pos4), _p(rb_idx), n, C.c_float(two_r), None, C.c_long(0))
+    out = np.zeros((max(cnt, 1), 2), np.int32)
+    _L.or_pairs_brute(_p(pos4), _p(rb_idx), n, C.c_float(two_r), _p(out), C.c_long(cnt))
+    return out[:cnt]
+
+
+def calc_hash(origin, cell, dims, pos4) -> np.ndarray:
+    g6 = _f32(list(origin) + list(np.broadcast_to(cell, 3)))
+    d3 = _u32(dims)
+    pos4 = _f32(pos4)
+    out = np.zeros(len(pos4), np.uint32)
+    _L.or_calc_hash(_p(g6), _p(d3), _p(pos4), C.c_long(len(pos4)), _p(out))
+    return out
+
+
+def reorder(shash, sidx, pos4, vel4, num_cells: int):
+    n = len(shash)
+    cs = np.zeros(num_cells, np.uint32)
+    ce = np.zeros(num_cells, np.uint32)
+    sp = np.zeros((n, 4), np.float32)
+    sv = np.zeros((n, 4), np.float32)
+    _L.or_reorder(_p(_u32(shash)), _p(_u32(sidx)), _p(_f32(pos4)), _p(_f32(vel4)), C.c_long(n),
+                  C.c_long(num_cells), _p(cs), _p(ce), _p(sp), _p(sv))
+    return cs, ce, sp, sv
+
+
+def collide_grid_dem(origin, cell, dims, prm5, rb_idx, spos4, svel4, rel4, gidx, cstart, cend,
+                     pf0=None, pt0=None):
+    n = len(spos4)
+    g6 = _f32(list(origin) + list(np.broadcast_to(cell, 3)))
+    pf = np.zeros((n, 4), np.float32) if pf0 is None else _f32(pf0).copy()
+    pt = np.zeros((n, 4), np.float32) if pt0 is None else _f32(pt0).copy()
+    args = [g6, _u32(dims), _f32(prm5), _i32(rb_idx), _f32(spos4), _f32(svel4), _f32(rel4),
+            _u32(gidx), _u32(cstart), _u32(cend)]
+    _L.or_collide_grid_dem(*[_p(a) for a in args], C.c_long(n), _p(pf), _p(pt))
+    return pf, pt
+
+
+def reduce_bodies(pf4, pt4, offsets):
+    nb = len(offsets) - 1
+    bf = np.zeros((nb, 4), np.float32)
+    bt = np.zeros((nb, 4), np.float32)
+    _L.or_reduce_bodies(_p(_f32(pf4)), _p(_f32(pt4)), _p(_i32(offsets)), nb, _p(bf), _p(bt))
+    return bf, bt
+
+
+def reduce_impulses(pf4, pt4, offsets, vel4, ang4, mass, ib9):
+    nb = len(offsets) - 1
+    v, a = _f32(vel4).copy(), _f32(ang4).copy()
+    _L.or_reduce_impulses(_p(_f32(pf4)), _p(_f32(pt4)), _p(_i32(offsets)), nb, _p(v), _p(a),
+                          _p(_f32(mass)), _p(_f32(ib9)))
+    return v, a
+
+
+def integrate_reference(gravity, w_damping, dt, state: dict) -> dict:
+    s = {k: _f32(v).copy() for k, v in state.items()}
+    nb = len(s["cms"])
+    _L.or_integrate_reference(_p(_f32(gravity)), C.c_float(w_damping), C.c_float(dt), nb,
+                              _p(s["cms"]), _p(s["vel"]), _p(s["ang"]), _p(s["quat"]),
+                              _p(s["ib"]), _p(s["cur"]), _p(s.get("model")), _p(s.get("cum")))
+    return s
+
+
+def global_attributes(cms4, rbvel4, rbang4, quat4, rb_idx, rel4):
+    n, nb = len(rel4), len(cms4)
+    q, rel = _f32(quat4).copy(), _f32(rel4).copy()
+    pos, vel = np.zeros((n, 4), np.float32), np.zeros((n, 4), np.float32)
+    _L.or_global_attributes(n, nb, _p(_f32(cms4)), _p(_f32(rbvel4)), _p(_f32(rbang4)), _p(q),
+                            _p(_i32(rb_idx)), _p(rel), _p(pos), _p(vel))
+    return rel, pos, vel, q
+
+
+def walls_reference(radius, ppos4, rbpos4, mn3, mx3, rbvel4, rbang4, ib9, mass, rb_idx, offsets):
+    v, a = _f32(rbvel4).copy(), _f32(rbang4).copy()
+    nb = len(offsets) - 1
+    _L.or_walls_reference(C.c_float(radius), _p(_f32(ppos4)), _p(_f32(rbpos4)), _p(_f32(mn3)),
+                          _p(_f32(mx3)), _p(v), _p(a), _p(_f32(ib9)), _p(_f32(mass)),
+                          _p(_i32(rb_idx)), _p(_i32(offsets)), nb)
+    return v, a
+
+
+# ---- the fused PHYSICAL step ---------------------------------------------------------------------
+def _next_pow2(v: int) -> int:
+    p = 1
+    while p < v and p < (1 << 31):
+        p <<= 1
+    return p
+
+
+def scene_grid(scene, cell_size: float | None = None, grid_log2=None):
+    """The grid the library gives a scene (same rule as the C++ scene set-up)."""
+    c = np.float32(cell_size if cell_size else (scene.cell_size or 2 * np.float32(scene.radius)))
+    g = list(scene.grid_log2 if grid_log2 is None else grid_log2)
+    origin = [float(x) for x in scene.box_min]
+    dims = []
+    for a in range(3):
+        if g[a] > 0:
+            dims.append(1 << int(g[a]))
+        else:
+            ext = float(scene.box_max[a]) - float(scene.box_min[a])
+            cells = int(math.ceil(ext / float(c)))
+            dims.append(max(4, _next_pow2(max(cells, 1))))
+    if not any(x > 0 for x in g):
+        cap = max(1 << 12, _next_pow2(8 * max(scene.num_particles, 1)))
+        while dims[0] * dims[1] * dims[2] > cap:
+            a = int(np.argmax(dims))
+            if dims[a] <= 4:
+                break
+            dims[a] >>= 1
+    return origin, [float(c)] * 3, dims
+
+
+def _scene_arrays(scene):
+    rel = _f32(scene.particle_rel).copy()
+    rel[:, 3] = scene.body_index().view(np.float32)
+    s15 = _f32(list(scene.box_min) + list(scene.box_max) + list(scene.gravity) +
+               [scene.radius, scene.dt, scene.spring, scene.damping, scene.shear,
+                scene.attraction])
+    return rel, s15
+
+
+def step(scene, steps: int = 1, grid=None, state: dict | None = None) -> dict:
+    """Float32 restatement of ar_step (operation for operation).  Returns the new body state
+    and, for the last step, the sorted keys / indices, per-particle forces and body sums."""
+    origin, cell, dims = grid if grid is not None else scene_grid(scene)
+    rel, s15 = _scene_arrays(scene)
+    st = state or {"pos": scene.body_pos, "quat": scene.body_quat, "vel": scene.body_vel,
+                   "angvel": scene.body_angvel}
+    st = {k: _f32(v).copy() for k, v in st.items()}
+    n, nb = scene.num_particles, scene.num_bodies
+    out = {"skeys": np.zeros(n, np.uint32), "sidx": np.zeros(n, np.uint32),
+           "pforce": np.zeros((n, 4), np.float32), "bforce": np.zeros((nb, 4), np.float32),
+           "btorque": np.zeros((nb, 4), np.float32)}
+    g6 = _f32(list(origin) + list(cell))
+    ok = _L.or_step(_p(s15), _p(g6), _p(_u32(dims)), nb, n, _p(st["pos"]), _p(st["quat"]),
+                    _p(st["vel"]), _p(st["angvel"]), _p(_f32(scene.body_mass)),
+                    _p(_f32(scene.body_inv_inertia)), _p(_i32(scene.body_offsets)), _p(rel),
+                    steps, _p(out["skeys"]), _p(out["sidx"]), _p(out["pforce"]),
+                    _p(out["bforce"]), _p(out["btorque"]))
+    st.update(out)
+    st["finite"] = bool(ok)
+    return st
+
+
+def step_f64(scene, steps: int = 1, state: dict | None = None, cell: float | None = None) -> dict:
+    """FP64 restatement of the same physics (contacts decided in double)."""
+    rel = np.ascontiguousarray(scene.particle_rel, np.float64).copy()
+    rel[:, 3] = scene.body_index()
+    s15 = np.ascontiguousarray(list(scene.box_min) + list(scene.box_max) + list(scene.gravity) +
+                               [scene.radius, scene.dt, scene.spring, scene.damping,
+                                scene.shear, scene.attraction], np.float64)
+    c = float(cell or scene_grid(scene)[1][0])
+    cell3 = np.array([c, c, c], np.float64)
+    st = state or {"pos": scene.body_pos, "quat": scene.body_quat, "vel": scene.body_vel,
+                   "angvel": scene.body_angvel}
+    st = {k: np.ascontiguousarray(v, np.float64).copy() for k, v in st.items()}
+    n, nb = scene.num_particles, scene.num_bodies
+    pf = np.zeros((n, 4), np.float64)
+    bf = np.zeros((nb, 4), np.float64)
+    bt = np.zeros((nb, 4), np.float64)
+    ok = _L.or_step_f64(_p(s15), _p(cell3), nb, n, _p(st["pos"]), _p(st["quat"]), _p(st["vel"]),
+                        _p(st["angvel"]), _p(np.ascontiguousarray(scene.body_mass, np.float64)),
+                        _p(np.ascontiguousarray(scene.body_inv_inertia, np.float64)),
+                        _p(_i32(scene.body_offsets)), _p(rel), steps, _p(pf), _p(bf), _p(bt))
+    st.update({"pforce": pf, "bforce": bf, "btorque": bt, "finite": bool(ok)})
+    return st

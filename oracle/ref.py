@@ -1,0 +1,198 @@
+"""numpy wrappers over oracle/_ref/libref_cpu.so -- the reference's own kernel bodies run on
+the CPU (built from the reference checkout by oracle/ref_build.py).
+
+TEST INFRASTRUCTURE ONLY.  Used to generate the golden fixtures, to pin oracle.cpu, and as
+the CPU baseline of bench.py's reference arm.  ``available()`` is False where the library
+was not built (no reference checkout when it was built).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+_SO = Path(__file__).resolve().parent / "_ref" / "libref_cpu.so"
+_L = None
+
+
+def available() -> bool:
+    return _SO.exists()
+
+
+def lib():
+    global _L
+    if _L is None:
+        if not _SO.exists():
+            raise FileNotFoundError(f"{_SO} not built (needs the reference checkout)")
+        _L = C.CDLL(str(_SO))
+        for name in dir(_L):
+            pass
+        _L.refcpu_max_threads.restype = C.c_int
+        _L.refcpu_sizeof_simparams.restype = C.c_int
+    return _L
+
+
+def _p(a):
+    # data_as keeps a reference to the array, so temporaries live through the call
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32)
+
+
+def set_threads(n: int) -> None:
+    lib().refcpu_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().refcpu_max_threads())
+
+
+def morton30(pos4, mn4, mx4):
+    pos4 = _f32(pos4)
+    n = len(pos4)
+    codes = np.zeros(n, np.uint32)
+    idx = np.zeros(n, np.int32)
+    lib().refcpu_morton30(_p(pos4), n, _p(_f32(mn4)), _p(_f32(mx4)), _p(codes), _p(idx))
+    return codes, idx
+
+
+def aabb(pos4):
+    pos4 = _f32(pos4)
+    mn, mx = np.zeros(4, np.float32), np.zeros(4, np.float32)
+    lib().refcpu_aabb(_p(pos4), len(pos4), _p(mn), _p(mx))
+    return mn, mx
+
+
+def sort_pairs_u32(keys, vals):
+    k, v = _u32(keys).copy(), _u32(vals).copy()
+    lib().refcpu_sort_pairs_u32(_p(k), _p(v), C.c_long(len(k)))
+    return k, v
+
+
+def radix_tree(sorted_codes):
+    codes = _u32(sorted_codes)
+    n = len(codes)
+    m = max(2 * n - 1, 1)
+    t = {"is_leaf": np.zeros(m, np.uint8), "left": np.full(m, -1, np.int32),
+         "right": np.full(m, -1, np.int32), "parent": np.full(m, -1, np.int32),
+         "min_r": np.full(m, -1, np.int32), "max_r": np.full(m, -1, np.int32)}
+    lib().refcpu_radix_tree(_p(codes), n, _p(t["is_leaf"]), _p(t["left"]), _p(t["right"]),
+                            _p(t["parent"]), _p(t["min_r"]), _p(t["max_r"]))
+    return t
+
+
+def leaves_and_refit(tree, sorted_idx, pos4, r):
+    n = len(sorted_idx)
+    cms = np.zeros((n, 4), np.float32)
+    bounds = np.zeros((max(2 * n - 1, 1), 8), np.float32)
+    radii = np.zeros(n, np.float32)
+    L = lib()
+    L.refcpu_leaf_nodes(n, _p(tree["is_leaf"]), _p(tree["left"]), _p(tree["right"]),
+                        _p(tree["parent"]), _p(tree["min_r"]), _p(tree["max_r"]), _p(cms),
+                        _p(bounds), _p(_i32(sorted_idx)), _p(radii), _p(_f32(pos4)),
+                        C.c_float(r))
+    leaf_bounds = bounds.copy()
+    L.refcpu_internal_nodes(n, _p(tree["left"]), _p(tree["right"]), _p(tree["parent"]),
+                            _p(bounds))
+    return cms, leaf_bounds, bounds, radii
+
+
+def calc_hash(params, pos4):
+    pos4 = _f32(pos4)
+    n = len(pos4)
+    h = np.zeros(n, np.uint32)
+    idx = np.zeros(n, np.uint32)
+    lib().refcpu_calc_hash(C.byref(params), _p(pos4), n, _p(h), _p(idx))
+    return h, idx
+
+
+def reorder(shash, sidx, pos4, vel4, num_cells):
+    n = len(shash)
+    cs = np.zeros(num_cells, np.uint32)
+    ce = np.zeros(num_cells, np.uint32)
+    sp = np.zeros((n, 4), np.float32)
+    sv = np.zeros((n, 4), np.float32)
+    lib().refcpu_reorder(_p(cs), _p(ce), _p(sp), _p(sv), _p(_u32(shash)), _p(_u32(sidx)),
+                         _p(_f32(pos4)), _p(_f32(vel4)), n, C.c_long(num_cells))
+    return cs, ce, sp, sv
+
+
+def collide_grid_dem(params, rb_idx, spos4, svel4, rel4, gidx, cstart, cend):
+    n = len(spos4)
+    pf = np.zeros((n, 4), np.float32)
+    pt = np.zeros((n, 4), np.float32)
+    lib().refcpu_collide_grid_dem(C.byref(params), _p(_i32(rb_idx)), _p(pf), _p(pt),
+                                  _p(_f32(spos4)), _p(_f32(svel4)), _p(_f32(rel4)),
+                                  _p(_u32(gidx)), _p(_u32(cstart)), _p(_u32(cend)), n)
+    return pf, pt
+
+
+def reduce_impulses(pf4, pt4, vel4, ang4, mass, ib9, counts):
+    v, a = _f32(vel4).copy(), _f32(ang4).copy()
+    lib().refcpu_reduce_impulses(_p(_f32(pf4)), _p(_f32(pt4)), _p(v), _p(a), _p(_f32(mass)),
+                                 _p(_f32(ib9)), _p(_i32(counts)), len(counts), len(pf4))
+    return v, a
+
+
+def gpu_integrator(params, dt, state):
+    s = {k: _f32(v).copy() for k, v in state.items()}
+    nb = len(s["cms"])
+    lib().refcpu_gpu_integrator(_p(s["cms"]), _p(s["vel"]), _p(s["ang"]), _p(s["quat"]),
+                                _p(s["ib"]), _p(s["cur"]), _p(s["model"]), _p(s["cum"]),
+                                C.c_float(dt), _p(_f32(np.ones(nb))), nb, C.byref(params))
+    return s
+
+
+def global_attributes(cms4, rbvel4, rbang4, quat4, rb_idx, rel4):
+    n, nb = len(rel4), len(cms4)
+    q, rel = _f32(quat4).copy(), _f32(rel4).copy()
+    pos, vel = np.zeros((n, 4), np.float32), np.zeros((n, 4), np.float32)
+    lib().refcpu_global_attributes(_p(_f32(cms4)), _p(_f32(rbvel4)), _p(rel), _p(pos), _p(vel),
+                                   _p(q), _p(_f32(rbang4)), _p(_i32(rb_idx)), n, nb)
+    return rel, pos, vel, q
+
+
+def collide_bvh_rigid(params, rb_idx, rel4, vel4, tree, cms4, bounds8, sorted_idx, radii):
+    n = len(sorted_idx)
+    pf = np.zeros((n, 4), np.float32)
+    pt = np.zeros((n, 4), np.float32)
+    pp = np.zeros((n, 4), np.float32)
+    lib().refcpu_collide_bvh_rigid(C.byref(params), _p(pf), _p(_i32(rb_idx)), _p(pp),
+                                   _p(_f32(rel4)), _p(pt), _p(_f32(vel4).copy()),
+                                   _p(tree["is_leaf"]), _p(tree["left"]), _p(tree["right"]),
+                                   _p(tree["min_r"]), _p(tree["max_r"]), _p(_f32(cms4)),
+                                   _p(_f32(bounds8)), _p(_i32(sorted_idx)), _p(_f32(radii)), n)
+    return pf, pt, pp
+
+
+def find_rb_collisions_bvh(params, rb_idx, tree, cms4, bounds8, sorted_idx, radii, cd0):
+    n = len(sorted_idx)
+    cd = _f32(cd0).copy()
+    cp = np.zeros(n, np.int32)
+    cb = np.zeros(n, np.int32)
+    lib().refcpu_find_rb_collisions_bvh(C.byref(params), _p(_i32(rb_idx)), _p(tree["is_leaf"]),
+                                        _p(tree["left"]), _p(tree["right"]), _p(tree["min_r"]),
+                                        _p(tree["max_r"]), _p(_f32(cms4)), _p(_f32(bounds8)),
+                                        _p(_i32(sorted_idx)), _p(_f32(radii)), n, _p(cd), _p(cp),
+                                        _p(cb))
+    return cd, cp, cb
+
+
+def wall_collisions(ppos4, rbpos4, mn3, mx3, rbvel4, rbang4, ib9, mass, rb_idx, counts, radius):
+    v, a = _f32(rbvel4).copy(), _f32(rbang4).copy()
+    lib().refcpu_wall_collisions(_p(_f32(ppos4)), _p(_f32(rbpos4)), _p(_f32(mn3)),
+                                 _p(_f32(mx3)), _p(v), _p(a), _p(_f32(ib9)), _p(_f32(mass)),
+                                 _p(_i32(rb_idx)), _p(_i32(counts)), len(counts), len(ppos4),
+                                 C.c_float(radius))
+    return v, a

@@ -1,0 +1,356 @@
+// Host driver for the reference's own kernel bodies ("ref_cpu").
+//
+// TEST INFRASTRUCTURE ONLY (oracle).  Built by oracle/ref_build.py into
+// oracle/_ref/libref_cpu.so; loaded only by tests/, bench.py's reference arm and
+// __graft_entry__.smoke() as a checker or as the timed CPU baseline.
+//
+// The kernel bodies come verbatim from the reference checkout (oracle/_ref/extracted.inc,
+// generated at build time, never committed) plus the reference's BVHSoAKernels.cu and
+// BVHAuxiliary.cuh included from their place in the checkout.  This file only supplies:
+//   * an emulated launch: every kernel runs once per (blockIdx, threadIdx) of the grid the
+//     reference wrapper would launch, in an OpenMP loop;
+//   * host restatements of the three pieces of the reference path that are not kernel
+//     bodies: the CUB radix sorts (stable LSD order, restated as a stable LSD sort with the
+//     same key-bit treatment), the CUB float4 inclusive scans (restated as the sequential
+//     float scan the reference's own DEBUG_SCAN check uses, UniformGridDEM.cu:559-588), and
+//     reorderDataAndFindCellStartD (shared memory + __syncthreads, particleKernels.cu:193-258,
+//     restated as its sequential neighbour compare);
+//   * extern "C" entry points with plain pointers for ctypes.
+#include "ref_prelude.h"
+
+thread_local uint3 threadIdx;
+thread_local uint3 blockIdx;
+thread_local dim3 blockDim;
+thread_local dim3 gridDim;
+
+#include "BVHAuxiliary.cuh"
+
+#ifndef GLM_FORCE_CUDA
+#define GLM_FORCE_CUDA
+#endif
+#include <glm/glm.hpp>
+#include <glm/gtc/quaternion.hpp>
+
+// Kernels/particleKernels.cu:42 keeps the parameters in __constant__ memory.
+SimParams params;
+
+#include "BVHSoAKernels.cu"
+#include "extracted.inc"
+
+#include <omp.h>
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace {
+
+int g_threads = 0;  // 0 = OpenMP default
+
+template <class F>
+void launch(long n_threads, int block, bool parallel, F&& body) {
+  long nb = (n_threads + block - 1) / block;
+  if (nb < 1) nb = 1;
+  const long total = nb * (long)block;
+  const int nt = g_threads > 0 ? g_threads : omp_get_max_threads();
+#pragma omp parallel for schedule(static) if (parallel) num_threads(nt)
+  for (long t = 0; t < total; ++t) {
+    blockIdx = make_uint3((unsigned)(t / block), 0, 0);
+    threadIdx = make_uint3((unsigned)(t % block), 0, 0);
+    blockDim = dim3(block);
+    gridDim = dim3((unsigned)nb);
+    body();
+  }
+}
+
+// Stable LSD radix sort of (key, value) pairs over all key bits: the order
+// cub::DeviceRadixSort::SortPairs produces (keys ascending, equal keys in input order).
+template <class K, class V>
+void stable_lsd(K* keys, V* vals, long n) {
+  std::vector<K> k2(n);
+  std::vector<V> v2(n);
+  K* ka = keys; V* va = vals; K* kb = k2.data(); V* vb = v2.data();
+  const int passes = (int)sizeof(K);
+  for (int p = 0; p < passes; ++p) {
+    const int shift = 8 * p;
+    long cnt[257] = {0};
+    for (long i = 0; i < n; ++i) cnt[((ka[i] >> shift) & 0xFF) + 1]++;
+    if (cnt[1 + ((ka[0] >> shift) & 0xFF)] == n && n > 0) continue;  // digit constant
+    for (int d = 0; d < 256; ++d) cnt[d + 1] += cnt[d];
+    for (long i = 0; i < n; ++i) {
+      long dst = cnt[(ka[i] >> shift) & 0xFF]++;
+      kb[dst] = ka[i];
+      vb[dst] = va[i];
+    }
+    std::swap(ka, kb);
+    std::swap(va, vb);
+  }
+  if (ka != keys) {
+    std::memcpy(keys, ka, n * sizeof(K));
+    std::memcpy(vals, va, n * sizeof(V));
+  }
+}
+
+// CUB's unsigned image of a float key (sign-magnitude flipped to two's-complement order).
+inline uint32_t float_key_bits(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+}  // namespace
+
+extern "C" {
+
+void refcpu_set_threads(int n) { g_threads = n; }
+int refcpu_max_threads(void) { return g_threads > 0 ? g_threads : omp_get_max_threads(); }
+int refcpu_sizeof_simparams(void) { return (int)sizeof(SimParams); }
+int refcpu_sizeof_aabb(void) { return (int)sizeof(AABB); }
+
+// ---- Morton codes: generateMortonCodes (BVHSource/BVHkernels.cu:694-716) ----------------
+void refcpu_morton30(const float* pos4, int n, const float* min4, const float* max4,
+                     uint32_t* codes, int32_t* idx) {
+  float4 mn = make_float4(min4[0], min4[1], min4[2], min4[3]);
+  float4 mx = make_float4(max4[0], max4[1], max4[2], max4[3]);
+  launch(n, 128, true, [&] {
+    generateMortonCodes((float4*)pos4, codes, idx, n, mn, mx);
+  });
+}
+
+// ---- scene AABB: findAABBCub (BVHSource/createMortonCodes.cu:65-107) ---------------------
+// Restated: CUB reduces with CustomMin4/CustomMax4 over all four lanes starting from
+// (float)0x7f800000 / -(float)0x7f800000 (the `inf` macro is an int, :10).
+void refcpu_aabb(const float* pos4, int n, float* min4, float* max4) {
+  float lo[4], hi[4];
+  for (int c = 0; c < 4; ++c) { lo[c] = (float)0x7f800000; hi[c] = -(float)0x7f800000; }
+  for (long i = 0; i < n; ++i)
+    for (int c = 0; c < 4; ++c) {
+      float v = pos4[4 * i + c];
+      lo[c] = (v < lo[c]) ? v : lo[c];
+      hi[c] = (v > hi[c]) ? v : hi[c];
+    }
+  for (int c = 0; c < 4; ++c) { min4[c] = lo[c]; max4[c] = hi[c]; }
+}
+
+// ---- CUB DeviceRadixSort::SortPairs (all key bits, stable) -----------------------------
+void refcpu_sort_pairs_u32(uint32_t* keys, uint32_t* vals, long n) { stable_lsd(keys, vals, n); }
+void refcpu_sort_pairs_u64(uint64_t* keys, uint32_t* vals, long n) { stable_lsd(keys, vals, n); }
+
+// ---- Karras radix tree: kernelConstructRadixTreeSoA (BVHSource/BVHSoAKernels.cu:7-99) --
+void refcpu_radix_tree(const uint32_t* sorted_codes, int n, uint8_t* is_leaf, int* left,
+                       int* right, int* parent, int* min_r, int* max_r) {
+  if (n < 2) return;
+  launch(n - 1, 128, true, [&] {
+    kernelConstructRadixTreeSoA(n - 1, (bool*)is_leaf, left, right, parent, min_r, max_r,
+                                (unsigned int*)sorted_codes);
+  });
+}
+
+// ---- leaves: initializeRadii + kernelConstructLeafNodesSoA (BVHSoAKernels.cu:108-138) --
+void refcpu_leaf_nodes(int n, uint8_t* is_leaf, int* left, int* right, int* parent,
+                       int* min_r, int* max_r, float* cms4, void* bounds,
+                       const int* sorted_idx, float* radii, const float* pos4, float r) {
+  for (int i = 0; i < n; ++i) radii[i] = r;  // initializeRadii (particleKernels.cu:694-701)
+  launch(n, 128, true, [&] {
+    kernelConstructLeafNodesSoA(n, (bool*)is_leaf, left, right, parent, min_r, max_r,
+                                (float4*)cms4, (AABB*)bounds, (int*)sorted_idx, radii,
+                                (float4*)pos4, r);
+  });
+}
+
+// ---- refit: kernelConstructInternalNodesSoA (BVHSoAKernels.cu:148-176) -------------------
+// Run on one thread: the reference has no fence between the counter and the child reads,
+// so only a serial run gives its intended result deterministically.
+void refcpu_internal_nodes(int n, int* left, int* right, int* parent, void* bounds) {
+  if (n < 2) return;
+  std::vector<int> counters(n - 1, 0);
+  launch(n, 128, false, [&] {
+    kernelConstructInternalNodesSoA(n, left, right, parent, (AABB*)bounds, counters.data());
+  });
+}
+
+// ---- grid hash: calcHashD (Kernels/particleKernels.cu:170-189) ---------------------------
+void refcpu_calc_hash(const void* sim_params, const float* pos4, int n, uint32_t* hash,
+                      uint32_t* idx) {
+  std::memcpy(&params, sim_params, sizeof(SimParams));
+  launch(n, 512, true, [&] { calcHashD(hash, idx, (float4*)pos4, (uint)n); });
+}
+
+// ---- reorderDataAndFindCellStart (particleKernelWrappers.cu:213-254 + kernel :193-258) --
+// Restated: cellStart memset to 0xffffffff over all cells, then the neighbour compare.
+void refcpu_reorder(uint32_t* cell_start, uint32_t* cell_end, float* sorted_pos4,
+                    float* sorted_vel4, const uint32_t* hash, const uint32_t* idx,
+                    const float* pos4, const float* vel4, int n, long num_cells) {
+  std::memset(cell_start, 0xff, num_cells * sizeof(uint32_t));
+  for (int i = 0; i < n; ++i) {
+    uint32_t h = hash[i];
+    if (i == 0 || h != hash[i - 1]) {
+      cell_start[h] = i;
+      if (i > 0) cell_end[hash[i - 1]] = i;
+    }
+    if (i == n - 1) cell_end[h] = i + 1;
+    std::memcpy(sorted_pos4 + 4l * i, pos4 + 4l * idx[i], 16);
+    std::memcpy(sorted_vel4 + 4l * i, vel4 + 4l * idx[i], 16);
+  }
+}
+
+// ---- DEM grid collide: FindAndHandleRigidBodyCollisionsUniformGridKernel
+//      (RigidBodies/UniformGridDEM.cu:133-204).  pForce/pTorque are accumulated (+=).
+void refcpu_collide_grid_dem(const void* sim_params, const int* rb_idx, float* p_force4,
+                             float* p_torque4, const float* sorted_pos4,
+                             const float* sorted_vel4, const float* rel4,
+                             const uint32_t* grid_idx, const uint32_t* cell_start,
+                             const uint32_t* cell_end, int n) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  std::vector<float4> color(n);
+  float3 zero = make_float3(0, 0, 0);
+  launch(n, 128, true, [&] {
+    FindAndHandleRigidBodyCollisionsUniformGridKernel(
+        (int*)rb_idx, (float4*)p_force4, (float4*)p_torque4, color.data(),
+        (float4*)sorted_pos4, (float4*)sorted_vel4, (float4*)rel4, zero, zero,
+        (uint*)grid_idx, (uint*)cell_start, (uint*)cell_end, (uint)n, p);
+  });
+}
+
+// ---- ReducePerParticleImpulses (UniformGridDEM.cu:462-666) with CombineReducedImpulses ---
+// The two CUB float4 inclusive scans are restated as sequential float scans.
+void refcpu_reduce_impulses(const float* p_force4, const float* p_torque4, float* rb_vel4,
+                            float* rb_ang4, const float* rb_mass, const float* rb_inv_inertia9,
+                            const int* particles_per_object, int num_bodies, int n) {
+  std::vector<float4> lin(n), ang(n);
+  float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0);
+  for (int i = 0; i < n; ++i) {
+    a += ((const float4*)p_force4)[i];
+    b += ((const float4*)p_torque4)[i];
+    lin[i] = a;
+    ang[i] = b;
+  }
+  std::vector<int> cum(num_bodies);
+  int run = 0;
+  for (int i = 0; i < num_bodies; ++i) { run += particles_per_object[i]; cum[i] = run; }
+  launch(num_bodies, 128, true, [&] {
+    CombineReducedImpulses(lin.data(), ang.data(), (float4*)rb_vel4, (float4*)rb_ang4,
+                           (float*)rb_mass, (glm::mat3*)rb_inv_inertia9, cum.data(), num_bodies);
+  });
+}
+
+// ---- GPUintegratorKernel (Kernels/rigidBodyKernels.cu:262-348) --------------------------
+void refcpu_gpu_integrator(float* cms4, float* vel4, float* ang4, float* quat4,
+                           const float* inv_inertia9, float* cur_inertia9, float* model16,
+                           float* cum_quat4, float dt, const float* mass, int num_bodies,
+                           const void* sim_params) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  launch(num_bodies, 128, true, [&] {
+    GPUintegratorKernel((float4*)cms4, (float4*)vel4, (float4*)ang4, (glm::quat*)quat4,
+                        (glm::mat3*)inv_inertia9, (glm::mat3*)cur_inertia9,
+                        (glm::mat4*)model16, (glm::quat*)cum_quat4, dt, (float*)mass,
+                        num_bodies, p);
+  });
+}
+
+// ---- computeGlobalAttributes + resetQuaternionKernel (rigidBodyKernels.cu:386-456) ------
+void refcpu_global_attributes(const float* cms4, const float* rb_vel4, float* rel4,
+                              float* pos4, float* vel4, float* quat4, const float* ang4,
+                              const int* rb_idx, int n, int num_bodies) {
+  launch(n, 128, true, [&] {
+    computeGlobalAttributes((float4*)cms4, (float4*)rb_vel4, (float4*)rel4, (float4*)pos4,
+                            (float4*)vel4, (glm::quat*)quat4, (float4*)ang4, (int*)rb_idx, n);
+  });
+  launch(num_bodies, 128, true, [&] { resetQuaternionKernel((glm::quat*)quat4, num_bodies); });
+}
+
+// ---- BVH DEM traversal: collideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:100-244) -------
+void refcpu_collide_bvh_rigid(const void* sim_params, float* p_force4, const int* rb_idx,
+                              float* p_positions4, const float* rel4, float* p_torque4,
+                              float* vel4, const uint8_t* is_leaf, const int* left,
+                              const int* right, const int* min_r, const int* max_r,
+                              const float* cms4, const void* bounds, const int* sorted_idx,
+                              const float* radii, int n) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  std::vector<float4> color(n);
+  launch(n, 128, true, [&] {
+    collideBVHSoARigidBody(color.data(), (float4*)p_force4, (int*)rb_idx,
+                           (float4*)p_positions4, nullptr, (float4*)rel4, (float4*)p_torque4,
+                           (float4*)vel4, (bool*)is_leaf, (int*)left, (int*)right,
+                           (int*)min_r, (int*)max_r, (float4*)cms4, (AABB*)bounds,
+                           (int*)sorted_idx, (float*)radii, n, p);
+  });
+}
+
+// ---- deepest contact per particle: FindRigidBodyCollisionsBVHKernel (:760-876) ----------
+void refcpu_find_rb_collisions_bvh(const void* sim_params, const int* rb_idx,
+                                   const uint8_t* is_leaf, const int* left, const int* right,
+                                   const int* min_r, const int* max_r, const float* cms4,
+                                   const void* bounds, const int* sorted_idx,
+                                   const float* radii, int n, float* contact_distance,
+                                   int* colliding_particle, int* colliding_body) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  std::vector<float4> color(n);
+  launch(n, 128, true, [&] {
+    FindRigidBodyCollisionsBVHKernel(color.data(), (int*)rb_idx, (bool*)is_leaf, (int*)left,
+                                     (int*)right, (int*)min_r, (int*)max_r, (float4*)cms4,
+                                     (AABB*)bounds, (int*)sorted_idx, (float*)radii, n, p,
+                                     contact_distance, colliding_particle, colliding_body);
+  });
+}
+
+// ---- WallCollisionWrapper (WallCollisions.cu:338-597) ------------------------------------
+// The six DetectWallCollisionKernel launches and HandleWallCollisionKernelUnmapped are the
+// reference bodies; the host glue (wall planes, the three stable CUB sorts, the prefix of
+// particle counts) is restated from the wrapper.
+void refcpu_wall_collisions(const float* particle_pos4, const float* rb_pos4,
+                            const float* min_pos3, const float* max_pos3, float* rb_vel4,
+                            float* rb_ang4, const float* inv_inertia9, const float* rb_mass,
+                            const int* rb_idx, const int* particles_per_rb, int num_bodies,
+                            int n, float radius) {
+  std::vector<float4> cn(n, make_float4(0, 0, 0, 0)), cp(n, make_float4(0, 0, 0, 0)),
+      cw(n, make_float4(0, 0, 0, 0));
+  std::vector<float> cd(n, 0.0f);
+  float3 mn = make_float3(min_pos3[0], min_pos3[1], min_pos3[2]);
+  float3 mx = make_float3(max_pos3[0], max_pos3[1], max_pos3[2]);
+  float4 unit = make_float4(1, 1, 1, 1);
+  const float4 normals[6] = {make_float4(1, 0, 0, 0),  make_float4(0, 1, 0, 0),
+                             make_float4(0, 0, 1, 0),  make_float4(-1, 0, 0, 0),
+                             make_float4(0, -1, 0, 0), make_float4(0, 0, -1, 0)};
+  for (int w = 0; w < 6; ++w) {
+    float4 nrm = normals[w];
+    float wall_pos;
+    if (w < 3) {
+      wall_pos = dot(make_float3(nrm), mx);
+    } else {
+      float sign = dot(nrm, unit);
+      wall_pos = dot(make_float3(nrm) * sign, mn);
+    }
+    launch(n, 128, true, [&] {
+      DetectWallCollisionKernel(radius, (float4*)particle_pos4, (int*)rb_idx, (float4*)rb_vel4,
+                                wall_pos, nrm, cn.data(), cp.data(), cw.data(), cd.data(), n);
+    });
+  }
+  // particleIndices sorted by distance; body flags sorted by distance; then indices
+  // sorted by flag (all stable).
+  std::vector<uint32_t> key(n), ids(n), flags(n);
+  long t = 0;
+  for (int b = 0; b < num_bodies; ++b)
+    for (int k = 0; k < particles_per_rb[b]; ++k) flags[t++] = (uint32_t)b;
+  for (int i = 0; i < n; ++i) { key[i] = float_key_bits(cd[i]); ids[i] = (uint32_t)i; }
+  std::vector<uint32_t> key2 = key;
+  stable_lsd(key.data(), ids.data(), n);
+  stable_lsd(key2.data(), flags.data(), n);
+  stable_lsd(flags.data(), ids.data(), n);
+  std::vector<int> contact_id(ids.begin(), ids.end());
+  std::vector<int> cum(num_bodies);
+  int run = 0;
+  for (int b = 0; b < num_bodies; ++b) { run += particles_per_rb[b]; cum[b] = run; }
+  launch(num_bodies, 128, true, [&] {
+    HandleWallCollisionKernelUnmapped(radius, (float4*)rb_pos4, (float4*)rb_vel4,
+                                      (float4*)rb_ang4, nullptr, nullptr,
+                                      (glm::mat3*)inv_inertia9, (float*)rb_mass, cn.data(),
+                                      cw.data(), cp.data(), cd.data(), contact_id.data(),
+                                      cum.data(), num_bodies);
+  });
+}
+
+}  // extern "C"
