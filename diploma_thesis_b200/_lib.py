@@ -109,6 +109,9 @@ SIGNATURES = {
     "ar_scene_destroy": [P],
     "ar_scene_footprint": [C.POINTER(SceneDesc)],
     "ar_scene_download": [P, P, P, P, P, S],
+    "ar_scene_upload": [P, P, P, P, P, S],
+    "ar_step_profile": [P, P, I, C.POINTER(F), S],
+    "ar_batch_profile": [P, P, I, C.POINTER(F), S],
     "ar_scene_get_view": [P, C.POINTER(SceneView)],
     "ar_scene_grid_info": [P, C.POINTER(F), C.POINTER(F), C.POINTER(C.c_uint32)],
     "ar_scene_step_view": [P, C.POINTER(StepView)],

@@ -112,6 +112,24 @@ class GpuScene:
              _np_ptr(out["vel"]), _np_ptr(out["angvel"]), stream_handle())
         return out
 
+    def upload(self, pos, quat, vel, angvel, stream=None) -> None:
+        """Overwrite body state from (preferably pinned) host arrays, asynchronously."""
+        call("ar_scene_upload", self.handle, *[_np_ptr(a) if a is not None else None
+                                               for a in (pos, quat, vel, angvel)],
+             stream_handle(stream))
+
+    def download_into(self, pos, quat, vel, angvel, stream=None) -> None:
+        call("ar_scene_download", self.handle, *[_np_ptr(a) if a is not None else None
+                                                 for a in (pos, quat, vel, angvel)],
+             stream_handle(stream))
+
+    def profile(self, n: int, stream=None) -> list[float]:
+        """Average device ms per stage over n eager steps (clear, repose_hash, sort,
+        scatter, collide, reduce_integrate)."""
+        out = (C.c_float * 6)()
+        call("ar_step_profile", self.ctx.handle, self.handle, int(n), out, stream_handle(stream))
+        return list(out)
+
     def view(self) -> SceneView:
         v = SceneView()
         call("ar_scene_get_view", self.handle, C.byref(v))
@@ -161,21 +179,35 @@ class Batch:
     def launches_per_step(self) -> int:
         return int(lib.ar_batch_launches_per_step(self.handle))
 
+    def profile(self, n: int, stream=None) -> list[float]:
+        out = (C.c_float * 6)()
+        call("ar_batch_profile", self.ctx.handle, self.handle, int(n), out, stream_handle(stream))
+        return list(out)
+
     def close(self) -> None:
         if self.handle:
             lib.ar_batch_destroy(self.handle)
             self.handle = C.c_void_p()
 
 
+class _DeviceArray:
+    """Minimal __cuda_array_interface__ exporter for a raw device address."""
+
+    _TYPESTR = {torch.float32: "<f4", torch.int32: "<i4", torch.int64: "<i8",
+                torch.uint8: "|u1", torch.float64: "<f8"}
+
+    def __init__(self, addr: int, count: int, dtype: torch.dtype):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": self._TYPESTR[dtype],
+                                         "data": (int(addr), True), "version": 3,
+                                         "strides": None}
+
+
 def device_view(addr: int, count: int, dtype: torch.dtype, device: int = 0) -> torch.Tensor:
     """Copy `count` elements starting at a raw device address into a new tensor."""
-    elem = torch.empty((), dtype=dtype).element_size()
-    out = torch.empty(count, dtype=dtype, device=f"cuda:{device}")
-    if count:
-        torch.cuda.synchronize()
-        cudart = torch.cuda.cudart()
-        cudart.cudaMemcpy(out.data_ptr(), addr, count * elem, 3)  # device to device
-    return out
+    if count == 0:
+        return torch.empty(0, dtype=dtype, device=f"cuda:{device}")
+    torch.cuda.synchronize()
+    return torch.as_tensor(_DeviceArray(addr, count, dtype), device=f"cuda:{device}").clone()
 
 
 def sim_params(radius: float, grid_origin, cell, grid_dims, spring=0.5, damping=0.02,

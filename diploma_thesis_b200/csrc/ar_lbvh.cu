@@ -101,7 +101,8 @@ __global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t* __rest
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int node = __ldg(parent + i);
-  while (true) {
+  for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
+    if (node < n || node >= 2 * n - 1) return;  // malformed parent link
     __threadfence();
     if (atomicAdd(counters + (node - n), 1) == 0) return;
     __threadfence();
@@ -148,10 +149,12 @@ __device__ __forceinline__ void walk(int n, const uint8_t* __restrict__ is_leaf,
                                      const int32_t* __restrict__ parent, Accept accept,
                                      Visit visit_leaf) {
   // The root (index n) is never left through its parent link, so parent[n] is not read.
+  // A valid tree is walked in fewer than 4 (2n - 1) moves; the bound only guards against a
+  // malformed tree passed in by a caller.
   int node = n;
   bool descending = true;
   int from = -1;
-  while (true) {
+  for (long moves = 8l * n + 64; moves > 0; --moves) {
     if (descending) {
       const int lc = __ldg(left + node), rc = __ldg(right + node);
       const bool ll = __ldg(is_leaf + lc), rl = __ldg(is_leaf + rc);

@@ -373,33 +373,70 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
   return arh::check_launch("batch prepare");
 }
 
-ar_status enqueue_step(ar_batch* B, cudaStream_t st) {
+// Stage boundaries for ar_step_profile: events[0] before the clear, events[i] after stage i.
+constexpr int kStages = 6;  // clear, repose_hash, sort, scatter, collide, reduce_integrate
+
+ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   if (B->nt == 0) return AR_OK;
   ar_ctx* ctx = B->ctx;
   const int ns = (int)B->scenes.size();
   const int nt = (int)B->nt, bt = (int)B->bt;
+  auto mark = [&](int i) {
+    if (ev) cudaEventRecord(ev[i], st);
+  };
+  mark(0);
   cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
+  mark(1);
   unsigned g1 = arh::grid_for(nt, kK1Threads);
   unsigned cap1 = (unsigned)ctx->num_sms * 4;
   repose_hash_kernel<<<g1 > cap1 ? cap1 : g1, kK1Threads, 0, st>>>(
       B->d_table, B->d_poff, ns, nt, B->d_prev_n, B->skeys, B->cells, B->keys,
       (uint32_t*)B->sort_ws, B->passes, B->last_bits);
+  mark(2);
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
                                   st, B->sort_ws, B->cap_sort, true);
   if (s != AR_OK) return s;
+  mark(3);
   unsigned g3 = arh::grid_for(nt, 256);
   unsigned cap3 = (unsigned)ctx->num_sms * 8;
   scatter_kernel<<<g3 > cap3 ? cap3 : g3, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->skeys,
                                                         B->svals, B->cells, B->spos, B->svel,
                                                         B->d_prev_n);
+  mark(4);
   int bs = 128;
   if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
   collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals,
                                                        B->cells, B->spos, B->svel, B->pforce);
+  mark(5);
   reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
       B->d_table, B->d_boff, ns, bt, B->pforce, ctx->d_err);
+  mark(6);
   B->host_prev_n = nt;
   return arh::check_launch("step");
+}
+
+// Run n_steps eagerly with events between the stages; average milliseconds per stage.
+ar_status profile_steps(ar_batch* B, int n_steps, float* stage_ms, cudaStream_t st) {
+  cudaEvent_t ev[kStages + 1];
+  for (auto& e : ev) cudaEventCreate(&e);
+  double acc[kStages] = {0};
+  ar_status s = AR_OK;
+  for (int i = 0; i < n_steps && s == AR_OK; ++i) {
+    s = enqueue_step(B, st, ev);
+    if (s != AR_OK) break;
+    if (cudaEventSynchronize(ev[kStages]) != cudaSuccess) {
+      s = arh::check_launch("profile");
+      break;
+    }
+    for (int k = 0; k < kStages; ++k) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+      acc[k] += ms;
+    }
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < kStages; ++k) stage_ms[k] = n_steps > 0 ? (float)(acc[k] / n_steps) : 0.f;
+  return s;
 }
 
 ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaStream_t st) {
@@ -635,6 +672,37 @@ ar_status ar_step(ar_ctx* ctx, ar_scene* s, int n_steps, int use_graph, ar_strea
   ar_status st = ensure_solo(s);
   if (st != AR_OK) return st;
   return batch_step(ctx, s->solo, n_steps, use_graph, arh::stream(stream));
+}
+
+ar_status ar_step_profile(ar_ctx* ctx, ar_scene* s, int n_steps, float* h_stage_ms,
+                          ar_stream_t stream) {
+  if (!ctx || !s || n_steps < 0 || !h_stage_ms) return AR_ERR_INVALID_ARG;
+  ar_status st = ensure_solo(s);
+  if (st != AR_OK) return st;
+  cudaStream_t cs = arh::stream(stream);
+  if ((st = prepare(s->solo, cs)) != AR_OK) return st;
+  return profile_steps(s->solo, n_steps, h_stage_ms, cs);
+}
+
+ar_status ar_batch_profile(ar_ctx* ctx, ar_batch* B, int n_steps, float* h_stage_ms,
+                           ar_stream_t stream) {
+  if (!ctx || !B || n_steps < 0 || !h_stage_ms) return AR_ERR_INVALID_ARG;
+  cudaStream_t cs = arh::stream(stream);
+  ar_status st = prepare(B, cs);
+  if (st != AR_OK) return st;
+  return profile_steps(B, n_steps, h_stage_ms, cs);
+}
+
+ar_status ar_scene_upload(ar_scene* s, const float* h_pos4, const float* h_quat4,
+                          const float* h_vel4, const float* h_ang4, ar_stream_t stream) {
+  if (!s) return AR_ERR_INVALID_ARG;
+  cudaStream_t st = arh::stream(stream);
+  const size_t bytes = 16 * (size_t)s->nb;
+  if (h_pos4) cudaMemcpyAsync(s->pos, h_pos4, bytes, cudaMemcpyHostToDevice, st);
+  if (h_quat4) cudaMemcpyAsync(s->quat, h_quat4, bytes, cudaMemcpyHostToDevice, st);
+  if (h_vel4) cudaMemcpyAsync(s->vel, h_vel4, bytes, cudaMemcpyHostToDevice, st);
+  if (h_ang4) cudaMemcpyAsync(s->ang, h_ang4, bytes, cudaMemcpyHostToDevice, st);
+  return arh::check_launch("ar_scene_upload");
 }
 
 ar_status ar_scene_particle_forces(ar_scene* s, float* p_force4, float* p_torque4,

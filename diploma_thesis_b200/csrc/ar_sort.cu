@@ -221,6 +221,10 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
     K k = sm.keys[i];
     uint32_t dd = digit_of(k, shift, mask);
     uint32_t dst = sm.gofs[dd] + (uint32_t)i - sm.digit_start[dd];
+    if (dst >= (uint32_t)n) {  // only after a timed-out look-back; never write out of range
+      ar::raise_error(err, ar::kErrTimeout);
+      continue;
+    }
     keys_out[dst] = k;
     vals_out[dst] = sm.vals[i];
   }

@@ -344,10 +344,16 @@ AR_API ar_status ar_scene_destroy(ar_scene* scene);
 /* Device bytes a scene with this description keeps resident (state + its share of the
  * step workspace); used for HBM-budget admission. */
 AR_API size_t ar_scene_footprint(const ar_scene_desc* desc);
-/* Copy body state to host arrays (any may be NULL). */
+/* Copy body state to host arrays (any may be NULL); synchronises the stream. */
 AR_API ar_status ar_scene_download(ar_scene* scene, float* h_body_pos4, float* h_body_quat4,
                                    float* h_body_vel4, float* h_body_angvel4,
                                    ar_stream_t stream);
+/* Overwrite body state from host arrays (any may be NULL); asynchronous (use pinned memory
+ * for overlap).  Replaces the reference's per-step host round trip of body state
+ * (Particles/updateFunctions.cpp:2903-2930). */
+AR_API ar_status ar_scene_upload(ar_scene* scene, const float* h_body_pos4,
+                                 const float* h_body_quat4, const float* h_body_vel4,
+                                 const float* h_body_angvel4, ar_stream_t stream);
 /* Device pointers of the scene's resident arrays (for tests / zero-copy consumers). */
 typedef struct ar_scene_view {
   int num_bodies, num_particles;
@@ -385,6 +391,13 @@ AR_API ar_status ar_scene_step_view(ar_scene* scene, ar_step_view* out);
 AR_API ar_status ar_step(ar_ctx* ctx, ar_scene* scene, int n_steps, int use_graph,
                          ar_stream_t stream);
 
+/* Run n_steps of the scene without a graph, with CUDA events between the stages, and return
+ * the average device milliseconds per stage in h_stage_ms[6]: clear, re-pose + hash,
+ * sort, scatter + cell ranges, DEM gather + walls, body sums + integration.  (Replaces the
+ * reference's clock() accumulators, e.g. RigidBodies/UniformGridUpdate.cpp:338-446.) */
+AR_API ar_status ar_step_profile(ar_ctx* ctx, ar_scene* scene, int n_steps, float* h_stage_ms,
+                                 ar_stream_t stream);
+
 /* Per-particle DEM + wall force of the last step (original particle order): copies N float4
  * to a device buffer.  p_torque4 is reserved and may be NULL (torques are summed per body
  * from the forces, see ar_scene_view.body_torque4). */
@@ -402,6 +415,9 @@ AR_API ar_status ar_batch_destroy(ar_batch* batch);
 AR_API ar_status ar_batch_set_scenes(ar_batch* batch, ar_scene* const* scenes, int n_scenes);
 AR_API ar_status ar_batch_step(ar_ctx* ctx, ar_batch* batch, int n_steps, int use_graph,
                                ar_stream_t stream);
+/* ar_step_profile for a batch. */
+AR_API ar_status ar_batch_profile(ar_ctx* ctx, ar_batch* batch, int n_steps,
+                                  float* h_stage_ms, ar_stream_t stream);
 /* Number of kernel launches one step of this batch issues (for launch accounting). */
 AR_API int ar_batch_launches_per_step(ar_batch* batch);
 AR_API int ar_scene_launches_per_step(ar_scene* scene);

@@ -1,0 +1,155 @@
+"""Generate the golden fixtures in this directory from the reference's own kernel bodies.
+
+    python tests/golden/make_golden.py
+
+Needs oracle/_ref/libref_cpu.so (built from the reference checkout by oracle/ref_build.py).
+Every array saved here is an output of the reference code (run on the CPU) on seeded
+inputs that are saved alongside; the oracle and the CUDA library are checked against them.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT))
+
+from diploma_thesis_b200 import scenes  # noqa: E402
+from diploma_thesis_b200._lib import SimParams  # noqa: E402  (struct layout only)
+from oracle import ref  # noqa: E402
+
+OUT = Path(__file__).resolve().parent
+
+
+def params_for(radius, origin, cell, dims, spring, damping, shear, attraction=0.0,
+               gravity=(0.0, -0.012, 0.0), w_damping=0.99):
+    p = SimParams()
+    p.particle_radius = radius
+    for a in range(3):
+        p.world_origin[a] = origin[a]
+        p.cell_size[a] = cell
+        p.grid_size[a] = dims[a]
+        p.gravity[a] = gravity[a]
+    p.num_cells = int(np.prod(dims))
+    p.spring, p.damping, p.shear, p.attraction = spring, damping, shear, attraction
+    p.w_damping = w_damping
+    return p
+
+
+def lbvh_case(seed: int, n: int, dup_frac: float):
+    rng = np.random.default_rng(seed)
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.random((n, 3), dtype=np.float32)
+    ndup = int(n * dup_frac)
+    src = rng.integers(0, n, ndup)
+    dst = rng.integers(0, n, ndup)
+    pos[dst] = pos[src]
+    mn, mx = ref.aabb(pos)
+    codes, idx = ref.morton30(pos, mn, mx)
+    skeys, svals = ref.sort_pairs_u32(codes, idx.view(np.uint32))
+    tree = ref.radix_tree(skeys)
+    r = np.float32(0.002)
+    cms, leaf_bounds, bounds, radii = ref.leaves_and_refit(tree, svals.astype(np.int32), pos, r)
+    return dict(pos=pos, mn=mn, mx=mx, codes=codes, skeys=skeys, svals=svals,
+                is_leaf=tree["is_leaf"], left=tree["left"], right=tree["right"],
+                parent=tree["parent"], min_r=tree["min_r"], max_r=tree["max_r"],
+                radius=np.float32(r), cms=cms, leaf_bounds=leaf_bounds, bounds=bounds)
+
+
+def dem_case(seed: int):
+    sc = scenes.small_scene(seed, nb_side=5, packed=True)
+    rng = np.random.default_rng(seed + 100)
+    pos = sc.world_positions()
+    n = len(pos)
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0, 0.3, (n, 3))
+    rel = sc.particle_rel.copy()
+    rb = sc.body_index()
+    dims = (16, 16, 16)  # wrapped grid (exercises the & (G-1) aliasing)
+    cell = np.float32(2 * sc.radius)
+    prm = params_for(sc.radius, (0.0, 0.0, 0.0), cell, dims, 0.5, 0.02, 0.1, 0.001)
+    h, idx = ref.calc_hash(prm, pos)
+    sh, si = ref.sort_pairs_u32(h, idx)
+    cs, ce, sp, sv = ref.reorder(sh, si, pos, vel, int(np.prod(dims)))
+    pf, pt = ref.collide_grid_dem(prm, rb, sp, sv, rel, si, cs, ce)
+    # BVH path on the same particles
+    mn, mx = ref.aabb(pos)
+    codes, cidx = ref.morton30(pos, mn, mx)
+    bk, bv = ref.sort_pairs_u32(codes, cidx.view(np.uint32))
+    tree = ref.radix_tree(bk)
+    cms, _, bounds, radii = ref.leaves_and_refit(tree, bv.astype(np.int32), pos, sc.radius)
+    bpf, bpt, bpp = ref.collide_bvh_rigid(prm, rb, rel, vel, tree, cms, bounds,
+                                          bv.astype(np.int32), radii)
+    cd, cpi, cbi = ref.find_rb_collisions_bvh(prm, rb, tree, cms, bounds, bv.astype(np.int32),
+                                              radii, np.zeros(n, np.float32))
+    # per-body reduction as the reference does it (scan differences)
+    nb = sc.num_bodies
+    bvel = rng.normal(0, 1, (nb, 4)).astype(np.float32)
+    bang = rng.normal(0, 1, (nb, 4)).astype(np.float32)
+    counts = np.diff(sc.body_offsets).astype(np.int32)
+    rvel, rang = ref.reduce_impulses(pf, pt, bvel, bang, sc.body_mass, sc.body_inv_inertia,
+                                     counts)
+    return dict(pos=pos, vel=vel, rel=rel, rb=rb, offsets=sc.body_offsets, radius=np.float32(sc.radius),
+                cell=cell, dims=np.array(dims, np.uint32), prm=np.array([0.5, 0.02, 0.1, 0.001], np.float32),
+                hash=h, shash=sh, sidx=si, cell_start=cs, cell_end=ce, spos=sp, svel=sv,
+                pforce=pf, ptorque=pt, mn=mn, mx=mx, bvh_keys=bk, bvh_idx=bv, cms=cms,
+                bounds=bounds, radii=radii, bvh_pforce=bpf, bvh_ptorque=bpt, bvh_ppos=bpp,
+                contact_distance=cd, contact_particle=cpi, contact_body=cbi,
+                body_mass=sc.body_mass, body_inv_inertia=sc.body_inv_inertia, bvel=bvel,
+                bang=bang, ref_reduced_vel=rvel, ref_reduced_ang=rang)
+
+
+def body_case(seed: int):
+    sc = scenes.small_scene(seed, nb_side=3, v_sigma=1.0)
+    rng = np.random.default_rng(seed + 7)
+    nb = sc.num_bodies
+    st = {"cms": sc.body_pos.copy(), "vel": rng.normal(0, 1, (nb, 4)).astype(np.float32),
+          "ang": rng.normal(0, 3, (nb, 4)).astype(np.float32), "quat": sc.body_quat.copy(),
+          "ib": sc.body_inv_inertia.copy(), "cur": np.zeros((nb, 9), np.float32),
+          "model": np.zeros((nb, 16), np.float32), "cum": scenes.random_quaternions(rng, nb).astype(np.float32)}
+    st["ang"][0] = 0.0  # below the rotation threshold: identity branch
+    prm = params_for(sc.radius, (0, 0, 0), 1.0, (1, 1, 1), 0.5, 0.0, 0.0)
+    out = ref.gpu_integrator(prm, 0.05, st)
+    rb = sc.body_index()
+    rel, pos, vel, q = ref.global_attributes(out["cms"], out["vel"], out["ang"], out["quat"], rb,
+                                             sc.particle_rel)
+    # walls: push the scene against the -x / +y walls with velocities toward them
+    ppos = pos.copy()
+    bpos = out["cms"].copy()
+    ppos[:, 0] -= 0.47
+    bpos[:, 0] -= 0.47
+    ppos[:, 1] += 0.47
+    bpos[:, 1] += 0.47
+    wv = out["vel"].copy()
+    wv[:, 0] = -np.abs(wv[:, 0])
+    wv[:, 1] = np.abs(wv[:, 1])
+    counts = np.diff(sc.body_offsets).astype(np.int32)
+    wvel, wang = ref.wall_collisions(ppos, bpos, [0, 0, 0], [1, 1, 1], wv, out["ang"],
+                                     sc.body_inv_inertia, sc.body_mass, rb, counts, sc.radius)
+    return dict(in_cms=st["cms"], in_vel=st["vel"], in_ang=st["ang"], in_quat=st["quat"],
+                in_cum=st["cum"], ib=st["ib"], dt=np.float32(0.05),
+                gravity=np.array([0, -0.012, 0], np.float32), w_damping=np.float32(0.99),
+                out_cms=out["cms"], out_vel=out["vel"], out_ang=out["ang"], out_quat=out["quat"],
+                out_cur=out["cur"], out_model=out["model"], out_cum=out["cum"],
+                rb=rb, in_rel=sc.particle_rel, out_rel=rel, out_pos=pos, out_pvel=vel,
+                out_q_reset=q, wall_ppos=ppos, wall_bpos=bpos, wall_vel_in=wv,
+                wall_ang_in=out["ang"], mass=sc.body_mass, offsets=sc.body_offsets,
+                radius=np.float32(sc.radius), wall_vel_out=wvel, wall_ang_out=wang)
+
+
+def main() -> None:
+    if not ref.available():
+        raise SystemExit("oracle/_ref/libref_cpu.so is not built (run oracle/ref_build.py)")
+    ref.set_threads(1)
+    np.savez_compressed(OUT / "lbvh_uniform.npz", **lbvh_case(11, 3000, 0.0))
+    np.savez_compressed(OUT / "lbvh_duplicates.npz", **lbvh_case(12, 3000, 0.2))
+    np.savez_compressed(OUT / "dem_small.npz", **dem_case(5))
+    np.savez_compressed(OUT / "bodies_small.npz", **body_case(9))
+    for f in sorted(OUT.glob("*.npz")):
+        print(f.name, f.stat().st_size)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,142 @@
+"""The fused step (ar_step / ar_batch_step) against the oracle's float32 restatement
+(bit-exact), against the FP64 oracle (stated tolerances), and batched against solo."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from diploma_thesis_b200 import api, scenes
+from gpu_util import host
+from oracle import cpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _scene_state(gs: api.GpuScene) -> dict:
+    return gs.download()
+
+
+def _sorted_arrays(gs: api.GpuScene):
+    v = gs.step_view()
+    n = v.num_particles
+    keys = api.device_view(v.sorted_keys, n, torch.int32).cpu().numpy().view(np.uint32)
+    idx = api.device_view(v.sorted_idx, n, torch.int32).cpu().numpy().view(np.uint32)
+    pf = api.device_view(v.particle_force4, 4 * n, torch.float32).cpu().numpy().reshape(n, 4)
+    return keys, idx, pf
+
+
+@pytest.mark.parametrize("seed,packed", [(1, True), (2, False)])
+def test_one_step_bit_exact_with_oracle(ctx, seed, packed):
+    sc = scenes.small_scene(seed, nb_side=5, packed=packed, r=1 / 128)
+    gs = api.GpuScene(ctx, sc)
+    o, c, d = gs.grid_info()
+    assert (o, d) == (cpu.scene_grid(sc)[0], cpu.scene_grid(sc)[2])
+    gs.step(1, use_graph=False)
+    ctx.check()
+    ref = cpu.step(sc, 1)
+    got = gs.download()
+    keys, idx, pf = _sorted_arrays(gs)
+    assert np.array_equal(keys, ref["skeys"]) and np.array_equal(idx, ref["sidx"])
+    assert np.array_equal(pf, ref["pforce"])
+    if packed:
+        assert (np.abs(pf).sum(1) > 0).sum() > 100
+    for k in ("pos", "quat", "vel", "angvel"):
+        assert np.array_equal(got[k], ref[k]), k
+    gs.close()
+
+
+def test_hundred_steps_bit_exact_and_near_fp64(ctx):
+    sc = scenes.small_scene(3, nb_side=4, packed=True, r=1 / 128)
+    gs = api.GpuScene(ctx, sc)
+    gs.step(100, use_graph=True)
+    ctx.check()
+    got = gs.download()
+    ref = cpu.step(sc, 100)
+    for k in ("pos", "quat", "vel", "angvel"):
+        assert np.array_equal(got[k], ref[k]), k
+    f64 = cpu.step_f64(sc, 100)
+    # trajectory tolerance against FP64 after 100 steps: 1e-3 r in position
+    assert np.abs(got["pos"][:, :3] - f64["pos"][:, :3]).max() <= 1e-3 * sc.radius
+    gs.close()
+
+
+def test_graph_and_eager_agree(ctx):
+    sc = scenes.small_scene(5, nb_side=4, packed=True, r=1 / 128)
+    a, b = api.GpuScene(ctx, sc), api.GpuScene(ctx, sc)
+    a.step(17, use_graph=True)
+    b.step(17, use_graph=False)
+    da, db = a.download(), b.download()
+    for k in da:
+        assert np.array_equal(da[k], db[k]), k
+    a.close()
+    b.close()
+
+
+def test_batch_equals_solo_bit_for_bit(ctx):
+    sizes = [(2, 3), (3, 4), (4, 3), (5, 5)]
+    solo, members = [], []
+    for i, (seed, side) in enumerate(sizes):
+        sc = scenes.small_scene(seed + 10, nb_side=side, packed=(i % 2 == 0), r=1 / 128,
+                                box=0.6 + 0.2 * i)
+        solo.append(api.GpuScene(ctx, sc))
+        members.append(api.GpuScene(ctx, sc))
+    batch = api.Batch(ctx, members)
+    batch.step(25)
+    for s in solo:
+        s.step(25)
+    ctx.check()
+    for s, m in zip(solo, members):
+        a, b = s.download(), m.download()
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+    # change membership mid-run: remaining scenes continue identically
+    batch.set_scenes(members[1:3])
+    batch.step(10)
+    for s in solo[1:3]:
+        s.step(10)
+    for s, m in zip(solo[1:3], members[1:3]):
+        a, b = s.download(), m.download()
+        for k in a:
+            assert np.array_equal(a[k], b[k]), k
+    batch.close()
+    for s in solo + members:
+        s.close()
+
+
+def test_nan_state_is_reported(ctx):
+    sc = scenes.small_scene(8, nb_side=2, r=1 / 128)
+    sc.body_vel[1, 0] = np.nan
+    gs = api.GpuScene(ctx, sc)
+    gs.step(1, use_graph=False)
+    assert ctx.status() == 4  # AR_ERR_NAN
+    assert ctx.status() == 0
+    gs.close()
+
+
+def test_invalid_scene_arguments(ctx):
+    from diploma_thesis_b200 import _lib
+    sc = scenes.small_scene(1, nb_side=2)
+    d = api.make_desc(sc)
+    d.block_size = 100
+    init = _lib.SceneInit()
+    h = C.c_void_p()
+    assert _lib.lib.ar_scene_create(ctx.handle, C.byref(d), C.byref(init), None, C.byref(h)) == 1
+    with pytest.raises(_lib.ArError):
+        sc2 = scenes.small_scene(1, nb_side=2)
+        sc2.body_offsets = sc2.body_offsets.copy()
+        sc2.body_offsets[-1] += 1
+        api.GpuScene(ctx, sc2)
+
+
+def test_config0_first_steps_bit_exact(ctx):
+    sc = scenes.config0(0)
+    gs = api.GpuScene(ctx, sc)
+    assert gs.grid_info()[2] == [128, 128, 128]
+    gs.step(2, use_graph=True)
+    ctx.check()
+    ref = cpu.step(sc, 2)
+    got = gs.download()
+    for k in ("pos", "quat", "vel", "angvel"):
+        assert np.array_equal(got[k], ref[k]), k
+    gs.close()
