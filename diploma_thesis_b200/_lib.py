@@ -104,6 +104,14 @@ SIGNATURES = {
     "ar_reduce_impulses": [P, P, P, P, I, P, P, P, P, S],
     "ar_integrate_reference": [P, C.POINTER(SimParams), F, I, P, P, P, P, P, P, P, P, P, S],
     "ar_global_attributes": [P, I, I, P, P, P, P, P, P, P, P, S],
+    "ar_reset_quaternions": [P, P, I, S],
+    "ar_integrate_momentum": [P, C.POINTER(SimParams), F, I, P, P, P, P, P, P, P, P, P, P, P, P,
+                              P, C.POINTER(F), C.POINTER(F), S],
+    "ar_integrate_particles": [P, C.POINTER(SimParams), F, P, P, P, I, C.POINTER(F),
+                               C.POINTER(F), S],
+    "ar_fill_f32": [P, P, C.c_long, F, S],
+    "ar_collide_grid_particles": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, I, P, P, P, S],
+    "ar_reduce_rigid_body_variables": [P, P, P, P, P, I, P, P, S],
     "ar_walls_reference": [P, F, P, P, C.POINTER(F), C.POINTER(F), P, P, P, P, P, P, I, I, S],
     "ar_scene_create": [P, C.POINTER(SceneDesc), C.POINTER(SceneInit), S, C.POINTER(P)],
     "ar_scene_destroy": [P],

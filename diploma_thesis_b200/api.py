@@ -198,7 +198,7 @@ class _DeviceArray:
 
     def __init__(self, addr: int, count: int, dtype: torch.dtype):
         self.__cuda_array_interface__ = {"shape": (count,), "typestr": self._TYPESTR[dtype],
-                                         "data": (int(addr), True), "version": 3,
+                                         "data": (int(addr), False), "version": 3,
                                          "strides": None}
 
 

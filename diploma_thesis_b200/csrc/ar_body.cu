@@ -129,6 +129,118 @@ __global__ void reset_quat_kernel(int nb, float4* __restrict__ quat) {
   if (b < nb) quat[b] = make_float4(0.f, 0.f, 0.f, 1.f);
 }
 
+// ---- integrateRigidBody (Kernels/rigidBodyKernels.cu:40-166): momentum form with box clamp --
+struct MomentumArgs {
+  float4 *cms, *vel, *force, *ang, *quat, *torque, *ang_mom, *lin_mom;
+  const float* inv_inertia;
+  float* cur_inertia;
+  float* ang_acc;  // glm::vec3 per body
+  const float *radii, *mass;
+};
+
+__global__ void __launch_bounds__(128) integrate_momentum_kernel(MomentumArgs a, float dt,
+                                                                 float3 mn, float3 mx,
+                                                                 float3 gravity, float bdamp,
+                                                                 float gdamp, int nb) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  float4 L = a.lin_mom[b];
+  const float4 F = a.force[b];
+  L = make_float4(L.x + F.x * dt, L.y + F.y * dt, L.z + F.z * dt, L.w + F.w * dt);
+  L = make_float4(L.x + gravity.x * dt, L.y + gravity.y * dt, L.z + gravity.z * dt, L.w + 0.f * dt);
+  // the box is widened by double-precision literals, as written in the reference
+  mx.x = (float)((double)mx.x + 0.1); mx.y = (float)((double)mx.y + 0.1); mx.z = (float)((double)mx.z + 0.1);
+  mn.x = (float)((double)mn.x - 0.1); mn.y = (float)((double)mn.y - 0.1); mn.z = mn.z - 1;
+  float4 p = a.cms[b];
+  const float m = a.mass[b], r = a.radii[b];
+  if (p.x > mx.x - r) { p.x = mx.x - r; L.x *= bdamp; }
+  if (p.x < mn.x + r) { p.x = mn.x + r; L.x *= bdamp; }
+  if (p.y > mx.y - r && L.y > 0) { p.y = mx.y - 2 * r; L.y *= bdamp; }
+  if (p.y < mn.y + r) { p.y = mn.y + r; L.y *= bdamp; }
+  if (p.z > mx.z - r) { p.z = mx.z - r; L.z *= bdamp; }
+  if (p.z < mn.z + r) { p.z = mn.z + r; L.z *= bdamp; }
+  L = make_float4(L.x * gdamp, L.y * gdamp, L.z * gdamp, L.w * gdamp);
+  float4 v = make_float4(L.x * m, L.y * m, L.z * m, L.w * m);
+  a.lin_mom[b] = L;
+  p = make_float4(p.x + v.x * dt, p.y + v.y * dt, p.z + v.z * dt, p.w + v.w * dt);
+  p.w = 0.f;
+  v.w = 0.f;
+  a.cms[b] = p;
+  a.vel[b] = v;
+  a.force[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 q = a.quat[b];
+  float R[9], I[9], RI[9], Rt[9], C[9];
+  ar_glm::mat3_cast(q, R);
+  for (int k = 0; k < 9; ++k) I[k] = a.inv_inertia[9 * b + k];
+  ar_glm::mm(R, I, RI);
+  ar_glm::transpose(R, Rt);
+  ar_glm::mm(RI, Rt, C);
+  float4 am = a.ang_mom[b];
+  const float4 tq = a.torque[b];
+  am = make_float4(am.x + tq.x * dt, am.y + tq.y * dt, am.z + tq.z * dt, am.w + tq.w * dt);
+  const float3 cm3 = ar::mk3(am.x, am.y, am.z);
+  float3 nv = ar_glm::mv(C, cm3);
+  const float3 acc = ar_glm::mv(C, ar_glm::cross3(cm3, nv));
+  float4 qd = ar_glm::qmul(make_float4(nv.x, nv.y, nv.z, 0.f), q);  // glm::quat(0, w) * q
+  qd = make_float4(qd.x / 2.f, qd.y / 2.f, qd.z / 2.f, qd.w / 2.f);
+  q = make_float4(q.x + qd.x * dt, q.y + qd.y * dt, q.z + qd.z * dt, q.w + qd.w * dt);
+  q = ar_glm::qnormalize(q);
+  nv = ar::mk3(nv.x - acc.x * dt, nv.y - acc.y * dt, nv.z - acc.z * dt);
+  if (a.ang_acc) {
+    a.ang_acc[3 * b] = acc.x; a.ang_acc[3 * b + 1] = acc.y; a.ang_acc[3 * b + 2] = acc.z;
+  }
+  for (int k = 0; k < 9; ++k) a.cur_inertia[9 * b + k] = C[k];
+  a.ang_mom[b] = am;
+  a.quat[b] = q;
+  a.ang[b] = make_float4(nv.x, nv.y, nv.z, 0.f);
+  a.torque[b] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// ---- integrate_functor (Kernels/particleKernels.cu:50-128): free particles only -------------
+__global__ void __launch_bounds__(256) integrate_particles_kernel(
+    float4* __restrict__ pos, float4* __restrict__ vel, const int32_t* __restrict__ rb_idx,
+    int n, float dt, float3 mn, float3 mx, float3 gravity, float gdamp, float bdamp, float r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (rb_idx[i] >= 0) return;  // particles of rigid bodies are moved by their body
+  const float4 p4 = pos[i], v4 = vel[i];
+  float3 p = ar::mk3(p4.x, p4.y, p4.z), v = ar::mk3(v4.x, v4.y, v4.z);
+  v = ar::add(v, ar::mk3(gravity.x * dt, gravity.y * dt, gravity.z * dt));
+  v = ar::mk3(v.x * gdamp, v.y * gdamp, v.z * gdamp);
+  p = ar::add(p, ar::mk3(v.x * dt, v.y * dt, v.z * dt));
+  mx.x = (float)((double)mx.x + 0.01); mx.y = (float)((double)mx.y + 0.01); mx.z = (float)((double)mx.z + 0.01);
+  mn.x = (float)((double)mn.x - 0.01); mn.y = (float)((double)mn.y - 0.01); mn.z = (float)((double)mn.z - 0.01);
+  if (p.x > mx.x - r) { p.x = mx.x - r; v.x *= bdamp; }
+  if (p.x < mn.x + r) { p.x = mn.x + r; v.x *= bdamp; }
+  if (p.y > mx.y - r && v.y > 0) { p.y = mx.y - r; v.y *= bdamp; }
+  if (p.z > mx.z - r) { p.z = mx.z - r; v.z *= bdamp; }
+  if (p.z < mn.z + r) { p.z = mn.z + r; v.z *= bdamp; }
+  if (p.y < mn.y + r) { p.y = mn.y + r; v.y *= bdamp; }
+  pos[i] = make_float4(p.x, p.y, p.z, p4.w);
+  vel[i] = make_float4(v.x, v.y, v.z, v4.w);
+}
+
+// ---- ReduceRigidBodyVariables (Kernels/rigidBodyKernels.cu:861-1043): per rigid object
+// rb_force += sum(p_force), rb_torque += sum(p_torque) over [start, start + count); a non-finite
+// sum raises the NaN error (the reference sets *toExit).
+__global__ void __launch_bounds__(256) reduce_rbvars_kernel(
+    const float4* __restrict__ pf, const float4* __restrict__ pt, const int32_t* __restrict__ start,
+    const int32_t* __restrict__ count, int nb, float4* __restrict__ bf, float4* __restrict__ bt,
+    int* __restrict__ err) {
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nb; b += warps) {
+    const int s = __ldg(start + b);
+    float3 f, t;
+    ar_body::warp_segment_sum(pf, pt, s, s + __ldg(count + b), &f, &t);
+    if (ar::lane_id() == 0) {
+      if (!isfinite(f.x + f.y + f.z) || !isfinite(t.x + t.y + t.z)) ar::raise_error(err, ar::kErrNaN);
+      float4 a = bf[b], c = bt[b];
+      bf[b] = make_float4(a.x + f.x, a.y + f.y, a.z + f.z, a.w);
+      bt[b] = make_float4(c.x + t.x, c.y + t.y, c.z + t.z, c.w);
+    }
+  }
+}
+
 // ---- WallCollisionWrapper (WallCollisions.cu:46-90, 95-129, 201-276, 338-597) -------------------
 struct Walls {
   float pos[6];  // wall position per plane, planes +x, +y, +z, -x, -y, -z
@@ -304,9 +416,72 @@ ar_status ar_global_attributes(ar_ctx* ctx, int n, int num_bodies, const float* 
     global_attributes_kernel<<<arh::grid_for(n, 256), 256, 0, st>>>(
         n, (const float4*)cms4, (const float4*)rb_vel4, (const float4*)rb_ang4,
         (const float4*)quat4, rb_idx, (float4*)rel4, (float4*)pos4, (float4*)vel4);
-  if (num_bodies > 0)
-    reset_quat_kernel<<<arh::grid_for(num_bodies, 256), 256, 0, st>>>(num_bodies, (float4*)quat4);
   return arh::check_launch("ar_global_attributes");
+}
+
+ar_status ar_reset_quaternions(ar_ctx* ctx, float* quat4, int num_bodies, ar_stream_t stream) {
+  if (!ctx || num_bodies < 0 || (num_bodies > 0 && !quat4)) return AR_ERR_INVALID_ARG;
+  if (num_bodies > 0)
+    reset_quat_kernel<<<arh::grid_for(num_bodies, 256), 256, 0, arh::stream(stream)>>>(
+        num_bodies, (float4*)quat4);
+  return arh::check_launch("ar_reset_quaternions");
+}
+
+ar_status ar_integrate_momentum(ar_ctx* ctx, const ar_sim_params* params, float dt,
+                                int num_bodies, float* cms4, float* vel4, float* force4,
+                                float* ang4, float* quat4, float* torque4, float* ang_mom4,
+                                float* lin_mom4, const float* inv_inertia9,
+                                float* cur_inv_inertia9, float* ang_acc3, const float* radii,
+                                const float* mass, const float h_min_pos3[3],
+                                const float h_max_pos3[3], ar_stream_t stream) {
+  if (!ctx || !params || !h_min_pos3 || !h_max_pos3 || num_bodies < 0 ||
+      (num_bodies > 0 && (!cms4 || !vel4 || !force4 || !ang4 || !quat4 || !torque4 ||
+                          !ang_mom4 || !lin_mom4 || !inv_inertia9 || !cur_inv_inertia9 ||
+                          !radii || !mass)))
+    return AR_ERR_INVALID_ARG;
+  if (num_bodies == 0) return AR_OK;
+  MomentumArgs a{(float4*)cms4, (float4*)vel4, (float4*)force4, (float4*)ang4, (float4*)quat4,
+                 (float4*)torque4, (float4*)ang_mom4, (float4*)lin_mom4, inv_inertia9,
+                 cur_inv_inertia9, ang_acc3, radii, mass};
+  integrate_momentum_kernel<<<arh::grid_for(num_bodies, 128), 128, 0, arh::stream(stream)>>>(
+      a, dt, make_float3(h_min_pos3[0], h_min_pos3[1], h_min_pos3[2]),
+      make_float3(h_max_pos3[0], h_max_pos3[1], h_max_pos3[2]),
+      make_float3(params->gravity[0], params->gravity[1], params->gravity[2]),
+      params->boundary_damping, params->global_damping, num_bodies);
+  return arh::check_launch("ar_integrate_momentum");
+}
+
+ar_status ar_integrate_particles(ar_ctx* ctx, const ar_sim_params* params, float dt, float* pos4,
+                                 float* vel4, const int32_t* rb_idx, int n,
+                                 const float h_min_pos3[3], const float h_max_pos3[3],
+                                 ar_stream_t stream) {
+  if (!ctx || !params || !h_min_pos3 || !h_max_pos3 || n < 0 ||
+      (n > 0 && (!pos4 || !vel4 || !rb_idx)))
+    return AR_ERR_INVALID_ARG;
+  if (n == 0) return AR_OK;
+  integrate_particles_kernel<<<arh::grid_for(n, 256), 256, 0, arh::stream(stream)>>>(
+      (float4*)pos4, (float4*)vel4, rb_idx, n, dt,
+      make_float3(h_min_pos3[0], h_min_pos3[1], h_min_pos3[2]),
+      make_float3(h_max_pos3[0], h_max_pos3[1], h_max_pos3[2]),
+      make_float3(params->gravity[0], params->gravity[1], params->gravity[2]),
+      params->global_damping, params->boundary_damping, params->particle_radius);
+  return arh::check_launch("ar_integrate_particles");
+}
+
+ar_status ar_reduce_rigid_body_variables(ar_ctx* ctx, const float* p_force4,
+                                         const float* p_torque4, const int32_t* starts,
+                                         const int32_t* counts, int num_bodies,
+                                         float* rb_force4, float* rb_torque4,
+                                         ar_stream_t stream) {
+  if (!ctx || num_bodies < 0 ||
+      (num_bodies > 0 && (!p_force4 || !p_torque4 || !starts || !counts || !rb_force4 ||
+                          !rb_torque4)))
+    return AR_ERR_INVALID_ARG;
+  if (num_bodies == 0) return AR_OK;
+  reduce_rbvars_kernel<<<warp_grid(ctx, num_bodies, 256), 256, 0, arh::stream(stream)>>>(
+      (const float4*)p_force4, (const float4*)p_torque4, starts, counts, num_bodies,
+      (float4*)rb_force4, (float4*)rb_torque4, ctx->d_err);
+  return arh::check_launch("ar_reduce_rigid_body_variables");
 }
 
 ar_status ar_walls_reference(ar_ctx* ctx, float radius, const float* particle_pos4,

@@ -1,6 +1,8 @@
 // (a13) grid hash, (a14) reorder + cell ranges, (a15) DEM gather, grid contact pairs.
 // Stage entry points with the reference wrappers' semantics; the fused step uses its own
 // kernels (ar_pipeline.cu) built from the same device functions.
+#include <cstring>
+
 #include "ar_internal.cuh"
 #include "ar_dem.cuh"
 #include "ar_grid.cuh"
@@ -91,6 +93,57 @@ __global__ void __launch_bounds__(128) collide_grid_kernel(
   const float3 t = ar::cross(ar::xyz(__ldg(rel + orig)), lin);
   float4 q = p_torque[orig];
   p_torque[orig] = make_float4(q.x + t.x, q.y + t.y, q.z + t.z, q.w + 0.f);
+}
+
+// collideD / collideCell / collideSpheres (Kernels/particleKernels.cu:261-406): the particle
+// variant -- every occupant that passes the body test contributes (zero when apart), torque
+// accumulates per cell, free particles (body -1) get their velocity updated instead.
+__global__ void __launch_bounds__(128) collide_particles_kernel(
+    ar_sim_params prm, ar_grid::Grid g, const int32_t* __restrict__ rb_idx,
+    const float4* __restrict__ spos, const float4* __restrict__ svel,
+    const float4* __restrict__ rel, const uint32_t* __restrict__ gidx,
+    const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, int n,
+    float4* __restrict__ p_force, float4* __restrict__ p_torque, float4* __restrict__ new_vel) {
+  const int index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= n) return;
+  const float3 pos = ar::xyz(__ldg(spos + index));
+  const float3 vel = ar::xyz(__ldg(svel + index));
+  const int3 gp = g.cell_of(pos);
+  const uint32_t orig = __ldg(gidx + index);
+  const int body = __ldg(rb_idx + orig);
+  const float cd = prm.particle_radius + prm.particle_radius;
+  const float3 r3 = ar::xyz(__ldg(rel + orig));
+  float3 force = ar::mk3(0.f, 0.f, 0.f), torque = ar::mk3(0.f, 0.f, 0.f);
+  for (int z = -1; z <= 1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x) {
+        float3 cf = ar::mk3(0.f, 0.f, 0.f);
+        const uint32_t h = g.hash(make_int3(gp.x + x, gp.y + y, gp.z + z));
+        const uint32_t st = __ldg(cstart + h);
+        if (st != ar::kEmpty) {
+          const uint32_t en = __ldg(cend + h);
+          for (uint32_t j = st; j < en; ++j) {
+            if (!(j != (uint32_t)index && (body != __ldg(rb_idx + __ldg(gidx + j)) || body == -1)))
+              continue;
+            const float3 p2 = ar::xyz(__ldg(spos + j));
+            const float3 rp = ar::sub(p2, pos);
+            const float dist = sqrtf(ar::dot(rp, rp));
+            float3 f = ar::mk3(0.f, 0.f, 0.f);
+            if (dist < cd)
+              f = ar_dem::spring_force(rp, dist, ar::sub(ar::xyz(__ldg(svel + j)), vel), cd,
+                                       prm.spring, prm.damping, prm.shear, prm.attraction);
+            cf = ar::add(cf, f);
+          }
+        }
+        force = ar::add(force, cf);
+        torque = ar::add(torque, ar::cross(r3, cf));
+      }
+  if (body == -1) {
+    if (new_vel) new_vel[orig] = make_float4(vel.x + force.x, vel.y + force.y, vel.z + force.z, 0.f);
+  } else {
+    p_force[orig] = make_float4(force.x, force.y, force.z, 0.f);
+    p_torque[orig] = make_float4(torque.x, torque.y, torque.z, 0.f);
+  }
 }
 
 __global__ void __launch_bounds__(128) pairs_grid_kernel(
@@ -191,6 +244,37 @@ ar_status ar_collide_grid_dem(ar_ctx* ctx, const ar_sim_params* params, const in
       (const float4*)rel4, grid_idx, cell_start, cell_end, n, (float4*)p_force4,
       (float4*)p_torque4);
   return arh::check_launch("ar_collide_grid_dem");
+}
+
+ar_status ar_collide_grid_particles(ar_ctx* ctx, const ar_sim_params* params,
+                                    const int32_t* rb_idx, const float* sorted_pos4,
+                                    const float* sorted_vel4, const float* rel4,
+                                    const uint32_t* grid_idx, const uint32_t* cell_start,
+                                    const uint32_t* cell_end, int n, float* p_force4,
+                                    float* p_torque4, float* new_vel4, ar_stream_t stream) {
+  if (!ctx || !params || n < 0 ||
+      (n > 0 && (!rb_idx || !sorted_pos4 || !sorted_vel4 || !rel4 || !grid_idx || !cell_start ||
+                 !cell_end || !p_force4 || !p_torque4)))
+    return AR_ERR_INVALID_ARG;
+  ar_grid::Grid g;
+  ar_status s = grid_from_params(params, &g);
+  if (s != AR_OK || n == 0) return s;
+  collide_particles_kernel<<<arh::grid_for(n, 128), 128, 0, arh::stream(stream)>>>(
+      *params, g, rb_idx, (const float4*)sorted_pos4, (const float4*)sorted_vel4,
+      (const float4*)rel4, grid_idx, cell_start, cell_end, n, (float4*)p_force4,
+      (float4*)p_torque4, (float4*)new_vel4);
+  return arh::check_launch("ar_collide_grid_particles");
+}
+
+ar_status ar_fill_f32(ar_ctx* ctx, float* dst, long n, float value, ar_stream_t stream) {
+  if (!ctx || n < 0 || (n > 0 && !dst)) return AR_ERR_INVALID_ARG;
+  if (n == 0) return AR_OK;
+  uint32_t bits;
+  memcpy(&bits, &value, 4);
+  unsigned g = arh::grid_for(n, 256);
+  unsigned cap = (unsigned)ctx->num_sms * 8;
+  fill_kernel<<<g > cap ? cap : g, 256, 0, arh::stream(stream)>>>((uint32_t*)dst, n, bits);
+  return arh::check_launch("ar_fill_f32");
 }
 
 ar_status ar_pairs_grid(ar_ctx* ctx, const ar_sim_params* params, const int32_t* rb_idx,

@@ -126,6 +126,19 @@ __global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t* __rest
   }
 }
 
+// Parent links from the child links, for callers with the reference's traversal signature
+// (collideBVHSoARigidBodyWrapper passes no parent array): one thread per internal node.
+__global__ void __launch_bounds__(256) parents_kernel(int n, const int32_t* __restrict__ left,
+                                                      const int32_t* __restrict__ right,
+                                                      int32_t* __restrict__ parent) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int node = n + i;
+  parent[__ldg(left + node)] = node;
+  parent[__ldg(right + node)] = node;
+  if (i == 0) parent[n] = -1;
+}
+
 // ---- traversal helpers -------------------------------------------------------------------------
 struct Box {
   float lx, ly, lz, hx, hy, hz;
@@ -301,6 +314,17 @@ __global__ void __launch_bounds__(128) pairs_bvh_kernel(
        });
 }
 
+
+// parent links: the caller's, or derived into scratch when the caller has none
+const int32_t* parents_or_derive(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
+                                 const int32_t* parent, cudaStream_t st) {
+  if (parent || n < 2) return parent;
+  int32_t* p = (int32_t*)arh::scratch(ctx, (size_t)(2 * n - 1) * sizeof(int32_t));
+  if (!p) return nullptr;
+  parents_kernel<<<arh::grid_for(n - 1, 256), 256, 0, st>>>(n, left, right, p);
+  return p;
+}
+
 }  // namespace
 
 extern "C" {
@@ -364,10 +388,12 @@ ar_status ar_collide_bvh_dem(ar_ctx* ctx, const ar_sim_params* params, const int
                              const float* radii, int n, float* p_force4, float* p_torque4,
                              float* p_positions4, ar_stream_t stream) {
   if (!ctx || !params || n < 0 ||
-      (n > 0 && (!rb_idx || !rel4 || !vel4 || !is_leaf || !left || !right || !parent ||
+      (n > 0 && (!rb_idx || !rel4 || !vel4 || !is_leaf || !left || !right ||
                  !cms4 || !bounds8 || !sorted_idx || !radii || !p_force4 || !p_torque4)))
     return AR_ERR_INVALID_ARG;
   if (n == 0) return AR_OK;
+  parent = parents_or_derive(ctx, n, left, right, parent, arh::stream(stream));
+  if (!parent && n >= 2) return AR_ERR_OOM;
   collide_bvh_kernel<<<arh::grid_for(n, 128), 128, 0, arh::stream(stream)>>>(
       *params, rb_idx, (const float4*)rel4, (const float4*)vel4, is_leaf, left, right, parent,
       (const float4*)cms4, (const float4*)bounds8, sorted_idx, radii, n, (float4*)p_force4,
@@ -382,11 +408,13 @@ ar_status ar_find_contacts_bvh(ar_ctx* ctx, const int32_t* rb_idx, const uint8_t
                                float* contact_distance, int32_t* colliding_particle,
                                int32_t* colliding_body, ar_stream_t stream) {
   if (!ctx || n < 0 ||
-      (n > 0 && (!rb_idx || !is_leaf || !left || !right || !parent || !max_r || !cms4 ||
+      (n > 0 && (!rb_idx || !is_leaf || !left || !right || !max_r || !cms4 ||
                  !bounds8 || !sorted_idx || !radii || !contact_distance ||
                  !colliding_particle || !colliding_body)))
     return AR_ERR_INVALID_ARG;
   if (n < 2) return AR_OK;
+  parent = parents_or_derive(ctx, n, left, right, parent, arh::stream(stream));
+  if (!parent) return AR_ERR_OOM;
   find_contacts_kernel<<<arh::grid_for(n, 128), 128, 0, arh::stream(stream)>>>(
       rb_idx, is_leaf, left, right, parent, max_r, (const float4*)cms4, (const float4*)bounds8,
       sorted_idx, radii, n, contact_distance, colliding_particle, colliding_body);
@@ -398,12 +426,14 @@ ar_status ar_pairs_bvh(ar_ctx* ctx, float radius, const int32_t* rb_idx, const u
                        const float* cms4, const float* bounds8, const int32_t* sorted_idx, int n,
                        int32_t* pairs2, int capacity, int32_t* d_count, ar_stream_t stream) {
   if (!ctx || n < 0 || capacity < 0 || !d_count ||
-      (n > 0 && (!rb_idx || !is_leaf || !left || !right || !parent || !cms4 || !bounds8 ||
+      (n > 0 && (!rb_idx || !is_leaf || !left || !right || !cms4 || !bounds8 ||
                  !sorted_idx || (capacity > 0 && !pairs2))))
     return AR_ERR_INVALID_ARG;
   cudaStream_t st = arh::stream(stream);
   cudaMemsetAsync(d_count, 0, sizeof(int32_t), st);
   if (n < 2) return arh::check_launch("ar_pairs_bvh");
+  parent = parents_or_derive(ctx, n, left, right, parent, st);
+  if (!parent) return AR_ERR_OOM;
   pairs_bvh_kernel<<<arh::grid_for(n, 128), 128, 0, st>>>(
       2.0f * radius, rb_idx, is_leaf, left, right, parent, (const float4*)cms4,
       (const float4*)bounds8, sorted_idx, n, (int2*)pairs2, capacity, d_count, ctx->d_err);

@@ -166,7 +166,9 @@ AR_API ar_status ar_lbvh_refit(ar_ctx* ctx, int n, const int32_t* left, const in
  * (:24-98): per sorted leaf, DEM force against every overlapping leaf of another body;
  * p_force4 / p_torque4 / p_positions4 are written at the particle's original index
  * (sorted_idx[leaf]); vel4 is the unsorted particle velocity.  Traversal is stackless
- * (parent links), so no per-thread stack limits the tree depth. */
+ * (parent links), so no per-thread stack limits the tree depth; `parent` may be NULL (the
+ * reference's wrapper signature has none), in which case the links are derived from
+ * left/right first.  Contacts are visited in the reference's order. */
 AR_API ar_status ar_collide_bvh_dem(ar_ctx* ctx, const ar_sim_params* params,
                                     const int32_t* rb_idx, const float* rel4,
                                     const float* vel4, const uint8_t* is_leaf,
@@ -236,6 +238,20 @@ AR_API ar_status ar_collide_grid_dem(ar_ctx* ctx, const ar_sim_params* params,
                                      const uint32_t* cell_end, int n, float* p_force4,
                                      float* p_torque4, ar_stream_t stream);
 
+/* collideD / collideCell / collideSpheres (Kernels/particleKernels.cu:261-406), the particle
+ * variant reached through collide() (Kernels/particleKernelWrappers.cu:256-305): same force
+ * law, torque accumulated per cell (rel x cell force), results written (not accumulated) to
+ * p_force4 / p_torque4 at the original index; particles with rb_idx -1 instead get
+ * new_vel4[orig] = v + F (new_vel4 may be NULL when there are none). */
+AR_API ar_status ar_collide_grid_particles(ar_ctx* ctx, const ar_sim_params* params,
+                                           const int32_t* rb_idx, const float* sorted_pos4,
+                                           const float* sorted_vel4, const float* rel4,
+                                           const uint32_t* grid_idx,
+                                           const uint32_t* cell_start,
+                                           const uint32_t* cell_end, int n, float* p_force4,
+                                           float* p_torque4, float* new_vel4,
+                                           ar_stream_t stream);
+
 /* ---- (a16/a17) per-body reduction --------------------------------------------------------------
  * Replaces ReducePerParticleImpulses + CombineReducedImpulses (RigidBodies/UniformGridDEM.cu:
  * 421-666) and ReduceRigidBodyVariables (Kernels/rigidBodyKernels.cu:861-1043): a fixed-order
@@ -255,6 +271,17 @@ AR_API ar_status ar_reduce_impulses(ar_ctx* ctx, const float* p_force4, const fl
                                     float* rb_ang4, const float* rb_mass,
                                     const float* rb_inv_inertia9, ar_stream_t stream);
 
+/* ReduceRigidBodyVariables (Kernels/rigidBodyKernels.cu:861-1043): for each rigid object b,
+ * rb_force4[b] += sum and rb_torque4[b] += sum of p_force4 / p_torque4 over
+ * [starts[b], starts[b] + counts[b]) (fixed order as above); a non-finite sum raises
+ * AR_ERR_NAN through ar_ctx_status (the reference sets *toExit).  One launch for all bodies
+ * instead of the reference's per-body host loop. */
+AR_API ar_status ar_reduce_rigid_body_variables(ar_ctx* ctx, const float* p_force4,
+                                                const float* p_torque4, const int32_t* starts,
+                                                const int32_t* counts, int num_bodies,
+                                                float* rb_force4, float* rb_torque4,
+                                                ar_stream_t stream);
+
 /* ---- (a2) body integration, reference semantics --------------------------------------------------
  * GPUintegratorKernel (Kernels/rigidBodyKernels.cu:262-348): x += v dt; q = axis-angle
  * rotation of omega*dt (identity below 1e-5 rad); current inverse inertia R I^-1 R^T;
@@ -267,13 +294,42 @@ AR_API ar_status ar_integrate_reference(ar_ctx* ctx, const ar_sim_params* params
                                         float* cum_quat4, const float* mass,
                                         ar_stream_t stream);
 
+/* ---- (a3) body integration, momentum form --------------------------------------------------------
+ * integrateRigidBody / integrateSystemRigidBodies (Kernels/rigidBodyKernels.cu:40-210):
+ * L += (F + g) dt with the box clamp (box widened by 0.1, 1.0 below in z) and boundary damping,
+ * v = L * mass (the reference's rbMass holds 1/m on this path), x += v dt; angular momentum
+ * += tau dt, w = R I^-1 R^T L, q += dt/2 (w,0) q normalised, w -= (R I^-1 R^T (L x w)) dt.
+ * Force and torque are reset to zero.  ang_acc3 (glm::vec3 per body) may be NULL. */
+AR_API ar_status ar_integrate_momentum(ar_ctx* ctx, const ar_sim_params* params, float dt,
+                                       int num_bodies, float* cms4, float* vel4, float* force4,
+                                       float* ang4, float* quat4, float* torque4,
+                                       float* ang_mom4, float* lin_mom4,
+                                       const float* inv_inertia9, float* cur_inv_inertia9,
+                                       float* ang_acc3, const float* radii, const float* mass,
+                                       const float h_min_pos3[3], const float h_max_pos3[3],
+                                       ar_stream_t stream);
+
 /* ---- (a4) particle re-posing, reference semantics -------------------------------------------------
- * computeGlobalAttributes + resetQuaternionKernel (Kernels/rigidBodyKernels.cu:386-456):
- * rel4 <- R(q) rel4 (in place), pos4 = rel + cm, vel4 = v + omega x rel; then q <- identity. */
+ * computeGlobalAttributes (Kernels/rigidBodyKernels.cu:386-421): rel4 <- R(q) rel4 (in place),
+ * pos4 = rel + cm, vel4 = v + omega x rel (particles with rb_idx -1 are skipped). */
 AR_API ar_status ar_global_attributes(ar_ctx* ctx, int n, int num_bodies, const float* cms4,
                                       const float* rb_vel4, const float* rb_ang4, float* quat4,
                                       const int32_t* rb_idx, float* rel4, float* pos4,
                                       float* vel4, ar_stream_t stream);
+/* resetQuaternionKernel (Kernels/rigidBodyKernels.cu:449-456): q <- identity. */
+AR_API ar_status ar_reset_quaternions(ar_ctx* ctx, float* quat4, int num_bodies,
+                                      ar_stream_t stream);
+
+/* ---- (a5) free particles ----------------------------------------------------------------------------
+ * integrate_functor / integrateSystem (Kernels/particleKernels.cu:50-148): for particles with
+ * rb_idx == -1: v += g dt, v *= global_damping, x += v dt, clamped to the box widened by 0.01
+ * with boundary_damping.  Particles of rigid bodies are untouched. */
+AR_API ar_status ar_integrate_particles(ar_ctx* ctx, const ar_sim_params* params, float dt,
+                                        float* pos4, float* vel4, const int32_t* rb_idx, int n,
+                                        const float h_min_pos3[3], const float h_max_pos3[3],
+                                        ar_stream_t stream);
+/* initializeRadii (Kernels/particleKernels.cu:694-708) and similar fills: dst[0..n) = value. */
+AR_API ar_status ar_fill_f32(ar_ctx* ctx, float* dst, long n, float value, ar_stream_t stream);
 
 /* ---- (a18) wall collisions, reference semantics ---------------------------------------------------
  * WallCollisionWrapper (WallCollisions.cu:338-597): per particle the deepest of the six box

@@ -313,3 +313,49 @@ def step_f64(scene, steps: int = 1, state: dict | None = None, cell: float | Non
                         _p(_i32(scene.body_offsets)), _p(rel), steps, _p(pf), _p(bf), _p(bt))
     st.update({"pforce": pf, "bforce": bf, "btorque": bt, "finite": bool(ok)})
     return st
+
+
+# ---- remaining reference stages ------------------------------------------------------------------
+_L.or_integrate_momentum.restype = None
+_L.or_integrate_particles.restype = None
+_L.or_collide_grid_particles.restype = None
+_L.or_reduce_rbvars.restype = C.c_int
+
+
+def integrate_momentum(state: dict, dt, radii, mass, mn3, mx3, gravity, bdamp, gdamp) -> dict:
+    """integrateRigidBody.  state keys: cms vel force ang quat torque angmom linmom ib cur acc."""
+    s = {k: _f32(v).copy() for k, v in state.items()}
+    nb = len(s["cms"])
+    _L.or_integrate_momentum(*[_p(s[k]) for k in ("cms", "vel", "force", "ang", "quat", "torque",
+                                                 "angmom", "linmom", "ib", "cur", "acc")],
+                             C.c_float(dt), _p(_f32(radii)), _p(_f32(mass)), _p(_f32(mn3)),
+                             _p(_f32(mx3)), _p(_f32(gravity)), C.c_float(bdamp), C.c_float(gdamp), nb)
+    return s
+
+
+def integrate_particles(pos4, vel4, rb_idx, dt, mn3, mx3, gravity, gdamp, bdamp, r):
+    p, v = _f32(pos4).copy(), _f32(vel4).copy()
+    _L.or_integrate_particles(_p(p), _p(v), _p(_i32(rb_idx)), len(p), C.c_float(dt), _p(_f32(mn3)),
+                              _p(_f32(mx3)), _p(_f32(gravity)), C.c_float(gdamp), C.c_float(bdamp),
+                              C.c_float(r))
+    return p, v
+
+
+def collide_grid_particles(origin, cell, dims, prm5, rb_idx, spos4, svel4, rel4, gidx, cstart,
+                           cend, vel_out=None):
+    n = len(spos4)
+    g6 = _f32(list(origin) + list(np.broadcast_to(cell, 3)))
+    pf = np.zeros((n, 4), np.float32)
+    pt = np.zeros((n, 4), np.float32)
+    nv = np.zeros((n, 4), np.float32) if vel_out is None else _f32(vel_out).copy()
+    args = [g6, _u32(dims), _f32(prm5), _i32(rb_idx), _f32(spos4), _f32(svel4), _f32(rel4),
+            _u32(gidx), _u32(cstart), _u32(cend)]
+    _L.or_collide_grid_particles(*[_p(a) for a in args], C.c_long(n), _p(pf), _p(pt), _p(nv))
+    return pf, pt, nv
+
+
+def reduce_rigid_body_variables(pf4, pt4, starts, counts, bf4, bt4):
+    bf, bt = _f32(bf4).copy(), _f32(bt4).copy()
+    ok = _L.or_reduce_rbvars(_p(_f32(pf4)), _p(_f32(pt4)), _p(_i32(starts)), _p(_i32(counts)),
+                             len(starts), _p(bf), _p(bt))
+    return bf, bt, bool(ok)

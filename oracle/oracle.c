@@ -1042,3 +1042,156 @@ int or_step_f64(const double* s15, const double* cell3, int nb, int n, double* b
   free(pp); free(pv); free(pf); free(ck); free(order); free(kk);
   return ok;
 }
+
+/* ====================================================================================
+ * (a3) integrateRigidBody (Kernels/rigidBodyKernels.cu:40-166), momentum form.
+ * ==================================================================================== */
+void or_integrate_momentum(float* cms4, float* vel4, float* force4, float* ang4, float* quat4,
+                           float* torque4, float* angmom4, float* linmom4, const float* ib9,
+                           float* cur9, float* acc3, float dt, const float* radii,
+                           const float* mass, const float* mn3, const float* mx3,
+                           const float* gravity3, float bdamp, float gdamp, int nb) {
+  for (int b = 0; b < nb; ++b) {
+    float* L = linmom4 + 4l * b;
+    const float* F = force4 + 4l * b;
+    float l[4] = {L[0] + F[0] * dt, L[1] + F[1] * dt, L[2] + F[2] * dt, L[3] + F[3] * dt};
+    l[0] = l[0] + gravity3[0] * dt; l[1] = l[1] + gravity3[1] * dt;
+    l[2] = l[2] + gravity3[2] * dt; l[3] = l[3] + 0.f * dt;
+    float mx[3] = {(float)((double)mx3[0] + 0.1), (float)((double)mx3[1] + 0.1), (float)((double)mx3[2] + 0.1)};
+    float mn[3] = {(float)((double)mn3[0] - 0.1), (float)((double)mn3[1] - 0.1), mn3[2] - 1};
+    float* P = cms4 + 4l * b;
+    float p[4] = {P[0], P[1], P[2], P[3]};
+    float m = mass[b], r = radii[b];
+    if (p[0] > mx[0] - r) { p[0] = mx[0] - r; l[0] *= bdamp; }
+    if (p[0] < mn[0] + r) { p[0] = mn[0] + r; l[0] *= bdamp; }
+    if (p[1] > mx[1] - r && l[1] > 0) { p[1] = mx[1] - 2 * r; l[1] *= bdamp; }
+    if (p[1] < mn[1] + r) { p[1] = mn[1] + r; l[1] *= bdamp; }
+    if (p[2] > mx[2] - r) { p[2] = mx[2] - r; l[2] *= bdamp; }
+    if (p[2] < mn[2] + r) { p[2] = mn[2] + r; l[2] *= bdamp; }
+    for (int c = 0; c < 4; ++c) l[c] = l[c] * gdamp;
+    float v[4] = {l[0] * m, l[1] * m, l[2] * m, l[3] * m};
+    memcpy(L, l, 16);
+    for (int c = 0; c < 4; ++c) p[c] = p[c] + v[c] * dt;
+    p[3] = 0.f; v[3] = 0.f;
+    memcpy(P, p, 16);
+    memcpy(vel4 + 4l * b, v, 16);
+    memset(force4 + 4l * b, 0, 16);
+    v4 q = ld4(quat4 + 4l * b);
+    float R[9], RI[9], Rt[9], C[9];
+    glm_mat3_cast(q, R);
+    glm_mm(R, ib9 + 9l * b, RI);
+    for (int c = 0; c < 3; ++c) for (int rr = 0; rr < 3; ++rr) Rt[c * 3 + rr] = R[rr * 3 + c];
+    glm_mm(RI, Rt, C);
+    float* A = angmom4 + 4l * b;
+    const float* T = torque4 + 4l * b;
+    float am[4] = {A[0] + T[0] * dt, A[1] + T[1] * dt, A[2] + T[2] * dt, A[3] + T[3] * dt};
+    v3 cm3 = mk3(am[0], am[1], am[2]);
+    v3 nv = glm_mv(C, cm3);
+    v3 acc = glm_mv(C, glm_cross(cm3, nv));
+    v4 wq = {nv.x, nv.y, nv.z, 0.f};
+    v4 qd = glm_qmul(wq, q);
+    qd.x = qd.x / 2.f; qd.y = qd.y / 2.f; qd.z = qd.z / 2.f; qd.w = qd.w / 2.f;
+    q.x = q.x + qd.x * dt; q.y = q.y + qd.y * dt; q.z = q.z + qd.z * dt; q.w = q.w + qd.w * dt;
+    q = glm_qnormalize(q);
+    nv = mk3(nv.x - acc.x * dt, nv.y - acc.y * dt, nv.z - acc.z * dt);
+    if (acc3) { acc3[3 * b] = acc.x; acc3[3 * b + 1] = acc.y; acc3[3 * b + 2] = acc.z; }
+    memcpy(cur9 + 9l * b, C, 36);
+    memcpy(A, am, 16);
+    st4(quat4 + 4l * b, q.x, q.y, q.z, q.w);
+    st4(ang4 + 4l * b, nv.x, nv.y, nv.z, 0.f);
+    memset(torque4 + 4l * b, 0, 16);
+  }
+}
+
+/* (a5) integrate_functor (Kernels/particleKernels.cu:50-128), free particles only. */
+void or_integrate_particles(float* pos4, float* vel4, const int* rb_idx, int n, float dt,
+                            const float* mn3, const float* mx3, const float* gravity3,
+                            float gdamp, float bdamp, float r) {
+  float mx[3] = {(float)((double)mx3[0] + 0.01), (float)((double)mx3[1] + 0.01), (float)((double)mx3[2] + 0.01)};
+  float mn[3] = {(float)((double)mn3[0] - 0.01), (float)((double)mn3[1] - 0.01), (float)((double)mn3[2] - 0.01)};
+  for (int i = 0; i < n; ++i) {
+    if (rb_idx[i] >= 0) continue;
+    float* P = pos4 + 4l * i;
+    float* V = vel4 + 4l * i;
+    v3 p = xyz(P), v = xyz(V);
+    v = add(v, mk3(gravity3[0] * dt, gravity3[1] * dt, gravity3[2] * dt));
+    v = mk3(v.x * gdamp, v.y * gdamp, v.z * gdamp);
+    p = add(p, mk3(v.x * dt, v.y * dt, v.z * dt));
+    if (p.x > mx[0] - r) { p.x = mx[0] - r; v.x *= bdamp; }
+    if (p.x < mn[0] + r) { p.x = mn[0] + r; v.x *= bdamp; }
+    if (p.y > mx[1] - r && v.y > 0) { p.y = mx[1] - r; v.y *= bdamp; }
+    if (p.z > mx[2] - r) { p.z = mx[2] - r; v.z *= bdamp; }
+    if (p.z < mn[2] + r) { p.z = mn[2] + r; v.z *= bdamp; }
+    if (p.y < mn[1] + r) { p.y = mn[1] + r; v.y *= bdamp; }
+    P[0] = p.x; P[1] = p.y; P[2] = p.z;
+    V[0] = v.x; V[1] = v.y; V[2] = v.z;
+  }
+}
+
+/* collideD / collideCell / collideSpheres (Kernels/particleKernels.cu:261-406). */
+void or_collide_grid_particles(const float* grid6, const uint32_t* dims3, const float* prm5,
+                               const int* rb_idx, const float* spos4, const float* svel4,
+                               const float* rel4, const uint32_t* gidx, const uint32_t* cstart,
+                               const uint32_t* cend, long n, float* p_force4, float* p_torque4,
+                               float* new_vel4) {
+  grid_t G;
+  memcpy(G.o, grid6, 12); memcpy(G.c, grid6 + 3, 12); memcpy(G.g, dims3, 12);
+  const float cd = prm5[4] + prm5[4];
+#pragma omp parallel for schedule(static)
+  for (long index = 0; index < n; ++index) {
+    v3 pos = xyz(spos4 + 4 * index), vel = xyz(svel4 + 4 * index);
+    int gp[3];
+    cell_of(&G, pos, gp);
+    uint32_t orig = gidx[index];
+    int body = rb_idx[orig];
+    v3 r3 = xyz(rel4 + 4l * orig);
+    v3 force = mk3(0.f, 0.f, 0.f), torque = mk3(0.f, 0.f, 0.f);
+    for (int z = -1; z <= 1; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int x = -1; x <= 1; ++x) {
+          v3 cf = mk3(0.f, 0.f, 0.f);
+          uint32_t h = hash3(&G, gp[0] + x, gp[1] + y, gp[2] + z);
+          uint32_t s = cstart[h];
+          if (s != EMPTY) {
+            uint32_t e = cend[h];
+            for (uint32_t j = s; j < e; ++j) {
+              if (!(j != (uint32_t)index && (body != rb_idx[gidx[j]] || body == -1))) continue;
+              v3 rp = sub(xyz(spos4 + 4l * j), pos);
+              float dist = sqrtf(dot(rp, rp));
+              v3 f = mk3(0.f, 0.f, 0.f);
+              if (dist < cd) f = spring_force(rp, dist, sub(xyz(svel4 + 4l * j), vel), cd, prm5);
+              cf = add(cf, f);
+            }
+          }
+          force = add(force, cf);
+          torque = add(torque, cross(r3, cf));
+        }
+    if (body == -1) {
+      if (new_vel4) st4(new_vel4 + 4l * orig, vel.x + force.x, vel.y + force.y, vel.z + force.z, 0.f);
+    } else {
+      st4(p_force4 + 4l * orig, force.x, force.y, force.z, 0.f);
+      st4(p_torque4 + 4l * orig, torque.x, torque.y, torque.z, 0.f);
+    }
+  }
+}
+
+/* (a17) ReduceRigidBodyVariables (Kernels/rigidBodyKernels.cu:861-1043): += fixed-order sums;
+ * returns 0 when a sum is not finite (the reference's *toExit). */
+int or_reduce_rbvars(const float* pf4, const float* pt4, const int* starts, const int* counts,
+                     int nb, float* bf4, float* bt4) {
+  int ok = 1;
+  for (int b = 0; b < nb; ++b) {
+    int s = starts[b], c = counts[b];
+    v3* f = (v3*)malloc(sizeof(v3) * (c + 1));
+    v3* t = (v3*)malloc(sizeof(v3) * (c + 1));
+    for (int i = 0; i < c; ++i) { f[i] = xyz(pf4 + 4l * (s + i)); t[i] = xyz(pt4 + 4l * (s + i)); }
+    v3 F = warp_sum(f, c), T = warp_sum(t, c);
+    free(f); free(t);
+    if (!isfinite(F.x + F.y + F.z) || !isfinite(T.x + T.y + T.z)) ok = 0;
+    float* o = bf4 + 4l * b;
+    o[0] = o[0] + F.x; o[1] = o[1] + F.y; o[2] = o[2] + F.z;
+    o = bt4 + 4l * b;
+    o[0] = o[0] + T.x; o[1] = o[1] + T.y; o[2] = o[2] + T.z;
+  }
+  return ok;
+}

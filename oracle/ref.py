@@ -196,3 +196,32 @@ def wall_collisions(ppos4, rbpos4, mn3, mx3, rbvel4, rbang4, ib9, mass, rb_idx, 
                                  _p(_i32(rb_idx)), _p(_i32(counts)), len(counts), len(ppos4),
                                  C.c_float(radius))
     return v, a
+
+
+def integrate_momentum(params, state, dt, radii, mass, mn3, mx3):
+    s = {k: _f32(v).copy() for k, v in state.items()}
+    nb = len(s["cms"])
+    lib().refcpu_integrate_momentum(*[_p(s[k]) for k in ("cms", "vel", "force", "ang", "quat",
+                                                        "torque", "angmom", "linmom", "ib", "cur",
+                                                        "acc")],
+                                    C.c_float(dt), _p(_f32(radii)), _p(_f32(mass)),
+                                    _p(_f32(mn3)), _p(_f32(mx3)), nb, C.byref(params))
+    return s
+
+
+def integrate_particles(params, pos4, vel4, rb_idx, dt, mn3, mx3):
+    p, v = _f32(pos4).copy(), _f32(vel4).copy()
+    lib().refcpu_integrate_particles(C.byref(params), _p(p), _p(v), _p(_i32(rb_idx).copy()), len(p),
+                                     C.c_float(dt), _p(_f32(mn3)), _p(_f32(mx3)))
+    return p, v
+
+
+def collide_particles(params, rb_idx, rel4, spos4, svel4, gidx, cstart, cend, vel_out=None):
+    n = len(spos4)
+    pf = np.zeros((n, 4), np.float32)
+    pt = np.zeros((n, 4), np.float32)
+    nv = np.zeros((n, 4), np.float32) if vel_out is None else _f32(vel_out).copy()
+    lib().refcpu_collide_particles(C.byref(params), _p(pf), _p(_i32(rb_idx)), _p(_f32(rel4)),
+                                   _p(pt), _p(nv), _p(_f32(spos4)), _p(_f32(svel4)),
+                                   _p(_u32(gidx)), _p(_u32(cstart)), _p(_u32(cend)), n)
+    return pf, pt, nv

@@ -37,7 +37,9 @@ OUT = HERE / "_ref"
 # (file relative to AR_Sim/, first line, last line, text the first line must contain)
 RANGES = [
     ("BVHSource/BVHkernels.cu", 646, 716, "Expands a 10-bit integer"),          # expandBits, morton3D, generateMortonCodes x2
+    ("Kernels/particleKernels.cu", 50, 128, "struct integrate_functor"),       # free-particle integrate
     ("Kernels/particleKernels.cu", 150, 189, "calculate position in uniform grid"),  # calcGridPos, calcGridHash, calcHashD
+    ("Kernels/particleKernels.cu", 260, 406, "collide two spheres using DEM"),   # collideSpheres, collideCell, collideD
     ("RigidBodies/UniformGridDEM.cu", 24, 204, "calculate position in uniform grid"),  # DEM grid collide cell + kernel
     ("RigidBodies/UniformGridDEM.cu", 420, 460, "Now apply total impulse"),      # CombineReducedImpulses
     ("Kernels/rigidBodyKernels.cu", 37, 166, "/*"),                              # integrateRigidBody

@@ -31,6 +31,8 @@ thread_local dim3 gridDim;
 #include <glm/glm.hpp>
 #include <glm/gtc/quaternion.hpp>
 
+#include <thrust/tuple.h>
+
 // Kernels/particleKernels.cu:42 keeps the parameters in __constant__ memory.
 SimParams params;
 
@@ -294,6 +296,54 @@ void refcpu_find_rb_collisions_bvh(const void* sim_params, const int* rb_idx,
                                      (int*)right, (int*)min_r, (int*)max_r, (float4*)cms4,
                                      (AABB*)bounds, (int*)sorted_idx, (float*)radii, n, p,
                                      contact_distance, colliding_particle, colliding_body);
+  });
+}
+
+// ---- integrateRigidBody (Kernels/rigidBodyKernels.cu:40-166) ------------------------------
+void refcpu_integrate_momentum(float* cms4, float* vel4, float* force4, float* ang4,
+                               float* quat4, float* torque4, float* ang_mom4, float* lin_mom4,
+                               const float* inv_inertia9, float* cur9, float* acc3, float dt,
+                               const float* radii, const float* mass, const float* mn3,
+                               const float* mx3, int nb, const void* sim_params) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  float3 mn = make_float3(mn3[0], mn3[1], mn3[2]), mx = make_float3(mx3[0], mx3[1], mx3[2]);
+  launch(nb, 128, true, [&] {
+    integrateRigidBody((float4*)cms4, (float4*)vel4, (float4*)force4, (float4*)ang4,
+                       (glm::quat*)quat4, (float4*)torque4, (float4*)ang_mom4,
+                       (float4*)lin_mom4, (glm::mat3*)inv_inertia9, (glm::mat3*)cur9,
+                       (glm::vec3*)acc3, dt, (float*)radii, (float*)mass, mn, mx, nb, p);
+  });
+}
+
+// ---- integrate_functor through integrateSystem (Kernels/particleKernels.cu:50-148) -------
+void refcpu_integrate_particles(const void* sim_params, float* pos4, float* vel4,
+                                int* rb_idx, int n, float dt, const float* mn3,
+                                const float* mx3) {
+  std::memcpy(&params, sim_params, sizeof(SimParams));
+  const integrate_functor f(dt, make_float3(mn3[0], mn3[1], mn3[2]),
+                            make_float3(mx3[0], mx3[1], mx3[2]));
+  for (int i = 0; i < n; ++i) {
+    // operator() widens the functor's own box members (particleKernels.cu:78-84); each device
+    // thread applies it to its own copy, so each particle gets a fresh copy here too
+    integrate_functor g = f;
+    thrust::tuple<float4&, float4&, int&> t(((float4*)pos4)[i], ((float4*)vel4)[i], rb_idx[i]);
+    g(t);
+  }
+}
+
+// ---- collideD (Kernels/particleKernels.cu:344-406) ------------------------------------------
+void refcpu_collide_particles(const void* sim_params, float* p_force4, const int* rb_idx,
+                              const float* rel4, float* p_torque4, float* new_vel4,
+                              const float* sorted_pos4, const float* sorted_vel4,
+                              const uint32_t* grid_idx, const uint32_t* cell_start,
+                              const uint32_t* cell_end, int n) {
+  std::memcpy(&params, sim_params, sizeof(SimParams));
+  std::vector<float4> color(n);
+  launch(n, 128, true, [&] {
+    collideD((float4*)p_force4, (int*)rb_idx, (float4*)rel4, (float4*)p_torque4, color.data(),
+             (float4*)new_vel4, (float4*)sorted_pos4, (float4*)sorted_vel4, (uint*)grid_idx,
+             (uint*)cell_start, (uint*)cell_end, (uint)n);
   });
 }
 

@@ -139,6 +139,53 @@ def body_case(seed: int):
                 radius=np.float32(sc.radius), wall_vel_out=wvel, wall_ang_out=wang)
 
 
+def extra_case(seed: int):
+    """integrateRigidBody, integrate_functor and collideD on seeded inputs."""
+    rng = np.random.default_rng(seed)
+    sc = scenes.small_scene(seed, nb_side=3, v_sigma=1.0)
+    nb = sc.num_bodies
+    st = {"cms": sc.body_pos.copy(), "vel": np.zeros((nb, 4), np.float32),
+          "force": rng.normal(0, 2, (nb, 4)).astype(np.float32),
+          "ang": np.zeros((nb, 4), np.float32), "quat": sc.body_quat.copy(),
+          "torque": rng.normal(0, 0.5, (nb, 4)).astype(np.float32),
+          "angmom": rng.normal(0, 0.05, (nb, 4)).astype(np.float32),
+          "linmom": rng.normal(0, 3, (nb, 4)).astype(np.float32),
+          "ib": sc.body_inv_inertia.copy(), "cur": np.zeros((nb, 9), np.float32),
+          "acc": np.zeros((nb, 3), np.float32)}
+    st["cms"][:3, 0] = [-0.2, 1.3, 0.5]  # exercise the box clamps
+    st["cms"][3:5, 2] = [-1.5, 1.2]
+    radii = np.full(nb, 0.05, np.float32)
+    inv_mass = (1.0 / sc.body_mass).astype(np.float32)
+    prm = params_for(sc.radius, (0, 0, 0), 1.0, (1, 1, 1), 0.5, 0.0, 0.0, gravity=(0, -0.5, 0))
+    prm.boundary_damping = -0.5
+    prm.global_damping = 0.999
+    mom = ref.integrate_momentum(prm, st, 0.02, radii, inv_mass, [0, 0, 0], [1, 1, 1])
+    # free particles (rb_idx -1) mixed with rigid ones
+    n = 500
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform(-0.05, 1.05, (n, 3))
+    pos[:, 3] = 1.0
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0, 1, (n, 3))
+    rbi = np.where(rng.random(n) < 0.5, -1, 0).astype(np.int32)
+    pp, pv = ref.integrate_particles(prm, pos, vel, rbi, 0.01, [0, 0, 0], [1, 1, 1])
+    # collideD on the dem_small inputs (dem_case(5)) with a few free particles
+    d = dem_case(5)
+    rb = d["rb"].copy()
+    rb[::17] = -1
+    prm2 = params_for(float(d["radius"]), (0, 0, 0), float(d["cell"]), tuple(d["dims"]), 0.5,
+                      0.02, 0.1, 0.001)
+    nv0 = np.zeros_like(d["pos"])
+    cpf, cpt, cnv = ref.collide_particles(prm2, rb, d["rel"], d["spos"], d["svel"], d["sidx"],
+                                          d["cell_start"], d["cell_end"], nv0)
+    out = {f"mom_in_{k}": v for k, v in st.items()}
+    out.update({f"mom_out_{k}": v for k, v in mom.items()})
+    out.update(dict(mom_radii=radii, mom_inv_mass=inv_mass, mom_dt=np.float32(0.02),
+                    fp_pos=pos, fp_vel=vel, fp_rb=rbi, fp_pos_out=pp, fp_vel_out=pv,
+                    cd_rb=rb, cd_pforce=cpf, cd_ptorque=cpt, cd_newvel=cnv))
+    return out
+
+
 def main() -> None:
     if not ref.available():
         raise SystemExit("oracle/_ref/libref_cpu.so is not built (run oracle/ref_build.py)")
@@ -147,6 +194,7 @@ def main() -> None:
     np.savez_compressed(OUT / "lbvh_duplicates.npz", **lbvh_case(12, 3000, 0.2))
     np.savez_compressed(OUT / "dem_small.npz", **dem_case(5))
     np.savez_compressed(OUT / "bodies_small.npz", **body_case(9))
+    np.savez_compressed(OUT / "reference_extra.npz", **extra_case(21))
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

@@ -92,7 +92,8 @@ def test_sort_u32_all_equal_and_begin_bit(ctx):
 def test_sort_u64(ctx, n, begin, end):
     rng = np.random.default_rng(n)
     keys = rng.integers(0, 1 << 63, n, dtype=np.uint64)
-    keys[::5] = keys[1::5][: len(keys[::5])]
+    m = len(keys[1::5])
+    keys[::5][:m] = keys[1::5]  # ties
     kin = dev(keys)
     kout, vout = empty(n, torch.int64), empty(n, torch.int32)
     call("ar_radix_sort_pairs_u64", ctx.handle, P(kin), None, P(kout), P(vout), n, begin, end, S())
@@ -328,6 +329,8 @@ def test_reference_integrator_and_reposing_golden(ctx):
     rel, pos, pvel = dev(g["in_rel"]), empty((n, 4)), empty((n, 4))
     call("ar_global_attributes", ctx.handle, n, nb, P(dev(g["out_cms"])), P(dev(g["out_vel"])),
          P(dev(g["out_ang"])), P(q), P(dev(g["rb"])), P(rel), P(pos), P(pvel), S())
+    assert np.array_equal(host(q), g["out_quat"])  # untouched until the reset
+    call("ar_reset_quaternions", ctx.handle, P(q), nb, S())
     assert np.array_equal(host(rel), g["out_rel"]) and np.array_equal(host(pos), g["out_pos"])
     assert np.array_equal(host(pvel), g["out_pvel"]) and np.array_equal(host(q), g["out_q_reset"])
 
