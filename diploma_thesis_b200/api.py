@@ -22,11 +22,19 @@ def stream_handle(stream: torch.cuda.Stream | None = None) -> C.c_void_p:
     return C.c_void_p(s.cuda_stream)
 
 
+class DevicePtr(C.c_void_p):
+    """A c_void_p that keeps its tensor alive for as long as the pointer object lives (so an
+    argument like ptr(torch.tensor(...)) is not freed, and its memory handed to the next
+    allocation, before the call it is passed to)."""
+
+
 def ptr(t: torch.Tensor | None) -> C.c_void_p:
     if t is None:
         return C.c_void_p(None)
     assert t.is_cuda and t.is_contiguous(), "device tensors must be contiguous CUDA tensors"
-    return C.c_void_p(t.data_ptr())
+    p = DevicePtr(t.data_ptr())
+    p.tensor = t
+    return p
 
 
 class Context:
