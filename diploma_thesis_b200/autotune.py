@@ -1,0 +1,124 @@
+"""Autotuner: per scene-size bucket, the grid cell size, the wrapped grid size and the block
+size of the DEM gather that give the fastest fused step on this GPU.
+
+Buckets are powers of two of the particle count.  For each bucket a representative scene
+(27-particle cubes, config-0 distributions) is stepped under every candidate and timed with
+CUDA events over CUDA-graph replays; the fastest candidate is kept.  Results are cached in a
+JSON file keyed by GPU name, so a deployment tunes once.
+
+Candidates: cell = f * 2r for f in CELL_FACTORS; cells per axis wrapped so that the grid
+holds at most next_pow2(m * N) cells for m in GRID_MULTS; block size in BLOCK_SIZES.  Every
+candidate gives the same contacts (the cell is never smaller than the contact distance and the
+wrap only aliases distant cells, which the distance test rejects), so the choice changes speed,
+not results -- except for the summation order of a particle's contacts, which follows the cell
+order.
+"""
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import asdict, dataclass
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import api, scenes
+
+CELL_FACTORS = (1.0, 1.25, 1.5)
+GRID_MULTS = (2, 8, 32)
+BLOCK_SIZES = (64, 128, 256)
+
+
+@dataclass
+class Choice:
+    cell_factor: float
+    grid_mult: int
+    block_size: int
+    ms_per_step: float
+
+
+def bucket_of(num_particles: int) -> int:
+    return max(10, int(math.ceil(math.log2(max(num_particles, 2)))))
+
+
+def grid_for(scene: scenes.Scene, cell: float, mult: int) -> tuple[int, int, int]:
+    """log2 cells per axis: cover the box, then halve the largest axis while the grid holds
+    more than next_pow2(mult * N) cells."""
+    dims = []
+    for a in range(3):
+        ext = float(scene.box_max[a]) - float(scene.box_min[a])
+        cells = max(1, int(math.ceil(ext / cell)))
+        dims.append(max(2, int(math.ceil(math.log2(cells)))))
+    cap = max(12, int(math.ceil(math.log2(mult * max(scene.num_particles, 1)))))
+    while sum(dims) > cap:
+        a = int(np.argmax(dims))
+        if dims[a] <= 2:
+            break
+        dims[a] -= 1
+    return tuple(dims)
+
+
+def apply(scene: scenes.Scene, choice: Choice) -> dict:
+    """Keyword arguments for api.GpuScene that realise a choice for this scene."""
+    cell = float(np.float32(choice.cell_factor * 2 * scene.radius))
+    return {"cell_size": cell, "grid_log2": grid_for(scene, cell, choice.grid_mult),
+            "block_size": choice.block_size}
+
+
+def _time_steps(ctx: api.Context, scene: scenes.Scene, kw: dict, steps: int) -> float:
+    gs = api.GpuScene(ctx, scene, **kw)
+    s = torch.cuda.Stream()
+    with torch.cuda.stream(s):
+        gs.step(3, use_graph=True, stream=s)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(s)
+        gs.step(steps, use_graph=True, stream=s)
+        b.record(s)
+        b.synchronize()
+    gs.close()
+    return a.elapsed_time(b) / steps
+
+
+def tune_bucket(ctx: api.Context, bucket: int, steps: int = 20, seed: int = 0) -> Choice:
+    n = 1 << bucket
+    side = float(np.clip((n / 27 * 0.035 ** 3 * 4) ** (1 / 3), 0.5, 2.0))
+    scene = scenes.cube_scene(seed + bucket, n // 27 * 27, side)
+    best = None
+    for f in CELL_FACTORS:
+        for m in GRID_MULTS:
+            for bs in BLOCK_SIZES:
+                c = Choice(f, m, bs, 0.0)
+                c.ms_per_step = _time_steps(ctx, scene, apply(scene, c), steps)
+                if best is None or c.ms_per_step < best.ms_per_step:
+                    best = c
+    return best
+
+
+class Tuner:
+    def __init__(self, ctx: api.Context, cache: str | Path | None = None):
+        self.ctx = ctx
+        self.cache = Path(cache) if cache else None
+        self.table: dict[int, Choice] = {}
+        self.gpu = torch.cuda.get_device_name()
+        if self.cache and self.cache.exists():
+            data = json.loads(self.cache.read_text())
+            for k, v in data.get(self.gpu, {}).items():
+                self.table[int(k)] = Choice(**v)
+
+    def choice(self, num_particles: int) -> Choice:
+        b = bucket_of(num_particles)
+        if b not in self.table:
+            self.table[b] = tune_bucket(self.ctx, b)
+            self.save()
+        return self.table[b]
+
+    def save(self) -> None:
+        if not self.cache:
+            return
+        data = json.loads(self.cache.read_text()) if self.cache.exists() else {}
+        data[self.gpu] = {str(k): asdict(v) for k, v in sorted(self.table.items())}
+        self.cache.write_text(json.dumps(data, indent=1))
+
+    def scene_kwargs(self, scene: scenes.Scene) -> dict:
+        return apply(scene, self.choice(scene.num_particles))
