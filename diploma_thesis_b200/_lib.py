@@ -89,6 +89,7 @@ SIGNATURES = {
     "ar_morton63": [P, P, I, P, P, P, P, S],
     "ar_radix_sort_pairs_u32": [P, P, P, P, P, I, I, I, S],
     "ar_radix_sort_pairs_u64": [P, P, P, P, P, I, I, I, S],
+    "ar_radix_sort_pairs_u32_noalloc": [P, P, P, P, I, I, I, P, S],
     "ar_lbvh_build": [P, P, I, P, P, P, P, P, P, S],
     "ar_lbvh_build64": [P, P, I, P, P, P, P, P, P, S],
     "ar_lbvh_leaves": [P, I, P, P, F, P, P, P, P, P, P, S],

@@ -14,6 +14,7 @@
 // Spin waits are bounded; on timeout the kernel raises kErrTimeout and finishes the pass
 // with whatever prefix it has (the result is then garbage, but nothing hangs).
 #include <cuda/atomic>
+#include <mutex>
 
 #include "ar_internal.cuh"
 #include "ar_sort.cuh"
@@ -320,6 +321,56 @@ __global__ void iota_kernel(uint32_t* v, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
 }
 
+// ---- allocation-free variant -------------------------------------------------------------------
+// Workspace of the u32 sort for up to kNoAllocMaxN pairs, laid out like ar_sort::layout
+// (histograms, tile counters, look-back status for 4 passes, ping-pong keys and values).
+constexpr int kNoAllocMaxN = 1 << 20;
+constexpr size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t noalloc_bytes() {
+  return up256(up256(up256(up256(up256((size_t)ar_sort::kMaxPasses * kRadix * 4) +
+                                       ar_sort::kMaxPasses * 4) +
+                                 (size_t)4 * (kNoAllocMaxN / kTile) * kRadix * 4) +
+                           (size_t)kNoAllocMaxN * 4) +
+               (size_t)kNoAllocMaxN * 4);
+}
+// One copy per GPU that loads the library, held until the process exits.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[noalloc_bytes()];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kNoAllocMaxDevices] = {};
+int g_noalloc_sms[kNoAllocMaxDevices] = {};
+
+// Per-device set-up, once, with that device current: the device address of the static
+// workspace (host code cannot use the symbol's name as an address) and the shared-memory
+// opt-in of the pass kernel.
+ar_status noalloc_setup(int dev, void** addr, int* sms) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      arh::set_error("allocation-free sort: cudaGetSymbolAddress failed (%s)",
+                     cudaGetErrorString(e));
+      return AR_ERR_CUDA;
+    }
+    e = cudaFuncSetAttribute(onesweep_kernel<uint32_t>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(PassSmem<uint32_t>));
+    if (e != cudaSuccess) {
+      arh::set_error("allocation-free sort: %s", cudaGetErrorString(e));
+      return AR_ERR_CUDA;
+    }
+    int n_sms = 148;
+    cudaDeviceGetAttribute(&n_sms, cudaDevAttrMultiProcessorCount, dev);
+    g_noalloc_sms[dev] = n_sms;
+    g_noalloc_addr[dev] = p;
+  }
+  *addr = g_noalloc_addr[dev];
+  *sms = g_noalloc_sms[dev];
+  return AR_OK;
+}
+
 }  // namespace
 
 namespace ar_sort {
@@ -382,6 +433,81 @@ ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in, const ui
                                   int end_bit, ar_stream_t stream) {
   return sort_entry<uint64_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
                               stream);
+}
+
+// The same sort as ar_radix_sort_pairs_u32, with its workspace in g_noalloc_scratch instead
+// of memory from cudaMalloc.  Shared by every call on a device: calls that overlap on the
+// GPU race; the histogram / look-back head is cleared at the start of each call.
+ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_t* vals_in,
+                                          uint32_t* keys_out, uint32_t* vals_out, int n,
+                                          int begin_bit, int end_bit, int32_t* d_status,
+                                          ar_stream_t stream) {
+  if (n < 0 || begin_bit < 0 || end_bit > 32 || begin_bit > end_bit) return AR_ERR_INVALID_ARG;
+  if (n > kNoAllocMaxN) {
+    arh::set_error("allocation-free sort: n = %d exceeds its limit of %d pairs", n, kNoAllocMaxN);
+    return AR_ERR_INVALID_ARG;
+  }
+  if (n > 0 && (!keys_in || !keys_out || !vals_out)) return AR_ERR_INVALID_ARG;
+  if (n > 0 && ((const void*)keys_in == (const void*)keys_out ||
+                (vals_in && (const void*)vals_in == (const void*)vals_out))) {
+    arh::set_error("allocation-free sort: outputs must not alias inputs");
+    return AR_ERR_INVALID_ARG;
+  }
+  if (n == 0) return AR_OK;
+  cudaStream_t st = arh::stream(stream);
+  if (begin_bit == end_bit) {
+    cudaMemcpyAsync(keys_out, keys_in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+    if (vals_in)
+      cudaMemcpyAsync(vals_out, vals_in, (size_t)n * 4, cudaMemcpyDeviceToDevice, st);
+    else
+      ar_sort::iota(vals_out, n, st);
+    return arh::check_launch("allocation-free sort copy");
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+    arh::set_error("allocation-free sort: no usable current device");
+    return AR_ERR_CUDA;
+  }
+  void* base_v = nullptr;
+  int sms = 148;
+  ar_status s = noalloc_setup(dev, &base_v, &sms);
+  if (s != AR_OK) return s;
+  const int total_bits = end_bit - begin_bit;
+  const int passes = (total_bits + 7) / 8;
+  const int last_bits = total_bits - 8 * (passes - 1);
+  const long tiles = ((long)n + kTile - 1) / kTile;
+  const ar_sort::Layout L = ar_sort::layout(n, 4, passes);
+  if (L.total > sizeof(g_noalloc_scratch)) {  // cannot happen for n <= kNoAllocMaxN
+    arh::set_error("allocation-free sort: workspace layout exceeds the static array");
+    return AR_ERR_INVALID_ARG;
+  }
+  char* base = (char*)base_v;
+  uint32_t* hist = (uint32_t*)(base + L.hist);
+  uint32_t* counters = (uint32_t*)(base + L.counters);
+  uint32_t* status = (uint32_t*)(base + L.status);
+  uint32_t* tmp_keys = (uint32_t*)(base + L.tmp_keys);
+  uint32_t* tmp_vals = (uint32_t*)(base + L.tmp_vals);
+  // the previous call's contents stay in the array: zero what must start at zero
+  cudaMemsetAsync(base, 0, L.status + (size_t)passes * tiles * kRadix * sizeof(uint32_t), st);
+  unsigned hgrid = (unsigned)((n + kThreads * 8 - 1) / (kThreads * 8));
+  if (hgrid > (unsigned)sms * 4) hgrid = (unsigned)sms * 4;
+  if (hgrid < 1) hgrid = 1;
+  hist_kernel<uint32_t><<<hgrid, kThreads, 0, st>>>(keys_in, n, begin_bit, passes, last_bits, hist);
+  hist_scan_kernel<<<1, 32 * ar_sort::kMaxPasses, 0, st>>>(hist, passes);
+  const uint32_t* src_k = keys_in;
+  const uint32_t* src_v = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    const bool to_out = ((passes - 1 - p) % 2) == 0;
+    uint32_t* dk = to_out ? keys_out : tmp_keys;
+    uint32_t* dv = to_out ? vals_out : tmp_vals;
+    const int bits = (p == passes - 1) ? last_bits : 8;
+    onesweep_kernel<uint32_t><<<(unsigned)tiles, kThreads, sizeof(PassSmem<uint32_t>), st>>>(
+        src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
+        status + (size_t)p * tiles * kRadix, counters + p, (int*)d_status);
+    src_k = dk;
+    src_v = dv;
+  }
+  return arh::check_launch("allocation-free sort");
 }
 
 }  // extern "C"

@@ -128,6 +128,24 @@ AR_API ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in,
                                          uint32_t* vals_out, int n, int begin_bit, int end_bit,
                                          ar_stream_t stream);
 
+/* Allocation-free variant of ar_radix_sort_pairs_u32.  No counterpart in the reference.
+ * For callers that cannot allocate device memory: a frame loop that must never stall on
+ * cudaMalloc's implicit device synchronisation, code running while another component owns
+ * the device memory pool, or a process whose device-memory budget is fixed at start-up.
+ * The workspace is a static array inside libarsim.so (about 9 MiB, held by every GPU that
+ * loads the library until the process exits), so n is limited to 1,048,576 pairs; larger n
+ * returns AR_ERR_INVALID_ARG.  No context is needed and nothing is allocated: the caller
+ * passes inputs and outputs, plus an optional device int (d_status, may be NULL) into which
+ * a timed-out look-back ORs 1.  The first call on each device sets up (looks up the array's
+ * device address with that device current); make that first call before any stream capture.
+ * Every call on a device shares the array, so calls that overlap on the GPU race: serialise
+ * them (one stream, or events). */
+AR_API ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in,
+                                                 const uint32_t* vals_in, uint32_t* keys_out,
+                                                 uint32_t* vals_out, int n, int begin_bit,
+                                                 int end_bit, int32_t* d_status,
+                                                 ar_stream_t stream);
+
 /* ---- (a9) Karras LBVH hierarchy --------------------------------------------------------------
  * kernelConstructRadixTreeSoA (BVHSource/BVHSoAKernels.cu:7-99) with longestCommonPrefix
  * (BVHSource/BVHAuxiliary.cuh:31-43): leaves at [0, n), internal node i at n + i, root at n;
