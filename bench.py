@@ -62,6 +62,30 @@ def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int) -> dict[str, 
     }
 
 
+BVH_STAGES = ["clear", "morton", "sort", "tree", "collide", "reduce_integrate"]
+
+
+def stage_bytes_bvh(n: int, nb: int, passes: int) -> dict[str, float]:
+    """The same accounting for the BVH broad phase (64-bit keys, 32-byte node boxes)."""
+    body_state = 16 * 4
+    tiles = (n + 4095) // 4096
+    return {
+        "clear": 4 * n,  # refit arrival counters
+        # read rel (16), write key (8); body pose (32) per body
+        "morton": n * (16 + 8) + nb * 32,
+        # histogram pass reads the keys; first pass reads keys, every pass writes key + index,
+        # later passes read both
+        "sort": n * 8 + n * (8 + 12) + (passes - 1) * n * 24 + passes * 4 * 256 * tiles,
+        # leaves: index, rel in; sorted pos + vel, box, flags, ranges out; nodes: keys in,
+        # flags, children, parent, ranges out; refit: links and child boxes in, box out
+        "tree": n * (4 + 16 + 32 + 32 + 9) + nb * body_state + n * (8 + 21 + 8) +
+                n * (12 + 64 + 32),
+        # own index, position + velocity, box; force out
+        "collide": n * (4 + 32 + 32 + 16),
+        "reduce_integrate": n * 32 + nb * (body_state + 4 + 36 + body_state + 32),
+    }
+
+
 def peaks() -> tuple[float, str]:
     if PEAKS.exists():
         try:
@@ -304,8 +328,10 @@ def run_ours(args):
     from diploma_thesis_b200 import api
 
     scene, desc = make_scene(args.workload)
+    if args.broadphase == "bvh":
+        desc = desc.replace("grid 256^3 wrapped", "BVH").replace("grid 128^3", "BVH")
     ctx = api.Context(local)
-    gs = api.GpuScene(ctx, scene)
+    gs = api.GpuScene(ctx, scene, broadphase=args.broadphase)
     n, nb = scene.num_particles, scene.num_bodies
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
@@ -334,13 +360,18 @@ def run_ours(args):
         prof_steps = max(5, min(args.steps, 50))
         stage_ms = gs.profile(prof_steps, stream=stream)
     sv = gs.step_view()
-    keys = api.device_view(sv.sorted_keys, n, torch.int32)
-    occupied = int((keys[1:] != keys[:-1]).sum().item()) + 1
     passes = (sv.key_bits + 7) // 8
-    sbytes = stage_bytes(n, nb, passes, occupied)
+    if args.broadphase == "bvh":
+        names = BVH_STAGES
+        sbytes = stage_bytes_bvh(n, nb, passes)
+    else:
+        names = STAGES
+        keys = api.device_view(sv.sorted_keys, n, torch.int32)
+        occupied = int((keys[1:] != keys[:-1]).sum().item()) + 1
+        sbytes = stage_bytes(n, nb, passes, occupied)
     hbm, peak_kind = peaks()
-    dom = max(range(len(STAGES)), key=lambda i: stage_ms[i])
-    dom_name = STAGES[dom]
+    dom = max(range(len(names)), key=lambda i: stage_ms[i])
+    dom_name = names[dom]
     achieved = sbytes[dom_name] / (stage_ms[dom] / 1e3) / 1e9
     step_bytes = sum(sbytes.values())
     step_ms_prof = sum(stage_ms)
@@ -375,14 +406,16 @@ def run_ours(args):
             cpu_baseline = {"value": rate / 1e6, "unit": "Mparticle-steps/s", "cores": cores,
                             "kind": kind, "sample": sample}
 
-    launches = args.steps * (gs.launches_per_step() - 1)  # minus the memset node
+    memsets = 2 if args.broadphase == "bvh" else 1  # memset nodes are not kernels
+    launches = args.steps * (gs.launches_per_step() - memsets)
     if rank == 0:
         line = {
             "metric": "Mparticle-steps/s", "value": value, "unit": "Mparticle-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "broadphase": "grid", "particles": n, "bodies": nb,
+            "config": {"workload": desc, "broadphase": args.broadphase, "particles": n,
+                       "bodies": nb,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "per-step working set > 126 MB L2 (inputs larger than L2)",
                        "timed": "CUDA graph replays, events on the launching stream"},
@@ -394,7 +427,7 @@ def run_ours(args):
             "step_roofline": {"achieved": step_bytes / (ms_per_step / 1e3) / 1e9, "peak": hbm,
                               "unit": "GB/s", "frac": step_bytes / (ms_per_step / 1e3) / 1e9 / hbm,
                               "bytes_per_particle_step": step_bytes / n},
-            "stages_ms": dict(zip(STAGES, stage_ms)), "stage_profile_ms_per_step": step_ms_prof,
+            "stages_ms": dict(zip(names, stage_ms)), "stage_profile_ms_per_step": step_ms_prof,
             "cpu_baseline": cpu_baseline,
             "e2e": {"value": e2e_value, "unit": "Mparticle-steps/s",
                     "h2d_bytes_per_step": 4 * 16 * nb, "d2h_bytes_per_step": 4 * 16 * nb,
@@ -411,18 +444,281 @@ def run_ours(args):
     return 0
 
 
+def _event_time(stream, fn) -> float:
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    fn()
+    b.record(stream)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
+def run_batched(args):
+    """Config 3: 256 independent scenes (log-uniform 2k-200k particles), batched (one launch
+    per stage, CUDA graph) against the plain one-scene-at-a-time form on the same GPU."""
+    import torch
+    from diploma_thesis_b200 import api, autotune, scenes
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    scs = scenes.config3(0)
+    tuner = autotune.Tuner(ctx, args.tune_cache) if args.tune else None
+    kws = [tuner.scene_kwargs(s) if tuner else {} for s in scs]
+    groups = autotune.group(kws)
+    if tuner:  # one launch per stage: a group uses the block size tuned for its median scene
+        for idx in groups.values():
+            med = sorted(scs[i].num_particles for i in idx)[len(idx) // 2]
+            bs = tuner.choice(med).block_size
+            for i in idx:
+                kws[i]["block_size"] = bs
+    n_total = sum(s.num_particles for s in scs)
+    stream = torch.cuda.Stream()
+    plain = [api.GpuScene(ctx, s, **kw) for s, kw in zip(scs, kws)]
+    batch_scenes = [api.GpuScene(ctx, s, **kw) for s, kw in zip(scs, kws)]
+    batches = [api.Batch(ctx, [batch_scenes[i] for i in idx]) for idx in groups.values()]
+    k = args.steps
+    with torch.cuda.stream(stream):
+        for g in plain:
+            g.step(args.warmup, use_graph=True, stream=stream)
+        for b in batches:
+            b.step(args.warmup, use_graph=True, stream=stream)
+        stream.synchronize()
+
+        def plain_steps():
+            for _ in range(k):
+                for g in plain:
+                    g.step(1, use_graph=True, stream=stream)
+
+        def batch_steps():
+            for _ in range(k):
+                for b in batches:
+                    b.step(1, use_graph=True, stream=stream)
+
+        ms_plain = _event_time(stream, plain_steps)
+        ms_batch = _event_time(stream, batch_steps)
+        ctx.check(stream)
+    # same states after the same number of steps: batched == solo, bit for bit
+    same = all(np.array_equal(a.download()["pos"], b.download()["pos"])
+               for a, b in zip(plain[::32], batch_scenes[::32]))
+    ss = len(scs) * k
+    line = {"metric": "scene-steps/s (batched)", "value": ss / (ms_batch / 1e3),
+            "unit": "scene-steps/s", "n_gpus": 1, "steps": k, "warmup": args.warmup,
+            "ms_per_step": ms_batch / k, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched: 256 scenes, particle counts log-uniform in "
+                                   "2k-200k (27-particle cubes), box side U[0.5,2]",
+                       "particles": n_total, "autotuned": bool(tuner),
+                       "broadphase_groups": {k2: len(v) for k2, v in groups.items()}},
+            "plain": {"value": ss / (ms_plain / 1e3), "unit": "scene-steps/s",
+                      "ms_per_step": ms_plain / k},
+            "batched_over_plain": ms_plain / ms_batch,
+            "mparticle_steps_per_s": {"batched": n_total * k / ms_batch / 1e3,
+                                      "plain": n_total * k / ms_plain / 1e3},
+            "batched_equals_plain": bool(same),
+            "gpu_launches": {"batched_per_step": sum(b.launches_per_step() for b in batches),
+                             "plain_per_step": sum(g.launches_per_step() for g in plain)}}
+    print(json.dumps(line))
+    for g in plain + batch_scenes:
+        g.close()
+    for b in batches:
+        b.close()
+    return 0
+
+
+def lbvh_bytes(kb: int, passes: int) -> dict[str, float]:
+    """Algorithmic bytes per point of the LBVH stages (kb = key bytes, 4 or 8)."""
+    return {
+        # AABB reads the points once; encoding reads them again and writes the key
+        "encode": 16 + 16 + kb,
+        # histogram pass reads the keys; first pass reads keys, every pass writes key + index,
+        # later passes read both
+        "sort": kb + kb + (kb + 4) + (passes - 1) * 2 * (kb + 4),
+        # own and neighbour keys (L2 reuse not counted); per internal node: flag, children,
+        # ranges, and the two children's parent links
+        "build": kb + 1 + 16 + 8,
+        # leaves: index and point in; centre, box, radius, flag and range out; refit per
+        # internal node: links and both child boxes in, own box out
+        "refit": (4 + 16 + 16 + 32 + 4 + 9) + (8 + 4 + 64 + 32),
+    }
+
+
+def run_lbvh(args):
+    """Config 1: LBVH microbenchmark.  N = 2^20, 2^22, 2^24 points, uniform or a 16-component
+    Gaussian mixture with 5 % exact duplicates, 30- and 63-bit Morton codes; encode (AABB +
+    codes), sort, build and leaves + refit timed separately with CUDA events (median of the
+    repetitions), each against the HBM roofline."""
+    import torch
+    from diploma_thesis_b200 import api, scenes
+    from diploma_thesis_b200._lib import call
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    P, S = api.ptr, api.stream_handle
+    stream = torch.cuda.Stream()
+    hbm, peak_kind = peaks()
+    sizes = [1 << 20, 1 << 22, 1 << 24] if not args.lbvh_sizes else \
+        [int(x) for x in args.lbvh_sizes.split(",")]
+    rows = []
+    for n in sizes:
+        for dist in ("uniform", "gmm"):
+            pts = torch.from_numpy(scenes.lbvh_points(n, dist, seed=1)).cuda()
+            for wide in (False, True):
+                kdt = torch.int64 if wide else torch.int32
+                kb, bits = (8, 63) if wide else (4, 30)
+                mn = torch.empty(4, device="cuda")
+                mx = torch.empty(4, device="cuda")
+                codes = torch.empty(n, dtype=kdt, device="cuda")
+                skeys = torch.empty(n, dtype=kdt, device="cuda")
+                svals = torch.empty(n, dtype=torch.int32, device="cuda")
+                m = 2 * n - 1
+                t = {k: torch.empty(m, dtype=torch.int32, device="cuda")
+                     for k in ("left", "right", "parent", "min_r", "max_r")}
+                leaf = torch.empty(m, dtype=torch.uint8, device="cuda")
+                cms = torch.empty((n, 4), device="cuda")
+                bounds = torch.empty((m, 8), device="cuda")
+                radii = torch.empty(n, device="cuda")
+                st = S(stream)
+
+                def encode():
+                    call("ar_scene_aabb", ctx.handle, P(pts), n, P(mn), P(mx), st)
+                    call("ar_morton63" if wide else "ar_morton30", ctx.handle, P(pts), n, P(mn),
+                         P(mx), P(codes), None, st)
+
+                def sort():
+                    call("ar_radix_sort_pairs_u64" if wide else "ar_radix_sort_pairs_u32",
+                         ctx.handle, P(codes), None, P(skeys), P(svals), n, 0, bits, st)
+
+                def build():
+                    call("ar_lbvh_build64" if wide else "ar_lbvh_build", ctx.handle, P(skeys), n,
+                         P(leaf), P(t["left"]), P(t["right"]), P(t["parent"]), P(t["min_r"]),
+                         P(t["max_r"]), st)
+
+                def refit():
+                    call("ar_lbvh_leaves", ctx.handle, n, P(svals), P(pts), 1e-3, P(leaf),
+                         P(t["min_r"]), P(t["max_r"]), P(cms), P(bounds), P(radii), st)
+                    call("ar_lbvh_refit", ctx.handle, n, P(t["left"]), P(t["right"]),
+                         P(t["parent"]), P(bounds), st)
+
+                stages = {"encode": encode, "sort": sort, "build": build, "refit": refit}
+                times = {k: [] for k in stages}
+                with torch.cuda.stream(stream):
+                    for rep in range(args.warmup + args.lbvh_reps):
+                        for name, fn in stages.items():
+                            ms = _event_time(stream, fn)
+                            if rep >= args.warmup:
+                                times[name].append(ms)
+                    ctx.check(stream)
+                    ok = bool((skeys[1:] >= skeys[:-1]).all().item())
+                med = {k: float(np.median(v)) for k, v in times.items()}
+                total = sum(med.values())
+                by = lbvh_bytes(kb, (bits + 7) // 8)
+                rows.append({
+                    "n": n, "dist": dist, "bits": bits, "ms": med, "total_ms": total,
+                    "mpoints_per_s": n / total / 1e3,
+                    "roofline_frac": {k: by[k] * n / (med[k] / 1e3) / 1e9 / hbm for k in med},
+                    "sorted": ok})
+                del codes, skeys, svals, t, leaf, cms, bounds, radii
+            del pts
+            torch.cuda.empty_cache()
+    big = [r for r in rows if r["n"] == max(sizes)]
+    head = max(big, key=lambda r: r["mpoints_per_s"])
+    line = {"metric": "Mpoints/s (LBVH encode+sort+build+refit)", "value": head["mpoints_per_s"],
+            "unit": "Mpoints/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "warmup": args.warmup, "reps": args.lbvh_reps,
+            "config": {"workload": "LBVH microbenchmark: uniform / 16-component Gaussian mixture "
+                                   "with 5% duplicates, 30/63-bit Morton",
+                       "headline": {k: head[k] for k in ("n", "dist", "bits")}},
+            "peak_gbs": hbm, "peak_kind": f"{peak_kind} hbm_gbs",
+            "bytes_per_point": {"30": lbvh_bytes(4, 4), "63": lbvh_bytes(8, 8)},
+            "rows": rows}
+    print(json.dumps(line))
+    return 0
+
+
+def run_served(args):
+    """Config 4: Poisson request stream (scenes of 1k-500k particles, cubes and rods, K in
+    10..500) served with continuous batching under an HBM budget; the plain form serves the
+    same requests one at a time."""
+    import torch
+    from diploma_thesis_b200 import api, scenes, serve
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    rng = np.random.default_rng(1)
+    pool = [scenes.config4_request(rng) for _ in range(args.pool)]  # distinct scenes, reused
+
+    def make(r):
+        sc, _ = pool[int(r.integers(len(pool)))]
+        return sc, int(r.integers(10, 501))
+
+    reqs = serve.poisson_requests(args.rate, args.duration, make, seed=2)
+    server = serve.Server(ctx, args.hbm_budget_gb * 1e9, tick_steps=10)
+    stats = server.run(reqs, time_limit=args.duration)
+    s = stats.summary()
+    # plain: a sample of the same requests, one at a time (create, K steps, download)
+    sample = reqs[: min(len(reqs), 40)]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    steps = parts = 0
+    for r in sample:
+        g = api.GpuScene(ctx, r.scene)
+        g.step(r.steps, use_graph=True)
+        g.download()
+        g.close()
+        steps += r.steps
+        parts += r.steps * r.scene.num_particles
+    plain_s = time.perf_counter() - t0
+    offered = sum(r.steps * r.scene.num_particles for r in reqs) / args.duration / 1e6
+    line = {"metric": "scene-steps/s (served)", "value": s["scene_steps_per_s"],
+            "unit": "scene-steps/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"served: Poisson {args.rate}/s for {args.duration} s, "
+                                   "scenes 1k-500k particles (cubes/rods 50/50), K in 10..500, "
+                                   f"HBM budget {args.hbm_budget_gb} GB",
+                       "scene_pool": args.pool},
+            "p50_latency_s": s["p50_latency_s"], "p99_latency_s": s["p99_latency_s"],
+            "completed": s["completed"], "offered_requests": s["offered"],
+            "mparticle_steps_per_s": s["mparticle_steps_per_s"],
+            "offered_mparticle_steps_per_s": offered,
+            "plain": {"scene_steps_per_s": steps / plain_s,
+                      "mparticle_steps_per_s": parts / plain_s / 1e6,
+                      "sample_requests": len(sample)},
+            "served_over_plain": s["scene_steps_per_s"] / (steps / plain_s),
+            "peak_resident_scenes": s["peak_resident_scenes"],
+            "peak_resident_gb": s["peak_resident_bytes"] / 1e9, "ticks": s["ticks"]}
+    print(json.dumps(line))
+    server.close()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["pile", "plain"], default="pile")
+    ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh"],
+                    default="pile")
+    ap.add_argument("--lbvh-sizes", default="", help="lbvh: comma-separated point counts")
+    ap.add_argument("--lbvh-reps", type=int, default=10, help="lbvh: timed repetitions")
+    ap.add_argument("--broadphase", choices=["grid", "bvh"], default="grid",
+                    help="pile / plain: broad phase of the fused step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--tune", action="store_true", help="batched: autotune per size bucket")
+    ap.add_argument("--tune-cache", default=str(ROOT / "diploma_thesis_b200" / "autotune_b200.json"))
+    ap.add_argument("--rate", type=float, default=2000.0, help="served: requests per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="served: seconds of arrivals")
+    ap.add_argument("--pool", type=int, default=64, help="served: distinct scenes drawn from")
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
+    if args.workload == "served":
+        return run_served(args)
+    if args.workload == "lbvh":
+        return run_lbvh(args)
     return run_ours(args)
 
 

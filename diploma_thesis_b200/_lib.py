@@ -63,11 +63,18 @@ class SceneView(C.Structure):
                 ("body_force4", C.c_void_p), ("body_torque4", C.c_void_p)]
 
 
+AR_MAX_BATCH_CELLS = (1 << 32) - 1
+AR_MAX_BATCH_PARTICLES = (1 << 30) - 1
+
+
 class StepView(C.Structure):
     _fields_ = [("num_particles", C.c_int), ("num_cells", C.c_uint64), ("key_bits", C.c_int),
                 ("sorted_keys", C.c_void_p), ("sorted_idx", C.c_void_p),
                 ("sorted_pos4", C.c_void_p), ("sorted_vel4", C.c_void_p),
-                ("particle_force4", C.c_void_p), ("cells2", C.c_void_p)]
+                ("particle_force4", C.c_void_p), ("cells2", C.c_void_p),
+                ("key_bytes", C.c_int), ("broadphase", C.c_int), ("tree_left", C.c_void_p),
+                ("tree_right", C.c_void_p), ("tree_parent", C.c_void_p),
+                ("tree_bounds8", C.c_void_p)]
 
 
 P = C.c_void_p
@@ -117,6 +124,7 @@ SIGNATURES = {
     "ar_scene_create": [P, C.POINTER(SceneDesc), C.POINTER(SceneInit), S, C.POINTER(P)],
     "ar_scene_destroy": [P],
     "ar_scene_footprint": [C.POINTER(SceneDesc)],
+    "ar_scene_cells": [C.POINTER(SceneDesc)],
     "ar_scene_download": [P, P, P, P, P, S],
     "ar_scene_upload": [P, P, P, P, P, S],
     "ar_step_profile": [P, P, I, C.POINTER(F), S],
@@ -134,7 +142,8 @@ SIGNATURES = {
     "ar_scene_launches_per_step": [P],
 }
 _RESTYPE = {"ar_last_error": C.c_char_p, "ar_version": C.c_char_p,
-            "ar_scene_footprint": C.c_size_t, "ar_batch_launches_per_step": C.c_int,
+            "ar_scene_footprint": C.c_size_t, "ar_scene_cells": C.c_uint64,
+            "ar_batch_launches_per_step": C.c_int,
             "ar_scene_launches_per_step": C.c_int}
 
 

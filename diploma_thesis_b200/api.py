@@ -62,6 +62,18 @@ class Context:
             pass
 
 
+def broadphase_code(b) -> int:
+    """'grid' / 'bvh' (or the AR_BROADPHASE_* value) -> AR_BROADPHASE_*."""
+    if isinstance(b, str):
+        codes = {"grid": AR_BROADPHASE_GRID, "bvh": AR_BROADPHASE_BVH}
+        if b not in codes:
+            raise ValueError(f"unknown broad phase {b!r} (grid or bvh)")
+        return codes[b]
+    if b not in (AR_BROADPHASE_GRID, AR_BROADPHASE_BVH):
+        raise ValueError(f"unknown broad phase {b!r}")
+    return int(b)
+
+
 def make_desc(scene: Scene, broadphase: int = AR_BROADPHASE_GRID, block_size: int = 0,
               cell_size: float | None = None, grid_log2=None) -> SceneDesc:
     d = SceneDesc()
@@ -94,10 +106,11 @@ class GpuScene:
     """A scene resident on the device, advanced by ar_step."""
 
     def __init__(self, ctx: Context, scene: Scene, block_size: int = 0,
-                 cell_size: float | None = None, grid_log2=None):
+                 cell_size: float | None = None, grid_log2=None, broadphase="grid"):
         self.ctx = ctx
         self.scene = scene
-        self.desc = make_desc(scene, AR_BROADPHASE_GRID, block_size, cell_size, grid_log2)
+        self.broadphase = broadphase_code(broadphase)
+        self.desc = make_desc(scene, self.broadphase, block_size, cell_size, grid_log2)
         self._keep = [np.ascontiguousarray(a) for a in (
             scene.body_pos, scene.body_quat, scene.body_vel, scene.body_angvel,
             scene.body_mass.astype(np.float32), scene.body_inv_inertia.astype(np.float32),

@@ -1,17 +1,19 @@
-"""Autotuner: per scene-size bucket, the grid cell size, the wrapped grid size and the block
-size of the DEM gather that give the fastest fused step on this GPU.
+"""Autotuner: per scene-size bucket, the broad phase (uniform grid or BVH), and for the grid the
+cell size and wrapped grid size, and the block size of the DEM gather, that give the fastest
+fused step on this GPU.
 
 Buckets are powers of two of the particle count.  For each bucket a representative scene
 (27-particle cubes, config-0 distributions) is stepped under every candidate and timed with
 CUDA events over CUDA-graph replays; the fastest candidate is kept.  Results are cached in a
 JSON file keyed by GPU name, so a deployment tunes once.
 
-Candidates: cell = f * 2r for f in CELL_FACTORS; cells per axis wrapped so that the grid
-holds at most next_pow2(m * N) cells for m in GRID_MULTS; block size in BLOCK_SIZES.  Every
-candidate gives the same contacts (the cell is never smaller than the contact distance and the
+Candidates: grid with cell = f * 2r for f in CELL_FACTORS and cells per axis wrapped so that
+the grid holds at most next_pow2(m * N) cells for m in GRID_MULTS, or the BVH; block size in
+BLOCK_SIZES.  Every candidate gives the same contacts (the cell is never smaller than the contact distance and the
 wrap only aliases distant cells, which the distance test rejects), so the choice changes speed,
 not results -- except for the summation order of a particle's contacts, which follows the cell
-order.
+order (grid) or the tree's visit order (BVH).  Scenes of one batch share a broad phase, so a
+mixed table is stepped as one batch per broad phase (``group``).
 """
 from __future__ import annotations
 
@@ -36,6 +38,7 @@ class Choice:
     grid_mult: int
     block_size: int
     ms_per_step: float
+    broadphase: str = "grid"
 
 
 def bucket_of(num_particles: int) -> int:
@@ -61,6 +64,8 @@ def grid_for(scene: scenes.Scene, cell: float, mult: int) -> tuple[int, int, int
 
 def apply(scene: scenes.Scene, choice: Choice) -> dict:
     """Keyword arguments for api.GpuScene that realise a choice for this scene."""
+    if choice.broadphase == "bvh":
+        return {"broadphase": "bvh", "block_size": choice.block_size}
     cell = float(np.float32(choice.cell_factor * 2 * scene.radius))
     return {"cell_size": cell, "grid_log2": grid_for(scene, cell, choice.grid_mult),
             "block_size": choice.block_size}
@@ -92,15 +97,31 @@ def tune_bucket(ctx: api.Context, bucket: int, steps: int = 20, seed: int = 0) -
                 c.ms_per_step = _time_steps(ctx, scene, apply(scene, c), steps)
                 if best is None or c.ms_per_step < best.ms_per_step:
                     best = c
+    for bs in BLOCK_SIZES:
+        c = Choice(1.0, 0, bs, 0.0, "bvh")
+        c.ms_per_step = _time_steps(ctx, scene, apply(scene, c), steps)
+        if c.ms_per_step < best.ms_per_step:
+            best = c
     return best
 
 
+def group(kwargs: list[dict]) -> dict[str, list[int]]:
+    """Indices of the scenes per broad phase (each group is stepped as one batch)."""
+    out: dict[str, list[int]] = {}
+    for i, kw in enumerate(kwargs):
+        out.setdefault(kw.get("broadphase", "grid"), []).append(i)
+    return out
+
+
 class Tuner:
-    def __init__(self, ctx: api.Context, cache: str | Path | None = None):
+    """Per-bucket choices, tuned on first use and cached per GPU name."""
+
+    def __init__(self, ctx: api.Context, cache: str | Path | None = None,
+                 gpu_name: str | None = None):
         self.ctx = ctx
         self.cache = Path(cache) if cache else None
         self.table: dict[int, Choice] = {}
-        self.gpu = torch.cuda.get_device_name()
+        self.gpu = gpu_name or torch.cuda.get_device_name()
         if self.cache and self.cache.exists():
             data = json.loads(self.cache.read_text())
             for k, v in data.get(self.gpu, {}).items():

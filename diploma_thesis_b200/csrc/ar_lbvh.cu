@@ -11,25 +11,17 @@
 // contacts in the same order keeps the float sums identical to the reference's.
 #include "ar_internal.cuh"
 #include "ar_dem.cuh"
+#include "ar_lbvh.cuh"
+
+using ar_lbvh::Box;
+using ar_lbvh::load_box;
+using ar_lbvh::overlap;
 
 namespace {
 
-// ---- longest common prefix (BVHSource/BVHAuxiliary.cuh:31-43) ------------------------------
-__device__ __forceinline__ int lcp(const uint32_t* __restrict__ c, int n, int i, int j) {
-  if (j < 0 || j >= n) return -1;
-  uint32_t a = __ldg(c + i), b = __ldg(c + j);
-  return a != b ? __clz(a ^ b) : __clz(i ^ j) + 32;
-}
-__device__ __forceinline__ int lcp(const uint64_t* __restrict__ c, int n, int i, int j) {
-  if (j < 0 || j >= n) return -1;
-  uint64_t a = __ldg((const unsigned long long*)c + i), b = __ldg((const unsigned long long*)c + j);
-  return a != b ? __clzll(a ^ b) : __clz(i ^ j) + 64;
-}
-
 // ---- Karras 2012 internal nodes (kernelConstructRadixTreeSoA, BVHSoAKernels.cu:7-99) -------
-template <class K>
-__global__ void __launch_bounds__(256) build_kernel(const K* __restrict__ codes, int n,
-                                                    uint8_t* __restrict__ is_leaf,
+template <class Lcp>
+__global__ void __launch_bounds__(256) build_kernel(Lcp lcp, int n, uint8_t* __restrict__ is_leaf,
                                                     int32_t* __restrict__ left,
                                                     int32_t* __restrict__ right,
                                                     int32_t* __restrict__ parent,
@@ -38,37 +30,7 @@ __global__ void __launch_bounds__(256) build_kernel(const K* __restrict__ codes,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) parent[n] = -1;  // root: no parent (the reference leaves it unset)
   if (i >= n - 1) return;
-  const int d = (lcp(codes, n, i, i + 1) - lcp(codes, n, i, i - 1)) > 0 ? 1 : -1;
-  const int sig_min = lcp(codes, n, i, i - d);
-  int lmax = 2;
-  while (lcp(codes, n, i, i + lmax * d) > sig_min) lmax *= 2;
-  int l = 0;
-  for (int t = lmax / 2; t >= 1; t /= 2) {
-    if (lcp(codes, n, i, i + (l + t) * d) > sig_min) l += t;
-    if (t == 1) break;
-  }
-  const int j = i + l * d;
-  const int sig_node = lcp(codes, n, i, j);
-  // split search: t = ceil(l / 2^k), k = 1, 2, ... (the reference's double division by a
-  // power of two is exact, so the integer ceiling is the same value)
-  int s = 0;
-  for (int k = 1;; ++k) {
-    int t = (int)(((long long)l + (1ll << k) - 1) >> k);
-    if (lcp(codes, n, i, i + (s + t) * d) > sig_node) s += t;
-    if (t <= 1) break;
-  }
-  const int gamma = i + s * d + min(d, 0);
-  const int node = n + i;
-  const int lo = min(i, j), hi = max(i, j);
-  is_leaf[node] = 0;
-  const int lc = (lo == gamma) ? gamma : gamma + n;
-  const int rc = (hi == gamma + 1) ? gamma + 1 : gamma + 1 + n;
-  left[node] = lc;
-  right[node] = rc;
-  parent[lc] = node;
-  parent[rc] = node;
-  min_r[node] = lo;
-  max_r[node] = hi;
+  ar_lbvh::karras_node(i, n, lcp, is_leaf, left, right, parent, min_r, max_r);
 }
 
 // ---- leaves (kernelConstructLeafNodesSoA + initializeRadii, BVHSoAKernels.cu:108-138) ------
@@ -93,37 +55,13 @@ __global__ void __launch_bounds__(256) leaves_kernel(int n, const int32_t* __res
 }
 
 // ---- refit (kernelConstructInternalNodesSoA, BVHSoAKernels.cu:148-176) ----------------------
-// Release (fence before the counter) / acquire (fence after it, L2 loads of the children).
 __global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t* __restrict__ left,
                                                     const int32_t* __restrict__ right,
                                                     const int32_t* __restrict__ parent,
                                                     float4* bounds, int* __restrict__ counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  int node = __ldg(parent + i);
-  for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
-    if (node < n || node >= 2 * n - 1) return;  // malformed parent link
-    __threadfence();
-    if (atomicAdd(counters + (node - n), 1) == 0) return;
-    __threadfence();
-    const int a = __ldg(left + node), b = __ldg(right + node);
-    float4 a0 = __ldcg(bounds + 2 * a), a1 = __ldcg(bounds + 2 * a + 1);
-    float4 b0 = __ldcg(bounds + 2 * b), b1 = __ldcg(bounds + 2 * b + 1);
-    // mergeBounds (BVHAuxiliary.cuh:83-94): min via `a < b ? a : b`, max via `a > b ? a : b`
-    float4 m0, m1;
-    m0.x = a0.x < b0.x ? a0.x : b0.x;
-    m0.y = a0.y < b0.y ? a0.y : b0.y;
-    m0.z = a0.z < b0.z ? a0.z : b0.z;
-    m0.w = a0.w > b0.w ? a0.w : b0.w;  // max.x
-    m1.x = a1.x > b1.x ? a1.x : b1.x;  // max.y
-    m1.y = a1.y > b1.y ? a1.y : b1.y;  // max.z
-    m1.z = 0.f;
-    m1.w = 0.f;
-    __stcg(bounds + 2 * node, m0);
-    __stcg(bounds + 2 * node + 1, m1);
-    if (node == n) return;
-    node = __ldg(parent + node);
-  }
+  ar_lbvh::refit_from_leaf(i, n, left, right, parent, bounds, counters);
 }
 
 // Parent links from the child links, for callers with the reference's traversal signature
@@ -137,58 +75,6 @@ __global__ void __launch_bounds__(256) parents_kernel(int n, const int32_t* __re
   parent[__ldg(left + node)] = node;
   parent[__ldg(right + node)] = node;
   if (i == 0) parent[n] = -1;
-}
-
-// ---- traversal helpers -------------------------------------------------------------------------
-struct Box {
-  float lx, ly, lz, hx, hy, hz;
-};
-__device__ __forceinline__ Box load_box(const float4* __restrict__ b, int node) {
-  float4 p = __ldg(b + 2 * node), q = __ldg(b + 2 * node + 1);
-  return Box{p.x, p.y, p.z, p.w, q.x, q.y};
-}
-// checkOverlap(AABB, AABB) (BVHAuxiliary.cuh:139-152)
-__device__ __forceinline__ bool overlap(const Box& a, const Box& b) {
-  return (a.lx <= b.hx && a.hx >= b.lx) && (a.ly <= b.hy && a.hy >= b.ly) &&
-         (a.lz <= b.hz && a.hz >= b.lz);
-}
-
-// Walk the tree in the reference's order, calling visit_leaf(leaf, is_left_child) for every
-// leaf child that `accept(child)` admits, and descending into internal children it admits.
-template <class Accept, class Visit>
-__device__ __forceinline__ void walk(int n, const uint8_t* __restrict__ is_leaf,
-                                     const int32_t* __restrict__ left,
-                                     const int32_t* __restrict__ right,
-                                     const int32_t* __restrict__ parent, Accept accept,
-                                     Visit visit_leaf) {
-  // The root (index n) is never left through its parent link, so parent[n] is not read.
-  // A valid tree is walked in fewer than 4 (2n - 1) moves; the bound only guards against a
-  // malformed tree passed in by a caller.
-  int node = n;
-  bool descending = true;
-  int from = -1;
-  for (long moves = 8l * n + 64; moves > 0; --moves) {
-    if (descending) {
-      const int lc = __ldg(left + node), rc = __ldg(right + node);
-      const bool ll = __ldg(is_leaf + lc), rl = __ldg(is_leaf + rc);
-      const bool ol = accept(lc), orr = accept(rc);
-      if (ol && ll) visit_leaf(lc, true);
-      if (orr && rl) visit_leaf(rc, false);
-      if (ol && !ll) { node = lc; continue; }
-      if (orr && !rl) { node = rc; continue; }
-      descending = false;
-    } else {
-      const int rc = __ldg(right + node);
-      if (from == __ldg(left + node) && !__ldg(is_leaf + rc) && accept(rc)) {
-        node = rc;
-        descending = true;
-        continue;
-      }
-    }
-    if (node == n) return;
-    from = node;
-    node = __ldg(parent + node);
-  }
 }
 
 // ---- collideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:100-244) ------------------------------
@@ -214,7 +100,7 @@ __global__ void __launch_bounds__(128) collide_bvh_kernel(
   float4 corr = make_float4(0.f, 0.f, 0.f, 0.f);
   const float3 r3 = ar::xyz(qrel);
   if (n >= 2) {
-    walk(n, is_leaf, left, right, parent,
+    ar_lbvh::walk(n, n, is_leaf, left, right, parent,
          [&](int c) { return c != index && overlap(qbox, load_box(bounds, c)); },
          [&](int c, bool is_left) {
            const int oc = __ldg(sorted_idx + c);
@@ -260,7 +146,7 @@ __global__ void __launch_bounds__(128) find_contacts_kernel(
   float best = contact_distance[q];
   int best_p = 0, best_b = 0;
   bool found = false;
-  walk(n, is_leaf, left, right, parent,
+  ar_lbvh::walk(n, n, is_leaf, left, right, parent,
        [&](int c) {
          return c != index && __ldg(max_r + c) >= index && overlap(qbox, load_box(bounds, c));
        },
@@ -299,7 +185,7 @@ __global__ void __launch_bounds__(128) pairs_bvh_kernel(
   const float4 qpos = __ldg(cms + index);
   const Box qbox = load_box(bounds, index);
   const int qbody = __ldg(rb_idx + q);
-  walk(n, is_leaf, left, right, parent,
+  ar_lbvh::walk(n, n, is_leaf, left, right, parent,
        [&](int c) { return c != index && overlap(qbox, load_box(bounds, c)); },
        [&](int c, bool) {
          if (c < index) return;  // each unordered pair once (from its lower sorted leaf)
@@ -336,8 +222,8 @@ ar_status ar_lbvh_build(ar_ctx* ctx, const uint32_t* sorted_codes, int n, uint8_
                                   !min_r || !max_r)))
     return AR_ERR_INVALID_ARG;
   if (n < 2) return AR_OK;
-  build_kernel<uint32_t><<<arh::grid_for(n - 1, 256), 256, 0, arh::stream(stream)>>>(
-      sorted_codes, n, is_leaf, left, right, parent, min_r, max_r);
+  build_kernel<<<arh::grid_for(n - 1, 256), 256, 0, arh::stream(stream)>>>(
+      ar_lbvh::Lcp32{sorted_codes, n}, n, is_leaf, left, right, parent, min_r, max_r);
   return arh::check_launch("ar_lbvh_build");
 }
 
@@ -348,8 +234,8 @@ ar_status ar_lbvh_build64(ar_ctx* ctx, const uint64_t* sorted_codes, int n, uint
                                   !min_r || !max_r)))
     return AR_ERR_INVALID_ARG;
   if (n < 2) return AR_OK;
-  build_kernel<uint64_t><<<arh::grid_for(n - 1, 256), 256, 0, arh::stream(stream)>>>(
-      sorted_codes, n, is_leaf, left, right, parent, min_r, max_r);
+  build_kernel<<<arh::grid_for(n - 1, 256), 256, 0, arh::stream(stream)>>>(
+      ar_lbvh::Lcp64{sorted_codes, n}, n, is_leaf, left, right, parent, min_r, max_r);
   return arh::check_launch("ar_lbvh_build64");
 }
 

@@ -1,0 +1,173 @@
+// LBVH device routines shared by the stage entry points (ar_lbvh.cu) and the fused BVH step
+// (ar_pipeline.cu): Karras node construction, fenced bottom-up refit, box tests and the
+// stackless traversal in the reference's visit order.
+//
+// Node numbering is the reference's SoA layout (BVHSource/BVHSoAKernels.cu): leaf i at index
+// i, internal node i at n + i, root at n.  Boxes are the reference's 32-byte AABB
+// {min.xyz, max.xyz, pad, pad}, read as two float4.
+#pragma once
+#include "ar_internal.cuh"
+
+namespace ar_lbvh {
+
+// ---- longest common prefix (BVHSource/BVHAuxiliary.cuh:31-43) ------------------------------
+struct Lcp32 {
+  const uint32_t* __restrict__ c;
+  int n;
+  __device__ __forceinline__ int operator()(int i, int j) const {
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = __ldg(c + i), b = __ldg(c + j);
+    return a != b ? __clz(a ^ b) : __clz(i ^ j) + 32;
+  }
+};
+struct Lcp64 {
+  const uint64_t* __restrict__ c;
+  int n;
+  __device__ __forceinline__ int operator()(int i, int j) const {
+    if (j < 0 || j >= n) return -1;
+    const uint64_t a = __ldg((const unsigned long long*)c + i),
+                   b = __ldg((const unsigned long long*)c + j);
+    return a != b ? __clzll(a ^ b) : __clz(i ^ j) + 64;
+  }
+};
+// 64-bit keys whose top bits (>> shift) name a scene: equal keys are tie-broken by their index
+// within the scene, so a scene's subtree is the same as in a tree built over the scene alone.
+struct Lcp64Scene {
+  const uint64_t* __restrict__ c;
+  int n;
+  const int* __restrict__ poff;
+  int shift;
+  __device__ __forceinline__ int operator()(int i, int j) const {
+    if (j < 0 || j >= n) return -1;
+    const uint64_t a = __ldg((const unsigned long long*)c + i),
+                   b = __ldg((const unsigned long long*)c + j);
+    if (a != b) return __clzll(a ^ b);
+    const int base = __ldg(poff + (int)(a >> shift));
+    return __clz((i - base) ^ (j - base)) + 64;
+  }
+};
+
+// ---- Karras 2012 internal node i (kernelConstructRadixTreeSoA, BVHSoAKernels.cu:7-99) ----
+template <class Lcp>
+__device__ __forceinline__ void karras_node(int i, int n, const Lcp& lcp, uint8_t* is_leaf,
+                                            int32_t* left, int32_t* right, int32_t* parent,
+                                            int32_t* min_r, int32_t* max_r) {
+  const int d = (lcp(i, i + 1) - lcp(i, i - 1)) > 0 ? 1 : -1;
+  const int sig_min = lcp(i, i - d);
+  int lmax = 2;
+  while (lcp(i, i + lmax * d) > sig_min) lmax *= 2;
+  int l = 0;
+  for (int t = lmax / 2; t >= 1; t /= 2) {
+    if (lcp(i, i + (l + t) * d) > sig_min) l += t;
+    if (t == 1) break;
+  }
+  const int j = i + l * d;
+  const int sig_node = lcp(i, j);
+  // split search: t = ceil(l / 2^k), k = 1, 2, ... (the reference's double division by a
+  // power of two is exact, so the integer ceiling is the same value)
+  int s = 0;
+  for (int k = 1;; ++k) {
+    const int t = (int)(((long long)l + (1ll << k) - 1) >> k);
+    if (lcp(i, i + (s + t) * d) > sig_node) s += t;
+    if (t <= 1) break;
+  }
+  const int gamma = i + s * d + min(d, 0);
+  const int node = n + i;
+  const int lo = min(i, j), hi = max(i, j);
+  is_leaf[node] = 0;
+  const int lc = (lo == gamma) ? gamma : gamma + n;
+  const int rc = (hi == gamma + 1) ? gamma + 1 : gamma + 1 + n;
+  left[node] = lc;
+  right[node] = rc;
+  parent[lc] = node;
+  parent[rc] = node;
+  min_r[node] = lo;
+  max_r[node] = hi;
+}
+
+// ---- bottom-up refit from leaf i (kernelConstructInternalNodesSoA, BVHSoAKernels.cu:148-176)
+// Release (fence before the counter) / acquire (fence after it, L2 loads of the children); the
+// second thread to reach a node merges its children (mergeBounds, BVHAuxiliary.cuh:83-94).
+__device__ __forceinline__ void refit_from_leaf(int i, int n, const int32_t* __restrict__ left,
+                                                const int32_t* __restrict__ right,
+                                                const int32_t* __restrict__ parent,
+                                                float4* bounds, int* __restrict__ counters) {
+  int node = __ldg(parent + i);
+  for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
+    if (node < n || node >= 2 * n - 1) return;  // malformed parent link
+    __threadfence();
+    if (atomicAdd(counters + (node - n), 1) == 0) return;
+    __threadfence();
+    const int a = __ldg(left + node), b = __ldg(right + node);
+    const float4 a0 = __ldcg(bounds + 2 * a), a1 = __ldcg(bounds + 2 * a + 1);
+    const float4 b0 = __ldcg(bounds + 2 * b), b1 = __ldcg(bounds + 2 * b + 1);
+    float4 m0, m1;
+    m0.x = a0.x < b0.x ? a0.x : b0.x;
+    m0.y = a0.y < b0.y ? a0.y : b0.y;
+    m0.z = a0.z < b0.z ? a0.z : b0.z;
+    m0.w = a0.w > b0.w ? a0.w : b0.w;  // max.x
+    m1.x = a1.x > b1.x ? a1.x : b1.x;  // max.y
+    m1.y = a1.y > b1.y ? a1.y : b1.y;  // max.z
+    m1.z = 0.f;
+    m1.w = 0.f;
+    __stcg(bounds + 2 * node, m0);
+    __stcg(bounds + 2 * node + 1, m1);
+    if (node == n) return;
+    node = __ldg(parent + node);
+  }
+}
+
+// ---- boxes -----------------------------------------------------------------------------------
+struct Box {
+  float lx, ly, lz, hx, hy, hz;
+};
+__device__ __forceinline__ Box load_box(const float4* __restrict__ b, int node) {
+  const float4 p = __ldg(b + 2 * node), q = __ldg(b + 2 * node + 1);
+  return Box{p.x, p.y, p.z, p.w, q.x, q.y};
+}
+// checkOverlap(AABB, AABB) (BVHAuxiliary.cuh:139-152)
+__device__ __forceinline__ bool overlap(const Box& a, const Box& b) {
+  return (a.lx <= b.hx && a.hx >= b.lx) && (a.ly <= b.hy && a.hy >= b.ly) &&
+         (a.lz <= b.hz && a.hz >= b.lz);
+}
+
+// ---- stackless traversal in the reference's order (RB_BVHKernels.cu:145-214) -------------------
+// From internal node `root`: at each internal node, the overlapping leaf children are handled
+// left then right, then the walk descends into the left internal child if it overlaps, and on
+// the way back up into the right one.  visit_leaf(leaf, is_left_child) for every leaf child
+// that accept(child) admits.  `root` is never left through its parent link.  A valid tree is
+// walked in fewer than 4 (2n - 1) moves; the bound only guards against a malformed tree.
+template <class Accept, class Visit>
+__device__ __forceinline__ void walk(int root, int n, const uint8_t* __restrict__ is_leaf,
+                                     const int32_t* __restrict__ left,
+                                     const int32_t* __restrict__ right,
+                                     const int32_t* __restrict__ parent, Accept accept,
+                                     Visit visit_leaf) {
+  int node = root;
+  bool descending = true;
+  int from = -1;
+  for (long moves = 8l * n + 64; moves > 0; --moves) {
+    if (descending) {
+      const int lc = __ldg(left + node), rc = __ldg(right + node);
+      const bool ll = __ldg(is_leaf + lc), rl = __ldg(is_leaf + rc);
+      const bool ol = accept(lc), orr = accept(rc);
+      if (ol && ll) visit_leaf(lc, true);
+      if (orr && rl) visit_leaf(rc, false);
+      if (ol && !ll) { node = lc; continue; }
+      if (orr && !rl) { node = rc; continue; }
+      descending = false;
+    } else {
+      const int rc = __ldg(right + node);
+      if (from == __ldg(left + node) && !__ldg(is_leaf + rc) && accept(rc)) {
+        node = rc;
+        descending = true;
+        continue;
+      }
+    }
+    if (node == root) return;
+    from = node;
+    node = __ldg(parent + node);
+  }
+}
+
+}  // namespace ar_lbvh

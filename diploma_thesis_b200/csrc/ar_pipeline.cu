@@ -14,6 +14,12 @@
 // A scene's keys live in its own cell range, so sorting all scenes together orders them by
 // scene and within a scene exactly as a solo sort would: batched and solo steps are
 // bit-identical.  The sequence is captured once into a CUDA graph and replayed.
+//
+// Batches of BVH scenes replace K1-K4 by: 64-bit keys (scene index above the particle's 30-bit
+// Morton code), a 64-bit onesweep sort, leaves in sorted order, Karras nodes over all scenes
+// (equal codes tie-broken by the index within the scene), each scene's subtree root, fenced
+// refit, and a stackless walk of the scene's subtree per particle in the reference's visit
+// order.  K5 is shared.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -21,6 +27,7 @@
 
 #include "ar_internal.cuh"
 #include "ar_dem.cuh"
+#include "ar_lbvh.cuh"
 #include "ar_pipeline.cuh"
 #include "ar_sort.cuh"
 
@@ -72,7 +79,7 @@ __global__ void __launch_bounds__(kK1Threads) repose_hash_kernel(
       float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
       const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
       keys[g] = key;
-      ar_sort::hist_count(s_hist, key, 0, passes, last_bits);
+      ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
     }
   }
   __syncthreads();
@@ -110,7 +117,11 @@ __global__ void __launch_bounds__(256) scatter_kernel(
 // Per sorted particle: the 27 neighbour cells in z, y, x order, occupants in sorted order,
 // skipping itself and its own body; per-cell partial sums added to the total (the order of
 // FindAndHandleRigidBodyCollisionsUniformGridKernel, RigidBodies/UniformGridDEM.cu:166-193).
-__global__ void __launch_bounds__(128) collide_kernel(
+// The three cells of an x-row are walked as one flattened loop (candidate t of the row maps
+// to cell A, B or C and to that cell's partial sum), so a warp's lanes stay in step across
+// cells.  Candidates at squared distance >= the float just above (2r)^2 are rejected without
+// the square root: for them sqrtf(d2) >= 2r exactly, so the contact test is unchanged.
+__global__ void __launch_bounds__(256, 4) collide_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
     const uint32_t* __restrict__ svals, const uint2* __restrict__ cells,
     const float4* __restrict__ spos, const float4* __restrict__ svel,
@@ -118,34 +129,195 @@ __global__ void __launch_bounds__(128) collide_kernel(
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
   const int g = (int)__ldg(svals + k);
-  const SceneDev& S = table[find_range(poff, ns, g)];
+  const SceneDev& S = table[ns == 1 ? 0 : find_range(poff, ns, g)];
   const float4 p4 = __ldg(spos + k);
   const float3 pos = ar::xyz(p4);
   const int body = __float_as_int(p4.w);
   const float3 vel = ar::xyz(__ldg(svel + k));
   const float thr = 2.0f * S.r;
+  const float thr2_up = nextafterf(thr * thr, INFINITY);
   const float kk = S.k, dmp = S.damping, shr = S.shear, att = S.attraction;
   const int3 gp = ar_pipe::cell_of(S, pos);
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
   for (int z = -1; z <= 1; ++z)
-    for (int y = -1; y <= 1; ++y)
-      for (int x = -1; x <= 1; ++x) {
-        float3 cell_f = ar::mk3(0.f, 0.f, 0.f);
-        const uint2 se = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x + x, gp.y + y, gp.z + z)));
-        if (se.x != ar::kEmpty) {
-          for (uint32_t j = se.x; j < se.y; ++j) {
-            const float4 q4 = __ldg(spos + j);
-            if (j == (uint32_t)k || __float_as_int(q4.w) == body) continue;
-            const float3 rp = ar::sub(ar::xyz(q4), pos);
-            const float dist = sqrtf(ar::dot(rp, rp));
-            if (dist < thr) {
-              const float3 v2 = ar::xyz(__ldg(svel + j));
-              cell_f = ar::add(cell_f, ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att));
-            }
-          }
-        }
-        lin = ar::add(lin, cell_f);
+    for (int y = -1; y <= 1; ++y) {
+      const uint2 ca = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x - 1, gp.y + y, gp.z + z)));
+      const uint2 cb = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x, gp.y + y, gp.z + z)));
+      const uint2 cc = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x + 1, gp.y + y, gp.z + z)));
+      const uint32_t na = ca.x == ar::kEmpty ? 0u : ca.y - ca.x;
+      const uint32_t nb = cb.x == ar::kEmpty ? 0u : cb.y - cb.x;
+      const uint32_t nc = cc.x == ar::kEmpty ? 0u : cc.y - cc.x;
+      const uint32_t nab = na + nb, total = nab + nc;
+      float3 fa = ar::mk3(0.f, 0.f, 0.f), fb = fa, fc = fa;
+      for (uint32_t t = 0; t < total; ++t) {
+        const uint32_t j = t < na ? ca.x + t : (t < nab ? cb.x + (t - na) : cc.x + (t - nab));
+        const float4 q4 = __ldg(spos + j);
+        if (j == (uint32_t)k || __float_as_int(q4.w) == body) continue;
+        const float3 rp = ar::sub(ar::xyz(q4), pos);
+        const float d2 = ar::dot(rp, rp);
+        if (!(d2 < thr2_up)) continue;
+        const float dist = sqrtf(d2);
+        if (!(dist < thr)) continue;
+        const float3 v2 = ar::xyz(__ldg(svel + j));
+        const float3 f = ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att);
+        if (t < na) fa = ar::add(fa, f);
+        else if (t < nab) fb = ar::add(fb, f);
+        else fc = ar::add(fc, f);
       }
+      lin = ar::add(lin, fa);
+      lin = ar::add(lin, fb);
+      lin = ar::add(lin, fc);
+    }
+  lin = ar::add(lin, ar_pipe::wall_force(S, pos, vel));
+  pforce[g] = make_float4(lin.x, lin.y, lin.z, 0.f);
+}
+
+// ---- BVH broad phase ---------------------------------------------------------------------------
+// Key = scene index above a 30-bit Morton code of the particle's world position normalised to
+// its scene's box (generateMortonCodes, BVHSource/BVHkernels.cu:646-716).  Sorting all scenes
+// together keeps each scene's leaves contiguous, and since no other scene shares its prefix,
+// each scene's leaves are one subtree of the Karras tree; equal codes are tie-broken by the
+// index within the scene, so that subtree is the one the scene alone would get.
+constexpr int kMortonBits = 30;
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restrict__ table,
+                                                         const int* __restrict__ poff, int ns,
+                                                         int nt, uint64_t* __restrict__ keys) {
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
+    const int s = ns == 1 ? 0 : find_range(poff, ns, g);
+    const SceneDev& S = table[s];
+    const float4 r4 = __ldg(S.rel + (g - S.poff));
+    const int b = __float_as_int(r4.w);
+    const float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
+    const float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
+    const float x = (p.x - S.bmin[0]) / (S.bmax[0] - S.bmin[0]);
+    const float y = (p.y - S.bmin[1]) / (S.bmax[1] - S.bmin[1]);
+    const float z = (p.z - S.bmin[2]) / (S.bmax[2] - S.bmin[2]);
+    const uint32_t code = (spread10((uint32_t)fminf(fmaxf(x * 1024.0f, 0.0f), 1023.0f)) << 2) |
+                          (spread10((uint32_t)fminf(fmaxf(y * 1024.0f, 0.0f), 1023.0f)) << 1) |
+                          spread10((uint32_t)fminf(fmaxf(z * 1024.0f, 0.0f), 1023.0f));
+    keys[g] = ((uint64_t)s << kMortonBits) | code;
+  }
+}
+
+// Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
+// state, box = position +/- r, leaf flags and ranges.
+__global__ void __launch_bounds__(256) bvh_leaves_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const uint32_t* __restrict__ svals, float4* __restrict__ spos, float4* __restrict__ svel,
+    float4* __restrict__ bounds, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
+    int32_t* __restrict__ max_r) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+    const int g = (int)__ldg(svals + k);
+    const SceneDev& S = table[ns == 1 ? 0 : find_range(poff, ns, g)];
+    const float4 r4 = __ldg(S.rel + (g - S.poff));
+    const int b = __float_as_int(r4.w);
+    float3 r, p, v;
+    ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
+                    ar::mk3(r4.x, r4.y, r4.z), &r, &p, &v);
+    spos[k] = make_float4(p.x, p.y, p.z, __int_as_float(S.boff + b));
+    svel[k] = make_float4(v.x, v.y, v.z, 0.f);
+    const float rr = S.r;
+    bounds[2 * k] = make_float4(p.x - rr, p.y - rr, p.z - rr, p.x + rr);
+    bounds[2 * k + 1] = make_float4(p.y + rr, p.z + rr, 0.f, 0.f);
+    is_leaf[k] = 1;
+    min_r[k] = k;
+    max_r[k] = k;
+  }
+}
+
+__global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp, int n,
+                                                        uint8_t* __restrict__ is_leaf,
+                                                        int32_t* __restrict__ left,
+                                                        int32_t* __restrict__ right,
+                                                        int32_t* __restrict__ parent,
+                                                        int32_t* __restrict__ min_r,
+                                                        int32_t* __restrict__ max_r) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) parent[n] = -1;
+  if (i >= n - 1) return;
+  ar_lbvh::karras_node(i, n, lcp, is_leaf, left, right, parent, min_r, max_r);
+}
+
+// Each scene's subtree root: the lowest ancestor of its first leaf covering its last leaf.
+__global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
+                                 const int32_t* __restrict__ parent,
+                                 const int32_t* __restrict__ min_r,
+                                 const int32_t* __restrict__ max_r, int32_t* __restrict__ roots) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const int lo = poff[s], hi = poff[s + 1] - 1;
+  if (hi <= lo) {  // zero or one particle: no internal node
+    roots[s] = -1;
+    return;
+  }
+  int node = parent[lo];
+  for (int depth = 0; depth < nt && node >= 0; ++depth) {
+    if (min_r[node] <= lo && max_r[node] >= hi) break;
+    node = parent[node];
+  }
+  roots[s] = node;
+}
+
+__global__ void __launch_bounds__(256) bvh_refit_kernel(int n, const int32_t* __restrict__ left,
+                                                        const int32_t* __restrict__ right,
+                                                        const int32_t* __restrict__ parent,
+                                                        float4* bounds,
+                                                        int* __restrict__ counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  ar_lbvh::refit_from_leaf(i, n, left, right, parent, bounds, counters);
+}
+
+// DEM gather through the scene's subtree in the reference's visit order
+// (Kernels/RB_BVHKernels.cu:145-214), contacts summed in visit order, then the walls.
+__global__ void __launch_bounds__(256) bvh_collide_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const uint32_t* __restrict__ svals, const float4* __restrict__ spos,
+    const float4* __restrict__ svel, const float4* __restrict__ bounds,
+    const uint8_t* __restrict__ is_leaf, const int32_t* __restrict__ left,
+    const int32_t* __restrict__ right, const int32_t* __restrict__ parent,
+    const int32_t* __restrict__ roots, float4* __restrict__ pforce) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  const int g = (int)__ldg(svals + k);
+  const int s = ns == 1 ? 0 : find_range(poff, ns, g);
+  const SceneDev& S = table[s];
+  const float4 p4 = __ldg(spos + k);
+  const float3 pos = ar::xyz(p4);
+  const int body = __float_as_int(p4.w);
+  const float3 vel = ar::xyz(__ldg(svel + k));
+  const float thr = 2.0f * S.r;
+  const float thr2_up = nextafterf(thr * thr, INFINITY);
+  const float kk = S.k, dmp = S.damping, shr = S.shear, att = S.attraction;
+  float3 lin = ar::mk3(0.f, 0.f, 0.f);
+  const int root = __ldg(roots + s);
+  if (root >= nt) {  // an internal node
+    const ar_lbvh::Box qbox = ar_lbvh::load_box(bounds, k);
+    ar_lbvh::walk(root, nt, is_leaf, left, right, parent,
+                  [&](int c) { return c != k && ar_lbvh::overlap(qbox, ar_lbvh::load_box(bounds, c)); },
+                  [&](int c, bool) {
+                    const float4 q4 = __ldg(spos + c);
+                    if (__float_as_int(q4.w) == body) return;
+                    const float3 rp = ar::sub(ar::xyz(q4), pos);
+                    const float d2 = ar::dot(rp, rp);
+                    if (!(d2 < thr2_up)) return;
+                    const float dist = sqrtf(d2);
+                    if (!(dist < thr)) return;
+                    const float3 v2 = ar::xyz(__ldg(svel + c));
+                    lin = ar::add(lin, ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk,
+                                                            dmp, shr, att));
+                  });
+  }
   lin = ar::add(lin, ar_pipe::wall_force(S, pos, vel));
   pforce[g] = make_float4(lin.x, lin.y, lin.z, 0.f);
 }
@@ -239,6 +411,18 @@ struct ar_batch {
   uint64_t total_cells = 0;
   int key_bits = 1, passes = 1, last_bits = 1;
   int host_prev_n = 0;  // particles whose cells are marked in skeys (0 after a clear)
+  // BVH broad phase (allocated only for BVH batches)
+  int broadphase = AR_BROADPHASE_GRID;
+  long cap_bvh = 0;
+  size_t cap_sort64 = 0;
+  uint64_t *keys64 = nullptr, *skeys64 = nullptr;
+  uint8_t* is_leaf = nullptr;
+  int32_t *left = nullptr, *right = nullptr, *parent = nullptr, *min_r = nullptr,
+          *max_r = nullptr, *roots = nullptr;
+  float4* bounds = nullptr;
+  int* counters = nullptr;
+  char* sort64_ws = nullptr;
+  int bvh_key_bits = kMortonBits;
   // graph
   cudaGraphExec_t graph = nullptr;
   cudaStream_t cap_stream = nullptr;
@@ -258,6 +442,17 @@ void free_batch_buffers(ar_batch* B) {
   B->cap_n = B->cap_b = B->cap_s = 0;
   B->cap_cells = 0;
   B->cap_sort = 0;
+  cudaFree(B->keys64); cudaFree(B->skeys64); cudaFree(B->is_leaf); cudaFree(B->left);
+  cudaFree(B->right); cudaFree(B->parent); cudaFree(B->min_r); cudaFree(B->max_r);
+  cudaFree(B->roots); cudaFree(B->bounds); cudaFree(B->counters); cudaFree(B->sort64_ws);
+  B->keys64 = B->skeys64 = nullptr;
+  B->is_leaf = nullptr;
+  B->left = B->right = B->parent = B->min_r = B->max_r = B->roots = nullptr;
+  B->bounds = nullptr;
+  B->counters = nullptr;
+  B->sort64_ws = nullptr;
+  B->cap_bvh = 0;
+  B->cap_sort64 = 0;
 }
 
 void drop_graph(ar_batch* B) {
@@ -281,7 +476,7 @@ uint64_t scene_cells(const ar_scene* s) {
 
 // Clear the cells the last step marked (so the table is all-empty before a layout change).
 void clear_marked(ar_batch* B, cudaStream_t st) {
-  if (B->host_prev_n > 0 && B->cells) {
+  if (B->host_prev_n > 0 && B->cells && B->broadphase == AR_BROADPHASE_GRID) {
     clear_cells_kernel<<<arh::grid_for(B->host_prev_n, 256) > 4096 ? 4096
                                                                    : arh::grid_for(B->host_prev_n, 256),
                          256, 0, st>>>(B->skeys, B->host_prev_n, B->cells);
@@ -322,7 +517,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     boff.push_back((int)bt);
     nt += s->n;
     bt += s->nb;
-    cells += scene_cells(s);
+    if (D.broadphase == AR_BROADPHASE_GRID) cells += scene_cells(s);
   }
   poff.push_back((int)nt);
   boff.push_back((int)bt);
@@ -357,6 +552,33 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     cudaMemsetAsync(B->cells, 0xff, cc * sizeof(uint2), st);
     cudaMemsetAsync(B->d_prev_n, 0, sizeof(int), st);
   }
+  B->broadphase = ns > 0 ? B->scenes[0]->desc.broadphase : AR_BROADPHASE_GRID;
+  if (B->broadphase == AR_BROADPHASE_BVH) {
+    B->bvh_key_bits = kMortonBits + std::max(0, ceil_log2((uint64_t)std::max(ns, 1l)));
+    const int passes64 = (B->bvh_key_bits + 7) / 8;
+    const size_t s64 = ar_sort::layout(std::max(nt, 1l), 8, passes64).total;
+    if (nt > B->cap_bvh || s64 > B->cap_sort64) {
+      cudaStreamSynchronize(st);
+      const long cn = B->cap_n;
+      const size_t m = 2 * (size_t)cn;
+      const size_t csort = ar_sort::layout(cn, 8, passes64).total;
+      cudaFree(B->keys64); cudaFree(B->skeys64); cudaFree(B->is_leaf); cudaFree(B->left);
+      cudaFree(B->right); cudaFree(B->parent); cudaFree(B->min_r); cudaFree(B->max_r);
+      cudaFree(B->roots); cudaFree(B->bounds); cudaFree(B->counters); cudaFree(B->sort64_ws);
+      bool ok = alloc(&B->keys64, cn) && alloc(&B->skeys64, cn) && alloc(&B->is_leaf, m) &&
+                alloc(&B->left, m) && alloc(&B->right, m) && alloc(&B->parent, m) &&
+                alloc(&B->min_r, m) && alloc(&B->max_r, m) && alloc(&B->roots, B->cap_s) &&
+                alloc(&B->bounds, 2 * m) && alloc(&B->counters, cn) &&
+                alloc(&B->sort64_ws, csort);
+      if (!ok) {
+        free_batch_buffers(B);
+        arh::set_error("BVH workspace allocation failed (%ld particles)", nt);
+        return AR_ERR_OOM;
+      }
+      B->cap_bvh = cn;
+      B->cap_sort64 = csort;
+    }
+  }
   if (ns > 0) {
     cudaMemcpyAsync(B->d_table, tab.data(), tab.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(B->d_poff, poff.data(), poff.size() * sizeof(int), cudaMemcpyHostToDevice, st);
@@ -384,7 +606,40 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   auto mark = [&](int i) {
     if (ev) cudaEventRecord(ev[i], st);
   };
+  int bs = 128;
+  if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
   mark(0);
+  if (B->broadphase == AR_BROADPHASE_BVH) {
+    // clear | Morton keys | sort | tree (leaves, Karras nodes, scene roots, refit) | collide |
+    // reduce_integrate
+    cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);
+    mark(1);
+    const unsigned gp = std::min(arh::grid_for(nt, 256), (unsigned)ctx->num_sms * 8);
+    morton_key_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->keys64);
+    mark(2);
+    ar_status s = ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
+                                    B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
+    if (s != AR_OK) return s;
+    mark(3);
+    bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals, B->spos,
+                                          B->svel, B->bounds, B->is_leaf, B->min_r, B->max_r);
+    bvh_build_kernel<<<arh::grid_for(std::max(nt - 1, 1), 256), 256, 0, st>>>(
+        ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
+        B->right, B->parent, B->min_r, B->max_r);
+    bvh_roots_kernel<<<arh::grid_for(ns, 128), 128, 0, st>>>(B->d_poff, ns, nt, B->parent,
+                                                              B->min_r, B->max_r, B->roots);
+    bvh_refit_kernel<<<arh::grid_for(nt, 256), 256, 0, st>>>(nt, B->left, B->right, B->parent,
+                                                              B->bounds, B->counters);
+    mark(4);
+    bvh_collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(
+        B->d_table, B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->bounds, B->is_leaf,
+        B->left, B->right, B->parent, B->roots, B->pforce);
+    mark(5);
+    reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
+        B->d_table, B->d_boff, ns, bt, B->pforce, ctx->d_err);
+    mark(6);
+    return arh::check_launch("step (BVH)");
+  }
   cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
   mark(1);
   unsigned g1 = arh::grid_for(nt, kK1Threads);
@@ -403,8 +658,6 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
                                                         B->svals, B->cells, B->spos, B->svel,
                                                         B->d_prev_n);
   mark(4);
-  int bs = 128;
-  if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
   collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals,
                                                        B->cells, B->spos, B->svel, B->pforce);
   mark(5);
@@ -479,7 +732,8 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
   }
   for (int i = 0; i < n_steps; ++i)
     if (cudaGraphLaunch(B->graph, st) != cudaSuccess) return arh::check_launch("graph launch");
-  B->host_prev_n = (int)B->nt;
+  // only the grid step marks cells (the BVH step never writes the grid keys)
+  if (B->broadphase == AR_BROADPHASE_GRID) B->host_prev_n = (int)B->nt;
   return arh::check_launch("graph launch");
 }
 
@@ -521,13 +775,24 @@ extern "C" {
 
 size_t ar_scene_footprint(const ar_scene_desc* d) {
   if (!d) return 0;
+  const size_t n = (size_t)std::max(d->num_particles, 0), b = (size_t)std::max(d->num_bodies, 0);
+  const size_t per_body = 16 * 6 + 4 + 36 + 4;
+  const size_t shared = 16 /*rel*/ + 16 * 3 /*spos svel pforce*/ + 4 /*svals*/ + 1;
+  if (d->broadphase == AR_BROADPHASE_BVH) {
+    const size_t per_particle = shared + 8 * 2 /*keys64*/ + 12 /*sort tmp*/ +
+                                2 * (1 + 4 * 5) /*tree*/ + 2 * 32 /*boxes*/ + 4 /*counters*/;
+    return n * per_particle + b * per_body + 4096;
+  }
+  const size_t per_particle = shared + 4 * 2 /*keys*/ + 8 /*sort tmp*/;
+  return n * per_particle + b * per_body + (size_t)ar_scene_cells(d) * 8 + 4096;
+}
+
+uint64_t ar_scene_cells(const ar_scene_desc* d) {
+  if (!d || d->broadphase != AR_BROADPHASE_GRID) return 0;
   float o[3], c[3];
   uint32_t g[3];
   scene_grid(*d, o, c, g);
-  const size_t n = (size_t)std::max(d->num_particles, 0), b = (size_t)std::max(d->num_bodies, 0);
-  const size_t per_particle = 16 /*rel*/ + 4 * 3 /*keys*/ + 16 * 3 /*spos svel pforce*/ + 8 /*sort tmp*/ + 1;
-  const size_t per_body = 16 * 6 + 4 + 36 + 4;
-  return n * per_particle + b * per_body + (size_t)g[0] * g[1] * g[2] * 8 + 4096;
+  return (uint64_t)g[0] * g[1] * g[2];
 }
 
 ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene_init* init,
@@ -545,8 +810,8 @@ ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene
   }
   for (int a = 0; a < 3; ++a)
     if (D.grid_log2[a] < 0 || D.grid_log2[a] > 20) return AR_ERR_INVALID_ARG;
-  if (D.block_size != 0 && (D.block_size < 32 || D.block_size > 1024 || D.block_size % 32)) {
-    arh::set_error("ar_scene_create: block_size must be a multiple of 32 in [32, 1024]");
+  if (D.block_size != 0 && (D.block_size < 32 || D.block_size > 256 || D.block_size % 32)) {
+    arh::set_error("ar_scene_create: block_size must be a multiple of 32 in [32, 256]");
     return AR_ERR_INVALID_ARG;
   }
   if (!init->body_pos4 || !init->body_quat4 || !init->body_vel4 || !init->body_angvel4 ||
@@ -665,10 +930,6 @@ static ar_status ensure_solo(ar_scene* s) {
 
 ar_status ar_step(ar_ctx* ctx, ar_scene* s, int n_steps, int use_graph, ar_stream_t stream) {
   if (!ctx || !s || n_steps < 0) return AR_ERR_INVALID_ARG;
-  if (s->desc.broadphase != AR_BROADPHASE_GRID) {
-    arh::set_error("ar_step: the fused step implements the grid broad phase");
-    return AR_ERR_UNSUPPORTED;
-  }
   ar_status st = ensure_solo(s);
   if (st != AR_OK) return st;
   return batch_step(ctx, s->solo, n_steps, use_graph, arh::stream(stream));
@@ -717,15 +978,22 @@ ar_status ar_scene_particle_forces(ar_scene* s, float* p_force4, float* p_torque
 ar_status ar_scene_step_view(ar_scene* s, ar_step_view* v) {
   if (!s || !v || !s->solo) return AR_ERR_INVALID_ARG;
   ar_batch* B = s->solo;
+  const bool bvh = B->broadphase == AR_BROADPHASE_BVH;
   v->num_particles = (int)B->nt;
-  v->num_cells = B->total_cells;
-  v->key_bits = B->key_bits;
-  v->sorted_keys = B->skeys;
+  v->num_cells = bvh ? 0 : B->total_cells;
+  v->key_bits = bvh ? B->bvh_key_bits : B->key_bits;
+  v->sorted_keys = bvh ? (uint32_t*)B->skeys64 : B->skeys;
   v->sorted_idx = B->svals;
   v->sorted_pos4 = (float*)B->spos;
   v->sorted_vel4 = (float*)B->svel;
   v->particle_force4 = (float*)B->pforce;
-  v->cells2 = (uint32_t*)B->cells;
+  v->cells2 = bvh ? nullptr : (uint32_t*)B->cells;
+  v->key_bytes = bvh ? 8 : 4;
+  v->broadphase = B->broadphase;
+  v->tree_left = bvh ? B->left : nullptr;
+  v->tree_right = bvh ? B->right : nullptr;
+  v->tree_parent = bvh ? B->parent : nullptr;
+  v->tree_bounds8 = bvh ? (float*)B->bounds : nullptr;
   return AR_OK;
 }
 
@@ -751,9 +1019,9 @@ ar_status ar_batch_set_scenes(ar_batch* B, ar_scene* const* scenes, int n_scenes
   if (!B || n_scenes < 0 || (n_scenes > 0 && !scenes)) return AR_ERR_INVALID_ARG;
   for (int i = 0; i < n_scenes; ++i) {
     if (!scenes[i]) return AR_ERR_INVALID_ARG;
-    if (scenes[i]->desc.broadphase != AR_BROADPHASE_GRID) {
-      arh::set_error("ar_batch_set_scenes: the fused step implements the grid broad phase");
-      return AR_ERR_UNSUPPORTED;
+    if (scenes[i]->desc.broadphase != scenes[0]->desc.broadphase) {
+      arh::set_error("ar_batch_set_scenes: all scenes of a batch use one broad phase");
+      return AR_ERR_INVALID_ARG;
     }
   }
   B->scenes.assign(scenes, scenes + n_scenes);
@@ -769,6 +1037,8 @@ ar_status ar_batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph,
 
 int ar_batch_launches_per_step(ar_batch* B) {
   if (!B) return 0;
+  if (B->broadphase == AR_BROADPHASE_BVH)  // memset, keys, sort, 4 tree kernels, collide, reduce
+    return 1 + 1 + ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 2;
   return 1 /*memset*/ + 1 /*K1*/ + ar_sort::launches(0, B->key_bits, true) + 3;
 }
 

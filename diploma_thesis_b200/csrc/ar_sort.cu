@@ -89,7 +89,7 @@ struct PassSmem {
 };
 
 template <class K>
-__global__ void __launch_bounds__(kThreads) onesweep_kernel(
+__global__ void __launch_bounds__(kThreads, sizeof(K) == 4 ? 4 : 2) onesweep_kernel(
     const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     const uint32_t* __restrict__ digit_base, uint32_t* __restrict__ status,
@@ -105,42 +105,37 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
   const uint32_t tile = sm.tile_id;
   const long tile_base = (long)tile * kTile;
 
-  // load (coalesced: item j of lane l in warp w is element base + w*kItems*32 + j*32 + l)
+  // load keys (coalesced: item j of lane l in warp w is element base + w*kItems*32 + j*32 + l);
+  // values are read only when the items are staged, and digits are recomputed from the keys,
+  // which keeps the register count (and so the occupancy) down
   K key[kItems];
-  uint32_t val[kItems];
-  uint32_t dig[kItems];
   uint32_t rank[kItems];
   const long wbase = tile_base + (long)warp * kItems * 32;
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
     long g = wbase + j * 32 + lane;
-    if (g < n) {
-      key[j] = keys_in[g];
-      val[j] = vals_in ? vals_in[g] : (uint32_t)g;
-      dig[j] = digit_of(key[j], shift, mask);
-    } else {
-      key[j] = (K)~(K)0;
-      val[j] = 0;
-      dig[j] = kRadix - 1;  // after every valid item of the tile; never written
-    }
+    // invalid items take digit kRadix-1 (after every valid item of the tile; never written)
+    key[j] = g < n ? keys_in[g] : (K)~(K)0;
   }
 
   // stable warp multi-split: peers = lanes holding the same digit
   const uint32_t lt = (1u << lane) - 1;
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
+    const long g = wbase + j * 32 + lane;
+    const uint32_t dj = g < n ? digit_of(key[j], shift, mask) : kRadix - 1;
     uint32_t peers = 0xffffffffu;
     for (int b = 0; b < 8; ++b) {
-      uint32_t bit = (dig[j] >> b) & 1u;
+      uint32_t bit = (dj >> b) & 1u;
       uint32_t m = __ballot_sync(0xffffffffu, bit);
       peers &= bit ? m : ~m;
     }
     uint32_t before = __popc(peers & lt);
     int leader = __ffs(peers) - 1;
     __syncwarp();
-    uint32_t old = sm.warp_hist[warp][dig[j]];
+    uint32_t old = sm.warp_hist[warp][dj];
     __syncwarp();
-    if (lane == leader) sm.warp_hist[warp][dig[j]] = old + __popc(peers);
+    if (lane == leader) sm.warp_hist[warp][dj] = old + __popc(peers);
     rank[j] = old + before;
   }
   __syncthreads();
@@ -208,9 +203,10 @@ __global__ void __launch_bounds__(kThreads) onesweep_kernel(
   for (int j = 0; j < kItems; ++j) {
     long g = wbase + j * 32 + lane;
     if (g < n) {
-      uint32_t pos = sm.digit_start[dig[j]] + sm.warp_hist[warp][dig[j]] + rank[j];
+      const uint32_t dj = digit_of(key[j], shift, mask);
+      uint32_t pos = sm.digit_start[dj] + sm.warp_hist[warp][dj] + rank[j];
       sm.keys[pos] = key[j];
-      sm.vals[pos] = val[j];
+      sm.vals[pos] = vals_in ? vals_in[g] : (uint32_t)g;
     }
   }
   __syncthreads();
@@ -405,6 +401,14 @@ ar_status sort_u32(ar_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in
   if (n == 0) return AR_OK;
   return sort_impl<uint32_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
                              st, ws, ws_bytes, external_hist);
+}
+
+ar_status sort_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in,
+                   uint64_t* keys_out, uint32_t* vals_out, int n, int begin_bit, int end_bit,
+                   cudaStream_t st, void* ws, size_t ws_bytes) {
+  if (n == 0) return AR_OK;
+  return sort_impl<uint64_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
+                             st, ws, ws_bytes, false);
 }
 
 size_t clear_bytes(long n, int passes) {

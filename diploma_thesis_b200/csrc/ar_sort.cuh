@@ -31,6 +31,11 @@ ar_status sort_u32(ar_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in
                    uint32_t* keys_out, uint32_t* vals_out, int n, int begin_bit, int end_bit,
                    cudaStream_t st, void* ws, size_t ws_bytes, bool external_hist = false);
 
+// The same for u64 keys (histogram computed inside; workspace layout(n, 8, passes)).
+ar_status sort_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in,
+                   uint64_t* keys_out, uint32_t* vals_out, int n, int begin_bit, int end_bit,
+                   cudaStream_t st, void* ws, size_t ws_bytes);
+
 // Bytes at the head of the workspace that must be zero before a sort whose histogram is
 // accumulated externally (histograms, tile counters, look-back status).
 size_t clear_bytes(long n, int passes);
@@ -43,6 +48,20 @@ __device__ __forceinline__ void hist_count(uint32_t (*s_hist)[256], uint32_t key
   for (int p = 0; p < passes; ++p) {
     uint32_t mask = (p == passes - 1) ? ((1u << last_bits) - 1) : 0xffu;
     atomicAdd(&s_hist[p][(key >> (begin_bit + 8 * p)) & mask], 1u);
+  }
+}
+// hist_count with one shared-memory atomic per distinct digit per warp (the lanes holding the
+// same digit are counted by their lowest lane): particles of a body are adjacent in the
+// original order and mostly share digits, so this removes most same-address contention.
+__device__ __forceinline__ void hist_count_warp(uint32_t (*s_hist)[256], uint32_t key,
+                                                int begin_bit, int passes, int last_bits) {
+  const uint32_t active = __activemask();
+  const int lane = threadIdx.x & 31;
+  for (int p = 0; p < passes; ++p) {
+    const uint32_t mask = (p == passes - 1) ? ((1u << last_bits) - 1) : 0xffu;
+    const uint32_t d = (key >> (begin_bit + 8 * p)) & mask;
+    const uint32_t peers = __match_any_sync(active, d);
+    if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[p][d], (uint32_t)__popc(peers));
   }
 }
 // Block histogram -> workspace head (ws + 0 holds uint32 [kMaxPasses][256]).

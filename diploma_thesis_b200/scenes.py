@@ -126,14 +126,13 @@ def _assemble(shapes: list[np.ndarray], centres: np.ndarray, quats: np.ndarray,
     offsets[1:] = np.cumsum(counts)
     rel = np.zeros((int(offsets[-1]), 4), np.float32)
     rel[:, :3] = np.concatenate(shapes).astype(np.float32)
-    # inverse inertia per distinct shape
+    # inverse inertia per distinct shape (shapes are shared objects)
     inv = np.zeros((nb, 9), np.float32)
-    cache: dict[bytes, np.ndarray] = {}
+    cache: dict[int, np.ndarray] = {}
     for b, s in enumerate(shapes):
-        key = s.astype(np.float32).tobytes()
-        if key not in cache:
-            cache[key] = inverse_inertia(s.astype(np.float32).astype(np.float64))
-        inv[b] = cache[key]
+        if id(s) not in cache:
+            cache[id(s)] = inverse_inertia(s.astype(np.float32).astype(np.float64))
+        inv[b] = cache[id(s)]
     pos = np.zeros((nb, 4), np.float32)
     pos[:, :3] = centres
     vel = np.zeros((nb, 4), np.float32)
@@ -265,20 +264,19 @@ def cube_scene(seed: int, num_particles: int, box_side: float, r: float = 1.0 / 
     per_axis = max(1, int(side / slot))
     layers = -(-nb // (per_axis * per_axis))
     height = max(side, (layers + 1) * slot)
-    centres = []
-    for b in range(nb):
-        layer, rem = divmod(b, per_axis * per_axis)
-        i, j = divmod(rem, per_axis)
-        c = np.array([(i + 0.5) * side / per_axis, (layer + 0.5) * slot, (j + 0.5) * side / per_axis])
-        c += rng.uniform(-0.1, 0.1, 3) * slot
-        centres.append(c)
+    b = np.arange(nb)
+    layer, rem = np.divmod(b, per_axis * per_axis)
+    i, j = np.divmod(rem, per_axis)
+    centres = np.stack([(i + 0.5) * side / per_axis, (layer + 0.5) * slot,
+                        (j + 0.5) * side / per_axis], -1)
+    centres = centres + rng.uniform(-0.1, 0.1, (nb, 3)) * slot
     quats = random_quaternions(rng, nb)
     if mix_rods:  # rods stay horizontal so neighbouring slots never overlap
         yaw = rng.uniform(0, 2 * np.pi, nb)
         rq = np.stack([np.zeros(nb), np.sin(yaw / 2), np.zeros(nb), np.cos(yaw / 2)], -1)
         quats = np.where(kinds[:, None], rq, quats)
     shapes = [rod if k else cube for k in kinds]
-    return _assemble(shapes, np.array(centres), quats, rng.normal(0.0, 0.1, (nb, 3)), r,
+    return _assemble(shapes, centres, quats, rng.normal(0.0, 0.1, (nb, 3)), r,
                      (0, 0, 0), (side, height, side), name=f"{nb} bodies x 27")
 
 
@@ -299,3 +297,25 @@ def config4_request(rng: np.random.Generator) -> tuple[Scene, int]:
     side = float(rng.uniform(0.5, 2.0))
     k = int(rng.integers(10, 501))
     return cube_scene(int(rng.integers(1 << 31)), n, side, mix_rods=True), k
+
+
+# ---- LBVH point sets ------------------------------------------------------------------------
+def lbvh_points(n: int, dist: str, seed: int = 0) -> np.ndarray:
+    """[n,4] float32 points (w = 0) for the LBVH microbenchmark: 'uniform' in [0,1]^3, or
+    'gmm', a 16-component Gaussian mixture (sigma 0.02, means uniform in [0.1,0.9]^3, clipped
+    to [0,1]^3) in which 5 % of the points are replaced by exact copies of other points, so
+    that equal Morton codes exercise the index tie-break."""
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, 4), np.float32)
+    if dist == "uniform":
+        out[:, :3] = rng.random((n, 3), dtype=np.float32)
+    elif dist == "gmm":
+        means = rng.uniform(0.1, 0.9, (16, 3))
+        comp = rng.integers(0, 16, n)
+        p = means[comp] + rng.normal(0.0, 0.02, (n, 3))
+        out[:, :3] = np.clip(p, 0.0, 1.0)
+        dup = rng.choice(n, n // 20, replace=False)
+        out[dup] = out[rng.integers(0, n, len(dup))]
+    else:
+        raise ValueError(f"unknown point distribution {dist!r}")
+    return out

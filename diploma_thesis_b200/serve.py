@@ -5,7 +5,8 @@ resident on the device and, every tick:
 
   1. admits waiting requests in arrival order while their footprint fits the HBM budget
      (``ar_scene_footprint``, which counts the scene's state and its share of the step
-     workspace) -- admission is never blocked by a request that arrived later;
+     workspace) and the batch stays within its particle and cell limits -- admission is
+     never blocked by a request that arrived later;
   2. advances all resident scenes together as one batch (``ar_batch_step``: one launch per
      stage, CUDA graph) by ``min(tick_steps, smallest remaining K)`` steps, so no scene is
      stepped past its K;
@@ -21,6 +22,8 @@ arrivals are scheduled against the same clock.
 """
 from __future__ import annotations
 
+import contextlib
+import ctypes as C
 import heapq
 import time
 from dataclasses import dataclass, field
@@ -29,7 +32,7 @@ import numpy as np
 import torch
 
 from . import api
-from ._lib import lib
+from ._lib import AR_MAX_BATCH_CELLS, AR_MAX_BATCH_PARTICLES, lib
 from .scenes import Scene
 
 
@@ -71,32 +74,51 @@ class ServerStats:
 
 
 class Server:
-    def __init__(self, ctx: api.Context, hbm_budget_bytes: float, tick_steps: int = 10,
-                 keep_results: bool = False):
+    """Continuous-batching request loop.
+
+    Admission needs the request's footprint to fit the HBM budget and the resident batch to
+    stay within the library's batch limits (AR_MAX_BATCH_PARTICLES particles and
+    AR_MAX_BATCH_CELLS grid cells) and the optional ``max_batch_particles`` cap.
+    ``scene_factory(ctx, scene)`` and ``batch`` default to the device classes; they are
+    parameters so that the admission and tick logic can be driven by host-only stand-ins."""
+
+    def __init__(self, ctx, hbm_budget_bytes: float, tick_steps: int = 10,
+                 keep_results: bool = False, max_batch_particles: int | None = None,
+                 broadphase: str = "grid", scene_factory=None, batch=None, stream=None):
         self.ctx = ctx
         self.budget = float(hbm_budget_bytes)
         self.tick_steps = int(tick_steps)
         self.keep_results = keep_results
-        self.batch = api.Batch(ctx)
-        self.stream = torch.cuda.Stream()
+        self.max_particles = min(int(max_batch_particles or AR_MAX_BATCH_PARTICLES),
+                                 AR_MAX_BATCH_PARTICLES)
+        self.broadphase = broadphase
+        self.scene_factory = scene_factory or (
+            lambda c, sc: api.GpuScene(c, sc, broadphase=self.broadphase))
+        self.batch = batch if batch is not None else api.Batch(ctx)
+        self.stream = stream if stream is not None else torch.cuda.Stream()
 
-    @staticmethod
-    def footprint(scene: Scene) -> int:
-        import ctypes as C
-        d = api.make_desc(scene)
-        return int(lib.ar_scene_footprint(C.byref(d)))
+    def cost(self, scene: Scene) -> tuple[int, int]:
+        """(device bytes, grid cells) a scene holds while resident."""
+        d = api.make_desc(scene, api.broadphase_code(self.broadphase))
+        return int(lib.ar_scene_footprint(C.byref(d))), int(lib.ar_scene_cells(C.byref(d)))
+
+    def _fits(self, used, need) -> bool:
+        return (used[0] + need[0] <= self.budget and used[1] + need[1] <= AR_MAX_BATCH_CELLS
+                and used[2] + need[2] <= self.max_particles)
 
     def run(self, requests: list[Request], time_limit: float | None = None) -> ServerStats:
         pending = list(requests)
         heapq.heapify(pending)
         waiting: list[Request] = []
-        active: list[tuple[Request, api.GpuScene, int, int]] = []  # req, scene, remaining, bytes
-        used = 0
+        active: list[list] = []  # [req, scene, remaining, (bytes, cells, particles)]
+        used = [0, 0, 0]
         done: list[Request] = []
         scene_steps = particle_steps = 0
         peak_res = peak_bytes = ticks = 0
         t0 = time.perf_counter()
-        with torch.cuda.stream(self.stream):
+        stream_ctx = torch.cuda.stream(self.stream) if isinstance(self.stream, torch.cuda.Stream) \
+            else contextlib.nullcontext()
+        with stream_ctx:
             while pending or waiting or active:
                 now = time.perf_counter() - t0
                 if time_limit is not None and now > time_limit and not active:
@@ -105,14 +127,18 @@ class Server:
                     waiting.append(heapq.heappop(pending))
                 changed = False
                 while waiting and (time_limit is None or now <= time_limit):
-                    need = self.footprint(waiting[0].scene)
-                    if used + need > self.budget and active:
-                        break  # wait for memory to free up
+                    nbytes, cells = self.cost(waiting[0].scene)
+                    need = (nbytes, cells, waiting[0].scene.num_particles)
+                    if not self._fits(used, need):
+                        if active:
+                            break  # wait for resident scenes to retire
+                        if need[1] > AR_MAX_BATCH_CELLS or need[2] > self.max_particles:
+                            raise ValueError(f"request {waiting[0].rid} can never be admitted")
                     req = waiting.pop(0)
-                    gs = api.GpuScene(self.ctx, req.scene)
+                    gs = self.scene_factory(self.ctx, req.scene)
                     req.admitted = time.perf_counter() - t0
-                    active.append((req, gs, req.steps, need))
-                    used += need
+                    active.append([req, gs, req.steps, need])
+                    used = [u + x for u, x in zip(used, need)]
                     changed = True
                 if not active:
                     if pending:  # idle until the next arrival
@@ -124,30 +150,26 @@ class Server:
                 self.batch.step(k, use_graph=True, stream=self.stream)
                 ticks += 1
                 peak_res = max(peak_res, len(active))
-                peak_bytes = max(peak_bytes, used)
-                still = []
+                peak_bytes = max(peak_bytes, used[0])
                 finished = []
-                for req, gs, rem, nbytes in active:
+                for a in active:
                     scene_steps += k
-                    particle_steps += k * gs.num_particles
-                    if rem - k <= 0:
-                        finished.append((req, gs, nbytes))
-                    else:
-                        still.append((req, gs, rem - k, nbytes))
+                    particle_steps += k * a[0].scene.num_particles
+                    a[2] -= k
+                    if a[2] <= 0:
+                        finished.append(a)
                 if finished:
                     self.stream.synchronize()
                     tdone = time.perf_counter() - t0
-                    for req, gs, nbytes in finished:
+                    for req, gs, _, need in finished:
                         req.done = tdone
                         if self.keep_results:
                             req.result = gs.download()
                         gs.close()
-                        used -= nbytes
+                        used = [u - x for u, x in zip(used, need)]
                         done.append(req)
-                    active = still
+                    active = [a for a in active if a[2] > 0]
                     self.batch.set_scenes([a[1] for a in active])
-                else:
-                    active = still
             self.stream.synchronize()
         wall = time.perf_counter() - t0
         self.ctx.check(self.stream)

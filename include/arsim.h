@@ -391,7 +391,8 @@ typedef struct ar_scene_desc {
   int broadphase;        /* AR_BROADPHASE_GRID or AR_BROADPHASE_BVH */
   float cell_size;       /* grid cell edge; 0 -> 2r */
   int grid_log2[3];      /* log2 grid cells per axis (wrapped); 0 -> derived from the box */
-  int block_size;        /* threads per CTA for the per-particle kernels; 0 -> 128 */
+  int block_size;        /* threads per CTA for the collision kernel: 0 -> 128, else a
+                            multiple of 32 in [32, 256] */
 } ar_scene_desc;
 
 typedef struct ar_scene ar_scene;
@@ -418,6 +419,12 @@ AR_API ar_status ar_scene_destroy(ar_scene* scene);
 /* Device bytes a scene with this description keeps resident (state + its share of the
  * step workspace); used for HBM-budget admission. */
 AR_API size_t ar_scene_footprint(const ar_scene_desc* desc);
+/* Cells of the grid a scene with this description gets (0 for the BVH broad phase).  A
+ * batch holds fewer than AR_MAX_BATCH_CELLS cells and AR_MAX_BATCH_PARTICLES particles in
+ * total (cell keys and particle indices are 32-bit); ar_batch_step rejects larger batches. */
+#define AR_MAX_BATCH_CELLS 4294967295ull
+#define AR_MAX_BATCH_PARTICLES 1073741823
+AR_API uint64_t ar_scene_cells(const ar_scene_desc* desc);
 /* Copy body state to host arrays (any may be NULL); synchronises the stream. */
 AR_API ar_status ar_scene_download(ar_scene* scene, float* h_body_pos4, float* h_body_quat4,
                                    float* h_body_vel4, float* h_body_angvel4,
@@ -443,20 +450,29 @@ AR_API ar_status ar_scene_grid_info(ar_scene* scene, float origin[3], float cell
                                     uint32_t dims[3]);
 
 /* Device pointers into the workspace of the scene's last ar_step (for parity tests and
- * consumers that want the sorted state): the sorted cell keys and the particle index of each
+ * consumers that want the sorted state): the sorted keys and the particle index of each
  * sorted slot, sorted positions (w = body index, int bits) and velocities, the per-particle
- * DEM + wall force at the original index, and the cell table as (start, end) pairs
- * (start = 0xffffffff for an empty cell). */
+ * DEM + wall force at the original index, and for the grid broad phase the cell table as
+ * (start, end) pairs (start = 0xffffffff for an empty cell).  Grid keys are uint32 cell keys
+ * (key_bytes 4); BVH keys are uint64 Morton codes (key_bytes 8), and the BVH view adds the
+ * tree (leaf i at i, internal node i at N + i, root N; tree_bounds8: 8 floats per node,
+ * min.xyz, max.xyz, 0, 0).  Tree pointers are NULL for the grid, cells2 NULL for the BVH. */
 typedef struct ar_step_view {
   int num_particles;
   uint64_t num_cells;
   int key_bits;
-  uint32_t* sorted_keys;
+  uint32_t* sorted_keys; /* uint64_t* when key_bytes == 8 */
   uint32_t* sorted_idx;
   float* sorted_pos4;
   float* sorted_vel4;
   float* particle_force4;
   uint32_t* cells2;
+  int key_bytes;
+  int broadphase;
+  int32_t* tree_left;
+  int32_t* tree_right;
+  int32_t* tree_parent;
+  float* tree_bounds8;
 } ar_step_view;
 AR_API ar_status ar_scene_step_view(ar_scene* scene, ar_step_view* out);
 

@@ -268,9 +268,13 @@ def _scene_arrays(scene):
     return rel, s15
 
 
-def step(scene, steps: int = 1, grid=None, state: dict | None = None) -> dict:
+def step(scene, steps: int = 1, grid=None, state: dict | None = None,
+         broadphase: str = "grid") -> dict:
     """Float32 restatement of ar_step (operation for operation).  Returns the new body state
-    and, for the last step, the sorted keys / indices, per-particle forces and body sums."""
+    and, for the last step, the sorted keys / indices, per-particle forces and body sums.
+    broadphase 'bvh' restates the BVH step (sorted keys are then the 30-bit Morton codes)."""
+    if broadphase == "bvh":
+        return _step_bvh(scene, steps, state)
     origin, cell, dims = grid if grid is not None else scene_grid(scene)
     rel, s15 = _scene_arrays(scene)
     st = state or {"pos": scene.body_pos, "quat": scene.body_quat, "vel": scene.body_vel,
@@ -286,6 +290,28 @@ def step(scene, steps: int = 1, grid=None, state: dict | None = None) -> dict:
                     _p(_f32(scene.body_inv_inertia)), _p(_i32(scene.body_offsets)), _p(rel),
                     steps, _p(out["skeys"]), _p(out["sidx"]), _p(out["pforce"]),
                     _p(out["bforce"]), _p(out["btorque"]))
+    st.update(out)
+    st["finite"] = bool(ok)
+    return st
+
+
+_L.or_step_bvh.restype = C.c_int
+
+
+def _step_bvh(scene, steps: int, state: dict | None) -> dict:
+    rel, s15 = _scene_arrays(scene)
+    st = state or {"pos": scene.body_pos, "quat": scene.body_quat, "vel": scene.body_vel,
+                   "angvel": scene.body_angvel}
+    st = {k: _f32(v).copy() for k, v in st.items()}
+    n, nb = scene.num_particles, scene.num_bodies
+    out = {"skeys": np.zeros(n, np.uint64), "sidx": np.zeros(n, np.uint32),
+           "pforce": np.zeros((n, 4), np.float32), "bforce": np.zeros((nb, 4), np.float32),
+           "btorque": np.zeros((nb, 4), np.float32)}
+    ok = _L.or_step_bvh(_p(s15), nb, n, _p(st["pos"]), _p(st["quat"]), _p(st["vel"]),
+                        _p(st["angvel"]), _p(_f32(scene.body_mass)),
+                        _p(_f32(scene.body_inv_inertia)), _p(_i32(scene.body_offsets)), _p(rel),
+                        steps, _p(out["skeys"]), _p(out["sidx"]), _p(out["pforce"]),
+                        _p(out["bforce"]), _p(out["btorque"]))
     st.update(out)
     st["finite"] = bool(ok)
     return st

@@ -822,6 +822,34 @@ static long lower_bound_u32(const uint32_t* a, long n, uint32_t v) {
   return lo;
 }
 
+/* Per body: fixed-order sums of F and r x F (warp_sum), then integrate_body.  0 on a
+ * non-finite state. */
+static int bodies_step(const scene_t* S, int nb, const float* pf, float* bpos4, float* bquat4,
+                       float* bvel4, float* bang4, const float* mass, const float* ib9,
+                       const int* off, const float* rel4, float* bforce4_out,
+                       float* btorque4_out) {
+  int ok = 1;
+  for (int b = 0; b < nb; ++b) {
+    int s0 = off[b], s1 = off[b + 1];
+    v3* fv = (v3*)malloc(sizeof(v3) * (s1 - s0 + 1));
+    v3* tv = (v3*)malloc(sizeof(v3) * (s1 - s0 + 1));
+    v4 q = ld4(bquat4 + 4l * b);
+    for (int i = s0; i < s1; ++i) {
+      v3 f = xyz(pf + 4l * i);
+      fv[i - s0] = f;
+      tv[i - s0] = cross(quat_rotate(q, xyz(rel4 + 4l * i)), f);
+    }
+    v3 F = warp_sum(fv, s1 - s0), T = warp_sum(tv, s1 - s0);
+    free(fv); free(tv);
+    if (!integrate_body(S, F, T, mass[b], ib9 + 9l * b, bpos4 + 4l * b, bquat4 + 4l * b,
+                        bvel4 + 4l * b, bang4 + 4l * b))
+      ok = 0;
+    if (bforce4_out) st4(bforce4_out + 4l * b, F.x, F.y, F.z, 0.f);
+    if (btorque4_out) st4(btorque4_out + 4l * b, T.x, T.y, T.z, 0.f);
+  }
+  return ok;
+}
+
 int or_step(const float* s15, const float* grid6, const uint32_t* dims3, int nb, int n,
             float* bpos4, float* bquat4, float* bvel4, float* bang4, const float* mass,
             const float* ib9, const int* off, const float* rel4, int steps, uint32_t* skeys_out,
@@ -883,29 +911,140 @@ int or_step(const float* s15, const float* grid6, const uint32_t* dims3, int nb,
       lin = add(lin, wall_force(&S, pos, vel));
       st4(pf + 4l * sv[k], lin.x, lin.y, lin.z, 0.f);
     }
-    for (int b = 0; b < nb; ++b) {
-      int s0 = off[b], s1 = off[b + 1];
-      v3* fv = (v3*)malloc(sizeof(v3) * (s1 - s0 + 1));
-      v3* tv = (v3*)malloc(sizeof(v3) * (s1 - s0 + 1));
-      v4 q = ld4(bquat4 + 4l * b);
-      for (int i = s0; i < s1; ++i) {
-        v3 f = xyz(pf + 4l * i);
-        fv[i - s0] = f;
-        tv[i - s0] = cross(quat_rotate(q, xyz(rel4 + 4l * i)), f);
-      }
-      v3 F = warp_sum(fv, s1 - s0), T = warp_sum(tv, s1 - s0);
-      free(fv); free(tv);
-      if (!integrate_body(&S, F, T, mass[b], ib9 + 9l * b, bpos4 + 4l * b, bquat4 + 4l * b,
-                          bvel4 + 4l * b, bang4 + 4l * b))
-        ok = 0;
-      if (bforce4_out) st4(bforce4_out + 4l * b, F.x, F.y, F.z, 0.f);
-      if (btorque4_out) st4(btorque4_out + 4l * b, T.x, T.y, T.z, 0.f);
-    }
+    if (!bodies_step(&S, nb, pf, bpos4, bquat4, bvel4, bang4, mass, ib9, off, rel4, bforce4_out,
+                     btorque4_out))
+      ok = 0;
   }
   if (skeys_out) memcpy(skeys_out, sk, 4l * n);
   if (sidx_out) memcpy(sidx_out, sv, 4l * n);
   if (pforce4_out) memcpy(pforce4_out, pf, 16l * n);
   free(keys); free(sk); free(sv); free(sp); free(svl); free(pf);
+  return ok;
+}
+
+/* ====================================================================================
+ * Fused PHYSICAL step with the BVH broad phase (the product's ar_step on a BVH scene):
+ *   30-bit Morton code of each particle's world position normalised to the scene box
+ *   (morton3D / expandBits, BVHSource/BVHkernels.cu:646-716) -> stable sort -> Karras tree
+ *   with the index tie-break (or_radix_tree_u64) -> leaf boxes p +/- r -> refit -> per particle
+ *   the explicit-stack traversal of collideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:100-244),
+ *   contacts summed in visit order, then the walls -> the same body sums and integration as
+ *   or_step.  s15 as in or_step.  Outputs (optional): sorted codes and indices, per-particle
+ *   force, per-body sums.
+ * ==================================================================================== */
+static uint32_t morton_box(v3 p, const float* lo, const float* hi) {
+  uint32_t q[3];
+  q[0] = quantise((p.x - lo[0]) / (hi[0] - lo[0]), 1024.0f, 1023.0f);
+  q[1] = quantise((p.y - lo[1]) / (hi[1] - lo[1]), 1024.0f, 1023.0f);
+  q[2] = quantise((p.z - lo[2]) / (hi[2] - lo[2]), 1024.0f, 1023.0f);
+  uint32_t c = 0;
+  for (int b = 0; b < 10; ++b)
+    c |= (((q[0] >> b) & 1u) << (3 * b + 2)) | (((q[1] >> b) & 1u) << (3 * b + 1)) |
+         (((q[2] >> b) & 1u) << (3 * b));
+  return c;
+}
+int or_step_bvh(const float* s15, int nb, int n, float* bpos4, float* bquat4, float* bvel4,
+                float* bang4, const float* mass, const float* ib9, const int* off,
+                const float* rel4, int steps, uint64_t* skeys_out, uint32_t* sidx_out,
+                float* pforce4_out, float* bforce4_out, float* btorque4_out) {
+  scene_t S;
+  const float g6[6] = {0, 0, 0, 1, 1, 1};
+  const uint32_t d3[3] = {1, 1, 1};
+  scene_from(s15, g6, d3, &S);
+  uint64_t* keys = (uint64_t*)malloc(8l * n + 8);
+  uint64_t* sk = (uint64_t*)malloc(8l * n + 8);
+  uint32_t* sv = (uint32_t*)malloc(4l * n + 4);
+  float* sp = (float*)malloc(16l * n + 16);
+  float* svl = (float*)malloc(16l * n + 16);
+  float* pf = (float*)malloc(16l * n + 16);
+  const long m = 2l * n + 2;
+  uint8_t* is_leaf = (uint8_t*)calloc(m, 1);
+  int* left = (int*)calloc(m, sizeof(int));
+  int* right = (int*)calloc(m, sizeof(int));
+  int* parent = (int*)calloc(m, sizeof(int));
+  int* min_r = (int*)calloc(m, sizeof(int));
+  int* max_r = (int*)calloc(m, sizeof(int));
+  float* bounds = (float*)calloc(8 * m, sizeof(float));
+  int ok = 1;
+  for (int step = 0; step < steps; ++step) {
+    for (int i = 0; i < n; ++i) {
+      int b = f2i(rel4[4l * i + 3]);
+      v3 r = quat_rotate(ld4(bquat4 + 4l * b), xyz(rel4 + 4l * i));
+      v3 p = add(xyz(bpos4 + 4l * b), r);
+      keys[i] = morton_box(p, S.bmin, S.bmax);
+    }
+    or_sort_pairs_u64(keys, NULL, sk, sv, n, 0, 30);
+    for (int k = 0; k < n; ++k) {
+      int g = (int)sv[k];
+      int b = f2i(rel4[4l * g + 3]);
+      v4 q = ld4(bquat4 + 4l * b);
+      v3 r = quat_rotate(q, xyz(rel4 + 4l * g));
+      v3 p = add(xyz(bpos4 + 4l * b), r);
+      v3 v = add(xyz(bvel4 + 4l * b), cross(xyz(bang4 + 4l * b), r));
+      st4(sp + 4l * k, p.x, p.y, p.z, i2f(b));
+      st4(svl + 4l * k, v.x, v.y, v.z, 0.f);
+      float* bb = bounds + 8l * k;
+      bb[0] = p.x - S.r; bb[1] = p.y - S.r; bb[2] = p.z - S.r;
+      bb[3] = p.x + S.r; bb[4] = p.y + S.r; bb[5] = p.z + S.r;
+      bb[6] = 0.f; bb[7] = 0.f;
+      is_leaf[k] = 1;
+      min_r[k] = max_r[k] = k;
+    }
+    if (n >= 2) {
+      or_radix_tree_u64(sk, n, is_leaf, left, right, parent, min_r, max_r);
+      or_refit(n, left, right, bounds);
+    }
+    const float thr = 2.0f * S.r;
+    const float prm[4] = {S.k, S.damping, S.shear, S.attraction};
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int k = 0; k < n; ++k) {
+      v3 pos = xyz(sp + 4l * k), vel = xyz(svl + 4l * k);
+      int body = f2i(sp[4l * k + 3]);
+      const float* qbox = bounds + 8l * k;
+      v3 lin = mk3(0.f, 0.f, 0.f);
+      if (n >= 2) {
+        int cap = 64, top = 0;
+        int* st = (int*)malloc(sizeof(int) * cap);
+        st[top++] = -1;
+        int node = n;
+        do {
+          int lc = left[node], rc = right[node];
+          int ol = lc != k && overlap8(qbox, bounds + 8l * lc);
+          int orr = rc != k && overlap8(qbox, bounds + 8l * rc);
+          int ll = is_leaf[lc], rl = is_leaf[rc];
+          for (int side = 0; side < 2; ++side) {
+            int c = side == 0 ? lc : rc;
+            if (!((side == 0 ? ol : orr) && (side == 0 ? ll : rl))) continue;
+            if (f2i(sp[4l * c + 3]) == body) continue;
+            v3 rp = sub(xyz(sp + 4l * c), pos);
+            float dist = sqrtf(dot(rp, rp));
+            if (dist < thr) lin = add(lin, spring_force(rp, dist, sub(xyz(svl + 4l * c), vel), thr, prm));
+          }
+          int tl = ol && !ll, tr = orr && !rl;
+          if (!tl && !tr) {
+            node = st[--top];
+          } else {
+            node = tl ? lc : rc;
+            if (tl && tr) {
+              if (top == cap) { cap *= 2; st = (int*)realloc(st, sizeof(int) * cap); }
+              st[top++] = rc;
+            }
+          }
+        } while (node != -1);
+        free(st);
+      }
+      lin = add(lin, wall_force(&S, pos, vel));
+      st4(pf + 4l * sv[k], lin.x, lin.y, lin.z, 0.f);
+    }
+    if (!bodies_step(&S, nb, pf, bpos4, bquat4, bvel4, bang4, mass, ib9, off, rel4, bforce4_out,
+                     btorque4_out))
+      ok = 0;
+  }
+  if (skeys_out) memcpy(skeys_out, sk, 8l * n);
+  if (sidx_out) memcpy(sidx_out, sv, 4l * n);
+  if (pforce4_out) memcpy(pforce4_out, pf, 16l * n);
+  free(keys); free(sk); free(sv); free(sp); free(svl); free(pf);
+  free(is_leaf); free(left); free(right); free(parent); free(min_r); free(max_r); free(bounds);
   return ok;
 }
 
