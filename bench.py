@@ -684,7 +684,8 @@ def run_served(args):
                       "sample_requests": len(sample)},
             "served_over_plain": s["scene_steps_per_s"] / (steps / plain_s),
             "peak_resident_scenes": s["peak_resident_scenes"],
-            "peak_resident_gb": s["peak_resident_bytes"] / 1e9, "ticks": s["ticks"]}
+            "peak_resident_gb": s["peak_resident_bytes"] / 1e9, "ticks": s["ticks"],
+            "host_s": s["host_s"]}
     print(json.dumps(line))
     server.close()
     return 0

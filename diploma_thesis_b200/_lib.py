@@ -74,7 +74,7 @@ class StepView(C.Structure):
                 ("particle_force4", C.c_void_p), ("cells2", C.c_void_p),
                 ("key_bytes", C.c_int), ("broadphase", C.c_int), ("tree_left", C.c_void_p),
                 ("tree_right", C.c_void_p), ("tree_parent", C.c_void_p),
-                ("tree_bounds8", C.c_void_p)]
+                ("tree_nodes16", C.c_void_p)]
 
 
 P = C.c_void_p

@@ -6,6 +6,8 @@
 // i, internal node i at n + i, root at n.  Boxes are the reference's 32-byte AABB
 // {min.xyz, max.xyz, pad, pad}, read as two float4.
 #pragma once
+#include <cuda/atomic>
+
 #include "ar_internal.cuh"
 
 namespace ar_lbvh {
@@ -48,8 +50,9 @@ struct Lcp64Scene {
 };
 
 // ---- Karras 2012 internal node i (kernelConstructRadixTreeSoA, BVHSoAKernels.cu:7-99) ----
+// Returns the node's (left, right) child ids.
 template <class Lcp>
-__device__ __forceinline__ void karras_node(int i, int n, const Lcp& lcp, uint8_t* is_leaf,
+__device__ __forceinline__ int2 karras_node(int i, int n, const Lcp& lcp, uint8_t* is_leaf,
                                             int32_t* left, int32_t* right, int32_t* parent,
                                             int32_t* min_r, int32_t* max_r) {
   const int d = (lcp(i, i + 1) - lcp(i, i - 1)) > 0 ? 1 : -1;
@@ -83,11 +86,20 @@ __device__ __forceinline__ void karras_node(int i, int n, const Lcp& lcp, uint8_
   parent[rc] = node;
   min_r[node] = lo;
   max_r[node] = hi;
+  return make_int2(lc, rc);
+}
+
+// Arrival counter of a refit node: an acquire-release increment at device scope, so the first
+// thread's box stores (made before its increment) are visible to the second thread's loads
+// (made after its increment).  Returns the previous count.
+__device__ __forceinline__ int arrive(int* counter) {
+  cuda::atomic_ref<int, cuda::thread_scope_device> a(*counter);
+  return a.fetch_add(1, cuda::memory_order_acq_rel);
 }
 
 // ---- bottom-up refit from leaf i (kernelConstructInternalNodesSoA, BVHSoAKernels.cu:148-176)
-// Release (fence before the counter) / acquire (fence after it, L2 loads of the children); the
-// second thread to reach a node merges its children (mergeBounds, BVHAuxiliary.cuh:83-94).
+// The second thread to reach a node merges its children (mergeBounds, BVHAuxiliary.cuh:83-94);
+// child boxes are read and written through L2.
 __device__ __forceinline__ void refit_from_leaf(int i, int n, const int32_t* __restrict__ left,
                                                 const int32_t* __restrict__ right,
                                                 const int32_t* __restrict__ parent,
@@ -95,9 +107,7 @@ __device__ __forceinline__ void refit_from_leaf(int i, int n, const int32_t* __r
   int node = __ldg(parent + i);
   for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
     if (node < n || node >= 2 * n - 1) return;  // malformed parent link
-    __threadfence();
-    if (atomicAdd(counters + (node - n), 1) == 0) return;
-    __threadfence();
+    if (arrive(counters + (node - n)) == 0) return;
     const int a = __ldg(left + node), b = __ldg(right + node);
     const float4 a0 = __ldcg(bounds + 2 * a), a1 = __ldcg(bounds + 2 * a + 1);
     const float4 b0 = __ldcg(bounds + 2 * b), b1 = __ldcg(bounds + 2 * b + 1);

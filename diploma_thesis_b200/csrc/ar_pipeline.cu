@@ -101,7 +101,8 @@ __global__ void __launch_bounds__(256) scatter_kernel(
     }
     if (k == nt - 1) cells[key].y = (uint32_t)nt;
     const int g = (int)__ldg(svals + k);
-    const SceneDev& S = table[find_range(poff, ns, g)];
+    const int sc = ns == 1 ? 0 : find_range(poff, ns, g);
+    const SceneDev& S = table[sc];
     const int i = g - S.poff;
     const float4 r4 = __ldg(S.rel + i);
     const int b = __float_as_int(r4.w);
@@ -109,67 +110,98 @@ __global__ void __launch_bounds__(256) scatter_kernel(
     ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
                     ar::mk3(r4.x, r4.y, r4.z), &r, &p, &v);
     spos[k] = make_float4(p.x, p.y, p.z, __int_as_float(S.boff + b));
-    svel[k] = make_float4(v.x, v.y, v.z, 0.f);
+    svel[k] = make_float4(v.x, v.y, v.z, __int_as_float(sc));  // w = scene index
   }
 }
 
 // ---- K4: DEM gather + walls ----------------------------------------------------------------
 // Per sorted particle: the 27 neighbour cells in z, y, x order, occupants in sorted order,
-// skipping itself and its own body; per-cell partial sums added to the total (the order of
-// FindAndHandleRigidBodyCollisionsUniformGridKernel, RigidBodies/UniformGridDEM.cu:166-193).
-// The three cells of an x-row are walked as one flattened loop (candidate t of the row maps
-// to cell A, B or C and to that cell's partial sum), so a warp's lanes stay in step across
-// cells.  Candidates at squared distance >= the float just above (2r)^2 are rejected without
-// the square root: for them sqrtf(d2) >= 2r exactly, so the contact test is unchanged.
+// skipping its own body (itself included); per-cell partial sums added to the total (the order
+// of FindAndHandleRigidBodyCollisionsUniformGridKernel, RigidBodies/UniformGridDEM.cu:166-193).
+// The particle's cell comes from its sorted key and its scene from the sorted velocity's w.
+// Three cells of an x-row that do not wrap have consecutive keys, so their occupants form one
+// contiguous run of the sorted arrays: the row is walked as that run, and a contact goes to
+// the partial sum of the cell whose sub-range holds it.  Rows that wrap in x walk the three
+// ranges one after the other.  The next row's cell entries are loaded before the current row
+// is walked.  Candidates at squared distance >= the float just above (2r)^2 are rejected
+// without the square root: for them sqrtf(d2) >= 2r exactly, so the contact test is unchanged.
+struct RowCells {
+  uint2 a, b, c;
+};
+
 __global__ void __launch_bounds__(256, 4) collide_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const SceneDev* __restrict__ table, int nt, const uint32_t* __restrict__ skeys,
     const uint32_t* __restrict__ svals, const uint2* __restrict__ cells,
     const float4* __restrict__ spos, const float4* __restrict__ svel,
     float4* __restrict__ pforce) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
-  const int g = (int)__ldg(svals + k);
-  const SceneDev& S = table[ns == 1 ? 0 : find_range(poff, ns, g)];
   const float4 p4 = __ldg(spos + k);
-  const float3 pos = ar::xyz(p4);
+  const float4 v4 = __ldg(svel + k);
+  const SceneDev& S = table[__float_as_int(v4.w)];
+  const float3 pos = ar::xyz(p4), vel = ar::xyz(v4);
   const int body = __float_as_int(p4.w);
-  const float3 vel = ar::xyz(__ldg(svel + k));
   const float thr = 2.0f * S.r;
   const float thr2_up = nextafterf(thr * thr, INFINITY);
   const float kk = S.k, dmp = S.damping, shr = S.shear, att = S.attraction;
-  const int3 gp = ar_pipe::cell_of(S, pos);
+  const uint32_t lx = S.lx, ly = S.ly, mx = S.gx - 1, my = S.gy - 1, mz = S.gz - 1;
+  const uint32_t base = S.cell_base, local = __ldg(skeys + k) - base;
+  const uint32_t x = local & mx, y = (local >> lx) & my, z = local >> (lx + ly);
+  const uint32_t xa = (x - 1) & mx, xc = (x + 1) & mx;
+  const bool straight = x >= 1 && x + 1 <= mx;  // x-1, x, x+1 have consecutive keys
+  auto row_of = [&](int r) {  // r = 3 (dz + 1) + (dy + 1)
+    const uint32_t zz = (z + (uint32_t)(r / 3) - 1u) & mz, yy = (y + (uint32_t)(r % 3) - 1u) & my;
+    const uint32_t row = base + (zz << (lx + ly)) + (yy << lx);
+    return RowCells{__ldg(cells + row + xa), __ldg(cells + row + x), __ldg(cells + row + xc)};
+  };
+  auto contact = [&](uint32_t j, float3* f) {
+    const float4 q4 = __ldg(spos + j);
+    if (__float_as_int(q4.w) == body) return false;
+    const float3 rp = ar::sub(ar::xyz(q4), pos);
+    const float d2 = ar::dot(rp, rp);
+    if (!(d2 < thr2_up)) return false;
+    const float dist = sqrtf(d2);
+    if (!(dist < thr)) return false;
+    const float3 v2 = ar::xyz(__ldg(svel + j));
+    *f = ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att);
+    return true;
+  };
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
-  for (int z = -1; z <= 1; ++z)
-    for (int y = -1; y <= 1; ++y) {
-      const uint2 ca = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x - 1, gp.y + y, gp.z + z)));
-      const uint2 cb = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x, gp.y + y, gp.z + z)));
-      const uint2 cc = __ldg(cells + ar_pipe::cell_key(S, make_int3(gp.x + 1, gp.y + y, gp.z + z)));
-      const uint32_t na = ca.x == ar::kEmpty ? 0u : ca.y - ca.x;
-      const uint32_t nb = cb.x == ar::kEmpty ? 0u : cb.y - cb.x;
-      const uint32_t nc = cc.x == ar::kEmpty ? 0u : cc.y - cc.x;
+  RowCells next = row_of(0);
+  for (int r = 0; r < 9; ++r) {
+    const RowCells cur = next;
+    if (r < 8) next = row_of(r + 1);
+    const uint32_t na = cur.a.x == ar::kEmpty ? 0u : cur.a.y - cur.a.x;
+    const uint32_t nb = cur.b.x == ar::kEmpty ? 0u : cur.b.y - cur.b.x;
+    const uint32_t nc = cur.c.x == ar::kEmpty ? 0u : cur.c.y - cur.c.x;
+    float3 fa = ar::mk3(0.f, 0.f, 0.f), fb = fa, fc = fa;
+    float3 f;
+    if (straight) {
+      // first occupant of the run, and the ends of cells a and b within it
+      const uint32_t j0 = na ? cur.a.x : (nb ? cur.b.x : cur.c.x);
+      const uint32_t ea = j0 + na, eb = ea + nb, e = eb + nc;
+      for (uint32_t j = j0; j < e; ++j) {
+        if (!contact(j, &f)) continue;
+        if (j < ea) fa = ar::add(fa, f);
+        else if (j < eb) fb = ar::add(fb, f);
+        else fc = ar::add(fc, f);
+      }
+    } else {
       const uint32_t nab = na + nb, total = nab + nc;
-      float3 fa = ar::mk3(0.f, 0.f, 0.f), fb = fa, fc = fa;
       for (uint32_t t = 0; t < total; ++t) {
-        const uint32_t j = t < na ? ca.x + t : (t < nab ? cb.x + (t - na) : cc.x + (t - nab));
-        const float4 q4 = __ldg(spos + j);
-        if (j == (uint32_t)k || __float_as_int(q4.w) == body) continue;
-        const float3 rp = ar::sub(ar::xyz(q4), pos);
-        const float d2 = ar::dot(rp, rp);
-        if (!(d2 < thr2_up)) continue;
-        const float dist = sqrtf(d2);
-        if (!(dist < thr)) continue;
-        const float3 v2 = ar::xyz(__ldg(svel + j));
-        const float3 f = ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att);
+        const uint32_t j = t < na ? cur.a.x + t : (t < nab ? cur.b.x + (t - na) : cur.c.x + (t - nab));
+        if (!contact(j, &f)) continue;
         if (t < na) fa = ar::add(fa, f);
         else if (t < nab) fb = ar::add(fb, f);
         else fc = ar::add(fc, f);
       }
-      lin = ar::add(lin, fa);
-      lin = ar::add(lin, fb);
-      lin = ar::add(lin, fc);
     }
+    lin = ar::add(lin, fa);
+    lin = ar::add(lin, fb);
+    lin = ar::add(lin, fc);
+  }
   lin = ar::add(lin, ar_pipe::wall_force(S, pos, vel));
-  pforce[g] = make_float4(lin.x, lin.y, lin.z, 0.f);
+  pforce[__ldg(svals + k)] = make_float4(lin.x, lin.y, lin.z, 0.f);
 }
 
 // ---- BVH broad phase ---------------------------------------------------------------------------
@@ -209,30 +241,24 @@ __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restr
   }
 }
 
-// Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
-// state, box = position +/- r, leaf flags and ranges.
-__global__ void __launch_bounds__(256) bvh_leaves_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
-    const uint32_t* __restrict__ svals, float4* __restrict__ spos, float4* __restrict__ svel,
-    float4* __restrict__ bounds, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
-    int32_t* __restrict__ max_r) {
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
-    const int g = (int)__ldg(svals + k);
-    const SceneDev& S = table[ns == 1 ? 0 : find_range(poff, ns, g)];
-    const float4 r4 = __ldg(S.rel + (g - S.poff));
-    const int b = __float_as_int(r4.w);
-    float3 r, p, v;
-    ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
-                    ar::mk3(r4.x, r4.y, r4.z), &r, &p, &v);
-    spos[k] = make_float4(p.x, p.y, p.z, __int_as_float(S.boff + b));
-    svel[k] = make_float4(v.x, v.y, v.z, 0.f);
-    const float rr = S.r;
-    bounds[2 * k] = make_float4(p.x - rr, p.y - rr, p.z - rr, p.x + rr);
-    bounds[2 * k + 1] = make_float4(p.y + rr, p.z + rr, 0.f, 0.f);
-    is_leaf[k] = 1;
-    min_r[k] = k;
-    max_r[k] = k;
-  }
+// Internal node i (global id n + i) of the fused BVH holds both children's boxes and ids, so
+// one 64-byte fetch decides a traversal step:
+//   c[0] = left box (lo.x, lo.y, lo.z, hi.x)    c[1] = (hi.y, hi.z, left id, parent id)
+//   c[2] = right box (lo.x, lo.y, lo.z, hi.x)   c[3] = (hi.y, hi.z, right id, 0)
+// Ids < n are leaves (sorted particle slots); the root's parent id is -1.
+struct __align__(64) WideNode {
+  float4 c[4];
+};
+
+__device__ __forceinline__ int* node_ints(WideNode* nodes, int internal) {
+  return reinterpret_cast<int*>(nodes + internal);
+}
+// Box of child `side` (0 left, 1 right) into the parent's slot, ids untouched.
+__device__ __forceinline__ void put_child_box(WideNode* nodes, int internal, int side, float4 lo,
+                                              float2 hi_yz) {
+  float4* c = nodes[internal].c + 2 * side;
+  __stcg(c, lo);
+  __stcg(reinterpret_cast<float2*>(c + 1), hi_yz);
 }
 
 __global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp, int n,
@@ -241,11 +267,51 @@ __global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp,
                                                         int32_t* __restrict__ right,
                                                         int32_t* __restrict__ parent,
                                                         int32_t* __restrict__ min_r,
-                                                        int32_t* __restrict__ max_r) {
+                                                        int32_t* __restrict__ max_r,
+                                                        WideNode* __restrict__ nodes) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) parent[n] = -1;
   if (i >= n - 1) return;
-  ar_lbvh::karras_node(i, n, lcp, is_leaf, left, right, parent, min_r, max_r);
+  const int2 ch = ar_lbvh::karras_node(i, n, lcp, is_leaf, left, right, parent, min_r, max_r);
+  int* w = node_ints(nodes, i);
+  w[6] = ch.x;
+  w[14] = ch.y;
+  w[15] = 0;
+  if (i == 0) w[7] = -1;
+  if (ch.x >= n) node_ints(nodes, ch.x - n)[7] = n + i;
+  if (ch.y >= n) node_ints(nodes, ch.y - n)[7] = n + i;
+}
+
+// Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
+// state; the leaf box (position +/- r) goes into its parent's slot; leaf flags and ranges.
+__global__ void __launch_bounds__(256) bvh_leaves_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const uint32_t* __restrict__ svals, const int32_t* __restrict__ left,
+    const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
+    WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
+    int32_t* __restrict__ max_r) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+    const int g = (int)__ldg(svals + k);
+    const int sc = ns == 1 ? 0 : find_range(poff, ns, g);
+    const SceneDev& S = table[sc];
+    const float4 r4 = __ldg(S.rel + (g - S.poff));
+    const int b = __float_as_int(r4.w);
+    float3 r, p, v;
+    ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
+                    ar::mk3(r4.x, r4.y, r4.z), &r, &p, &v);
+    spos[k] = make_float4(p.x, p.y, p.z, __int_as_float(S.boff + b));
+    svel[k] = make_float4(v.x, v.y, v.z, __int_as_float(sc));  // w = scene index
+    if (nt >= 2) {
+      const float rr = S.r;
+      const int pn = __ldg(parent + k);
+      put_child_box(nodes, pn - nt, __ldg(left + pn) == k ? 0 : 1,
+                    make_float4(p.x - rr, p.y - rr, p.z - rr, p.x + rr),
+                    make_float2(p.y + rr, p.z + rr));
+    }
+    is_leaf[k] = 1;
+    min_r[k] = k;
+    max_r[k] = k;
+  }
 }
 
 // Each scene's subtree root: the lowest ancestor of its first leaf covering its last leaf.
@@ -268,58 +334,102 @@ __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
   roots[s] = node;
 }
 
+// Bottom-up refit (kernelConstructInternalNodesSoA, BVHSource/BVHSoAKernels.cu:148-176): one
+// thread per leaf climbs; the second thread to reach a node merges the two child boxes held in
+// the node (mergeBounds, BVHAuxiliary.cuh:83-94) and stores the result into the node's slot in
+// its parent.  Release / acquire through the arrival counter; boxes through L2.
 __global__ void __launch_bounds__(256) bvh_refit_kernel(int n, const int32_t* __restrict__ left,
-                                                        const int32_t* __restrict__ right,
                                                         const int32_t* __restrict__ parent,
-                                                        float4* bounds,
+                                                        WideNode* nodes,
                                                         int* __restrict__ counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  ar_lbvh::refit_from_leaf(i, n, left, right, parent, bounds, counters);
+  if (i >= n || n < 2) return;
+  int node = __ldg(parent + i);
+  for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
+    if (node < n || node >= 2 * n - 1) return;  // malformed parent link
+    if (ar_lbvh::arrive(counters + (node - n)) == 0) return;
+    const float4* c = nodes[node - n].c;
+    const float4 a0 = __ldcg(c), a1 = __ldcg(c + 1), b0 = __ldcg(c + 2), b1 = __ldcg(c + 3);
+    if (node == n) return;  // the root's box is not stored anywhere
+    float4 lo;
+    lo.x = a0.x < b0.x ? a0.x : b0.x;
+    lo.y = a0.y < b0.y ? a0.y : b0.y;
+    lo.z = a0.z < b0.z ? a0.z : b0.z;
+    lo.w = a0.w > b0.w ? a0.w : b0.w;  // max.x
+    const float2 hi = make_float2(a1.x > b1.x ? a1.x : b1.x, a1.y > b1.y ? a1.y : b1.y);
+    const int pn = __ldg(parent + node);
+    put_child_box(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1, lo, hi);
+    node = pn;
+  }
 }
 
 // DEM gather through the scene's subtree in the reference's visit order
-// (Kernels/RB_BVHKernels.cu:145-214), contacts summed in visit order, then the walls.
+// (collideBVHSoARigidBody, Kernels/RB_BVHKernels.cu:145-214): at a node the overlapping leaf
+// children are handled left then right, then the walk goes into the left internal child if it
+// overlaps, deferring the right one on a short stack.  Contacts are summed in visit order,
+// then the walls.  A scene subtree is at most 30 + 32 levels deep (code bits + index bits),
+// so the stack never holds more than 62 entries.
+constexpr int kBvhStack = 64;
+
 __global__ void __launch_bounds__(256) bvh_collide_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
     const uint32_t* __restrict__ svals, const float4* __restrict__ spos,
-    const float4* __restrict__ svel, const float4* __restrict__ bounds,
-    const uint8_t* __restrict__ is_leaf, const int32_t* __restrict__ left,
-    const int32_t* __restrict__ right, const int32_t* __restrict__ parent,
-    const int32_t* __restrict__ roots, float4* __restrict__ pforce) {
+    const float4* __restrict__ svel, const WideNode* __restrict__ nodes,
+    const int32_t* __restrict__ roots, float4* __restrict__ pforce, int* __restrict__ err) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
-  const int g = (int)__ldg(svals + k);
-  const int s = ns == 1 ? 0 : find_range(poff, ns, g);
-  const SceneDev& S = table[s];
   const float4 p4 = __ldg(spos + k);
-  const float3 pos = ar::xyz(p4);
+  const float4 v4 = __ldg(svel + k);
+  const int s = __float_as_int(v4.w);
+  const SceneDev& S = table[s];
+  const float3 pos = ar::xyz(p4), vel = ar::xyz(v4);
   const int body = __float_as_int(p4.w);
-  const float3 vel = ar::xyz(__ldg(svel + k));
-  const float thr = 2.0f * S.r;
+  const float rr = S.r;
+  const float thr = 2.0f * rr;
   const float thr2_up = nextafterf(thr * thr, INFINITY);
   const float kk = S.k, dmp = S.damping, shr = S.shear, att = S.attraction;
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
   const int root = __ldg(roots + s);
   if (root >= nt) {  // an internal node
-    const ar_lbvh::Box qbox = ar_lbvh::load_box(bounds, k);
-    ar_lbvh::walk(root, nt, is_leaf, left, right, parent,
-                  [&](int c) { return c != k && ar_lbvh::overlap(qbox, ar_lbvh::load_box(bounds, c)); },
-                  [&](int c, bool) {
-                    const float4 q4 = __ldg(spos + c);
-                    if (__float_as_int(q4.w) == body) return;
-                    const float3 rp = ar::sub(ar::xyz(q4), pos);
-                    const float d2 = ar::dot(rp, rp);
-                    if (!(d2 < thr2_up)) return;
-                    const float dist = sqrtf(d2);
-                    if (!(dist < thr)) return;
-                    const float3 v2 = ar::xyz(__ldg(svel + c));
-                    lin = ar::add(lin, ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk,
-                                                            dmp, shr, att));
-                  });
+    const ar_lbvh::Box q{pos.x - rr, pos.y - rr, pos.z - rr, pos.x + rr, pos.y + rr, pos.z + rr};
+    auto visit = [&](int c) {
+      const float4 q4 = __ldg(spos + c);
+      if (__float_as_int(q4.w) == body) return;
+      const float3 rp = ar::sub(ar::xyz(q4), pos);
+      const float d2 = ar::dot(rp, rp);
+      if (!(d2 < thr2_up)) return;
+      const float dist = sqrtf(d2);
+      if (!(dist < thr)) return;
+      const float3 v2 = ar::xyz(__ldg(svel + c));
+      lin = ar::add(lin, ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att));
+    };
+    int stack[kBvhStack];
+    int top = 0;
+    int node = root;
+    for (int guard = 2 * nt; guard > 0; --guard) {
+      const float4* c = nodes[node - nt].c;
+      const float4 a0 = __ldg(c), a1 = __ldg(c + 1), b0 = __ldg(c + 2), b1 = __ldg(c + 3);
+      const int lc = __float_as_int(a1.z), rc = __float_as_int(b1.z);
+      const bool ol = lc != k && ar_lbvh::overlap(q, ar_lbvh::Box{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y});
+      const bool orr = rc != k && ar_lbvh::overlap(q, ar_lbvh::Box{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y});
+      const bool ll = lc < nt, rl = rc < nt;
+      if (ol && ll) visit(lc);
+      if (orr && rl) visit(rc);
+      const bool tl = ol && !ll, tr = orr && !rl;
+      if (!tl && !tr) {
+        if (top == 0) break;
+        node = stack[--top];
+      } else {
+        node = tl ? lc : rc;
+        if (tl && tr) {
+          if (top < kBvhStack) stack[top++] = rc;
+          else ar::raise_error(err, ar::kErrOverflow);
+        }
+      }
+    }
   }
   lin = ar::add(lin, ar_pipe::wall_force(S, pos, vel));
-  pforce[g] = make_float4(lin.x, lin.y, lin.z, 0.f);
+  pforce[__ldg(svals + k)] = make_float4(lin.x, lin.y, lin.z, 0.f);
 }
 
 // ---- K5: fixed-order body sums + integration ---------------------------------------------------
@@ -419,7 +529,7 @@ struct ar_batch {
   uint8_t* is_leaf = nullptr;
   int32_t *left = nullptr, *right = nullptr, *parent = nullptr, *min_r = nullptr,
           *max_r = nullptr, *roots = nullptr;
-  float4* bounds = nullptr;
+  WideNode* nodes = nullptr;
   int* counters = nullptr;
   char* sort64_ws = nullptr;
   int bvh_key_bits = kMortonBits;
@@ -444,11 +554,11 @@ void free_batch_buffers(ar_batch* B) {
   B->cap_sort = 0;
   cudaFree(B->keys64); cudaFree(B->skeys64); cudaFree(B->is_leaf); cudaFree(B->left);
   cudaFree(B->right); cudaFree(B->parent); cudaFree(B->min_r); cudaFree(B->max_r);
-  cudaFree(B->roots); cudaFree(B->bounds); cudaFree(B->counters); cudaFree(B->sort64_ws);
+  cudaFree(B->roots); cudaFree(B->nodes); cudaFree(B->counters); cudaFree(B->sort64_ws);
   B->keys64 = B->skeys64 = nullptr;
   B->is_leaf = nullptr;
   B->left = B->right = B->parent = B->min_r = B->max_r = B->roots = nullptr;
-  B->bounds = nullptr;
+  B->nodes = nullptr;
   B->counters = nullptr;
   B->sort64_ws = nullptr;
   B->cap_bvh = 0;
@@ -507,6 +617,8 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     d.r = D.radius; d.dt = D.dt; d.k = D.spring; d.damping = D.damping; d.shear = D.shear;
     d.attraction = D.attraction;
     d.gx = s->gdim[0]; d.gy = s->gdim[1]; d.gz = s->gdim[2];
+    d.lx = (uint32_t)ceil_log2(d.gx);
+    d.ly = (uint32_t)ceil_log2(d.gy);
     d.cell_base = (uint32_t)cells;
     d.poff = (int)nt; d.boff = (int)bt; d.n = s->n; d.nb = s->nb;
     d.pos = s->pos; d.quat = s->quat; d.vel = s->vel; d.ang = s->ang;
@@ -564,11 +676,11 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
       const size_t csort = ar_sort::layout(cn, 8, passes64).total;
       cudaFree(B->keys64); cudaFree(B->skeys64); cudaFree(B->is_leaf); cudaFree(B->left);
       cudaFree(B->right); cudaFree(B->parent); cudaFree(B->min_r); cudaFree(B->max_r);
-      cudaFree(B->roots); cudaFree(B->bounds); cudaFree(B->counters); cudaFree(B->sort64_ws);
+      cudaFree(B->roots); cudaFree(B->nodes); cudaFree(B->counters); cudaFree(B->sort64_ws);
       bool ok = alloc(&B->keys64, cn) && alloc(&B->skeys64, cn) && alloc(&B->is_leaf, m) &&
                 alloc(&B->left, m) && alloc(&B->right, m) && alloc(&B->parent, m) &&
                 alloc(&B->min_r, m) && alloc(&B->max_r, m) && alloc(&B->roots, B->cap_s) &&
-                alloc(&B->bounds, 2 * m) && alloc(&B->counters, cn) &&
+                alloc(&B->nodes, cn) && alloc(&B->counters, cn) &&
                 alloc(&B->sort64_ws, csort);
       if (!ok) {
         free_batch_buffers(B);
@@ -610,7 +722,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
   mark(0);
   if (B->broadphase == AR_BROADPHASE_BVH) {
-    // clear | Morton keys | sort | tree (leaves, Karras nodes, scene roots, refit) | collide |
+    // clear | Morton keys | sort | tree (Karras nodes, leaves, scene roots, refit) | collide |
     // reduce_integrate
     cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);
     mark(1);
@@ -621,19 +733,20 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
                                     B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
     if (s != AR_OK) return s;
     mark(3);
-    bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals, B->spos,
-                                          B->svel, B->bounds, B->is_leaf, B->min_r, B->max_r);
     bvh_build_kernel<<<arh::grid_for(std::max(nt - 1, 1), 256), 256, 0, st>>>(
         ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
-        B->right, B->parent, B->min_r, B->max_r);
+        B->right, B->parent, B->min_r, B->max_r, B->nodes);
+    bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals, B->left,
+                                          B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
+                                          B->min_r, B->max_r);
     bvh_roots_kernel<<<arh::grid_for(ns, 128), 128, 0, st>>>(B->d_poff, ns, nt, B->parent,
                                                               B->min_r, B->max_r, B->roots);
-    bvh_refit_kernel<<<arh::grid_for(nt, 256), 256, 0, st>>>(nt, B->left, B->right, B->parent,
-                                                              B->bounds, B->counters);
+    bvh_refit_kernel<<<arh::grid_for(nt, 256), 256, 0, st>>>(nt, B->left, B->parent, B->nodes,
+                                                              B->counters);
     mark(4);
     bvh_collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(
-        B->d_table, B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->bounds, B->is_leaf,
-        B->left, B->right, B->parent, B->roots, B->pforce);
+        B->d_table, B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots,
+        B->pforce, ctx->d_err);
     mark(5);
     reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
         B->d_table, B->d_boff, ns, bt, B->pforce, ctx->d_err);
@@ -658,7 +771,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
                                                         B->svals, B->cells, B->spos, B->svel,
                                                         B->d_prev_n);
   mark(4);
-  collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals,
+  collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, nt, B->skeys, B->svals,
                                                        B->cells, B->spos, B->svel, B->pforce);
   mark(5);
   reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
@@ -993,7 +1106,7 @@ ar_status ar_scene_step_view(ar_scene* s, ar_step_view* v) {
   v->tree_left = bvh ? B->left : nullptr;
   v->tree_right = bvh ? B->right : nullptr;
   v->tree_parent = bvh ? B->parent : nullptr;
-  v->tree_bounds8 = bvh ? (float*)B->bounds : nullptr;
+  v->tree_nodes16 = bvh ? (float*)B->nodes : nullptr;
   return AR_OK;
 }
 

@@ -1,6 +1,6 @@
 // Device-side scene table and the PHYSICAL-mode per-particle / per-body math of the fused
 // step.  Every function here is mirrored operation for operation by the oracle
-// (oracle/oracle.c, ar_oracle_step), which is what makes stepped states bit-identical.
+// (oracle/oracle.c, or_step / or_step_bvh), which is what makes stepped states bit-identical.
 #pragma once
 #include "ar_internal.cuh"
 #include "ar_glm.cuh"
@@ -15,6 +15,7 @@ struct SceneDev {
   float r, dt, k, damping, shear, attraction;
   float origin[3], cell[3]; // grid
   uint32_t gx, gy, gz;      // cells per axis (powers of two)
+  uint32_t lx, ly;          // log2 gx, log2 gy
   uint32_t cell_base;       // first cell of the scene in the batch's global cell space
   int poff, boff, n, nb;    // first particle / body in the batch, counts
   float4* pos;              // body centre (w unused)

@@ -59,6 +59,7 @@ class ServerStats:
     peak_resident: int
     peak_bytes: int
     ticks: int
+    host_s: dict = field(default_factory=dict)  # host seconds per loop phase
 
     def summary(self) -> dict:
         lat = self.latencies
@@ -69,7 +70,7 @@ class ServerStats:
             "p50_latency_s": float(np.percentile(lat, 50)) if len(lat) else None,
             "p99_latency_s": float(np.percentile(lat, 99)) if len(lat) else None,
             "peak_resident_scenes": self.peak_resident, "peak_resident_bytes": self.peak_bytes,
-            "ticks": self.ticks,
+            "ticks": self.ticks, "host_s": self.host_s,
         }
 
 
@@ -115,6 +116,7 @@ class Server:
         done: list[Request] = []
         scene_steps = particle_steps = 0
         peak_res = peak_bytes = ticks = 0
+        phase = {"admit": 0.0, "set_scenes": 0.0, "step": 0.0, "retire": 0.0}
         t0 = time.perf_counter()
         stream_ctx = torch.cuda.stream(self.stream) if isinstance(self.stream, torch.cuda.Stream) \
             else contextlib.nullcontext()
@@ -135,7 +137,9 @@ class Server:
                         if need[1] > AR_MAX_BATCH_CELLS or need[2] > self.max_particles:
                             raise ValueError(f"request {waiting[0].rid} can never be admitted")
                     req = waiting.pop(0)
+                    ta = time.perf_counter()
                     gs = self.scene_factory(self.ctx, req.scene)
+                    phase["admit"] += time.perf_counter() - ta
                     req.admitted = time.perf_counter() - t0
                     active.append([req, gs, req.steps, need])
                     used = [u + x for u, x in zip(used, need)]
@@ -144,10 +148,15 @@ class Server:
                     if pending:  # idle until the next arrival
                         time.sleep(max(0.0, min(0.001, pending[0].arrival - now)))
                     continue
+                tb = time.perf_counter()
                 if changed or ticks == 0:
                     self.batch.set_scenes([a[1] for a in active])
                 k = min(self.tick_steps, min(a[2] for a in active))
+                tc = time.perf_counter()
                 self.batch.step(k, use_graph=True, stream=self.stream)
+                td = time.perf_counter()
+                phase["set_scenes"] += tc - tb
+                phase["step"] += td - tc
                 ticks += 1
                 peak_res = max(peak_res, len(active))
                 peak_bytes = max(peak_bytes, used[0])
@@ -159,6 +168,7 @@ class Server:
                     if a[2] <= 0:
                         finished.append(a)
                 if finished:
+                    tr = time.perf_counter()
                     self.stream.synchronize()
                     tdone = time.perf_counter() - t0
                     for req, gs, _, need in finished:
@@ -170,12 +180,13 @@ class Server:
                         done.append(req)
                     active = [a for a in active if a[2] > 0]
                     self.batch.set_scenes([a[1] for a in active])
+                    phase["retire"] += time.perf_counter() - tr
             self.stream.synchronize()
         wall = time.perf_counter() - t0
         self.ctx.check(self.stream)
         lat = np.array([r.done - r.arrival for r in done])
         return ServerStats(len(done), len(requests), wall, scene_steps, particle_steps, lat,
-                           peak_res, peak_bytes, ticks)
+                           peak_res, peak_bytes, ticks, phase)
 
     def close(self) -> None:
         self.batch.close()

@@ -455,8 +455,10 @@ AR_API ar_status ar_scene_grid_info(ar_scene* scene, float origin[3], float cell
  * DEM + wall force at the original index, and for the grid broad phase the cell table as
  * (start, end) pairs (start = 0xffffffff for an empty cell).  Grid keys are uint32 cell keys
  * (key_bytes 4); BVH keys are uint64 Morton codes (key_bytes 8), and the BVH view adds the
- * tree (leaf i at i, internal node i at N + i, root N; tree_bounds8: 8 floats per node,
- * min.xyz, max.xyz, 0, 0).  Tree pointers are NULL for the grid, cells2 NULL for the BVH. */
+ * tree (leaf i at i, internal node i at N + i, root N) and tree_nodes16: 16 floats per
+ * internal node holding both children's boxes and ids -- left lo.xyz, hi.x | hi.y, hi.z,
+ * left id, parent id | right lo.xyz, hi.x | hi.y, hi.z, right id, 0 (ids as int bits; the
+ * root's parent id is -1).  Tree pointers are NULL for the grid, cells2 NULL for the BVH. */
 typedef struct ar_step_view {
   int num_particles;
   uint64_t num_cells;
@@ -472,7 +474,7 @@ typedef struct ar_step_view {
   int32_t* tree_left;
   int32_t* tree_right;
   int32_t* tree_parent;
-  float* tree_bounds8;
+  float* tree_nodes16;
 } ar_step_view;
 AR_API ar_status ar_scene_step_view(ar_scene* scene, ar_step_view* out);
 
