@@ -125,7 +125,10 @@ SIGNATURES = {
     "ar_scene_destroy": [P],
     "ar_scene_footprint": [C.POINTER(SceneDesc)],
     "ar_scene_cells": [C.POINTER(SceneDesc)],
+    "ar_scene_destroy_async": [P, S],
+    "ar_batch_set_scenes_limited": [P, C.POINTER(P), I, P],
     "ar_scene_download": [P, P, P, P, P, S],
+    "ar_scene_download_async": [P, P, P, P, P, S],
     "ar_scene_upload": [P, P, P, P, P, S],
     "ar_step_profile": [P, P, I, C.POINTER(F), S],
     "ar_batch_profile": [P, P, I, C.POINTER(F), S],

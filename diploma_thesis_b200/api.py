@@ -106,7 +106,8 @@ class GpuScene:
     """A scene resident on the device, advanced by ar_step."""
 
     def __init__(self, ctx: Context, scene: Scene, block_size: int = 0,
-                 cell_size: float | None = None, grid_log2=None, broadphase="grid"):
+                 cell_size: float | None = None, grid_log2=None, broadphase="grid",
+                 stream=None):
         self.ctx = ctx
         self.scene = scene
         self.broadphase = broadphase_code(broadphase)
@@ -118,7 +119,7 @@ class GpuScene:
         init = SceneInit(*[_np_ptr(a) for a in self._keep])
         self.handle = C.c_void_p()
         call("ar_scene_create", ctx.handle, C.byref(self.desc), C.byref(init),
-             stream_handle(), C.byref(self.handle))
+             stream_handle(stream), C.byref(self.handle))
         self.num_bodies = scene.num_bodies
         self.num_particles = scene.num_particles
 
@@ -176,6 +177,25 @@ class GpuScene:
             lib.ar_scene_destroy(self.handle)
             self.handle = C.c_void_p()
 
+    def download_async(self, stream=None) -> dict[str, np.ndarray]:
+        """Queue a copy of the body state into pinned host arrays on `stream` (no wait); the
+        arrays are valid once the stream has reached this point."""
+        nb = self.num_bodies
+        pinned = {k: torch.empty((nb, 4), dtype=torch.float32, pin_memory=True)
+                  for k in ("pos", "quat", "vel", "angvel")}
+        out = {k: v.numpy() for k, v in pinned.items()}
+        call("ar_scene_download_async", self.handle, *[_np_ptr(out[k]) for k in
+                                                       ("pos", "quat", "vel", "angvel")],
+             stream_handle(stream))
+        out["_pinned"] = pinned  # keeps the pinned blocks alive
+        return out
+
+    def close_async(self, stream=None) -> None:
+        """Free in stream order on `stream`; every use of the scene must precede that point."""
+        if self.handle:
+            call("ar_scene_destroy_async", self.handle, stream_handle(stream))
+            self.handle = C.c_void_p()
+
 
 class Batch:
     """Many resident scenes advanced together (one launch per stage, CUDA graph)."""
@@ -188,10 +208,18 @@ class Batch:
         if scenes:
             self.set_scenes(scenes)
 
-    def set_scenes(self, scenes: list[GpuScene]) -> None:
+    def set_scenes(self, scenes: list[GpuScene], steps_left=None) -> None:
+        """Member list; steps_left[i] (optional) caps how many of the following steps integrate
+        scene i (it is frozen afterwards)."""
         self.scenes = list(scenes)
         arr = (C.c_void_p * max(1, len(scenes)))(*[s.handle for s in scenes])
-        call("ar_batch_set_scenes", self.handle, arr, len(scenes))
+        if steps_left is None:
+            call("ar_batch_set_scenes", self.handle, arr, len(scenes))
+        else:
+            lim = np.ascontiguousarray(steps_left, dtype=np.int64)
+            assert len(lim) == len(scenes)
+            call("ar_batch_set_scenes_limited", self.handle, arr, len(scenes),
+                 C.c_void_p(lim.ctypes.data))
 
     def step(self, n: int = 1, use_graph: bool = True, stream=None) -> None:
         call("ar_batch_step", self.ctx.handle, self.handle, int(n), int(use_graph),

@@ -73,6 +73,14 @@ ar_status ar_ctx_create(int device, ar_ctx** out) {
   }
   cudaMemset(c->d_err, 0, sizeof(int));
   *c->h_err = 0;
+  // scenes come from the device's stream-ordered pool: keep freed memory in the pool instead
+  // of returning it to the driver at every synchronisation
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  cudaGetLastError();
   ar_sort::init();
   if (cudaDeviceSynchronize() != cudaSuccess) {
     arh::set_error("ar_ctx_create: device error");

@@ -21,6 +21,7 @@
 // refit, and a stackless walk of the scene's subtree per particle in the reference's visit
 // order.  K5 is shared.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -46,6 +47,18 @@ __device__ __forceinline__ int find_range(const int* __restrict__ off, int count
   return lo;
 }
 
+// Scene index of every particle and body of the batch (run when the member list changes).
+__global__ void __launch_bounds__(256) scene_ids_kernel(const int* __restrict__ poff,
+                                                        const int* __restrict__ boff, int ns,
+                                                        int nt, int bt, int* __restrict__ pscene,
+                                                        int* __restrict__ bscene) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nt || i < bt;
+       i += gridDim.x * blockDim.x) {
+    if (i < nt) pscene[i] = find_range(poff, ns, i);
+    if (i < bt) bscene[i] = find_range(boff, ns, i);
+  }
+}
+
 // ---- K0: reset the cells a previous layout touched -------------------------------------------
 __global__ void __launch_bounds__(256) clear_cells_kernel(const uint32_t* __restrict__ skeys,
                                                           int prev_n, uint2* __restrict__ cells) {
@@ -57,10 +70,12 @@ __global__ void __launch_bounds__(256) clear_cells_kernel(const uint32_t* __rest
 
 // ---- K1: re-pose + hash + sort histogram -----------------------------------------------------
 __global__ void __launch_bounds__(kK1Threads) repose_hash_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
     int* __restrict__ d_prev_n, const uint32_t* __restrict__ prev_skeys, uint2* __restrict__ cells,
-    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits) {
+    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits,
+    long long* __restrict__ d_step) {
   __shared__ uint32_t s_hist[4][256];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
   for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
   const int prev_n = *d_prev_n;
@@ -71,7 +86,7 @@ __global__ void __launch_bounds__(kK1Threads) repose_hash_kernel(
       if (g == 0 || k0 != __ldg(prev_skeys + g - 1)) cells[k0].x = ar::kEmpty;
     }
     if (g < nt) {
-      const SceneDev& S = table[find_range(poff, ns, g)];
+      const SceneDev& S = table[__ldg(pscene + g)];
       const int i = g - S.poff;
       const float4 r4 = __ldg(S.rel + i);
       const int b = __float_as_int(r4.w);
@@ -88,7 +103,7 @@ __global__ void __launch_bounds__(kK1Threads) repose_hash_kernel(
 
 // ---- K3: scatter + cell ranges ------------------------------------------------------------
 __global__ void __launch_bounds__(256) scatter_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
     const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
     uint2* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
     int* __restrict__ d_prev_n) {
@@ -101,7 +116,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(
     }
     if (k == nt - 1) cells[key].y = (uint32_t)nt;
     const int g = (int)__ldg(svals + k);
-    const int sc = ns == 1 ? 0 : find_range(poff, ns, g);
+    const int sc = __ldg(pscene + g);
     const SceneDev& S = table[sc];
     const int i = g - S.poff;
     const float4 r4 = __ldg(S.rel + i);
@@ -222,10 +237,12 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
 }
 
 __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restrict__ table,
-                                                         const int* __restrict__ poff, int ns,
-                                                         int nt, uint64_t* __restrict__ keys) {
+                                                         const int* __restrict__ pscene, int ns,
+                                                         int nt, uint64_t* __restrict__ keys,
+                                                         long long* __restrict__ d_step) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
-    const int s = ns == 1 ? 0 : find_range(poff, ns, g);
+    const int s = __ldg(pscene + g);
     const SceneDev& S = table[s];
     const float4 r4 = __ldg(S.rel + (g - S.poff));
     const int b = __float_as_int(r4.w);
@@ -285,14 +302,14 @@ __global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp,
 // Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
 // state; the leaf box (position +/- r) goes into its parent's slot; leaf flags and ranges.
 __global__ void __launch_bounds__(256) bvh_leaves_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
     const uint32_t* __restrict__ svals, const int32_t* __restrict__ left,
     const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
     WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
     int32_t* __restrict__ max_r) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const int g = (int)__ldg(svals + k);
-    const int sc = ns == 1 ? 0 : find_range(poff, ns, g);
+    const int sc = __ldg(pscene + g);
     const SceneDev& S = table[sc];
     const float4 r4 = __ldg(S.rel + (g - S.poff));
     const int b = __float_as_int(r4.w);
@@ -433,13 +450,18 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
 }
 
 // ---- K5: fixed-order body sums + integration ---------------------------------------------------
+// A scene whose step budget is spent (batch step number > end_step) is frozen: its state is
+// left untouched.
 __global__ void __launch_bounds__(256) reduce_integrate_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ boff, int ns, int bt,
-    const float4* __restrict__ pforce, int* __restrict__ err) {
+    const SceneDev* __restrict__ table, const int* __restrict__ bscene, int ns, int bt,
+    const float4* __restrict__ pforce, const long long* __restrict__ d_step,
+    int* __restrict__ err) {
   const int warps = (gridDim.x * blockDim.x) >> 5;
   const int lane = ar::lane_id();
+  const long long step = *d_step;
   for (int gb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gb < bt; gb += warps) {
-    const SceneDev& S = table[find_range(boff, ns, gb)];
+    const SceneDev& S = table[__ldg(bscene + gb)];
+    if (step > S.end_step) continue;
     const int b = gb - S.boff;
     const int s0 = __ldg(S.offsets + b), s1 = __ldg(S.offsets + b + 1);
     const float4 q = S.quat[b];
@@ -496,6 +518,7 @@ struct ar_scene {
   float4 *bforce = nullptr, *btorque = nullptr, *rel = nullptr;
   float *mass = nullptr, *inv_inertia = nullptr;
   int32_t* offsets = nullptr;
+  void* block = nullptr;  // one stream-ordered allocation holding all of the above
   float origin[3], cell[3];
   uint32_t gdim[3];
   ar_batch* solo = nullptr;
@@ -516,6 +539,15 @@ struct ar_batch {
   char* sort_ws = nullptr;
   SceneDev* d_table = nullptr;
   int *d_poff = nullptr, *d_boff = nullptr, *d_prev_n = nullptr;
+  int *d_pscene = nullptr, *d_bscene = nullptr;  // scene index per particle / body
+  long long* d_step = nullptr;   // number of the step being run (incremented by its first kernel)
+  long long host_step = 0;       // steps enqueued so far
+  std::vector<long long> end_steps;  // per scene: last step that integrates it (empty: none)
+  // pinned staging of the scene table, two alternating buffers
+  char* h_stage[2] = {nullptr, nullptr};
+  size_t h_stage_cap[2] = {0, 0};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  int stage_i = 0;
   // layout
   long nt = 0, bt = 0;
   uint64_t total_cells = 0;
@@ -545,6 +577,8 @@ void free_batch_buffers(ar_batch* B) {
   cudaFree(B->spos); cudaFree(B->svel); cudaFree(B->pforce);
   cudaFree(B->cells); cudaFree(B->sort_ws);
   cudaFree(B->d_table); cudaFree(B->d_poff); cudaFree(B->d_boff); cudaFree(B->d_prev_n);
+  cudaFree(B->d_pscene); cudaFree(B->d_bscene);
+  B->d_pscene = B->d_bscene = nullptr;
   B->keys = B->skeys = B->svals = nullptr;
   B->spos = B->svel = B->pforce = nullptr;
   B->cells = nullptr; B->sort_ws = nullptr; B->d_table = nullptr;
@@ -624,6 +658,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     d.pos = s->pos; d.quat = s->quat; d.vel = s->vel; d.ang = s->ang;
     d.mass = s->mass; d.inv_inertia = s->inv_inertia; d.offsets = s->offsets; d.rel = s->rel;
     d.bforce = s->bforce; d.btorque = s->btorque;
+    d.end_step = B->end_steps.empty() ? LLONG_MAX : B->end_steps[tab.size()];
     tab.push_back(d);
     poff.push_back((int)nt);
     boff.push_back((int)bt);
@@ -646,14 +681,17 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
   if (realloc_needed) {
     cudaStreamSynchronize(st);
     free_batch_buffers(B);
-    long cn = std::max(nt, 1l) + std::max(nt, 1l) / 8, cb = std::max(bt, 1l) + 8,
-         cs = ns + 8;
-    uint64_t cc = std::max<uint64_t>(cells, 1);
+    // growth with head room, so that a batch whose membership changes every tick (a server)
+    // rarely reallocates
+    long cn = std::max(nt, 1l) + std::max(nt, 1l) / 2, cb = std::max(bt, 1l) + bt / 2 + 8,
+         cs = ns + ns / 2 + 8;
+    uint64_t cc = std::min<uint64_t>(std::max<uint64_t>(cells, 1) + cells / 4, 1ull << 32);
     size_t csort = ar_sort::layout(cn, 4, passes).total;
     bool ok = alloc(&B->keys, cn) && alloc(&B->skeys, cn) && alloc(&B->svals, cn) &&
               alloc(&B->spos, cn) && alloc(&B->svel, cn) && alloc(&B->pforce, cn) &&
               alloc(&B->cells, cc) && alloc(&B->sort_ws, csort) && alloc(&B->d_table, cs) &&
-              alloc(&B->d_poff, cs + 1) && alloc(&B->d_boff, cs + 1) && alloc(&B->d_prev_n, 1);
+              alloc(&B->d_poff, cs + 1) && alloc(&B->d_boff, cs + 1) && alloc(&B->d_prev_n, 1) &&
+              alloc(&B->d_pscene, cn) && alloc(&B->d_bscene, cb);
     if (!ok) {
       free_batch_buffers(B);
       arh::set_error("batch workspace allocation failed (%ld particles, %llu cells)", nt,
@@ -692,11 +730,38 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     }
   }
   if (ns > 0) {
-    cudaMemcpyAsync(B->d_table, tab.data(), tab.size() * sizeof(SceneDev), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(B->d_poff, poff.data(), poff.size() * sizeof(int), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(B->d_boff, boff.data(), boff.size() * sizeof(int), cudaMemcpyHostToDevice, st);
+    // table and offsets -> pinned staging -> device, ordered on the stream without a host
+    // wait for the steps in flight (they read the previous table; the copy lands after them).
+    // Two staging buffers alternate; a buffer is reused once its previous copy has run.
+    const size_t tab_b = tab.size() * sizeof(SceneDev), off_b = poff.size() * sizeof(int);
+    const size_t need = tab_b + 2 * off_b;
+    const int i = B->stage_i;
+    if (B->stage_ev[i]) cudaEventSynchronize(B->stage_ev[i]);
+    else cudaEventCreateWithFlags(&B->stage_ev[i], cudaEventDisableTiming);
+    if (need > B->h_stage_cap[i]) {
+      if (B->h_stage[i]) cudaFreeHost(B->h_stage[i]);
+      B->h_stage[i] = nullptr;
+      B->h_stage_cap[i] = 0;
+      if (cudaMallocHost((void**)&B->h_stage[i], 2 * need) != cudaSuccess) {
+        cudaGetLastError();
+        arh::set_error("batch prepare: pinned staging allocation failed");
+        return AR_ERR_OOM;
+      }
+      B->h_stage_cap[i] = 2 * need;
+    }
+    char* h = B->h_stage[i];
+    std::memcpy(h, tab.data(), tab_b);
+    std::memcpy(h + tab_b, poff.data(), off_b);
+    std::memcpy(h + tab_b + off_b, boff.data(), off_b);
+    cudaMemcpyAsync(B->d_table, h, tab_b, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(B->d_poff, h + tab_b, off_b, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(B->d_boff, h + tab_b + off_b, off_b, cudaMemcpyHostToDevice, st);
+    cudaEventRecord(B->stage_ev[i], st);
+    B->stage_i ^= 1;
+    const long m = std::max(nt, bt);
+    scene_ids_kernel<<<std::min(arh::grid_for(m, 256), 4096u), 256, 0, st>>>(
+        B->d_poff, B->d_boff, (int)ns, (int)nt, (int)bt, B->d_pscene, B->d_bscene);
   }
-  cudaStreamSynchronize(st);  // host vectors go out of scope
   B->nt = nt;
   B->bt = bt;
   B->total_cells = cells;
@@ -727,7 +792,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);
     mark(1);
     const unsigned gp = std::min(arh::grid_for(nt, 256), (unsigned)ctx->num_sms * 8);
-    morton_key_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->keys64);
+    morton_key_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->keys64, B->d_step);
     mark(2);
     ar_status s = ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
                                     B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
@@ -736,7 +801,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     bvh_build_kernel<<<arh::grid_for(std::max(nt - 1, 1), 256), 256, 0, st>>>(
         ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
         B->right, B->parent, B->min_r, B->max_r, B->nodes);
-    bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->svals, B->left,
+    bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->svals, B->left,
                                           B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
                                           B->min_r, B->max_r);
     bvh_roots_kernel<<<arh::grid_for(ns, 128), 128, 0, st>>>(B->d_poff, ns, nt, B->parent,
@@ -749,7 +814,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
         B->pforce, ctx->d_err);
     mark(5);
     reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
-        B->d_table, B->d_boff, ns, bt, B->pforce, ctx->d_err);
+        B->d_table, B->d_bscene, ns, bt, B->pforce, B->d_step, ctx->d_err);
     mark(6);
     return arh::check_launch("step (BVH)");
   }
@@ -758,8 +823,8 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   unsigned g1 = arh::grid_for(nt, kK1Threads);
   unsigned cap1 = (unsigned)ctx->num_sms * 4;
   repose_hash_kernel<<<g1 > cap1 ? cap1 : g1, kK1Threads, 0, st>>>(
-      B->d_table, B->d_poff, ns, nt, B->d_prev_n, B->skeys, B->cells, B->keys,
-      (uint32_t*)B->sort_ws, B->passes, B->last_bits);
+      B->d_table, B->d_pscene, ns, nt, B->d_prev_n, B->skeys, B->cells, B->keys,
+      (uint32_t*)B->sort_ws, B->passes, B->last_bits, B->d_step);
   mark(2);
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
                                   st, B->sort_ws, B->cap_sort, true);
@@ -767,7 +832,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   mark(3);
   unsigned g3 = arh::grid_for(nt, 256);
   unsigned cap3 = (unsigned)ctx->num_sms * 8;
-  scatter_kernel<<<g3 > cap3 ? cap3 : g3, 256, 0, st>>>(B->d_table, B->d_poff, ns, nt, B->skeys,
+  scatter_kernel<<<g3 > cap3 ? cap3 : g3, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->skeys,
                                                         B->svals, B->cells, B->spos, B->svel,
                                                         B->d_prev_n);
   mark(4);
@@ -775,7 +840,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
                                                        B->cells, B->spos, B->svel, B->pforce);
   mark(5);
   reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
-      B->d_table, B->d_boff, ns, bt, B->pforce, ctx->d_err);
+      B->d_table, B->d_bscene, ns, bt, B->pforce, B->d_step, ctx->d_err);
   mark(6);
   B->host_prev_n = nt;
   return arh::check_launch("step");
@@ -790,6 +855,7 @@ ar_status profile_steps(ar_batch* B, int n_steps, float* stage_ms, cudaStream_t 
   for (int i = 0; i < n_steps && s == AR_OK; ++i) {
     s = enqueue_step(B, st, ev);
     if (s != AR_OK) break;
+    ++B->host_step;
     if (cudaEventSynchronize(ev[kStages]) != cudaSuccess) {
       s = arh::check_launch("profile");
       break;
@@ -810,8 +876,10 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
   if (s != AR_OK) return s;
   if (B->nt == 0 || n_steps <= 0) return AR_OK;
   if (!use_graph) {
-    for (int i = 0; i < n_steps; ++i)
+    for (int i = 0; i < n_steps; ++i) {
       if ((s = enqueue_step(B, st)) != AR_OK) return s;
+      ++B->host_step;
+    }
     return AR_OK;
   }
   if (!B->graph) {
@@ -820,8 +888,8 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
       arh::set_error("capture stream creation failed");
       return AR_ERR_CUDA;
     }
-    // work already queued on `st` (table uploads, clears) must precede the graph
-    cudaStreamSynchronize(st);
+    // capture records without executing; the graph's launches on `st` are ordered after the
+    // work already queued there (table uploads, clears)
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
       arh::set_error("cudaStreamBeginCapture failed");
@@ -843,8 +911,10 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
       return AR_ERR_CUDA;
     }
   }
-  for (int i = 0; i < n_steps; ++i)
+  for (int i = 0; i < n_steps; ++i) {
     if (cudaGraphLaunch(B->graph, st) != cudaSuccess) return arh::check_launch("graph launch");
+    ++B->host_step;
+  }
   // only the grid step marks cells (the BVH step never writes the grid keys)
   if (B->broadphase == AR_BROADPHASE_GRID) B->host_prev_n = (int)B->nt;
   return arh::check_launch("graph launch");
@@ -946,14 +1016,34 @@ ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene
   s->n = n;
   s->nb = nb;
   scene_grid(D, s->origin, s->cell, s->gdim);
-  bool ok = alloc(&s->pos, nb) && alloc(&s->quat, nb) && alloc(&s->vel, nb) &&
-            alloc(&s->ang, nb) && alloc(&s->bforce, nb) && alloc(&s->btorque, nb) &&
-            alloc(&s->mass, nb) && alloc(&s->inv_inertia, 9 * (size_t)nb) &&
-            alloc(&s->offsets, nb + 1) && alloc(&s->rel, n);
-  if (!ok) {
+  cudaStream_t st = arh::stream(stream);
+  // one allocation from the stream-ordered pool (no device-wide synchronisation), carved into
+  // 256-byte aligned arrays
+  const size_t a6 = 16 * (size_t)nb, sizes[5] = {6 * ((a6 + 255) & ~(size_t)255),
+                                                 4 * (size_t)nb, 36 * (size_t)nb,
+                                                 4 * (size_t)(nb + 1), 16 * (size_t)n};
+  size_t total = 0;
+  for (size_t z : sizes) total += (z + 255) & ~(size_t)255;
+  if (cudaMallocAsync(&s->block, total, st) != cudaSuccess) {
+    cudaGetLastError();
+    s->block = nullptr;
     ar_scene_destroy(s);
     arh::set_error("ar_scene_create: out of device memory");
     return AR_ERR_OOM;
+  }
+  {
+    char* b = (char*)s->block;
+    const size_t s6 = (a6 + 255) & ~(size_t)255;
+    float4** arr6[6] = {&s->pos, &s->quat, &s->vel, &s->ang, &s->bforce, &s->btorque};
+    for (int i = 0; i < 6; ++i) *arr6[i] = (float4*)(b + i * s6);
+    b += (sizes[0] + 255) & ~(size_t)255;
+    s->mass = (float*)b;
+    b += (sizes[1] + 255) & ~(size_t)255;
+    s->inv_inertia = (float*)b;
+    b += (sizes[2] + 255) & ~(size_t)255;
+    s->offsets = (int32_t*)b;
+    b += (sizes[3] + 255) & ~(size_t)255;
+    s->rel = (float4*)b;
   }
   // particle rel with the body index in w
   std::vector<float4> rel(n);
@@ -964,7 +1054,6 @@ ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene
       std::memcpy(&w, &b, 4);
       rel[i] = make_float4(r[0], r[1], r[2], w);
     }
-  cudaStream_t st = arh::stream(stream);
   cudaMemcpyAsync(s->pos, init->body_pos4, 16 * (size_t)nb, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(s->quat, init->body_quat4, 16 * (size_t)nb, cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(s->vel, init->body_vel4, 16 * (size_t)nb, cudaMemcpyHostToDevice, st);
@@ -988,15 +1077,24 @@ ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene
 ar_status ar_scene_destroy(ar_scene* s) {
   if (!s) return AR_ERR_INVALID_ARG;
   if (s->solo) ar_batch_destroy(s->solo);
-  cudaFree(s->pos); cudaFree(s->quat); cudaFree(s->vel); cudaFree(s->ang);
-  cudaFree(s->bforce); cudaFree(s->btorque); cudaFree(s->mass); cudaFree(s->inv_inertia);
-  cudaFree(s->offsets); cudaFree(s->rel);
+  if (s->block) cudaFree(s->block);  // waits for the device, like any cudaFree
   delete s;
   return AR_OK;
 }
 
-ar_status ar_scene_download(ar_scene* s, float* h_pos4, float* h_quat4, float* h_vel4,
-                            float* h_ang4, ar_stream_t stream) {
+ar_status ar_scene_destroy_async(ar_scene* s, ar_stream_t stream) {
+  if (!s) return AR_ERR_INVALID_ARG;
+  if (s->solo) ar_batch_destroy(s->solo);
+  if (s->block && cudaFreeAsync(s->block, arh::stream(stream)) != cudaSuccess) {
+    delete s;
+    return arh::check_launch("ar_scene_destroy_async");
+  }
+  delete s;
+  return AR_OK;
+}
+
+ar_status ar_scene_download_async(ar_scene* s, float* h_pos4, float* h_quat4, float* h_vel4,
+                                  float* h_ang4, ar_stream_t stream) {
   if (!s) return AR_ERR_INVALID_ARG;
   cudaStream_t st = arh::stream(stream);
   const size_t bytes = 16 * (size_t)s->nb;
@@ -1004,7 +1102,14 @@ ar_status ar_scene_download(ar_scene* s, float* h_pos4, float* h_quat4, float* h
   if (h_quat4) cudaMemcpyAsync(h_quat4, s->quat, bytes, cudaMemcpyDeviceToHost, st);
   if (h_vel4) cudaMemcpyAsync(h_vel4, s->vel, bytes, cudaMemcpyDeviceToHost, st);
   if (h_ang4) cudaMemcpyAsync(h_ang4, s->ang, bytes, cudaMemcpyDeviceToHost, st);
-  cudaError_t e = cudaStreamSynchronize(st);
+  return arh::check_launch("ar_scene_download_async");
+}
+
+ar_status ar_scene_download(ar_scene* s, float* h_pos4, float* h_quat4, float* h_vel4,
+                            float* h_ang4, ar_stream_t stream) {
+  ar_status r = ar_scene_download_async(s, h_pos4, h_quat4, h_vel4, h_ang4, stream);
+  if (r != AR_OK) return r;
+  cudaError_t e = cudaStreamSynchronize(arh::stream(stream));
   if (e != cudaSuccess) {
     arh::set_error("ar_scene_download: %s", cudaGetErrorString(e));
     return AR_ERR_CUDA;
@@ -1114,6 +1219,14 @@ ar_status ar_batch_create(ar_ctx* ctx, ar_batch** out) {
   if (!ctx || !out) return AR_ERR_INVALID_ARG;
   ar_batch* B = new ar_batch();
   B->ctx = ctx;
+  if (cudaMalloc(&B->d_step, sizeof(long long)) != cudaSuccess ||
+      cudaMemset(B->d_step, 0, sizeof(long long)) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(B->d_step);
+    delete B;
+    arh::set_error("ar_batch_create: allocation failed");
+    return AR_ERR_OOM;
+  }
   *out = B;
   return AR_OK;
 }
@@ -1124,6 +1237,11 @@ ar_status ar_batch_destroy(ar_batch* B) {
   drop_graph(B);
   if (B->cap_stream) cudaStreamDestroy(B->cap_stream);
   free_batch_buffers(B);
+  cudaFree(B->d_step);
+  for (int i = 0; i < 2; ++i) {
+    if (B->h_stage[i]) cudaFreeHost(B->h_stage[i]);
+    if (B->stage_ev[i]) cudaEventDestroy(B->stage_ev[i]);
+  }
   delete B;
   return AR_OK;
 }
@@ -1138,7 +1256,18 @@ ar_status ar_batch_set_scenes(ar_batch* B, ar_scene* const* scenes, int n_scenes
     }
   }
   B->scenes.assign(scenes, scenes + n_scenes);
+  B->end_steps.clear();
   B->table_dirty = true;
+  return AR_OK;
+}
+
+ar_status ar_batch_set_scenes_limited(ar_batch* B, ar_scene* const* scenes, int n_scenes,
+                                      const int64_t* steps_left) {
+  ar_status s = ar_batch_set_scenes(B, scenes, n_scenes);
+  if (s != AR_OK || !steps_left) return s;
+  B->end_steps.resize(n_scenes);
+  for (int i = 0; i < n_scenes; ++i)
+    B->end_steps[i] = steps_left[i] < 0 ? LLONG_MAX : B->host_step + steps_left[i];
   return AR_OK;
 }
 

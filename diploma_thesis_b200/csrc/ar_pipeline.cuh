@@ -18,6 +18,7 @@ struct SceneDev {
   uint32_t lx, ly;          // log2 gx, log2 gy
   uint32_t cell_base;       // first cell of the scene in the batch's global cell space
   int poff, boff, n, nb;    // first particle / body in the batch, counts
+  long long end_step;       // last batch step that integrates the scene (then it is frozen)
   float4* pos;              // body centre (w unused)
   float4* quat;             // (x, y, z, w)
   float4* vel;

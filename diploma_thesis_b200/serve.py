@@ -1,28 +1,31 @@
 """Continuous-batching server for scene-step requests.
 
 A request is a new scene plus a number of steps K.  The server keeps every admitted scene
-resident on the device and, every tick:
+resident on the device and runs fixed-size ticks of ``tick_steps`` batch steps:
 
   1. admits waiting requests in arrival order while their footprint fits the HBM budget
      (``ar_scene_footprint``, which counts the scene's state and its share of the step
      workspace) and the batch stays within its particle and cell limits -- admission is
-     never blocked by a request that arrived later;
+     never blocked by a request that arrived later.  New scenes are uploaded on a separate
+     admission stream; the compute stream waits for the upload before the next tick;
   2. advances all resident scenes together as one batch (``ar_batch_step``: one launch per
-     stage, CUDA graph) by ``min(tick_steps, smallest remaining K)`` steps, so no scene is
-     stepped past its K;
-  3. retires finished scenes (their device memory is freed and reused by the next admissions)
-     and records completion times.
+     stage, CUDA graph) with a step budget per scene (``ar_batch_set_scenes_limited``): a
+     scene whose K runs out inside a tick is frozen on the device after exactly K steps;
+  3. queues, on the compute stream behind the tick, the copy of each finished scene's state
+     into pinned host memory; at the next member change the finished scenes leave the batch
+     and their memory is released in stream order (``ar_scene_destroy_async``) for the next
+     admissions.  A request completes when the host sees its copy done.
 
-Batching is continuous: a request arriving while others run joins the next tick without
-waiting for the batch to drain.  Because every scene occupies its own key range in the
-batch's sort, a scene's result does not depend on which other scenes shared its batches.
+The host never waits for the tick it has just queued: it runs at most ``max_inflight`` ticks
+ahead of the device, so admission (scene building and upload) overlaps device work.
+Because every scene occupies its own key range in the batch's sort and frozen scenes do not
+change, a scene's result does not depend on which other scenes shared its batches.
 
 Latency = completion - arrival (queueing + service).  Times are wall-clock on the host;
 arrivals are scheduled against the same clock.
 """
 from __future__ import annotations
 
-import contextlib
 import ctypes as C
 import heapq
 import time
@@ -80,12 +83,14 @@ class Server:
     Admission needs the request's footprint to fit the HBM budget and the resident batch to
     stay within the library's batch limits (AR_MAX_BATCH_PARTICLES particles and
     AR_MAX_BATCH_CELLS grid cells) and the optional ``max_batch_particles`` cap.
-    ``scene_factory(ctx, scene)`` and ``batch`` default to the device classes; they are
-    parameters so that the admission and tick logic can be driven by host-only stand-ins."""
+    ``scene_factory(ctx, scene, stream)``, ``batch`` and the streams default to the device
+    classes; they are parameters so that the admission and tick logic can be driven by
+    host-only stand-ins (objects with the same methods)."""
 
     def __init__(self, ctx, hbm_budget_bytes: float, tick_steps: int = 10,
                  keep_results: bool = False, max_batch_particles: int | None = None,
-                 broadphase: str = "grid", scene_factory=None, batch=None, stream=None):
+                 broadphase: str = "grid", scene_factory=None, batch=None, stream=None,
+                 admission_stream=None, max_inflight: int = 2):
         self.ctx = ctx
         self.budget = float(hbm_budget_bytes)
         self.tick_steps = int(tick_steps)
@@ -93,10 +98,13 @@ class Server:
         self.max_particles = min(int(max_batch_particles or AR_MAX_BATCH_PARTICLES),
                                  AR_MAX_BATCH_PARTICLES)
         self.broadphase = broadphase
+        self.max_inflight = max(1, int(max_inflight))
         self.scene_factory = scene_factory or (
-            lambda c, sc: api.GpuScene(c, sc, broadphase=self.broadphase))
+            lambda c, sc, st: api.GpuScene(c, sc, broadphase=self.broadphase, stream=st))
         self.batch = batch if batch is not None else api.Batch(ctx)
         self.stream = stream if stream is not None else torch.cuda.Stream()
+        self.adm_stream = admission_stream if admission_stream is not None else (
+            torch.cuda.Stream() if isinstance(self.stream, torch.cuda.Stream) else self.stream)
 
     def cost(self, scene: Scene) -> tuple[int, int]:
         """(device bytes, grid cells) a scene holds while resident."""
@@ -111,77 +119,112 @@ class Server:
         pending = list(requests)
         heapq.heapify(pending)
         waiting: list[Request] = []
-        active: list[list] = []  # [req, scene, remaining, (bytes, cells, particles)]
+        active: list[list] = []    # [req, scene, steps left, (bytes, cells, particles)]
+        retiring: list[list] = []  # [req, scene, need, host copy, copy-done event]
+        leaving: list = []         # finished scenes still members of the batch
+        inflight: list = []        # events of queued ticks, oldest first
         used = [0, 0, 0]
         done: list[Request] = []
         scene_steps = particle_steps = 0
         peak_res = peak_bytes = ticks = 0
-        phase = {"admit": 0.0, "set_scenes": 0.0, "step": 0.0, "retire": 0.0}
+        changed = False
+        phase = {"admit": 0.0, "set_scenes": 0.0, "step": 0.0, "retire": 0.0, "wait": 0.0}
         t0 = time.perf_counter()
-        stream_ctx = torch.cuda.stream(self.stream) if isinstance(self.stream, torch.cuda.Stream) \
-            else contextlib.nullcontext()
-        with stream_ctx:
-            while pending or waiting or active:
-                now = time.perf_counter() - t0
-                if time_limit is not None and now > time_limit and not active:
+        while pending or waiting or active or retiring:
+            now = time.perf_counter() - t0
+            while pending and pending[0].arrival <= now:
+                waiting.append(heapq.heappop(pending))
+            # ---- admission (overlaps the ticks in flight) ----
+            ta = time.perf_counter()
+            admitted = False
+            while waiting and (time_limit is None or now <= time_limit):
+                nbytes, cells = self.cost(waiting[0].scene)
+                need = (nbytes, cells, waiting[0].scene.num_particles)
+                if not self._fits(used, need):
+                    if active or retiring:
+                        break  # wait for resident scenes to retire
+                    if need[1] > AR_MAX_BATCH_CELLS or need[2] > self.max_particles:
+                        raise ValueError(f"request {waiting[0].rid} can never be admitted")
+                req = waiting.pop(0)
+                gs = self.scene_factory(self.ctx, req.scene, self.adm_stream)
+                req.admitted = time.perf_counter() - t0
+                active.append([req, gs, req.steps, need])
+                used = [u + x for u, x in zip(used, need)]
+                admitted = changed = True
+            if admitted and self.adm_stream is not self.stream:
+                self.stream.wait_event(self.adm_stream.record_event())
+            phase["admit"] += time.perf_counter() - ta
+            # ---- retire: finished copies the host can see ----
+            tr = time.perf_counter()
+            still = []
+            for item in retiring:
+                req, gs, need, host, ev = item
+                if ev.query():
+                    req.done = time.perf_counter() - t0
+                    if self.keep_results:
+                        req.result = {k: v.copy() for k, v in host.items() if k != "_pinned"}
+                    used = [u - x for u, x in zip(used, need)]
+                    done.append(req)
+                else:
+                    still.append(item)
+            retiring = still
+            phase["retire"] += time.perf_counter() - tr
+            if not active:
+                if retiring:  # nothing to step: wait for the oldest copy
+                    tw = time.perf_counter()
+                    retiring[0][4].synchronize()
+                    phase["wait"] += time.perf_counter() - tw
+                elif pending:  # idle until the next arrival
+                    time.sleep(max(0.0, min(0.001, pending[0].arrival - now)))
+                elif time_limit is not None and now > time_limit:
                     break
-                while pending and pending[0].arrival <= now:
-                    waiting.append(heapq.heappop(pending))
+                if leaving and not active:
+                    self.batch.set_scenes([])
+                    for gs in leaving:
+                        gs.close_async(self.stream)
+                    leaving = []
+                continue
+            # ---- queue one tick ----
+            tb = time.perf_counter()
+            if changed or ticks == 0:
+                self.batch.set_scenes([a[1] for a in active], [a[2] for a in active])
                 changed = False
-                while waiting and (time_limit is None or now <= time_limit):
-                    nbytes, cells = self.cost(waiting[0].scene)
-                    need = (nbytes, cells, waiting[0].scene.num_particles)
-                    if not self._fits(used, need):
-                        if active:
-                            break  # wait for resident scenes to retire
-                        if need[1] > AR_MAX_BATCH_CELLS or need[2] > self.max_particles:
-                            raise ValueError(f"request {waiting[0].rid} can never be admitted")
-                    req = waiting.pop(0)
-                    ta = time.perf_counter()
-                    gs = self.scene_factory(self.ctx, req.scene)
-                    phase["admit"] += time.perf_counter() - ta
-                    req.admitted = time.perf_counter() - t0
-                    active.append([req, gs, req.steps, need])
-                    used = [u + x for u, x in zip(used, need)]
-                    changed = True
-                if not active:
-                    if pending:  # idle until the next arrival
-                        time.sleep(max(0.0, min(0.001, pending[0].arrival - now)))
-                    continue
-                tb = time.perf_counter()
-                if changed or ticks == 0:
-                    self.batch.set_scenes([a[1] for a in active])
-                k = min(self.tick_steps, min(a[2] for a in active))
-                tc = time.perf_counter()
-                self.batch.step(k, use_graph=True, stream=self.stream)
-                td = time.perf_counter()
-                phase["set_scenes"] += tc - tb
-                phase["step"] += td - tc
-                ticks += 1
-                peak_res = max(peak_res, len(active))
-                peak_bytes = max(peak_bytes, used[0])
-                finished = []
-                for a in active:
-                    scene_steps += k
-                    particle_steps += k * a[0].scene.num_particles
-                    a[2] -= k
-                    if a[2] <= 0:
-                        finished.append(a)
-                if finished:
-                    tr = time.perf_counter()
-                    self.stream.synchronize()
-                    tdone = time.perf_counter() - t0
-                    for req, gs, _, need in finished:
-                        req.done = tdone
-                        if self.keep_results:
-                            req.result = gs.download()
-                        gs.close()
-                        used = [u - x for u, x in zip(used, need)]
-                        done.append(req)
-                    active = [a for a in active if a[2] > 0]
-                    self.batch.set_scenes([a[1] for a in active])
-                    phase["retire"] += time.perf_counter() - tr
-            self.stream.synchronize()
+                for gs in leaving:  # no longer members: free behind the ticks that used them
+                    gs.close_async(self.stream)
+                leaving = []
+            phase["set_scenes"] += time.perf_counter() - tb
+            tw = time.perf_counter()
+            while len(inflight) >= self.max_inflight:
+                inflight.pop(0).synchronize()
+            phase["wait"] += time.perf_counter() - tw
+            tc = time.perf_counter()
+            k = self.tick_steps
+            self.batch.step(k, use_graph=True, stream=self.stream)
+            ticks += 1
+            peak_res = max(peak_res, len(active))
+            peak_bytes = max(peak_bytes, used[0])
+            finished = []
+            for a in active:
+                n = min(k, a[2])
+                scene_steps += n
+                particle_steps += n * a[0].scene.num_particles
+                a[2] -= k
+                if a[2] <= 0:
+                    finished.append(a)
+            for req, gs, _, need in finished:  # frozen on the device after exactly K steps
+                host = gs.download_async(self.stream)
+                retiring.append([req, gs, need, host, self.stream.record_event()])
+                leaving.append(gs)
+            if finished:
+                active = [a for a in active if a[2] > 0]
+                changed = True
+            inflight.append(self.stream.record_event())
+            phase["step"] += time.perf_counter() - tc
+        if leaving:
+            self.batch.set_scenes([])
+            for gs in leaving:
+                gs.close_async(self.stream)
+        self.stream.synchronize()
         wall = time.perf_counter() - t0
         self.ctx.check(self.stream)
         lat = np.array([r.done - r.arrival for r in done])

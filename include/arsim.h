@@ -416,6 +416,12 @@ AR_API ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc,
                                  const ar_scene_init* init, ar_stream_t stream,
                                  ar_scene** out);
 AR_API ar_status ar_scene_destroy(ar_scene* scene);
+/* Release a scene's device memory in stream order (cudaFreeAsync on `stream`), without a
+ * host or device-wide synchronisation.  Every use of the scene must be ordered before this
+ * point of `stream` (e.g. the scene was removed from its batches before the batch's next step
+ * on that stream).  Scene memory comes from the device's stream-ordered pool, so a server can
+ * admit and retire scenes while steps run. */
+AR_API ar_status ar_scene_destroy_async(ar_scene* scene, ar_stream_t stream);
 /* Device bytes a scene with this description keeps resident (state + its share of the
  * step workspace); used for HBM-budget admission. */
 AR_API size_t ar_scene_footprint(const ar_scene_desc* desc);
@@ -429,6 +435,12 @@ AR_API uint64_t ar_scene_cells(const ar_scene_desc* desc);
 AR_API ar_status ar_scene_download(ar_scene* scene, float* h_body_pos4, float* h_body_quat4,
                                    float* h_body_vel4, float* h_body_angvel4,
                                    ar_stream_t stream);
+/* The same without the synchronisation: the copies are queued on the stream (truly
+ * asynchronous into pinned host memory); the arrays are valid once the stream has reached
+ * this point. */
+AR_API ar_status ar_scene_download_async(ar_scene* scene, float* h_body_pos4,
+                                         float* h_body_quat4, float* h_body_vel4,
+                                         float* h_body_angvel4, ar_stream_t stream);
 /* Overwrite body state from host arrays (any may be NULL); asynchronous (use pinned memory
  * for overlap).  Replaces the reference's per-step host round trip of body state
  * (Particles/updateFunctions.cpp:2903-2930). */
@@ -503,8 +515,17 @@ AR_API ar_status ar_scene_particle_forces(ar_scene* scene, float* p_force4, floa
 typedef struct ar_batch ar_batch;
 AR_API ar_status ar_batch_create(ar_ctx* ctx, ar_batch** out);
 AR_API ar_status ar_batch_destroy(ar_batch* batch);
-/* Replace the batch's member list (scenes stay resident and owned by the caller). */
+/* Replace the batch's member list (scenes stay resident and owned by the caller).  All
+ * scenes of a batch use one broad phase.  Changing the list costs no host synchronisation
+ * unless the batch's workspace has to grow. */
 AR_API ar_status ar_batch_set_scenes(ar_batch* batch, ar_scene* const* scenes, int n_scenes);
+/* The same with a step budget per scene: scene i is integrated by at most steps_left[i] of the
+ * batch's following steps (< 0: no limit) and is frozen afterwards -- it still takes part in
+ * the broad phase, but its state no longer changes, so it may be read (or removed at the next
+ * member change) while later steps run.  A frozen scene's state equals that of the scene
+ * stepped alone steps_left[i] times.  Used by a server that steps fixed-size ticks. */
+AR_API ar_status ar_batch_set_scenes_limited(ar_batch* batch, ar_scene* const* scenes,
+                                             int n_scenes, const int64_t* steps_left);
 AR_API ar_status ar_batch_step(ar_ctx* ctx, ar_batch* batch, int n_steps, int use_graph,
                                ar_stream_t stream);
 /* ar_step_profile for a batch. */

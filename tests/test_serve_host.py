@@ -14,13 +14,14 @@ class FakeScene:
         self.scene = scene
         self.num_particles = scene.num_particles
         self.steps = 0
+        self.budget = None
         self.closed = False
         log.append(self)
 
-    def download(self):
-        return {"steps": self.steps}
+    def download_async(self, stream=None):
+        return {"steps": np.array(self.steps)}
 
-    def close(self):
+    def close_async(self, stream=None):
         self.closed = True
 
 
@@ -30,15 +31,23 @@ class FakeBatch:
         self.ticks = []
         self.delay = 0.0
 
-    def set_scenes(self, members):
+    def set_scenes(self, members, steps_left=None):
         assert len({id(m) for m in members}) == len(members)
+        for m in members:
+            assert not m.closed
         self.members = list(members)
+        for i, m in enumerate(self.members):
+            m.budget = None if steps_left is None else int(steps_left[i])
 
     def step(self, k, use_graph=True, stream=None):
+        """Scenes with a budget are integrated by at most that many steps, then frozen."""
         assert k >= 1
         for m in self.members:
             assert not m.closed
-            m.steps += k
+            n = k if m.budget is None else max(0, min(k, m.budget))
+            m.steps += n
+            if m.budget is not None:
+                m.budget -= n
         self.ticks.append((k, [id(m) for m in self.members]))
         if self.delay:
             time.sleep(self.delay)
@@ -47,8 +56,22 @@ class FakeBatch:
         pass
 
 
+class FakeEvent:
+    def query(self):
+        return True
+
+    def synchronize(self):
+        pass
+
+
 class FakeStream:
     def synchronize(self):
+        pass
+
+    def record_event(self):
+        return FakeEvent()
+
+    def wait_event(self, ev):
         pass
 
 
@@ -61,7 +84,7 @@ def _server(budget, **kw):
     log = []
     batch = FakeBatch()
     srv = serve.Server(FakeCtx(), budget, tick_steps=4, keep_results=True,
-                       scene_factory=lambda c, sc: FakeScene(sc, log), batch=batch,
+                       scene_factory=lambda c, sc, st: FakeScene(sc, log), batch=batch,
                        stream=FakeStream(), **kw)
     return srv, batch, log
 
@@ -78,7 +101,7 @@ def test_every_request_gets_exactly_k_steps():
     stats = srv.run(reqs)
     assert stats.completed == 12
     for r in reqs:
-        assert r.result["steps"] == r.steps
+        assert int(r.result["steps"]) == r.steps
         assert r.done >= r.admitted >= r.arrival - 1e-9
     assert all(s.closed for s in log)
     assert stats.scene_steps == sum(r.steps for r in reqs)
@@ -129,3 +152,15 @@ def test_request_that_can_never_fit_is_an_error():
     srv, batch, log = _server(1e12, max_batch_particles=1)
     with pytest.raises(ValueError):
         srv.run(reqs)
+
+
+def test_frozen_scenes_leave_and_are_freed_after_the_next_member_change():
+    rng = np.random.default_rng(3)
+    reqs = _requests(8, rng.integers(1, 25, 8), spread=0.0)
+    srv, batch, log = _server(1e12)
+    srv.tick_steps = 7
+    stats = srv.run(reqs)
+    assert stats.completed == 8
+    for r in reqs:  # budgets freeze every scene after exactly K steps, whatever the tick size
+        assert int(r.result["steps"]) == r.steps
+    assert all(s.closed for s in log) and batch.members == []
