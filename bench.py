@@ -38,52 +38,69 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Algorithmic bytes per particle and per body for each stage of the fused step (compulsory
 # traffic of this design: every array element read or written once; neighbour reads that hit
-# in L2 are not counted).  P = sort passes, ppb = particles per body.
-STAGES = ["clear", "repose_hash", "sort", "scatter", "collide", "reduce_integrate"]
+# in L2 are not counted).  P = sort passes, ppb = particles per body.  A step runs: sort |
+# scatter + cell table | collide | clear | body (sums, integration, next step's keys).
+STAGES = ["sort", "scatter", "collide", "clear", "body", "none"]
+BODY_STATE = 16 * 4  # pos, quat, vel, angvel (float4 each)
+
+
+def _body_bytes(nb: int) -> int:
+    # state + mass + inverse inertia in, state + force / torque sums out
+    return nb * (BODY_STATE + 4 + 36 + BODY_STATE + 32)
 
 
 def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int) -> dict[str, float]:
-    body_state = 16 * 4  # pos, quat, vel, angvel (float4 each)
+    tiles = (n + 4095) // 4096
     return {
-        # sort workspace head (histograms + look-back status), written once
-        "clear": 4 * 256 * 8 + passes * 4 * 256 * ((n + 4095) // 4096),
-        # read rel (16) + previous sorted key (4), write key (4); body pose (32) per body;
-        # reset of the previous step's occupied cells (4 each)
-        "repose_hash": n * (16 + 4 + 4) + nb * 32 + occupied_cells * 4,
         # first pass reads the key only; every pass writes key + index; later passes read both
-        "sort": n * (4 + 8) + (passes - 1) * n * 16 + passes * 4 * 256 * ((n + 4095) // 4096),
-        # read sorted key + index (8) and rel (16); write sorted pos + vel (32); body state per
-        # body; cell (start, end) per occupied cell
-        "scatter": n * (8 + 16 + 32) + nb * body_state + occupied_cells * 8,
-        # own index (4), position + velocity (32); force (16) out
-        "collide": n * (4 + 32 + 16),
-        # force + rel (32) in; body state + mass + inverse inertia in, body state + sums out
-        "reduce_integrate": n * 32 + nb * (body_state + 4 + 36 + body_state + 32),
+        "sort": n * (4 + 8) + (passes - 1) * n * 16 + passes * 4 * 256 * tiles,
+        # sorted key + index and rel in, sorted position + velocity out; body state per body;
+        # one 16-byte cell entry per occupied cell
+        "scatter": n * (8 + 16 + 32) + nb * BODY_STATE + occupied_cells * 16,
+        # own key, index, position, velocity in; force out
+        "collide": n * (4 + 4 + 32 + 16),
+        # next sort's histogram / look-back head
+        "clear": 4 * 256 * 8 + passes * 4 * 256 * tiles,
+        # force + rel in, next key out; sorted key in and one reset per occupied cell
+        "body": n * (16 + 16 + 4 + 4) + occupied_cells * 4 + _body_bytes(nb),
+        "none": 0,
     }
 
 
-BVH_STAGES = ["clear", "morton", "sort", "tree", "collide", "reduce_integrate"]
+BVH_STAGES = ["sort", "tree", "collide", "clear", "body", "none"]
 
 
 def stage_bytes_bvh(n: int, nb: int, passes: int) -> dict[str, float]:
-    """The same accounting for the BVH broad phase (64-bit keys, 32-byte node boxes)."""
-    body_state = 16 * 4
+    """The same accounting for the BVH broad phase (64-bit keys, 64-byte wide nodes)."""
     tiles = (n + 4095) // 4096
     return {
-        "clear": 4 * n,  # refit arrival counters
-        # read rel (16), write key (8); body pose (32) per body
-        "morton": n * (16 + 8) + nb * 32,
         # histogram pass reads the keys; first pass reads keys, every pass writes key + index,
         # later passes read both
         "sort": n * 8 + n * (8 + 12) + (passes - 1) * n * 24 + passes * 4 * 256 * tiles,
-        # leaves: index, rel in; sorted pos + vel, box, flags, ranges out; nodes: keys in,
-        # flags, children, parent, ranges out; refit: links and child boxes in, box out
-        "tree": n * (4 + 16 + 32 + 32 + 9) + nb * body_state + n * (8 + 21 + 8) +
-                n * (12 + 64 + 32),
-        # own index, position + velocity, box; force out
-        "collide": n * (4 + 32 + 32 + 16),
-        "reduce_integrate": n * 32 + nb * (body_state + 4 + 36 + body_state + 32),
+        # nodes: keys in, flags, children, parent, ranges and wide-node ids out; leaves: index,
+        # rel in, sorted pos + vel and the leaf box out, body state per body; refit: links and
+        # the node's two child boxes in, its box out
+        "tree": n * (8 + 21 + 8 + 8) + n * (4 + 16 + 32 + 24 + 9) + nb * BODY_STATE +
+                n * (8 + 64 + 24),
+        # own index, position + velocity in; force out
+        "collide": n * (4 + 32 + 16),
+        "clear": 4 * n,  # refit arrival counters
+        "body": n * (16 + 16 + 8) + _body_bytes(nb),
+        "none": 0,
     }
+
+
+TRAFFIC = ROOT / "profiles" / "traffic.json"
+
+
+def measured_traffic(workload: str, broadphase: str, kernel: str):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu capture of this
+    workload (profiles/traffic.json), with the capture it came from; None when there is none."""
+    try:
+        t = json.loads(TRAFFIC.read_text())[f"{workload}/{broadphase}/{kernel}"]
+        return t["bytes_per_launch"], t["source"]
+    except Exception:
+        return None, None
 
 
 def peaks() -> tuple[float, str]:
@@ -162,7 +179,9 @@ def make_scene(workload: str):
     raise SystemExit(f"unknown workload {workload}")
 
 
-def dist_setup(ngpus: int):
+def dist_setup(ngpus: int, backend: str = "nccl"):
+    """Replicas: one process per GPU (RANK / LOCAL_RANK / WORLD_SIZE from torchrun); the
+    process group only carries the barrier and the max-over-ranks timing, never data."""
     import torch
     import torch.distributed as dist
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -170,9 +189,12 @@ def dist_setup(ngpus: int):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
-                                device_id=torch.device(f"cuda:{local}"))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                    device_id=torch.device(f"cuda:{local}"))
+        else:
+            dist.init_process_group(backend, timeout=timedelta(seconds=60))
     return world, rank, local
 
 
@@ -187,9 +209,16 @@ def max_over_ranks(x: float, world: int) -> float:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(world: int, units_per_rank: int, steps: int, ms: float) -> float:
+    """Whole-job throughput in millions of units per second: every rank processes
+    units_per_rank per step, the time is the slowest rank's."""
+    return world * units_per_rank * steps / (ms / 1e3) / 1e6
 
 
 # ---- CPU legs (oracle) ---------------------------------------------------------------------
@@ -353,7 +382,7 @@ def run_ours(args):
         ctx.check(stream)
     ms = max_over_ranks(ms, world)
     ms_per_step = ms / args.steps
-    value = world * n * args.steps / (ms / 1e3) / 1e6
+    value = job_rate(world, n, args.steps, ms)
 
     # ---- stage profile (event-bracketed eager steps right after the timed region) ----
     with torch.cuda.stream(stream):
@@ -372,6 +401,7 @@ def run_ours(args):
     hbm, peak_kind = peaks()
     dom = max(range(len(names)), key=lambda i: stage_ms[i])
     dom_name = names[dom]
+    traffic, traffic_src = measured_traffic(args.workload, args.broadphase, dom_name)
     achieved = sbytes[dom_name] / (stage_ms[dom] / 1e3) / 1e9
     step_bytes = sum(sbytes.values())
     step_ms_prof = sum(stage_ms)
@@ -406,7 +436,7 @@ def run_ours(args):
             cpu_baseline = {"value": rate / 1e6, "unit": "Mparticle-steps/s", "cores": cores,
                             "kind": kind, "sample": sample}
 
-    memsets = 2 if args.broadphase == "bvh" else 1  # memset nodes are not kernels
+    memsets = 2 if args.broadphase == "bvh" else 1  # memset nodes are not kernels (steady step)
     launches = args.steps * (gs.launches_per_step() - memsets)
     if rank == 0:
         line = {
@@ -421,7 +451,8 @@ def run_ours(args):
                        "timed": "CUDA graph replays, events on the launching stream"},
             "roofline": {"bound": "hbm", "kernel": dom_name, "achieved": achieved,
                          "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "peak_kind": f"{peak_kind} hbm_gbs", "traffic": None,
+                         "peak_kind": f"{peak_kind} hbm_gbs", "traffic": traffic,
+                         "traffic_source": traffic_src,
                          "algorithmic_bytes_per_launch": sbytes[dom_name],
                          "launch_ms": stage_ms[dom]},
             "step_roofline": {"achieved": step_bytes / (ms_per_step / 1e3) / 1e9, "peak": hbm,
@@ -596,8 +627,8 @@ def run_lbvh(args):
                 def refit():
                     call("ar_lbvh_leaves", ctx.handle, n, P(svals), P(pts), 1e-3, P(leaf),
                          P(t["min_r"]), P(t["max_r"]), P(cms), P(bounds), P(radii), st)
-                    call("ar_lbvh_refit", ctx.handle, n, P(t["left"]), P(t["right"]),
-                         P(t["parent"]), P(bounds), st)
+                    call("ar_lbvh_refit_ranged", ctx.handle, n, P(t["left"]), P(t["right"]),
+                         P(t["parent"]), P(t["min_r"]), P(t["max_r"]), P(bounds), st)
 
                 stages = {"encode": encode, "sort": sort, "build": build, "refit": refit}
                 times = {k: [] for k in stages}

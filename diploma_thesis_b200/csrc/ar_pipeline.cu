@@ -59,68 +59,59 @@ __global__ void __launch_bounds__(256) scene_ids_kernel(const int* __restrict__ 
   }
 }
 
-// ---- K0: reset the cells a previous layout touched -------------------------------------------
-__global__ void __launch_bounds__(256) clear_cells_kernel(const uint32_t* __restrict__ skeys,
-                                                          int prev_n, uint2* __restrict__ cells) {
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < prev_n; g += gridDim.x * blockDim.x) {
-    const uint32_t k0 = skeys[g];
-    if (g == 0 || k0 != skeys[g - 1]) cells[k0].x = ar::kEmpty;
-  }
-}
-
-// ---- K1: re-pose + hash + sort histogram -----------------------------------------------------
-__global__ void __launch_bounds__(kK1Threads) repose_hash_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
-    int* __restrict__ d_prev_n, const uint32_t* __restrict__ prev_skeys, uint2* __restrict__ cells,
-    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits,
-    long long* __restrict__ d_step) {
-  __shared__ uint32_t s_hist[4][256];
-  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
+// ---- prologue: cell keys + sort histogram from the current body state ----------------------
+// Steps compute the next step's keys at their end (body_step_kernel); this kernel computes
+// them only when the state did not come from a step (a new member list, an upload).
+__global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
+    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits) {
+  __shared__ uint32_t s_hist[ar_sort::kMaxPasses][256];
   for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
-  const int prev_n = *d_prev_n;
-  const int lim = nt > prev_n ? nt : prev_n;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < lim; g += gridDim.x * blockDim.x) {
-    if (g < prev_n) {
-      const uint32_t k0 = __ldg(prev_skeys + g);
-      if (g == 0 || k0 != __ldg(prev_skeys + g - 1)) cells[k0].x = ar::kEmpty;
-    }
-    if (g < nt) {
-      const SceneDev& S = table[__ldg(pscene + g)];
-      const int i = g - S.poff;
-      const float4 r4 = __ldg(S.rel + i);
-      const int b = __float_as_int(r4.w);
-      float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
-      float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
-      const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
-      keys[g] = key;
-      ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
-    }
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
+    const SceneDev& S = table[__ldg(pscene + g)];
+    const int i = g - S.poff;
+    const float4 r4 = __ldg(S.rel + i);
+    const int b = __float_as_int(r4.w);
+    const float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
+    const float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
+    const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
+    keys[g] = key;
+    ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
   }
   __syncthreads();
   ar_sort::hist_flush(s_hist, ws_hist, passes);
 }
 
-// ---- K3: scatter + cell ranges ------------------------------------------------------------
+// ---- K3: scatter + cell table -------------------------------------------------------------
+// Cell entry = {first sorted slot, end slot, body tag, 0}; the tag is the global body id when
+// every occupant belongs to one body (else kEmpty), so that a particle skips a neighbour cell
+// of its own body without loading its occupants (they could only be rejected).  The thread
+// at a cell's first slot writes the whole entry.
 __global__ void __launch_bounds__(256) scatter_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
     const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
-    uint2* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
-    int* __restrict__ d_prev_n) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *d_prev_n = nt;
+    uint4* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
+    long long* __restrict__ d_step) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const uint32_t key = __ldg(skeys + k);
-    if (k == 0 || key != __ldg(skeys + k - 1)) {
-      cells[key].x = (uint32_t)k;
-      if (k > 0) cells[__ldg(skeys + k - 1)].y = (uint32_t)k;
-    }
-    if (k == nt - 1) cells[key].y = (uint32_t)nt;
     const int g = (int)__ldg(svals + k);
     const int sc = __ldg(pscene + g);
     const SceneDev& S = table[sc];
     const int i = g - S.poff;
     const float4 r4 = __ldg(S.rel + i);
     const int b = __float_as_int(r4.w);
+    if (k == 0 || key != __ldg(skeys + k - 1)) {
+      // occupants of one cell belong to one scene
+      uint32_t tag = (uint32_t)(S.boff + b);
+      int e = k + 1;
+      for (; e < nt && __ldg(skeys + e) == key; ++e) {
+        const int ge = (int)__ldg(svals + e);
+        if (__float_as_int(__ldg(S.rel + (ge - S.poff)).w) != b) tag = ar::kEmpty;
+      }
+      cells[key] = make_uint4((uint32_t)k, (uint32_t)e, tag, 0u);
+    }
     float3 r, p, v;
     ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
                     ar::mk3(r4.x, r4.y, r4.z), &r, &p, &v);
@@ -134,19 +125,20 @@ __global__ void __launch_bounds__(256) scatter_kernel(
 // skipping its own body (itself included); per-cell partial sums added to the total (the order
 // of FindAndHandleRigidBodyCollisionsUniformGridKernel, RigidBodies/UniformGridDEM.cu:166-193).
 // The particle's cell comes from its sorted key and its scene from the sorted velocity's w.
-// Three cells of an x-row that do not wrap have consecutive keys, so their occupants form one
-// contiguous run of the sorted arrays: the row is walked as that run, and a contact goes to
-// the partial sum of the cell whose sub-range holds it.  Rows that wrap in x walk the three
-// ranges one after the other.  The next row's cell entries are loaded before the current row
-// is walked.  Candidates at squared distance >= the float just above (2r)^2 are rejected
-// without the square root: for them sqrtf(d2) >= 2r exactly, so the contact test is unchanged.
+// The three cells of an x-row are walked as one flattened loop (candidate t of the row maps to
+// cell a, b or c and to that cell's partial sum), so a warp's lanes stay in step across cells;
+// cells that hold only this particle's body are skipped from their tag without loading their
+// occupants, which could only be rejected.  The next row's cell entries are loaded before the
+// current row is walked.  Candidates at squared distance >= the float just above (2r)^2 are
+// rejected without the square root: for them sqrtf(d2) >= 2r exactly, so the contact test is
+// unchanged.
 struct RowCells {
-  uint2 a, b, c;
+  uint4 a, b, c;
 };
 
 __global__ void __launch_bounds__(256, 4) collide_kernel(
     const SceneDev* __restrict__ table, int nt, const uint32_t* __restrict__ skeys,
-    const uint32_t* __restrict__ svals, const uint2* __restrict__ cells,
+    const uint32_t* __restrict__ svals, const uint4* __restrict__ cells,
     const float4* __restrict__ spos, const float4* __restrict__ svel,
     float4* __restrict__ pforce) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -163,53 +155,37 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
   const uint32_t base = S.cell_base, local = __ldg(skeys + k) - base;
   const uint32_t x = local & mx, y = (local >> lx) & my, z = local >> (lx + ly);
   const uint32_t xa = (x - 1) & mx, xc = (x + 1) & mx;
-  const bool straight = x >= 1 && x + 1 <= mx;  // x-1, x, x+1 have consecutive keys
   auto row_of = [&](int r) {  // r = 3 (dz + 1) + (dy + 1)
     const uint32_t zz = (z + (uint32_t)(r / 3) - 1u) & mz, yy = (y + (uint32_t)(r % 3) - 1u) & my;
     const uint32_t row = base + (zz << (lx + ly)) + (yy << lx);
     return RowCells{__ldg(cells + row + xa), __ldg(cells + row + x), __ldg(cells + row + xc)};
   };
-  auto contact = [&](uint32_t j, float3* f) {
-    const float4 q4 = __ldg(spos + j);
-    if (__float_as_int(q4.w) == body) return false;
-    const float3 rp = ar::sub(ar::xyz(q4), pos);
-    const float d2 = ar::dot(rp, rp);
-    if (!(d2 < thr2_up)) return false;
-    const float dist = sqrtf(d2);
-    if (!(dist < thr)) return false;
-    const float3 v2 = ar::xyz(__ldg(svel + j));
-    *f = ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att);
-    return true;
+  // occupants to visit: none for an empty cell or a cell holding only this particle's body
+  auto visits = [&](const uint4& c) {
+    return (c.x == ar::kEmpty || c.z == (uint32_t)body) ? 0u : c.y - c.x;
   };
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
   RowCells next = row_of(0);
   for (int r = 0; r < 9; ++r) {
     const RowCells cur = next;
     if (r < 8) next = row_of(r + 1);
-    const uint32_t na = cur.a.x == ar::kEmpty ? 0u : cur.a.y - cur.a.x;
-    const uint32_t nb = cur.b.x == ar::kEmpty ? 0u : cur.b.y - cur.b.x;
-    const uint32_t nc = cur.c.x == ar::kEmpty ? 0u : cur.c.y - cur.c.x;
+    const uint32_t na = visits(cur.a), nb = visits(cur.b), nc = visits(cur.c);
+    const uint32_t nab = na + nb, total = nab + nc;
     float3 fa = ar::mk3(0.f, 0.f, 0.f), fb = fa, fc = fa;
-    float3 f;
-    if (straight) {
-      // first occupant of the run, and the ends of cells a and b within it
-      const uint32_t j0 = na ? cur.a.x : (nb ? cur.b.x : cur.c.x);
-      const uint32_t ea = j0 + na, eb = ea + nb, e = eb + nc;
-      for (uint32_t j = j0; j < e; ++j) {
-        if (!contact(j, &f)) continue;
-        if (j < ea) fa = ar::add(fa, f);
-        else if (j < eb) fb = ar::add(fb, f);
-        else fc = ar::add(fc, f);
-      }
-    } else {
-      const uint32_t nab = na + nb, total = nab + nc;
-      for (uint32_t t = 0; t < total; ++t) {
-        const uint32_t j = t < na ? cur.a.x + t : (t < nab ? cur.b.x + (t - na) : cur.c.x + (t - nab));
-        if (!contact(j, &f)) continue;
-        if (t < na) fa = ar::add(fa, f);
-        else if (t < nab) fb = ar::add(fb, f);
-        else fc = ar::add(fc, f);
-      }
+    for (uint32_t t = 0; t < total; ++t) {
+      const uint32_t j = t < na ? cur.a.x + t : (t < nab ? cur.b.x + (t - na) : cur.c.x + (t - nab));
+      const float4 q4 = __ldg(spos + j);
+      if (__float_as_int(q4.w) == body) continue;
+      const float3 rp = ar::sub(ar::xyz(q4), pos);
+      const float d2 = ar::dot(rp, rp);
+      if (!(d2 < thr2_up)) continue;
+      const float dist = sqrtf(d2);
+      if (!(dist < thr)) continue;
+      const float3 v2 = ar::xyz(__ldg(svel + j));
+      const float3 f = ar_dem::spring_force(rp, dist, ar::sub(v2, vel), thr, kk, dmp, shr, att);
+      if (t < na) fa = ar::add(fa, f);
+      else if (t < nab) fb = ar::add(fb, f);
+      else fc = ar::add(fc, f);
     }
     lin = ar::add(lin, fa);
     lin = ar::add(lin, fb);
@@ -236,11 +212,19 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   return v;
 }
 
+__device__ __forceinline__ uint64_t morton_key(const SceneDev& S, int s, float3 p) {
+  const float x = (p.x - S.bmin[0]) / (S.bmax[0] - S.bmin[0]);
+  const float y = (p.y - S.bmin[1]) / (S.bmax[1] - S.bmin[1]);
+  const float z = (p.z - S.bmin[2]) / (S.bmax[2] - S.bmin[2]);
+  const uint32_t code = (spread10((uint32_t)fminf(fmaxf(x * 1024.0f, 0.0f), 1023.0f)) << 2) |
+                        (spread10((uint32_t)fminf(fmaxf(y * 1024.0f, 0.0f), 1023.0f)) << 1) |
+                        spread10((uint32_t)fminf(fmaxf(z * 1024.0f, 0.0f), 1023.0f));
+  return ((uint64_t)s << kMortonBits) | code;
+}
+
 __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restrict__ table,
                                                          const int* __restrict__ pscene, int ns,
-                                                         int nt, uint64_t* __restrict__ keys,
-                                                         long long* __restrict__ d_step) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
+                                                         int nt, uint64_t* __restrict__ keys) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
     const int s = __ldg(pscene + g);
     const SceneDev& S = table[s];
@@ -248,13 +232,7 @@ __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restr
     const int b = __float_as_int(r4.w);
     const float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
     const float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
-    const float x = (p.x - S.bmin[0]) / (S.bmax[0] - S.bmin[0]);
-    const float y = (p.y - S.bmin[1]) / (S.bmax[1] - S.bmin[1]);
-    const float z = (p.z - S.bmin[2]) / (S.bmax[2] - S.bmin[2]);
-    const uint32_t code = (spread10((uint32_t)fminf(fmaxf(x * 1024.0f, 0.0f), 1023.0f)) << 2) |
-                          (spread10((uint32_t)fminf(fmaxf(y * 1024.0f, 0.0f), 1023.0f)) << 1) |
-                          spread10((uint32_t)fminf(fmaxf(z * 1024.0f, 0.0f), 1023.0f));
-    keys[g] = ((uint64_t)s << kMortonBits) | code;
+    keys[g] = morton_key(S, s, p);
   }
 }
 
@@ -306,7 +284,8 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
     const uint32_t* __restrict__ svals, const int32_t* __restrict__ left,
     const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
     WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
-    int32_t* __restrict__ max_r) {
+    int32_t* __restrict__ max_r, long long* __restrict__ d_step) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const int g = (int)__ldg(svals + k);
     const int sc = __ldg(pscene + g);
@@ -331,7 +310,10 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
   }
 }
 
-// Each scene's subtree root: the lowest ancestor of its first leaf covering its last leaf.
+// Each scene's subtree root.  The scene's leaves [lo, hi] are one subtree, whose root covers
+// exactly [lo, hi]; a Karras internal node i has i as one end of its range, so the root is
+// internal node lo or internal node hi.  (The walk up from the first leaf is kept only as a
+// guard against a malformed tree.)
 __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
                                  const int32_t* __restrict__ parent,
                                  const int32_t* __restrict__ min_r,
@@ -342,6 +324,12 @@ __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
   if (hi <= lo) {  // zero or one particle: no internal node
     roots[s] = -1;
     return;
+  }
+  for (const int cand : {nt + lo, nt + hi}) {
+    if (cand <= 2 * nt - 2 && min_r[cand] == lo && max_r[cand] == hi) {
+      roots[s] = cand;
+      return;
+    }
   }
   int node = parent[lo];
   for (int depth = 0; depth < nt && node >= 0; ++depth) {
@@ -355,29 +343,33 @@ __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
 // thread per leaf climbs; the second thread to reach a node merges the two child boxes held in
 // the node (mergeBounds, BVHAuxiliary.cuh:83-94) and stores the result into the node's slot in
 // its parent.  Release / acquire through the arrival counter; boxes through L2.
-__global__ void __launch_bounds__(256) bvh_refit_kernel(int n, const int32_t* __restrict__ left,
-                                                        const int32_t* __restrict__ parent,
-                                                        WideNode* nodes,
-                                                        int* __restrict__ counters) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+// One thread per leaf (ar_lbvh::refit_climb): the leaf's box is in its parent's slot (written
+// by the leaves kernel); each merged box goes into the node's slot in its parent.
+__global__ void __launch_bounds__(ar_lbvh::kRefitBlock) bvh_refit_kernel(
+    int n, const int32_t* __restrict__ left, const int32_t* __restrict__ parent,
+    const int32_t* __restrict__ min_r, const int32_t* __restrict__ max_r, WideNode* nodes,
+    int* __restrict__ counters) {
+  __shared__ ar_lbvh::RefitShared sh;
+  ar_lbvh::refit_shared_init(sh);
+  __syncthreads();
+  const int blo = blockIdx.x * ar_lbvh::kRefitBlock;
+  const int i = blo + threadIdx.x;
   if (i >= n || n < 2) return;
-  int node = __ldg(parent + i);
-  for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
-    if (node < n || node >= 2 * n - 1) return;  // malformed parent link
-    if (ar_lbvh::arrive(counters + (node - n)) == 0) return;
-    const float4* c = nodes[node - n].c;
-    const float4 a0 = __ldcg(c), a1 = __ldcg(c + 1), b0 = __ldcg(c + 2), b1 = __ldcg(c + 3);
+  auto slot = [&](int node, int side) {  // box of child `side` of internal node `node`
+    const float4* c = nodes[node - n].c + 2 * side;
+    const float4 a = __ldcg(c), b = __ldcg(c + 1);
+    return ar_lbvh::Box6{a.x, a.y, a.z, a.w, b.x, b.y};
+  };
+  auto store = [&](int node, const ar_lbvh::Box6& b) {
     if (node == n) return;  // the root's box is not stored anywhere
-    float4 lo;
-    lo.x = a0.x < b0.x ? a0.x : b0.x;
-    lo.y = a0.y < b0.y ? a0.y : b0.y;
-    lo.z = a0.z < b0.z ? a0.z : b0.z;
-    lo.w = a0.w > b0.w ? a0.w : b0.w;  // max.x
-    const float2 hi = make_float2(a1.x > b1.x ? a1.x : b1.x, a1.y > b1.y ? a1.y : b1.y);
     const int pn = __ldg(parent + node);
-    put_child_box(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1, lo, hi);
-    node = pn;
-  }
+    put_child_box(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1,
+                  make_float4(b.lx, b.ly, b.lz, b.hx), make_float2(b.hy, b.hz));
+  };
+  auto sibling = [&](int node, int side) { return slot(node, 1 - side); };
+  const int p0 = __ldg(parent + i);
+  ar_lbvh::refit_climb(i, slot(p0, __ldg(left + p0) == i ? 0 : 1), n, left, parent, min_r,
+                       max_r, blo, sh, counters, store, sibling);
 }
 
 // DEM gather through the scene's subtree in the reference's visit order
@@ -449,55 +441,100 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
   pforce[__ldg(svals + k)] = make_float4(lin.x, lin.y, lin.z, 0.f);
 }
 
-// ---- K5: fixed-order body sums + integration ---------------------------------------------------
-// A scene whose step budget is spent (batch step number > end_step) is frozen: its state is
-// left untouched.
-__global__ void __launch_bounds__(256) reduce_integrate_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ bscene, int ns, int bt,
+// ---- K5: fixed-order body sums + integration + next step's keys ----------------------------
+// One warp per body: fixed-order lane sums of F and r x F over the body's particles, xor-tree
+// across lanes, integration by lane 0.  Then the warp re-poses the body's particles from the
+// new state and writes the next step's sort keys (grid: cell key, with the sort histogram
+// accumulated in shared memory; BVH: scene-prefixed Morton code), so no separate pass over the
+// particles is needed.  The grid variant also resets the cells this step occupied.  A scene
+// whose step budget is spent (batch step number > end_step) is frozen: its state is left
+// untouched, but its keys are still written (it stays in the broad phase).
+template <bool kBvh>
+__global__ void __launch_bounds__(256) body_step_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
     const float4* __restrict__ pforce, const long long* __restrict__ d_step,
-    int* __restrict__ err) {
+    int* __restrict__ err, uint32_t* __restrict__ keys, uint64_t* __restrict__ keys64,
+    uint32_t* __restrict__ ws_hist, int passes, int last_bits,
+    const uint32_t* __restrict__ skeys, int nt, uint4* __restrict__ cells) {
+  __shared__ uint32_t s_hist[kBvh ? 1 : ar_sort::kMaxPasses][256];
+  if (!kBvh) {
+    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
+    // this step's cells back to empty (every reader of the table has run)
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
+      const uint32_t key = __ldg(skeys + k);
+      if (k == 0 || key != __ldg(skeys + k - 1)) cells[key].x = ar::kEmpty;
+    }
+    __syncthreads();
+  }
   const int warps = (gridDim.x * blockDim.x) >> 5;
   const int lane = ar::lane_id();
   const long long step = *d_step;
   for (int gb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gb < bt; gb += warps) {
-    const SceneDev& S = table[__ldg(bscene + gb)];
-    if (step > S.end_step) continue;
+    const int sc = __ldg(bscene + gb);
+    const SceneDev& S = table[sc];
     const int b = gb - S.boff;
     const int s0 = __ldg(S.offsets + b), s1 = __ldg(S.offsets + b + 1);
-    const float4 q = S.quat[b];
-    float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
+    float4 q = S.quat[b];
+    float4 c = S.pos[b];
+    if (step <= S.end_step) {
+      float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
+      for (int i = s0 + lane; i < s1; i += 32) {
+        const float4 f4 = __ldcs(pforce + S.poff + i);
+        const float4 r4 = __ldg(S.rel + i);
+        const float3 f = ar::xyz(f4);
+        const float3 t = ar::cross(ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z)), f);
+        fx += f.x; fy += f.y; fz += f.z;
+        tx += t.x; ty += t.y; tz += t.z;
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+        tx += __shfl_xor_sync(0xffffffffu, tx, o);
+        ty += __shfl_xor_sync(0xffffffffu, ty, o);
+        tz += __shfl_xor_sync(0xffffffffu, tz, o);
+      }
+      if (lane == 0) {
+        float ib[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) ib[k] = __ldg(S.inv_inertia + 9 * b + k);
+        float4 vel = S.vel[b], ang = S.ang[b];
+        const float3 F = ar::mk3(fx, fy, fz), T = ar::mk3(tx, ty, tz);
+        if (!ar_pipe::integrate_body(S, F, T, __ldg(S.mass + b), ib, &c, &q, &vel, &ang))
+          ar::raise_error(err, ar::kErrNaN);
+        S.pos[b] = c;
+        S.quat[b] = q;
+        S.vel[b] = vel;
+        S.ang[b] = ang;
+        S.bforce[b] = make_float4(fx, fy, fz, 0.f);
+        S.btorque[b] = make_float4(tx, ty, tz, 0.f);
+      }
+      // every lane takes lane 0's new pose
+      q.x = __shfl_sync(0xffffffffu, q.x, 0);
+      q.y = __shfl_sync(0xffffffffu, q.y, 0);
+      q.z = __shfl_sync(0xffffffffu, q.z, 0);
+      q.w = __shfl_sync(0xffffffffu, q.w, 0);
+      c.x = __shfl_sync(0xffffffffu, c.x, 0);
+      c.y = __shfl_sync(0xffffffffu, c.y, 0);
+      c.z = __shfl_sync(0xffffffffu, c.z, 0);
+    }
     for (int i = s0 + lane; i < s1; i += 32) {
-      const float4 f4 = __ldcs(pforce + S.poff + i);
       const float4 r4 = __ldg(S.rel + i);
-      const float3 f = ar::xyz(f4);
-      const float3 t = ar::cross(ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z)), f);
-      fx += f.x; fy += f.y; fz += f.z;
-      tx += t.x; ty += t.y; tz += t.z;
+      const float3 r = ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z));
+      const float3 p = ar::add(ar::xyz(c), r);
+      if (kBvh) {
+        keys64[S.poff + i] = morton_key(S, sc, p);
+      } else {
+        const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
+        keys[S.poff + i] = key;
+        ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
+      }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      fx += __shfl_xor_sync(0xffffffffu, fx, o);
-      fy += __shfl_xor_sync(0xffffffffu, fy, o);
-      fz += __shfl_xor_sync(0xffffffffu, fz, o);
-      tx += __shfl_xor_sync(0xffffffffu, tx, o);
-      ty += __shfl_xor_sync(0xffffffffu, ty, o);
-      tz += __shfl_xor_sync(0xffffffffu, tz, o);
-    }
-    if (lane == 0) {
-      float ib[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) ib[k] = __ldg(S.inv_inertia + 9 * b + k);
-      float4 pos = S.pos[b], quat = q, vel = S.vel[b], ang = S.ang[b];
-      const float3 F = ar::mk3(fx, fy, fz), T = ar::mk3(tx, ty, tz);
-      if (!ar_pipe::integrate_body(S, F, T, __ldg(S.mass + b), ib, &pos, &quat, &vel, &ang))
-        ar::raise_error(err, ar::kErrNaN);
-      S.pos[b] = pos;
-      S.quat[b] = quat;
-      S.vel[b] = vel;
-      S.ang[b] = ang;
-      S.bforce[b] = make_float4(fx, fy, fz, 0.f);
-      S.btorque[b] = make_float4(tx, ty, tz, 0.f);
-    }
+  }
+  if (!kBvh) {
+    __syncthreads();
+    ar_sort::hist_flush(s_hist, ws_hist, passes);
   }
 }
 
@@ -519,6 +556,7 @@ struct ar_scene {
   float *mass = nullptr, *inv_inertia = nullptr;
   int32_t* offsets = nullptr;
   void* block = nullptr;  // one stream-ordered allocation holding all of the above
+  unsigned epoch = 0;     // bumped by every upload of body state
   float origin[3], cell[3];
   uint32_t gdim[3];
   ar_batch* solo = nullptr;
@@ -535,10 +573,10 @@ struct ar_batch {
   // buffers
   uint32_t *keys = nullptr, *skeys = nullptr, *svals = nullptr;
   float4 *spos = nullptr, *svel = nullptr, *pforce = nullptr;
-  uint2* cells = nullptr;
+  uint4* cells = nullptr;  // {first slot, end slot, body tag, 0} per cell
   char* sort_ws = nullptr;
   SceneDev* d_table = nullptr;
-  int *d_poff = nullptr, *d_boff = nullptr, *d_prev_n = nullptr;
+  int *d_poff = nullptr, *d_boff = nullptr;
   int *d_pscene = nullptr, *d_bscene = nullptr;  // scene index per particle / body
   long long* d_step = nullptr;   // number of the step being run (incremented by its first kernel)
   long long host_step = 0;       // steps enqueued so far
@@ -552,7 +590,10 @@ struct ar_batch {
   long nt = 0, bt = 0;
   uint64_t total_cells = 0;
   int key_bits = 1, passes = 1, last_bits = 1;
-  int host_prev_n = 0;  // particles whose cells are marked in skeys (0 after a clear)
+  // the keys of the current state exist (written by the last step or a prologue); the cell
+  // table is empty between steps (each step resets the cells it occupied)
+  bool keys_valid = false;
+  std::vector<unsigned> epochs;  // member scenes' upload epochs the keys were made from
   // BVH broad phase (allocated only for BVH batches)
   int broadphase = AR_BROADPHASE_GRID;
   long cap_bvh = 0;
@@ -576,13 +617,13 @@ void free_batch_buffers(ar_batch* B) {
   cudaFree(B->keys); cudaFree(B->skeys); cudaFree(B->svals);
   cudaFree(B->spos); cudaFree(B->svel); cudaFree(B->pforce);
   cudaFree(B->cells); cudaFree(B->sort_ws);
-  cudaFree(B->d_table); cudaFree(B->d_poff); cudaFree(B->d_boff); cudaFree(B->d_prev_n);
+  cudaFree(B->d_table); cudaFree(B->d_poff); cudaFree(B->d_boff);
   cudaFree(B->d_pscene); cudaFree(B->d_bscene);
   B->d_pscene = B->d_bscene = nullptr;
   B->keys = B->skeys = B->svals = nullptr;
   B->spos = B->svel = B->pforce = nullptr;
   B->cells = nullptr; B->sort_ws = nullptr; B->d_table = nullptr;
-  B->d_poff = B->d_boff = B->d_prev_n = nullptr;
+  B->d_poff = B->d_boff = nullptr;
   B->cap_n = B->cap_b = B->cap_s = 0;
   B->cap_cells = 0;
   B->cap_sort = 0;
@@ -618,22 +659,11 @@ uint64_t scene_cells(const ar_scene* s) {
   return (uint64_t)s->gdim[0] * s->gdim[1] * s->gdim[2];
 }
 
-// Clear the cells the last step marked (so the table is all-empty before a layout change).
-void clear_marked(ar_batch* B, cudaStream_t st) {
-  if (B->host_prev_n > 0 && B->cells && B->broadphase == AR_BROADPHASE_GRID) {
-    clear_cells_kernel<<<arh::grid_for(B->host_prev_n, 256) > 4096 ? 4096
-                                                                   : arh::grid_for(B->host_prev_n, 256),
-                         256, 0, st>>>(B->skeys, B->host_prev_n, B->cells);
-    cudaMemsetAsync(B->d_prev_n, 0, sizeof(int), st);
-  }
-  B->host_prev_n = 0;
-}
-
 // (Re)build the scene table and make sure every buffer is large enough.
 ar_status prepare(ar_batch* B, cudaStream_t st) {
   if (!B->table_dirty) return AR_OK;
-  clear_marked(B, st);
   drop_graph(B);
+  B->keys_valid = false;
   long nt = 0, bt = 0;
   uint64_t cells = 0;
   std::vector<SceneDev> tab;
@@ -690,7 +720,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     bool ok = alloc(&B->keys, cn) && alloc(&B->skeys, cn) && alloc(&B->svals, cn) &&
               alloc(&B->spos, cn) && alloc(&B->svel, cn) && alloc(&B->pforce, cn) &&
               alloc(&B->cells, cc) && alloc(&B->sort_ws, csort) && alloc(&B->d_table, cs) &&
-              alloc(&B->d_poff, cs + 1) && alloc(&B->d_boff, cs + 1) && alloc(&B->d_prev_n, 1) &&
+              alloc(&B->d_poff, cs + 1) && alloc(&B->d_boff, cs + 1) &&
               alloc(&B->d_pscene, cn) && alloc(&B->d_bscene, cb);
     if (!ok) {
       free_batch_buffers(B);
@@ -699,8 +729,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
       return AR_ERR_OOM;
     }
     B->cap_n = cn; B->cap_b = cb; B->cap_s = cs; B->cap_cells = cc; B->cap_sort = csort;
-    cudaMemsetAsync(B->cells, 0xff, cc * sizeof(uint2), st);
-    cudaMemsetAsync(B->d_prev_n, 0, sizeof(int), st);
+    cudaMemsetAsync(B->cells, 0xff, cc * sizeof(uint4), st);
   }
   B->broadphase = ns > 0 ? B->scenes[0]->desc.broadphase : AR_BROADPHASE_GRID;
   if (B->broadphase == AR_BROADPHASE_BVH) {
@@ -772,8 +801,31 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
   return arh::check_launch("batch prepare");
 }
 
-// Stage boundaries for ar_step_profile: events[0] before the clear, events[i] after stage i.
-constexpr int kStages = 6;  // clear, repose_hash, sort, scatter, collide, reduce_integrate
+// Stage boundaries for ar_step_profile: events[0] before the step, events[i] after stage i.
+// Grid: sort | scatter + cell table | collide | clear (next sort's histogram head) |
+// body sums + integration + next keys | (empty).  BVH: sort | tree (Karras nodes, leaves,
+// scene roots, refit) | collide | clear (refit counters) | body sums + integration + next
+// keys | (empty).
+constexpr int kStages = 6;
+
+// Keys (and, for the grid, the sort histogram) of the current state; a step's last kernel
+// writes them for the next step, so this runs only when the state did not come from a step.
+ar_status enqueue_keys(ar_batch* B, cudaStream_t st) {
+  const int nt = (int)B->nt;
+  const unsigned g = std::min(arh::grid_for(nt, 256), (unsigned)B->ctx->num_sms * 8);
+  if (B->broadphase == AR_BROADPHASE_BVH) {
+    // steps zero the refit counters at their end for the next step; the first needs them too
+    cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);
+    morton_key_kernel<<<g, 256, 0, st>>>(B->d_table, B->d_pscene, (int)B->scenes.size(), nt,
+                                         B->keys64);
+  } else {
+    cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
+    grid_keys_kernel<<<std::min(arh::grid_for(nt, kK1Threads), (unsigned)B->ctx->num_sms * 4),
+                       kK1Threads, 0, st>>>(B->d_table, B->d_pscene, nt, B->keys,
+                                            (uint32_t*)B->sort_ws, B->passes, B->last_bits);
+  }
+  return arh::check_launch("step keys");
+}
 
 ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   if (B->nt == 0) return AR_OK;
@@ -785,69 +837,73 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   };
   int bs = 128;
   if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
+  const unsigned gp = std::min(arh::grid_for(nt, 256), (unsigned)ctx->num_sms * 8);
+  const unsigned g5 = arh::grid_for((long)bt * 32, 256);
   mark(0);
   if (B->broadphase == AR_BROADPHASE_BVH) {
-    // clear | Morton keys | sort | tree (Karras nodes, leaves, scene roots, refit) | collide |
-    // reduce_integrate
-    cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);
-    mark(1);
-    const unsigned gp = std::min(arh::grid_for(nt, 256), (unsigned)ctx->num_sms * 8);
-    morton_key_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->keys64, B->d_step);
-    mark(2);
     ar_status s = ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
                                     B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
     if (s != AR_OK) return s;
-    mark(3);
+    mark(1);
     bvh_build_kernel<<<arh::grid_for(std::max(nt - 1, 1), 256), 256, 0, st>>>(
         ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
         B->right, B->parent, B->min_r, B->max_r, B->nodes);
     bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->svals, B->left,
                                           B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
-                                          B->min_r, B->max_r);
+                                          B->min_r, B->max_r, B->d_step);
     bvh_roots_kernel<<<arh::grid_for(ns, 128), 128, 0, st>>>(B->d_poff, ns, nt, B->parent,
                                                               B->min_r, B->max_r, B->roots);
-    bvh_refit_kernel<<<arh::grid_for(nt, 256), 256, 0, st>>>(nt, B->left, B->parent, B->nodes,
-                                                              B->counters);
-    mark(4);
+    bvh_refit_kernel<<<arh::grid_for(nt, ar_lbvh::kRefitBlock), ar_lbvh::kRefitBlock, 0, st>>>(
+        nt, B->left, B->parent, B->min_r, B->max_r, B->nodes, B->counters);
+    mark(2);
     bvh_collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(
         B->d_table, B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots,
         B->pforce, ctx->d_err);
+    mark(3);
+    cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);  // next step's refit
+    mark(4);
+    body_step_kernel<true><<<g5, 256, 0, st>>>(
+        B->d_table, B->d_bscene, bt, B->pforce, B->d_step, ctx->d_err, nullptr, B->keys64,
+        nullptr, 0, 0, nullptr, nt, nullptr);
     mark(5);
-    reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
-        B->d_table, B->d_bscene, ns, bt, B->pforce, B->d_step, ctx->d_err);
     mark(6);
     return arh::check_launch("step (BVH)");
   }
-  cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
-  mark(1);
-  unsigned g1 = arh::grid_for(nt, kK1Threads);
-  unsigned cap1 = (unsigned)ctx->num_sms * 4;
-  repose_hash_kernel<<<g1 > cap1 ? cap1 : g1, kK1Threads, 0, st>>>(
-      B->d_table, B->d_pscene, ns, nt, B->d_prev_n, B->skeys, B->cells, B->keys,
-      (uint32_t*)B->sort_ws, B->passes, B->last_bits, B->d_step);
-  mark(2);
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
                                   st, B->sort_ws, B->cap_sort, true);
   if (s != AR_OK) return s;
-  mark(3);
-  unsigned g3 = arh::grid_for(nt, 256);
-  unsigned cap3 = (unsigned)ctx->num_sms * 8;
-  scatter_kernel<<<g3 > cap3 ? cap3 : g3, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->skeys,
-                                                        B->svals, B->cells, B->spos, B->svel,
-                                                        B->d_prev_n);
-  mark(4);
+  mark(1);
+  scatter_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->skeys, B->svals,
+                                     B->cells, B->spos, B->svel, B->d_step);
+  mark(2);
   collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, nt, B->skeys, B->svals,
                                                        B->cells, B->spos, B->svel, B->pforce);
+  mark(3);
+  cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);  // next sort's head
+  mark(4);
+  body_step_kernel<false><<<g5, 256, 0, st>>>(
+      B->d_table, B->d_bscene, bt, B->pforce, B->d_step, ctx->d_err, B->keys, nullptr,
+      (uint32_t*)B->sort_ws, B->passes, B->last_bits, B->skeys, nt, B->cells);
   mark(5);
-  reduce_integrate_kernel<<<arh::grid_for((long)bt * 32, 256), 256, 0, st>>>(
-      B->d_table, B->d_bscene, ns, bt, B->pforce, B->d_step, ctx->d_err);
   mark(6);
-  B->host_prev_n = nt;
   return arh::check_launch("step");
+}
+
+// The keys of the current state exist (else enqueue them first).
+ar_status ensure_keys(ar_batch* B, cudaStream_t st) {
+  bool valid = B->keys_valid && B->epochs.size() == B->scenes.size();
+  for (size_t i = 0; valid && i < B->scenes.size(); ++i)
+    valid = B->epochs[i] == B->scenes[i]->epoch;
+  if (valid || B->nt == 0) return AR_OK;
+  B->epochs.resize(B->scenes.size());
+  for (size_t i = 0; i < B->scenes.size(); ++i) B->epochs[i] = B->scenes[i]->epoch;
+  B->keys_valid = true;
+  return enqueue_keys(B, st);
 }
 
 // Run n_steps eagerly with events between the stages; average milliseconds per stage.
 ar_status profile_steps(ar_batch* B, int n_steps, float* stage_ms, cudaStream_t st) {
+  if (ar_status k = ensure_keys(B, st); k != AR_OK) return k;
   cudaEvent_t ev[kStages + 1];
   for (auto& e : ev) cudaEventCreate(&e);
   double acc[kStages] = {0};
@@ -875,6 +931,7 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
   ar_status s = prepare(B, st);
   if (s != AR_OK) return s;
   if (B->nt == 0 || n_steps <= 0) return AR_OK;
+  if ((s = ensure_keys(B, st)) != AR_OK) return s;
   if (!use_graph) {
     for (int i = 0; i < n_steps; ++i) {
       if ((s = enqueue_step(B, st)) != AR_OK) return s;
@@ -915,8 +972,6 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
     if (cudaGraphLaunch(B->graph, st) != cudaSuccess) return arh::check_launch("graph launch");
     ++B->host_step;
   }
-  // only the grid step marks cells (the BVH step never writes the grid keys)
-  if (B->broadphase == AR_BROADPHASE_GRID) B->host_prev_n = (int)B->nt;
   return arh::check_launch("graph launch");
 }
 
@@ -967,7 +1022,7 @@ size_t ar_scene_footprint(const ar_scene_desc* d) {
     return n * per_particle + b * per_body + 4096;
   }
   const size_t per_particle = shared + 4 * 2 /*keys*/ + 8 /*sort tmp*/;
-  return n * per_particle + b * per_body + (size_t)ar_scene_cells(d) * 8 + 4096;
+  return n * per_particle + b * per_body + (size_t)ar_scene_cells(d) * 16 + 4096;
 }
 
 uint64_t ar_scene_cells(const ar_scene_desc* d) {
@@ -1177,6 +1232,7 @@ ar_status ar_scene_upload(ar_scene* s, const float* h_pos4, const float* h_quat4
   if (!s) return AR_ERR_INVALID_ARG;
   cudaStream_t st = arh::stream(stream);
   const size_t bytes = 16 * (size_t)s->nb;
+  ++s->epoch;  // the batches' next step recomputes the keys of this state
   if (h_pos4) cudaMemcpyAsync(s->pos, h_pos4, bytes, cudaMemcpyHostToDevice, st);
   if (h_quat4) cudaMemcpyAsync(s->quat, h_quat4, bytes, cudaMemcpyHostToDevice, st);
   if (h_vel4) cudaMemcpyAsync(s->vel, h_vel4, bytes, cudaMemcpyHostToDevice, st);
@@ -1279,9 +1335,11 @@ ar_status ar_batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph,
 
 int ar_batch_launches_per_step(ar_batch* B) {
   if (!B) return 0;
-  if (B->broadphase == AR_BROADPHASE_BVH)  // memset, keys, sort, 4 tree kernels, collide, reduce
-    return 1 + 1 + ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 2;
-  return 1 /*memset*/ + 1 /*K1*/ + ar_sort::launches(0, B->key_bits, true) + 3;
+  // steady-state step (the keys prologue runs only after a member change or an upload)
+  if (B->broadphase == AR_BROADPHASE_BVH)  // sort, 4 tree kernels, collide, memset, body
+    return ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 1 + 1 + 1;
+  return ar_sort::launches(0, B->key_bits, true) + 1 /*scatter*/ + 1 /*collide*/ +
+         1 /*memset*/ + 1 /*body*/;
 }
 
 int ar_scene_launches_per_step(ar_scene* s) {

@@ -174,10 +174,18 @@ AR_API ar_status ar_lbvh_leaves(ar_ctx* ctx, int n, const int32_t* sorted_idx,
 /* ---- (a11) bottom-up AABB refit --------------------------------------------------------------
  * kernelConstructInternalNodesSoA (BVHSoAKernels.cu:148-176): one thread per leaf climbs to
  * the root; the second thread to reach a node merges its children's boxes.  Unlike the
- * reference, the arrival counter is ordered by release/acquire fences, so the merge always
- * sees both children's final boxes. */
+ * reference, the arrival counter has acquire-release semantics, so the merge always sees both
+ * children's final boxes. */
 AR_API ar_status ar_lbvh_refit(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
                                const int32_t* parent, float* bounds8, ar_stream_t stream);
+/* The same, given the build's leaf ranges (min_r / max_r of ar_lbvh_build and
+ * ar_lbvh_leaves): a node whose leaves are all climbed by threads of one block is
+ * synchronised at block scope instead of device scope, which removes most device-wide fences.
+ * New (the reference's wrapperConstructInternalNodesSoA has no ranges); same result. */
+AR_API ar_status ar_lbvh_refit_ranged(ar_ctx* ctx, int n, const int32_t* left,
+                                      const int32_t* right, const int32_t* parent,
+                                      const int32_t* min_r, const int32_t* max_r,
+                                      float* bounds8, ar_stream_t stream);
 
 /* ---- (a12) BVH traversal ---------------------------------------------------------------------
  * collideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:100-244) with collideStaticSpheresBVH
@@ -496,9 +504,14 @@ AR_API ar_status ar_step(ar_ctx* ctx, ar_scene* scene, int n_steps, int use_grap
                          ar_stream_t stream);
 
 /* Run n_steps of the scene without a graph, with CUDA events between the stages, and return
- * the average device milliseconds per stage in h_stage_ms[6]: clear, re-pose + hash,
- * sort, scatter + cell ranges, DEM gather + walls, body sums + integration.  (Replaces the
- * reference's clock() accumulators, e.g. RigidBodies/UniformGridUpdate.cpp:338-446.) */
+ * the average device milliseconds per stage in h_stage_ms[6].  Grid: sort, scatter + cell
+ * table, DEM gather + walls, clear (next sort's histogram head), body sums + integration +
+ * next step's keys, 0.  BVH: sort, tree (build, leaves, scene roots, refit), DEM traversal +
+ * walls, clear (refit counters), body sums + integration + next keys, 0.  A step computes the
+ * next step's sort keys in its last kernel; the keys of a state that did not come from a step
+ * (new member list, upload) are computed once before the first step and are not part of any
+ * stage.  (Replaces the reference's clock() accumulators, e.g.
+ * RigidBodies/UniformGridUpdate.cpp:338-446.) */
 AR_API ar_status ar_step_profile(ar_ctx* ctx, ar_scene* scene, int n_steps, float* h_stage_ms,
                                  ar_stream_t stream);
 

@@ -63,8 +63,10 @@ def test_context_without_gpu_fails_cleanly():
 def test_scene_footprint_scales_with_size():
     from diploma_thesis_b200 import _lib, api, scenes
     s = scenes.small_scene(0, nb_side=4)
-    d = api.make_desc(s)
-    f1 = _lib.lib.ar_scene_footprint(C.byref(d))
-    d.num_particles *= 10
-    d.num_bodies *= 10
-    assert _lib.lib.ar_scene_footprint(C.byref(d)) > 5 * f1 > 0
+    for bp, factor in ((0, 2), (1, 5)):  # grid: the cell table grows slower than N
+        d = api.make_desc(s, bp)
+        f1 = _lib.lib.ar_scene_footprint(C.byref(d))
+        d.num_particles *= 10
+        d.num_bodies *= 10
+        assert _lib.lib.ar_scene_footprint(C.byref(d)) > factor * f1 > 0
+        assert (_lib.lib.ar_scene_cells(C.byref(d)) > 0) == (bp == 0)
