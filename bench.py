@@ -40,7 +40,7 @@ FALLBACK_HBM_GBS = 6650.0
 # traffic of this design: every array element read or written once; neighbour reads that hit
 # in L2 are not counted).  P = sort passes, ppb = particles per body.  A step runs: sort |
 # scatter + cell table | collide | clear | body (sums, integration, next step's keys).
-STAGES = ["sort", "scatter", "collide", "clear", "body", "none"]
+STAGES = ["clear", "keys", "sort", "scatter", "collide", "body"]
 BODY_STATE = 16 * 4  # pos, quat, vel, angvel (float4 each)
 
 
@@ -52,6 +52,10 @@ def _body_bytes(nb: int) -> int:
 def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int) -> dict[str, float]:
     tiles = (n + 4095) // 4096
     return {
+        # sort histogram / look-back head
+        "clear": 4 * 256 * 8 + passes * 4 * 256 * tiles,
+        # rel in, key out; body pose (32) per body
+        "keys": n * (16 + 4) + nb * 32,
         # first pass reads the key only; every pass writes key + index; later passes read both
         "sort": n * (4 + 8) + (passes - 1) * n * 16 + passes * 4 * 256 * tiles,
         # sorted key + index and rel in, sorted position + velocity out; body state per body;
@@ -59,21 +63,21 @@ def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int) -> dict[str, 
         "scatter": n * (8 + 16 + 32) + nb * BODY_STATE + occupied_cells * 16,
         # own key, index, position, velocity in; force out
         "collide": n * (4 + 4 + 32 + 16),
-        # next sort's histogram / look-back head
-        "clear": 4 * 256 * 8 + passes * 4 * 256 * tiles,
-        # force + rel in, next key out; sorted key in and one reset per occupied cell
-        "body": n * (16 + 16 + 4 + 4) + occupied_cells * 4 + _body_bytes(nb),
-        "none": 0,
+        # force + rel in; sorted key in and one reset per occupied cell; body state
+        "body": n * (16 + 16 + 4) + occupied_cells * 4 + _body_bytes(nb),
     }
 
 
-BVH_STAGES = ["sort", "tree", "collide", "clear", "body", "none"]
+BVH_STAGES = ["clear", "keys", "sort", "tree", "collide", "body"]
 
 
 def stage_bytes_bvh(n: int, nb: int, passes: int) -> dict[str, float]:
     """The same accounting for the BVH broad phase (64-bit keys, 64-byte wide nodes)."""
     tiles = (n + 4095) // 4096
     return {
+        "clear": 4 * n,  # refit arrival counters
+        # rel in, 64-bit key out; body pose per body
+        "keys": n * (16 + 8) + nb * 32,
         # histogram pass reads the keys; first pass reads keys, every pass writes key + index,
         # later passes read both
         "sort": n * 8 + n * (8 + 12) + (passes - 1) * n * 24 + passes * 4 * 256 * tiles,
@@ -84,9 +88,7 @@ def stage_bytes_bvh(n: int, nb: int, passes: int) -> dict[str, float]:
                 n * (8 + 64 + 24),
         # own index, position + velocity in; force out
         "collide": n * (4 + 32 + 16),
-        "clear": 4 * n,  # refit arrival counters
-        "body": n * (16 + 16 + 8) + _body_bytes(nb),
-        "none": 0,
+        "body": n * (16 + 16) + _body_bytes(nb),
     }
 
 
@@ -284,7 +286,32 @@ class ReferenceCPUStep:
             pf, pt, self.st["vel"], self.st["ang"], s.body_mass, s.body_inv_inertia, self.counts)
 
 
-def cpu_reference_rate(scene, grid, target_s: float, steps: int | None = None):
+class ReferenceCPUStepBVH(ReferenceCPUStep):
+    """The BVH form of the same step, from the reference's own kernel bodies on the host cores:
+    GPUintegratorKernel, computeGlobalAttributes, findAABBCub, generateMortonCodes, the
+    CUB-order stable sort, kernelConstructRadixTreeSoA, kernelConstructLeafNodesSoA,
+    kernelConstructInternalNodesSoA, collideBVHSoARigidBody and ReducePerParticleImpulses."""
+
+    def step(self):
+        ref, s = self.ref, self.s
+        self.st = ref.gpu_integrator(self.prm, s.dt, self.st)
+        self.rel, pos, vel, q = ref.global_attributes(self.st["cms"], self.st["vel"],
+                                                      self.st["ang"], self.st["quat"], self.rb,
+                                                      self.rel)
+        self.st["quat"] = q
+        mn, mx = ref.aabb(pos)
+        codes, idx = ref.morton30(pos, mn, mx)
+        sk, si = ref.sort_pairs_u32(codes, idx)
+        tree = ref.radix_tree(sk)
+        cms, _, bounds, radii = ref.leaves_and_refit(tree, si, pos, s.radius)
+        pf, pt, _ = ref.collide_bvh_rigid(self.prm, self.rb, self.rel, vel, tree, cms, bounds, si,
+                                          radii)
+        self.st["vel"], self.st["ang"] = ref.reduce_impulses(
+            pf, pt, self.st["vel"], self.st["ang"], s.body_mass, s.body_inv_inertia, self.counts)
+
+
+def cpu_reference_rate(scene, grid, target_s: float, steps: int | None = None,
+                       broadphase: str = "grid"):
     """Particle-steps/s of the reference CPU step on a bounded sample; returns
     (rate, cores, kind, sample description, steps run, seconds)."""
     from oracle import ref
@@ -292,7 +319,7 @@ def cpu_reference_rate(scene, grid, target_s: float, steps: int | None = None):
         return None
     bodies = min(scene.num_bodies, 4096)
     sample = reference_sample(scene, bodies)
-    runner = ReferenceCPUStep(sample, grid)
+    runner = (ReferenceCPUStepBVH if broadphase == "bvh" else ReferenceCPUStep)(sample, grid)
     cores = ref.max_threads()
     runner.step()  # warm caches / page in
     t0 = time.perf_counter()
@@ -304,8 +331,9 @@ def cpu_reference_rate(scene, grid, target_s: float, steps: int | None = None):
         if (steps is not None and k >= steps) or (steps is None and el >= target_s):
             break
     rate = sample.num_particles * k / el
-    desc = (f"first {bodies} bodies ({sample.num_particles} particles) of the workload on the "
-            f"same grid, {k} reference steps in {el:.1f} s")
+    where = "BVH" if broadphase == "bvh" else "same grid"
+    desc = (f"first {bodies} bodies ({sample.num_particles} particles) of the workload, "
+            f"{where} path, {k} reference steps in {el:.1f} s")
     return rate, cores, "reference", desc, k, el
 
 
@@ -324,7 +352,7 @@ def run_reference(args):
         return 0
     bodies = min(scene.num_bodies, 2048 if args.workload == "pile" else 4096)
     sample = reference_sample(scene, bodies)
-    runner = ReferenceCPUStep(sample, grid)
+    runner = (ReferenceCPUStepBVH if args.broadphase == "bvh" else ReferenceCPUStep)(sample, grid)
     for _ in range(args.warmup):
         runner.step()
     t0 = time.perf_counter()
@@ -338,7 +366,7 @@ def run_reference(args):
             "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "sample": f"first {bodies} bodies "
-                       f"({sample.num_particles} particles)", "broadphase": "grid"},
+                       f"({sample.num_particles} particles)", "broadphase": args.broadphase},
             "cpu_baseline": {"value": rate, "unit": "Mparticle-steps/s", "cores": cores,
                              "kind": "reference",
                              "sample": f"first {bodies} bodies ({sample.num_particles} particles) "
@@ -430,7 +458,8 @@ def run_ours(args):
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import cpu
-        r = cpu_reference_rate(scene, cpu.scene_grid(scene), target_s=15.0)
+        r = cpu_reference_rate(scene, cpu.scene_grid(scene), target_s=15.0,
+                               broadphase=args.broadphase)
         if r is not None:
             rate, cores, kind, sample, k, el = r
             cpu_baseline = {"value": rate / 1e6, "unit": "Mparticle-steps/s", "cores": cores,
@@ -653,6 +682,25 @@ def run_lbvh(args):
             torch.cuda.empty_cache()
     big = [r for r in rows if r["n"] == max(sizes)]
     head = max(big, key=lambda r: r["mpoints_per_s"])
+    # reference kernel bodies on the host cores: findAABBCub, generateMortonCodes, the CUB-order
+    # stable sort, kernelConstructRadixTreeSoA, leaf and internal nodes (2^20 uniform points)
+    cpu_baseline = None
+    if not args.no_cpu:
+        from oracle import ref
+        if ref.available():
+            pts = scenes.lbvh_points(1 << 20, "uniform", seed=1)
+            k, t0 = 0, time.perf_counter()
+            while time.perf_counter() - t0 < 10.0 or k == 0:
+                mn, mx = ref.aabb(pts)
+                codes, idx = ref.morton30(pts, mn, mx)
+                sk, si = ref.sort_pairs_u32(codes, idx)
+                tree = ref.radix_tree(sk)
+                ref.leaves_and_refit(tree, si, pts, 1e-3)
+                k += 1
+            el = time.perf_counter() - t0
+            cpu_baseline = {"value": k * len(pts) / el / 1e6, "unit": "Mpoints/s",
+                            "cores": ref.max_threads(), "kind": "reference",
+                            "sample": f"2^20 uniform points, 30-bit, {k} builds in {el:.1f} s"}
     line = {"metric": "Mpoints/s (LBVH encode+sort+build+refit)", "value": head["mpoints_per_s"],
             "unit": "Mpoints/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic", "warmup": args.warmup, "reps": args.lbvh_reps,
@@ -661,7 +709,7 @@ def run_lbvh(args):
                        "headline": {k: head[k] for k in ("n", "dist", "bits")}},
             "peak_gbs": hbm, "peak_kind": f"{peak_kind} hbm_gbs",
             "bytes_per_point": {"30": lbvh_bytes(4, 4), "63": lbvh_bytes(8, 8)},
-            "rows": rows}
+            "cpu_baseline": cpu_baseline, "rows": rows}
     print(json.dumps(line))
     return 0
 

@@ -146,8 +146,8 @@ class GpuScene:
              stream_handle(stream))
 
     def profile(self, n: int, stream=None) -> list[float]:
-        """Average device ms per stage over n eager steps: grid (sort, scatter, collide,
-        clear, body, 0); BVH (sort, tree, collide, clear, body, 0)."""
+        """Average device ms per stage over n eager steps: grid (clear, keys, sort, scatter,
+        collide, body); BVH (clear, keys, sort, tree, collide, body)."""
         out = (C.c_float * 6)()
         call("ar_step_profile", self.ctx.handle, self.handle, int(n), out, stream_handle(stream))
         return list(out)

@@ -47,6 +47,13 @@ __device__ __forceinline__ int find_range(const int* __restrict__ off, int count
   return lo;
 }
 
+// Cell entries carry the number of the step that wrote them; an entry of another step is
+// empty.  Epochs live in [0, 2^31), so the all-ones fill of a fresh table never matches, and
+// the table is refilled whenever the step number enters a new 2^31 window (batch_step).
+__device__ __forceinline__ uint32_t cell_epoch(long long step) {
+  return (uint32_t)(step & 0x7fffffffLL);
+}
+
 // Scene index of every particle and body of the batch (run when the member list changes).
 __global__ void __launch_bounds__(256) scene_ids_kernel(const int* __restrict__ poff,
                                                         const int* __restrict__ boff, int ns,
@@ -59,13 +66,13 @@ __global__ void __launch_bounds__(256) scene_ids_kernel(const int* __restrict__ 
   }
 }
 
-// ---- prologue: cell keys + sort histogram from the current body state ----------------------
-// Steps compute the next step's keys at their end (body_step_kernel); this kernel computes
-// them only when the state did not come from a step (a new member list, an upload).
+// ---- K1: re-pose + cell keys + sort histogram ---------------------------------------------
 __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
-    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits) {
+    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits,
+    long long* __restrict__ d_step) {
   __shared__ uint32_t s_hist[ar_sort::kMaxPasses][256];
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
   for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
@@ -84,23 +91,25 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
 }
 
 // ---- K3: scatter + cell table -------------------------------------------------------------
-// Cell entry = {first sorted slot, end slot, body tag, 0}; the tag is the global body id when
-// every occupant belongs to one body (else kEmpty), so that a particle skips a neighbour cell
-// of its own body without loading its occupants (they could only be rejected).  The thread
-// at a cell's first slot writes the whole entry.
+// One thread per sorted slot k: sorted position (w = global body id) and velocity (w = scene
+// index) recomputed from the body state of particle svals[k].  (Gathering by sorted slot is
+// faster here than pushing from the original order: scattered 16-byte stores cost more than
+// the gathers.)  Cell entry = {first sorted slot, end slot, body tag, 0}; the tag is the
+// global body id when every occupant belongs to one body (else kEmpty), so that a particle
+// skips a neighbour cell of its own body without loading its occupants (they could only be
+// rejected).  The thread at a cell's first slot writes the whole entry.
 __global__ void __launch_bounds__(256) scatter_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
+    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
     const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
     uint4* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
-    long long* __restrict__ d_step) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
+    const long long* __restrict__ d_step) {
+  const uint32_t epoch = cell_epoch(*d_step);
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const uint32_t key = __ldg(skeys + k);
     const int g = (int)__ldg(svals + k);
     const int sc = __ldg(pscene + g);
     const SceneDev& S = table[sc];
-    const int i = g - S.poff;
-    const float4 r4 = __ldg(S.rel + i);
+    const float4 r4 = __ldg(S.rel + (g - S.poff));
     const int b = __float_as_int(r4.w);
     if (k == 0 || key != __ldg(skeys + k - 1)) {
       // occupants of one cell belong to one scene
@@ -110,7 +119,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(
         const int ge = (int)__ldg(svals + e);
         if (__float_as_int(__ldg(S.rel + (ge - S.poff)).w) != b) tag = ar::kEmpty;
       }
-      cells[key] = make_uint4((uint32_t)k, (uint32_t)e, tag, 0u);
+      cells[key] = make_uint4((uint32_t)k, (uint32_t)e, tag, epoch);
     }
     float3 r, p, v;
     ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
@@ -140,9 +149,10 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
     const SceneDev* __restrict__ table, int nt, const uint32_t* __restrict__ skeys,
     const uint32_t* __restrict__ svals, const uint4* __restrict__ cells,
     const float4* __restrict__ spos, const float4* __restrict__ svel,
-    float4* __restrict__ pforce) {
+    float4* __restrict__ pforce, const long long* __restrict__ d_step) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
+  const uint32_t epoch = cell_epoch(*d_step);
   const float4 p4 = __ldg(spos + k);
   const float4 v4 = __ldg(svel + k);
   const SceneDev& S = table[__float_as_int(v4.w)];
@@ -160,9 +170,10 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
     const uint32_t row = base + (zz << (lx + ly)) + (yy << lx);
     return RowCells{__ldg(cells + row + xa), __ldg(cells + row + x), __ldg(cells + row + xc)};
   };
-  // occupants to visit: none for an empty cell or a cell holding only this particle's body
+  // occupants to visit: none for an empty cell (another step's entry) or a cell holding only
+  // this particle's body
   auto visits = [&](const uint4& c) {
-    return (c.x == ar::kEmpty || c.z == (uint32_t)body) ? 0u : c.y - c.x;
+    return (c.w != epoch || c.z == (uint32_t)body) ? 0u : c.y - c.x;
   };
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
   RowCells next = row_of(0);
@@ -224,7 +235,9 @@ __device__ __forceinline__ uint64_t morton_key(const SceneDev& S, int s, float3 
 
 __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restrict__ table,
                                                          const int* __restrict__ pscene, int ns,
-                                                         int nt, uint64_t* __restrict__ keys) {
+                                                         int nt, uint64_t* __restrict__ keys,
+                                                         long long* __restrict__ d_step) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
     const int s = __ldg(pscene + g);
     const SceneDev& S = table[s];
@@ -284,8 +297,7 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
     const uint32_t* __restrict__ svals, const int32_t* __restrict__ left,
     const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
     WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
-    int32_t* __restrict__ max_r, long long* __restrict__ d_step) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number (read by K5)
+    int32_t* __restrict__ max_r) {
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const int g = (int)__ldg(svals + k);
     const int sc = __ldg(pscene + g);
@@ -441,100 +453,56 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
   pforce[__ldg(svals + k)] = make_float4(lin.x, lin.y, lin.z, 0.f);
 }
 
-// ---- K5: fixed-order body sums + integration + next step's keys ----------------------------
+// ---- K5: fixed-order body sums + integration ----------------------------------------------
 // One warp per body: fixed-order lane sums of F and r x F over the body's particles, xor-tree
-// across lanes, integration by lane 0.  Then the warp re-poses the body's particles from the
-// new state and writes the next step's sort keys (grid: cell key, with the sort histogram
-// accumulated in shared memory; BVH: scene-prefixed Morton code), so no separate pass over the
-// particles is needed.  The grid variant also resets the cells this step occupied.  A scene
-// whose step budget is spent (batch step number > end_step) is frozen: its state is left
-// untouched, but its keys are still written (it stays in the broad phase).
-template <bool kBvh>
+// across lanes, integration by lane 0.  A scene whose step budget is spent (batch step
+// number > end_step) is frozen: its state is left untouched.
 __global__ void __launch_bounds__(256) body_step_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
     const float4* __restrict__ pforce, const long long* __restrict__ d_step,
-    int* __restrict__ err, uint32_t* __restrict__ keys, uint64_t* __restrict__ keys64,
-    uint32_t* __restrict__ ws_hist, int passes, int last_bits,
-    const uint32_t* __restrict__ skeys, int nt, uint4* __restrict__ cells) {
-  __shared__ uint32_t s_hist[kBvh ? 1 : ar_sort::kMaxPasses][256];
-  if (!kBvh) {
-    for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
-    // this step's cells back to empty (every reader of the table has run)
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
-      const uint32_t key = __ldg(skeys + k);
-      if (k == 0 || key != __ldg(skeys + k - 1)) cells[key].x = ar::kEmpty;
-    }
-    __syncthreads();
-  }
+    int* __restrict__ err) {
   const int warps = (gridDim.x * blockDim.x) >> 5;
   const int lane = ar::lane_id();
   const long long step = *d_step;
   for (int gb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gb < bt; gb += warps) {
-    const int sc = __ldg(bscene + gb);
-    const SceneDev& S = table[sc];
+    const SceneDev& S = table[__ldg(bscene + gb)];
+    if (step > S.end_step) continue;
     const int b = gb - S.boff;
     const int s0 = __ldg(S.offsets + b), s1 = __ldg(S.offsets + b + 1);
-    float4 q = S.quat[b];
-    float4 c = S.pos[b];
-    if (step <= S.end_step) {
-      float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
-      for (int i = s0 + lane; i < s1; i += 32) {
-        const float4 f4 = __ldcs(pforce + S.poff + i);
-        const float4 r4 = __ldg(S.rel + i);
-        const float3 f = ar::xyz(f4);
-        const float3 t = ar::cross(ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z)), f);
-        fx += f.x; fy += f.y; fz += f.z;
-        tx += t.x; ty += t.y; tz += t.z;
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        fx += __shfl_xor_sync(0xffffffffu, fx, o);
-        fy += __shfl_xor_sync(0xffffffffu, fy, o);
-        fz += __shfl_xor_sync(0xffffffffu, fz, o);
-        tx += __shfl_xor_sync(0xffffffffu, tx, o);
-        ty += __shfl_xor_sync(0xffffffffu, ty, o);
-        tz += __shfl_xor_sync(0xffffffffu, tz, o);
-      }
-      if (lane == 0) {
-        float ib[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) ib[k] = __ldg(S.inv_inertia + 9 * b + k);
-        float4 vel = S.vel[b], ang = S.ang[b];
-        const float3 F = ar::mk3(fx, fy, fz), T = ar::mk3(tx, ty, tz);
-        if (!ar_pipe::integrate_body(S, F, T, __ldg(S.mass + b), ib, &c, &q, &vel, &ang))
-          ar::raise_error(err, ar::kErrNaN);
-        S.pos[b] = c;
-        S.quat[b] = q;
-        S.vel[b] = vel;
-        S.ang[b] = ang;
-        S.bforce[b] = make_float4(fx, fy, fz, 0.f);
-        S.btorque[b] = make_float4(tx, ty, tz, 0.f);
-      }
-      // every lane takes lane 0's new pose
-      q.x = __shfl_sync(0xffffffffu, q.x, 0);
-      q.y = __shfl_sync(0xffffffffu, q.y, 0);
-      q.z = __shfl_sync(0xffffffffu, q.z, 0);
-      q.w = __shfl_sync(0xffffffffu, q.w, 0);
-      c.x = __shfl_sync(0xffffffffu, c.x, 0);
-      c.y = __shfl_sync(0xffffffffu, c.y, 0);
-      c.z = __shfl_sync(0xffffffffu, c.z, 0);
-    }
+    const float4 q = S.quat[b];
+    float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
     for (int i = s0 + lane; i < s1; i += 32) {
+      const float4 f4 = __ldcs(pforce + S.poff + i);
       const float4 r4 = __ldg(S.rel + i);
-      const float3 r = ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z));
-      const float3 p = ar::add(ar::xyz(c), r);
-      if (kBvh) {
-        keys64[S.poff + i] = morton_key(S, sc, p);
-      } else {
-        const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
-        keys[S.poff + i] = key;
-        ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
-      }
+      const float3 f = ar::xyz(f4);
+      const float3 t = ar::cross(ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z)), f);
+      fx += f.x; fy += f.y; fz += f.z;
+      tx += t.x; ty += t.y; tz += t.z;
     }
-  }
-  if (!kBvh) {
-    __syncthreads();
-    ar_sort::hist_flush(s_hist, ws_hist, passes);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      fx += __shfl_xor_sync(0xffffffffu, fx, o);
+      fy += __shfl_xor_sync(0xffffffffu, fy, o);
+      fz += __shfl_xor_sync(0xffffffffu, fz, o);
+      tx += __shfl_xor_sync(0xffffffffu, tx, o);
+      ty += __shfl_xor_sync(0xffffffffu, ty, o);
+      tz += __shfl_xor_sync(0xffffffffu, tz, o);
+    }
+    if (lane == 0) {
+      float ib[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) ib[k] = __ldg(S.inv_inertia + 9 * b + k);
+      float4 pos = S.pos[b], quat = q, vel = S.vel[b], ang = S.ang[b];
+      const float3 F = ar::mk3(fx, fy, fz), T = ar::mk3(tx, ty, tz);
+      if (!ar_pipe::integrate_body(S, F, T, __ldg(S.mass + b), ib, &pos, &quat, &vel, &ang))
+        ar::raise_error(err, ar::kErrNaN);
+      S.pos[b] = pos;
+      S.quat[b] = quat;
+      S.vel[b] = vel;
+      S.ang[b] = ang;
+      S.bforce[b] = make_float4(fx, fy, fz, 0.f);
+      S.btorque[b] = make_float4(tx, ty, tz, 0.f);
+    }
   }
 }
 
@@ -556,7 +524,6 @@ struct ar_scene {
   float *mass = nullptr, *inv_inertia = nullptr;
   int32_t* offsets = nullptr;
   void* block = nullptr;  // one stream-ordered allocation holding all of the above
-  unsigned epoch = 0;     // bumped by every upload of body state
   float origin[3], cell[3];
   uint32_t gdim[3];
   ar_batch* solo = nullptr;
@@ -590,10 +557,7 @@ struct ar_batch {
   long nt = 0, bt = 0;
   uint64_t total_cells = 0;
   int key_bits = 1, passes = 1, last_bits = 1;
-  // the keys of the current state exist (written by the last step or a prologue); the cell
-  // table is empty between steps (each step resets the cells it occupied)
-  bool keys_valid = false;
-  std::vector<unsigned> epochs;  // member scenes' upload epochs the keys were made from
+  // the cell table is empty between steps (each step resets the cells it occupied)
   // BVH broad phase (allocated only for BVH batches)
   int broadphase = AR_BROADPHASE_GRID;
   long cap_bvh = 0;
@@ -663,7 +627,6 @@ uint64_t scene_cells(const ar_scene* s) {
 ar_status prepare(ar_batch* B, cudaStream_t st) {
   if (!B->table_dirty) return AR_OK;
   drop_graph(B);
-  B->keys_valid = false;
   long nt = 0, bt = 0;
   uint64_t cells = 0;
   std::vector<SceneDev> tab;
@@ -677,6 +640,14 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
       d.g[a] = D.gravity[a];
       d.origin[a] = s->origin[a];
       d.cell[a] = s->cell[a];
+      d.inv_cell[a] = 1.0f / s->cell[a];
+    }
+    d.cell_pow2 = 1;
+    for (int a = 0; a < 3; ++a) {
+      int e = 0;
+      if (!(std::frexp(s->cell[a], &e) == 0.5f) || !std::isnormal(s->cell[a]) ||
+          !std::isnormal(d.inv_cell[a]))
+        d.cell_pow2 = 0;
     }
     d.r = D.radius; d.dt = D.dt; d.k = D.spring; d.damping = D.damping; d.shear = D.shear;
     d.attraction = D.attraction;
@@ -802,30 +773,10 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
 }
 
 // Stage boundaries for ar_step_profile: events[0] before the step, events[i] after stage i.
-// Grid: sort | scatter + cell table | collide | clear (next sort's histogram head) |
-// body sums + integration + next keys | (empty).  BVH: sort | tree (Karras nodes, leaves,
-// scene roots, refit) | collide | clear (refit counters) | body sums + integration + next
-// keys | (empty).
+// Grid: clear (sort histogram head) | cell keys + histogram | sort | scatter + cell table |
+// collide | body sums + integration (+ cell reset).  BVH: clear (refit counters) | Morton keys
+// | sort | tree (Karras nodes, leaves, scene roots, refit) | collide | body sums + integration.
 constexpr int kStages = 6;
-
-// Keys (and, for the grid, the sort histogram) of the current state; a step's last kernel
-// writes them for the next step, so this runs only when the state did not come from a step.
-ar_status enqueue_keys(ar_batch* B, cudaStream_t st) {
-  const int nt = (int)B->nt;
-  const unsigned g = std::min(arh::grid_for(nt, 256), (unsigned)B->ctx->num_sms * 8);
-  if (B->broadphase == AR_BROADPHASE_BVH) {
-    // steps zero the refit counters at their end for the next step; the first needs them too
-    cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);
-    morton_key_kernel<<<g, 256, 0, st>>>(B->d_table, B->d_pscene, (int)B->scenes.size(), nt,
-                                         B->keys64);
-  } else {
-    cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
-    grid_keys_kernel<<<std::min(arh::grid_for(nt, kK1Threads), (unsigned)B->ctx->num_sms * 4),
-                       kK1Threads, 0, st>>>(B->d_table, B->d_pscene, nt, B->keys,
-                                            (uint32_t*)B->sort_ws, B->passes, B->last_bits);
-  }
-  return arh::check_launch("step keys");
-}
 
 ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) {
   if (B->nt == 0) return AR_OK;
@@ -841,74 +792,74 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   const unsigned g5 = arh::grid_for((long)bt * 32, 256);
   mark(0);
   if (B->broadphase == AR_BROADPHASE_BVH) {
+    cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);  // refit arrival counters
+    mark(1);
+    morton_key_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->keys64,
+                                          B->d_step);
+    mark(2);
     ar_status s = ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
                                     B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
     if (s != AR_OK) return s;
-    mark(1);
+    mark(3);
     bvh_build_kernel<<<arh::grid_for(std::max(nt - 1, 1), 256), 256, 0, st>>>(
         ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
         B->right, B->parent, B->min_r, B->max_r, B->nodes);
     bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->svals, B->left,
                                           B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
-                                          B->min_r, B->max_r, B->d_step);
+                                          B->min_r, B->max_r);
     bvh_roots_kernel<<<arh::grid_for(ns, 128), 128, 0, st>>>(B->d_poff, ns, nt, B->parent,
                                                               B->min_r, B->max_r, B->roots);
     bvh_refit_kernel<<<arh::grid_for(nt, ar_lbvh::kRefitBlock), ar_lbvh::kRefitBlock, 0, st>>>(
         nt, B->left, B->parent, B->min_r, B->max_r, B->nodes, B->counters);
-    mark(2);
+    mark(4);
     bvh_collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(
         B->d_table, B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots,
         B->pforce, ctx->d_err);
-    mark(3);
-    cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);  // next step's refit
-    mark(4);
-    body_step_kernel<true><<<g5, 256, 0, st>>>(
-        B->d_table, B->d_bscene, bt, B->pforce, B->d_step, ctx->d_err, nullptr, B->keys64,
-        nullptr, 0, 0, nullptr, nt, nullptr);
     mark(5);
+    body_step_kernel<<<g5, 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->pforce, B->d_step,
+                                         ctx->d_err);
     mark(6);
     return arh::check_launch("step (BVH)");
   }
+  cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
+  mark(1);
+  grid_keys_kernel<<<std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4),
+                     kK1Threads, 0, st>>>(B->d_table, B->d_pscene, nt, B->keys,
+                                          (uint32_t*)B->sort_ws, B->passes, B->last_bits,
+                                          B->d_step);
+  mark(2);
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
                                   st, B->sort_ws, B->cap_sort, true);
   if (s != AR_OK) return s;
-  mark(1);
-  scatter_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->skeys, B->svals,
-                                     B->cells, B->spos, B->svel, B->d_step);
-  mark(2);
-  collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, nt, B->skeys, B->svals,
-                                                       B->cells, B->spos, B->svel, B->pforce);
   mark(3);
-  cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);  // next sort's head
+  scatter_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, nt, B->skeys, B->svals,
+                                     B->cells, B->spos, B->svel, B->d_step);
   mark(4);
-  body_step_kernel<false><<<g5, 256, 0, st>>>(
-      B->d_table, B->d_bscene, bt, B->pforce, B->d_step, ctx->d_err, B->keys, nullptr,
-      (uint32_t*)B->sort_ws, B->passes, B->last_bits, B->skeys, nt, B->cells);
+  collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, nt, B->skeys, B->svals,
+                                                       B->cells, B->spos, B->svel, B->pforce,
+                                                       B->d_step);
   mark(5);
+  body_step_kernel<<<g5, 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->pforce, B->d_step,
+                                       ctx->d_err);
   mark(6);
   return arh::check_launch("step");
 }
 
-// The keys of the current state exist (else enqueue them first).
-ar_status ensure_keys(ar_batch* B, cudaStream_t st) {
-  bool valid = B->keys_valid && B->epochs.size() == B->scenes.size();
-  for (size_t i = 0; valid && i < B->scenes.size(); ++i)
-    valid = B->epochs[i] == B->scenes[i]->epoch;
-  if (valid || B->nt == 0) return AR_OK;
-  B->epochs.resize(B->scenes.size());
-  for (size_t i = 0; i < B->scenes.size(); ++i) B->epochs[i] = B->scenes[i]->epoch;
-  B->keys_valid = true;
-  return enqueue_keys(B, st);
+// Before the step numbered host_step + 1: when that number opens a new 2^31 window of cell
+// epochs, refill the cell table so that no entry of the previous window can match.
+void before_step(ar_batch* B, cudaStream_t st) {
+  if (B->broadphase == AR_BROADPHASE_GRID && B->cells && ((B->host_step + 1) & 0x7fffffffLL) == 0)
+    cudaMemsetAsync(B->cells, 0xff, B->cap_cells * sizeof(uint4), st);
 }
 
 // Run n_steps eagerly with events between the stages; average milliseconds per stage.
 ar_status profile_steps(ar_batch* B, int n_steps, float* stage_ms, cudaStream_t st) {
-  if (ar_status k = ensure_keys(B, st); k != AR_OK) return k;
   cudaEvent_t ev[kStages + 1];
   for (auto& e : ev) cudaEventCreate(&e);
   double acc[kStages] = {0};
   ar_status s = AR_OK;
   for (int i = 0; i < n_steps && s == AR_OK; ++i) {
+    before_step(B, st);
     s = enqueue_step(B, st, ev);
     if (s != AR_OK) break;
     ++B->host_step;
@@ -931,9 +882,9 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
   ar_status s = prepare(B, st);
   if (s != AR_OK) return s;
   if (B->nt == 0 || n_steps <= 0) return AR_OK;
-  if ((s = ensure_keys(B, st)) != AR_OK) return s;
   if (!use_graph) {
     for (int i = 0; i < n_steps; ++i) {
+      before_step(B, st);
       if ((s = enqueue_step(B, st)) != AR_OK) return s;
       ++B->host_step;
     }
@@ -969,6 +920,7 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
     }
   }
   for (int i = 0; i < n_steps; ++i) {
+    before_step(B, st);
     if (cudaGraphLaunch(B->graph, st) != cudaSuccess) return arh::check_launch("graph launch");
     ++B->host_step;
   }
@@ -1232,7 +1184,6 @@ ar_status ar_scene_upload(ar_scene* s, const float* h_pos4, const float* h_quat4
   if (!s) return AR_ERR_INVALID_ARG;
   cudaStream_t st = arh::stream(stream);
   const size_t bytes = 16 * (size_t)s->nb;
-  ++s->epoch;  // the batches' next step recomputes the keys of this state
   if (h_pos4) cudaMemcpyAsync(s->pos, h_pos4, bytes, cudaMemcpyHostToDevice, st);
   if (h_quat4) cudaMemcpyAsync(s->quat, h_quat4, bytes, cudaMemcpyHostToDevice, st);
   if (h_vel4) cudaMemcpyAsync(s->vel, h_vel4, bytes, cudaMemcpyHostToDevice, st);
@@ -1335,11 +1286,10 @@ ar_status ar_batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph,
 
 int ar_batch_launches_per_step(ar_batch* B) {
   if (!B) return 0;
-  // steady-state step (the keys prologue runs only after a member change or an upload)
-  if (B->broadphase == AR_BROADPHASE_BVH)  // sort, 4 tree kernels, collide, memset, body
-    return ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 1 + 1 + 1;
-  return ar_sort::launches(0, B->key_bits, true) + 1 /*scatter*/ + 1 /*collide*/ +
-         1 /*memset*/ + 1 /*body*/;
+  if (B->broadphase == AR_BROADPHASE_BVH)  // memset, keys, sort, 4 tree kernels, collide, body
+    return 1 + 1 + ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 1 + 1;
+  return 1 /*memset*/ + 1 /*keys*/ + ar_sort::launches(0, B->key_bits, true) + 1 /*scatter*/ +
+         1 /*collide*/ + 1 /*body*/;
 }
 
 int ar_scene_launches_per_step(ar_scene* s) {

@@ -14,6 +14,8 @@ struct SceneDev {
   float g[3];               // gravity
   float r, dt, k, damping, shear, attraction;
   float origin[3], cell[3]; // grid
+  float inv_cell[3];        // 1 / cell, used when every cell edge is a power of two
+  int cell_pow2;            // (then x * inv_cell == x / cell exactly)
   uint32_t gx, gy, gz;      // cells per axis (powers of two)
   uint32_t lx, ly;          // log2 gx, log2 gy
   uint32_t cell_base;       // first cell of the scene in the batch's global cell space
@@ -32,6 +34,10 @@ struct SceneDev {
 };
 
 __host__ __device__ __forceinline__ int3 cell_of(const SceneDev& s, float3 p) {
+  if (s.cell_pow2)  // division by a power of two is the multiplication by its inverse
+    return make_int3((int)floorf((p.x - s.origin[0]) * s.inv_cell[0]),
+                     (int)floorf((p.y - s.origin[1]) * s.inv_cell[1]),
+                     (int)floorf((p.z - s.origin[2]) * s.inv_cell[2]));
   return make_int3((int)floorf((p.x - s.origin[0]) / s.cell[0]),
                    (int)floorf((p.y - s.origin[1]) / s.cell[1]),
                    (int)floorf((p.z - s.origin[2]) / s.cell[2]));

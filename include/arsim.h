@@ -504,13 +504,11 @@ AR_API ar_status ar_step(ar_ctx* ctx, ar_scene* scene, int n_steps, int use_grap
                          ar_stream_t stream);
 
 /* Run n_steps of the scene without a graph, with CUDA events between the stages, and return
- * the average device milliseconds per stage in h_stage_ms[6].  Grid: sort, scatter + cell
- * table, DEM gather + walls, clear (next sort's histogram head), body sums + integration +
- * next step's keys, 0.  BVH: sort, tree (build, leaves, scene roots, refit), DEM traversal +
- * walls, clear (refit counters), body sums + integration + next keys, 0.  A step computes the
- * next step's sort keys in its last kernel; the keys of a state that did not come from a step
- * (new member list, upload) are computed once before the first step and are not part of any
- * stage.  (Replaces the reference's clock() accumulators, e.g.
+ * the average device milliseconds per stage in h_stage_ms[6].  Grid: clear (sort histogram
+ * head), re-pose + cell keys + histogram, sort, scatter + cell table, DEM gather + walls, body
+ * sums + integration (+ cell reset).  BVH: clear (refit counters), Morton keys, sort, tree
+ * (build, leaves, scene roots, refit), DEM traversal + walls, body sums + integration.
+ * (Replaces the reference's clock() accumulators, e.g.
  * RigidBodies/UniformGridUpdate.cpp:338-446.) */
 AR_API ar_status ar_step_profile(ar_ctx* ctx, ar_scene* scene, int n_steps, float* h_stage_ms,
                                  ar_stream_t stream);
