@@ -128,6 +128,8 @@ SIGNATURES = {
     "ar_scene_cells": [C.POINTER(SceneDesc)],
     "ar_scene_destroy_async": [P, S],
     "ar_batch_set_scenes_limited": [P, C.POINTER(P), I, P],
+    "ar_batch_model_matrices": [P, P, S],
+    "ar_scene_model_matrices": [P, P, S],
     "ar_scene_download": [P, P, P, P, P, S],
     "ar_scene_download_async": [P, P, P, P, P, S],
     "ar_scene_upload": [P, P, P, P, P, S],

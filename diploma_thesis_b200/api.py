@@ -190,6 +190,13 @@ class GpuScene:
         out["_pinned"] = pinned  # keeps the pinned blocks alive
         return out
 
+    def model_matrices(self, stream=None) -> torch.Tensor:
+        """[B, 4, 4] device tensor of per-body model matrices (glm column-major: row i of the
+        tensor is column i of the matrix) for a renderer."""
+        out = torch.empty((self.num_bodies, 4, 4), dtype=torch.float32, device="cuda")
+        call("ar_scene_model_matrices", self.handle, ptr(out), stream_handle(stream))
+        return out
+
     def close_async(self, stream=None) -> None:
         """Free in stream order on `stream`; every use of the scene must precede that point."""
         if self.handle:

@@ -506,6 +506,26 @@ __global__ void __launch_bounds__(256) body_step_kernel(
   }
 }
 
+// ---- render hand-off: per-body model matrices -------------------------------------------------
+// The matrix GPUintegratorKernel writes for the renderer (Kernels/rigidBodyKernels.cu:322-331):
+// glm::mat4 (column-major) holding mat3_cast of the orientation and the centre as translation.
+__global__ void __launch_bounds__(256) model_matrices_kernel(const SceneDev* __restrict__ table,
+                                                             const int* __restrict__ bscene,
+                                                             int bt, float* __restrict__ out) {
+  for (int gb = blockIdx.x * blockDim.x + threadIdx.x; gb < bt; gb += gridDim.x * blockDim.x) {
+    const SceneDev& S = table[__ldg(bscene + gb)];
+    const int b = gb - S.boff;
+    const float4 q = S.quat[b], c = S.pos[b];
+    float m[9];
+    ar_glm::mat3_cast(q, m);
+    float4* o = reinterpret_cast<float4*>(out + 16 * (size_t)gb);
+    o[0] = make_float4(m[0], m[1], m[2], 0.f);
+    o[1] = make_float4(m[3], m[4], m[5], 0.f);
+    o[2] = make_float4(m[6], m[7], m[8], 0.f);
+    o[3] = make_float4(c.x, c.y, c.z, 1.f);
+  }
+}
+
 int ceil_log2(uint64_t v) {
   int b = 0;
   while ((1ull << b) < v) ++b;
@@ -1282,6 +1302,28 @@ ar_status ar_batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph,
                         ar_stream_t stream) {
   if (!ctx || !B || n_steps < 0) return AR_ERR_INVALID_ARG;
   return batch_step(ctx, B, n_steps, use_graph, arh::stream(stream));
+}
+
+ar_status ar_batch_model_matrices(ar_batch* B, float* d_model16, ar_stream_t stream) {
+  if (!B || !d_model16) return AR_ERR_INVALID_ARG;
+  if (((uintptr_t)d_model16 & 15u) != 0) {
+    arh::set_error("ar_batch_model_matrices: the output must be 16-byte aligned");
+    return AR_ERR_INVALID_ARG;
+  }
+  cudaStream_t st = arh::stream(stream);
+  ar_status s = prepare(B, st);
+  if (s != AR_OK) return s;
+  if (B->bt == 0) return AR_OK;
+  model_matrices_kernel<<<std::min(arh::grid_for(B->bt, 256), 4096u), 256, 0, st>>>(
+      B->d_table, B->d_bscene, (int)B->bt, d_model16);
+  return arh::check_launch("ar_batch_model_matrices");
+}
+
+ar_status ar_scene_model_matrices(ar_scene* s, float* d_model16, ar_stream_t stream) {
+  if (!s) return AR_ERR_INVALID_ARG;
+  ar_status st = ensure_solo(s);
+  if (st != AR_OK) return st;
+  return ar_batch_model_matrices(s->solo, d_model16, stream);
 }
 
 int ar_batch_launches_per_step(ar_batch* B) {

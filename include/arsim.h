@@ -542,6 +542,13 @@ AR_API ar_status ar_batch_step(ar_ctx* ctx, ar_batch* batch, int n_steps, int us
 /* ar_step_profile for a batch. */
 AR_API ar_status ar_batch_profile(ar_ctx* ctx, ar_batch* batch, int n_steps,
                                   float* h_stage_ms, ar_stream_t stream);
+/* Render hand-off (replaces the reference's modelMatrixGPU output of GPUintegratorKernel,
+ * Kernels/rigidBodyKernels.cu:322-331, and its GL buffer): one glm::mat4 per body,
+ * column-major (16 floats: mat3_cast of the orientation, translation = body centre), written
+ * to a 16-byte aligned device buffer -- for a batch in member order, one launch. */
+AR_API ar_status ar_batch_model_matrices(ar_batch* batch, float* d_model16, ar_stream_t stream);
+AR_API ar_status ar_scene_model_matrices(ar_scene* scene, float* d_model16, ar_stream_t stream);
+
 /* Number of kernel launches one step of this batch issues (for launch accounting). */
 AR_API int ar_batch_launches_per_step(ar_batch* batch);
 AR_API int ar_scene_launches_per_step(ar_scene* scene);

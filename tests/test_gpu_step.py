@@ -140,3 +140,17 @@ def test_config0_first_steps_bit_exact(ctx):
     for k in ("pos", "quat", "vel", "angvel"):
         assert np.array_equal(got[k], ref[k]), k
     gs.close()
+
+
+def test_model_matrices_for_the_renderer(ctx):
+    sc = scenes.small_scene(12, nb_side=3, packed=True, r=1 / 128)
+    gs = api.GpuScene(ctx, sc)
+    gs.step(5, use_graph=True)
+    m = gs.model_matrices().cpu().numpy()
+    st = gs.download()
+    R = scenes.quat_to_matrix(st["quat"].astype(np.float64))
+    # glm column-major: m[b, c, r] = element (r, c); column 3 holds the centre
+    assert np.allclose(m[:, :3, :3], np.transpose(R, (0, 2, 1)), atol=2e-6)
+    assert np.array_equal(m[:, 3, :3], st["pos"][:, :3])
+    assert np.all(m[:, :3, 3] == 0) and np.all(m[:, 3, 3] == 1)
+    gs.close()
