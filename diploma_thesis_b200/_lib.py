@@ -109,6 +109,7 @@ SIGNATURES = {
     "ar_calc_hash": [P, C.POINTER(SimParams), P, I, P, P, S],
     "ar_reorder_cells": [P, P, P, P, P, I, C.c_uint32, P, P, P, P, S],
     "ar_collide_grid_dem": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, I, P, P, S],
+    "ar_collide_static_scene_dem": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, I, P, P, P, S],
     "ar_reduce_bodies": [P, P, P, P, I, P, P, S],
     "ar_reduce_impulses": [P, P, P, P, I, P, P, P, P, S],
     "ar_integrate_reference": [P, C.POINTER(SimParams), F, I, P, P, P, P, P, P, P, P, P, S],

@@ -95,6 +95,64 @@ __global__ void __launch_bounds__(128) collide_grid_kernel(
   p_torque[orig] = make_float4(q.x + t.x, q.y + t.y, q.z + t.z, q.w + 0.f);
 }
 
+// FindAndHandleAugmentedRealityCollisionsUniformGridKernel (RigidBodies/UniformGridDEM.cu:
+// 243-377): per sorted particle, the static scene's particles (sorted into the same grid, with
+// their own cell table) in the 27 neighbour cells, z, y, x order; for d < 2r a DEM impulse
+// along the negated scene normal of the scene particle (unsorted normals, indexed through the
+// scene's sorted indices): -spring (2r - d) n + damping v_rel + shear v_t + attraction p_rel,
+// v_rel = 0 - v.  Summed per cell, then added to the particle's linear impulse, and
+// rel x sum to its angular impulse; colour set to green on any contact.
+__global__ void __launch_bounds__(128) collide_static_kernel(
+    ar_sim_params prm, ar_grid::Grid g, const float4* __restrict__ spos,
+    const float4* __restrict__ svel, const float4* __restrict__ rel,
+    const float4* __restrict__ scene_spos, const float4* __restrict__ scene_normals,
+    const uint32_t* __restrict__ gidx, const uint32_t* __restrict__ scene_gidx,
+    const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, int n,
+    float4* __restrict__ p_lin, float4* __restrict__ p_ang, float4* __restrict__ color) {
+  const int index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= n) return;
+  const float3 pos = ar::xyz(__ldg(spos + index));
+  const float3 vel = ar::xyz(__ldg(svel + index));
+  const int3 gp = g.cell_of(pos);
+  const uint32_t orig = __ldg(gidx + index);
+  const float thr = 2.0f * prm.particle_radius;
+  int contacts = 0;
+  float4 lin = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int z = -1; z <= 1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x) {
+        float4 cell_f = make_float4(0.f, 0.f, 0.f, 0.f);
+        const uint32_t h = g.hash(make_int3(gp.x + x, gp.y + y, gp.z + z));
+        const uint32_t st = __ldg(cstart + h);
+        if (st != ar::kEmpty) {
+          const uint32_t en = __ldg(cend + h);
+          for (uint32_t j = st; j < en; ++j) {
+            const uint32_t o2 = __ldg(scene_gidx + j);
+            const float3 rp = ar::sub(ar::xyz(__ldg(scene_spos + j)), pos);
+            const float dist = sqrtf(ar::dot(rp, rp));
+            if (!(dist < thr)) continue;
+            const float3 nn = ar::xyz(__ldg(scene_normals + o2));
+            const float3 nrm = ar::mk3(-nn.x, -nn.y, -nn.z);
+            const float3 rv = ar::mk3(0.f - vel.x, 0.f - vel.y, 0.f - vel.z);
+            const float3 tv = ar::sub(rv, ar::scl(ar::dot(rv, nrm), nrm));
+            float3 f = ar::scl(-prm.spring * (thr - dist), nrm);
+            f = ar::add(f, ar::scl(prm.damping, rv));
+            f = ar::add(f, ar::scl(prm.shear, tv));
+            f = ar::add(f, ar::scl(prm.attraction, rp));
+            cell_f = make_float4(cell_f.x + f.x, cell_f.y + f.y, cell_f.z + f.z, cell_f.w + 0.f);
+            ++contacts;
+          }
+        }
+        lin = make_float4(lin.x + cell_f.x, lin.y + cell_f.y, lin.z + cell_f.z, lin.w + cell_f.w);
+      }
+  if (contacts && color) color[orig] = make_float4(0.f, 1.f, 0.f, 0.f);
+  const float4 a = p_lin[orig];
+  p_lin[orig] = make_float4(a.x + lin.x, a.y + lin.y, a.z + lin.z, a.w + lin.w);
+  const float3 t = ar::cross(ar::xyz(__ldg(rel + orig)), ar::xyz(lin));
+  const float4 b = p_ang[orig];
+  p_ang[orig] = make_float4(b.x + t.x, b.y + t.y, b.z + t.z, b.w + 0.f);
+}
+
 // collideD / collideCell / collideSpheres (Kernels/particleKernels.cu:261-406): the particle
 // variant -- every occupant that passes the body test contributes (zero when apart), torque
 // accumulates per cell, free particles (body -1) get their velocity updated instead.
@@ -244,6 +302,31 @@ ar_status ar_collide_grid_dem(ar_ctx* ctx, const ar_sim_params* params, const in
       (const float4*)rel4, grid_idx, cell_start, cell_end, n, (float4*)p_force4,
       (float4*)p_torque4);
   return arh::check_launch("ar_collide_grid_dem");
+}
+
+ar_status ar_collide_static_scene_dem(ar_ctx* ctx, const ar_sim_params* params,
+                                      const float* sorted_pos4, const float* sorted_vel4,
+                                      const float* rel4, const float* scene_sorted_pos4,
+                                      const float* scene_normals4, const uint32_t* grid_idx,
+                                      const uint32_t* scene_grid_idx,
+                                      const uint32_t* scene_cell_start,
+                                      const uint32_t* scene_cell_end, int n,
+                                      float* p_linear4, float* p_angular4, float* color4,
+                                      ar_stream_t stream) {
+  if (!ctx || !params || n < 0 ||
+      (n > 0 && (!sorted_pos4 || !sorted_vel4 || !rel4 || !scene_sorted_pos4 ||
+                 !scene_normals4 || !grid_idx || !scene_grid_idx || !scene_cell_start ||
+                 !scene_cell_end || !p_linear4 || !p_angular4)))
+    return AR_ERR_INVALID_ARG;
+  ar_grid::Grid g;
+  ar_status s = grid_from_params(params, &g);
+  if (s != AR_OK || n == 0) return s;
+  collide_static_kernel<<<arh::grid_for(n, 128), 128, 0, arh::stream(stream)>>>(
+      *params, g, (const float4*)sorted_pos4, (const float4*)sorted_vel4, (const float4*)rel4,
+      (const float4*)scene_sorted_pos4, (const float4*)scene_normals4, grid_idx, scene_grid_idx,
+      scene_cell_start, scene_cell_end, n, (float4*)p_linear4, (float4*)p_angular4,
+      (float4*)color4);
+  return arh::check_launch("ar_collide_static_scene_dem");
 }
 
 ar_status ar_collide_grid_particles(ar_ctx* ctx, const ar_sim_params* params,

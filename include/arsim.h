@@ -250,6 +250,26 @@ AR_API ar_status ar_reorder_cells(ar_ctx* ctx, const uint32_t* sorted_hash,
                                   uint32_t* cell_start, uint32_t* cell_end, float* sorted_pos4,
                                   float* sorted_vel4, ar_stream_t stream);
 
+/* ---- AR static scene (point cloud with normals) against the particles ---------------------
+ * FindAndHandleAugmentedRealityCollisionsUniformGridKernel (RigidBodies/UniformGridDEM.cu:
+ * 243-377): the scene's particles are hashed, sorted and given cell ranges with the same grid
+ * (ar_calc_hash, ar_radix_sort_pairs_u32, ar_reorder_cells); then per sorted particle, the
+ * scene particles in its 27 neighbour cells (z, y, x order) with d < 2r give
+ *   I += -spring (2r - d) n + damping v_rel + shear v_t + attraction p_rel,
+ * n = -(normal of the scene particle, unsorted, through scene_grid_idx), v_rel = -v; summed
+ * per cell, then p_linear4[orig] += I, p_angular4[orig] += rel4[orig] x I, and color4[orig] =
+ * (0, 1, 0, 0) when any contact (color4 may be NULL). */
+AR_API ar_status ar_collide_static_scene_dem(ar_ctx* ctx, const ar_sim_params* params,
+                                             const float* sorted_pos4, const float* sorted_vel4,
+                                             const float* rel4, const float* scene_sorted_pos4,
+                                             const float* scene_normals4,
+                                             const uint32_t* grid_idx,
+                                             const uint32_t* scene_grid_idx,
+                                             const uint32_t* scene_cell_start,
+                                             const uint32_t* scene_cell_end, int n,
+                                             float* p_linear4, float* p_angular4,
+                                             float* color4, ar_stream_t stream);
+
 /* ---- (a15) DEM contact forces on the grid ------------------------------------------------------
  * FindAndHandleRigidBodyCollisionsUniformGridKernel (RigidBodies/UniformGridDEM.cu:57-241):
  * per sorted particle, the 27 neighbour cells in z, y, x order (-1..1), occupants in sorted

@@ -337,6 +337,20 @@ void FindAndHandleRigidBodyCollisionsUniformGridWrapper(
             "FindAndHandleRigidBodyCollisionsUniformGridWrapper");
 }
 
+void FindAndHandleAugmentedRealityCollisionsUniformGridWrapper(
+    float4* pLinearImpulse, float4* pAngularImpulse, float4* color, float4* sortedPos,
+    float4* sortedVel, float4* relativePos, float4* ARPos, float4* ARnormals,
+    uint* gridParticleIndex, uint* gridParticleIndexAR, uint* cellStart, uint* cellEnd,
+    uint numParticles, SimParams params, int numThreads) {
+  (void)numThreads;
+  ARC_CHECK(ar_collide_static_scene_dem(
+                ARC_CTX, arsim_compat_detail::P(params), (float*)sortedPos, (float*)sortedVel,
+                (float*)relativePos, (float*)ARPos, (float*)ARnormals, gridParticleIndex,
+                gridParticleIndexAR, cellStart, cellEnd, (int)numParticles,
+                (float*)pLinearImpulse, (float*)pAngularImpulse, (float*)color, nullptr),
+            "FindAndHandleAugmentedRealityCollisionsUniformGridWrapper");
+}
+
 void ReducePerParticleImpulses(int* rbIndices, float4* pLinearImpulse, float4* pAngularImpulse,
                                float4* rbVel, float4* rbAng, float* rbMass, glm::mat3* rbInertia,
                                int* particlesPerObject, int numRigidBodies, int numParticles,

@@ -385,3 +385,23 @@ def reduce_rigid_body_variables(pf4, pt4, starts, counts, bf4, bt4):
     ok = _L.or_reduce_rbvars(_p(_f32(pf4)), _p(_f32(pt4)), _p(_i32(starts)), _p(_i32(counts)),
                              len(starts), _p(bf), _p(bt))
     return bf, bt, bool(ok)
+
+
+_L.or_collide_static_scene.restype = None
+
+
+def collide_static_scene(origin, cell, dims, radius, prm4, spos4, svel4, rel4, scene_spos4,
+                         scene_normals4, gidx, scene_gidx, cstart, cend, lin4, ang4):
+    """FindAndHandleAugmentedRealityCollisionsUniformGridKernel; returns updated (linear,
+    angular, color)."""
+    n = len(spos4)
+    lin, ang = _f32(lin4).copy(), _f32(ang4).copy()
+    color = np.zeros((len(lin), 4), np.float32)
+    g6 = _f32(list(origin) + list(cell))
+    _L.or_collide_static_scene(_p(g6), _p(_u32(dims)), C.c_float(radius), _p(_f32(prm4)),
+                               _p(_f32(spos4)), _p(_f32(svel4)), _p(_f32(rel4)),
+                               _p(_f32(scene_spos4)), _p(_f32(scene_normals4)), _p(_u32(gidx)),
+                               _p(_u32(scene_gidx)), _p(_u32(cstart)), _p(_u32(cend)), n,
+                               _p(lin), _p(ang), _p(color))
+    return lin, ang, color
+

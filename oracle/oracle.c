@@ -1048,6 +1048,65 @@ int or_step_bvh(const float* s15, int nb, int n, float* bpos4, float* bquat4, fl
   return ok;
 }
 
+/* ====================================================================================
+ * AR static scene against the particles -- FindAndHandleAugmentedRealityCollisionsUniform-
+ * GridCell / Kernel (RigidBodies/UniformGridDEM.cu:243-377).  The scene's particles are
+ * sorted into the same grid with their own cell table; normals are unsorted.
+ * prm = {spring, damping, shear, attraction}.  lin4 / ang4 are accumulated in place; color4
+ * (may be NULL) is set to (0, 1, 0, 0) for particles with a contact.
+ * ==================================================================================== */
+void or_collide_static_scene(const float* grid6, const uint32_t* dims3, float radius,
+                             const float* prm, const float* spos4, const float* svel4,
+                             const float* rel4, const float* scene_spos4,
+                             const float* scene_normals4, const uint32_t* gidx,
+                             const uint32_t* scene_gidx, const uint32_t* cstart,
+                             const uint32_t* cend, int n, float* lin4, float* ang4,
+                             float* color4) {
+  grid_t G;
+  memcpy(G.o, grid6, 12); memcpy(G.c, grid6 + 3, 12); memcpy(G.g, dims3, 12);
+  const float thr = 2.0f * radius;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; ++k) {
+    v3 pos = xyz(spos4 + 4l * k), vel = xyz(svel4 + 4l * k);
+    int gp[3];
+    cell_of(&G, pos, gp);
+    uint32_t orig = gidx[k];
+    int contacts = 0;
+    float lin[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int z = -1; z <= 1; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int x = -1; x <= 1; ++x) {
+          float cf[4] = {0.f, 0.f, 0.f, 0.f};
+          uint32_t h = hash3(&G, gp[0] + x, gp[1] + y, gp[2] + z);
+          if (cstart[h] != 0xffffffffu) {
+            for (uint32_t j = cstart[h]; j < cend[h]; ++j) {
+              uint32_t o2 = scene_gidx[j];
+              v3 rp = sub(xyz(scene_spos4 + 4l * j), pos);
+              float dist = sqrtf(dot(rp, rp));
+              if (!(dist < thr)) continue;
+              v3 nn = xyz(scene_normals4 + 4l * o2);
+              v3 nrm = mk3(-nn.x, -nn.y, -nn.z);
+              v3 rv = mk3(0.f - vel.x, 0.f - vel.y, 0.f - vel.z);
+              v3 tv = sub(rv, scl(dot(rv, nrm), nrm));
+              v3 f = scl(-prm[0] * (thr - dist), nrm);
+              f = add(f, scl(prm[1], rv));
+              f = add(f, scl(prm[2], tv));
+              f = add(f, scl(prm[3], rp));
+              cf[0] = cf[0] + f.x; cf[1] = cf[1] + f.y; cf[2] = cf[2] + f.z; cf[3] = cf[3] + 0.f;
+              ++contacts;
+            }
+          }
+          for (int c = 0; c < 4; ++c) lin[c] = lin[c] + cf[c];
+        }
+    if (contacts && color4) st4(color4 + 4l * orig, 0.f, 1.f, 0.f, 0.f);
+    float* L = lin4 + 4l * orig;
+    st4(L, L[0] + lin[0], L[1] + lin[1], L[2] + lin[2], L[3] + lin[3]);
+    v3 t = cross(xyz(rel4 + 4l * orig), mk3(lin[0], lin[1], lin[2]));
+    float* A = ang4 + 4l * orig;
+    st4(A, A[0] + t.x, A[1] + t.y, A[2] + t.z, A[3] + 0.f);
+  }
+}
+
 /* ---- FP64 oracle of the same physics (summation order free, all-pairs within cells) ---- */
 static d3 dk3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
 static d3 dadd(d3 a, d3 b) { return dk3(a.x + b.x, a.y + b.y, a.z + b.z); }

@@ -163,6 +163,21 @@ def global_attributes(cms4, rbvel4, rbang4, quat4, rb_idx, rel4):
     return rel, pos, vel, q
 
 
+def collide_static_scene(params, spos4, svel4, rel4, scene_spos4, scene_normals4, gidx,
+                         scene_gidx, cstart, cend, lin4, ang4):
+    """FindAndHandleAugmentedRealityCollisionsUniformGridKernel; returns updated (linear,
+    angular, color)."""
+    n = len(spos4)
+    lin, ang = _f32(lin4).copy(), _f32(ang4).copy()
+    color = np.zeros((len(lin), 4), np.float32)
+    lib().refcpu_collide_static_scene(C.byref(params), _p(lin), _p(ang), _p(color),
+                                      _p(_f32(spos4)), _p(_f32(svel4)), _p(_f32(rel4)),
+                                      _p(_f32(scene_spos4)), _p(_f32(scene_normals4)),
+                                      _p(_u32(gidx)), _p(_u32(scene_gidx)), _p(_u32(cstart)),
+                                      _p(_u32(cend)), n)
+    return lin, ang, color
+
+
 def collide_bvh_rigid(params, rb_idx, rel4, vel4, tree, cms4, bounds8, sorted_idx, radii):
     n = len(sorted_idx)
     pf = np.zeros((n, 4), np.float32)

@@ -41,6 +41,7 @@ RANGES = [
     ("Kernels/particleKernels.cu", 150, 189, "calculate position in uniform grid"),  # calcGridPos, calcGridHash, calcHashD
     ("Kernels/particleKernels.cu", 260, 406, "collide two spheres using DEM"),   # collideSpheres, collideCell, collideD
     ("RigidBodies/UniformGridDEM.cu", 24, 204, "calculate position in uniform grid"),  # DEM grid collide cell + kernel
+    ("RigidBodies/UniformGridDEM.cu", 243, 377, "__device__"),                    # AR static-scene DEM cell + kernel
     ("RigidBodies/UniformGridDEM.cu", 420, 460, "Now apply total impulse"),      # CombineReducedImpulses
     ("Kernels/rigidBodyKernels.cu", 37, 166, "/*"),                              # integrateRigidBody
     ("Kernels/rigidBodyKernels.cu", 262, 348, "GPUintegratorKernel"),            # GPUintegratorKernel

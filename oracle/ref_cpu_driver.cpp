@@ -214,6 +214,25 @@ void refcpu_collide_grid_dem(const void* sim_params, const int* rb_idx, float* p
   });
 }
 
+// ---- FindAndHandleAugmentedRealityCollisionsUniformGridKernel (UniformGridDEM.cu:243-377) --
+// The static scene's particles are sorted into their own grid (cell_start/cell_end over the
+// scene's sorted order); impulses are added to p_linear4 / p_angular4 in place.
+void refcpu_collide_static_scene(const void* sim_params, float* p_linear4, float* p_angular4,
+                                 float* color4, const float* sorted_pos4,
+                                 const float* sorted_vel4, const float* rel4,
+                                 const float* scene_sorted_pos4, const float* scene_normals4,
+                                 const uint32_t* grid_idx, const uint32_t* scene_grid_idx,
+                                 const uint32_t* cell_start, const uint32_t* cell_end, int n) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  launch(n, 128, true, [&] {
+    FindAndHandleAugmentedRealityCollisionsUniformGridKernel(
+        (float4*)p_linear4, (float4*)p_angular4, (float4*)color4, (float4*)sorted_pos4,
+        (float4*)sorted_vel4, (float4*)rel4, (float4*)scene_sorted_pos4, (float4*)scene_normals4,
+        (uint*)grid_idx, (uint*)scene_grid_idx, (uint*)cell_start, (uint*)cell_end, (uint)n, p);
+  });
+}
+
 // ---- ReducePerParticleImpulses (UniformGridDEM.cu:462-666) with CombineReducedImpulses ---
 // The two CUB float4 inclusive scans are restated as sequential float scans.
 void refcpu_reduce_impulses(const float* p_force4, const float* p_torque4, float* rb_vel4,

@@ -11,6 +11,7 @@
 //   __clz, __int2double_rn, __double2int_ru     -> exact integer / double equivalents
 //   __fsqrt_rz                                  -> square root rounded toward zero
 //   atomicAdd(int*)                             -> a sequentially consistent fetch-add
+//   unary minus on a float3 rvalue              -> a const overload
 //   min/max on float and unsigned               -> fminf/fmaxf and unsigned compare
 //     (device code resolves min/max(float) to fminf/fmaxf; the reference's host
 //      helper header only declares int versions, which would truncate floats)
@@ -38,3 +39,6 @@ inline float min(float a, float b) { return std::fmin(a, b); }
 inline float max(float a, float b) { return std::fmax(a, b); }
 inline unsigned int min(unsigned int a, unsigned int b) { return a < b ? a : b; }
 inline unsigned int max(unsigned int a, unsigned int b) { return a > b ? a : b; }
+// helper_math.h's unary minus takes float3& (MSVC bound an rvalue to it at
+// RigidBodies/UniformGridDEM.cu:284); a const overload gives the same negation for rvalues.
+inline float3 operator-(const float3& a) { return make_float3(-a.x, -a.y, -a.z); }

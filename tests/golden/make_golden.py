@@ -101,6 +101,51 @@ def dem_case(seed: int):
                 bang=bang, ref_reduced_vel=rvel, ref_reduced_ang=rang)
 
 
+def static_scene_case(seed: int):
+    """Particles of a packed scene against a wavy static point cloud with normals (the AR
+    scene) that cuts through them."""
+    sc = scenes.small_scene(seed, nb_side=4, packed=True)
+    rng = np.random.default_rng(seed + 200)
+    pos = sc.world_positions()
+    n = len(pos)
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0, 0.3, (n, 3))
+    rel = sc.particle_rel.copy()
+    r = sc.radius
+    lo, hi = pos[:, :3].min(0), pos[:, :3].max(0)
+    xs = np.arange(lo[0] - 2 * r, hi[0] + 2 * r, 2 * r, dtype=np.float32)
+    zs = np.arange(lo[2] - 2 * r, hi[2] + 2 * r, 2 * r, dtype=np.float32)
+    X, Z = np.meshgrid(xs, zs, indexing="ij")
+    ymid = 0.5 * (lo[1] + hi[1])
+    Y = ymid + 3 * r * np.sin(X * 40.0) * np.cos(Z * 30.0)
+    m = X.size
+    spos = np.zeros((m, 4), np.float32)
+    spos[:, 0], spos[:, 1], spos[:, 2] = X.ravel(), Y.ravel(), Z.ravel()
+    nrm = np.zeros((m, 4), np.float32)
+    gx = -3 * r * 40.0 * np.cos(X * 40.0) * np.cos(Z * 30.0)
+    gz = 3 * r * 30.0 * np.sin(X * 40.0) * np.sin(Z * 30.0)
+    nv = np.stack([-gx.ravel(), np.ones(m), -gz.ravel()], 1)
+    nrm[:, :3] = nv / np.linalg.norm(nv, axis=1, keepdims=True)
+    dims = (16, 16, 16)
+    cell = np.float32(2 * r)
+    prm = params_for(r, (0.0, 0.0, 0.0), cell, dims, 0.5, 0.02, 0.1, 0.001)
+    h, idx = ref.calc_hash(prm, pos)
+    sh, si = ref.sort_pairs_u32(h, idx)
+    _, _, sp, sv = ref.reorder(sh, si, pos, vel, int(np.prod(dims)))
+    ah, aidx = ref.calc_hash(prm, spos)
+    ash, asi = ref.sort_pairs_u32(ah, aidx)
+    acs, ace, asp, _ = ref.reorder(ash, asi, spos, np.zeros_like(spos), int(np.prod(dims)))
+    lin0 = rng.normal(0, 1, (n, 4)).astype(np.float32)
+    ang0 = rng.normal(0, 1, (n, 4)).astype(np.float32)
+    lin, ang, color = ref.collide_static_scene(prm, sp, sv, rel, asp, nrm, si, asi, acs, ace,
+                                               lin0, ang0)
+    return dict(radius=np.float32(r), cell=cell, dims=np.array(dims, np.uint32),
+                prm=np.array([0.5, 0.02, 0.1, 0.001], np.float32), spos=sp, svel=sv, rel=rel,
+                sidx=si, scene_pos=spos, scene_normals=nrm, scene_spos=asp, scene_sidx=asi,
+                scene_cell_start=acs, scene_cell_end=ace, lin0=lin0, ang0=ang0, lin=lin,
+                ang=ang, color=color)
+
+
 def body_case(seed: int):
     sc = scenes.small_scene(seed, nb_side=3, v_sigma=1.0)
     rng = np.random.default_rng(seed + 7)
@@ -195,6 +240,7 @@ def main() -> None:
     np.savez_compressed(OUT / "dem_small.npz", **dem_case(5))
     np.savez_compressed(OUT / "bodies_small.npz", **body_case(9))
     np.savez_compressed(OUT / "reference_extra.npz", **extra_case(21))
+    np.savez_compressed(OUT / "static_scene.npz", **static_scene_case(31))
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
 

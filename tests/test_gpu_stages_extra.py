@@ -94,3 +94,21 @@ def test_bvh_traversal_without_parent_array(ctx):
          P(bounds), P(sidx), P(radii), n, P(pf), P(pt), P(pp), S())
     assert np.array_equal(host(pf), d["bvh_pforce"])
     assert np.array_equal(host(pt), d["bvh_ptorque"])
+
+
+def test_static_scene_collisions_golden(ctx):
+    """AR static scene: the reference kernel's impulses, angular impulses and colours."""
+    g = golden("static_scene")
+    n = len(g["spos"])
+    prm = api.sim_params(float(g["radius"]), (0, 0, 0), float(g["cell"]), g["dims"],
+                         *[float(x) for x in g["prm"]])
+    lin, ang = dev(g["lin0"]), dev(g["ang0"])
+    color = empty((n, 4))
+    call("ar_collide_static_scene_dem", ctx.handle, C.byref(prm), P(dev(g["spos"])),
+         P(dev(g["svel"])), P(dev(g["rel"])), P(dev(g["scene_spos"])),
+         P(dev(g["scene_normals"])), P(dev(g["sidx"])), P(dev(g["scene_sidx"])),
+         P(dev(g["scene_cell_start"])), P(dev(g["scene_cell_end"])), n, P(lin), P(ang),
+         P(color), S())
+    ctx.check()
+    assert np.array_equal(host(lin), g["lin"]) and np.array_equal(host(ang), g["ang"])
+    assert np.array_equal(host(color), g["color"])

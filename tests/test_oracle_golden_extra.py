@@ -54,3 +54,17 @@ def test_reduce_rigid_body_variables_adds_and_flags_nan():
         np.testing.assert_allclose(bf[b, :3], bf0[b, :3] + s, rtol=1e-5, atol=1e-5)
     pf[45, 1] = np.nan
     assert not cpu.reduce_rigid_body_variables(pf, pt, starts, counts, bf0, bt0)[2]
+
+
+def test_static_scene_collisions_match_reference():
+    """FindAndHandleAugmentedRealityCollisionsUniformGridKernel: particles against a static
+    point cloud with normals (RigidBodies/UniformGridDEM.cu:243-377)."""
+    g = golden("static_scene")
+    c = float(g["cell"])
+    lin, ang, color = cpu.collide_static_scene(
+        (0.0, 0.0, 0.0), (c, c, c), g["dims"], float(g["radius"]), g["prm"], g["spos"],
+        g["svel"], g["rel"], g["scene_spos"], g["scene_normals"], g["sidx"], g["scene_sidx"],
+        g["scene_cell_start"], g["scene_cell_end"], g["lin0"], g["ang0"])
+    assert (g["color"][:, 1] == 1).sum() > 100
+    assert np.array_equal(lin, g["lin"]) and np.array_equal(ang, g["ang"])
+    assert np.array_equal(color, g["color"])
