@@ -50,7 +50,7 @@ def _body_bytes(nb: int) -> int:
 
 
 def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int) -> dict[str, float]:
-    tiles = (n + 4095) // 4096
+    tiles = (n + 8191) // 8192
     return {
         # sort histogram / look-back head
         "clear": 4 * 256 * 8 + passes * 4 * 256 * tiles,
@@ -73,7 +73,7 @@ BVH_STAGES = ["clear", "keys", "sort", "tree", "collide", "body"]
 
 def stage_bytes_bvh(n: int, nb: int, passes: int) -> dict[str, float]:
     """The same accounting for the BVH broad phase (64-bit keys, 64-byte wide nodes)."""
-    tiles = (n + 4095) // 4096
+    tiles = (n + 8191) // 8192
     return {
         "clear": 4 * n,  # refit arrival counters
         # rel in, 64-bit key out; body pose per body

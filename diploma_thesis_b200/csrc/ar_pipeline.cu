@@ -137,10 +137,9 @@ __global__ void __launch_bounds__(256) scatter_kernel(
 // The three cells of an x-row are walked as one flattened loop (candidate t of the row maps to
 // cell a, b or c and to that cell's partial sum), so a warp's lanes stay in step across cells;
 // cells that hold only this particle's body are skipped from their tag without loading their
-// occupants, which could only be rejected.  The next row's cell entries are loaded before the
-// current row is walked.  Candidates at squared distance >= the float just above (2r)^2 are
-// rejected without the square root: for them sqrtf(d2) >= 2r exactly, so the contact test is
-// unchanged.
+// occupants, which could only be rejected.  Candidates at squared distance >= the float just
+// above (2r)^2 are rejected without the square root: for them sqrtf(d2) >= 2r exactly, so the
+// contact test is unchanged.
 struct RowCells {
   uint4 a, b, c;
 };
@@ -176,10 +175,8 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
     return (c.w != epoch || c.z == (uint32_t)body) ? 0u : c.y - c.x;
   };
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
-  RowCells next = row_of(0);
   for (int r = 0; r < 9; ++r) {
-    const RowCells cur = next;
-    if (r < 8) next = row_of(r + 1);
+    const RowCells cur = row_of(r);
     const uint32_t na = visits(cur.a), nb = visits(cur.b), nc = visits(cur.c);
     const uint32_t nab = na + nb, total = nab + nc;
     float3 fa = ar::mk3(0.f, 0.f, 0.f), fb = fa, fc = fa;
@@ -453,10 +450,12 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
   pforce[__ldg(svals + k)] = make_float4(lin.x, lin.y, lin.z, 0.f);
 }
 
-// ---- K5: fixed-order body sums + integration ----------------------------------------------
+// ---- K5: fixed-order body sums, then integration ------------------------------------------
 // One warp per body: fixed-order lane sums of F and r x F over the body's particles, xor-tree
-// across lanes, integration by lane 0.  A scene whose step budget is spent (batch step
-// number > end_step) is frozen: its state is left untouched.
+// across lanes, totals stored per body.  Then one thread per body integrates (a separate
+// kernel, so that the integration runs on every lane instead of lane 0 of each warp).  A scene
+// whose step budget is spent (batch step number > end_step) is frozen: its state and sums are
+// left untouched.
 __global__ void __launch_bounds__(256) body_step_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
     const float4* __restrict__ pforce, const long long* __restrict__ d_step,
@@ -489,20 +488,32 @@ __global__ void __launch_bounds__(256) body_step_kernel(
       tz += __shfl_xor_sync(0xffffffffu, tz, o);
     }
     if (lane == 0) {
-      float ib[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) ib[k] = __ldg(S.inv_inertia + 9 * b + k);
-      float4 pos = S.pos[b], quat = q, vel = S.vel[b], ang = S.ang[b];
-      const float3 F = ar::mk3(fx, fy, fz), T = ar::mk3(tx, ty, tz);
-      if (!ar_pipe::integrate_body(S, F, T, __ldg(S.mass + b), ib, &pos, &quat, &vel, &ang))
-        ar::raise_error(err, ar::kErrNaN);
-      S.pos[b] = pos;
-      S.quat[b] = quat;
-      S.vel[b] = vel;
-      S.ang[b] = ang;
       S.bforce[b] = make_float4(fx, fy, fz, 0.f);
       S.btorque[b] = make_float4(tx, ty, tz, 0.f);
     }
+  }
+}
+
+__global__ void __launch_bounds__(256) integrate_kernel(
+    const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
+    const long long* __restrict__ d_step, int* __restrict__ err) {
+  const long long step = *d_step;
+  for (int gb = blockIdx.x * blockDim.x + threadIdx.x; gb < bt; gb += gridDim.x * blockDim.x) {
+    const SceneDev& S = table[__ldg(bscene + gb)];
+    if (step > S.end_step) continue;
+    const int b = gb - S.boff;
+    float ib[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) ib[k] = __ldg(S.inv_inertia + 9 * b + k);
+    float4 pos = S.pos[b], quat = S.quat[b], vel = S.vel[b], ang = S.ang[b];
+    const float4 F4 = S.bforce[b], T4 = S.btorque[b];
+    if (!ar_pipe::integrate_body(S, ar::xyz(F4), ar::xyz(T4), __ldg(S.mass + b), ib, &pos, &quat,
+                                 &vel, &ang))
+      ar::raise_error(err, ar::kErrNaN);
+    S.pos[b] = pos;
+    S.quat[b] = quat;
+    S.vel[b] = vel;
+    S.ang[b] = ang;
   }
 }
 
@@ -838,6 +849,8 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     mark(5);
     body_step_kernel<<<g5, 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->pforce, B->d_step,
                                          ctx->d_err);
+    integrate_kernel<<<arh::grid_for(bt, 256), 256, 0, st>>>(B->d_table, B->d_bscene, bt,
+                                                             B->d_step, ctx->d_err);
     mark(6);
     return arh::check_launch("step (BVH)");
   }
@@ -861,6 +874,8 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   mark(5);
   body_step_kernel<<<g5, 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->pforce, B->d_step,
                                        ctx->d_err);
+  integrate_kernel<<<arh::grid_for(bt, 256), 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->d_step,
+                                                           ctx->d_err);
   mark(6);
   return arh::check_launch("step");
 }
@@ -1328,10 +1343,11 @@ ar_status ar_scene_model_matrices(ar_scene* s, float* d_model16, ar_stream_t str
 
 int ar_batch_launches_per_step(ar_batch* B) {
   if (!B) return 0;
-  if (B->broadphase == AR_BROADPHASE_BVH)  // memset, keys, sort, 4 tree kernels, collide, body
-    return 1 + 1 + ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 1 + 1;
+  // memset, keys, sort, 4 tree kernels, collide, body sums, integration
+  if (B->broadphase == AR_BROADPHASE_BVH)
+    return 1 + 1 + ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 1 + 2;
   return 1 /*memset*/ + 1 /*keys*/ + ar_sort::launches(0, B->key_bits, true) + 1 /*scatter*/ +
-         1 /*collide*/ + 1 /*body*/;
+         1 /*collide*/ + 2 /*body sums, integration*/;
 }
 
 int ar_scene_launches_per_step(ar_scene* s) {

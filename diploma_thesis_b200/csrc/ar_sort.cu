@@ -21,10 +21,12 @@
 
 namespace {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kItems = 16;
-constexpr int kTile = kThreads * kItems;  // 4096
+constexpr int kThreads = 256;  // histogram kernel
+constexpr int kItems = 16;     // keys per thread in a digit pass
+// Threads per digit-pass tile: 512 (8192-key tiles: fewer tiles, shorter look-back chains) from
+// 2^19 keys on, 256 below (more tiles to spread over the SMs).
+inline int pass_threads(long n) { return n >= (1l << 19) ? 512 : 256; }
+inline long tile_items(long n) { return (long)pass_threads(n) * kItems; }
 constexpr int kRadix = 256;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
@@ -78,29 +80,31 @@ __global__ void hist_scan_kernel(uint32_t* __restrict__ hist, int passes) {
 }
 
 // ---- one digit pass ---------------------------------------------------------------------------
-template <class K>
+template <class K, int kT>
 struct PassSmem {
-  K keys[kTile];
-  uint32_t vals[kTile];
-  uint32_t warp_hist[kWarps][kRadix];
+  K keys[kT * kItems];
+  uint32_t vals[kT * kItems];
+  uint32_t warp_hist[kT / 32][kRadix];
   uint32_t digit_start[kRadix];  // tile-local exclusive start of each digit
   uint32_t gofs[kRadix];         // global destination of the digit's first tile element
   uint32_t tile_id;
 };
 
-template <class K>
-__global__ void __launch_bounds__(kThreads, sizeof(K) == 4 ? 4 : 2) onesweep_kernel(
+template <class K, int kT>
+__global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) onesweep_kernel(
     const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     const uint32_t* __restrict__ digit_base, uint32_t* __restrict__ status,
     uint32_t* __restrict__ tile_counter, int* __restrict__ err) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  PassSmem<K>& sm = *reinterpret_cast<PassSmem<K>*>(smem_raw);
+  constexpr int kWarps = kT / 32;
+  constexpr int kTile = kT * kItems;
+  PassSmem<K, kT>& sm = *reinterpret_cast<PassSmem<K, kT>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t mask = (1u << bits) - 1;
 
   if (tid == 0) sm.tile_id = atomicAdd(tile_counter, 1u);
-  for (int i = tid; i < kWarps * kRadix; i += kThreads) (&sm.warp_hist[0][0])[i] = 0;
+  for (int i = tid; i < kWarps * kRadix; i += kT) (&sm.warp_hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = sm.tile_id;
   const long tile_base = (long)tile * kTile;
@@ -141,17 +145,19 @@ __global__ void __launch_bounds__(kThreads, sizeof(K) == 4 ? 4 : 2) onesweep_ker
   __syncthreads();
 
   // per digit: exclusive over warps, tile count
-  const int d = tid;  // kThreads == kRadix
+  const int d = tid;  // threads below kRadix own one digit each
   uint32_t tile_count = 0;
+  if (d < kRadix) {
 #pragma unroll
-  for (int w = 0; w < kWarps; ++w) {
-    uint32_t c = sm.warp_hist[w][d];
-    sm.warp_hist[w][d] = tile_count;
-    tile_count += c;
+    for (int w = 0; w < kWarps; ++w) {
+      uint32_t c = sm.warp_hist[w][d];
+      sm.warp_hist[w][d] = tile_count;
+      tile_count += c;
+    }
   }
 
   // publish aggregate / look back / publish inclusive prefix
-  {
+  if (d < kRadix) {
     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(long)tile * kRadix + d]);
     uint32_t excl = 0;
     if (tile == 0) {
@@ -194,7 +200,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(K) == 4 ? 4 : 2) onesweep_ker
     __syncthreads();
     uint32_t add = 0;
     for (int w = 0; w < warp; ++w) add += s_wsum[w];
-    sm.digit_start[d] = add + x - tile_count;
+    if (d < kRadix) sm.digit_start[d] = add + x - tile_count;
   }
   __syncthreads();
 
@@ -214,7 +220,7 @@ __global__ void __launch_bounds__(kThreads, sizeof(K) == 4 ? 4 : 2) onesweep_ker
   // coalesced write-out
   long valid = n - tile_base;
   int count = valid < kTile ? (int)valid : kTile;
-  for (int i = tid; i < count; i += kThreads) {
+  for (int i = tid; i < count; i += kT) {
     K k = sm.keys[i];
     uint32_t dd = digit_of(k, shift, mask);
     uint32_t dst = sm.gofs[dd] + (uint32_t)i - sm.digit_start[dd];
@@ -237,7 +243,8 @@ ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* k
   const int total_bits = end_bit - begin_bit;
   const int passes = (total_bits + 7) / 8;
   const int last_bits = total_bits - 8 * (passes - 1);
-  const long tiles = ((long)n + kTile - 1) / kTile;
+  const int kt = pass_threads(n);
+  const long tiles = ((long)n + tile_items(n) - 1) / tile_items(n);
   ar_sort::Layout L = ar_sort::layout(n, sizeof(K), passes);
   if (ws_bytes < L.total) {
     arh::set_error("radix sort: workspace too small");
@@ -261,7 +268,7 @@ ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* k
   }
   hist_scan_kernel<<<1, 32 * ar_sort::kMaxPasses, 0, st>>>(hist, passes);
 
-  const size_t smem = sizeof(PassSmem<K>);
+
   // ping-pong so that the last pass lands in keys_out
   const K* src_k = keys_in;
   const uint32_t* src_v = vals_in;
@@ -270,9 +277,14 @@ ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* k
     K* dk = to_out ? keys_out : tmp_keys;
     uint32_t* dv = to_out ? vals_out : tmp_vals;
     int bits = (p == passes - 1) ? last_bits : 8;
-    onesweep_kernel<K><<<(unsigned)tiles, kThreads, smem, st>>>(
-        src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
-        status + (size_t)p * tiles * kRadix, counters + p, err);
+    if (kt == 512)
+      onesweep_kernel<K, 512><<<(unsigned)tiles, 512, sizeof(PassSmem<K, 512>), st>>>(
+          src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
+          status + (size_t)p * tiles * kRadix, counters + p, err);
+    else
+      onesweep_kernel<K, 256><<<(unsigned)tiles, 256, sizeof(PassSmem<K, 256>), st>>>(
+          src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
+          status + (size_t)p * tiles * kRadix, counters + p, err);
     src_k = dk;
     src_v = dv;
   }
@@ -325,7 +337,7 @@ constexpr size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t noalloc_bytes() {
   return up256(up256(up256(up256(up256((size_t)ar_sort::kMaxPasses * kRadix * 4) +
                                        ar_sort::kMaxPasses * 4) +
-                                 (size_t)4 * (kNoAllocMaxN / kTile) * kRadix * 4) +
+                                 (size_t)4 * (kNoAllocMaxN / (256 * kItems)) * kRadix * 4) +
                            (size_t)kNoAllocMaxN * 4) +
                (size_t)kNoAllocMaxN * 4);
 }
@@ -350,9 +362,13 @@ ar_status noalloc_setup(int dev, void** addr, int* sms) {
                      cudaGetErrorString(e));
       return AR_ERR_CUDA;
     }
-    e = cudaFuncSetAttribute(onesweep_kernel<uint32_t>,
+    e = cudaFuncSetAttribute(onesweep_kernel<uint32_t, 256>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(PassSmem<uint32_t>));
+                             (int)sizeof(PassSmem<uint32_t, 256>));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(onesweep_kernel<uint32_t, 512>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)sizeof(PassSmem<uint32_t, 512>));
     if (e != cudaSuccess) {
       arh::set_error("allocation-free sort: %s", cudaGetErrorString(e));
       return AR_ERR_CUDA;
@@ -372,14 +388,22 @@ ar_status noalloc_setup(int dev, void** addr, int* sms) {
 namespace ar_sort {
 
 void init() {
-  cudaFuncSetAttribute(onesweep_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(PassSmem<uint32_t>));
-  cudaFuncSetAttribute(onesweep_kernel<uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(PassSmem<uint64_t>));
+  cudaFuncSetAttribute(onesweep_kernel<uint32_t, 256>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PassSmem<uint32_t, 256>));
+  cudaFuncSetAttribute(onesweep_kernel<uint32_t, 512>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PassSmem<uint32_t, 512>));
+  cudaFuncSetAttribute(onesweep_kernel<uint64_t, 256>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PassSmem<uint64_t, 256>));
+  cudaFuncSetAttribute(onesweep_kernel<uint64_t, 512>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)sizeof(PassSmem<uint64_t, 512>));
 }
 
 Layout layout(long n, size_t key_bytes, int passes) {
-  const long tiles = (n + kTile - 1) / kTile;
+  const long tiles = (n + tile_items(n) - 1) / tile_items(n);
   auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
   Layout L;
   L.hist = 0;
@@ -412,7 +436,7 @@ ar_status sort_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in
 }
 
 size_t clear_bytes(long n, int passes) {
-  const long tiles = (n + kTile - 1) / kTile;
+  const long tiles = (n + tile_items(n) - 1) / tile_items(n);
   Layout L = layout(n, 4, passes);
   return L.status + (size_t)passes * tiles * kRadix * sizeof(uint32_t);
 }
@@ -479,7 +503,8 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
   const int total_bits = end_bit - begin_bit;
   const int passes = (total_bits + 7) / 8;
   const int last_bits = total_bits - 8 * (passes - 1);
-  const long tiles = ((long)n + kTile - 1) / kTile;
+  const int kt = pass_threads(n);
+  const long tiles = ((long)n + tile_items(n) - 1) / tile_items(n);
   const ar_sort::Layout L = ar_sort::layout(n, 4, passes);
   if (L.total > sizeof(g_noalloc_scratch)) {  // cannot happen for n <= kNoAllocMaxN
     arh::set_error("allocation-free sort: workspace layout exceeds the static array");
@@ -505,9 +530,18 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
     uint32_t* dk = to_out ? keys_out : tmp_keys;
     uint32_t* dv = to_out ? vals_out : tmp_vals;
     const int bits = (p == passes - 1) ? last_bits : 8;
-    onesweep_kernel<uint32_t><<<(unsigned)tiles, kThreads, sizeof(PassSmem<uint32_t>), st>>>(
-        src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
-        status + (size_t)p * tiles * kRadix, counters + p, (int*)d_status);
+    if (kt == 512)
+      onesweep_kernel<uint32_t, 512><<<(unsigned)tiles, 512, sizeof(PassSmem<uint32_t, 512>),
+                                       st>>>(src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits,
+                                             hist + p * kRadix,
+                                             status + (size_t)p * tiles * kRadix, counters + p,
+                                             (int*)d_status);
+    else
+      onesweep_kernel<uint32_t, 256><<<(unsigned)tiles, 256, sizeof(PassSmem<uint32_t, 256>),
+                                       st>>>(src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits,
+                                             hist + p * kRadix,
+                                             status + (size_t)p * tiles * kRadix, counters + p,
+                                             (int*)d_status);
     src_k = dk;
     src_v = dv;
   }
