@@ -656,8 +656,8 @@ def run_lbvh(args):
                 def refit():
                     call("ar_lbvh_leaves", ctx.handle, n, P(svals), P(pts), 1e-3, P(leaf),
                          P(t["min_r"]), P(t["max_r"]), P(cms), P(bounds), P(radii), st)
-                    call("ar_lbvh_refit_ranged", ctx.handle, n, P(t["left"]), P(t["right"]),
-                         P(t["parent"]), P(t["min_r"]), P(t["max_r"]), P(bounds), st)
+                    call("ar_lbvh_refit", ctx.handle, n, P(t["left"]), P(t["right"]),
+                         P(t["parent"]), P(bounds), st)
 
                 stages = {"encode": encode, "sort": sort, "build": build, "refit": refit}
                 times = {k: [] for k in stages}

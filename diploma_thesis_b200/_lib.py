@@ -101,7 +101,6 @@ SIGNATURES = {
     "ar_lbvh_build64": [P, P, I, P, P, P, P, P, P, S],
     "ar_lbvh_leaves": [P, I, P, P, F, P, P, P, P, P, P, S],
     "ar_lbvh_refit": [P, I, P, P, P, P, S],
-    "ar_lbvh_refit_ranged": [P, I, P, P, P, P, P, P, S],
     "ar_collide_bvh_dem": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, P, P, I, P, P, P, S],
     "ar_find_contacts_bvh": [P, P, P, P, P, P, P, P, P, P, P, I, P, P, P, S],
     "ar_pairs_bvh": [P, F, P, P, P, P, P, P, P, P, I, P, I, P, S],

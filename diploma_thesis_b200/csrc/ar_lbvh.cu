@@ -55,30 +55,24 @@ __global__ void __launch_bounds__(256) leaves_kernel(int n, const int32_t* __res
 }
 
 // ---- refit (kernelConstructInternalNodesSoA, BVHSoAKernels.cu:148-176) ----------------------
-// One thread per leaf, kRefitBlock leaves per block; with the build's leaf ranges the nodes
-// inside a block are merged through shared memory (ar_lbvh::refit_climb).
-__global__ void __launch_bounds__(ar_lbvh::kRefitBlock) refit_kernel(
-    int n, const int32_t* __restrict__ left, const int32_t* __restrict__ right,
-    const int32_t* __restrict__ parent, const int32_t* __restrict__ min_r,
-    const int32_t* __restrict__ max_r, float4* bounds, int* __restrict__ counters) {
-  __shared__ ar_lbvh::RefitShared sh;
-  ar_lbvh::refit_shared_init(sh);
-  __syncthreads();
-  const int blo = blockIdx.x * ar_lbvh::kRefitBlock;
-  const int i = blo + threadIdx.x;
+__global__ void __launch_bounds__(256) refit_kernel(int n, const int32_t* __restrict__ left,
+                                                    const int32_t* __restrict__ right,
+                                                    const int32_t* __restrict__ parent,
+                                                    float4* bounds, int* __restrict__ counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float4 p0 = __ldcg(bounds + 2 * i), p1 = __ldcg(bounds + 2 * i + 1);
-  auto store = [&](int node, const ar_lbvh::Box6& b) {
-    __stcg(bounds + 2 * node, make_float4(b.lx, b.ly, b.lz, b.hx));
-    __stcg(bounds + 2 * node + 1, make_float4(b.hy, b.hz, 0.f, 0.f));
+  auto children = [&](int node, ar_lbvh::Box6* a, ar_lbvh::Box6* b) {
+    const int l = __ldg(left + node), r = __ldg(right + node);
+    const float4 a0 = __ldcg(bounds + 2 * l), a1 = __ldcg(bounds + 2 * l + 1);
+    const float4 b0 = __ldcg(bounds + 2 * r), b1 = __ldcg(bounds + 2 * r + 1);
+    *a = ar_lbvh::Box6{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y};
+    *b = ar_lbvh::Box6{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y};
   };
-  auto sibling = [&](int node, int side) {
-    const int c = side == 0 ? __ldg(right + node) : __ldg(left + node);
-    const float4 a = __ldcg(bounds + 2 * c), b = __ldcg(bounds + 2 * c + 1);
-    return ar_lbvh::Box6{a.x, a.y, a.z, a.w, b.x, b.y};
+  auto store = [&](int node, const ar_lbvh::Box6& m) {
+    __stcg(bounds + 2 * node, make_float4(m.lx, m.ly, m.lz, m.hx));
+    __stcg(bounds + 2 * node + 1, make_float4(m.hy, m.hz, 0.f, 0.f));
   };
-  ar_lbvh::refit_climb(i, ar_lbvh::Box6{p0.x, p0.y, p0.z, p0.w, p1.x, p1.y}, n, left, parent,
-                       min_r, max_r, blo, sh, counters, store, sibling);
+  ar_lbvh::refit_climb(i, n, parent, counters, children, store);
 }
 
 // Parent links from the child links, for callers with the reference's traversal signature
@@ -270,25 +264,18 @@ ar_status ar_lbvh_leaves(ar_ctx* ctx, int n, const int32_t* sorted_idx, const fl
   return arh::check_launch("ar_lbvh_leaves");
 }
 
-ar_status ar_lbvh_refit_ranged(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
-                               const int32_t* parent, const int32_t* min_r,
-                               const int32_t* max_r, float* bounds8, ar_stream_t stream) {
-  if (!ctx || n < 0 || (n > 0 && (!left || !right || !parent || !bounds8)) ||
-      ((min_r == nullptr) != (max_r == nullptr)))
+ar_status ar_lbvh_refit(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
+                        const int32_t* parent, float* bounds8, ar_stream_t stream) {
+  if (!ctx || n < 0 || (n > 0 && (!left || !right || !parent || !bounds8)))
     return AR_ERR_INVALID_ARG;
   if (n < 2) return AR_OK;
   int* counters = (int*)arh::scratch(ctx, (size_t)(n - 1) * sizeof(int));
   if (!counters) return AR_ERR_OOM;
   cudaStream_t st = arh::stream(stream);
   cudaMemsetAsync(counters, 0, (size_t)(n - 1) * sizeof(int), st);
-  refit_kernel<<<arh::grid_for(n, ar_lbvh::kRefitBlock), ar_lbvh::kRefitBlock, 0, st>>>(
-      n, left, right, parent, min_r, max_r, (float4*)bounds8, counters);
+  refit_kernel<<<arh::grid_for(n, 256), 256, 0, st>>>(n, left, right, parent, (float4*)bounds8,
+                                                      counters);
   return arh::check_launch("ar_lbvh_refit");
-}
-
-ar_status ar_lbvh_refit(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
-                        const int32_t* parent, float* bounds8, ar_stream_t stream) {
-  return ar_lbvh_refit_ranged(ctx, n, left, right, parent, nullptr, nullptr, bounds8, stream);
 }
 
 ar_status ar_collide_bvh_dem(ar_ctx* ctx, const ar_sim_params* params, const int32_t* rb_idx,

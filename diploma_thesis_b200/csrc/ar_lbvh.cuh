@@ -92,15 +92,11 @@ __device__ __forceinline__ int2 karras_node(int i, int n, const Lcp& lcp, uint8_
 // ---- bottom-up refit (kernelConstructInternalNodesSoA, BVHSoAKernels.cu:148-176) ------------
 // One thread per leaf climbs; the second thread to reach a node merges its children's boxes
 // (mergeBounds, BVHAuxiliary.cuh:83-94: min of the mins and max of the maxes, left child
-// first) and continues.  Blocks own kRefitBlock consecutive leaves.  A node whose leaf range
-// lies inside its block's leaves is only ever reached by threads of that block, and a Karras
-// internal node i has i inside its own range, so its arrival counter and child boxes live in
-// shared memory at index i - (first leaf of the block): synchronised by shared-memory atomics
-// and block fences.  The other nodes use a device-scope acquire-release counter in global
-// memory and read the sibling's box through L2.  Without leaf ranges every node is treated
-// as the latter.
-constexpr int kRefitBlock = 512;
-
+// first) and continues.  The arrival counter is a device-scope acquire-release increment, so
+// the first thread's box stores (made before its increment) are visible to the second
+// thread's loads (made after it); boxes are read and written through L2.  (Merging the nodes
+// inside a block through shared memory instead was measured slower: more dependent loads per
+// level outweighed the fences it saved.)
 struct Box6 {
   float lx, ly, lz, hx, hy, hz;
 };
@@ -109,57 +105,27 @@ __device__ __forceinline__ Box6 merge_boxes(const Box6& a, const Box6& b) {  // 
               a.hx > b.hx ? a.hx : b.hx, a.hy > b.hy ? a.hy : b.hy, a.hz > b.hz ? a.hz : b.hz};
 }
 
-// Device-scope arrival: the first thread's box stores (made before its increment) are visible
-// to the second thread's loads (made after its increment).  Returns the previous count.
+// Returns the previous count.
 __device__ __forceinline__ int arrive(int* counter) {
   cuda::atomic_ref<int, cuda::thread_scope_device> a(*counter);
   return a.fetch_add(1, cuda::memory_order_acq_rel);
 }
 
-struct RefitShared {
-  int cnt[kRefitBlock];
-  Box6 box[kRefitBlock][2];
-};
-
-// Zero the block's shared counters (call before refit_climb, followed by __syncthreads).
-__device__ __forceinline__ void refit_shared_init(RefitShared& sh) {
-  for (int i = threadIdx.x; i < kRefitBlock; i += blockDim.x) sh.cnt[i] = 0;
-}
-
-// Climb from `leaf` with its box.  `store(node, box)` publishes a node's merged box to global
-// memory (before any device-scope arrival that follows); `sibling(node, side)` reads the box of
-// the other child of `node` from global memory.  Returns when this thread arrived first.
-template <class Store, class Sibling>
-__device__ __forceinline__ void refit_climb(int leaf, Box6 box, int n,
-                                            const int32_t* __restrict__ left,
-                                            const int32_t* __restrict__ parent,
-                                            const int32_t* __restrict__ min_r,
-                                            const int32_t* __restrict__ max_r, int blo,
-                                            RefitShared& sh, int* __restrict__ counters,
-                                            Store store, Sibling sibling) {
-  const int bhi = blo + kRefitBlock - 1;
-  int child = leaf;
+// Climb from `leaf`.  `children(node, &left_box, &right_box)` reads both child boxes of
+// `node` through L2; `store(node, box)` publishes a node's merged box (before the next
+// arrival).  Returns when this thread arrived first or at the root.
+template <class Children, class Store>
+__device__ __forceinline__ void refit_climb(int leaf, int n, const int32_t* __restrict__ parent,
+                                            int* __restrict__ counters, Children children,
+                                            Store store) {
   int node = __ldg(parent + leaf);
   for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
     if (node < n || node >= 2 * n - 1) return;  // malformed parent link
-    const int side = __ldg(left + node) == child ? 0 : 1;
-    const bool local = min_r && __ldg(min_r + node) >= blo && __ldg(max_r + node) <= bhi;
-    Box6 other;
-    if (local) {
-      const int li = node - n - blo;
-      sh.box[li][side] = box;
-      __threadfence_block();
-      if (atomicAdd(&sh.cnt[li], 1) == 0) return;
-      __threadfence_block();
-      other = sh.box[li][1 - side];
-    } else {
-      if (arrive(counters + (node - n)) == 0) return;
-      other = sibling(node, side);
-    }
-    box = side == 0 ? merge_boxes(box, other) : merge_boxes(other, box);
-    store(node, box);
+    if (arrive(counters + (node - n)) == 0) return;
+    Box6 a, b;
+    children(node, &a, &b);
+    store(node, merge_boxes(a, b));
     if (node == n) return;
-    child = node;
     node = __ldg(parent + node);
   }
 }

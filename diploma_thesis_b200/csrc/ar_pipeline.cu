@@ -352,33 +352,28 @@ __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
 // thread per leaf climbs; the second thread to reach a node merges the two child boxes held in
 // the node (mergeBounds, BVHAuxiliary.cuh:83-94) and stores the result into the node's slot in
 // its parent.  Release / acquire through the arrival counter; boxes through L2.
-// One thread per leaf (ar_lbvh::refit_climb): the leaf's box is in its parent's slot (written
-// by the leaves kernel); each merged box goes into the node's slot in its parent.
-__global__ void __launch_bounds__(ar_lbvh::kRefitBlock) bvh_refit_kernel(
-    int n, const int32_t* __restrict__ left, const int32_t* __restrict__ parent,
-    const int32_t* __restrict__ min_r, const int32_t* __restrict__ max_r, WideNode* nodes,
-    int* __restrict__ counters) {
-  __shared__ ar_lbvh::RefitShared sh;
-  ar_lbvh::refit_shared_init(sh);
-  __syncthreads();
-  const int blo = blockIdx.x * ar_lbvh::kRefitBlock;
-  const int i = blo + threadIdx.x;
+// One thread per leaf (ar_lbvh::refit_climb): a node's two child boxes are in its own wide node
+// (leaf boxes written by the leaves kernel); each merged box goes into the node's slot in its
+// parent.
+__global__ void __launch_bounds__(256) bvh_refit_kernel(int n, const int32_t* __restrict__ left,
+                                                        const int32_t* __restrict__ parent,
+                                                        WideNode* nodes,
+                                                        int* __restrict__ counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || n < 2) return;
-  auto slot = [&](int node, int side) {  // box of child `side` of internal node `node`
-    const float4* c = nodes[node - n].c + 2 * side;
-    const float4 a = __ldcg(c), b = __ldcg(c + 1);
-    return ar_lbvh::Box6{a.x, a.y, a.z, a.w, b.x, b.y};
+  auto children = [&](int node, ar_lbvh::Box6* a, ar_lbvh::Box6* b) {
+    const float4* c = nodes[node - n].c;
+    const float4 a0 = __ldcg(c), a1 = __ldcg(c + 1), b0 = __ldcg(c + 2), b1 = __ldcg(c + 3);
+    *a = ar_lbvh::Box6{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y};
+    *b = ar_lbvh::Box6{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y};
   };
-  auto store = [&](int node, const ar_lbvh::Box6& b) {
+  auto store = [&](int node, const ar_lbvh::Box6& m) {
     if (node == n) return;  // the root's box is not stored anywhere
     const int pn = __ldg(parent + node);
     put_child_box(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1,
-                  make_float4(b.lx, b.ly, b.lz, b.hx), make_float2(b.hy, b.hz));
+                  make_float4(m.lx, m.ly, m.lz, m.hx), make_float2(m.hy, m.hz));
   };
-  auto sibling = [&](int node, int side) { return slot(node, 1 - side); };
-  const int p0 = __ldg(parent + i);
-  ar_lbvh::refit_climb(i, slot(p0, __ldg(left + p0) == i ? 0 : 1), n, left, parent, min_r,
-                       max_r, blo, sh, counters, store, sibling);
+  ar_lbvh::refit_climb(i, n, parent, counters, children, store);
 }
 
 // DEM gather through the scene's subtree in the reference's visit order
@@ -840,8 +835,8 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
                                           B->min_r, B->max_r);
     bvh_roots_kernel<<<arh::grid_for(ns, 128), 128, 0, st>>>(B->d_poff, ns, nt, B->parent,
                                                               B->min_r, B->max_r, B->roots);
-    bvh_refit_kernel<<<arh::grid_for(nt, ar_lbvh::kRefitBlock), ar_lbvh::kRefitBlock, 0, st>>>(
-        nt, B->left, B->parent, B->min_r, B->max_r, B->nodes, B->counters);
+    bvh_refit_kernel<<<arh::grid_for(nt, 256), 256, 0, st>>>(nt, B->left, B->parent, B->nodes,
+                                                              B->counters);
     mark(4);
     bvh_collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(
         B->d_table, B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots,

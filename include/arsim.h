@@ -178,14 +178,7 @@ AR_API ar_status ar_lbvh_leaves(ar_ctx* ctx, int n, const int32_t* sorted_idx,
  * children's final boxes. */
 AR_API ar_status ar_lbvh_refit(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
                                const int32_t* parent, float* bounds8, ar_stream_t stream);
-/* The same, given the build's leaf ranges (min_r / max_r of ar_lbvh_build and
- * ar_lbvh_leaves): a node whose leaves are all climbed by threads of one block is
- * synchronised at block scope instead of device scope, which removes most device-wide fences.
- * New (the reference's wrapperConstructInternalNodesSoA has no ranges); same result. */
-AR_API ar_status ar_lbvh_refit_ranged(ar_ctx* ctx, int n, const int32_t* left,
-                                      const int32_t* right, const int32_t* parent,
-                                      const int32_t* min_r, const int32_t* max_r,
-                                      float* bounds8, ar_stream_t stream);
+
 
 /* ---- (a12) BVH traversal ---------------------------------------------------------------------
  * collideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:100-244) with collideStaticSpheresBVH

@@ -37,8 +37,8 @@ def _pipeline(ctx, pts: np.ndarray, wide: bool):
     cms, bounds, radii = empty((n, 4)), empty((m, 8)), empty(n)
     call("ar_lbvh_leaves", ctx.handle, n, P(svals), P(d), 1e-3, P(t["is_leaf"]), P(t["min_r"]),
          P(t["max_r"]), P(cms), P(bounds), P(radii), S())
-    call("ar_lbvh_refit_ranged", ctx.handle, n, P(t["left"]), P(t["right"]), P(t["parent"]),
-         P(t["min_r"]), P(t["max_r"]), P(bounds), S())
+    call("ar_lbvh_refit", ctx.handle, n, P(t["left"]), P(t["right"]), P(t["parent"]),
+         P(bounds), S())
     ctx.check()
     return d, mn, mx, codes, skeys, svals, t, bounds
 

@@ -144,14 +144,9 @@ def test_lbvh_topology_leaves_refit_golden(ctx, case):
          P(t["is_leaf"]), P(t["min_r"]), P(t["max_r"]), P(cms), P(bounds), P(radii), S())
     assert np.array_equal(host(cms), g["cms"])
     assert np.array_equal(host(bounds)[:n, :6], g["leaf_bounds"][:n, :6])
-    leaf_boxes = bounds.clone()
     call("ar_lbvh_refit", ctx.handle, n, P(t["left"]), P(t["right"]), P(t["parent"]),
          P(bounds), S())
     assert np.array_equal(host(bounds)[:, :6], g["bounds"][:, :6])
-    # the ranged refit (block-scope synchronisation inside blocks) gives the same boxes
-    call("ar_lbvh_refit_ranged", ctx.handle, n, P(t["left"]), P(t["right"]), P(t["parent"]),
-         P(t["min_r"]), P(t["max_r"]), P(leaf_boxes), S())
-    assert np.array_equal(host(leaf_boxes), host(bounds))
     assert np.array_equal(host(t["is_leaf"]), np.r_[np.ones(n), np.zeros(n - 1)].astype(np.uint8))
 
 
