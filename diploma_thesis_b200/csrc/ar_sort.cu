@@ -7,8 +7,10 @@
 //     already running or finished (look-back always makes progress);
 //   * warps rank their items stably with a ballot multi-split (items are visited in input
 //     order: warp w owns a contiguous sub-range, item j of lane l is element j*32 + l);
-//   * per digit, the tile count is published, earlier tiles are looked back through until an
-//     inclusive prefix is found, and the tile's own inclusive prefix is published;
+//   * per digit, the tile count is published, earlier tiles are looked back through (eight
+//     status words per round trip) until an inclusive prefix is found, and the tile's own
+//     inclusive prefix is published; the keys are staged and the value loads issued before
+//     the look-back, so its latency overlaps them;
 //   * items are staged in shared memory in (digit, rank) order and written out with
 //     consecutive threads, so each digit run is a coalesced write.
 // Spin waits are bounded; on timeout the kernel raises kErrTimeout and finishes the pass
@@ -32,6 +34,7 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1;
 constexpr long kSpinLimit = 1l << 24;
+constexpr int kLookWindow = 8;  // look-back status words read per round trip
 
 template <class K>
 __device__ __forceinline__ uint32_t digit_of(K key, int shift, uint32_t mask) {
@@ -110,7 +113,7 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
   const long tile_base = (long)tile * kTile;
 
   // load keys (coalesced: item j of lane l in warp w is element base + w*kItems*32 + j*32 + l);
-  // values are read only when the items are staged, and digits are recomputed from the keys,
+  // values are read only after the keys are staged, and digits are recomputed from the keys,
   // which keeps the register count (and so the occupancy) down
   K key[kItems];
   uint32_t rank[kItems];
@@ -144,7 +147,7 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
   }
   __syncthreads();
 
-  // per digit: exclusive over warps, tile count
+  // per digit: exclusive over warps, tile count; the tile's aggregate is published at once
   const int d = tid;  // threads below kRadix own one digit each
   uint32_t tile_count = 0;
   if (d < kRadix) {
@@ -154,37 +157,8 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
       sm.warp_hist[w][d] = tile_count;
       tile_count += c;
     }
-  }
-
-  // publish aggregate / look back / publish inclusive prefix
-  if (d < kRadix) {
     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(long)tile * kRadix + d]);
-    uint32_t excl = 0;
-    if (tile == 0) {
-      mine.store(kFlagPrefix | tile_count, cuda::memory_order_relaxed);
-    } else {
-      mine.store(kFlagAgg | tile_count, cuda::memory_order_relaxed);
-      long k = (long)tile - 1;
-      long spins = 0;
-      while (k >= 0) {
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> other(status[k * kRadix + d]);
-        uint32_t v = other.load(cuda::memory_order_relaxed);
-        uint32_t flag = v & ~kValueMask;
-        if (flag == 0) {
-          if (++spins > kSpinLimit) {
-            ar::raise_error(err, ar::kErrTimeout);
-            break;
-          }
-          if (spins > 64) __nanosleep(64);
-          continue;
-        }
-        excl += v & kValueMask;
-        if (flag == kFlagPrefix) break;
-        --k;
-      }
-      mine.store(kFlagPrefix | ((excl + tile_count) & kValueMask), cuda::memory_order_relaxed);
-    }
-    sm.gofs[d] = digit_base[d] + excl;
+    mine.store((tile == 0 ? kFlagPrefix : kFlagAgg) | tile_count, cuda::memory_order_relaxed);
   }
 
   // tile-local exclusive scan over digits (block scan of one value per thread)
@@ -204,16 +178,74 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
   }
   __syncthreads();
 
-  // stage in (digit, rank) order
+  // stage the keys in (digit, rank) order (rank[] becomes the staging slot), then start the
+  // value loads so that they are in flight during the look-back
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
-    long g = wbase + j * 32 + lane;
+    const long g = wbase + j * 32 + lane;
     if (g < n) {
       const uint32_t dj = digit_of(key[j], shift, mask);
-      uint32_t pos = sm.digit_start[dj] + sm.warp_hist[warp][dj] + rank[j];
-      sm.keys[pos] = key[j];
-      sm.vals[pos] = vals_in ? vals_in[g] : (uint32_t)g;
+      rank[j] += sm.digit_start[dj] + sm.warp_hist[warp][dj];
+      sm.keys[rank[j]] = key[j];
     }
+  }
+  uint32_t val[kItems];
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    const long g = wbase + j * 32 + lane;
+    val[j] = g < n ? (vals_in ? __ldg(vals_in + g) : (uint32_t)g) : 0u;
+  }
+
+  // look back through the earlier tiles, kLookWindow status words per round trip, until an
+  // inclusive prefix is found; then publish this tile's inclusive prefix
+  if (d < kRadix) {
+    uint32_t excl = 0;
+    if (tile != 0) {
+      long k = (long)tile - 1;  // next tile to read
+      long spins = 0;
+      bool found = false;
+      while (!found) {
+        uint32_t v[kLookWindow];
+#pragma unroll
+        for (int w = 0; w < kLookWindow; ++w) {
+          v[w] = kFlagPrefix;  // before tile 0: never reached (tile 0 is inclusive)
+          if (k - w >= 0) {
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> other(
+                status[(k - w) * kRadix + d]);
+            v[w] = other.load(cuda::memory_order_relaxed);
+          }
+        }
+        int used = 0;
+#pragma unroll
+        for (int w = 0; w < kLookWindow; ++w) {
+          const uint32_t flag = v[w] & ~kValueMask;
+          if (flag == 0) break;  // not published yet: read again from this tile
+          excl += v[w] & kValueMask;
+          ++used;
+          if (flag == kFlagPrefix) {
+            found = true;
+            break;
+          }
+        }
+        k -= used;
+        if (!found && used == 0) {
+          if (++spins > kSpinLimit) {
+            ar::raise_error(err, ar::kErrTimeout);
+            break;
+          }
+          if (spins > 64) __nanosleep(64);
+        }
+      }
+      cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(long)tile * kRadix + d]);
+      mine.store(kFlagPrefix | ((excl + tile_count) & kValueMask), cuda::memory_order_relaxed);
+    }
+    sm.gofs[d] = digit_base[d] + excl;
+  }
+
+#pragma unroll
+  for (int j = 0; j < kItems; ++j) {
+    const long g = wbase + j * 32 + lane;
+    if (g < n) sm.vals[rank[j]] = val[j];
   }
   __syncthreads();
 
