@@ -1,13 +1,14 @@
 // Fused PHYSICAL-mode step over a table of resident scenes.
 //
 // Per step (one launch per stage, whatever the number of scenes):
-//   memset   clear the sort's histogram / look-back head
+//   K0       clear the sort's histogram / look-back head and one 255th of the cell table
+//            (see cell_epoch)
 //   K1       re-pose + hash: key = scene cell base + wrapped cell of the particle's world
-//            position; the sort histogram is accumulated on the fly; cells touched by the
-//            previous step are reset to empty (no full-table clear)
+//            position; the sort histogram is accumulated on the fly
 //   sort     onesweep passes over the global keys (values = global particle index)
-//   K3       scatter + cell ranges: sorted position (w = global body id) and velocity,
-//            recomputed from the body state; start/end of every occupied cell
+//   K3       scatter + cell table: sorted position (w = global body id) and velocity,
+//            recomputed from the body state; first slot, count, step epoch and body tag of
+//            every occupied cell
 //   K4       DEM gather over the 27 neighbour cells + box walls -> per-particle force at the
 //            particle's original index (no atomics)
 //   K5       one warp per body: fixed-order sum of F and r x F, then integration
@@ -47,11 +48,26 @@ __device__ __forceinline__ int find_range(const int* __restrict__ off, int count
   return lo;
 }
 
-// Cell entries carry the number of the step that wrote them; an entry of another step is
-// empty.  Epochs live in [0, 2^31), so the all-ones fill of a fresh table never matches, and
-// the table is refilled whenever the step number enters a new 2^31 window (batch_step).
+// Cell entry (8 bytes): {first sorted slot, meta}, meta = occupant count (bits 0-4; 31 means
+// "31 or more", the end is then found from the sorted keys) | epoch (bits 5-12) | body tag
+// (bits 13-31: scene-local body + 1 when every occupant belongs to that body, else 0).
+// The epoch is the step number mod 255, plus 1; an entry whose epoch is not the current
+// step's reads as empty, so the table is never cleared as a whole.  Instead the first kernel
+// of each step zeroes one of 255 slices of the table (slice = step number mod 255), so every
+// entry is zeroed within 255 steps of being written, before its epoch can recur; a zero entry
+// has epoch 0, which never matches.
+constexpr uint32_t kCountMask = 31;
+constexpr uint32_t kEpochShift = 5;
+constexpr uint32_t kEpochMask = 255;
+constexpr uint32_t kTagShift = 13;
+constexpr uint32_t kMaxTag = (1u << 19) - 1;  // bodies of a scene with local index + 1 above
+                                              // this carry no tag (never skipped)
+constexpr int kEpochSlices = 255;
 __device__ __forceinline__ uint32_t cell_epoch(long long step) {
-  return (uint32_t)(step & 0x7fffffffLL);
+  return (uint32_t)(step % kEpochSlices) + 1u;
+}
+__device__ __forceinline__ uint32_t body_tag(int local_body) {
+  return (uint32_t)local_body + 1u <= kMaxTag ? (uint32_t)local_body + 1u : 0u;
 }
 
 // Scene index of every particle and body of the batch (run when the member list changes).
@@ -66,7 +82,27 @@ __global__ void __launch_bounds__(256) scene_ids_kernel(const int* __restrict__ 
   }
 }
 
+// ---- K0: clears ------------------------------------------------------------------------------
+// Zeroes the sort's histogram / look-back head and the cell-table slice of the step about to
+// run (its number is *d_step + 1; K1 increments the counter).
+__global__ void __launch_bounds__(256) step_clear_kernel(uint4* __restrict__ head, long head16,
+                                                         uint2* __restrict__ cells,
+                                                         unsigned long long num_cells,
+                                                         const long long* __restrict__ d_step) {
+  const long stride = (long)gridDim.x * blockDim.x;
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (long i = t; i < head16; i += stride) head[i] = make_uint4(0u, 0u, 0u, 0u);
+  const unsigned long long len = (num_cells + kEpochSlices - 1) / kEpochSlices;
+  const unsigned long long lo = (unsigned long long)((*d_step + 1) % kEpochSlices) * len;
+  const unsigned long long hi = lo + len < num_cells ? lo + len : num_cells;
+  for (unsigned long long i = lo + t; i < hi; i += stride) cells[i] = make_uint2(0u, 0u);
+}
+
 // ---- K1: re-pose + cell keys + sort histogram ---------------------------------------------
+// Each thread takes kKeysBatch particles per round (stride apart, so each load is coalesced)
+// and issues the loads of all of them before using any, which keeps several dependent
+// gathers (scene -> offset -> body) in flight per thread.
+constexpr int kKeysBatch = 2;
 __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
     uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits,
@@ -75,16 +111,45 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
   if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
   for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
   __syncthreads();
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
-    const SceneDev& S = table[__ldg(pscene + g)];
-    const int i = g - S.poff;
-    const float4 r4 = __ldg(S.rel + i);
-    const int b = __float_as_int(r4.w);
-    const float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
-    const float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
-    const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
-    keys[g] = key;
-    ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
+  const int stride = gridDim.x * blockDim.x;
+  for (int g0 = blockIdx.x * blockDim.x + threadIdx.x; g0 < nt; g0 += stride * kKeysBatch) {
+    int sc[kKeysBatch];
+    float4 r4[kKeysBatch], q[kKeysBatch], c[kKeysBatch];
+#pragma unroll
+    for (int u = 0; u < kKeysBatch; ++u) {
+      const int g = g0 + u * stride;
+      sc[u] = g < nt ? __ldg(pscene + g) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kKeysBatch; ++u) {
+      const int g = g0 + u * stride;
+      if (g < nt) {
+        const SceneDev& S = table[sc[u]];
+        r4[u] = __ldg(S.rel + (g - S.poff));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kKeysBatch; ++u) {
+      const int g = g0 + u * stride;
+      if (g < nt) {
+        const SceneDev& S = table[sc[u]];
+        const int b = __float_as_int(r4[u].w);
+        q[u] = __ldg(S.quat + b);
+        c[u] = __ldg(S.pos + b);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kKeysBatch; ++u) {
+      const int g = g0 + u * stride;
+      if (g < nt) {
+        const SceneDev& S = table[sc[u]];
+        const float3 r = ar::quat_rotate(q[u], ar::mk3(r4[u].x, r4[u].y, r4[u].z));
+        const float3 p = ar::add(ar::xyz(c[u]), r);
+        const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
+        keys[g] = key;
+        ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
+      }
+    }
   }
   __syncthreads();
   ar_sort::hist_flush(s_hist, ws_hist, passes);
@@ -94,38 +159,77 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
 // One thread per sorted slot k: sorted position (w = global body id) and velocity (w = scene
 // index) recomputed from the body state of particle svals[k].  (Gathering by sorted slot is
 // faster here than pushing from the original order: scattered 16-byte stores cost more than
-// the gathers.)  Cell entry = {first sorted slot, end slot, body tag, 0}; the tag is the
-// global body id when every occupant belongs to one body (else kEmpty), so that a particle
-// skips a neighbour cell of its own body without loading its occupants (they could only be
-// rejected).  The thread at a cell's first slot writes the whole entry.
+// the gathers.)  Cell entry = {first sorted slot, count | epoch | body tag}; the tag names the
+// body when every occupant belongs to one body, so that a particle skips a neighbour cell of
+// its own body without loading its occupants (they could only be rejected).  The thread at a
+// cell's first slot writes the whole entry.
+// kScatterBatch sorted slots per thread and round, loads issued before use (as in K1).
+constexpr int kScatterBatch = 1;
 __global__ void __launch_bounds__(256) scatter_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
     const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
-    uint4* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
+    uint2* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
     const long long* __restrict__ d_step) {
-  const uint32_t epoch = cell_epoch(*d_step);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
-    const uint32_t key = __ldg(skeys + k);
-    const int g = (int)__ldg(svals + k);
-    const int sc = __ldg(pscene + g);
-    const SceneDev& S = table[sc];
-    const float4 r4 = __ldg(S.rel + (g - S.poff));
-    const int b = __float_as_int(r4.w);
-    if (k == 0 || key != __ldg(skeys + k - 1)) {
-      // occupants of one cell belong to one scene
-      uint32_t tag = (uint32_t)(S.boff + b);
-      int e = k + 1;
-      for (; e < nt && __ldg(skeys + e) == key; ++e) {
-        const int ge = (int)__ldg(svals + e);
-        if (__float_as_int(__ldg(S.rel + (ge - S.poff)).w) != b) tag = ar::kEmpty;
+  const uint32_t epoch = cell_epoch(*d_step) << kEpochShift;
+  const int stride = gridDim.x * blockDim.x;
+  for (int k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < nt; k0 += stride * kScatterBatch) {
+    uint32_t key[kScatterBatch];
+    int g[kScatterBatch], sc[kScatterBatch];
+    bool first[kScatterBatch];
+    float4 r4[kScatterBatch], q[kScatterBatch], c[kScatterBatch], v[kScatterBatch],
+        w[kScatterBatch];
+#pragma unroll
+    for (int u = 0; u < kScatterBatch; ++u) {
+      const int k = k0 + u * stride;
+      if (k < nt) {
+        key[u] = __ldg(skeys + k);
+        g[u] = (int)__ldg(svals + k);
+        first[u] = k == 0 || key[u] != __ldg(skeys + k - 1);
       }
-      cells[key] = make_uint4((uint32_t)k, (uint32_t)e, tag, epoch);
     }
-    float3 r, p, v;
-    ar_pipe::repose(__ldg(S.quat + b), __ldg(S.pos + b), __ldg(S.vel + b), __ldg(S.ang + b),
-                    ar::mk3(r4.x, r4.y, r4.z), &r, &p, &v);
-    spos[k] = make_float4(p.x, p.y, p.z, __int_as_float(S.boff + b));
-    svel[k] = make_float4(v.x, v.y, v.z, __int_as_float(sc));  // w = scene index
+#pragma unroll
+    for (int u = 0; u < kScatterBatch; ++u)
+      if (k0 + u * stride < nt) sc[u] = __ldg(pscene + g[u]);
+#pragma unroll
+    for (int u = 0; u < kScatterBatch; ++u) {
+      if (k0 + u * stride < nt) {
+        const SceneDev& S = table[sc[u]];
+        r4[u] = __ldg(S.rel + (g[u] - S.poff));
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kScatterBatch; ++u) {
+      if (k0 + u * stride < nt) {
+        const SceneDev& S = table[sc[u]];
+        const int b = __float_as_int(r4[u].w);
+        q[u] = __ldg(S.quat + b);
+        c[u] = __ldg(S.pos + b);
+        v[u] = __ldg(S.vel + b);
+        w[u] = __ldg(S.ang + b);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kScatterBatch; ++u) {
+      const int k = k0 + u * stride;
+      if (k >= nt) continue;
+      const SceneDev& S = table[sc[u]];
+      const int b = __float_as_int(r4[u].w);
+      if (first[u]) {
+        // occupants of one cell belong to one scene
+        uint32_t tag = body_tag(b);
+        int e = k + 1;
+        for (; e < nt && __ldg(skeys + e) == key[u]; ++e) {
+          const int ge = (int)__ldg(svals + e);
+          if (__float_as_int(__ldg(S.rel + (ge - S.poff)).w) != b) tag = 0;
+        }
+        const uint32_t count = (uint32_t)(e - k) < kCountMask ? (uint32_t)(e - k) : kCountMask;
+        cells[key[u]] = make_uint2((uint32_t)k, count | epoch | (tag << kTagShift));
+      }
+      float3 r, p, vv;
+      ar_pipe::repose(q[u], c[u], v[u], w[u], ar::mk3(r4[u].x, r4[u].y, r4[u].z), &r, &p, &vv);
+      spos[k] = make_float4(p.x, p.y, p.z, __int_as_float(S.boff + b));
+      svel[k] = make_float4(vv.x, vv.y, vv.z, __int_as_float(sc[u]));  // w = scene index
+    }
   }
 }
 
@@ -141,12 +245,12 @@ __global__ void __launch_bounds__(256) scatter_kernel(
 // above (2r)^2 are rejected without the square root: for them sqrtf(d2) >= 2r exactly, so the
 // contact test is unchanged.
 struct RowCells {
-  uint4 a, b, c;
+  uint2 a, b, c;
 };
 
 __global__ void __launch_bounds__(256, 4) collide_kernel(
     const SceneDev* __restrict__ table, int nt, const uint32_t* __restrict__ skeys,
-    const uint32_t* __restrict__ svals, const uint4* __restrict__ cells,
+    const uint32_t* __restrict__ svals, const uint2* __restrict__ cells,
     const float4* __restrict__ spos, const float4* __restrict__ svel,
     float4* __restrict__ pforce, const long long* __restrict__ d_step) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -157,6 +261,10 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
   const SceneDev& S = table[__float_as_int(v4.w)];
   const float3 pos = ar::xyz(p4), vel = ar::xyz(v4);
   const int body = __float_as_int(p4.w);
+  // the meta word of a cell holding only this body, count bits cleared (an impossible word
+  // when the body has no tag)
+  const uint32_t btag = body_tag(body - S.boff);
+  const uint32_t own = btag ? (epoch << kEpochShift) | (btag << kTagShift) : 0xffffffffu;
   const float thr = 2.0f * S.r;
   const float thr2_up = nextafterf(thr * thr, INFINITY);
   const float kk = S.k, dmp = S.damping, shr = S.shear, att = S.attraction;
@@ -164,20 +272,27 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
   const uint32_t base = S.cell_base, local = __ldg(skeys + k) - base;
   const uint32_t x = local & mx, y = (local >> lx) & my, z = local >> (lx + ly);
   const uint32_t xa = (x - 1) & mx, xc = (x + 1) & mx;
+  uint32_t row = 0;
   auto row_of = [&](int r) {  // r = 3 (dz + 1) + (dy + 1)
     const uint32_t zz = (z + (uint32_t)(r / 3) - 1u) & mz, yy = (y + (uint32_t)(r % 3) - 1u) & my;
-    const uint32_t row = base + (zz << (lx + ly)) + (yy << lx);
+    row = base + (zz << (lx + ly)) + (yy << lx);
     return RowCells{__ldg(cells + row + xa), __ldg(cells + row + x), __ldg(cells + row + xc)};
   };
   // occupants to visit: none for an empty cell (another step's entry) or a cell holding only
-  // this particle's body
-  auto visits = [&](const uint4& c) {
-    return (c.w != epoch || c.z == (uint32_t)body) ? 0u : c.y - c.x;
+  // this particle's body; a saturated count is resolved from the sorted keys
+  auto visits = [&](const uint2& c, uint32_t cell) {
+    const uint32_t m = c.y & ~kCountMask;
+    if (((m >> kEpochShift) & kEpochMask) != epoch || m == own) return 0u;
+    uint32_t n = c.y & kCountMask;
+    if (n == kCountMask)
+      while (c.x + n < (uint32_t)nt && __ldg(skeys + c.x + n) == cell) ++n;
+    return n;
   };
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
   for (int r = 0; r < 9; ++r) {
     const RowCells cur = row_of(r);
-    const uint32_t na = visits(cur.a), nb = visits(cur.b), nc = visits(cur.c);
+    const uint32_t na = visits(cur.a, row + xa), nb = visits(cur.b, row + x),
+                   nc = visits(cur.c, row + xc);
     const uint32_t nab = na + nb, total = nab + nc;
     float3 fa = ar::mk3(0.f, 0.f, 0.f), fb = fa, fc = fa;
     for (uint32_t t = 0; t < total; ++t) {
@@ -566,7 +681,7 @@ struct ar_batch {
   // buffers
   uint32_t *keys = nullptr, *skeys = nullptr, *svals = nullptr;
   float4 *spos = nullptr, *svel = nullptr, *pforce = nullptr;
-  uint4* cells = nullptr;  // {first slot, end slot, body tag, 0} per cell
+  uint2* cells = nullptr;  // {first slot, count | epoch | body tag} per cell
   char* sort_ws = nullptr;
   SceneDev* d_table = nullptr;
   int *d_poff = nullptr, *d_boff = nullptr;
@@ -583,7 +698,6 @@ struct ar_batch {
   long nt = 0, bt = 0;
   uint64_t total_cells = 0;
   int key_bits = 1, passes = 1, last_bits = 1;
-  // the cell table is empty between steps (each step resets the cells it occupied)
   // BVH broad phase (allocated only for BVH batches)
   int broadphase = AR_BROADPHASE_GRID;
   long cap_bvh = 0;
@@ -726,7 +840,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
       return AR_ERR_OOM;
     }
     B->cap_n = cn; B->cap_b = cb; B->cap_s = cs; B->cap_cells = cc; B->cap_sort = csort;
-    cudaMemsetAsync(B->cells, 0xff, cc * sizeof(uint4), st);
+    cudaMemsetAsync(B->cells, 0, cc * sizeof(uint2), st);  // epoch 0: empty
   }
   B->broadphase = ns > 0 ? B->scenes[0]->desc.broadphase : AR_BROADPHASE_GRID;
   if (B->broadphase == AR_BROADPHASE_BVH) {
@@ -799,8 +913,8 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
 }
 
 // Stage boundaries for ar_step_profile: events[0] before the step, events[i] after stage i.
-// Grid: clear (sort histogram head) | cell keys + histogram | sort | scatter + cell table |
-// collide | body sums + integration (+ cell reset).  BVH: clear (refit counters) | Morton keys
+// Grid: clear (sort histogram head, cell-table slice) | cell keys + histogram | sort |
+// scatter + cell table | collide | body sums + integration.  BVH: clear (refit counters) | Morton keys
 // | sort | tree (Karras nodes, leaves, scene roots, refit) | collide | body sums + integration.
 constexpr int kStages = 6;
 
@@ -849,7 +963,9 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     mark(6);
     return arh::check_launch("step (BVH)");
   }
-  cudaMemsetAsync(B->sort_ws, 0, ar_sort::clear_bytes(nt, B->passes), st);
+  step_clear_kernel<<<ctx->num_sms * 2, 256, 0, st>>>(
+      (uint4*)B->sort_ws, (long)(ar_sort::clear_bytes(nt, B->passes) / 16), B->cells,
+      B->cap_cells, B->d_step);
   mark(1);
   grid_keys_kernel<<<std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4),
                      kK1Threads, 0, st>>>(B->d_table, B->d_pscene, nt, B->keys,
@@ -875,13 +991,6 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   return arh::check_launch("step");
 }
 
-// Before the step numbered host_step + 1: when that number opens a new 2^31 window of cell
-// epochs, refill the cell table so that no entry of the previous window can match.
-void before_step(ar_batch* B, cudaStream_t st) {
-  if (B->broadphase == AR_BROADPHASE_GRID && B->cells && ((B->host_step + 1) & 0x7fffffffLL) == 0)
-    cudaMemsetAsync(B->cells, 0xff, B->cap_cells * sizeof(uint4), st);
-}
-
 // Run n_steps eagerly with events between the stages; average milliseconds per stage.
 ar_status profile_steps(ar_batch* B, int n_steps, float* stage_ms, cudaStream_t st) {
   cudaEvent_t ev[kStages + 1];
@@ -889,7 +998,6 @@ ar_status profile_steps(ar_batch* B, int n_steps, float* stage_ms, cudaStream_t 
   double acc[kStages] = {0};
   ar_status s = AR_OK;
   for (int i = 0; i < n_steps && s == AR_OK; ++i) {
-    before_step(B, st);
     s = enqueue_step(B, st, ev);
     if (s != AR_OK) break;
     ++B->host_step;
@@ -914,7 +1022,6 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
   if (B->nt == 0 || n_steps <= 0) return AR_OK;
   if (!use_graph) {
     for (int i = 0; i < n_steps; ++i) {
-      before_step(B, st);
       if ((s = enqueue_step(B, st)) != AR_OK) return s;
       ++B->host_step;
     }
@@ -950,7 +1057,6 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
     }
   }
   for (int i = 0; i < n_steps; ++i) {
-    before_step(B, st);
     if (cudaGraphLaunch(B->graph, st) != cudaSuccess) return arh::check_launch("graph launch");
     ++B->host_step;
   }
@@ -1004,7 +1110,7 @@ size_t ar_scene_footprint(const ar_scene_desc* d) {
     return n * per_particle + b * per_body + 4096;
   }
   const size_t per_particle = shared + 4 * 2 /*keys*/ + 8 /*sort tmp*/;
-  return n * per_particle + b * per_body + (size_t)ar_scene_cells(d) * 16 + 4096;
+  return n * per_particle + b * per_body + (size_t)ar_scene_cells(d) * sizeof(uint2) + 4096;
 }
 
 uint64_t ar_scene_cells(const ar_scene_desc* d) {

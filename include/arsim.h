@@ -485,8 +485,11 @@ AR_API ar_status ar_scene_grid_info(ar_scene* scene, float origin[3], float cell
 /* Device pointers into the workspace of the scene's last ar_step (for parity tests and
  * consumers that want the sorted state): the sorted keys and the particle index of each
  * sorted slot, sorted positions (w = body index, int bits) and velocities, the per-particle
- * DEM + wall force at the original index, and for the grid broad phase the cell table as
- * (start, end) pairs (start = 0xffffffff for an empty cell).  Grid keys are uint32 cell keys
+ * DEM + wall force at the original index, and for the grid broad phase the cell table: two
+ * uint32 per cell, {first sorted slot, meta}, meta = occupant count (bits 0-4, 31 meaning 31
+ * or more) | step epoch (bits 5-12: the step number mod 255, plus 1; any other value marks an
+ * empty cell) | body tag (bits 13-31: scene-local body + 1 when every occupant belongs to that
+ * body, else 0).  Grid keys are uint32 cell keys
  * (key_bytes 4); BVH keys are uint64 Morton codes (key_bytes 8), and the BVH view adds the
  * tree (leaf i at i, internal node i at N + i, root N) and tree_nodes16: 16 floats per
  * internal node holding both children's boxes and ids -- left lo.xyz, hi.x | hi.y, hi.z,

@@ -154,3 +154,53 @@ def test_model_matrices_for_the_renderer(ctx):
     assert np.array_equal(m[:, 3, :3], st["pos"][:, :3])
     assert np.all(m[:, :3, 3] == 0) and np.all(m[:, 3, 3] == 1)
     gs.close()
+
+
+def _cell_table(gs: api.GpuScene):
+    v = gs.step_view()
+    cells = api.device_view(v.cells2, 2 * v.num_cells, torch.int32).cpu().numpy().view(np.uint32)
+    return cells.reshape(-1, 2)
+
+
+def test_cell_epochs_recur_without_stale_entries(ctx):
+    """Epochs repeat every 255 steps; the rolling slice clear keeps stale entries from
+    matching, so 600 graph-replayed steps stay bit-exact."""
+    sc = scenes.small_scene(4, nb_side=4, packed=True, r=1 / 128)
+    gs = api.GpuScene(ctx, sc)
+    gs.step(600, use_graph=True)
+    ctx.check()
+    got = gs.download()
+    ref = cpu.step(sc, 600)
+    for k in ("pos", "quat", "vel", "angvel"):
+        assert np.array_equal(got[k], ref[k]), k
+    gs.close()
+
+
+def test_cell_table_entries(ctx):
+    """Every occupied cell: first sorted slot, saturating count, this step's epoch and the body
+    tag; a 4^3 wrapped grid crowds more than 31 particles into some cells, whose end is then
+    found from the sorted keys (results stay bit-exact)."""
+    sc = scenes.small_scene(6, nb_side=5, packed=True, r=1 / 128)
+    sc.grid_log2 = (2, 2, 2)
+    gs = api.GpuScene(ctx, sc)
+    steps = 3
+    gs.step(steps, use_graph=False)
+    ctx.check()
+    ref = cpu.step(sc, steps)
+    got = gs.download()
+    for k in ("pos", "quat", "vel", "angvel"):
+        assert np.array_equal(got[k], ref[k]), k
+    keys, idx, pf = _sorted_arrays(gs)
+    assert np.array_equal(pf, ref["pforce"])
+    table = _cell_table(gs)
+    body = sc.body_index()
+    uk, first, cnt = np.unique(keys, return_index=True, return_counts=True)
+    assert cnt.max() > 31
+    meta = table[uk, 1]
+    assert np.array_equal(table[uk, 0], first)
+    assert np.array_equal(meta & 31, np.minimum(cnt, 31))
+    assert np.all(((meta >> 5) & 255) == steps % 255 + 1)
+    sb = body[idx]
+    single = np.minimum.reduceat(sb, first) == np.maximum.reduceat(sb, first)
+    assert np.array_equal(meta >> 13, np.where(single, sb[first] + 1, 0))
+    gs.close()
