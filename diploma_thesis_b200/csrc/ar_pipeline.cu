@@ -272,25 +272,43 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
   const uint32_t base = S.cell_base, local = __ldg(skeys + k) - base;
   const uint32_t x = local & mx, y = (local >> lx) & my, z = local >> (lx + ly);
   const uint32_t xa = (x - 1) & mx, xc = (x + 1) & mx;
-  uint32_t row = 0;
-  auto row_of = [&](int r) {  // r = 3 (dz + 1) + (dy + 1)
+  auto row_base = [&](int r) {  // r = 3 (dz + 1) + (dy + 1)
     const uint32_t zz = (z + (uint32_t)(r / 3) - 1u) & mz, yy = (y + (uint32_t)(r % 3) - 1u) & my;
-    row = base + (zz << (lx + ly)) + (yy << lx);
-    return RowCells{__ldg(cells + row + xa), __ldg(cells + row + x), __ldg(cells + row + xc)};
+    return base + (zz << (lx + ly)) + (yy << lx);
   };
-  // occupants to visit: none for an empty cell (another step's entry) or a cell holding only
-  // this particle's body; a saturated count is resolved from the sorted keys
-  auto visits = [&](const uint2& c, uint32_t cell) {
-    const uint32_t m = c.y & ~kCountMask;
-    if (((m >> kEpochShift) & kEpochMask) != epoch || m == own) return 0u;
+  // a cell has occupants to visit unless it is empty (another step's entry) or holds only this
+  // particle's body
+  auto live = [&](uint32_t m) {
+    m &= ~kCountMask;
+    return ((m >> kEpochShift) & kEpochMask) == epoch && m != own ? 1u : 0u;
+  };
+  // pass 1: the meta words of all 27 cells (independent loads, all in flight together) ->
+  // bit 3 r + i set when cell i (x-1, x, x+1) of row r has occupants to visit
+  const uint32_t* __restrict__ meta = reinterpret_cast<const uint32_t*>(cells) + 1;
+  uint32_t todo = 0;
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    const size_t rb = row_base(r);
+    const uint32_t ma = __ldg(meta + 2 * (rb + xa)), mb = __ldg(meta + 2 * (rb + x)),
+                   mc = __ldg(meta + 2 * (rb + xc));
+    todo |= (live(ma) | (live(mb) << 1) | (live(mc) << 2)) << (3 * r);
+  }
+  // pass 2: rows with occupants to visit, in order.  A row without any would add +0 to every
+  // component of the total, which leaves it unchanged (the total starts at +0, and a float sum
+  // is -0 only when both addends are), so such rows are skipped.
+  auto visits = [&](const uint2& c, uint32_t cell) {  // a saturated count is resolved from the keys
+    if (!live(c.y)) return 0u;
     uint32_t n = c.y & kCountMask;
     if (n == kCountMask)
       while (c.x + n < (uint32_t)nt && __ldg(skeys + c.x + n) == cell) ++n;
     return n;
   };
   float3 lin = ar::mk3(0.f, 0.f, 0.f);
-  for (int r = 0; r < 9; ++r) {
-    const RowCells cur = row_of(r);
+  while (todo) {
+    const int r = (__ffs(todo) - 1) / 3;
+    todo &= ~(7u << (3 * r));
+    const uint32_t row = row_base(r);
+    const RowCells cur{__ldg(cells + row + xa), __ldg(cells + row + x), __ldg(cells + row + xc)};
     const uint32_t na = visits(cur.a, row + xa), nb = visits(cur.b, row + x),
                    nc = visits(cur.c, row + xc);
     const uint32_t nab = na + nb, total = nab + nc;
