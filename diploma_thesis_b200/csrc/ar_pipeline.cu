@@ -105,11 +105,12 @@ __global__ void __launch_bounds__(256) step_clear_kernel(uint4* __restrict__ hea
 constexpr int kKeysBatch = 2;
 __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
-    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, int passes, int last_bits,
+    uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, ar_sort::Plan plan,
     long long* __restrict__ d_step) {
-  __shared__ uint32_t s_hist[ar_sort::kMaxPasses][256];
+  __shared__ uint32_t s_hist[ar_sort::kMaxPasses][ar_sort::kMaxRadix];
   if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
-  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) (&s_hist[0][0])[i] = 0;
+  for (int i = threadIdx.x; i < plan.passes * ar_sort::kMaxRadix; i += blockDim.x)
+    (&s_hist[0][0])[i] = 0;
   __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   for (int g0 = blockIdx.x * blockDim.x + threadIdx.x; g0 < nt; g0 += stride * kKeysBatch) {
@@ -147,12 +148,12 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
         const float3 p = ar::add(ar::xyz(c[u]), r);
         const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
         keys[g] = key;
-        ar_sort::hist_count_warp(s_hist, key, 0, passes, last_bits);
+        ar_sort::hist_count_warp(s_hist, key, plan);
       }
     }
   }
   __syncthreads();
-  ar_sort::hist_flush(s_hist, ws_hist, passes);
+  ar_sort::hist_flush(s_hist, ws_hist, plan.passes);
 }
 
 // ---- K3: scatter + cell table -------------------------------------------------------------
@@ -715,7 +716,8 @@ struct ar_batch {
   // layout
   long nt = 0, bt = 0;
   uint64_t total_cells = 0;
-  int key_bits = 1, passes = 1, last_bits = 1;
+  int key_bits = 1;
+  ar_sort::Plan plan{};  // digit passes of the cell-key sort
   // BVH broad phase (allocated only for BVH batches)
   int broadphase = AR_BROADPHASE_GRID;
   long cap_bvh = 0;
@@ -832,7 +834,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     return AR_ERR_INVALID_ARG;
   }
   const int key_bits = std::max(1, ceil_log2(cells));
-  const int passes = (key_bits + 7) / 8;
+  const int passes = ar_sort::make_plan(0, key_bits).passes;
   const size_t sort_bytes = ar_sort::layout(std::max(nt, 1l), 4, passes).total;
   const long ns = (long)B->scenes.size();
   bool realloc_needed = nt > B->cap_n || bt > B->cap_b || ns + 1 > B->cap_s ||
@@ -863,7 +865,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
   B->broadphase = ns > 0 ? B->scenes[0]->desc.broadphase : AR_BROADPHASE_GRID;
   if (B->broadphase == AR_BROADPHASE_BVH) {
     B->bvh_key_bits = kMortonBits + std::max(0, ceil_log2((uint64_t)std::max(ns, 1l)));
-    const int passes64 = (B->bvh_key_bits + 7) / 8;
+    const int passes64 = ar_sort::make_plan(0, B->bvh_key_bits).passes;
     const size_t s64 = ar_sort::layout(std::max(nt, 1l), 8, passes64).total;
     if (nt > B->cap_bvh || s64 > B->cap_sort64) {
       cudaStreamSynchronize(st);
@@ -924,8 +926,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
   B->bt = bt;
   B->total_cells = cells;
   B->key_bits = key_bits;
-  B->passes = passes;
-  B->last_bits = key_bits - 8 * (passes - 1);
+  B->plan = ar_sort::make_plan(0, key_bits);
   B->table_dirty = false;
   return arh::check_launch("batch prepare");
 }
@@ -982,12 +983,12 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     return arh::check_launch("step (BVH)");
   }
   step_clear_kernel<<<ctx->num_sms * 2, 256, 0, st>>>(
-      (uint4*)B->sort_ws, (long)(ar_sort::clear_bytes(nt, B->passes) / 16), B->cells,
+      (uint4*)B->sort_ws, (long)(ar_sort::clear_bytes(nt, B->plan.passes) / 16), B->cells,
       B->cap_cells, B->d_step);
   mark(1);
   grid_keys_kernel<<<std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4),
                      kK1Threads, 0, st>>>(B->d_table, B->d_pscene, nt, B->keys,
-                                          (uint32_t*)B->sort_ws, B->passes, B->last_bits,
+                                          (uint32_t*)B->sort_ws, B->plan,
                                           B->d_step);
   mark(2);
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,

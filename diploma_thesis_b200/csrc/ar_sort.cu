@@ -2,7 +2,7 @@
 // decoupled look-back).  Replaces cub::DeviceRadixSort::SortPairs on the reference's path
 // (Kernels/particleKernelWrappers.cu:419-534, BVHSource/createMortonCodes.cu:183-218).
 //
-// Pass structure (per 8-bit digit):
+// Pass structure (per digit of 8 bits, or 9 where that saves a pass; ar_sort::make_plan):
 //   * each CTA takes the next tile index from an atomic counter, so every earlier tile is
 //     already running or finished (look-back always makes progress);
 //   * warps rank their items stably with a ballot multi-split (items are visited in input
@@ -29,7 +29,7 @@ constexpr int kItems = 16;     // keys per thread in a digit pass
 // 2^19 keys on, 256 below (more tiles to spread over the SMs).
 inline int pass_threads(long n) { return n >= (1l << 19) ? 512 : 256; }
 inline long tile_items(long n) { return (long)pass_threads(n) * kItems; }
-constexpr int kRadix = 256;
+constexpr int kRadix = ar_sort::kMaxRadix;  // histogram / status stride per pass
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1;
@@ -44,17 +44,16 @@ __device__ __forceinline__ uint32_t digit_of(K key, int shift, uint32_t mask) {
 // ---- histogram of every pass, one read of the keys -----------------------------------------
 template <class K>
 __global__ void __launch_bounds__(kThreads) hist_kernel(const K* __restrict__ keys, int n,
-                                                       int begin_bit, int passes, int last_bits,
+                                                       ar_sort::Plan plan,
                                                        uint32_t* __restrict__ hist) {
   __shared__ uint32_t s_hist[ar_sort::kMaxPasses][kRadix];
+  const int passes = plan.passes;
   for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) (&s_hist[0][0])[i] = 0;
   __syncthreads();
   for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
     K k = keys[i];
-    for (int p = 0; p < passes; ++p) {
-      uint32_t mask = (p == passes - 1) ? ((1u << last_bits) - 1) : 0xffu;
-      atomicAdd(&s_hist[p][digit_of(k, begin_bit + 8 * p, mask)], 1u);
-    }
+    for (int p = 0; p < passes; ++p)
+      atomicAdd(&s_hist[p][digit_of(k, plan.shift[p], (1u << plan.bits[p]) - 1)], 1u);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) {
@@ -63,7 +62,7 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const K* __restrict__ ke
   }
 }
 
-// Exclusive scan of each pass's 256-bin histogram (one warp per pass).
+// Exclusive scan of each pass's histogram (kRadix bins; one warp per pass).
 __global__ void hist_scan_kernel(uint32_t* __restrict__ hist, int passes) {
   int p = threadIdx.x >> 5;
   if (p >= passes) return;
@@ -83,17 +82,18 @@ __global__ void hist_scan_kernel(uint32_t* __restrict__ hist, int passes) {
 }
 
 // ---- one digit pass ---------------------------------------------------------------------------
-template <class K, int kT>
+template <class K, int kT, int kBits>
 struct PassSmem {
   K keys[kT * kItems];
   uint32_t vals[kT * kItems];
-  uint32_t warp_hist[kT / 32][kRadix];
-  uint32_t digit_start[kRadix];  // tile-local exclusive start of each digit
-  uint32_t gofs[kRadix];         // global destination of the digit's first tile element
+  uint32_t warp_hist[kT / 32][1 << kBits];
+  uint32_t digit_start[1 << kBits];  // tile-local exclusive start of each digit
+  uint32_t gofs[1 << kBits];         // global destination of the digit's first tile element
   uint32_t tile_id;
 };
 
-template <class K, int kT>
+// One digit pass of at most kBits bits (kBits 9 only with kT 512: one digit per thread).
+template <class K, int kT, int kBits>
 __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) onesweep_kernel(
     const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int n, int shift, int bits,
@@ -102,12 +102,14 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kWarps = kT / 32;
   constexpr int kTile = kT * kItems;
-  PassSmem<K, kT>& sm = *reinterpret_cast<PassSmem<K, kT>*>(smem_raw);
+  constexpr int kDigits = 1 << kBits;
+  static_assert(kDigits <= kT, "one digit per thread");
+  PassSmem<K, kT, kBits>& sm = *reinterpret_cast<PassSmem<K, kT, kBits>*>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t mask = (1u << bits) - 1;
 
   if (tid == 0) sm.tile_id = atomicAdd(tile_counter, 1u);
-  for (int i = tid; i < kWarps * kRadix; i += kT) (&sm.warp_hist[0][0])[i] = 0;
+  for (int i = tid; i < kWarps * kDigits; i += kT) (&sm.warp_hist[0][0])[i] = 0;
   __syncthreads();
   const uint32_t tile = sm.tile_id;
   const long tile_base = (long)tile * kTile;
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
     long g = wbase + j * 32 + lane;
-    // invalid items take digit kRadix-1 (after every valid item of the tile; never written)
+    // invalid items take digit kDigits-1 (after every valid item of the tile; never written)
     key[j] = g < n ? keys_in[g] : (K)~(K)0;
   }
 
@@ -130,9 +132,9 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
     const long g = wbase + j * 32 + lane;
-    const uint32_t dj = g < n ? digit_of(key[j], shift, mask) : kRadix - 1;
+    const uint32_t dj = g < n ? digit_of(key[j], shift, mask) : kDigits - 1;
     uint32_t peers = 0xffffffffu;
-    for (int b = 0; b < 8; ++b) {
+    for (int b = 0; b < kBits; ++b) {
       uint32_t bit = (dj >> b) & 1u;
       uint32_t m = __ballot_sync(0xffffffffu, bit);
       peers &= bit ? m : ~m;
@@ -148,9 +150,9 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
   __syncthreads();
 
   // per digit: exclusive over warps, tile count; the tile's aggregate is published at once
-  const int d = tid;  // threads below kRadix own one digit each
+  const int d = tid;  // threads below kDigits own one digit each
   uint32_t tile_count = 0;
-  if (d < kRadix) {
+  if (d < kDigits) {
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
       uint32_t c = sm.warp_hist[w][d];
@@ -174,7 +176,7 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
     __syncthreads();
     uint32_t add = 0;
     for (int w = 0; w < warp; ++w) add += s_wsum[w];
-    if (d < kRadix) sm.digit_start[d] = add + x - tile_count;
+    if (d < kDigits) sm.digit_start[d] = add + x - tile_count;
   }
   __syncthreads();
 
@@ -198,7 +200,7 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
 
   // look back through the earlier tiles, kLookWindow status words per round trip, until an
   // inclusive prefix is found; then publish this tile's inclusive prefix
-  if (d < kRadix) {
+  if (d < kDigits) {
     uint32_t excl = 0;
     if (tile != 0) {
       long k = (long)tile - 1;  // next tile to read
@@ -265,18 +267,48 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
   }
 }
 
-// external_hist: the caller already cleared the workspace head (ar_sort::clear) and
-// accumulated the per-pass histograms into it (ar_sort::hist_accumulate), e.g. fused into the
-// kernel that produced the keys.
+// The digit passes of `plan`, ping-ponging so that the last one lands in keys_out.  `status`
+// holds one [tiles][kRadix] block per pass, tiles = the most tiles any pass uses.
+template <class K>
+void launch_passes(const ar_sort::Plan& plan, int n, const K* keys_in, const uint32_t* vals_in,
+                   K* keys_out, uint32_t* vals_out, K* tmp_keys, uint32_t* tmp_vals,
+                   const uint32_t* hist, uint32_t* status, uint32_t* counters, int* err,
+                   cudaStream_t st) {
+  const long status_tiles = ((long)n + tile_items(n) - 1) / tile_items(n);
+  const K* src_k = keys_in;
+  const uint32_t* src_v = vals_in;
+  for (int p = 0; p < plan.passes; ++p) {
+    const bool to_out = ((plan.passes - 1 - p) % 2) == 0;
+    K* dk = to_out ? keys_out : tmp_keys;
+    uint32_t* dv = to_out ? vals_out : tmp_vals;
+    const int bits = plan.bits[p], shift = plan.shift[p];
+    const int kt = bits > 8 ? 512 : pass_threads(n);
+    const unsigned tiles = (unsigned)(((long)n + (long)kt * kItems - 1) / ((long)kt * kItems));
+    const uint32_t* base = hist + p * kRadix;
+    uint32_t* stat = status + (size_t)p * status_tiles * kRadix;
+    if (bits > 8)
+      onesweep_kernel<K, 512, 9><<<tiles, 512, sizeof(PassSmem<K, 512, 9>), st>>>(
+          src_k, src_v, dk, dv, n, shift, bits, base, stat, counters + p, err);
+    else if (kt == 512)
+      onesweep_kernel<K, 512, 8><<<tiles, 512, sizeof(PassSmem<K, 512, 8>), st>>>(
+          src_k, src_v, dk, dv, n, shift, bits, base, stat, counters + p, err);
+    else
+      onesweep_kernel<K, 256, 8><<<tiles, 256, sizeof(PassSmem<K, 256, 8>), st>>>(
+          src_k, src_v, dk, dv, n, shift, bits, base, stat, counters + p, err);
+    src_k = dk;
+    src_v = dv;
+  }
+}
+
+// external_hist: the caller already cleared the workspace head (ar_sort::clear_bytes) and
+// accumulated the per-pass histograms into it (ar_sort::hist_count_warp + hist_flush), e.g.
+// fused into the kernel that produced the keys.
 template <class K>
 ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* keys_out,
                     uint32_t* vals_out, int n, int begin_bit, int end_bit, cudaStream_t st,
                     void* ws, size_t ws_bytes, bool external_hist = false) {
-  const int total_bits = end_bit - begin_bit;
-  const int passes = (total_bits + 7) / 8;
-  const int last_bits = total_bits - 8 * (passes - 1);
-  const int kt = pass_threads(n);
-  const long tiles = ((long)n + tile_items(n) - 1) / tile_items(n);
+  const ar_sort::Plan plan = ar_sort::make_plan(begin_bit, end_bit);
+  const int passes = plan.passes;
   ar_sort::Layout L = ar_sort::layout(n, sizeof(K), passes);
   if (ws_bytes < L.total) {
     arh::set_error("radix sort: workspace too small");
@@ -291,35 +323,16 @@ ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* k
   int* err = ctx ? ctx->d_err : nullptr;
 
   if (!external_hist) {
-  cudaMemsetAsync(base, 0, L.status + (size_t)passes * tiles * kRadix * sizeof(uint32_t), st);
-  unsigned hgrid = (unsigned)((n + kThreads * 8 - 1) / (kThreads * 8));
-  unsigned cap = (unsigned)(ctx ? ctx->num_sms : 148) * 4;
-  if (hgrid > cap) hgrid = cap;
-  if (hgrid < 1) hgrid = 1;
-  hist_kernel<K><<<hgrid, kThreads, 0, st>>>(keys_in, n, begin_bit, passes, last_bits, hist);
+    cudaMemsetAsync(base, 0, ar_sort::clear_bytes(n, passes), st);
+    unsigned hgrid = (unsigned)((n + kThreads * 8 - 1) / (kThreads * 8));
+    unsigned cap = (unsigned)(ctx ? ctx->num_sms : 148) * 4;
+    if (hgrid > cap) hgrid = cap;
+    if (hgrid < 1) hgrid = 1;
+    hist_kernel<K><<<hgrid, kThreads, 0, st>>>(keys_in, n, plan, hist);
   }
   hist_scan_kernel<<<1, 32 * ar_sort::kMaxPasses, 0, st>>>(hist, passes);
-
-
-  // ping-pong so that the last pass lands in keys_out
-  const K* src_k = keys_in;
-  const uint32_t* src_v = vals_in;
-  for (int p = 0; p < passes; ++p) {
-    bool to_out = ((passes - 1 - p) % 2) == 0;
-    K* dk = to_out ? keys_out : tmp_keys;
-    uint32_t* dv = to_out ? vals_out : tmp_vals;
-    int bits = (p == passes - 1) ? last_bits : 8;
-    if (kt == 512)
-      onesweep_kernel<K, 512><<<(unsigned)tiles, 512, sizeof(PassSmem<K, 512>), st>>>(
-          src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
-          status + (size_t)p * tiles * kRadix, counters + p, err);
-    else
-      onesweep_kernel<K, 256><<<(unsigned)tiles, 256, sizeof(PassSmem<K, 256>), st>>>(
-          src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits, hist + p * kRadix,
-          status + (size_t)p * tiles * kRadix, counters + p, err);
-    src_k = dk;
-    src_v = dv;
-  }
+  launch_passes<K>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
+                   status, counters, err, st);
   return arh::check_launch("radix sort");
 }
 
@@ -349,7 +362,7 @@ ar_status sort_entry(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* 
       ar_sort::iota(vals_out, n, st);
     return arh::check_launch("radix sort copy");
   }
-  const int passes = (end_bit - begin_bit + 7) / 8;
+  const int passes = ar_sort::make_plan(begin_bit, end_bit).passes;
   ar_sort::Layout L = ar_sort::layout(n, sizeof(K), passes);
   void* ws = arh::scratch(ctx, L.total);
   if (!ws) return AR_ERR_OOM;
@@ -359,6 +372,23 @@ ar_status sort_entry(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* 
 
 __global__ void iota_kernel(uint32_t* v, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v[i] = i;
+}
+
+// Dynamic shared-memory opt-in of every digit-pass instantiation (current device).
+template <class K, int kT, int kBits>
+cudaError_t set_pass_attribute() {
+  return cudaFuncSetAttribute(onesweep_kernel<K, kT, kBits>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)sizeof(PassSmem<K, kT, kBits>));
+}
+cudaError_t set_pass_attributes() {
+  cudaError_t e = set_pass_attribute<uint32_t, 256, 8>();
+  if (e == cudaSuccess) e = set_pass_attribute<uint32_t, 512, 8>();
+  if (e == cudaSuccess) e = set_pass_attribute<uint32_t, 512, 9>();
+  if (e == cudaSuccess) e = set_pass_attribute<uint64_t, 256, 8>();
+  if (e == cudaSuccess) e = set_pass_attribute<uint64_t, 512, 8>();
+  if (e == cudaSuccess) e = set_pass_attribute<uint64_t, 512, 9>();
+  return e;
 }
 
 // ---- allocation-free variant -------------------------------------------------------------------
@@ -394,13 +424,7 @@ ar_status noalloc_setup(int dev, void** addr, int* sms) {
                      cudaGetErrorString(e));
       return AR_ERR_CUDA;
     }
-    e = cudaFuncSetAttribute(onesweep_kernel<uint32_t, 256>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(PassSmem<uint32_t, 256>));
-    if (e == cudaSuccess)
-      e = cudaFuncSetAttribute(onesweep_kernel<uint32_t, 512>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)sizeof(PassSmem<uint32_t, 512>));
+    e = set_pass_attributes();
     if (e != cudaSuccess) {
       arh::set_error("allocation-free sort: %s", cudaGetErrorString(e));
       return AR_ERR_CUDA;
@@ -419,20 +443,7 @@ ar_status noalloc_setup(int dev, void** addr, int* sms) {
 
 namespace ar_sort {
 
-void init() {
-  cudaFuncSetAttribute(onesweep_kernel<uint32_t, 256>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(PassSmem<uint32_t, 256>));
-  cudaFuncSetAttribute(onesweep_kernel<uint32_t, 512>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(PassSmem<uint32_t, 512>));
-  cudaFuncSetAttribute(onesweep_kernel<uint64_t, 256>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(PassSmem<uint64_t, 256>));
-  cudaFuncSetAttribute(onesweep_kernel<uint64_t, 512>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)sizeof(PassSmem<uint64_t, 512>));
-}
+void init() { set_pass_attributes(); }
 
 Layout layout(long n, size_t key_bytes, int passes) {
   const long tiles = (n + tile_items(n) - 1) / tile_items(n);
@@ -474,7 +485,7 @@ size_t clear_bytes(long n, int passes) {
 }
 
 int launches(int begin_bit, int end_bit, bool external_hist) {
-  return (external_hist ? 1 : 3) + (end_bit - begin_bit + 7) / 8;
+  return (external_hist ? 1 : 3) + make_plan(begin_bit, end_bit).passes;
 }
 
 }  // namespace ar_sort
@@ -532,11 +543,8 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
   int sms = 148;
   ar_status s = noalloc_setup(dev, &base_v, &sms);
   if (s != AR_OK) return s;
-  const int total_bits = end_bit - begin_bit;
-  const int passes = (total_bits + 7) / 8;
-  const int last_bits = total_bits - 8 * (passes - 1);
-  const int kt = pass_threads(n);
-  const long tiles = ((long)n + tile_items(n) - 1) / tile_items(n);
+  const ar_sort::Plan plan = ar_sort::make_plan(begin_bit, end_bit);
+  const int passes = plan.passes;
   const ar_sort::Layout L = ar_sort::layout(n, 4, passes);
   if (L.total > sizeof(g_noalloc_scratch)) {  // cannot happen for n <= kNoAllocMaxN
     arh::set_error("allocation-free sort: workspace layout exceeds the static array");
@@ -549,34 +557,14 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
   uint32_t* tmp_keys = (uint32_t*)(base + L.tmp_keys);
   uint32_t* tmp_vals = (uint32_t*)(base + L.tmp_vals);
   // the previous call's contents stay in the array: zero what must start at zero
-  cudaMemsetAsync(base, 0, L.status + (size_t)passes * tiles * kRadix * sizeof(uint32_t), st);
+  cudaMemsetAsync(base, 0, ar_sort::clear_bytes(n, passes), st);
   unsigned hgrid = (unsigned)((n + kThreads * 8 - 1) / (kThreads * 8));
   if (hgrid > (unsigned)sms * 4) hgrid = (unsigned)sms * 4;
   if (hgrid < 1) hgrid = 1;
-  hist_kernel<uint32_t><<<hgrid, kThreads, 0, st>>>(keys_in, n, begin_bit, passes, last_bits, hist);
+  hist_kernel<uint32_t><<<hgrid, kThreads, 0, st>>>(keys_in, n, plan, hist);
   hist_scan_kernel<<<1, 32 * ar_sort::kMaxPasses, 0, st>>>(hist, passes);
-  const uint32_t* src_k = keys_in;
-  const uint32_t* src_v = vals_in;
-  for (int p = 0; p < passes; ++p) {
-    const bool to_out = ((passes - 1 - p) % 2) == 0;
-    uint32_t* dk = to_out ? keys_out : tmp_keys;
-    uint32_t* dv = to_out ? vals_out : tmp_vals;
-    const int bits = (p == passes - 1) ? last_bits : 8;
-    if (kt == 512)
-      onesweep_kernel<uint32_t, 512><<<(unsigned)tiles, 512, sizeof(PassSmem<uint32_t, 512>),
-                                       st>>>(src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits,
-                                             hist + p * kRadix,
-                                             status + (size_t)p * tiles * kRadix, counters + p,
-                                             (int*)d_status);
-    else
-      onesweep_kernel<uint32_t, 256><<<(unsigned)tiles, 256, sizeof(PassSmem<uint32_t, 256>),
-                                       st>>>(src_k, src_v, dk, dv, n, begin_bit + 8 * p, bits,
-                                             hist + p * kRadix,
-                                             status + (size_t)p * tiles * kRadix, counters + p,
-                                             (int*)d_status);
-    src_k = dk;
-    src_v = dv;
-  }
+  launch_passes<uint32_t>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
+                          status, counters, (int*)d_status, st);
   return arh::check_launch("allocation-free sort");
 }
 

@@ -11,6 +11,32 @@ struct ar_ctx;
 namespace ar_sort {
 
 constexpr int kMaxPasses = 8;
+constexpr int kMaxRadix = 512;  // digits are 8 bits wide, or 9 where that saves a pass
+
+// Digit passes of a sort over key bits [begin, end): as few passes as 9-bit digits allow,
+// 8-bit digits where the bits suffice and 9-bit digits for the last (bits - 8 * passes)
+// passes otherwise (24 bits: 8, 8, 8; 25 bits: 8, 8, 9; 30 bits: 8, 8, 8, 6; 63 bits: 9 x 7).
+struct Plan {
+  int passes;
+  int shift[kMaxPasses];
+  int bits[kMaxPasses];
+};
+inline Plan make_plan(int begin_bit, int end_bit) {
+  Plan p{};
+  const int total = end_bit - begin_bit;
+  p.passes = total <= 0 ? 0 : (total + 8) / 9;
+  const int wide = total - 8 * p.passes;  // > 0: passes that take 9 bits
+  int shift = begin_bit;
+  for (int i = 0; i < p.passes; ++i) {
+    int b = 8;
+    if (wide > 0 && i >= p.passes - wide) b = 9;
+    if (wide <= 0 && i == p.passes - 1) b = total - 8 * (p.passes - 1);
+    p.shift[i] = shift;
+    p.bits[i] = b;
+    shift += b;
+  }
+  return p;
+}
 
 // Per-device kernel attributes (dynamic shared memory opt-in); called by ar_ctx_create so
 // that no attribute call ever happens inside a graph capture.
@@ -40,34 +66,25 @@ ar_status sort_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in
 // accumulated externally (histograms, tile counters, look-back status).
 size_t clear_bytes(long n, int passes);
 
-// Histogram of `key` for every pass into the workspace head (call from a kernel that holds
-// a shared [kMaxPasses][256] block histogram; see hist_flush).  Digit width 8, last pass
-// `last_bits` wide.
-__device__ __forceinline__ void hist_count(uint32_t (*s_hist)[256], uint32_t key, int begin_bit,
-                                           int passes, int last_bits) {
-  for (int p = 0; p < passes; ++p) {
-    uint32_t mask = (p == passes - 1) ? ((1u << last_bits) - 1) : 0xffu;
-    atomicAdd(&s_hist[p][(key >> (begin_bit + 8 * p)) & mask], 1u);
-  }
-}
-// hist_count with one shared-memory atomic per distinct digit per warp (the lanes holding the
-// same digit are counted by their lowest lane): particles of a body are adjacent in the
-// original order and mostly share digits, so this removes most same-address contention.
-__device__ __forceinline__ void hist_count_warp(uint32_t (*s_hist)[256], uint32_t key,
-                                                int begin_bit, int passes, int last_bits) {
+// Histogram of `key` for every pass of `plan` into a shared [kMaxPasses][kMaxRadix] block
+// histogram (then hist_flush), with one shared-memory atomic per distinct digit per warp (the
+// lanes holding the same digit are counted by their lowest lane): particles of a body are
+// adjacent in the original order and mostly share digits, so this removes most same-address
+// contention.
+__device__ __forceinline__ void hist_count_warp(uint32_t (*s_hist)[kMaxRadix], uint32_t key,
+                                                const Plan& plan) {
   const uint32_t active = __activemask();
   const int lane = threadIdx.x & 31;
-  for (int p = 0; p < passes; ++p) {
-    const uint32_t mask = (p == passes - 1) ? ((1u << last_bits) - 1) : 0xffu;
-    const uint32_t d = (key >> (begin_bit + 8 * p)) & mask;
+  for (int p = 0; p < plan.passes; ++p) {
+    const uint32_t d = (key >> plan.shift[p]) & ((1u << plan.bits[p]) - 1);
     const uint32_t peers = __match_any_sync(active, d);
     if (lane == __ffs(peers) - 1) atomicAdd(&s_hist[p][d], (uint32_t)__popc(peers));
   }
 }
-// Block histogram -> workspace head (ws + 0 holds uint32 [kMaxPasses][256]).
-__device__ __forceinline__ void hist_flush(uint32_t (*s_hist)[256], uint32_t* ws_hist,
+// Block histogram -> workspace head (ws + 0 holds uint32 [kMaxPasses][kMaxRadix]).
+__device__ __forceinline__ void hist_flush(uint32_t (*s_hist)[kMaxRadix], uint32_t* ws_hist,
                                            int passes) {
-  for (int i = threadIdx.x; i < passes * 256; i += blockDim.x) {
+  for (int i = threadIdx.x; i < passes * kMaxRadix; i += blockDim.x) {
     uint32_t v = (&s_hist[0][0])[i];
     if (v) atomicAdd(ws_hist + i, v);
   }

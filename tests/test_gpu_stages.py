@@ -56,7 +56,10 @@ def test_morton_random_with_edges(ctx, n):
 
 # ---- (a8) radix sort --------------------------------------------------------------------------
 @pytest.mark.parametrize("n,bits", [(1, 32), (2, 1), (4095, 8), (4096, 9), (4097, 16),
-                                    (100003, 21), (1 << 20, 32), (777777, 30)])
+                                    (100003, 21), (1 << 20, 32), (777777, 30),
+                                    # plans with 9-bit passes: 8+9; 8+9+9 with 256- and
+                                    # 512-thread tiles in one sort; 8+8+9 at 2M keys
+                                    (50001, 17), (300001, 26), ((1 << 21) + 3, 25)])
 def test_sort_u32_matches_stable_order(ctx, n, bits):
     rng = np.random.default_rng(bits * 7 + n)
     keys = rng.integers(0, 1 << bits, n, dtype=np.uint64).astype(np.uint32)
