@@ -5,7 +5,7 @@
 
 Workload (default "pile"): the plain large pile -- 2,097,152 particles, 32,768 bodies of 64
 (cubes, rods, padded spheres), r = 1/512, 1 x 3 x 1 box, dt = 1e-4, k = 5e4, damping 0.02,
-shear 0.1, grid broad phase (256^3 wrapped cells of 2r).  "plain" is the 110,592-particle
+shear 0.1, grid broad phase (256 x 512 x 256 wrapped cells of 2r).  "plain" is the 110,592-particle
 single scene (4,096 cubes, 128^3 grid).  Seeded synthetic scenes; no dataset exists.
 
 Metric: Mparticle-steps/s (whole job).  A step is one pass of the fused pipeline over the
@@ -38,8 +38,8 @@ FALLBACK_HBM_GBS = 6650.0
 
 # Algorithmic bytes per particle and per body for each stage of the fused step (compulsory
 # traffic of this design: every array element read or written once; neighbour reads that hit
-# in L2 are not counted).  P = sort passes, ppb = particles per body.  A step runs: sort |
-# scatter + cell table | collide | clear | body (sums, integration, next step's keys).
+# in L2 are not counted).  P = sort passes, ppb = particles per body.  A step runs: clear |
+# keys | sort | scatter + cell table | collide | body (sums, integration).
 STAGES = ["clear", "keys", "sort", "scatter", "collide", "body"]
 BODY_STATE = 16 * 4  # pos, quat, vel, angvel (float4 each)
 
@@ -49,22 +49,29 @@ def _body_bytes(nb: int) -> int:
     return nb * (BODY_STATE + 4 + 36 + BODY_STATE + 32)
 
 
-def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int) -> dict[str, float]:
+def sort_passes(bits: int) -> int:
+    """Digit passes of the radix sort over `bits` key bits (8-bit digits, 9 where that saves
+    a pass: 24 bits -> 3, 25 -> 3, 30 -> 4, 63 -> 7)."""
+    return (bits + 8) // 9 if bits > 0 else 0
+
+
+def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int,
+                cells: int = 0) -> dict[str, float]:
     tiles = (n + 8191) // 8192
     return {
-        # sort histogram / look-back head
-        "clear": 4 * 256 * 8 + passes * 4 * 256 * tiles,
+        # sort histogram / look-back head; one 255th of the 8-byte cell table
+        "clear": 4 * 512 * 8 + passes * 4 * 512 * tiles + 8 * cells // 255,
         # rel in, key out; body pose (32) per body
         "keys": n * (16 + 4) + nb * 32,
         # first pass reads the key only; every pass writes key + index; later passes read both
-        "sort": n * (4 + 8) + (passes - 1) * n * 16 + passes * 4 * 256 * tiles,
+        "sort": n * (4 + 8) + (passes - 1) * n * 16 + passes * 4 * 512 * tiles,
         # sorted key + index and rel in, sorted position + velocity out; body state per body;
-        # one 16-byte cell entry per occupied cell
-        "scatter": n * (8 + 16 + 32) + nb * BODY_STATE + occupied_cells * 16,
+        # one 8-byte cell entry per occupied cell
+        "scatter": n * (8 + 16 + 32) + nb * BODY_STATE + occupied_cells * 8,
         # own key, index, position, velocity in; force out
         "collide": n * (4 + 4 + 32 + 16),
-        # force + rel in; sorted key in and one reset per occupied cell; body state
-        "body": n * (16 + 16 + 4) + occupied_cells * 4 + _body_bytes(nb),
+        # force + rel in; body state
+        "body": n * (16 + 16) + _body_bytes(nb),
     }
 
 
@@ -80,7 +87,7 @@ def stage_bytes_bvh(n: int, nb: int, passes: int) -> dict[str, float]:
         "keys": n * (16 + 8) + nb * 32,
         # histogram pass reads the keys; first pass reads keys, every pass writes key + index,
         # later passes read both
-        "sort": n * 8 + n * (8 + 12) + (passes - 1) * n * 24 + passes * 4 * 256 * tiles,
+        "sort": n * 8 + n * (8 + 12) + (passes - 1) * n * 24 + passes * 4 * 512 * tiles,
         # nodes: keys in, flags, children, parent, ranges and wide-node ids out; leaves: index,
         # rel in, sorted pos + vel and the leaf box out, body state per body; refit: links and
         # the node's two child boxes in, its box out
@@ -173,7 +180,7 @@ def make_scene(workload: str):
     from diploma_thesis_b200 import scenes
     if workload == "pile":
         return scenes.config2(0), ("plain large pile: 2,097,152 particles, 32,768 bodies x 64 "
-                                   "(cubes/rods/spheres), r=1/512, box 1x3x1, grid 256^3 "
+                                   "(cubes/rods/spheres), r=1/512, box 1x3x1, grid 256x512x256 "
                                    "wrapped, dt=1e-4, k=5e4")
     if workload == "plain":
         return scenes.config0(0), ("plain single scene: 110,592 particles, 4,096 cubes x 27, "
@@ -386,7 +393,7 @@ def run_ours(args):
 
     scene, desc = make_scene(args.workload)
     if args.broadphase == "bvh":
-        desc = desc.replace("grid 256^3 wrapped", "BVH").replace("grid 128^3", "BVH")
+        desc = desc.replace("grid 256x512x256 wrapped", "BVH").replace("grid 128^3", "BVH")
     ctx = api.Context(local)
     gs = api.GpuScene(ctx, scene, broadphase=args.broadphase)
     n, nb = scene.num_particles, scene.num_bodies
@@ -417,7 +424,7 @@ def run_ours(args):
         prof_steps = max(5, min(args.steps, 50))
         stage_ms = gs.profile(prof_steps, stream=stream)
     sv = gs.step_view()
-    passes = (sv.key_bits + 7) // 8
+    passes = sort_passes(sv.key_bits)
     if args.broadphase == "bvh":
         names = BVH_STAGES
         sbytes = stage_bytes_bvh(n, nb, passes)
@@ -425,7 +432,7 @@ def run_ours(args):
         names = STAGES
         keys = api.device_view(sv.sorted_keys, n, torch.int32)
         occupied = int((keys[1:] != keys[:-1]).sum().item()) + 1
-        sbytes = stage_bytes(n, nb, passes, occupied)
+        sbytes = stage_bytes(n, nb, passes, occupied, int(sv.num_cells))
     hbm, peak_kind = peaks()
     dom = max(range(len(names)), key=lambda i: stage_ms[i])
     dom_name = names[dom]
@@ -671,7 +678,7 @@ def run_lbvh(args):
                     ok = bool((skeys[1:] >= skeys[:-1]).all().item())
                 med = {k: float(np.median(v)) for k, v in times.items()}
                 total = sum(med.values())
-                by = lbvh_bytes(kb, (bits + 7) // 8)
+                by = lbvh_bytes(kb, sort_passes(bits))
                 rows.append({
                     "n": n, "dist": dist, "bits": bits, "ms": med, "total_ms": total,
                     "mpoints_per_s": n / total / 1e3,
@@ -708,7 +715,8 @@ def run_lbvh(args):
                                    "with 5% duplicates, 30/63-bit Morton",
                        "headline": {k: head[k] for k in ("n", "dist", "bits")}},
             "peak_gbs": hbm, "peak_kind": f"{peak_kind} hbm_gbs",
-            "bytes_per_point": {"30": lbvh_bytes(4, 4), "63": lbvh_bytes(8, 8)},
+            "bytes_per_point": {"30": lbvh_bytes(4, sort_passes(30)),
+                                "63": lbvh_bytes(8, sort_passes(63))},
             "cpu_baseline": cpu_baseline, "rows": rows}
     print(json.dumps(line))
     return 0

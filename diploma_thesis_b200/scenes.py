@@ -185,7 +185,10 @@ def config2(seed: int = 0, num_bodies: int = 32768) -> Scene:
     voxelised spheres padded to 64), r = 1/512, dropped from heights in [0.5, 2] into the box
     [0,1] x [0,3] x [0,1] (y up).  Bodies are laid out in horizontal layers: rod layers (rods
     along x or z, alternating) and block layers (cubes and spheres, random orientations),
-    interleaved from y = 0.5 upward, each body jittered inside its slot."""
+    interleaved from y = 0.5 upward, each body jittered inside its slot.  Grid: cell 2r,
+    256 x 512 x 256 wrapped cells (25-bit keys), so y in [0, 2) -- the whole pile -- maps to
+    distinct cells; a 256^3 grid would fold y = 1 .. 1.8 onto y = 0 .. 0.8 and make the
+    gather visit the folded occupants."""
     rng = np.random.default_rng(seed)
     r = 1.0 / 512
     sp = 2 * r
@@ -243,7 +246,7 @@ def config2(seed: int = 0, num_bodies: int = 32768) -> Scene:
         shapes.append([cube, rod, sph][kinds[b]])
     scene = _assemble(shapes, np.array(centres), np.array(quats),
                       rng.normal(0.0, 0.1, (num_bodies, 3)), r, (0, 0, 0), (1, 3, 1),
-                      name="plain large pile: 32768 bodies x 64")
+                      grid_log2=(8, 9, 8), name="plain large pile: 32768 bodies x 64")
     scene.extra["top"] = float(y)
     return scene
 

@@ -132,7 +132,7 @@ AR_API ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in,
  * For callers that cannot allocate device memory: a frame loop that must never stall on
  * cudaMalloc's implicit device synchronisation, code running while another component owns
  * the device memory pool, or a process whose device-memory budget is fixed at start-up.
- * The workspace is a static array inside libarsim.so (about 9 MiB, held by every GPU that
+ * The workspace is a static array inside libarsim.so (about 10 MiB, held by every GPU that
  * loads the library until the process exits), so n is limited to 1,048,576 pairs; larger n
  * returns AR_ERR_INVALID_ARG.  No context is needed and nothing is allocated: the caller
  * passes inputs and outputs, plus an optional device int (d_status, may be NULL) into which
