@@ -55,6 +55,13 @@ __device__ __forceinline__ void raise_error(int* err, int bits) {
   if (err) atomicOr(err, bits);
 }
 
+// Programmatic dependent launch: a kernel started with arh::launch_pdl may begin while the
+// kernel before it on the stream is still finishing, so it calls pdl_wait() before it reads
+// or writes anything that kernel (or earlier work) touches; the wait returns once the
+// previous kernel has completed and its writes are visible.  In a kernel launched the
+// ordinary way it returns at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 }  // namespace ar
 
 // ---- host-side helpers ---------------------------------------------------------------------
@@ -66,6 +73,26 @@ inline unsigned grid_for(long n, int block) {
   long g = (n + block - 1) / block;
   return (unsigned)(g < 1 ? 1 : g);
 }
+#ifdef __CUDACC__
+// Launch with programmatic stream serialisation: the kernel's blocks may be scheduled as the
+// previous kernel's blocks retire (its launch latency overlaps that kernel's tail); the
+// kernel must call ar::pdl_wait() before touching shared state.
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                       cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr{};
+  attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr.val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+#endif
 }  // namespace arh
 
 // Context: one per device.  Owns the device error word and a grow-only scratch arena that

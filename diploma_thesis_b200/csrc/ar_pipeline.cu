@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(256) step_clear_kernel(uint4* __restrict__ hea
                                                          uint2* __restrict__ cells,
                                                          unsigned long long num_cells,
                                                          const long long* __restrict__ d_step) {
+  ar::pdl_wait();
   const long stride = (long)gridDim.x * blockDim.x;
   const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
   for (long i = t; i < head16; i += stride) head[i] = make_uint4(0u, 0u, 0u, 0u);
@@ -107,6 +108,7 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
     uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, ar_sort::Plan plan,
     long long* __restrict__ d_step) {
+  ar::pdl_wait();
   __shared__ uint32_t s_hist[ar_sort::kMaxPasses][ar_sort::kMaxRadix];
   if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
   for (int i = threadIdx.x; i < plan.passes * ar_sort::kMaxRadix; i += blockDim.x)
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(
     const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
     uint2* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
     const long long* __restrict__ d_step) {
+  ar::pdl_wait();
   const uint32_t epoch = cell_epoch(*d_step) << kEpochShift;
   const int stride = gridDim.x * blockDim.x;
   for (int k0 = blockIdx.x * blockDim.x + threadIdx.x; k0 < nt; k0 += stride * kScatterBatch) {
@@ -254,6 +257,7 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
     const uint32_t* __restrict__ svals, const uint2* __restrict__ cells,
     const float4* __restrict__ spos, const float4* __restrict__ svel,
     float4* __restrict__ pforce, const long long* __restrict__ d_step) {
+  ar::pdl_wait();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
   const uint32_t epoch = cell_epoch(*d_step);
@@ -368,6 +372,7 @@ __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restr
                                                          const int* __restrict__ pscene, int ns,
                                                          int nt, uint64_t* __restrict__ keys,
                                                          long long* __restrict__ d_step) {
+  ar::pdl_wait();
   if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
     const int s = __ldg(pscene + g);
@@ -408,6 +413,7 @@ __global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp,
                                                         int32_t* __restrict__ min_r,
                                                         int32_t* __restrict__ max_r,
                                                         WideNode* __restrict__ nodes) {
+  ar::pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) parent[n] = -1;
   if (i >= n - 1) return;
@@ -429,6 +435,7 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
     const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
     WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
     int32_t* __restrict__ max_r) {
+  ar::pdl_wait();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const int g = (int)__ldg(svals + k);
     const int sc = __ldg(pscene + g);
@@ -461,6 +468,7 @@ __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
                                  const int32_t* __restrict__ parent,
                                  const int32_t* __restrict__ min_r,
                                  const int32_t* __restrict__ max_r, int32_t* __restrict__ roots) {
+  ar::pdl_wait();
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= ns) return;
   const int lo = poff[s], hi = poff[s + 1] - 1;
@@ -493,6 +501,7 @@ __global__ void __launch_bounds__(256) bvh_refit_kernel(int n, const int32_t* __
                                                         const int32_t* __restrict__ parent,
                                                         WideNode* nodes,
                                                         int* __restrict__ counters) {
+  ar::pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || n < 2) return;
   auto children = [&](int node, ar_lbvh::Box6* a, ar_lbvh::Box6* b) {
@@ -523,6 +532,7 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
     const uint32_t* __restrict__ svals, const float4* __restrict__ spos,
     const float4* __restrict__ svel, const WideNode* __restrict__ nodes,
     const int32_t* __restrict__ roots, float4* __restrict__ pforce, int* __restrict__ err) {
+  ar::pdl_wait();
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
   const float4 p4 = __ldg(spos + k);
@@ -589,6 +599,7 @@ __global__ void __launch_bounds__(256) body_step_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
     const float4* __restrict__ pforce, const long long* __restrict__ d_step,
     int* __restrict__ err) {
+  ar::pdl_wait();
   const int warps = (gridDim.x * blockDim.x) >> 5;
   const int lane = ar::lane_id();
   const long long step = *d_step;
@@ -626,6 +637,7 @@ __global__ void __launch_bounds__(256) body_step_kernel(
 __global__ void __launch_bounds__(256) integrate_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
     const long long* __restrict__ d_step, int* __restrict__ err) {
+  ar::pdl_wait();
   const long long step = *d_step;
   for (int gb = blockIdx.x * blockDim.x + threadIdx.x; gb < bt; gb += gridDim.x * blockDim.x) {
     const SceneDev& S = table[__ldg(bscene + gb)];
@@ -953,59 +965,54 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   if (B->broadphase == AR_BROADPHASE_BVH) {
     cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);  // refit arrival counters
     mark(1);
-    morton_key_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->keys64,
-                                          B->d_step);
+    arh::launch_pdl(morton_key_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, ns, nt,
+        B->keys64, B->d_step);
     mark(2);
     ar_status s = ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
                                     B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
     if (s != AR_OK) return s;
     mark(3);
-    bvh_build_kernel<<<arh::grid_for(std::max(nt - 1, 1), 256), 256, 0, st>>>(
-        ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
+    arh::launch_pdl(bvh_build_kernel, dim3(arh::grid_for(std::max(nt - 1, 1), 256)), dim3(256), 0,
+        st, ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
         B->right, B->parent, B->min_r, B->max_r, B->nodes);
-    bvh_leaves_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, ns, nt, B->svals, B->left,
-                                          B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
-                                          B->min_r, B->max_r);
-    bvh_roots_kernel<<<arh::grid_for(ns, 128), 128, 0, st>>>(B->d_poff, ns, nt, B->parent,
-                                                              B->min_r, B->max_r, B->roots);
-    bvh_refit_kernel<<<arh::grid_for(nt, 256), 256, 0, st>>>(nt, B->left, B->parent, B->nodes,
-                                                              B->counters);
+    arh::launch_pdl(bvh_leaves_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, ns, nt,
+        B->svals, B->left, B->parent, B->spos, B->svel, B->nodes, B->is_leaf, B->min_r, B->max_r);
+    arh::launch_pdl(bvh_roots_kernel, dim3(arh::grid_for(ns, 128)), dim3(128), 0, st, B->d_poff, ns,
+        nt, B->parent, B->min_r, B->max_r, B->roots);
+    arh::launch_pdl(bvh_refit_kernel, dim3(arh::grid_for(nt, 256)), dim3(256), 0, st, nt, B->left,
+        B->parent, B->nodes, B->counters);
     mark(4);
-    bvh_collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(
-        B->d_table, B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots,
-        B->pforce, ctx->d_err);
+    arh::launch_pdl(bvh_collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), 0, st, B->d_table,
+        B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots, B->pforce, ctx->d_err);
     mark(5);
-    body_step_kernel<<<g5, 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->pforce, B->d_step,
-                                         ctx->d_err);
-    integrate_kernel<<<arh::grid_for(bt, 256), 256, 0, st>>>(B->d_table, B->d_bscene, bt,
-                                                             B->d_step, ctx->d_err);
+    arh::launch_pdl(body_step_kernel, dim3(g5), dim3(256), 0, st, B->d_table, B->d_bscene, bt,
+        B->pforce, B->d_step, ctx->d_err);
+    arh::launch_pdl(integrate_kernel, dim3(arh::grid_for(bt, 256)), dim3(256), 0, st, B->d_table,
+        B->d_bscene, bt, B->d_step, ctx->d_err);
     mark(6);
     return arh::check_launch("step (BVH)");
   }
-  step_clear_kernel<<<ctx->num_sms * 2, 256, 0, st>>>(
-      (uint4*)B->sort_ws, (long)(ar_sort::clear_bytes(nt, B->plan.passes) / 16), B->cells,
-      B->cap_cells, B->d_step);
+  arh::launch_pdl(step_clear_kernel, dim3(ctx->num_sms * 2), dim3(256), 0, st, (uint4*)B->sort_ws,
+      (long)(ar_sort::clear_bytes(nt, B->plan.passes) / 16), B->cells, B->cap_cells, B->d_step);
   mark(1);
-  grid_keys_kernel<<<std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4),
-                     kK1Threads, 0, st>>>(B->d_table, B->d_pscene, nt, B->keys,
-                                          (uint32_t*)B->sort_ws, B->plan,
-                                          B->d_step);
+  arh::launch_pdl(grid_keys_kernel,
+      dim3(std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4)), dim3(kK1Threads),
+      0, st, B->d_table, B->d_pscene, nt, B->keys, (uint32_t*)B->sort_ws, B->plan, B->d_step);
   mark(2);
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
                                   st, B->sort_ws, B->cap_sort, true);
   if (s != AR_OK) return s;
   mark(3);
-  scatter_kernel<<<gp, 256, 0, st>>>(B->d_table, B->d_pscene, nt, B->skeys, B->svals,
-                                     B->cells, B->spos, B->svel, B->d_step);
+  arh::launch_pdl(scatter_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, nt, B->skeys,
+      B->svals, B->cells, B->spos, B->svel, B->d_step);
   mark(4);
-  collide_kernel<<<arh::grid_for(nt, bs), bs, 0, st>>>(B->d_table, nt, B->skeys, B->svals,
-                                                       B->cells, B->spos, B->svel, B->pforce,
-                                                       B->d_step);
+  arh::launch_pdl(collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), 0, st, B->d_table, nt,
+      B->skeys, B->svals, B->cells, B->spos, B->svel, B->pforce, B->d_step);
   mark(5);
-  body_step_kernel<<<g5, 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->pforce, B->d_step,
-                                       ctx->d_err);
-  integrate_kernel<<<arh::grid_for(bt, 256), 256, 0, st>>>(B->d_table, B->d_bscene, bt, B->d_step,
-                                                           ctx->d_err);
+  arh::launch_pdl(body_step_kernel, dim3(g5), dim3(256), 0, st, B->d_table, B->d_bscene, bt,
+      B->pforce, B->d_step, ctx->d_err);
+  arh::launch_pdl(integrate_kernel, dim3(arh::grid_for(bt, 256)), dim3(256), 0, st, B->d_table,
+      B->d_bscene, bt, B->d_step, ctx->d_err);
   mark(6);
   return arh::check_launch("step");
 }

@@ -46,6 +46,7 @@ template <class K>
 __global__ void __launch_bounds__(kThreads) hist_kernel(const K* __restrict__ keys, int n,
                                                        ar_sort::Plan plan,
                                                        uint32_t* __restrict__ hist) {
+  ar::pdl_wait();
   __shared__ uint32_t s_hist[ar_sort::kMaxPasses][kRadix];
   const int passes = plan.passes;
   for (int i = threadIdx.x; i < passes * kRadix; i += kThreads) (&s_hist[0][0])[i] = 0;
@@ -64,6 +65,7 @@ __global__ void __launch_bounds__(kThreads) hist_kernel(const K* __restrict__ ke
 
 // Exclusive scan of each pass's histogram (kRadix bins; one warp per pass).
 __global__ void hist_scan_kernel(uint32_t* __restrict__ hist, int passes) {
+  ar::pdl_wait();
   int p = threadIdx.x >> 5;
   if (p >= passes) return;
   uint32_t* h = hist + p * kRadix;
@@ -99,6 +101,7 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
     uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     const uint32_t* __restrict__ digit_base, uint32_t* __restrict__ status,
     uint32_t* __restrict__ tile_counter, int* __restrict__ err) {
+  ar::pdl_wait();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kWarps = kT / 32;
   constexpr int kTile = kT * kItems;
@@ -287,14 +290,17 @@ void launch_passes(const ar_sort::Plan& plan, int n, const K* keys_in, const uin
     const uint32_t* base = hist + p * kRadix;
     uint32_t* stat = status + (size_t)p * status_tiles * kRadix;
     if (bits > 8)
-      onesweep_kernel<K, 512, 9><<<tiles, 512, sizeof(PassSmem<K, 512, 9>), st>>>(
-          src_k, src_v, dk, dv, n, shift, bits, base, stat, counters + p, err);
+      arh::launch_pdl(onesweep_kernel<K, 512, 9>, dim3(tiles), dim3(512),
+          sizeof(PassSmem<K, 512, 9>), st, src_k, src_v, dk, dv, n, shift, bits, base, stat,
+          counters + p, err);
     else if (kt == 512)
-      onesweep_kernel<K, 512, 8><<<tiles, 512, sizeof(PassSmem<K, 512, 8>), st>>>(
-          src_k, src_v, dk, dv, n, shift, bits, base, stat, counters + p, err);
+      arh::launch_pdl(onesweep_kernel<K, 512, 8>, dim3(tiles), dim3(512),
+          sizeof(PassSmem<K, 512, 8>), st, src_k, src_v, dk, dv, n, shift, bits, base, stat,
+          counters + p, err);
     else
-      onesweep_kernel<K, 256, 8><<<tiles, 256, sizeof(PassSmem<K, 256, 8>), st>>>(
-          src_k, src_v, dk, dv, n, shift, bits, base, stat, counters + p, err);
+      arh::launch_pdl(onesweep_kernel<K, 256, 8>, dim3(tiles), dim3(256),
+          sizeof(PassSmem<K, 256, 8>), st, src_k, src_v, dk, dv, n, shift, bits, base, stat,
+          counters + p, err);
     src_k = dk;
     src_v = dv;
   }
@@ -328,9 +334,9 @@ ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* k
     unsigned cap = (unsigned)(ctx ? ctx->num_sms : 148) * 4;
     if (hgrid > cap) hgrid = cap;
     if (hgrid < 1) hgrid = 1;
-    hist_kernel<K><<<hgrid, kThreads, 0, st>>>(keys_in, n, plan, hist);
+    arh::launch_pdl(hist_kernel<K>, dim3(hgrid), dim3(kThreads), 0, st, keys_in, n, plan, hist);
   }
-  hist_scan_kernel<<<1, 32 * ar_sort::kMaxPasses, 0, st>>>(hist, passes);
+  arh::launch_pdl(hist_scan_kernel, dim3(1), dim3(32 * ar_sort::kMaxPasses), 0, st, hist, passes);
   launch_passes<K>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
                    status, counters, err, st);
   return arh::check_launch("radix sort");
@@ -561,8 +567,9 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
   unsigned hgrid = (unsigned)((n + kThreads * 8 - 1) / (kThreads * 8));
   if (hgrid > (unsigned)sms * 4) hgrid = (unsigned)sms * 4;
   if (hgrid < 1) hgrid = 1;
-  hist_kernel<uint32_t><<<hgrid, kThreads, 0, st>>>(keys_in, n, plan, hist);
-  hist_scan_kernel<<<1, 32 * ar_sort::kMaxPasses, 0, st>>>(hist, passes);
+  arh::launch_pdl(hist_kernel<uint32_t>, dim3(hgrid), dim3(kThreads), 0, st, keys_in, n, plan,
+      hist);
+  arh::launch_pdl(hist_scan_kernel, dim3(1), dim3(32 * ar_sort::kMaxPasses), 0, st, hist, passes);
   launch_passes<uint32_t>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
                           status, counters, (int*)d_status, st);
   return arh::check_launch("allocation-free sort");
