@@ -385,11 +385,14 @@ __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restr
   }
 }
 
-// Internal node i (global id n + i) of the fused BVH holds both children's boxes and ids, so
-// one 64-byte fetch decides a traversal step:
-//   c[0] = left box (lo.x, lo.y, lo.z, hi.x)    c[1] = (hi.y, hi.z, left id, parent id)
-//   c[2] = right box (lo.x, lo.y, lo.z, hi.x)   c[3] = (hi.y, hi.z, right id, 0)
-// Ids < n are leaves (sorted particle slots); the root's parent id is -1.
+// Internal node i (global id n + i) of the fused BVH holds both children's boxes, ids and body
+// tags, so one 64-byte fetch decides a traversal step:
+//   c[0] = left box (lo.x, lo.y, lo.z, hi.x)    c[1] = (hi.y, hi.z, left id, left tag)
+//   c[2] = right box (lo.x, lo.y, lo.z, hi.x)   c[3] = (hi.y, hi.z, right id, right tag)
+// Ids < n are leaves (sorted particle slots).  A child's tag is the global body id when every
+// leaf below it belongs to that body, else -1: a particle skips a child that holds only its
+// own body's particles without descending (they could only be rejected), which leaves the
+// order of everything it does visit unchanged.
 struct __align__(64) WideNode {
   float4 c[4];
 };
@@ -397,12 +400,12 @@ struct __align__(64) WideNode {
 __device__ __forceinline__ int* node_ints(WideNode* nodes, int internal) {
   return reinterpret_cast<int*>(nodes + internal);
 }
-// Box of child `side` (0 left, 1 right) into the parent's slot, ids untouched.
-__device__ __forceinline__ void put_child_box(WideNode* nodes, int internal, int side, float4 lo,
-                                              float2 hi_yz) {
+// Box, id and body tag of child `side` (0 left, 1 right) into the parent's slot.
+__device__ __forceinline__ void put_child(WideNode* nodes, int internal, int side, float4 lo,
+                                          float2 hi_yz, int id, int tag) {
   float4* c = nodes[internal].c + 2 * side;
   __stcg(c, lo);
-  __stcg(reinterpret_cast<float2*>(c + 1), hi_yz);
+  __stcg(c + 1, make_float4(hi_yz.x, hi_yz.y, __int_as_float(id), __int_as_float(tag)));
 }
 
 __global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp, int n,
@@ -417,14 +420,7 @@ __global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) parent[n] = -1;
   if (i >= n - 1) return;
-  const int2 ch = ar_lbvh::karras_node(i, n, lcp, is_leaf, left, right, parent, min_r, max_r);
-  int* w = node_ints(nodes, i);
-  w[6] = ch.x;
-  w[14] = ch.y;
-  w[15] = 0;
-  if (i == 0) w[7] = -1;
-  if (ch.x >= n) node_ints(nodes, ch.x - n)[7] = n + i;
-  if (ch.y >= n) node_ints(nodes, ch.y - n)[7] = n + i;
+  ar_lbvh::karras_node(i, n, lcp, is_leaf, left, right, parent, min_r, max_r);
 }
 
 // Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
@@ -450,9 +446,9 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
     if (nt >= 2) {
       const float rr = S.r;
       const int pn = __ldg(parent + k);
-      put_child_box(nodes, pn - nt, __ldg(left + pn) == k ? 0 : 1,
-                    make_float4(p.x - rr, p.y - rr, p.z - rr, p.x + rr),
-                    make_float2(p.y + rr, p.z + rr));
+      put_child(nodes, pn - nt, __ldg(left + pn) == k ? 0 : 1,
+                make_float4(p.x - rr, p.y - rr, p.z - rr, p.x + rr), make_float2(p.y + rr, p.z + rr),
+                k, S.boff + b);
     }
     is_leaf[k] = 1;
     min_r[k] = k;
@@ -513,8 +509,12 @@ __global__ void __launch_bounds__(256) bvh_refit_kernel(int n, const int32_t* __
   auto store = [&](int node, const ar_lbvh::Box6& m) {
     if (node == n) return;  // the root's box is not stored anywhere
     const int pn = __ldg(parent + node);
-    put_child_box(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1,
-                  make_float4(m.lx, m.ly, m.lz, m.hx), make_float2(m.hy, m.hz));
+    // both children have arrived, so their tags are visible like their boxes
+    const int* w = node_ints(nodes, node - n);
+    const int tl = __ldcg(w + 7), tr = __ldcg(w + 15);
+    put_child(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1,
+              make_float4(m.lx, m.ly, m.lz, m.hx), make_float2(m.hy, m.hz), node,
+              tl == tr ? tl : -1);
   };
   ar_lbvh::refit_climb(i, n, parent, counters, children, store);
 }
@@ -567,8 +567,11 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
       const float4* c = nodes[node - nt].c;
       const float4 a0 = __ldg(c), a1 = __ldg(c + 1), b0 = __ldg(c + 2), b1 = __ldg(c + 3);
       const int lc = __float_as_int(a1.z), rc = __float_as_int(b1.z);
-      const bool ol = lc != k && ar_lbvh::overlap(q, ar_lbvh::Box{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y});
-      const bool orr = rc != k && ar_lbvh::overlap(q, ar_lbvh::Box{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y});
+      // a child holding only this particle's body (this particle's own leaf included) is skipped
+      const bool ol = __float_as_int(a1.w) != body &&
+                      ar_lbvh::overlap(q, ar_lbvh::Box{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y});
+      const bool orr = __float_as_int(b1.w) != body &&
+                       ar_lbvh::overlap(q, ar_lbvh::Box{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y});
       const bool ll = lc < nt, rl = rc < nt;
       if (ol && ll) visit(lc);
       if (orr && rl) visit(rc);

@@ -492,9 +492,10 @@ AR_API ar_status ar_scene_grid_info(ar_scene* scene, float origin[3], float cell
  * body, else 0).  Grid keys are uint32 cell keys
  * (key_bytes 4); BVH keys are uint64 Morton codes (key_bytes 8), and the BVH view adds the
  * tree (leaf i at i, internal node i at N + i, root N) and tree_nodes16: 16 floats per
- * internal node holding both children's boxes and ids -- left lo.xyz, hi.x | hi.y, hi.z,
- * left id, parent id | right lo.xyz, hi.x | hi.y, hi.z, right id, 0 (ids as int bits; the
- * root's parent id is -1).  Tree pointers are NULL for the grid, cells2 NULL for the BVH. */
+ * internal node holding both children's boxes, ids and body tags -- left lo.xyz, hi.x |
+ * hi.y, hi.z, left id, left tag | right lo.xyz, hi.x | hi.y, hi.z, right id, right tag (ids
+ * and tags as int bits; a tag is the global body id when every leaf below that child belongs
+ * to one body, else -1).  Tree pointers are NULL for the grid, cells2 NULL for the BVH. */
 typedef struct ar_step_view {
   int num_particles;
   uint64_t num_cells;
