@@ -49,6 +49,22 @@ struct Lcp64Scene {
   }
 };
 
+// The same for 32-bit keys (scene index above the 30-bit code, at most 4 scenes).  Its
+// values are those of Lcp64Scene minus 32 for the same keys, so the topology is the same.
+struct Lcp32Scene {
+  const uint32_t* __restrict__ c;
+  int n;
+  const int* __restrict__ poff;
+  int shift;
+  __device__ __forceinline__ int operator()(int i, int j) const {
+    if (j < 0 || j >= n) return -1;
+    const uint32_t a = __ldg(c + i), b = __ldg(c + j);
+    if (a != b) return __clz(a ^ b);
+    const int base = __ldg(poff + (int)(a >> shift));
+    return __clz((i - base) ^ (j - base)) + 32;
+  }
+};
+
 // ---- Karras 2012 internal node i (kernelConstructRadixTreeSoA, BVHSoAKernels.cu:7-99) ----
 // Returns the node's (left, right) child ids.
 template <class Lcp>

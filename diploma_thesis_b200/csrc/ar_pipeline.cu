@@ -368,9 +368,10 @@ __device__ __forceinline__ uint64_t morton_key(const SceneDev& S, int s, float3 
   return ((uint64_t)s << kMortonBits) | code;
 }
 
+template <class K>
 __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restrict__ table,
                                                          const int* __restrict__ pscene, int ns,
-                                                         int nt, uint64_t* __restrict__ keys,
+                                                         int nt, K* __restrict__ keys,
                                                          long long* __restrict__ d_step) {
   ar::pdl_wait();
   if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
@@ -381,7 +382,7 @@ __global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restr
     const int b = __float_as_int(r4.w);
     const float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
     const float3 p = ar::add(ar::xyz(__ldg(S.pos + b)), r);
-    keys[g] = morton_key(S, s, p);
+    keys[g] = (K)morton_key(S, s, p);
   }
 }
 
@@ -408,7 +409,8 @@ __device__ __forceinline__ void put_child(WideNode* nodes, int internal, int sid
   __stcg(c + 1, make_float4(hi_yz.x, hi_yz.y, __int_as_float(id), __int_as_float(tag)));
 }
 
-__global__ void __launch_bounds__(256) bvh_build_kernel(ar_lbvh::Lcp64Scene lcp, int n,
+template <class Lcp>
+__global__ void __launch_bounds__(256) bvh_build_kernel(Lcp lcp, int n,
                                                         uint8_t* __restrict__ is_leaf,
                                                         int32_t* __restrict__ left,
                                                         int32_t* __restrict__ right,
@@ -968,16 +970,30 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   if (B->broadphase == AR_BROADPHASE_BVH) {
     cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);  // refit arrival counters
     mark(1);
-    arh::launch_pdl(morton_key_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, ns, nt,
-        B->keys64, B->d_step);
+    // keys of at most 32 bits (up to 4 scenes) are sorted as uint32: half the bytes per pass
+    const bool k32 = B->bvh_key_bits <= 32;
+    if (k32)
+      arh::launch_pdl(morton_key_kernel<uint32_t>, dim3(gp), dim3(256), 0, st, B->d_table,
+          B->d_pscene, ns, nt, B->keys, B->d_step);
+    else
+      arh::launch_pdl(morton_key_kernel<uint64_t>, dim3(gp), dim3(256), 0, st, B->d_table,
+          B->d_pscene, ns, nt, B->keys64, B->d_step);
     mark(2);
-    ar_status s = ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
-                                    B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
+    ar_status s = k32 ? ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0,
+                                          B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64)
+                      : ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
+                                          B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
     if (s != AR_OK) return s;
     mark(3);
-    arh::launch_pdl(bvh_build_kernel, dim3(arh::grid_for(std::max(nt - 1, 1), 256)), dim3(256), 0,
-        st, ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
-        B->right, B->parent, B->min_r, B->max_r, B->nodes);
+    const dim3 gb(arh::grid_for(std::max(nt - 1, 1), 256));
+    if (k32)
+      arh::launch_pdl(bvh_build_kernel<ar_lbvh::Lcp32Scene>, gb, dim3(256), 0, st,
+          ar_lbvh::Lcp32Scene{B->skeys, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
+          B->right, B->parent, B->min_r, B->max_r, B->nodes);
+    else
+      arh::launch_pdl(bvh_build_kernel<ar_lbvh::Lcp64Scene>, gb, dim3(256), 0, st,
+          ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
+          B->right, B->parent, B->min_r, B->max_r, B->nodes);
     arh::launch_pdl(bvh_leaves_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, ns, nt,
         B->svals, B->left, B->parent, B->spos, B->svel, B->nodes, B->is_leaf, B->min_r, B->max_r);
     arh::launch_pdl(bvh_roots_kernel, dim3(arh::grid_for(ns, 128)), dim3(128), 0, st, B->d_poff, ns,
@@ -1372,13 +1388,14 @@ ar_status ar_scene_step_view(ar_scene* s, ar_step_view* v) {
   v->num_particles = (int)B->nt;
   v->num_cells = bvh ? 0 : B->total_cells;
   v->key_bits = bvh ? B->bvh_key_bits : B->key_bits;
-  v->sorted_keys = bvh ? (uint32_t*)B->skeys64 : B->skeys;
+  const bool k64 = bvh && B->bvh_key_bits > 32;
+  v->sorted_keys = k64 ? (uint32_t*)B->skeys64 : B->skeys;
   v->sorted_idx = B->svals;
   v->sorted_pos4 = (float*)B->spos;
   v->sorted_vel4 = (float*)B->svel;
   v->particle_force4 = (float*)B->pforce;
   v->cells2 = bvh ? nullptr : (uint32_t*)B->cells;
-  v->key_bytes = bvh ? 8 : 4;
+  v->key_bytes = k64 ? 8 : 4;
   v->broadphase = B->broadphase;
   v->tree_left = bvh ? B->left : nullptr;
   v->tree_right = bvh ? B->right : nullptr;

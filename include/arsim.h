@@ -490,7 +490,9 @@ AR_API ar_status ar_scene_grid_info(ar_scene* scene, float origin[3], float cell
  * or more) | step epoch (bits 5-12: the step number mod 255, plus 1; any other value marks an
  * empty cell) | body tag (bits 13-31: scene-local body + 1 when every occupant belongs to that
  * body, else 0).  Grid keys are uint32 cell keys
- * (key_bytes 4); BVH keys are uint64 Morton codes (key_bytes 8), and the BVH view adds the
+ * (key_bytes 4); BVH keys are the scene index above a 30-bit Morton code, uint32 when they
+ * fit in 32 bits (at most 4 scenes; key_bytes 4) and uint64 otherwise (key_bytes 8), and the
+ * BVH view adds the
  * tree (leaf i at i, internal node i at N + i, root N) and tree_nodes16: 16 floats per
  * internal node holding both children's boxes, ids and body tags -- left lo.xyz, hi.x |
  * hi.y, hi.z, left id, left tag | right lo.xyz, hi.x | hi.y, hi.z, right id, right tag (ids

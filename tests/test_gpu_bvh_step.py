@@ -1,5 +1,5 @@
-"""The fused step with the BVH broad phase (Morton keys -> 64-bit onesweep sort -> Karras tree
--> refit -> stackless walk) against the oracle's float32 restatement (bit-exact), batched
+"""The fused step with the BVH broad phase (Morton keys -> onesweep sort of 32-bit keys, or
+64-bit keys for more than 4 scenes -> Karras tree -> refit -> stackless walk) against the oracle's float32 restatement (bit-exact), batched
 against solo, and against the grid broad phase (same contacts, forces within 1e-5 relative)."""
 import numpy as np
 import pytest
@@ -12,11 +12,21 @@ from oracle import cpu
 pytestmark = pytest.mark.gpu
 
 
+def _keys(v) -> np.ndarray:
+    """Sorted BVH keys as uint64 (32-bit keys when they fit, at most 4 scenes)."""
+    n = v.num_particles
+    assert v.key_bytes == (4 if v.key_bits <= 32 else 8)
+    if v.key_bytes == 4:
+        k = api.device_view(v.sorted_keys, n, torch.int32).cpu().numpy().view(np.uint32)
+        return k.astype(np.uint64)
+    return api.device_view(v.sorted_keys, 2 * n, torch.int32).cpu().numpy().view(np.uint64)
+
+
 def _view(gs: api.GpuScene):
     v = gs.step_view()
     n = v.num_particles
-    assert v.key_bytes == 8 and v.broadphase == 1 and not v.cells2
-    keys = api.device_view(v.sorted_keys, 2 * n, torch.int32).cpu().numpy().view(np.uint64)
+    assert v.broadphase == 1 and not v.cells2
+    keys = _keys(v)
     idx = api.device_view(v.sorted_idx, n, torch.int32).cpu().numpy().view(np.uint32)
     pf = api.device_view(v.particle_force4, 4 * n, torch.float32).cpu().numpy().reshape(n, 4)
     return keys, idx, pf
@@ -47,7 +57,7 @@ def test_bvh_tree_matches_oracle_radix_tree(ctx):
     ctx.check()
     v = gs.step_view()
     n = v.num_particles
-    keys = api.device_view(v.sorted_keys, 2 * n, torch.int32).cpu().numpy().view(np.uint64)
+    keys = _keys(v)
     left = api.device_view(v.tree_left, 2 * n, torch.int32).cpu().numpy()
     right = api.device_view(v.tree_right, 2 * n, torch.int32).cpu().numpy()
     parent = api.device_view(v.tree_parent, 2 * n, torch.int32).cpu().numpy()
@@ -77,9 +87,10 @@ def test_bvh_hundred_steps_bit_exact_graph_and_eager(ctx):
     b.close()
 
 
-def test_bvh_batch_equals_solo_bit_for_bit(ctx):
+@pytest.mark.parametrize("sides", [(3, 5, 2, 4, 1, 4), (3, 2, 4)])  # 64- and 32-bit keys
+def test_bvh_batch_equals_solo_bit_for_bit(ctx, sides):
     group = []
-    for i, side in enumerate((3, 5, 2, 4, 1, 4)):
+    for i, side in enumerate(sides):
         sc = scenes.small_scene(i + 20, nb_side=side, packed=(i % 2 == 0), r=1 / 128)
         group.append(sc)
     solo = [api.GpuScene(ctx, sc, broadphase="bvh") for sc in group]
