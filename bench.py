@@ -443,18 +443,19 @@ def run_ours(args):
 
     # ---- end to end: host state in, step, host state out, every step ----
     e2e_steps = max(3, min(args.steps, 100))
-    pinned = {k: torch.empty((nb, 4), dtype=torch.float32).pin_memory() for k in
-              ("pos", "quat", "vel", "angvel")}
-    host = {k: v.numpy() for k, v in pinned.items()}
-    gs.download_into(host["pos"], host["quat"], host["vel"], host["angvel"], stream=stream)
+    # body state (pos, quat, vel, angvel) in one pinned host array; each step uploads it,
+    # steps, and returns only once the new state is back on the host
+    pinned = torch.empty((4, nb, 4), dtype=torch.float32).pin_memory()
+    host = pinned.numpy()
+    gs.download_state(host, stream=stream)
     with torch.cuda.stream(stream):
         barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            gs.upload(host["pos"], host["quat"], host["vel"], host["angvel"], stream=stream)
+            gs.upload_state(host, stream=stream)
             gs.step(1, use_graph=True, stream=stream)
-            gs.download_into(host["pos"], host["quat"], host["vel"], host["angvel"], stream=stream)
+            gs.download_state(host, stream=stream)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
         barrier(world)

@@ -133,6 +133,9 @@ SIGNATURES = {
     "ar_scene_download": [P, P, P, P, P, S],
     "ar_scene_download_async": [P, P, P, P, P, S],
     "ar_scene_upload": [P, P, P, P, P, S],
+    "ar_scene_upload_state": [P, P, S],
+    "ar_scene_download_state": [P, P, S],
+    "ar_scene_download_state_async": [P, P, S],
     "ar_step_profile": [P, P, I, C.POINTER(F), S],
     "ar_batch_profile": [P, P, I, C.POINTER(F), S],
     "ar_scene_get_view": [P, C.POINTER(SceneView)],

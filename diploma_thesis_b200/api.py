@@ -140,6 +140,25 @@ class GpuScene:
                                                for a in (pos, quat, vel, angvel)],
              stream_handle(stream))
 
+    def upload_state(self, state: np.ndarray, stream=None) -> None:
+        """Overwrite body state from one (preferably pinned) [4, B, 4] float32 host array:
+        pos, quat, vel, angvel; asynchronous, one copy."""
+        assert state.dtype == np.float32 and state.size == 16 * self.num_bodies
+        assert state.flags.c_contiguous
+        call("ar_scene_upload_state", self.handle, _np_ptr(state), stream_handle(stream))
+
+    def download_state(self, state: np.ndarray | None = None, stream=None,
+                       wait: bool = True) -> np.ndarray:
+        """Body state into a [4, B, 4] float32 host array (pos, quat, vel, angvel) with one
+        copy; with wait=False the copy is only queued on `stream` (pinned memory)."""
+        if state is None:
+            state = np.zeros((4, self.num_bodies, 4), np.float32)
+        assert state.dtype == np.float32 and state.size == 16 * self.num_bodies
+        assert state.flags.c_contiguous
+        call("ar_scene_download_state" if wait else "ar_scene_download_state_async", self.handle,
+             _np_ptr(state), stream_handle(stream))
+        return state
+
     def download_into(self, pos, quat, vel, angvel, stream=None) -> None:
         call("ar_scene_download", self.handle, *[_np_ptr(a) if a is not None else None
                                                  for a in (pos, quat, vel, angvel)],

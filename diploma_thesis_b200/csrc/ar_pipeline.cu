@@ -1372,6 +1372,41 @@ ar_status ar_scene_upload(ar_scene* s, const float* h_pos4, const float* h_quat4
   return arh::check_launch("ar_scene_upload");
 }
 
+// The four body-state arrays sit at a fixed pitch in the scene's block (pos, quat, vel, ang),
+// so one 2D copy moves all of them.
+static size_t state_pitch(const ar_scene* s) {
+  return (size_t)((char*)s->quat - (char*)s->pos);
+}
+
+ar_status ar_scene_upload_state(ar_scene* s, const float* h_state16, ar_stream_t stream) {
+  if (!s || !h_state16) return AR_ERR_INVALID_ARG;
+  if (s->nb == 0) return AR_OK;
+  const size_t row = 16 * (size_t)s->nb;
+  cudaMemcpy2DAsync(s->pos, state_pitch(s), h_state16, row, row, 4, cudaMemcpyHostToDevice,
+                    arh::stream(stream));
+  return arh::check_launch("ar_scene_upload_state");
+}
+
+ar_status ar_scene_download_state_async(ar_scene* s, float* h_state16, ar_stream_t stream) {
+  if (!s || !h_state16) return AR_ERR_INVALID_ARG;
+  if (s->nb == 0) return AR_OK;
+  const size_t row = 16 * (size_t)s->nb;
+  cudaMemcpy2DAsync(h_state16, row, s->pos, state_pitch(s), row, 4, cudaMemcpyDeviceToHost,
+                    arh::stream(stream));
+  return arh::check_launch("ar_scene_download_state_async");
+}
+
+ar_status ar_scene_download_state(ar_scene* s, float* h_state16, ar_stream_t stream) {
+  ar_status r = ar_scene_download_state_async(s, h_state16, stream);
+  if (r != AR_OK) return r;
+  cudaError_t e = cudaStreamSynchronize(arh::stream(stream));
+  if (e != cudaSuccess) {
+    arh::set_error("ar_scene_download_state: %s", cudaGetErrorString(e));
+    return AR_ERR_CUDA;
+  }
+  return AR_OK;
+}
+
 ar_status ar_scene_particle_forces(ar_scene* s, float* p_force4, float* p_torque4,
                                    ar_stream_t stream) {
   (void)p_torque4;

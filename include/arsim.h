@@ -468,6 +468,17 @@ AR_API ar_status ar_scene_download_async(ar_scene* scene, float* h_body_pos4,
 AR_API ar_status ar_scene_upload(ar_scene* scene, const float* h_body_pos4,
                                  const float* h_body_quat4, const float* h_body_vel4,
                                  const float* h_body_angvel4, ar_stream_t stream);
+/* Packed body state: h_state16 holds pos[nb], quat[nb], vel[nb], angvel[nb] back to back
+ * (16 floats per body in all), moved with one strided copy each way instead of four.
+ * ar_scene_upload_state is asynchronous (pinned memory for overlap);
+ * ar_scene_download_state returns once the state is on the host, and
+ * ar_scene_download_state_async once the copy is queued on `stream`.  Same role as
+ * ar_scene_upload / ar_scene_download (Particles/updateFunctions.cpp:2903-2930). */
+AR_API ar_status ar_scene_upload_state(ar_scene* scene, const float* h_state16,
+                                       ar_stream_t stream);
+AR_API ar_status ar_scene_download_state(ar_scene* scene, float* h_state16, ar_stream_t stream);
+AR_API ar_status ar_scene_download_state_async(ar_scene* scene, float* h_state16,
+                                               ar_stream_t stream);
 /* Device pointers of the scene's resident arrays (for tests / zero-copy consumers). */
 typedef struct ar_scene_view {
   int num_bodies, num_particles;

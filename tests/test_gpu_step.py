@@ -204,3 +204,28 @@ def test_cell_table_entries(ctx):
     single = np.minimum.reduceat(sb, first) == np.maximum.reduceat(sb, first)
     assert np.array_equal(meta >> 13, np.where(single, sb[first] + 1, 0))
     gs.close()
+
+
+def test_packed_state_transfers(ctx):
+    """ar_scene_upload_state / ar_scene_download_state move the same bytes as the four-array
+    calls, with one copy each way (the device arrays sit at a padded pitch)."""
+    sc = scenes.small_scene(9, nb_side=3, packed=True, r=1 / 128)  # 27 bodies: padded pitch
+    a, b = api.GpuScene(ctx, sc), api.GpuScene(ctx, sc)
+    a.step(5, use_graph=False)
+    got = a.download()
+    packed = a.download_state()
+    assert np.array_equal(packed, np.stack([got[k] for k in ("pos", "quat", "vel", "angvel")]))
+    pinned = torch.empty((4, sc.num_bodies, 4), dtype=torch.float32).pin_memory().numpy()
+    a.download_state(pinned, wait=False)
+    torch.cuda.synchronize()
+    assert np.array_equal(pinned, packed)
+    # b takes a's state through the packed upload; both then step identically
+    b.upload_state(packed)
+    a.step(3, use_graph=False)
+    b.step(3, use_graph=False)
+    ctx.check()
+    x, y = a.download(), b.download()
+    for k in x:
+        assert np.array_equal(x[k], y[k]), k
+    a.close()
+    b.close()
