@@ -133,6 +133,9 @@ SIGNATURES = {
     "ar_scene_download": [P, P, P, P, P, S],
     "ar_scene_download_async": [P, P, P, P, P, S],
     "ar_scene_upload": [P, P, P, P, P, S],
+    "ar_find_contacts_grid": [P, P, P, P, P, P, P, I, P, P, P, S],
+    "ar_gather_contacts": [P, P, I, P, P, P, P, P, P, P, P, I, P, P, P, P, P, P, P, P, P, S],
+    "ar_sequential_impulse": [P, P, P, I, P, P, P, P, P, P, P, P, I, P, P, P, P, P, I, S],
     "ar_scene_upload_state": [P, P, S],
     "ar_scene_download_state": [P, P, S],
     "ar_scene_download_state_async": [P, P, S],

@@ -1,0 +1,445 @@
+// The reference's sequential-impulse path (updateUniformGridSIS, RigidBodies/UniformGridUpdate.cpp
+// :734-815) on the GPU, in REFERENCE semantics: per-particle deepest contact on the uniform grid,
+// the contact list in particle order, and the Gauss-Seidel impulse iterations.  The reference
+// runs the last two on the host (Particles/updateFunctions.cpp:1431-1874) with a device round
+// trip every step.
+//
+// The solver is exact, not a parallel approximation.  A contact's update reads and writes only
+// the velocities of its (one or two) bodies and its own accumulated impulses, so two contacts
+// that share no body commute.  Contacts are therefore given levels -- level(c) = 1 + the highest
+// level among earlier contacts on either of its bodies -- and one level at a time is solved in
+// parallel: every body sees exactly the sequence of updates of the reference's loop, so the
+// results are the reference's bit for bit.  The level assignment is the same in every
+// iteration, since it depends only on which bodies each contact touches.
+#include "ar_glm.cuh"
+#include "ar_grid.cuh"
+#include "ar_internal.cuh"
+
+namespace {
+
+using ar_glm::cross3;
+using ar_glm::dot3;
+using ar_glm::mv;
+
+__device__ __forceinline__ float3 f3(float4 a) { return ar::mk3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return ar::add(a, b); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return ar::sub(a, b); }
+__device__ __forceinline__ float3 mul3(float s, float3 a) { return ar::mk3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float3 div3(float3 a, float s) { return ar::mk3(a.x / s, a.y / s, a.z / s); }
+// glm::normalize(vec3): v * inversesqrt(dot(v, v)), inversesqrt(x) = 1 / sqrt(x)
+__device__ __forceinline__ float3 gnormalize(float3 v) {
+  const float inv = 1.0f / sqrtf(dot3(v, v));
+  return ar::mk3(v.x * inv, v.y * inv, v.z * inv);
+}
+
+// ---- FindRigidBodyCollisionsUniformGridKernel (Kernels/RB_UniformGridKernels.cu:731-842) --------
+// Per sorted particle: over the 27 neighbour cells (z, y, x = -1..1), occupants of other bodies;
+// the deepest penetration 2r - |p - q| above the running maximum (re-read per cell, as the
+// reference does) is kept with the other particle's original index and body.
+__global__ void __launch_bounds__(128) find_contacts_grid_kernel(
+    ar_grid::Grid g, float radius, const int32_t* __restrict__ rb_idx,
+    const float4* __restrict__ spos, const uint32_t* __restrict__ gidx,
+    const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ cend, int n,
+    float* __restrict__ contact_distance, int32_t* __restrict__ colliding_body,
+    int32_t* __restrict__ colliding_particle) {
+  const int index = blockIdx.x * blockDim.x + threadIdx.x;
+  if (index >= n) return;
+  const float3 pos = f3(__ldg(spos + index));
+  const int3 gp = g.cell_of(pos);
+  const uint32_t orig = __ldg(gidx + index);
+  const int body = __ldg(rb_idx + orig);
+  const float threshold = 2 * radius;
+  for (int z = -1; z <= 1; ++z)
+    for (int y = -1; y <= 1; ++y)
+      for (int x = -1; x <= 1; ++x) {
+        const uint32_t h = g.hash(make_int3(gp.x + x, gp.y + y, gp.z + z));
+        const uint32_t st = __ldg(cstart + h);
+        float best = contact_distance[orig];
+        if (st == ar::kEmpty) continue;
+        const uint32_t en = __ldg(cend + h);
+        for (uint32_t j = st; j < en; ++j) {
+          const int o2 = (int)__ldg(gidx + j);
+          const int b2 = __ldg(rb_idx + o2);
+          if (j == (uint32_t)index || b2 == body) continue;
+          const float3 d = sub3(pos, f3(__ldg(spos + j)));
+          const float dist = sqrtf(ar::dot(d, d));
+          if (threshold - dist > best) {
+            best = threshold - dist;
+            contact_distance[orig] = best;
+            colliding_particle[orig] = o2;
+            colliding_body[orig] = b2;
+          }
+        }
+      }
+}
+
+// ---- GatherRigidBodyCollisions (Particles/updateFunctions.cpp:1431-1500) -----------------------
+// Particles with a contact (distance > 0), in particle order, become contacts: the contact point
+// and normal of findExactContactPoint (Particles/CPU_Engine.cpp:461-473, float4 arithmetic with
+// helper_math's host normalize, 1 / sqrt), the bias restitution * relative normal velocity, and
+// zeroed accumulated impulses.  Order-preserving compaction: per-block counts, their scan, and
+// the scatter.
+constexpr int kGatherBlock = 256;
+
+__global__ void __launch_bounds__(kGatherBlock) gather_count_kernel(
+    const float* __restrict__ contact_distance, int n, int* __restrict__ block_counts) {
+  const int i = blockIdx.x * kGatherBlock + threadIdx.x;
+  const bool hit = i < n && __ldg(contact_distance + i) > 0.f;
+  const int c = __syncthreads_count(hit);
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = c;
+}
+
+// Exclusive scan of the block counts in one block (any number of blocks, 1024 at a time).
+__global__ void __launch_bounds__(1024) gather_scan_kernel(int* __restrict__ block_counts,
+                                                           int blocks, int* __restrict__ total) {
+  __shared__ int s_warp[32];
+  __shared__ int s_carry;
+  if (threadIdx.x == 0) s_carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < blocks; base += 1024) {
+    const int i = base + threadIdx.x;
+    const int v = i < blocks ? block_counts[i] : 0;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = s_warp[lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += y;
+      }
+      s_warp[lane] = w;
+    }
+    __syncthreads();
+    const int carry = s_carry;
+    const int excl = carry + (warp > 0 ? s_warp[warp - 1] : 0) + x - v;
+    if (i < blocks) block_counts[i] = excl;
+    __syncthreads();
+    if (threadIdx.x == 1023) s_carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = s_carry;
+}
+
+__global__ void __launch_bounds__(kGatherBlock) gather_write_kernel(
+    float radius, float restitution, const int32_t* __restrict__ rb_idx,
+    const float4* __restrict__ cms, const float4* __restrict__ vel, const float4* __restrict__ ang,
+    const float4* __restrict__ rel, const float* __restrict__ contact_distance,
+    const int32_t* __restrict__ colliding_body, const int32_t* __restrict__ colliding_particle,
+    int n, const int* __restrict__ block_offsets, int capacity, float4* __restrict__ normal,
+    float4* __restrict__ point, int32_t* __restrict__ body1, int32_t* __restrict__ body2,
+    float* __restrict__ bias, float* __restrict__ acc_impulse, float* __restrict__ acc_friction,
+    float* __restrict__ acc_friction2, int* __restrict__ err) {
+  __shared__ int s_warp[kGatherBlock / 32];
+  const int i = blockIdx.x * kGatherBlock + threadIdx.x;
+  const bool hit = i < n && __ldg(contact_distance + i) > 0.f;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t m = __ballot_sync(0xffffffffu, hit);
+  if (lane == 0) s_warp[warp] = __popc(m);
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < warp; ++w) before += s_warp[w];
+  if (!hit) return;
+  const int c = block_offsets[blockIdx.x] + before + __popc(m & ((1u << lane) - 1));
+  if (c >= capacity) {
+    ar::raise_error(err, ar::kErrOverflow);
+    return;
+  }
+  const int b = __ldg(rb_idx + i);
+  const int j = __ldg(colliding_particle + i);
+  const int b2 = __ldg(colliding_body + i);
+  const float4 cm1 = __ldg(cms + b), cm2 = __ldg(cms + b2);
+  const float4 r1 = __ldg(rel + i), r2 = __ldg(rel + j);
+  const float4 p1 = make_float4(cm1.x + r1.x, cm1.y + r1.y, cm1.z + r1.z, cm1.w + r1.w);
+  const float4 p2 = make_float4(cm2.x + r2.x, cm2.y + r2.y, cm2.z + r2.z, cm2.w + r2.w);
+  const float t = radius / (radius + radius);
+  const float4 cp = make_float4(p1.x + (p2.x - p1.x) * t, p1.y + (p2.y - p1.y) * t,
+                                p1.z + (p2.z - p1.z) * t, p1.w + (p2.w - p1.w) * t);
+  const float4 d = make_float4(p2.x - p1.x, p2.y - p1.y, p2.z - p1.z, p2.w - p1.w);
+  const float inv = 1.0f / sqrtf(d.x * d.x + d.y * d.y + d.z * d.z + d.w * d.w);
+  const float4 cn = make_float4(d.x * inv * (-1.f), d.y * inv * (-1.f), d.z * inv * (-1.f),
+                                d.w * inv * (-1.f));
+  const float3 n3 = f3(cn);
+  const float3 v1 = f3(__ldg(vel + b)), w1 = f3(__ldg(ang + b));
+  const float3 v2 = f3(__ldg(vel + b2)), w2 = f3(__ldg(ang + b2));
+  const float v_rel = ar::dot(add3(v1, ar::cross(w1, f3(r1))), n3) -
+                      ar::dot(add3(v2, ar::cross(w2, f3(r2))), n3);
+  normal[c] = cn;
+  point[c] = cp;
+  body1[c] = b;
+  body2[c] = b2;
+  bias[c] = restitution * v_rel;
+  acc_impulse[c] = 0.f;
+  acc_friction[c] = 0.f;
+  acc_friction2[c] = 0.f;
+}
+
+// ---- SequentialImpulseSolver (Particles/updateFunctions.cpp:1580-1874) --------------------------
+struct Contacts {
+  const float4* normal;
+  const float4* point;
+  const int32_t* body1;
+  const int32_t* body2;
+  const float* bias;
+  float* acc_impulse;
+  float* acc_friction;
+  float* acc_friction2;
+};
+struct Bodies {
+  const float4* cms;
+  float4* vel;
+  float4* ang;
+  const float* inv_inertia;  // current (world) inverse inertia, glm::mat3
+  const float* mass;
+};
+
+__device__ __forceinline__ float clampf(float v, float lo, float hi) {
+  return v < lo ? lo : (v > hi ? hi : v);
+}
+
+// One contact's update, the reference's loop body.  The reference compares the float values
+// with double constants (abs(x) < 0.00001), so the comparisons are made in double here too.
+__device__ void solve_contact(int c, const Contacts& C, const Bodies& B, float ar_friction,
+                              float rb_friction, float abs_gravity_y, float upper_bound) {
+  const float3 n = f3(C.normal[c]);
+  const float4 point = C.point[c];
+  const int i1 = C.body1[c], i2 = C.body2[c];
+  const float4 cm1 = B.cms[i1];
+  const float3 p1 = ar::mk3(point.x - cm1.x, point.y - cm1.y, point.z - cm1.z);
+  const float* I1 = B.inv_inertia + 9 * i1;
+  const float m1 = B.mass[i1];
+  float3 v1 = f3(B.vel[i1]), w1 = f3(B.ang[i1]);
+  if (i2 == -1) {
+    float mc = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n);
+    if ((double)fabsf(mc) < 0.00001) mc = 1.f;
+    const float v_rel = dot3(add3(v1, cross3(w1, p1)), n);
+    float corrective = -(v_rel + C.bias[c]) / mc;
+    float acc = C.acc_impulse[c];
+    float tmp = clampf(acc + corrective, 0.f, upper_bound);
+    corrective = tmp - acc;
+    C.acc_impulse[c] = tmp;
+    const float bound = ar_friction * mc * abs_gravity_y;
+    const float3 vel = add3(v1, cross3(w1, p1));
+    float3 t1 = ar::mk3(1.f, 0.f, 0.f);
+    if ((double)fabsf(t1.x - n.x) < 0.0001) t1 = ar::mk3(0.f, 1.f, 0.f);
+    else if ((double)fabsf(t1.x + n.x) < 0.0001) t1 = ar::mk3(0.f, 1.f, 0.f);
+    t1 = gnormalize(sub3(t1, mul3(dot3(t1, n), n)));
+    const float k1 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1);
+    float cf1 = -dot3(vel, t1) / k1;
+    const float a1 = C.acc_friction[c];
+    const float f1 = clampf(a1 + cf1, -bound, bound);
+    cf1 = f1 - a1;
+    C.acc_friction[c] = f1;
+    const float3 t2 = gnormalize(cross3(t1, n));
+    const float k2 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2);
+    float cf2 = -dot3(vel, t2) / k2;
+    const float a2 = C.acc_friction2[c];
+    const float f2 = clampf(a2 + cf2, -bound, bound);
+    cf2 = f2 - a2;
+    C.acc_friction2[c] = f2;
+    const float3 imp = add3(add3(mul3(corrective, n), mul3(cf1, t1)), mul3(cf2, t2));
+    v1 = add3(v1, div3(imp, m1));
+    w1 = add3(w1, mv(I1, cross3(p1, imp)));
+    B.vel[i1] = make_float4(v1.x, v1.y, v1.z, 0.f);
+    B.ang[i1] = make_float4(w1.x, w1.y, w1.z, 0.f);
+    return;
+  }
+  const float4 cm2 = B.cms[i2];
+  const float3 p2 = ar::mk3(point.x - cm2.x, point.y - cm2.y, point.z - cm2.z);
+  const float* I2 = B.inv_inertia + 9 * i2;
+  const float m2 = B.mass[i2];
+  float3 v2 = f3(B.vel[i2]), w2 = f3(B.ang[i2]);
+  float mc = 1 / m1 + 1 / m2 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n) +
+             dot3(cross3(mv(I2, cross3(p2, n)), p2), n);
+  if ((double)fabsf(mc) < 0.00001) mc = 1.f;
+  const float v_rel = dot3(add3(v1, cross3(w1, p1)), n) - dot3(add3(v2, cross3(w2, p2)), n);
+  float corrective = -(v_rel + C.bias[c]) / mc;
+  const float acc = C.acc_impulse[c];
+  const float tmp = clampf(acc + corrective, 0.f, upper_bound);
+  corrective = tmp - acc;
+  C.acc_impulse[c] = tmp;
+  // friction is accumulated as the reference does, but (as there) not applied between bodies
+  const float bound = rb_friction * mc * abs_gravity_y;
+  const float3 vel = add3(add3(add3(mul3(-1.f, v1), cross3(w1, p1)), v2), cross3(w2, p2));
+  float3 t1 = ar::mk3(1.f, 0.f, 0.f);
+  if ((double)fabsf(t1.x - n.x) < 0.0001) t1 = ar::mk3(0.f, 1.f, 0.f);
+  t1 = gnormalize(sub3(t1, mul3(dot3(t1, n), n)));
+  const float k1 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1)) +
+                   (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t1)), p2), t1));
+  const float cf1 = -dot3(vel, t1) / k1;
+  const float a1 = C.acc_friction[c];
+  C.acc_friction[c] = clampf(a1 + cf1, -bound, bound);
+  const float3 t2 = gnormalize(cross3(t1, n));
+  const float k2 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2)) +
+                   (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t2)), p2), t2));
+  const float cf2 = -dot3(vel, t2) / k2;
+  const float a2 = C.acc_friction2[c];
+  C.acc_friction2[c] = clampf(a2 + cf2, -bound, bound);
+  const float3 imp = mul3(corrective, n);
+  v1 = add3(v1, div3(imp, m1));
+  w1 = add3(w1, mv(I1, cross3(p1, imp)));
+  B.vel[i1] = make_float4(v1.x, v1.y, v1.z, 0.f);
+  B.ang[i1] = make_float4(w1.x, w1.y, w1.z, 0.f);
+  v2 = sub3(v2, div3(imp, m2));
+  w2 = sub3(w2, mv(I2, cross3(p2, imp)));
+  B.vel[i2] = make_float4(v2.x, v2.y, v2.z, 0.f);
+  B.ang[i2] = make_float4(w2.x, w2.y, w2.z, 0.f);
+}
+
+constexpr int kSisThreads = 1024;
+
+// One block: levels (one thread walks the contacts in order), contacts bucketed by level,
+// then `iterations` sweeps, each solving the levels in order with a barrier between them.
+// Scratch: level[capacity], order[capacity], level_start[capacity + 2], last[num_bodies].
+__global__ void __launch_bounds__(kSisThreads) sis_kernel(
+    Contacts C, Bodies B, const int* __restrict__ d_count, int capacity, int num_bodies,
+    int iterations, float ar_friction, float rb_friction, float abs_gravity_y, float upper_bound,
+    int* __restrict__ level, int* __restrict__ order, int* __restrict__ last,
+    int* __restrict__ level_start, int* __restrict__ err) {
+  __shared__ int s_levels;
+  int count = *d_count;
+  if (count > capacity) {
+    if (threadIdx.x == 0) ar::raise_error(err, ar::kErrOverflow);
+    count = capacity;
+  }
+  for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) last[b] = 0;
+  for (int l = threadIdx.x; l < count + 2; l += blockDim.x) level_start[l] = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int top = 0;
+    for (int c = 0; c < count; ++c) {
+      const int b1 = C.body1[c], b2 = C.body2[c];
+      int l = last[b1];
+      if (b2 >= 0 && last[b2] > l) l = last[b2];
+      ++l;
+      level[c] = l;
+      last[b1] = l;
+      if (b2 >= 0) last[b2] = l;
+      if (l > top) top = l;
+    }
+    s_levels = top;
+  }
+  __syncthreads();
+  const int levels = s_levels;
+  // bucket by level: counts at level_start[l] (levels are 1..levels), exclusive scan (one
+  // thread; levels <= count), scatter with the starts as cursors -- afterwards level l occupies
+  // [level_start[l - 1], level_start[l]) with level_start[0] = 0.  The order inside a level is
+  // free: its contacts share no body.
+  for (int c = threadIdx.x; c < count; c += blockDim.x) atomicAdd(level_start + level[c], 1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int run = 0;
+    for (int l = 1; l <= levels; ++l) {
+      const int v = level_start[l];
+      level_start[l] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+  for (int c = threadIdx.x; c < count; c += blockDim.x)
+    order[atomicAdd(level_start + level[c], 1)] = c;
+  __syncthreads();
+  for (int it = 0; it < iterations; ++it)
+    for (int l = 1; l <= levels; ++l) {
+      const int lo = level_start[l - 1], hi = level_start[l];
+      for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
+        solve_contact(order[i], C, B, ar_friction, rb_friction, abs_gravity_y, upper_bound);
+      __syncthreads();
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+ar_status ar_find_contacts_grid(ar_ctx* ctx, const ar_sim_params* params, const int32_t* rb_idx,
+                                const float* sorted_pos4, const uint32_t* grid_idx,
+                                const uint32_t* cell_start, const uint32_t* cell_end, int n,
+                                float* contact_distance, int32_t* colliding_body,
+                                int32_t* colliding_particle, ar_stream_t stream) {
+  if (!ctx || !params || n < 0 ||
+      (n > 0 && (!rb_idx || !sorted_pos4 || !grid_idx || !cell_start || !cell_end ||
+                 !contact_distance || !colliding_body || !colliding_particle)))
+    return AR_ERR_INVALID_ARG;
+  for (int a = 0; a < 3; ++a) {
+    const uint32_t g = params->grid_size[a];
+    if (!g || (g & (g - 1))) {
+      arh::set_error("grid_size must be powers of two (the hash wraps with & (G-1))");
+      return AR_ERR_INVALID_ARG;
+    }
+  }
+  if (n == 0) return AR_OK;
+  find_contacts_grid_kernel<<<arh::grid_for(n, 128), 128, 0, arh::stream(stream)>>>(
+      ar_grid::Grid::from_params(*params), params->particle_radius, rb_idx,
+      (const float4*)sorted_pos4, grid_idx, cell_start, cell_end, n, contact_distance,
+      colliding_body, colliding_particle);
+  return arh::check_launch("ar_find_contacts_grid");
+}
+
+ar_status ar_gather_contacts(ar_ctx* ctx, const ar_sim_params* params, int n,
+                             const int32_t* rb_idx, const float* cms4, const float* vel4,
+                             const float* ang4, const float* rel4, const float* contact_distance,
+                             const int32_t* colliding_body, const int32_t* colliding_particle,
+                             int capacity, float* normal4, float* point4, int32_t* body1,
+                             int32_t* body2, float* bias, float* acc_impulse,
+                             float* acc_friction, float* acc_friction2, int32_t* d_count,
+                             ar_stream_t stream) {
+  if (!ctx || !params || n < 0 || capacity < 0 || !d_count ||
+      (n > 0 && (!rb_idx || !cms4 || !vel4 || !ang4 || !rel4 || !contact_distance ||
+                 !colliding_body || !colliding_particle)) ||
+      (capacity > 0 && (!normal4 || !point4 || !body1 || !body2 || !bias || !acc_impulse ||
+                        !acc_friction || !acc_friction2)))
+    return AR_ERR_INVALID_ARG;
+  cudaStream_t st = arh::stream(stream);
+  if (n == 0) {
+    cudaMemsetAsync(d_count, 0, sizeof(int32_t), st);
+    return arh::check_launch("ar_gather_contacts");
+  }
+  const int blocks = (int)arh::grid_for(n, kGatherBlock);
+  int* offsets = (int*)arh::scratch(ctx, sizeof(int) * (size_t)blocks);
+  if (!offsets) return AR_ERR_OOM;
+  gather_count_kernel<<<blocks, kGatherBlock, 0, st>>>(contact_distance, n, offsets);
+  gather_scan_kernel<<<1, 1024, 0, st>>>(offsets, blocks, d_count);
+  gather_write_kernel<<<blocks, kGatherBlock, 0, st>>>(
+      params->particle_radius, params->rb_restitution, rb_idx, (const float4*)cms4,
+      (const float4*)vel4, (const float4*)ang4, (const float4*)rel4, contact_distance,
+      colliding_body, colliding_particle, n, offsets, capacity, (float4*)normal4,
+      (float4*)point4, body1, body2, bias, acc_impulse, acc_friction, acc_friction2, ctx->d_err);
+  return arh::check_launch("ar_gather_contacts");
+}
+
+ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params, const int32_t* d_count,
+                                int capacity, const float* normal4, const float* point4,
+                                const int32_t* body1, const int32_t* body2, const float* bias,
+                                float* acc_impulse, float* acc_friction, float* acc_friction2,
+                                int num_bodies, const float* cms4, float* vel4, float* ang4,
+                                const float* cur_inv_inertia9, const float* mass, int iterations,
+                                ar_stream_t stream) {
+  if (!ctx || !params || !d_count || capacity < 0 || num_bodies < 0 || iterations < 0 ||
+      (capacity > 0 && (!normal4 || !point4 || !body1 || !body2 || !bias || !acc_impulse ||
+                        !acc_friction || !acc_friction2)) ||
+      (num_bodies > 0 && (!cms4 || !vel4 || !ang4 || !cur_inv_inertia9 || !mass)))
+    return AR_ERR_INVALID_ARG;
+  if (capacity == 0 || num_bodies == 0 || iterations == 0) return AR_OK;
+  // scratch: level[capacity], order[capacity], level_start[capacity + 2], last[num_bodies]
+  const size_t words = 3 * (size_t)capacity + 2 + (size_t)num_bodies;
+  int* w = (int*)arh::scratch(ctx, sizeof(int) * words);
+  if (!w) return AR_ERR_OOM;
+  Contacts C{(const float4*)normal4, (const float4*)point4, body1, body2, bias, acc_impulse,
+             acc_friction, acc_friction2};
+  Bodies B{(const float4*)cms4, (float4*)vel4, (float4*)ang4, cur_inv_inertia9, mass};
+  sis_kernel<<<1, kSisThreads, 0, arh::stream(stream)>>>(
+      C, B, d_count, capacity, num_bodies, iterations, params->ar_friction, params->rb_friction,
+      fabsf(params->gravity[1]), 100.f, w, w + capacity, w + 3 * (size_t)capacity + 2,
+      w + 2 * (size_t)capacity, ctx->d_err);
+  return arh::check_launch("ar_sequential_impulse");
+}
+
+}  // extern "C"

@@ -384,6 +384,53 @@ AR_API ar_status ar_walls_reference(ar_ctx* ctx, float radius, const float* part
                                     const int32_t* rb_idx, const int32_t* offsets,
                                     int num_bodies, int n, ar_stream_t stream);
 
+/* ---- sequential-impulse path (updateUniformGridSIS, RigidBodies/UniformGridUpdate.cpp:734-815) ----
+ * REFERENCE semantics, all on the device (the reference gathers and solves on the host).
+ *
+ * FindRigidBodyCollisionsUniformGridKernel (Kernels/RB_UniformGridKernels.cu:731-842): per
+ * sorted particle over the 27 neighbour cells, the deepest penetration 2r - |p - q| by a
+ * particle of another body that exceeds contact_distance[original index] (the running maximum:
+ * zero it before the call, as the reference does), with that particle's original index and
+ * body.  Inputs are ar_calc_hash / sort / ar_reorder_cells outputs. */
+AR_API ar_status ar_find_contacts_grid(ar_ctx* ctx, const ar_sim_params* params,
+                                       const int32_t* rb_idx, const float* sorted_pos4,
+                                       const uint32_t* grid_idx, const uint32_t* cell_start,
+                                       const uint32_t* cell_end, int n, float* contact_distance,
+                                       int32_t* colliding_body, int32_t* colliding_particle,
+                                       ar_stream_t stream);
+/* GatherRigidBodyCollisions (Particles/updateFunctions.cpp:1431-1500): every particle with
+ * contact_distance > 0, in particle order (particles stored body by body, rb_idx their
+ * bodies), becomes contact c: point and normal of findExactContactPoint on CM + rel of the
+ * two particles (float4 arithmetic, Particles/CPU_Engine.cpp:461-473), body1 = its body,
+ * body2 = the colliding body, bias = rb_restitution * relative normal velocity, accumulated
+ * impulse and frictions 0.  *d_count (device) receives the number of contacts; those beyond
+ * capacity are dropped and raise AR_ERR_OVERFLOW through ar_ctx_status. */
+AR_API ar_status ar_gather_contacts(ar_ctx* ctx, const ar_sim_params* params, int n,
+                                    const int32_t* rb_idx, const float* cms4, const float* vel4,
+                                    const float* ang4, const float* rel4,
+                                    const float* contact_distance, const int32_t* colliding_body,
+                                    const int32_t* colliding_particle, int capacity,
+                                    float* normal4, float* point4, int32_t* body1,
+                                    int32_t* body2, float* bias, float* acc_impulse,
+                                    float* acc_friction, float* acc_friction2, int32_t* d_count,
+                                    ar_stream_t stream);
+/* SequentialImpulseSolver (Particles/updateFunctions.cpp:1580-1874): `iterations` (the
+ * reference uses 18) Gauss-Seidel sweeps over the *d_count contacts in order; accumulated
+ * impulse clamped to [0, 100], friction to +-friction * mc * |g.y| (ar_friction for one-body
+ * contacts, body2 == -1, whose impulse includes friction; rb_friction for body pairs, whose
+ * applied impulse is the normal part only, as in the reference); body velocities and angular
+ * velocities updated in place.  Bit-identical to the sequential loop: contacts that share no
+ * body are solved together, one dependency level at a time, in one thread block. */
+AR_API ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params,
+                                       const int32_t* d_count, int capacity,
+                                       const float* normal4, const float* point4,
+                                       const int32_t* body1, const int32_t* body2,
+                                       const float* bias, float* acc_impulse,
+                                       float* acc_friction, float* acc_friction2,
+                                       int num_bodies, const float* cms4, float* vel4,
+                                       float* ang4, const float* cur_inv_inertia9,
+                                       const float* mass, int iterations, ar_stream_t stream);
+
 /* ==== fused step: scenes and batches ================================================================
  * A scene is one independent rigid-body world resident on the device.  ar_step advances it
  * with the fused pipeline (re-pose + hash, onesweep sort, scatter + cell ranges, DEM

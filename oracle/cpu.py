@@ -405,3 +405,58 @@ def collide_static_scene(origin, cell, dims, radius, prm4, spos4, svel4, rel4, s
                                _p(lin), _p(ang), _p(color))
     return lin, ang, color
 
+
+
+# ---- sequential-impulse path ---------------------------------------------------------------------
+_L.or_find_contacts_grid.restype = None
+_L.or_gather_contacts.restype = C.c_long
+_L.or_sequential_impulse.restype = None
+
+
+def find_contacts_grid(origin, cell, dims, radius, rb_idx, spos4, gidx, cstart, cend,
+                       contact_distance=None):
+    """FindRigidBodyCollisionsUniformGridKernel on sorted arrays -> (distance, body, particle)
+    per original particle index (distance starts at contact_distance, default 0)."""
+    n = len(spos4)
+    g6 = _f32(list(origin) + list(np.broadcast_to(cell, 3)))
+    cd = np.zeros(n, np.float32) if contact_distance is None else _f32(contact_distance).copy()
+    cb = np.zeros(n, np.int32)
+    cp = np.zeros(n, np.int32)
+    _L.or_find_contacts_grid(_p(g6), _p(_u32(dims)), C.c_float(radius), _p(_i32(rb_idx)),
+                             _p(_f32(spos4)), _p(_u32(gidx)), _p(_u32(cstart)), _p(_u32(cend)),
+                             C.c_long(n), _p(cd), _p(cb), _p(cp))
+    return cd, cb, cp
+
+
+def gather_contacts(radius, restitution, rb_idx, cms4, vel4, ang4, rel4, contact_distance,
+                    colliding_body, colliding_particle) -> dict:
+    """GatherRigidBodyCollisions: the contact list in particle order."""
+    n = len(rb_idx)
+    out = {"normal": np.zeros((n, 4), np.float32), "point": np.zeros((n, 4), np.float32),
+           "body1": np.zeros(n, np.int32), "body2": np.zeros(n, np.int32),
+           "bias": np.zeros(n, np.float32)}
+    c = _L.or_gather_contacts(C.c_float(radius), C.c_float(restitution), C.c_long(n),
+                              _p(_i32(rb_idx)), _p(_f32(cms4)), _p(_f32(vel4)), _p(_f32(ang4)),
+                              _p(_f32(rel4)), _p(_f32(contact_distance)),
+                              _p(_i32(colliding_body)), _p(_i32(colliding_particle)),
+                              _p(out["normal"]), _p(out["point"]), _p(out["body1"]),
+                              _p(out["body2"]), _p(out["bias"]))
+    return {k: v[:c] for k, v in out.items()}
+
+
+def sequential_impulse(contacts: dict, cms4, vel4, ang4, inertia9, mass, iterations=18,
+                       ar_friction=0.3, rb_friction=0.1, gravity_y=-9.81, acc=None):
+    """SequentialImpulseSolver as the reference's host loop -> (vel4, ang4, accumulated
+    impulse, friction, friction 2)."""
+    k = len(contacts["body1"])
+    vel, ang = _f32(vel4).copy(), _f32(ang4).copy()
+    if acc is None:
+        acc = tuple(np.zeros(k, np.float32) for _ in range(3))
+    a0, a1, a2 = (_f32(a).copy() for a in acc)
+    _L.or_sequential_impulse(C.c_long(k), _p(_f32(contacts["normal"])), _p(_f32(contacts["point"])),
+                             _p(_i32(contacts["body1"])), _p(_i32(contacts["body2"])),
+                             _p(_f32(contacts["bias"])), _p(a0), _p(a1), _p(a2), _p(_f32(cms4)),
+                             _p(vel), _p(ang), _p(_f32(inertia9)), _p(_f32(mass)),
+                             C.c_int(iterations), C.c_float(ar_friction), C.c_float(rb_friction),
+                             C.c_float(gravity_y))
+    return vel, ang, a0, a1, a2

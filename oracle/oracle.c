@@ -1393,3 +1393,189 @@ int or_reduce_rbvars(const float* pf4, const float* pt4, const int* starts, cons
   }
   return ok;
 }
+
+/* ====================================================================================
+ * Sequential-impulse path (updateUniformGridSIS, RigidBodies/UniformGridUpdate.cpp:734-815).
+ * ==================================================================================== */
+
+/* FindRigidBodyCollisionsUniformGridCell / Kernel (Kernels/RB_UniformGridKernels.cu:731-842):
+ * per sorted particle, the deepest penetration by a particle of another body, above the running
+ * maximum contact_distance[original] (re-read per neighbour cell). */
+void or_find_contacts_grid(const float* grid6, const uint32_t* dims3, float radius,
+                           const int* rb_idx, const float* spos4, const uint32_t* gidx,
+                           const uint32_t* cstart, const uint32_t* cend, long n,
+                           float* contact_distance, int* colliding_body,
+                           int* colliding_particle) {
+  grid_t G;
+  memcpy(G.o, grid6, 12); memcpy(G.c, grid6 + 3, 12); memcpy(G.g, dims3, 12);
+  const float threshold = 2 * radius;
+  for (long index = 0; index < n; ++index) {
+    v3 pos = xyz(spos4 + 4 * index);
+    int gp[3];
+    cell_of(&G, pos, gp);
+    uint32_t orig = gidx[index];
+    int body = rb_idx[orig];
+    for (int z = -1; z <= 1; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int x = -1; x <= 1; ++x) {
+          uint32_t h = hash3(&G, gp[0] + x, gp[1] + y, gp[2] + z);
+          uint32_t st = cstart[h];
+          float best = contact_distance[orig];
+          if (st == EMPTY) continue;
+          uint32_t en = cend[h];
+          for (uint32_t j = st; j < en; ++j) {
+            int o2 = (int)gidx[j];
+            int b2 = rb_idx[o2];
+            if (j == (uint32_t)index || b2 == body) continue;
+            v3 d = sub(pos, xyz(spos4 + 4 * j));
+            float dist = sqrtf(dot(d, d));
+            if (threshold - dist > best) {
+              best = threshold - dist;
+              contact_distance[orig] = best;
+              colliding_particle[orig] = o2;
+              colliding_body[orig] = b2;
+            }
+          }
+        }
+  }
+}
+
+/* GatherRigidBodyCollisions (Particles/updateFunctions.cpp:1431-1500) with findExactContactPoint
+ * (Particles/CPU_Engine.cpp:461-473): float4 arithmetic, normalize = v * (1 / sqrt(dot4)). */
+long or_gather_contacts(float radius, float restitution, long n, const int* rb_idx,
+                        const float* cms4, const float* vel4, const float* ang4,
+                        const float* rel4, const float* contact_distance,
+                        const int* colliding_body, const int* colliding_particle,
+                        float* normal4, float* point4, int* body1, int* body2, float* bias) {
+  long c = 0;
+  for (long i = 0; i < n; ++i) {
+    if (!(contact_distance[i] > 0)) continue;
+    int b = rb_idx[i], j = colliding_particle[i], b2 = colliding_body[i];
+    const float *cm1 = cms4 + 4 * b, *cm2 = cms4 + 4 * b2, *r1 = rel4 + 4 * (long)i,
+                *r2 = rel4 + 4 * (long)j;
+    float p1[4], p2[4], cp[4], d[4], cn[4];
+    for (int k = 0; k < 4; ++k) {
+      p1[k] = cm1[k] + r1[k];
+      p2[k] = cm2[k] + r2[k];
+    }
+    float t = radius / (radius + radius);
+    for (int k = 0; k < 4; ++k) {
+      cp[k] = p1[k] + (p2[k] - p1[k]) * t;
+      d[k] = p2[k] - p1[k];
+    }
+    float inv = 1.0f / sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2] + d[3] * d[3]);
+    for (int k = 0; k < 4; ++k) cn[k] = d[k] * inv * (-1.f);
+    v3 n3 = mk3(cn[0], cn[1], cn[2]);
+    v3 v1 = xyz(vel4 + 4 * b), w1 = xyz(ang4 + 4 * b);
+    v3 v2 = xyz(vel4 + 4 * b2), w2 = xyz(ang4 + 4 * b2);
+    float v_rel = dot(add(v1, cross(w1, xyz(r1))), n3) - dot(add(v2, cross(w2, xyz(r2))), n3);
+    memcpy(normal4 + 4 * c, cn, 16);
+    memcpy(point4 + 4 * c, cp, 16);
+    body1[c] = b;
+    body2[c] = b2;
+    bias[c] = restitution * v_rel;
+    ++c;
+  }
+  return c;
+}
+
+static float clampf_(float v, float lo, float hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static v3 gnormalize_(v3 v) {
+  float inv = 1.0f / sqrtf(dot(v, v));
+  return mk3(v.x * inv, v.y * inv, v.z * inv);
+}
+
+/* SequentialImpulseSolver (Particles/updateFunctions.cpp:1580-1874), the host loop as written:
+ * float arithmetic, the abs(x) < 0.00001 / 0.0001 tests in double (float promoted), accumulated
+ * impulse clamped to [0, 100]. */
+void or_sequential_impulse(long count, const float* normal4, const float* point4,
+                           const int* body1, const int* body2, const float* bias,
+                           float* acc_impulse, float* acc_friction, float* acc_friction2,
+                           const float* cms4, float* vel4, float* ang4, const float* inertia9,
+                           const float* mass, int iterations, float ar_friction,
+                           float rb_friction, float gravity_y) {
+  const float upper = 100.f, g = fabsf(gravity_y);
+  for (int it = 0; it < iterations; ++it)
+    for (long c = 0; c < count; ++c) {
+      v3 n = xyz(normal4 + 4 * c);
+      const float* pt = point4 + 4 * c;
+      int i1 = body1[c], i2 = body2[c];
+      const float* cm1 = cms4 + 4 * i1;
+      v3 p1 = mk3(pt[0] - cm1[0], pt[1] - cm1[1], pt[2] - cm1[2]);
+      const float* I1 = inertia9 + 9 * i1;
+      float m1 = mass[i1];
+      v3 v1 = xyz(vel4 + 4 * i1), w1 = xyz(ang4 + 4 * i1);
+      if (i2 == -1) {
+        float mc = 1 / m1 + dot(glm_cross(glm_mv(I1, glm_cross(p1, n)), p1), n);
+        if ((double)fabsf(mc) < 0.00001) mc = 1.f;
+        float v_rel = dot(add(v1, glm_cross(w1, p1)), n);
+        float corr = -(v_rel + bias[c]) / mc;
+        float acc = acc_impulse[c];
+        float tmp = clampf_(acc + corr, 0.f, upper);
+        corr = tmp - acc;
+        acc_impulse[c] = tmp;
+        float bound = ar_friction * mc * g;
+        v3 vel = add(v1, glm_cross(w1, p1));
+        v3 t1 = mk3(1.f, 0.f, 0.f);
+        if ((double)fabsf(t1.x - n.x) < 0.0001) t1 = mk3(0.f, 1.f, 0.f);
+        else if ((double)fabsf(t1.x + n.x) < 0.0001) t1 = mk3(0.f, 1.f, 0.f);
+        t1 = gnormalize_(sub(t1, scl(dot(t1, n), n)));
+        float k1 = 1 / m1 + dot(glm_cross(glm_mv(I1, glm_cross(p1, t1)), p1), t1);
+        float cf1 = -dot(vel, t1) / k1;
+        float a1 = acc_friction[c];
+        float f1 = clampf_(a1 + cf1, -bound, bound);
+        cf1 = f1 - a1;
+        acc_friction[c] = f1;
+        v3 t2 = gnormalize_(glm_cross(t1, n));
+        float k2 = 1 / m1 + dot(glm_cross(glm_mv(I1, glm_cross(p1, t2)), p1), t2);
+        float cf2 = -dot(vel, t2) / k2;
+        float a2 = acc_friction2[c];
+        float f2 = clampf_(a2 + cf2, -bound, bound);
+        cf2 = f2 - a2;
+        acc_friction2[c] = f2;
+        v3 imp = add(add(scl(corr, n), scl(cf1, t1)), scl(cf2, t2));
+        v1 = add(v1, divs(imp, m1));
+        w1 = add(w1, glm_mv(I1, glm_cross(p1, imp)));
+        st4(vel4 + 4 * i1, v1.x, v1.y, v1.z, 0.f);
+        st4(ang4 + 4 * i1, w1.x, w1.y, w1.z, 0.f);
+        continue;
+      }
+      const float* cm2 = cms4 + 4 * i2;
+      v3 p2 = mk3(pt[0] - cm2[0], pt[1] - cm2[1], pt[2] - cm2[2]);
+      const float* I2 = inertia9 + 9 * i2;
+      float m2 = mass[i2];
+      v3 v2 = xyz(vel4 + 4 * i2), w2 = xyz(ang4 + 4 * i2);
+      float mc = 1 / m1 + 1 / m2 + dot(glm_cross(glm_mv(I1, glm_cross(p1, n)), p1), n) +
+                 dot(glm_cross(glm_mv(I2, glm_cross(p2, n)), p2), n);
+      if ((double)fabsf(mc) < 0.00001) mc = 1.f;
+      float v_rel = dot(add(v1, glm_cross(w1, p1)), n) - dot(add(v2, glm_cross(w2, p2)), n);
+      float corr = -(v_rel + bias[c]) / mc;
+      float acc = acc_impulse[c];
+      float tmp = clampf_(acc + corr, 0.f, upper);
+      corr = tmp - acc;
+      acc_impulse[c] = tmp;
+      float bound = rb_friction * mc * g;
+      v3 vel = add(add(add(scl(-1.f, v1), glm_cross(w1, p1)), v2), glm_cross(w2, p2));
+      v3 t1 = mk3(1.f, 0.f, 0.f);
+      if ((double)fabsf(t1.x - n.x) < 0.0001) t1 = mk3(0.f, 1.f, 0.f);
+      t1 = gnormalize_(sub(t1, scl(dot(t1, n), n)));
+      float k1 = (1 / m1 + dot(glm_cross(glm_mv(I1, glm_cross(p1, t1)), p1), t1)) +
+                 (1 / m2 + dot(glm_cross(glm_mv(I2, glm_cross(p2, t1)), p2), t1));
+      float cf1 = -dot(vel, t1) / k1;
+      acc_friction[c] = clampf_(acc_friction[c] + cf1, -bound, bound);
+      v3 t2 = gnormalize_(glm_cross(t1, n));
+      float k2 = (1 / m1 + dot(glm_cross(glm_mv(I1, glm_cross(p1, t2)), p1), t2)) +
+                 (1 / m2 + dot(glm_cross(glm_mv(I2, glm_cross(p2, t2)), p2), t2));
+      float cf2 = -dot(vel, t2) / k2;
+      acc_friction2[c] = clampf_(acc_friction2[c] + cf2, -bound, bound);
+      v3 imp = scl(corr, n);
+      v1 = add(v1, divs(imp, m1));
+      w1 = add(w1, glm_mv(I1, glm_cross(p1, imp)));
+      st4(vel4 + 4 * i1, v1.x, v1.y, v1.z, 0.f);
+      st4(ang4 + 4 * i1, w1.x, w1.y, w1.z, 0.f);
+      v2 = sub(v2, divs(imp, m2));
+      w2 = sub(w2, glm_mv(I2, glm_cross(p2, imp)));
+      st4(vel4 + 4 * i2, v2.x, v2.y, v2.z, 0.f);
+      st4(ang4 + 4 * i2, w2.x, w2.y, w2.z, 0.f);
+    }
+}

@@ -204,6 +204,18 @@ def find_rb_collisions_bvh(params, rb_idx, tree, cms4, bounds8, sorted_idx, radi
     return cd, cp, cb
 
 
+def find_rb_collisions_grid(params, rb_idx, spos4, gidx, cstart, cend, cd0):
+    """FindRigidBodyCollisionsUniformGridKernel -> (distance, body, particle) per original index."""
+    n = len(spos4)
+    cd = _f32(cd0).copy()
+    cb = np.zeros(n, np.int32)
+    cp = np.zeros(n, np.int32)
+    lib().refcpu_find_rb_collisions_grid(C.byref(params), _p(_i32(rb_idx)), _p(_f32(spos4)),
+                                         _p(_u32(gidx)), _p(_u32(cstart)), _p(_u32(cend)), n,
+                                         _p(cd), _p(cb), _p(cp))
+    return cd, cb, cp
+
+
 def wall_collisions(ppos4, rbpos4, mn3, mx3, rbvel4, rbang4, ib9, mass, rb_idx, counts, radius):
     v, a = _f32(rbvel4).copy(), _f32(rbang4).copy()
     lib().refcpu_wall_collisions(_p(_f32(ppos4)), _p(_f32(rbpos4)), _p(_f32(mn3)),

@@ -49,6 +49,8 @@ RANGES = [
     ("Kernels/rigidBodyKernels.cu", 449, 456, "resetQuaternionKernel"),
     ("Kernels/RB_BVHKernels.cu", 13, 244, "maxOpF4"),                            # collideStaticSpheresBVH, collideBVHSoARigidBody
     ("Kernels/RB_BVHKernels.cu", 760, 876, "FindRigidBodyCollisionsBVHKernel"),
+    ("Kernels/RB_UniformGridKernels.cu", 112, 128, "calcGridPosAuxil"),          # grid pos / hash
+    ("Kernels/RB_UniformGridKernels.cu", 730, 845, "__device__"),                # FindRigidBodyCollisionsUniformGrid cell + kernel
     ("WallCollisions.cu", 29, 35, "CreateIndexKernel"),
     ("WallCollisions.cu", 46, 129, "DetectWallCollisionKernel"),                 # + FindExactContactPoint, ComputeImpulseMagnitude
     ("WallCollisions.cu", 201, 276, "HandleWallCollisionKernelUnmapped"),

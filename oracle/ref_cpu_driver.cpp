@@ -318,6 +318,24 @@ void refcpu_find_rb_collisions_bvh(const void* sim_params, const int* rb_idx,
   });
 }
 
+// ---- deepest contact per particle on the grid: FindRigidBodyCollisionsUniformGridKernel
+// (Kernels/RB_UniformGridKernels.cu:731-842) ---------------------------------------------------
+void refcpu_find_rb_collisions_grid(const void* sim_params, const int* rb_idx,
+                                    const float* sorted_pos4, const uint32_t* grid_idx,
+                                    const uint32_t* cell_start, const uint32_t* cell_end, int n,
+                                    float* contact_distance, int* colliding_body,
+                                    int* colliding_particle) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  std::vector<float4> color(n);
+  launch(n, 128, true, [&] {
+    FindRigidBodyCollisionsUniformGridKernel((int*)rb_idx, colliding_body, colliding_particle,
+                                             contact_distance, color.data(), (float4*)sorted_pos4,
+                                             (uint*)grid_idx, (uint*)cell_start, (uint*)cell_end,
+                                             (uint)n, p);
+  });
+}
+
 // ---- integrateRigidBody (Kernels/rigidBodyKernels.cu:40-166) ------------------------------
 void refcpu_integrate_momentum(float* cms4, float* vel4, float* force4, float* ang4,
                                float* quat4, float* torque4, float* ang_mom4, float* lin_mom4,

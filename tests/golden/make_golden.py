@@ -231,16 +231,37 @@ def extra_case(seed: int):
     return out
 
 
+def sis_case(seed: int):
+    """FindRigidBodyCollisionsUniformGridKernel (the sequential-impulse path's contact search) on
+    the dem_small inputs: deepest contact per particle."""
+    d = dem_case(seed)
+    prm = params_for(float(d["radius"]), (0, 0, 0), float(d["cell"]), tuple(d["dims"]), 0.5,
+                     0.02, 0.1, 0.001)
+    cd, cb, cp = ref.find_rb_collisions_grid(prm, d["rb"], d["spos"], d["sidx"], d["cell_start"],
+                                             d["cell_end"], np.zeros(len(d["pos"]), np.float32))
+    return dict(rb=d["rb"], spos=d["spos"], sidx=d["sidx"], cell_start=d["cell_start"],
+                cell_end=d["cell_end"], radius=d["radius"], cell=d["cell"], dims=d["dims"],
+                contact_distance=cd, contact_body=cb, contact_particle=cp)
+
+
+CASES = {
+    "lbvh_uniform": lambda: lbvh_case(11, 3000, 0.0),
+    "lbvh_duplicates": lambda: lbvh_case(12, 3000, 0.2),
+    "dem_small": lambda: dem_case(5),
+    "bodies_small": lambda: body_case(9),
+    "reference_extra": lambda: extra_case(21),
+    "static_scene": lambda: static_scene_case(31),
+    "sis_find": lambda: sis_case(5),
+}
+
+
 def main() -> None:
+    """python tests/golden/make_golden.py [name ...]: (re)generate the named fixtures, or all."""
     if not ref.available():
         raise SystemExit("oracle/_ref/libref_cpu.so is not built (run oracle/ref_build.py)")
     ref.set_threads(1)
-    np.savez_compressed(OUT / "lbvh_uniform.npz", **lbvh_case(11, 3000, 0.0))
-    np.savez_compressed(OUT / "lbvh_duplicates.npz", **lbvh_case(12, 3000, 0.2))
-    np.savez_compressed(OUT / "dem_small.npz", **dem_case(5))
-    np.savez_compressed(OUT / "bodies_small.npz", **body_case(9))
-    np.savez_compressed(OUT / "reference_extra.npz", **extra_case(21))
-    np.savez_compressed(OUT / "static_scene.npz", **static_scene_case(31))
+    for name in sys.argv[1:] or CASES:
+        np.savez_compressed(OUT / f"{name}.npz", **CASES[name]())
     for f in sorted(OUT.glob("*.npz")):
         print(f.name, f.stat().st_size)
 
