@@ -206,22 +206,61 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) {
 
 // One contact's update, the reference's loop body.  The reference compares the float values
 // with double constants (abs(x) < 0.00001), so the comparisons are made in double here too.
-__device__ void solve_contact(int c, const Contacts& C, const Bodies& B, float ar_friction,
-                              float rb_friction, float abs_gravity_y, float upper_bound) {
-  const float3 n = f3(C.normal[c]);
-  const float4 point = C.point[c];
-  const int i1 = C.body1[c], i2 = C.body2[c];
-  const float4 cm1 = B.cms[i1];
+// What a contact's update reads apart from its bodies' velocities: its own data and
+// accumulated impulses (only this contact writes them) and its bodies' centres, masses and
+// inverse inertias (constant during the solve) -- loaded ahead of the contact's turn.
+struct ContactRec {
+  float4 normal, point, cm1, cm2;
+  int c, i1, i2;
+  float bias, m1, m2, a0, a1, a2;
+  float I1[9], I2[9];
+};
+__device__ __forceinline__ ContactRec load_contact(const Contacts& C, const Bodies& B, int c) {
+  ContactRec r;
+  r.c = c;
+  r.normal = C.normal[c];
+  r.point = C.point[c];
+  r.i1 = C.body1[c];
+  r.i2 = C.body2[c];
+  r.bias = C.bias[c];
+  r.a0 = C.acc_impulse[c];
+  r.a1 = C.acc_friction[c];
+  r.a2 = C.acc_friction2[c];
+  r.cm1 = B.cms[r.i1];
+  r.m1 = B.mass[r.i1];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r.I1[k] = B.inv_inertia[9 * r.i1 + k];
+  r.cm2 = make_float4(0.f, 0.f, 0.f, 0.f);
+  r.m2 = 1.f;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) r.I2[k] = 0.f;
+  if (r.i2 >= 0) {
+    r.cm2 = B.cms[r.i2];
+    r.m2 = B.mass[r.i2];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) r.I2[k] = B.inv_inertia[9 * r.i2 + k];
+  }
+  return r;
+}
+
+__device__ void solve_contact(const ContactRec& R, const Contacts& C, const Bodies& B,
+                              float ar_friction, float rb_friction, float abs_gravity_y,
+                              float upper_bound) {
+  const int c = R.c;
+  const float3 n = f3(R.normal);
+  const float4 point = R.point;
+  const int i1 = R.i1, i2 = R.i2;
+  const float4 cm1 = R.cm1;
   const float3 p1 = ar::mk3(point.x - cm1.x, point.y - cm1.y, point.z - cm1.z);
-  const float* I1 = B.inv_inertia + 9 * i1;
-  const float m1 = B.mass[i1];
+  const float* I1 = R.I1;
+  const float m1 = R.m1;
   float3 v1 = f3(B.vel[i1]), w1 = f3(B.ang[i1]);
   if (i2 == -1) {
     float mc = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n);
     if ((double)fabsf(mc) < 0.00001) mc = 1.f;
     const float v_rel = dot3(add3(v1, cross3(w1, p1)), n);
-    float corrective = -(v_rel + C.bias[c]) / mc;
-    float acc = C.acc_impulse[c];
+    float corrective = -(v_rel + R.bias) / mc;
+    float acc = R.a0;
     float tmp = clampf(acc + corrective, 0.f, upper_bound);
     corrective = tmp - acc;
     C.acc_impulse[c] = tmp;
@@ -233,14 +272,14 @@ __device__ void solve_contact(int c, const Contacts& C, const Bodies& B, float a
     t1 = gnormalize(sub3(t1, mul3(dot3(t1, n), n)));
     const float k1 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1);
     float cf1 = -dot3(vel, t1) / k1;
-    const float a1 = C.acc_friction[c];
+    const float a1 = R.a1;
     const float f1 = clampf(a1 + cf1, -bound, bound);
     cf1 = f1 - a1;
     C.acc_friction[c] = f1;
     const float3 t2 = gnormalize(cross3(t1, n));
     const float k2 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2);
     float cf2 = -dot3(vel, t2) / k2;
-    const float a2 = C.acc_friction2[c];
+    const float a2 = R.a2;
     const float f2 = clampf(a2 + cf2, -bound, bound);
     cf2 = f2 - a2;
     C.acc_friction2[c] = f2;
@@ -251,17 +290,17 @@ __device__ void solve_contact(int c, const Contacts& C, const Bodies& B, float a
     B.ang[i1] = make_float4(w1.x, w1.y, w1.z, 0.f);
     return;
   }
-  const float4 cm2 = B.cms[i2];
+  const float4 cm2 = R.cm2;
   const float3 p2 = ar::mk3(point.x - cm2.x, point.y - cm2.y, point.z - cm2.z);
-  const float* I2 = B.inv_inertia + 9 * i2;
-  const float m2 = B.mass[i2];
+  const float* I2 = R.I2;
+  const float m2 = R.m2;
   float3 v2 = f3(B.vel[i2]), w2 = f3(B.ang[i2]);
   float mc = 1 / m1 + 1 / m2 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n) +
              dot3(cross3(mv(I2, cross3(p2, n)), p2), n);
   if ((double)fabsf(mc) < 0.00001) mc = 1.f;
   const float v_rel = dot3(add3(v1, cross3(w1, p1)), n) - dot3(add3(v2, cross3(w2, p2)), n);
-  float corrective = -(v_rel + C.bias[c]) / mc;
-  const float acc = C.acc_impulse[c];
+  float corrective = -(v_rel + R.bias) / mc;
+  const float acc = R.a0;
   const float tmp = clampf(acc + corrective, 0.f, upper_bound);
   corrective = tmp - acc;
   C.acc_impulse[c] = tmp;
@@ -274,14 +313,12 @@ __device__ void solve_contact(int c, const Contacts& C, const Bodies& B, float a
   const float k1 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1)) +
                    (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t1)), p2), t1));
   const float cf1 = -dot3(vel, t1) / k1;
-  const float a1 = C.acc_friction[c];
-  C.acc_friction[c] = clampf(a1 + cf1, -bound, bound);
+  C.acc_friction[c] = clampf(R.a1 + cf1, -bound, bound);
   const float3 t2 = gnormalize(cross3(t1, n));
   const float k2 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2)) +
                    (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t2)), p2), t2));
   const float cf2 = -dot3(vel, t2) / k2;
-  const float a2 = C.acc_friction2[c];
-  C.acc_friction2[c] = clampf(a2 + cf2, -bound, bound);
+  C.acc_friction2[c] = clampf(R.a2 + cf2, -bound, bound);
   const float3 imp = mul3(corrective, n);
   v1 = add3(v1, div3(imp, m1));
   w1 = add3(w1, mv(I1, cross3(p1, imp)));
@@ -293,35 +330,43 @@ __device__ void solve_contact(int c, const Contacts& C, const Bodies& B, float a
   B.ang[i2] = make_float4(w2.x, w2.y, w2.z, 0.f);
 }
 
-constexpr int kSisThreads = 1024;
+constexpr int kSisThreads = 512;
+constexpr int kLevelCap = 8192;  // level bounds kept in shared memory when there are fewer
+constexpr size_t kSisSmemMax = 200 * 1024;
 
 // One block: levels (one thread walks the contacts in order), contacts bucketed by level,
 // then `iterations` sweeps, each solving the levels in order with a barrier between them.
+// kShared: the bodies' velocities and angular velocities (and the level bounds, when they
+// fit) live in shared memory for the sweeps, and each thread loads its contact of the next
+// level before the barrier that ends the current one.
 // Scratch: level[capacity], order[capacity], level_start[capacity + 2], last[num_bodies].
+template <bool kShared>
 __global__ void __launch_bounds__(kSisThreads) sis_kernel(
     Contacts C, Bodies B, const int* __restrict__ d_count, int capacity, int num_bodies,
     int iterations, float ar_friction, float rb_friction, float abs_gravity_y, float upper_bound,
     int* __restrict__ level, int* __restrict__ order, int* __restrict__ last,
     int* __restrict__ level_start, int* __restrict__ err) {
+  extern __shared__ float4 s_body[];  // kShared: vel[num_bodies], ang[num_bodies], bounds
   __shared__ int s_levels;
   int count = *d_count;
   if (count > capacity) {
     if (threadIdx.x == 0) ar::raise_error(err, ar::kErrOverflow);
     count = capacity;
   }
-  for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) last[b] = 0;
+  int* lastp = kShared ? reinterpret_cast<int*>(s_body) : last;
+  for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) lastp[b] = 0;
   for (int l = threadIdx.x; l < count + 2; l += blockDim.x) level_start[l] = 0;
   __syncthreads();
   if (threadIdx.x == 0) {
     int top = 0;
     for (int c = 0; c < count; ++c) {
       const int b1 = C.body1[c], b2 = C.body2[c];
-      int l = last[b1];
-      if (b2 >= 0 && last[b2] > l) l = last[b2];
+      int l = lastp[b1];
+      if (b2 >= 0 && lastp[b2] > l) l = lastp[b2];
       ++l;
       level[c] = l;
-      last[b1] = l;
-      if (b2 >= 0) last[b2] = l;
+      lastp[b1] = l;
+      if (b2 >= 0) lastp[b2] = l;
       if (l > top) top = l;
     }
     s_levels = top;
@@ -346,13 +391,56 @@ __global__ void __launch_bounds__(kSisThreads) sis_kernel(
   for (int c = threadIdx.x; c < count; c += blockDim.x)
     order[atomicAdd(level_start + level[c], 1)] = c;
   __syncthreads();
-  for (int it = 0; it < iterations; ++it)
-    for (int l = 1; l <= levels; ++l) {
-      const int lo = level_start[l - 1], hi = level_start[l];
-      for (int i = lo + (int)threadIdx.x; i < hi; i += blockDim.x)
-        solve_contact(order[i], C, B, ar_friction, rb_friction, abs_gravity_y, upper_bound);
-      __syncthreads();
+  Bodies W = B;
+  const int* bounds = level_start;
+  if (kShared) {
+    float4* sv = s_body;
+    float4* sa = s_body + num_bodies;
+    for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
+      sv[b] = B.vel[b];
+      sa[b] = B.ang[b];
     }
+    if (levels + 1 <= kLevelCap) {
+      int* sb = reinterpret_cast<int*>(s_body + 2 * num_bodies);
+      for (int l = threadIdx.x; l <= levels; l += blockDim.x) sb[l] = level_start[l];
+      bounds = sb;
+    }
+    W.vel = sv;
+    W.ang = sa;
+    __syncthreads();
+  }
+  const int tid = threadIdx.x;
+  // the thread's first contact of level l (later ones of a level wider than the block are
+  // loaded in turn)
+  auto first_of = [&](int l, ContactRec* r) {
+    const int i = bounds[l - 1] + tid;
+    if (i >= bounds[l]) return false;
+    *r = load_contact(C, B, order[i]);
+    return true;
+  };
+  for (int it = 0; it < iterations; ++it) {
+    ContactRec cur;
+    bool have = levels >= 1 && first_of(1, &cur);
+    for (int l = 1; l <= levels; ++l) {
+      ContactRec nxt;
+      const bool have_next = l < levels && first_of(l + 1, &nxt);
+      if (have) {
+        solve_contact(cur, C, W, ar_friction, rb_friction, abs_gravity_y, upper_bound);
+        for (int i = bounds[l - 1] + tid + (int)blockDim.x; i < bounds[l]; i += blockDim.x)
+          solve_contact(load_contact(C, B, order[i]), C, W, ar_friction, rb_friction,
+                        abs_gravity_y, upper_bound);
+      }
+      __syncthreads();
+      cur = nxt;
+      have = have_next;
+    }
+  }
+  if (kShared) {
+    for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
+      B.vel[b] = W.vel[b];
+      B.ang[b] = W.ang[b];
+    }
+  }
 }
 
 }  // namespace
@@ -435,10 +523,22 @@ ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params, const 
   Contacts C{(const float4*)normal4, (const float4*)point4, body1, body2, bias, acc_impulse,
              acc_friction, acc_friction2};
   Bodies B{(const float4*)cms4, (float4*)vel4, (float4*)ang4, cur_inv_inertia9, mass};
-  sis_kernel<<<1, kSisThreads, 0, arh::stream(stream)>>>(
-      C, B, d_count, capacity, num_bodies, iterations, params->ar_friction, params->rb_friction,
-      fabsf(params->gravity[1]), 100.f, w, w + capacity, w + 3 * (size_t)capacity + 2,
-      w + 2 * (size_t)capacity, ctx->d_err);
+  // bodies' velocities in shared memory when they fit (with the level bounds)
+  const size_t smem = 32 * (size_t)num_bodies + 4 * (size_t)kLevelCap;
+  cudaStream_t st = arh::stream(stream);
+  if (smem <= kSisSmemMax) {
+    cudaFuncSetAttribute(sis_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kSisSmemMax);
+    sis_kernel<true><<<1, kSisThreads, smem, st>>>(
+        C, B, d_count, capacity, num_bodies, iterations, params->ar_friction,
+        params->rb_friction, fabsf(params->gravity[1]), 100.f, w, w + capacity,
+        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, ctx->d_err);
+  } else {
+    sis_kernel<false><<<1, kSisThreads, 0, st>>>(
+        C, B, d_count, capacity, num_bodies, iterations, params->ar_friction,
+        params->rb_friction, fabsf(params->gravity[1]), 100.f, w, w + capacity,
+        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, ctx->d_err);
+  }
   return arh::check_launch("ar_sequential_impulse");
 }
 

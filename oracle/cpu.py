@@ -460,3 +460,25 @@ def sequential_impulse(contacts: dict, cms4, vel4, ang4, inertia9, mass, iterati
                              C.c_int(iterations), C.c_float(ar_friction), C.c_float(rb_friction),
                              C.c_float(gravity_y))
     return vel, ang, a0, a1, a2
+
+
+def sis_solve(state: dict, rb_idx, origin, cell, dims, radius, restitution=1.0,
+              ar_friction=0.3, rb_friction=0.1, gravity_y=-9.81e-3, iterations=18) -> dict:
+    """The second half of an updateUniformGridSIS step on a snapshot taken after the
+    integration: hash, sort, reorder, contact search, gather, SequentialImpulseSolver, and
+    computeGlobalAttributes with the (identity) step rotation."""
+    pos, pvel = _f32(state["pos"]), _f32(state["pvel"])
+    n = len(pos)
+    h = calc_hash(origin, cell, dims, pos)
+    sh, si = sort_pairs(h, np.arange(n, dtype=np.uint32))
+    cs, ce, sp, sv = reorder(sh, si, pos, pvel, int(np.prod(dims)))
+    cd, cb, cp = find_contacts_grid(origin, cell, dims, radius, rb_idx, sp, si, cs, ce)
+    contacts = gather_contacts(radius, restitution, rb_idx, state["cms"], state["vel"],
+                               state["ang"], state["rel"], cd, cb, cp)
+    vel, ang, a0, a1, a2 = sequential_impulse(contacts, state["cms"], state["vel"], state["ang"],
+                                              state["cur"], state["mass"], iterations,
+                                              ar_friction, rb_friction, gravity_y)
+    rel, ppos, ppvel, _ = global_attributes(state["cms"], vel, ang, state["quat"], rb_idx,
+                                            state["rel"])
+    return {"vel": vel, "ang": ang, "rel": rel, "pos": ppos, "pvel": ppvel,
+            "contacts": len(contacts["body1"]), "acc": a0}

@@ -139,3 +139,31 @@ def test_sequential_impulse_cube_on_ground(ctx):
     rv, rw, a0, _, _ = cpu.sequential_impulse(contacts, cms, vel, ang, ib, mass, iterations=it)
     assert np.array_equal(v, rv) and np.array_equal(acc[0], a0)
     assert abs(float(acc[0].sum()) - 1.0) < 1e-5
+
+
+def test_sis_steps_match_oracle(ctx):
+    """Steps of the sequential-impulse path: after each step's integration the device state is
+    snapshotted and the rest of the step (search, gather, solver, particle update) is run by
+    the oracle from it; the device's results must equal it bit for bit.  (The integration's
+    cosf / sinf are checked on their own, to 1e-5 relative.)"""
+    from diploma_thesis_b200 import scenes
+    from diploma_thesis_b200.sis import SISScene, ITERATIONS
+    sc = scenes.small_scene(4, nb_side=4, packed=True, r=1 / 128)
+    g = SISScene(ctx, sc, dt=1e-3, grid_log2=(5, 5, 5))
+    rb = sc.body_index()
+    dims = (32, 32, 32)
+    total = 0
+    for _ in range(4):
+        g.integrate()
+        before = g.state()
+        before["mass"] = sc.body_mass.astype(np.float32)
+        g.solve()
+        ctx.check()
+        after = g.state()
+        ref = cpu.sis_solve(before, rb, tuple(sc.box_min), 2 * np.float32(sc.radius), dims,
+                            sc.radius, gravity_y=g.params.gravity[1], iterations=ITERATIONS)
+        assert after["contacts"] == ref["contacts"]
+        total += ref["contacts"]
+        for k in ("vel", "ang", "rel", "pos", "pvel"):
+            assert np.array_equal(after[k], ref[k]), k
+    assert total > 500
