@@ -6,7 +6,8 @@
 Workload (default "pile"): the plain large pile -- 2,097,152 particles, 32,768 bodies of 64
 (cubes, rods, padded spheres), r = 1/512, 1 x 3 x 1 box, dt = 1e-4, k = 5e4, damping 0.02,
 shear 0.1, grid broad phase (256 x 512 x 256 wrapped cells of 2r).  "plain" is the 110,592-particle
-single scene (4,096 cubes, 128^3 grid).  Seeded synthetic scenes; no dataset exists.
+single scene (4,096 cubes, 128^3 grid); "sis" the reference's sequential-impulse update path
+(REFERENCE semantics) on 4,096 packed cubes.  Seeded synthetic scenes; no dataset exists.
 
 Metric: Mparticle-steps/s (whole job).  A step is one pass of the fused pipeline over the
 scene.  value: device-timed throughput with the scene resident in HBM (K graph replays
@@ -723,6 +724,59 @@ def run_lbvh(args):
     return 0
 
 
+def run_sis(args):
+    """The reference's default update path (updateUniformGridSIS) in REFERENCE semantics: a
+    packed 16^3 block of 4,096 cubes x 27 (110,592 particles, r = 1/256, 128^3 grid), every
+    cube in contact with its neighbours; per step the integration, the contact search, the
+    gather and 18 sequential-impulse sweeps, all on the device.  The CPU baseline is the
+    oracle's restatement of the same step (the reference's gather and solver are host loops;
+    kind "port"), one thread, one step."""
+    import torch
+    from diploma_thesis_b200 import api, scenes
+    from diploma_thesis_b200.sis import SISScene, ITERATIONS
+    torch.cuda.set_device(0)
+    ctx = api.Context(0)
+    sc = scenes.small_scene(4, nb_side=16, packed=True, r=1 / 256)
+    g = SISScene(ctx, sc, dt=1e-4, grid_log2=(7, 7, 7))
+    steps = max(1, min(args.steps, 20))
+    g.step(args.warmup)
+    torch.cuda.synchronize()
+    with ClockSampler(0) as clocks:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        g.step(steps)
+        b.record()
+        b.synchronize()
+    ms = a.elapsed_time(b) / steps
+    st = g.state()
+    ctx.check()
+    n = sc.num_particles
+    cpu = None
+    if not args.no_cpu:
+        from oracle import cpu as ocpu
+        before = dict(st)
+        before["mass"] = sc.body_mass.astype(np.float32)
+        t0 = time.perf_counter()
+        ocpu.sis_solve(before, sc.body_index(), tuple(sc.box_min), 2 * np.float32(sc.radius),
+                       (128, 128, 128), sc.radius, gravity_y=g.params.gravity[1],
+                       iterations=ITERATIONS)
+        cpu_s = time.perf_counter() - t0
+        cpu = {"value": n / cpu_s / 1e6, "unit": "Mparticle-steps/s", "cores": 1, "kind": "port",
+               "sample": "one step's contact search, gather, sequential-impulse sweeps and "
+                         "particle update of the same scene (oracle restatement, one thread)"}
+    print(json.dumps({
+        "metric": "Mparticle-steps/s (sequential-impulse path)", "value": n / ms / 1e3,
+        "unit": "Mparticle-steps/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "sequential-impulse path: 4,096 packed cubes x 27 (110,592 "
+                               "particles), r=1/256, grid 128^3, dt=1e-4, 18 sweeps, "
+                               "REFERENCE semantics",
+                   "contacts_per_step": st["contacts"], "timed": "eager stage calls, events"},
+        "cpu_baseline": cpu, "clocks": clocks.summary()}))
+    return 0
+
+
 def run_served(args):
     """Config 4: Poisson request stream (scenes of 1k-500k particles, cubes and rods, K in
     10..500) served with continuous batching under an HBM budget; the plain form serves the
@@ -785,7 +839,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh"],
+    ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh", "sis"],
                     default="pile")
     ap.add_argument("--lbvh-sizes", default="", help="lbvh: comma-separated point counts")
     ap.add_argument("--lbvh-reps", type=int, default=10, help="lbvh: timed repetitions")
@@ -808,6 +862,8 @@ def main(argv=None):
         return run_served(args)
     if args.workload == "lbvh":
         return run_lbvh(args)
+    if args.workload == "sis":
+        return run_sis(args)
     return run_ours(args)
 
 
