@@ -351,6 +351,25 @@ void FindAndHandleAugmentedRealityCollisionsUniformGridWrapper(
             "FindAndHandleAugmentedRealityCollisionsUniformGridWrapper");
 }
 
+// FindRigidBodyCollisionsUniformGridWrapper (Kernels/RB_UniformGridKernels.cu:844-874): the
+// deepest contact per particle.  The reference's debug colouring of colliding particles
+// (color) is not written.
+void FindRigidBodyCollisionsUniformGridWrapper(int* rbIndices, int* collidingRigidBodyIndex,
+                                               int* collidingParticleIndex,
+                                               float* contactDistance, float4* color,
+                                               float4* oldPos, uint* gridParticleIndex,
+                                               uint* cellStart, uint* cellEnd,
+                                               uint numParticles, SimParams params,
+                                               int numThreads) {
+  (void)color;
+  (void)numThreads;
+  ARC_CHECK(ar_find_contacts_grid(ARC_CTX, arsim_compat_detail::P(params), rbIndices,
+                                  (const float*)oldPos, gridParticleIndex, cellStart, cellEnd,
+                                  (int)numParticles, contactDistance, collidingRigidBodyIndex,
+                                  collidingParticleIndex, nullptr),
+            "FindRigidBodyCollisionsUniformGridWrapper");
+}
+
 void ReducePerParticleImpulses(int* rbIndices, float4* pLinearImpulse, float4* pAngularImpulse,
                                float4* rbVel, float4* rbAng, float* rbMass, glm::mat3* rbInertia,
                                int* particlesPerObject, int numRigidBodies, int numParticles,
