@@ -11,6 +11,8 @@
 // parallel: every body sees exactly the sequence of updates of the reference's loop, so the
 // results are the reference's bit for bit.  The level assignment is the same in every
 // iteration, since it depends only on which bodies each contact touches.
+#include <algorithm>
+
 #include "ar_glm.cuh"
 #include "ar_grid.cuh"
 #include "ar_internal.cuh"
@@ -206,83 +208,126 @@ __device__ __forceinline__ float clampf(float v, float lo, float hi) {
 
 // One contact's update, the reference's loop body.  The reference compares the float values
 // with double constants (abs(x) < 0.00001), so the comparisons are made in double here too.
-// What a contact's update reads apart from its bodies' velocities: its own data and
-// accumulated impulses (only this contact writes them) and its bodies' centres, masses and
-// inverse inertias (constant during the solve) -- loaded ahead of the contact's turn.
-struct ContactRec {
-  float4 normal, point, cm1, cm2;
-  int c, i1, i2;
-  float bias, m1, m2, a0, a1, a2;
-  float I1[9], I2[9];
+// A contact's geometry: everything in its update that does not depend on the velocities --
+// the lever arms, the effective mass mc (set to 1 below 1e-5, as the reference does), the two
+// tangent directions and their effective masses, and the friction bound.  It is the same in
+// every sweep, so it is computed once, with the reference's expressions, before the sweeps.
+struct Geometry {
+  float4 g0;  // p1, mc
+  float4 g1;  // p2, friction bound
+  float4 g2;  // t1, k1
+  float4 g3;  // t2, k2
 };
-__device__ __forceinline__ ContactRec load_contact(const Contacts& C, const Bodies& B, int c) {
-  ContactRec r;
-  r.c = c;
-  r.normal = C.normal[c];
-  r.point = C.point[c];
-  r.i1 = C.body1[c];
-  r.i2 = C.body2[c];
-  r.bias = C.bias[c];
-  r.a0 = C.acc_impulse[c];
-  r.a1 = C.acc_friction[c];
-  r.a2 = C.acc_friction2[c];
-  r.cm1 = B.cms[r.i1];
-  r.m1 = B.mass[r.i1];
-#pragma unroll
-  for (int k = 0; k < 9; ++k) r.I1[k] = B.inv_inertia[9 * r.i1 + k];
-  r.cm2 = make_float4(0.f, 0.f, 0.f, 0.f);
-  r.m2 = 1.f;
-#pragma unroll
-  for (int k = 0; k < 9; ++k) r.I2[k] = 0.f;
-  if (r.i2 >= 0) {
-    r.cm2 = B.cms[r.i2];
-    r.m2 = B.mass[r.i2];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) r.I2[k] = B.inv_inertia[9 * r.i2 + k];
-  }
-  return r;
-}
 
-__device__ void solve_contact(const ContactRec& R, const Contacts& C, const Bodies& B,
-                              float ar_friction, float rb_friction, float abs_gravity_y,
-                              float upper_bound) {
-  const int c = R.c;
-  const float3 n = f3(R.normal);
-  const float4 point = R.point;
-  const int i1 = R.i1, i2 = R.i2;
-  const float4 cm1 = R.cm1;
+__device__ Geometry contact_geometry(float3 n, float4 point, float4 cm1, float4 cm2,
+                                     const float* I1, const float* I2, float m1, float m2,
+                                     bool two_body, float ar_friction, float rb_friction,
+                                     float abs_gravity_y) {
   const float3 p1 = ar::mk3(point.x - cm1.x, point.y - cm1.y, point.z - cm1.z);
-  const float* I1 = R.I1;
-  const float m1 = R.m1;
-  float3 v1 = f3(B.vel[i1]), w1 = f3(B.ang[i1]);
-  if (i2 == -1) {
-    float mc = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n);
+  float3 p2 = ar::mk3(0.f, 0.f, 0.f);
+  float mc, bound, k1, k2;
+  float3 t1 = ar::mk3(1.f, 0.f, 0.f);
+  if (!two_body) {
+    mc = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n);
     if ((double)fabsf(mc) < 0.00001) mc = 1.f;
-    const float v_rel = dot3(add3(v1, cross3(w1, p1)), n);
-    float corrective = -(v_rel + R.bias) / mc;
-    float acc = R.a0;
-    float tmp = clampf(acc + corrective, 0.f, upper_bound);
-    corrective = tmp - acc;
-    C.acc_impulse[c] = tmp;
-    const float bound = ar_friction * mc * abs_gravity_y;
-    const float3 vel = add3(v1, cross3(w1, p1));
-    float3 t1 = ar::mk3(1.f, 0.f, 0.f);
+    bound = ar_friction * mc * abs_gravity_y;
     if ((double)fabsf(t1.x - n.x) < 0.0001) t1 = ar::mk3(0.f, 1.f, 0.f);
     else if ((double)fabsf(t1.x + n.x) < 0.0001) t1 = ar::mk3(0.f, 1.f, 0.f);
     t1 = gnormalize(sub3(t1, mul3(dot3(t1, n), n)));
-    const float k1 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1);
+    k1 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1);
+  } else {
+    p2 = ar::mk3(point.x - cm2.x, point.y - cm2.y, point.z - cm2.z);
+    mc = 1 / m1 + 1 / m2 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n) +
+         dot3(cross3(mv(I2, cross3(p2, n)), p2), n);
+    if ((double)fabsf(mc) < 0.00001) mc = 1.f;
+    bound = rb_friction * mc * abs_gravity_y;
+    if ((double)fabsf(t1.x - n.x) < 0.0001) t1 = ar::mk3(0.f, 1.f, 0.f);
+    t1 = gnormalize(sub3(t1, mul3(dot3(t1, n), n)));
+    k1 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1)) +
+         (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t1)), p2), t1));
+  }
+  const float3 t2 = gnormalize(cross3(t1, n));
+  if (!two_body)
+    k2 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2);
+  else
+    k2 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2)) +
+         (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t2)), p2), t2));
+  return Geometry{make_float4(p1.x, p1.y, p1.z, mc), make_float4(p2.x, p2.y, p2.z, bound),
+                  make_float4(t1.x, t1.y, t1.z, k1), make_float4(t2.x, t2.y, t2.z, k2)};
+}
+
+// Geometry of every contact (one thread per contact).
+__global__ void __launch_bounds__(256) sis_geometry_kernel(
+    Contacts C, Bodies B, const int* __restrict__ d_count, int capacity, float ar_friction,
+    float rb_friction, float abs_gravity_y, Geometry* __restrict__ geo) {
+  const int count = min(*d_count, capacity);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < count; c += gridDim.x * blockDim.x) {
+    const int i1 = C.body1[c], i2 = C.body2[c];
+    const bool two = i2 >= 0;
+    geo[c] = contact_geometry(f3(C.normal[c]), C.point[c], B.cms[i1],
+                              two ? B.cms[i2] : make_float4(0.f, 0.f, 0.f, 0.f),
+                              B.inv_inertia + 9 * i1, B.inv_inertia + 9 * (two ? i2 : i1),
+                              B.mass[i1], two ? B.mass[i2] : 1.f, two, ar_friction, rb_friction,
+                              abs_gravity_y);
+  }
+}
+
+// A contact in the solver's working order (by level): 11 float4 -- normal and bias, the four
+// geometry words, the two masses and body ids, the two inverse inertias -- so a thread block
+// can stage a window of them into shared memory with coalesced loads.
+constexpr int kRecWords = 11;
+__device__ __forceinline__ void pack_contact(const Contacts& C, const Bodies& B,
+                                             const Geometry* __restrict__ geo, int c,
+                                             float4* __restrict__ out) {
+  const int i1 = C.body1[c], i2 = C.body2[c];
+  const float4 n = C.normal[c];
+  const Geometry g = geo[c];
+  float I1[9], I2[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    I1[k] = B.inv_inertia[9 * i1 + k];
+    I2[k] = i2 >= 0 ? B.inv_inertia[9 * i2 + k] : 0.f;
+  }
+  out[0] = make_float4(n.x, n.y, n.z, C.bias[c]);
+  out[1] = g.g0;
+  out[2] = g.g1;
+  out[3] = g.g2;
+  out[4] = g.g3;
+  out[5] = make_float4(B.mass[i1], i2 >= 0 ? B.mass[i2] : 1.f, __int_as_float(i1),
+                       __int_as_float(i2));
+  out[6] = make_float4(I1[0], I1[1], I1[2], I1[3]);
+  out[7] = make_float4(I1[4], I1[5], I1[6], I1[7]);
+  out[8] = make_float4(I1[8], I2[0], I2[1], I2[2]);
+  out[9] = make_float4(I2[3], I2[4], I2[5], I2[6]);
+  out[10] = make_float4(I2[7], I2[8], 0.f, 0.f);
+}
+
+// One contact's update: the velocity-dependent part of the reference's loop body.  acc holds
+// the accumulated impulse and the two accumulated frictions.
+__device__ void solve_packed(const float4* __restrict__ r, float4* acc, const Bodies& B,
+                             float upper_bound) {
+  const float3 n = f3(r[0]);
+  const float bias = r[0].w;
+  const float3 p1 = f3(r[1]), t1 = f3(r[3]), t2 = f3(r[4]);
+  const float mc = r[1].w, bound = r[2].w, k1 = r[3].w, k2 = r[4].w;
+  const float m1 = r[5].x, m2 = r[5].y;
+  const int i1 = __float_as_int(r[5].z), i2 = __float_as_int(r[5].w);
+  const float I1[9] = {r[6].x, r[6].y, r[6].z, r[6].w, r[7].x, r[7].y, r[7].z, r[7].w, r[8].x};
+  const float4 a = *acc;
+  float3 v1 = f3(B.vel[i1]), w1 = f3(B.ang[i1]);
+  if (i2 == -1) {
+    const float3 vel = add3(v1, cross3(w1, p1));
+    const float v_rel = dot3(vel, n);
+    float corrective = -(v_rel + bias) / mc;
+    const float tmp = clampf(a.x + corrective, 0.f, upper_bound);
+    corrective = tmp - a.x;
     float cf1 = -dot3(vel, t1) / k1;
-    const float a1 = R.a1;
-    const float f1 = clampf(a1 + cf1, -bound, bound);
-    cf1 = f1 - a1;
-    C.acc_friction[c] = f1;
-    const float3 t2 = gnormalize(cross3(t1, n));
-    const float k2 = 1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2);
+    const float f1 = clampf(a.y + cf1, -bound, bound);
+    cf1 = f1 - a.y;
     float cf2 = -dot3(vel, t2) / k2;
-    const float a2 = R.a2;
-    const float f2 = clampf(a2 + cf2, -bound, bound);
-    cf2 = f2 - a2;
-    C.acc_friction2[c] = f2;
+    const float f2 = clampf(a.z + cf2, -bound, bound);
+    cf2 = f2 - a.z;
+    *acc = make_float4(tmp, f1, f2, 0.f);
     const float3 imp = add3(add3(mul3(corrective, n), mul3(cf1, t1)), mul3(cf2, t2));
     v1 = add3(v1, div3(imp, m1));
     w1 = add3(w1, mv(I1, cross3(p1, imp)));
@@ -290,35 +335,17 @@ __device__ void solve_contact(const ContactRec& R, const Contacts& C, const Bodi
     B.ang[i1] = make_float4(w1.x, w1.y, w1.z, 0.f);
     return;
   }
-  const float4 cm2 = R.cm2;
-  const float3 p2 = ar::mk3(point.x - cm2.x, point.y - cm2.y, point.z - cm2.z);
-  const float* I2 = R.I2;
-  const float m2 = R.m2;
+  const float3 p2 = f3(r[2]);
+  const float I2[9] = {r[8].y, r[8].z, r[8].w, r[9].x, r[9].y, r[9].z, r[9].w, r[10].x, r[10].y};
   float3 v2 = f3(B.vel[i2]), w2 = f3(B.ang[i2]);
-  float mc = 1 / m1 + 1 / m2 + dot3(cross3(mv(I1, cross3(p1, n)), p1), n) +
-             dot3(cross3(mv(I2, cross3(p2, n)), p2), n);
-  if ((double)fabsf(mc) < 0.00001) mc = 1.f;
   const float v_rel = dot3(add3(v1, cross3(w1, p1)), n) - dot3(add3(v2, cross3(w2, p2)), n);
-  float corrective = -(v_rel + R.bias) / mc;
-  const float acc = R.a0;
-  const float tmp = clampf(acc + corrective, 0.f, upper_bound);
-  corrective = tmp - acc;
-  C.acc_impulse[c] = tmp;
+  float corrective = -(v_rel + bias) / mc;
+  const float tmp = clampf(a.x + corrective, 0.f, upper_bound);
+  corrective = tmp - a.x;
   // friction is accumulated as the reference does, but (as there) not applied between bodies
-  const float bound = rb_friction * mc * abs_gravity_y;
   const float3 vel = add3(add3(add3(mul3(-1.f, v1), cross3(w1, p1)), v2), cross3(w2, p2));
-  float3 t1 = ar::mk3(1.f, 0.f, 0.f);
-  if ((double)fabsf(t1.x - n.x) < 0.0001) t1 = ar::mk3(0.f, 1.f, 0.f);
-  t1 = gnormalize(sub3(t1, mul3(dot3(t1, n), n)));
-  const float k1 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t1)), p1), t1)) +
-                   (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t1)), p2), t1));
-  const float cf1 = -dot3(vel, t1) / k1;
-  C.acc_friction[c] = clampf(R.a1 + cf1, -bound, bound);
-  const float3 t2 = gnormalize(cross3(t1, n));
-  const float k2 = (1 / m1 + dot3(cross3(mv(I1, cross3(p1, t2)), p1), t2)) +
-                   (1 / m2 + dot3(cross3(mv(I2, cross3(p2, t2)), p2), t2));
-  const float cf2 = -dot3(vel, t2) / k2;
-  C.acc_friction2[c] = clampf(R.a2 + cf2, -bound, bound);
+  *acc = make_float4(tmp, clampf(a.y + -dot3(vel, t1) / k1, -bound, bound),
+                     clampf(a.z + -dot3(vel, t2) / k2, -bound, bound), 0.f);
   const float3 imp = mul3(corrective, n);
   v1 = add3(v1, div3(imp, m1));
   w1 = add3(w1, mv(I1, cross3(p1, imp)));
@@ -330,47 +357,61 @@ __device__ void solve_contact(const ContactRec& R, const Contacts& C, const Bodi
   B.ang[i2] = make_float4(w2.x, w2.y, w2.z, 0.f);
 }
 
-constexpr int kSisThreads = 512;
+constexpr int kSisThreads = 256;
 constexpr int kLevelCap = 8192;  // level bounds kept in shared memory when there are fewer
-constexpr size_t kSisSmemMax = 200 * 1024;
+constexpr int kLevelChunk = 2048;  // body pairs staged per step of the level walk
+constexpr int kWinRecs = 256;      // contacts staged per window of a sweep
+constexpr size_t kSisSmemMax = 210 * 1024;  // dynamic; the kernel's static 16 KB stay below 227 KB
 
-// One block: levels (one thread walks the contacts in order), contacts bucketed by level,
-// then `iterations` sweeps, each solving the levels in order with a barrier between them.
-// kShared: the bodies' velocities and angular velocities (and the level bounds, when they
-// fit) live in shared memory for the sweeps, and each thread loads its contact of the next
-// level before the barrier that ends the current one.
-// Scratch: level[capacity], order[capacity], level_start[capacity + 2], last[num_bodies].
+// One block: levels (one thread walks the contacts in order), contacts bucketed by level and
+// packed in that order, then `iterations` sweeps, each solving the levels in order with a
+// barrier between them, a window of kWinRecs packed contacts staged in shared memory at a
+// time.  kShared: the bodies' velocities and angular velocities live in shared memory too.
+// Scratch: level[capacity], order[capacity], level_start[capacity + 2], last[num_bodies],
+// rec[capacity * kRecWords], accs[capacity].
 template <bool kShared>
 __global__ void __launch_bounds__(kSisThreads) sis_kernel(
-    Contacts C, Bodies B, const int* __restrict__ d_count, int capacity, int num_bodies,
-    int iterations, float ar_friction, float rb_friction, float abs_gravity_y, float upper_bound,
-    int* __restrict__ level, int* __restrict__ order, int* __restrict__ last,
-    int* __restrict__ level_start, int* __restrict__ err) {
-  extern __shared__ float4 s_body[];  // kShared: vel[num_bodies], ang[num_bodies], bounds
+    Contacts C, Bodies B, const Geometry* __restrict__ geo, const int* __restrict__ d_count,
+    int capacity, int num_bodies, int iterations, float upper_bound, int* __restrict__ level,
+    int* __restrict__ order, int* __restrict__ last, int* __restrict__ level_start,
+    float4* __restrict__ rec, float4* __restrict__ accs, int* __restrict__ err) {
+  // window records and accumulators, then (kShared) vel[num_bodies], ang[num_bodies], then
+  // the level bounds when they fit
+  extern __shared__ float4 s_mem[];
   __shared__ int s_levels;
   int count = *d_count;
   if (count > capacity) {
     if (threadIdx.x == 0) ar::raise_error(err, ar::kErrOverflow);
     count = capacity;
   }
-  int* lastp = kShared ? reinterpret_cast<int*>(s_body) : last;
+  int* lastp = kShared ? reinterpret_cast<int*>(s_mem + kWinRecs * (kRecWords + 1)) : last;
   for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) lastp[b] = 0;
   for (int l = threadIdx.x; l < count + 2; l += blockDim.x) level_start[l] = 0;
   __syncthreads();
-  if (threadIdx.x == 0) {
-    int top = 0;
-    for (int c = 0; c < count; ++c) {
-      const int b1 = C.body1[c], b2 = C.body2[c];
-      int l = lastp[b1];
-      if (b2 >= 0 && lastp[b2] > l) l = lastp[b2];
-      ++l;
-      level[c] = l;
-      lastp[b1] = l;
-      if (b2 >= 0) lastp[b2] = l;
-      if (l > top) top = l;
+  // levels: one thread walks the contacts in order; the block stages their body pairs in
+  // shared memory a chunk at a time, so the walk waits on global memory once per chunk
+  __shared__ int2 s_pair[kLevelChunk];
+  int top = 0;
+  for (int base = 0; base < count; base += kLevelChunk) {
+    const int m = min(kLevelChunk, count - base);
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+      s_pair[i] = make_int2(C.body1[base + i], C.body2[base + i]);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < m; ++i) {
+        const int b1 = s_pair[i].x, b2 = s_pair[i].y;
+        int l = lastp[b1];
+        if (b2 >= 0 && lastp[b2] > l) l = lastp[b2];
+        ++l;
+        level[base + i] = l;
+        lastp[b1] = l;
+        if (b2 >= 0) lastp[b2] = l;
+        if (l > top) top = l;
+      }
     }
-    s_levels = top;
+    __syncthreads();
   }
+  if (threadIdx.x == 0) s_levels = top;
   __syncthreads();
   const int levels = s_levels;
   // bucket by level: counts at level_start[l] (levels are 1..levels), exclusive scan (one
@@ -391,49 +432,59 @@ __global__ void __launch_bounds__(kSisThreads) sis_kernel(
   for (int c = threadIdx.x; c < count; c += blockDim.x)
     order[atomicAdd(level_start + level[c], 1)] = c;
   __syncthreads();
+  // contacts in level order, packed, with their accumulators
+  for (int p = threadIdx.x; p < count; p += blockDim.x) {
+    const int c = order[p];
+    pack_contact(C, B, geo, c, rec + (size_t)kRecWords * p);
+    accs[p] = make_float4(C.acc_impulse[c], C.acc_friction[c], C.acc_friction2[c], 0.f);
+  }
+  float4* s_win = s_mem;                          // window records
+  float4* s_acc = s_mem + kWinRecs * kRecWords;   // window accumulators
+  float4* s_bodies = s_acc + kWinRecs;
+  int* s_bounds = reinterpret_cast<int*>(s_bodies + (kShared ? 2 * num_bodies : 0));
   Bodies W = B;
   const int* bounds = level_start;
-  if (kShared) {
-    float4* sv = s_body;
-    float4* sa = s_body + num_bodies;
-    for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
-      sv[b] = B.vel[b];
-      sa[b] = B.ang[b];
-    }
-    if (levels + 1 <= kLevelCap) {
-      int* sb = reinterpret_cast<int*>(s_body + 2 * num_bodies);
-      for (int l = threadIdx.x; l <= levels; l += blockDim.x) sb[l] = level_start[l];
-      bounds = sb;
-    }
-    W.vel = sv;
-    W.ang = sa;
-    __syncthreads();
+  if (levels + 1 <= kLevelCap) {
+    for (int l = threadIdx.x; l <= levels; l += blockDim.x) s_bounds[l] = level_start[l];
+    bounds = s_bounds;
   }
-  const int tid = threadIdx.x;
-  // the thread's first contact of level l (later ones of a level wider than the block are
-  // loaded in turn)
-  auto first_of = [&](int l, ContactRec* r) {
-    const int i = bounds[l - 1] + tid;
-    if (i >= bounds[l]) return false;
-    *r = load_contact(C, B, order[i]);
-    return true;
-  };
-  for (int it = 0; it < iterations; ++it) {
-    ContactRec cur;
-    bool have = levels >= 1 && first_of(1, &cur);
-    for (int l = 1; l <= levels; ++l) {
-      ContactRec nxt;
-      const bool have_next = l < levels && first_of(l + 1, &nxt);
-      if (have) {
-        solve_contact(cur, C, W, ar_friction, rb_friction, abs_gravity_y, upper_bound);
-        for (int i = bounds[l - 1] + tid + (int)blockDim.x; i < bounds[l]; i += blockDim.x)
-          solve_contact(load_contact(C, B, order[i]), C, W, ar_friction, rb_friction,
-                        abs_gravity_y, upper_bound);
-      }
-      __syncthreads();
-      cur = nxt;
-      have = have_next;
+  if (kShared) {
+    for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
+      s_bodies[b] = B.vel[b];
+      s_bodies[num_bodies + b] = B.ang[b];
     }
+    W.vel = s_bodies;
+    W.ang = s_bodies + num_bodies;
+  }
+  __syncthreads();
+  // sweeps: windows of kWinRecs contacts staged in shared memory; inside a window the levels
+  // it covers are solved in order with a barrier after each (a level may span windows)
+  for (int it = 0; it < iterations; ++it) {
+    int l = 1;
+    for (int p0 = 0; p0 < count; p0 += kWinRecs) {
+      const int p1 = min(count, p0 + kWinRecs);
+      for (int j = threadIdx.x; j < (p1 - p0) * kRecWords; j += blockDim.x)
+        s_win[j] = rec[(size_t)kRecWords * p0 + j];
+      for (int j = threadIdx.x; j < p1 - p0; j += blockDim.x) s_acc[j] = accs[p0 + j];
+      __syncthreads();
+      while (l <= levels && bounds[l - 1] < p1) {
+        const int lo = max(p0, bounds[l - 1]), hi = min(p1, bounds[l]);
+        for (int p = lo + (int)threadIdx.x; p < hi; p += blockDim.x)
+          solve_packed(s_win + kRecWords * (p - p0), s_acc + (p - p0), W, upper_bound);
+        __syncthreads();
+        if (bounds[l] > p1) break;  // the level continues in the next window
+        ++l;
+      }
+      for (int j = threadIdx.x; j < p1 - p0; j += blockDim.x) accs[p0 + j] = s_acc[j];
+      __syncthreads();
+    }
+  }
+  for (int p = threadIdx.x; p < count; p += blockDim.x) {
+    const int c = order[p];
+    const float4 a = accs[p];
+    C.acc_impulse[c] = a.x;
+    C.acc_friction[c] = a.y;
+    C.acc_friction2[c] = a.z;
   }
   if (kShared) {
     for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
@@ -516,28 +567,39 @@ ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params, const 
       (num_bodies > 0 && (!cms4 || !vel4 || !ang4 || !cur_inv_inertia9 || !mass)))
     return AR_ERR_INVALID_ARG;
   if (capacity == 0 || num_bodies == 0 || iterations == 0) return AR_OK;
-  // scratch: level[capacity], order[capacity], level_start[capacity + 2], last[num_bodies]
+  // scratch: geometry[capacity] (64-byte aligned), then level[capacity], order[capacity],
+  // level_start[capacity + 2], last[num_bodies]
   const size_t words = 3 * (size_t)capacity + 2 + (size_t)num_bodies;
-  int* w = (int*)arh::scratch(ctx, sizeof(int) * words);
-  if (!w) return AR_ERR_OOM;
+  const size_t geo_bytes = sizeof(Geometry) * (size_t)capacity;
+  const size_t rec_bytes = sizeof(float4) * (size_t)capacity * (kRecWords + 1);
+  char* base = (char*)arh::scratch(ctx, geo_bytes + rec_bytes + sizeof(int) * words);
+  if (!base) return AR_ERR_OOM;
+  Geometry* geo = (Geometry*)base;
+  float4* rec = (float4*)(base + geo_bytes);
+  float4* accs = rec + (size_t)capacity * kRecWords;
+  int* w = (int*)(base + geo_bytes + rec_bytes);
   Contacts C{(const float4*)normal4, (const float4*)point4, body1, body2, bias, acc_impulse,
              acc_friction, acc_friction2};
   Bodies B{(const float4*)cms4, (float4*)vel4, (float4*)ang4, cur_inv_inertia9, mass};
-  // bodies' velocities in shared memory when they fit (with the level bounds)
-  const size_t smem = 32 * (size_t)num_bodies + 4 * (size_t)kLevelCap;
   cudaStream_t st = arh::stream(stream);
+  const unsigned gg = std::min(arh::grid_for(capacity, 256), (unsigned)ctx->num_sms * 8);
+  sis_geometry_kernel<<<gg, 256, 0, st>>>(C, B, d_count, capacity, params->ar_friction,
+                                          params->rb_friction, fabsf(params->gravity[1]), geo);
+  // window buffers and level bounds in shared memory; the bodies' velocities too when they fit
+  const size_t base_smem = sizeof(float4) * kWinRecs * (kRecWords + 1) + 4 * (size_t)kLevelCap;
+  const size_t smem = base_smem + 32 * (size_t)num_bodies;
   if (smem <= kSisSmemMax) {
     cudaFuncSetAttribute(sis_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kSisSmemMax);
+                         (int)smem);
     sis_kernel<true><<<1, kSisThreads, smem, st>>>(
-        C, B, d_count, capacity, num_bodies, iterations, params->ar_friction,
-        params->rb_friction, fabsf(params->gravity[1]), 100.f, w, w + capacity,
-        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, ctx->d_err);
+        C, B, geo, d_count, capacity, num_bodies, iterations, 100.f, w, w + capacity,
+        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, rec, accs, ctx->d_err);
   } else {
-    sis_kernel<false><<<1, kSisThreads, 0, st>>>(
-        C, B, d_count, capacity, num_bodies, iterations, params->ar_friction,
-        params->rb_friction, fabsf(params->gravity[1]), 100.f, w, w + capacity,
-        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, ctx->d_err);
+    cudaFuncSetAttribute(sis_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)base_smem);
+    sis_kernel<false><<<1, kSisThreads, base_smem, st>>>(
+        C, B, geo, d_count, capacity, num_bodies, iterations, 100.f, w, w + capacity,
+        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, rec, accs, ctx->d_err);
   }
   return arh::check_launch("ar_sequential_impulse");
 }
