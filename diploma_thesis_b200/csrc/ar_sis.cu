@@ -12,6 +12,7 @@
 // results are the reference's bit for bit.  The level assignment is the same in every
 // iteration, since it depends only on which bodies each contact touches.
 #include <algorithm>
+#include <climits>
 
 #include "ar_glm.cuh"
 #include "ar_grid.cuh"
@@ -27,7 +28,17 @@ __device__ __forceinline__ float3 f3(float4 a) { return ar::mk3(a.x, a.y, a.z); 
 __device__ __forceinline__ float3 add3(float3 a, float3 b) { return ar::add(a, b); }
 __device__ __forceinline__ float3 sub3(float3 a, float3 b) { return ar::sub(a, b); }
 __device__ __forceinline__ float3 mul3(float s, float3 a) { return ar::mk3(s * a.x, s * a.y, s * a.z); }
-__device__ __forceinline__ float3 div3(float3 a, float s) { return ar::mk3(a.x / s, a.y / s, a.z / s); }
+// x / y for the solver's updates.  A zero dividend over a finite non-zero divisor gives the
+// signed zero that IEEE division gives (sign = sign of x xor sign of y) without dividing;
+// bodies at rest make such quotients common, and the shortcut keeps them off the dependent
+// chain of the update.  Every other case is the division itself.
+__device__ __forceinline__ float qdiv(float x, float y) {
+  if (x == 0.f && isfinite(y) && y != 0.f) return signbit(y) ? -x : x;
+  return x / y;
+}
+__device__ __forceinline__ float3 qdiv3(float3 a, float s) {
+  return ar::mk3(qdiv(a.x, s), qdiv(a.y, s), qdiv(a.z, s));
+}
 // glm::normalize(vec3): v * inversesqrt(dot(v, v)), inversesqrt(x) = 1 / sqrt(x)
 __device__ __forceinline__ float3 gnormalize(float3 v) {
   const float inv = 1.0f / sqrtf(dot3(v, v));
@@ -272,13 +283,14 @@ __global__ void __launch_bounds__(256) sis_geometry_kernel(
   }
 }
 
-// A contact in the solver's working order (by level): 11 float4 -- normal and bias, the four
-// geometry words, the two masses and body ids, the two inverse inertias -- so a thread block
-// can stage a window of them into shared memory with coalesced loads.
+// A contact in the solver's working order: 11 float4 words -- normal and bias, the four
+// geometry words, the two masses and body ids, the two inverse inertias -- stored word-major
+// (word k of contact p at k * stride + p), so that a warp loading consecutive contacts reads
+// each word as one contiguous run.
 constexpr int kRecWords = 11;
 __device__ __forceinline__ void pack_contact(const Contacts& C, const Bodies& B,
                                              const Geometry* __restrict__ geo, int c,
-                                             float4* __restrict__ out) {
+                                             float4* __restrict__ out, size_t stride) {
   const int i1 = C.body1[c], i2 = C.body2[c];
   const float4 n = C.normal[c];
   const Geometry g = geo[c];
@@ -288,23 +300,23 @@ __device__ __forceinline__ void pack_contact(const Contacts& C, const Bodies& B,
     I1[k] = B.inv_inertia[9 * i1 + k];
     I2[k] = i2 >= 0 ? B.inv_inertia[9 * i2 + k] : 0.f;
   }
-  out[0] = make_float4(n.x, n.y, n.z, C.bias[c]);
-  out[1] = g.g0;
-  out[2] = g.g1;
-  out[3] = g.g2;
-  out[4] = g.g3;
-  out[5] = make_float4(B.mass[i1], i2 >= 0 ? B.mass[i2] : 1.f, __int_as_float(i1),
+  out[0 * stride] = make_float4(n.x, n.y, n.z, C.bias[c]);
+  out[1 * stride] = g.g0;
+  out[2 * stride] = g.g1;
+  out[3 * stride] = g.g2;
+  out[4 * stride] = g.g3;
+  out[5 * stride] = make_float4(B.mass[i1], i2 >= 0 ? B.mass[i2] : 1.f, __int_as_float(i1),
                        __int_as_float(i2));
-  out[6] = make_float4(I1[0], I1[1], I1[2], I1[3]);
-  out[7] = make_float4(I1[4], I1[5], I1[6], I1[7]);
-  out[8] = make_float4(I1[8], I2[0], I2[1], I2[2]);
-  out[9] = make_float4(I2[3], I2[4], I2[5], I2[6]);
-  out[10] = make_float4(I2[7], I2[8], 0.f, 0.f);
+  out[6 * stride] = make_float4(I1[0], I1[1], I1[2], I1[3]);
+  out[7 * stride] = make_float4(I1[4], I1[5], I1[6], I1[7]);
+  out[8 * stride] = make_float4(I1[8], I2[0], I2[1], I2[2]);
+  out[9 * stride] = make_float4(I2[3], I2[4], I2[5], I2[6]);
+  out[10 * stride] = make_float4(I2[7], I2[8], 0.f, 0.f);
 }
 
 // One contact's update: the velocity-dependent part of the reference's loop body.  acc holds
 // the accumulated impulse and the two accumulated frictions.
-__device__ void solve_packed(const float4* __restrict__ r, float4* acc, const Bodies& B,
+__device__ void solve_packed(const float4* r, float4* acc, const Bodies& B,
                              float upper_bound) {
   const float3 n = f3(r[0]);
   const float bias = r[0].w;
@@ -318,18 +330,18 @@ __device__ void solve_packed(const float4* __restrict__ r, float4* acc, const Bo
   if (i2 == -1) {
     const float3 vel = add3(v1, cross3(w1, p1));
     const float v_rel = dot3(vel, n);
-    float corrective = -(v_rel + bias) / mc;
+    float corrective = qdiv(-(v_rel + bias), mc);
     const float tmp = clampf(a.x + corrective, 0.f, upper_bound);
     corrective = tmp - a.x;
-    float cf1 = -dot3(vel, t1) / k1;
+    float cf1 = qdiv(-dot3(vel, t1), k1);
     const float f1 = clampf(a.y + cf1, -bound, bound);
     cf1 = f1 - a.y;
-    float cf2 = -dot3(vel, t2) / k2;
+    float cf2 = qdiv(-dot3(vel, t2), k2);
     const float f2 = clampf(a.z + cf2, -bound, bound);
     cf2 = f2 - a.z;
     *acc = make_float4(tmp, f1, f2, 0.f);
     const float3 imp = add3(add3(mul3(corrective, n), mul3(cf1, t1)), mul3(cf2, t2));
-    v1 = add3(v1, div3(imp, m1));
+    v1 = add3(v1, qdiv3(imp, m1));
     w1 = add3(w1, mv(I1, cross3(p1, imp)));
     B.vel[i1] = make_float4(v1.x, v1.y, v1.z, 0.f);
     B.ang[i1] = make_float4(w1.x, w1.y, w1.z, 0.f);
@@ -339,114 +351,258 @@ __device__ void solve_packed(const float4* __restrict__ r, float4* acc, const Bo
   const float I2[9] = {r[8].y, r[8].z, r[8].w, r[9].x, r[9].y, r[9].z, r[9].w, r[10].x, r[10].y};
   float3 v2 = f3(B.vel[i2]), w2 = f3(B.ang[i2]);
   const float v_rel = dot3(add3(v1, cross3(w1, p1)), n) - dot3(add3(v2, cross3(w2, p2)), n);
-  float corrective = -(v_rel + bias) / mc;
+  float corrective = qdiv(-(v_rel + bias), mc);
   const float tmp = clampf(a.x + corrective, 0.f, upper_bound);
   corrective = tmp - a.x;
   // friction is accumulated as the reference does, but (as there) not applied between bodies
   const float3 vel = add3(add3(add3(mul3(-1.f, v1), cross3(w1, p1)), v2), cross3(w2, p2));
-  *acc = make_float4(tmp, clampf(a.y + -dot3(vel, t1) / k1, -bound, bound),
-                     clampf(a.z + -dot3(vel, t2) / k2, -bound, bound), 0.f);
+  *acc = make_float4(tmp, clampf(a.y + qdiv(-dot3(vel, t1), k1), -bound, bound),
+                     clampf(a.z + qdiv(-dot3(vel, t2), k2), -bound, bound), 0.f);
   const float3 imp = mul3(corrective, n);
-  v1 = add3(v1, div3(imp, m1));
+  v1 = add3(v1, qdiv3(imp, m1));
   w1 = add3(w1, mv(I1, cross3(p1, imp)));
   B.vel[i1] = make_float4(v1.x, v1.y, v1.z, 0.f);
   B.ang[i1] = make_float4(w1.x, w1.y, w1.z, 0.f);
-  v2 = sub3(v2, div3(imp, m2));
+  v2 = sub3(v2, qdiv3(imp, m2));
   w2 = sub3(w2, mv(I2, cross3(p2, imp)));
   B.vel[i2] = make_float4(v2.x, v2.y, v2.z, 0.f);
   B.ang[i2] = make_float4(w2.x, w2.y, w2.z, 0.f);
 }
 
-constexpr int kSisThreads = 256;
-constexpr int kLevelCap = 8192;  // level bounds kept in shared memory when there are fewer
+constexpr int kSisThreads = 320;   // the sweep block
+constexpr int kLevelCap = 8192;    // level runs kept in shared memory up to this many levels
 constexpr int kLevelChunk = 2048;  // body pairs staged per step of the level walk
-constexpr int kWinRecs = 256;      // contacts staged per window of a sweep
-constexpr size_t kSisSmemMax = 210 * 1024;  // dynamic; the kernel's static 16 KB stay below 227 KB
+constexpr int kLayoutThreads = 1024;
+constexpr size_t kSisSmemMax = 220 * 1024;   // the sweep block's dynamic shared memory
+constexpr size_t kWalkSmemMax = 200 * 1024;  // the walk's (its static 16 KB stay below 227 KB)
+// The schedule's header in scratch memory: levels, shift, contact count.
+enum { kHdrLevels = 0, kHdrShift = 1, kHdrCount = 2, kHdrWords = 4 };
 
-// One block: levels (one thread walks the contacts in order), contacts bucketed by level and
-// packed in that order, then `iterations` sweeps, each solving the levels in order with a
-// barrier between them, a window of kWinRecs packed contacts staged in shared memory at a
-// time.  kShared: the bodies' velocities and angular velocities live in shared memory too.
-// Scratch: level[capacity], order[capacity], level_start[capacity + 2], last[num_bodies],
-// rec[capacity * kRecWords], accs[capacity].
+// Schedule.  Each contact gets a level: 1 + the highest level among earlier contacts on either
+// of its bodies.  Sweep s solves level b at step b + s * shift of one schedule, where shift
+// exceeds the span of levels that any body's contacts cover.  Then no step holds two contacts
+// of one body (two items of one step from sweeps s < s' on body x would need levels of x at
+// least shift apart), and each body's updates come in the reference's order: within a sweep
+// by level, and the last of sweep s (at step <= first + span + s * shift) before the first of
+// sweep s + 1.  Every update therefore reads exactly the values the reference's loop gives it,
+// while consecutive sweeps overlap.  Step l covers the levels b congruent to l (mod shift)
+// with max(1, l - (iterations - 1) shift) <= b <= min(levels, l), so the contacts are packed
+// by (level mod shift, level) and each step's contacts are one contiguous run.
+
+// Levels (one thread walks the contacts in order, the block stages their body pairs in shared
+// memory a chunk at a time), each body's first and last level, the span and the shift.
+// kShared: the walk's last / first levels live in shared memory.
 template <bool kShared>
-__global__ void __launch_bounds__(kSisThreads) sis_kernel(
-    Contacts C, Bodies B, const Geometry* __restrict__ geo, const int* __restrict__ d_count,
-    int capacity, int num_bodies, int iterations, float upper_bound, int* __restrict__ level,
-    int* __restrict__ order, int* __restrict__ last, int* __restrict__ level_start,
-    float4* __restrict__ rec, float4* __restrict__ accs, int* __restrict__ err) {
-  // window records and accumulators, then (kShared) vel[num_bodies], ang[num_bodies], then
-  // the level bounds when they fit
-  extern __shared__ float4 s_mem[];
-  __shared__ int s_levels;
+__global__ void __launch_bounds__(256) sis_levels_kernel(
+    const int32_t* __restrict__ body1, const int32_t* __restrict__ body2,
+    const int* __restrict__ d_count, int capacity, int num_bodies, int* __restrict__ level,
+    int* __restrict__ last, int* __restrict__ first, int* __restrict__ hdr,
+    int* __restrict__ err) {
+  extern __shared__ int s_walk[];
+  __shared__ int2 s_pair[kLevelChunk];
+  __shared__ int s_span;
   int count = *d_count;
   if (count > capacity) {
     if (threadIdx.x == 0) ar::raise_error(err, ar::kErrOverflow);
     count = capacity;
   }
-  int* lastp = kShared ? reinterpret_cast<int*>(s_mem + kWinRecs * (kRecWords + 1)) : last;
-  for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) lastp[b] = 0;
-  for (int l = threadIdx.x; l < count + 2; l += blockDim.x) level_start[l] = 0;
+  int* lastp = kShared ? s_walk : last;
+  int* firstp = kShared ? s_walk + num_bodies : first;
+  for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
+    lastp[b] = 0;
+    firstp[b] = 0;
+  }
+  if (threadIdx.x == 0) s_span = 0;
   __syncthreads();
-  // levels: one thread walks the contacts in order; the block stages their body pairs in
-  // shared memory a chunk at a time, so the walk waits on global memory once per chunk
-  __shared__ int2 s_pair[kLevelChunk];
   int top = 0;
   for (int base = 0; base < count; base += kLevelChunk) {
     const int m = min(kLevelChunk, count - base);
     for (int i = threadIdx.x; i < m; i += blockDim.x)
-      s_pair[i] = make_int2(C.body1[base + i], C.body2[base + i]);
+      s_pair[i] = make_int2(body1[base + i], body2[base + i]);
     __syncthreads();
     if (threadIdx.x == 0) {
       for (int i = 0; i < m; ++i) {
         const int b1 = s_pair[i].x, b2 = s_pair[i].y;
-        int l = lastp[b1];
-        if (b2 >= 0 && lastp[b2] > l) l = lastp[b2];
-        ++l;
+        const int u = lastp[b1], v = b2 >= 0 ? lastp[b2] : 0;
+        const int l = max(u, v) + 1;
         level[base + i] = l;
         lastp[b1] = l;
-        if (b2 >= 0) lastp[b2] = l;
-        if (l > top) top = l;
+        if (u == 0) firstp[b1] = l;
+        if (b2 >= 0) {
+          lastp[b2] = l;
+          if (v == 0) firstp[b2] = l;
+        }
+        top = max(top, l);
       }
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0) s_levels = top;
-  __syncthreads();
-  const int levels = s_levels;
-  // bucket by level: counts at level_start[l] (levels are 1..levels), exclusive scan (one
-  // thread; levels <= count), scatter with the starts as cursors -- afterwards level l occupies
-  // [level_start[l - 1], level_start[l]) with level_start[0] = 0.  The order inside a level is
-  // free: its contacts share no body.
-  for (int c = threadIdx.x; c < count; c += blockDim.x) atomicAdd(level_start + level[c], 1);
+  int span = 0;
+  for (int b = threadIdx.x; b < num_bodies; b += blockDim.x)
+    if (firstp[b] > 0) span = max(span, lastp[b] - firstp[b]);
+  atomicMax(&s_span, span);
   __syncthreads();
   if (threadIdx.x == 0) {
-    int run = 0;
-    for (int l = 1; l <= levels; ++l) {
-      const int v = level_start[l];
-      level_start[l] = run;
-      run += v;
-    }
+    hdr[kHdrLevels] = top;
+    hdr[kHdrShift] = max(2, s_span + 1);
+    hdr[kHdrCount] = count;
   }
+}
+
+// Level sizes (run[l].y, zeroed before).
+__global__ void __launch_bounds__(256) sis_sizes_kernel(const int* __restrict__ level,
+                                                        const int* __restrict__ hdr,
+                                                        int2* __restrict__ run) {
+  const int count = hdr[kHdrCount];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < count; c += gridDim.x * blockDim.x)
+    atomicAdd(&run[level[c]].y, 1);
+}
+
+// Position of level l in (level mod shift, level) order: class 0 (shift, 2 shift, ...) first,
+// then classes 1 .. shift - 1; with levels = Q shift + R, class r >= 1 holds Q + (r <= R)
+// levels, so it starts at r Q + min(r - 1, R).
+__device__ __forceinline__ int layout_index(int l, int shift, int q, int rem) {
+  const int r = l % shift;
+  return r == 0 ? l / shift - 1 : r * q + min(r - 1, rem) + (l - r) / shift;
+}
+
+// Lays the level runs out: tmp[layout_index(l)] = size of level l, an exclusive scan of tmp,
+// then run[l] = (start, start).  tmp holds `levels` ints.
+__global__ void __launch_bounds__(kLayoutThreads) sis_layout_kernel(const int* __restrict__ hdr,
+                                                                    int2* __restrict__ run,
+                                                                    int* __restrict__ tmp) {
+  __shared__ int s_warp[kLayoutThreads / 32];
+  __shared__ int s_carry;
+  const int levels = hdr[kHdrLevels], shift = hdr[kHdrShift];
+  const int q = levels / shift, rem = levels % shift;
+  for (int l = 1 + threadIdx.x; l <= levels; l += blockDim.x)
+    tmp[layout_index(l, shift, q, rem)] = run[l].y;
+  if (threadIdx.x == 0) s_carry = 0;
   __syncthreads();
-  for (int c = threadIdx.x; c < count; c += blockDim.x)
-    order[atomicAdd(level_start + level[c], 1)] = c;
-  __syncthreads();
-  // contacts in level order, packed, with their accumulators
-  for (int p = threadIdx.x; p < count; p += blockDim.x) {
-    const int c = order[p];
-    pack_contact(C, B, geo, c, rec + (size_t)kRecWords * p);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int base = 0; base < levels; base += blockDim.x) {
+    const int j = base + threadIdx.x;
+    const int v = j < levels ? tmp[j] : 0;
+    int x = v;  // inclusive warp scan
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, d);
+      if (lane >= d) x += y;
+    }
+    if (lane == 31) s_warp[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+      int w = lane < (int)(blockDim.x >> 5) ? s_warp[lane] : 0;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, w, d);
+        if (lane >= d) w += y;
+      }
+      s_warp[lane] = w;  // inclusive over warps
+    }
+    __syncthreads();
+    const int carry = s_carry;
+    const int excl = carry + (warp > 0 ? s_warp[warp - 1] : 0) + x - v;
+    if (j < levels) tmp[j] = excl;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) s_carry = excl + v;
+    __syncthreads();
+  }
+  for (int l = 1 + threadIdx.x; l <= levels; l += blockDim.x) {
+    const int start = tmp[layout_index(l, shift, q, rem)];
+    run[l] = make_int2(start, start);
+  }
+}
+
+// Each contact takes the next slot of its level's run (the order inside a level is free: its
+// contacts share no body) and is packed there with its accumulators; order[p] = contact.
+// Afterwards level l occupies [run[l].y, run[l].x).
+__global__ void __launch_bounds__(256) sis_pack_kernel(Contacts C, Bodies B,
+                                                       const Geometry* __restrict__ geo,
+                                                       const int* __restrict__ level,
+                                                       const int* __restrict__ hdr,
+                                                       int capacity, int2* __restrict__ run,
+                                                       int* __restrict__ order,
+                                                       float4* __restrict__ rec,
+                                                       float4* __restrict__ accs) {
+  const int count = hdr[kHdrCount];
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < count; c += gridDim.x * blockDim.x) {
+    const int p = atomicAdd(&run[level[c]].x, 1);
+    order[p] = c;
+    pack_contact(C, B, geo, c, rec + p, (size_t)capacity);
     accs[p] = make_float4(C.acc_impulse[c], C.acc_friction[c], C.acc_friction2[c], 0.f);
   }
-  float4* s_win = s_mem;                          // window records
-  float4* s_acc = s_mem + kWinRecs * kRecWords;   // window accumulators
-  float4* s_bodies = s_acc + kWinRecs;
-  int* s_bounds = reinterpret_cast<int*>(s_bodies + (kShared ? 2 * num_bodies : 0));
+}
+
+// The accumulated impulses back to the caller's arrays, in contact order.
+__global__ void __launch_bounds__(256) sis_writeback_kernel(Contacts C,
+                                                            const int* __restrict__ hdr,
+                                                            const int* __restrict__ order,
+                                                            const float4* __restrict__ accs) {
+  const int count = hdr[kHdrCount];
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < count; p += gridDim.x * blockDim.x) {
+    const int c = order[p];
+    const float4 a = accs[p];
+    C.acc_impulse[c] = a.x;
+    C.acc_friction[c] = a.y;
+    C.acc_friction2[c] = a.z;
+  }
+}
+
+// A packed contact and its accumulators, held in registers.
+struct Item {
+  float4 r[kRecWords];
+  float4 acc;
+  int p;  // packed index, -1: none
+};
+
+__device__ __forceinline__ void load_item(const float4* rec, size_t stride, const float4* accs,
+                                          int p, Item& it) {
+  it.p = p;
+  if (p < 0) return;
+#pragma unroll
+  for (int k = 0; k < kRecWords; ++k) it.r[k] = __ldcg(rec + k * stride + p);
+  it.acc = __ldcg(accs + p);
+}
+
+// The per-sweep levels lo, lo + shift, ..., hi that one step of the schedule covers, advanced
+// one step at a time without division.
+struct StepRange {
+  int lo, hi;  // the step has contacts while lo <= hi
+  int step;
+  __device__ void advance(int levels, int iterations, int shift) {
+    ++step;
+    // the largest level <= min(step, levels) congruent to step
+    if (++hi > levels) hi -= shift;
+    // the smallest level >= max(1, step - (iterations - 1) shift) congruent to step
+    if (step - 1 < iterations * shift) {
+      if (++lo > shift) lo -= shift;
+    } else {
+      ++lo;
+    }
+  }
+};
+
+// The sweeps, in one block: the steps are solved in order with a barrier between them; each
+// thread loads its item of the next step (record and accumulators, from L2) while it solves
+// the current one, which is safe because an item's accumulators were last written
+// shift >= 2 steps earlier.  kShared: the bodies' velocities and angular velocities live in
+// shared memory.
+template <bool kShared>
+__global__ void __launch_bounds__(kSisThreads) sis_sweep_kernel(
+    Bodies B, const int* __restrict__ hdr, int capacity, int num_bodies, int iterations,
+    float upper_bound, const int2* __restrict__ run, const float4* __restrict__ rec,
+    float4* __restrict__ accs) {
+  // (kShared) vel[num_bodies], ang[num_bodies], then the level runs when they fit
+  extern __shared__ float4 s_mem[];
+  const int levels = hdr[kHdrLevels], shift = hdr[kHdrShift];
+  float4* s_bodies = s_mem;
+  int2* s_run = reinterpret_cast<int2*>(s_bodies + (kShared ? 2 * num_bodies : 0));
   Bodies W = B;
-  const int* bounds = level_start;
+  const int2* runs = run;
   if (levels + 1 <= kLevelCap) {
-    for (int l = threadIdx.x; l <= levels; l += blockDim.x) s_bounds[l] = level_start[l];
-    bounds = s_bounds;
+    for (int l = threadIdx.x; l <= levels; l += blockDim.x) s_run[l] = run[l];
+    runs = s_run;
   }
   if (kShared) {
     for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
@@ -457,34 +613,41 @@ __global__ void __launch_bounds__(kSisThreads) sis_kernel(
     W.ang = s_bodies + num_bodies;
   }
   __syncthreads();
-  // sweeps: windows of kWinRecs contacts staged in shared memory; inside a window the levels
-  // it covers are solved in order with a barrier after each (a level may span windows)
-  for (int it = 0; it < iterations; ++it) {
-    int l = 1;
-    for (int p0 = 0; p0 < count; p0 += kWinRecs) {
-      const int p1 = min(count, p0 + kWinRecs);
-      for (int j = threadIdx.x; j < (p1 - p0) * kRecWords; j += blockDim.x)
-        s_win[j] = rec[(size_t)kRecWords * p0 + j];
-      for (int j = threadIdx.x; j < p1 - p0; j += blockDim.x) s_acc[j] = accs[p0 + j];
-      __syncthreads();
-      while (l <= levels && bounds[l - 1] < p1) {
-        const int lo = max(p0, bounds[l - 1]), hi = min(p1, bounds[l]);
-        for (int p = lo + (int)threadIdx.x; p < hi; p += blockDim.x)
-          solve_packed(s_win + kRecWords * (p - p0), s_acc + (p - p0), W, upper_bound);
-        __syncthreads();
-        if (bounds[l] > p1) break;  // the level continues in the next window
-        ++l;
+  if (levels > 0) {
+    const int steps = levels + (iterations - 1) * shift;  // fits in int: checked by the host
+    StepRange nr{1, 1, 1};  // step 1 covers level 1 of sweep 0 only
+    int next_lo = runs[1].y, next_hi = runs[1].x;
+    Item nxt;
+    load_item(rec, capacity, accs,
+              next_lo + (int)threadIdx.x < next_hi ? next_lo + (int)threadIdx.x : -1, nxt);
+    for (int step = 1; step <= steps; ++step) {
+      const Item cur = nxt;
+      const int lo = next_lo, hi = next_hi;
+      if (step < steps) {
+        nr.advance(levels, iterations, shift);
+        next_lo = next_hi = 0;
+        if (nr.lo <= nr.hi) {
+          next_lo = runs[nr.lo].y;
+          next_hi = runs[nr.hi].x;
+        }
+        const int p = next_lo + (int)threadIdx.x;
+        load_item(rec, capacity, accs, p < next_hi ? p : -1, nxt);
       }
-      for (int j = threadIdx.x; j < p1 - p0; j += blockDim.x) accs[p0 + j] = s_acc[j];
+      if (cur.p >= 0) {
+        float4 a = cur.acc;
+        solve_packed(cur.r, &a, W, upper_bound);
+        accs[cur.p] = a;
+        // items beyond one per thread
+        for (int p = lo + (int)(threadIdx.x + blockDim.x); p < hi; p += blockDim.x) {
+          Item more;
+          load_item(rec, capacity, accs, p, more);
+          a = more.acc;
+          solve_packed(more.r, &a, W, upper_bound);
+          accs[p] = a;
+        }
+      }
       __syncthreads();
     }
-  }
-  for (int p = threadIdx.x; p < count; p += blockDim.x) {
-    const int c = order[p];
-    const float4 a = accs[p];
-    C.acc_impulse[c] = a.x;
-    C.acc_friction[c] = a.y;
-    C.acc_friction2[c] = a.z;
   }
   if (kShared) {
     for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
@@ -567,17 +730,29 @@ ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params, const 
       (num_bodies > 0 && (!cms4 || !vel4 || !ang4 || !cur_inv_inertia9 || !mass)))
     return AR_ERR_INVALID_ARG;
   if (capacity == 0 || num_bodies == 0 || iterations == 0) return AR_OK;
-  // scratch: geometry[capacity] (64-byte aligned), then level[capacity], order[capacity],
-  // level_start[capacity + 2], last[num_bodies]
-  const size_t words = 3 * (size_t)capacity + 2 + (size_t)num_bodies;
+  // the schedule has at most capacity + (iterations - 1) (capacity + 1) steps, counted in int
+  if ((long long)iterations * ((long long)capacity + 1) > INT_MAX) {
+    arh::set_error("iterations x (capacity + 1) must stay below 2^31");
+    return AR_ERR_INVALID_ARG;
+  }
+  // scratch: geometry[capacity] (64-byte aligned), records (word-major) and accumulators,
+  // level runs run[capacity + 1], the schedule header, then level[capacity], order[capacity],
+  // last[num_bodies], first[num_bodies]
   const size_t geo_bytes = sizeof(Geometry) * (size_t)capacity;
   const size_t rec_bytes = sizeof(float4) * (size_t)capacity * (kRecWords + 1);
-  char* base = (char*)arh::scratch(ctx, geo_bytes + rec_bytes + sizeof(int) * words);
+  const size_t run_bytes = sizeof(int2) * ((size_t)capacity + 1);
+  const size_t words = kHdrWords + 2 * (size_t)capacity + 2 * (size_t)num_bodies;
+  char* base = (char*)arh::scratch(ctx, geo_bytes + rec_bytes + run_bytes + sizeof(int) * words);
   if (!base) return AR_ERR_OOM;
   Geometry* geo = (Geometry*)base;
   float4* rec = (float4*)(base + geo_bytes);
   float4* accs = rec + (size_t)capacity * kRecWords;
-  int* w = (int*)(base + geo_bytes + rec_bytes);
+  int2* run = (int2*)(base + geo_bytes + rec_bytes);
+  int* hdr = (int*)(base + geo_bytes + rec_bytes + run_bytes);
+  int* level = hdr + kHdrWords;
+  int* order = level + capacity;
+  int* last = order + capacity;
+  int* first = last + num_bodies;
   Contacts C{(const float4*)normal4, (const float4*)point4, body1, body2, bias, acc_impulse,
              acc_friction, acc_friction2};
   Bodies B{(const float4*)cms4, (float4*)vel4, (float4*)ang4, cur_inv_inertia9, mass};
@@ -585,22 +760,38 @@ ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params, const 
   const unsigned gg = std::min(arh::grid_for(capacity, 256), (unsigned)ctx->num_sms * 8);
   sis_geometry_kernel<<<gg, 256, 0, st>>>(C, B, d_count, capacity, params->ar_friction,
                                           params->rb_friction, fabsf(params->gravity[1]), geo);
-  // window buffers and level bounds in shared memory; the bodies' velocities too when they fit
-  const size_t base_smem = sizeof(float4) * kWinRecs * (kRecWords + 1) + 4 * (size_t)kLevelCap;
+  cudaMemsetAsync(run, 0, run_bytes, st);
+  // levels: the walk's last / first levels in shared memory when they fit
+  const size_t walk_smem = 8 * (size_t)num_bodies;
+  if (walk_smem <= kWalkSmemMax) {
+    cudaFuncSetAttribute(sis_levels_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)walk_smem);
+    sis_levels_kernel<true><<<1, 256, walk_smem, st>>>(body1, body2, d_count, capacity,
+                                                      num_bodies, level, last, first, hdr,
+                                                      ctx->d_err);
+  } else {
+    sis_levels_kernel<false><<<1, 256, 0, st>>>(body1, body2, d_count, capacity, num_bodies,
+                                               level, last, first, hdr, ctx->d_err);
+  }
+  sis_sizes_kernel<<<gg, 256, 0, st>>>(level, hdr, run);
+  sis_layout_kernel<<<1, kLayoutThreads, 0, st>>>(hdr, run, order);
+  sis_pack_kernel<<<gg, 256, 0, st>>>(C, B, geo, level, hdr, capacity, run, order, rec, accs);
+  // sweeps: level runs in shared memory; the bodies' velocities too when they fit
+  const size_t base_smem = sizeof(int2) * (size_t)kLevelCap;
   const size_t smem = base_smem + 32 * (size_t)num_bodies;
   if (smem <= kSisSmemMax) {
-    cudaFuncSetAttribute(sis_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(sis_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)smem);
-    sis_kernel<true><<<1, kSisThreads, smem, st>>>(
-        C, B, geo, d_count, capacity, num_bodies, iterations, 100.f, w, w + capacity,
-        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, rec, accs, ctx->d_err);
+    sis_sweep_kernel<true><<<1, kSisThreads, smem, st>>>(B, hdr, capacity, num_bodies,
+                                                         iterations, 100.f, run, rec, accs);
   } else {
-    cudaFuncSetAttribute(sis_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaFuncSetAttribute(sis_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)base_smem);
-    sis_kernel<false><<<1, kSisThreads, base_smem, st>>>(
-        C, B, geo, d_count, capacity, num_bodies, iterations, 100.f, w, w + capacity,
-        w + 3 * (size_t)capacity + 2, w + 2 * (size_t)capacity, rec, accs, ctx->d_err);
+    sis_sweep_kernel<false><<<1, kSisThreads, base_smem, st>>>(B, hdr, capacity, num_bodies,
+                                                               iterations, 100.f, run, rec,
+                                                               accs);
   }
+  sis_writeback_kernel<<<gg, 256, 0, st>>>(C, hdr, order, accs);
   return arh::check_launch("ar_sequential_impulse");
 }
 
