@@ -389,8 +389,17 @@ enum { kHdrLevels = 0, kHdrShift = 1, kHdrCount = 2, kHdrWords = 4 };
 // with max(1, l - (iterations - 1) shift) <= b <= min(levels, l), so the contacts are packed
 // by (level mod shift, level) and each step's contacts are one contiguous run.
 
-// Levels (one thread walks the contacts in order, the block stages their body pairs in shared
-// memory a chunk at a time), each body's first and last level, the span and the shift.
+// Levels, each body's first and last level, the span and the shift.  The block stages the
+// contacts' body pairs in shared memory a chunk at a time and warp 0 walks them in order, a run
+// at a time: a run is up to 32 consecutive contacts on one first body A (the gather emits each
+// body's contacts together).  Inside a run, with x_j the last level of contact j's other body
+// before the run, level_j = 1 + max(level_{j-1}, x_j): A's last level is the previous
+// contact's, and an other body met earlier in the same run was last touched at a level no
+// higher than level_{j-1}.  Unrolled, level_j = j + 1 + max(last level of A, max_{i<=j}
+// (x_i - i)), a prefix maximum over the warp's lanes.  A body's last level is then the level
+// of its last contact in the run (atomicMax), its first level the level of its first contact
+// when it had none before (atomicMin).  Any order of contacts is walked correctly; short runs
+// only leave lanes idle.
 // kShared: the walk's last / first levels live in shared memory.
 template <bool kShared>
 __global__ void __launch_bounds__(256) sis_levels_kernel(
@@ -410,36 +419,55 @@ __global__ void __launch_bounds__(256) sis_levels_kernel(
   int* firstp = kShared ? s_walk + num_bodies : first;
   for (int b = threadIdx.x; b < num_bodies; b += blockDim.x) {
     lastp[b] = 0;
-    firstp[b] = 0;
+    firstp[b] = INT_MAX;
   }
   if (threadIdx.x == 0) s_span = 0;
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   int top = 0;
   for (int base = 0; base < count; base += kLevelChunk) {
     const int m = min(kLevelChunk, count - base);
     for (int i = threadIdx.x; i < m; i += blockDim.x)
       s_pair[i] = make_int2(body1[base + i], body2[base + i]);
     __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int i = 0; i < m; ++i) {
-        const int b1 = s_pair[i].x, b2 = s_pair[i].y;
-        const int u = lastp[b1], v = b2 >= 0 ? lastp[b2] : 0;
-        const int l = max(u, v) + 1;
-        level[base + i] = l;
-        lastp[b1] = l;
-        if (u == 0) firstp[b1] = l;
-        if (b2 >= 0) {
-          lastp[b2] = l;
-          if (v == 0) firstp[b2] = l;
+    if (threadIdx.x < 32) {
+      for (int i = 0; i < m;) {  // one run (cut at 32 contacts and at the chunk's end)
+        const int j = i + lane;
+        const int2 pr = j < m ? s_pair[j] : make_int2(-1, -1);
+        const int a = __shfl_sync(0xffffffffu, pr.x, 0);
+        const uint32_t off = ~__ballot_sync(0xffffffffu, pr.x == a);
+        const int k = off ? __ffs(off) - 1 : 32;  // contacts in the run (lane 0 is one)
+        const bool in = lane < k;
+        const int b = in && pr.y >= 0 && pr.y != a ? pr.y : -1;  // a self pair touches A only
+        const int x = b >= 0 ? lastp[b] : 0;
+        const int a_last = lastp[a];
+        int y = in ? x - lane : INT_MIN / 2;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+          const int t = __shfl_up_sync(0xffffffffu, y, d);
+          if (lane >= d) y = max(y, t);
         }
-        top = max(top, l);
+        const int l = lane + 1 + max(a_last, y);
+        if (in) level[base + j] = l;
+        if (b >= 0) {
+          atomicMax(lastp + b, l);
+          if (x == 0) atomicMin(firstp + b, l);
+        }
+        const int run_last = __shfl_sync(0xffffffffu, l, k - 1);
+        if (lane == 0) {
+          lastp[a] = run_last;
+          if (a_last == 0) firstp[a] = l;
+        }
+        top = max(top, run_last);
+        i += k;
+        __syncwarp();
       }
     }
     __syncthreads();
   }
   int span = 0;
   for (int b = threadIdx.x; b < num_bodies; b += blockDim.x)
-    if (firstp[b] > 0) span = max(span, lastp[b] - firstp[b]);
+    if (firstp[b] != INT_MAX) span = max(span, lastp[b] - firstp[b]);
   atomicMax(&s_span, span);
   __syncthreads();
   if (threadIdx.x == 0) {
