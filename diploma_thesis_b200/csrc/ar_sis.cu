@@ -10,7 +10,9 @@
 // level among earlier contacts on either of its bodies -- and one level at a time is solved in
 // parallel: every body sees exactly the sequence of updates of the reference's loop, so the
 // results are the reference's bit for bit.  The level assignment is the same in every
-// iteration, since it depends only on which bodies each contact touches.
+// iteration, since it depends only on which bodies each contact touches, and the iterations
+// are laid onto one schedule in which each starts before the previous one ends (see the
+// schedule notes above sis_levels_kernel).
 #include <algorithm>
 #include <climits>
 

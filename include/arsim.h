@@ -420,7 +420,10 @@ AR_API ar_status ar_gather_contacts(ar_ctx* ctx, const ar_sim_params* params, in
  * contacts, body2 == -1, whose impulse includes friction; rb_friction for body pairs, whose
  * applied impulse is the normal part only, as in the reference); body velocities and angular
  * velocities updated in place.  Bit-identical to the sequential loop: contacts that share no
- * body are solved together, one dependency level at a time, in one thread block. */
+ * body are solved together, one dependency level at a time, in one thread block, and later
+ * sweeps start before earlier ones end wherever no body is shared (each body still sees the
+ * loop's order of updates).  iterations x (capacity + 1) must stay below 2^31
+ * (AR_ERR_INVALID_ARG otherwise). */
 AR_API ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params,
                                        const int32_t* d_count, int capacity,
                                        const float* normal4, const float* point4,
