@@ -133,6 +133,66 @@ def test_sequential_impulse_matches_oracle(ctx):
     assert np.abs(rv - vel).max() > 1e-3  # the impulses did something
 
 
+def _synthetic_contacts(rng, nb, pairs):
+    """Random bodies and one contact per (body1, body2) pair (body2 = -1: a one-body contact)."""
+    k = len(pairs)
+    cms = np.zeros((nb, 4), np.float32)
+    cms[:, :3] = rng.uniform(0, 1, (nb, 3))
+    vel = np.zeros((nb, 4), np.float32)
+    vel[:, :3] = rng.normal(0, 0.1, (nb, 3))
+    ang = np.zeros((nb, 4), np.float32)
+    ang[:, :3] = rng.normal(0, 0.5, (nb, 3))
+    ib = np.zeros((nb, 9), np.float32)
+    ib[:, [0, 4, 8]] = rng.uniform(10, 100, (nb, 3))
+    mass = rng.uniform(0.5, 2, nb).astype(np.float32)
+    b1 = np.array([a for a, _ in pairs], np.int32).reshape(k)
+    b2 = np.array([b for _, b in pairs], np.int32).reshape(k)
+    nrm = rng.normal(0, 1, (k, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    point = np.zeros((k, 4), np.float32)
+    point[:, :3] = cms[b1, :3] + rng.normal(0, 0.01, (k, 3))
+    contacts = {"normal": np.concatenate([nrm, np.zeros((k, 1))], 1).astype(np.float32),
+                "point": point, "body1": b1, "body2": b2,
+                "bias": rng.normal(0, 0.05, k).astype(np.float32)}
+    return contacts, cms, vel, ang, ib, mass
+
+
+def _schedule_case(name, rng):
+    if name == "disjoint":  # 1,200 contacts in one level: more than one per thread
+        return 2400, [(2 * i, 2 * i + 1) for i in range(1200)]
+    if name == "chain":  # few bodies, long dependency chains, one-body contacts among them
+        pairs = []
+        for i in range(120):
+            pairs += [(0, 1), (1, 2)] + ([(0, -1)] if i % 3 == 0 else [])
+        return 3, pairs
+    if name in ("random", "runs"):  # random bodies; "runs" groups them by first body
+        b1 = rng.integers(0, 300, 4000)
+        b2 = (b1 + rng.integers(1, 300, 4000)) % 300
+        b2[rng.random(4000) < 0.1] = -1
+        pairs = list(zip(b1.tolist(), b2.tolist()))
+        return 300, sorted(pairs, key=lambda p: p[0]) if name == "runs" else pairs
+    return 2, [(0, 1)]  # "single": one level
+
+
+@pytest.mark.parametrize("name,iterations", [("disjoint", 3), ("chain", 5), ("random", 7),
+                                             ("runs", 2), ("runs", 18), ("single", 1),
+                                             ("single", 4)])
+def test_sequential_impulse_schedules(ctx, name, iterations):
+    """Contact lists that stress the solver's schedule (one level wider than the block, long
+    chains, random order, runs on one body, a single contact): the overlapped sweeps equal the
+    sequential loop bit for bit."""
+    rng = np.random.default_rng(sum(name.encode()))
+    nb, pairs = _schedule_case(name, rng)
+    contacts, cms, vel, ang, ib, mass = _synthetic_contacts(rng, nb, pairs)
+    gv, gw, gacc = _solve_gpu(ctx, contacts, cms, vel, ang, ib, mass, iterations)
+    rv, rw, a0, a1, a2 = cpu.sequential_impulse(contacts, cms, vel, ang, ib, mass,
+                                                iterations=iterations)
+    assert np.array_equal(gv, rv) and np.array_equal(gw, rw)
+    for got, want in zip(gacc, (a0, a1, a2)):
+        assert np.array_equal(got, want)
+    assert np.abs(rv - vel).max() > 0
+
+
 def test_sequential_impulse_cube_on_ground(ctx):
     contacts, cms, vel, ang, ib, mass, it = cube_on_ground()
     v, w, acc = _solve_gpu(ctx, contacts, cms, vel, ang, ib, mass, it)
