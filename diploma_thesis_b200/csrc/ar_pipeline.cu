@@ -425,14 +425,43 @@ __global__ void __launch_bounds__(256) bvh_build_kernel(Lcp lcp, int n,
   ar_lbvh::karras_node(i, n, lcp, is_leaf, left, right, parent, min_r, max_r);
 }
 
+// Bottom-up refit (kernelConstructInternalNodesSoA, BVHSource/BVHSoAKernels.cu:148-176) from
+// one leaf whose box is already in its parent's slot (ar_lbvh::refit_climb): the second thread
+// to reach a node merges the two child boxes held in the node (mergeBounds,
+// BVHAuxiliary.cuh:83-94) and stores the result, with the merged body tag, into the node's slot
+// in its parent, then climbs on.  Release / acquire through the arrival counter; boxes through
+// L2.
+__device__ __forceinline__ void refit_from_leaf(int i, int n, const int32_t* __restrict__ left,
+                                                const int32_t* __restrict__ parent,
+                                                WideNode* nodes, int* __restrict__ counters) {
+  auto children = [&](int node, ar_lbvh::Box6* a, ar_lbvh::Box6* b) {
+    const float4* c = nodes[node - n].c;
+    const float4 a0 = __ldcg(c), a1 = __ldcg(c + 1), b0 = __ldcg(c + 2), b1 = __ldcg(c + 3);
+    *a = ar_lbvh::Box6{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y};
+    *b = ar_lbvh::Box6{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y};
+  };
+  auto store = [&](int node, const ar_lbvh::Box6& m) {
+    if (node == n) return;  // the root's box is not stored anywhere
+    const int pn = __ldg(parent + node);
+    // both children have arrived, so their tags are visible like their boxes
+    const int* w = node_ints(nodes, node - n);
+    const int tl = __ldcg(w + 7), tr = __ldcg(w + 15);
+    put_child(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1,
+              make_float4(m.lx, m.ly, m.lz, m.hx), make_float2(m.hy, m.hz), node,
+              tl == tr ? tl : -1);
+  };
+  ar_lbvh::refit_climb(i, n, parent, counters, children, store);
+}
+
 // Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
-// state; the leaf box (position +/- r) goes into its parent's slot; leaf flags and ranges.
+// state; the leaf box (position +/- r) goes into its parent's slot, and the thread climbs from
+// there (the refit); leaf flags and ranges.
 __global__ void __launch_bounds__(256) bvh_leaves_kernel(
     const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
     const uint32_t* __restrict__ svals, const int32_t* __restrict__ left,
     const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
     WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
-    int32_t* __restrict__ max_r) {
+    int32_t* __restrict__ max_r, int* __restrict__ counters) {
   ar::pdl_wait();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const int g = (int)__ldg(svals + k);
@@ -451,6 +480,7 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
       put_child(nodes, pn - nt, __ldg(left + pn) == k ? 0 : 1,
                 make_float4(p.x - rr, p.y - rr, p.z - rr, p.x + rr), make_float2(p.y + rr, p.z + rr),
                 k, S.boff + b);
+      refit_from_leaf(k, nt, left, parent, nodes, counters);  // the climb starts right here
     }
     is_leaf[k] = 1;
     min_r[k] = k;
@@ -486,39 +516,6 @@ __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
     node = parent[node];
   }
   roots[s] = node;
-}
-
-// Bottom-up refit (kernelConstructInternalNodesSoA, BVHSource/BVHSoAKernels.cu:148-176): one
-// thread per leaf climbs; the second thread to reach a node merges the two child boxes held in
-// the node (mergeBounds, BVHAuxiliary.cuh:83-94) and stores the result into the node's slot in
-// its parent.  Release / acquire through the arrival counter; boxes through L2.
-// One thread per leaf (ar_lbvh::refit_climb): a node's two child boxes are in its own wide node
-// (leaf boxes written by the leaves kernel); each merged box goes into the node's slot in its
-// parent.
-__global__ void __launch_bounds__(256) bvh_refit_kernel(int n, const int32_t* __restrict__ left,
-                                                        const int32_t* __restrict__ parent,
-                                                        WideNode* nodes,
-                                                        int* __restrict__ counters) {
-  ar::pdl_wait();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || n < 2) return;
-  auto children = [&](int node, ar_lbvh::Box6* a, ar_lbvh::Box6* b) {
-    const float4* c = nodes[node - n].c;
-    const float4 a0 = __ldcg(c), a1 = __ldcg(c + 1), b0 = __ldcg(c + 2), b1 = __ldcg(c + 3);
-    *a = ar_lbvh::Box6{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y};
-    *b = ar_lbvh::Box6{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y};
-  };
-  auto store = [&](int node, const ar_lbvh::Box6& m) {
-    if (node == n) return;  // the root's box is not stored anywhere
-    const int pn = __ldg(parent + node);
-    // both children have arrived, so their tags are visible like their boxes
-    const int* w = node_ints(nodes, node - n);
-    const int tl = __ldcg(w + 7), tr = __ldcg(w + 15);
-    put_child(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1,
-              make_float4(m.lx, m.ly, m.lz, m.hx), make_float2(m.hy, m.hz), node,
-              tl == tr ? tl : -1);
-  };
-  ar_lbvh::refit_climb(i, n, parent, counters, children, store);
 }
 
 // DEM gather through the scene's subtree in the reference's visit order
@@ -994,12 +991,12 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
       arh::launch_pdl(bvh_build_kernel<ar_lbvh::Lcp64Scene>, gb, dim3(256), 0, st,
           ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
           B->right, B->parent, B->min_r, B->max_r, B->nodes);
-    arh::launch_pdl(bvh_leaves_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, ns, nt,
-        B->svals, B->left, B->parent, B->spos, B->svel, B->nodes, B->is_leaf, B->min_r, B->max_r);
+    // one thread per leaf: each climbs after storing its leaf
+    arh::launch_pdl(bvh_leaves_kernel, dim3(arh::grid_for(nt, 256)), dim3(256), 0, st, B->d_table,
+        B->d_pscene, ns, nt, B->svals, B->left, B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
+        B->min_r, B->max_r, B->counters);
     arh::launch_pdl(bvh_roots_kernel, dim3(arh::grid_for(ns, 128)), dim3(128), 0, st, B->d_poff, ns,
         nt, B->parent, B->min_r, B->max_r, B->roots);
-    arh::launch_pdl(bvh_refit_kernel, dim3(arh::grid_for(nt, 256)), dim3(256), 0, st, nt, B->left,
-        B->parent, B->nodes, B->counters);
     mark(4);
     arh::launch_pdl(bvh_collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), 0, st, B->d_table,
         B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots, B->pforce, ctx->d_err);
