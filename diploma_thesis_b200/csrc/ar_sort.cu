@@ -6,8 +6,9 @@
 //   * each CTA takes the next tile index from an atomic counter, so every earlier tile is
 //     already running or finished (look-back always makes progress);
 //   * warps rank their items stably: the lanes holding the same digit are found with one
-//     match.any per item (items are visited in input order: warp w owns a contiguous
-//     sub-range, item j of lane l is element j*32 + l);
+//     match.any per item (8-bit digits) or one ballot per digit bit (9-bit digits); items are
+//     visited in input order: warp w owns a contiguous sub-range, item j of lane l is element
+//     j*32 + l;
 //   * per digit, the tile count is published, earlier tiles are looked back through (eight
 //     status words per round trip) until an inclusive prefix is found, and the tile's own
 //     inclusive prefix is published; the keys are staged and the value loads issued before
@@ -131,14 +132,24 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
     key[j] = g < n ? keys_in[g] : (K)~(K)0;
   }
 
-  // stable warp multi-split: peers = lanes holding the same digit (one match.any; the
-  // ballot-per-bit form measured slower)
+  // stable warp multi-split: peers = lanes holding the same digit -- one match.any per item for
+  // 8-bit digits, one ballot per digit bit for 9-bit ones (each measured faster there)
   const uint32_t lt = (1u << lane) - 1;
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
     const long g = wbase + j * 32 + lane;
     const uint32_t dj = g < n ? digit_of(key[j], shift, mask) : kDigits - 1;
-    const uint32_t peers = __match_any_sync(0xffffffffu, dj);
+    uint32_t peers;
+    if constexpr (kBits <= 8) {
+      peers = __match_any_sync(0xffffffffu, dj);
+    } else {
+      peers = 0xffffffffu;
+      for (int b = 0; b < kBits; ++b) {
+        const uint32_t bit = (dj >> b) & 1u;
+        const uint32_t m = __ballot_sync(0xffffffffu, bit);
+        peers &= bit ? m : ~m;
+      }
+    }
     uint32_t before = __popc(peers & lt);
     int leader = __ffs(peers) - 1;
     __syncwarp();
