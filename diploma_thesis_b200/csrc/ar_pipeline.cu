@@ -1015,8 +1015,9 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
       dim3(std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4)), dim3(kK1Threads),
       0, st, B->d_table, B->d_pscene, nt, B->keys, (uint32_t*)B->sort_ws, B->plan, B->d_step);
   mark(2);
+  // cell keys in particle order: a warp's keys share few digits, so match.any ranking
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
-                                  st, B->sort_ws, B->cap_sort, true);
+                                  st, B->sort_ws, B->cap_sort, true, true);
   if (s != AR_OK) return s;
   mark(3);
   arh::launch_pdl(scatter_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, nt, B->skeys,

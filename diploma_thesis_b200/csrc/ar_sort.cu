@@ -6,7 +6,7 @@
 //   * each CTA takes the next tile index from an atomic counter, so every earlier tile is
 //     already running or finished (look-back always makes progress);
 //   * warps rank their items stably: the lanes holding the same digit are found with one
-//     match.any per item (8-bit digits) or one ballot per digit bit (9-bit digits); items are
+//     ballot per digit bit, or (on request, 8-bit digits) one match.any per item; items are
 //     visited in input order: warp w owns a contiguous sub-range, item j of lane l is element
 //     j*32 + l;
 //   * per digit, the tile count is published, earlier tiles are looked back through (eight
@@ -97,7 +97,11 @@ struct PassSmem {
 };
 
 // One digit pass of at most kBits bits (kBits 9 only with kT 512: one digit per thread).
-template <class K, int kT, int kBits>
+// kMatch: rank 8-bit digits with one warp match.any per item instead of a ballot per digit
+// bit.  Which is faster depends on the keys: match.any wins when a warp's items hold few
+// distinct digits (cell keys of particles in input order), ballots win when they hold many
+// (Morton codes).
+template <class K, int kT, int kBits, bool kMatch = false>
 __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) onesweep_kernel(
     const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int n, int shift, int bits,
@@ -132,15 +136,14 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
     key[j] = g < n ? keys_in[g] : (K)~(K)0;
   }
 
-  // stable warp multi-split: peers = lanes holding the same digit -- one match.any per item for
-  // 8-bit digits, one ballot per digit bit for 9-bit ones (each measured faster there)
+  // stable warp multi-split: peers = lanes holding the same digit
   const uint32_t lt = (1u << lane) - 1;
 #pragma unroll
   for (int j = 0; j < kItems; ++j) {
     const long g = wbase + j * 32 + lane;
     const uint32_t dj = g < n ? digit_of(key[j], shift, mask) : kDigits - 1;
     uint32_t peers;
-    if constexpr (kBits <= 8) {
+    if constexpr (kMatch && kBits <= 8) {
       peers = __match_any_sync(0xffffffffu, dj);
     } else {
       peers = 0xffffffffu;
@@ -284,7 +287,7 @@ template <class K>
 void launch_passes(const ar_sort::Plan& plan, int n, const K* keys_in, const uint32_t* vals_in,
                    K* keys_out, uint32_t* vals_out, K* tmp_keys, uint32_t* tmp_vals,
                    const uint32_t* hist, uint32_t* status, uint32_t* counters, int* err,
-                   cudaStream_t st) {
+                   cudaStream_t st, bool match_rank) {
   const long status_tiles = ((long)n + tile_items(n) - 1) / tile_items(n);
   const K* src_k = keys_in;
   const uint32_t* src_v = vals_in;
@@ -302,13 +305,13 @@ void launch_passes(const ar_sort::Plan& plan, int n, const K* keys_in, const uin
           sizeof(PassSmem<K, 512, 9>), st, src_k, src_v, dk, dv, n, shift, bits, base, stat,
           counters + p, err);
     else if (kt == 512)
-      arh::launch_pdl(onesweep_kernel<K, 512, 8>, dim3(tiles), dim3(512),
-          sizeof(PassSmem<K, 512, 8>), st, src_k, src_v, dk, dv, n, shift, bits, base, stat,
-          counters + p, err);
+      arh::launch_pdl(match_rank ? onesweep_kernel<K, 512, 8, true> : onesweep_kernel<K, 512, 8>,
+          dim3(tiles), dim3(512), sizeof(PassSmem<K, 512, 8>), st, src_k, src_v, dk, dv, n, shift,
+          bits, base, stat, counters + p, err);
     else
-      arh::launch_pdl(onesweep_kernel<K, 256, 8>, dim3(tiles), dim3(256),
-          sizeof(PassSmem<K, 256, 8>), st, src_k, src_v, dk, dv, n, shift, bits, base, stat,
-          counters + p, err);
+      arh::launch_pdl(match_rank ? onesweep_kernel<K, 256, 8, true> : onesweep_kernel<K, 256, 8>,
+          dim3(tiles), dim3(256), sizeof(PassSmem<K, 256, 8>), st, src_k, src_v, dk, dv, n, shift,
+          bits, base, stat, counters + p, err);
     src_k = dk;
     src_v = dv;
   }
@@ -320,7 +323,8 @@ void launch_passes(const ar_sort::Plan& plan, int n, const K* keys_in, const uin
 template <class K>
 ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* keys_out,
                     uint32_t* vals_out, int n, int begin_bit, int end_bit, cudaStream_t st,
-                    void* ws, size_t ws_bytes, bool external_hist = false) {
+                    void* ws, size_t ws_bytes, bool external_hist = false,
+                    bool match_rank = false) {
   const ar_sort::Plan plan = ar_sort::make_plan(begin_bit, end_bit);
   const int passes = plan.passes;
   ar_sort::Layout L = ar_sort::layout(n, sizeof(K), passes);
@@ -346,7 +350,7 @@ ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* k
   }
   arh::launch_pdl(hist_scan_kernel, dim3(1), dim3(32 * ar_sort::kMaxPasses), 0, st, hist, passes);
   launch_passes<K>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
-                   status, counters, err, st);
+                   status, counters, err, st, match_rank);
   return arh::check_launch("radix sort");
 }
 
@@ -389,9 +393,9 @@ __global__ void iota_kernel(uint32_t* v, int n) {
 }
 
 // Dynamic shared-memory opt-in of every digit-pass instantiation (current device).
-template <class K, int kT, int kBits>
+template <class K, int kT, int kBits, bool kMatch = false>
 cudaError_t set_pass_attribute() {
-  return cudaFuncSetAttribute(onesweep_kernel<K, kT, kBits>,
+  return cudaFuncSetAttribute(onesweep_kernel<K, kT, kBits, kMatch>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize,
                               (int)sizeof(PassSmem<K, kT, kBits>));
 }
@@ -399,6 +403,8 @@ cudaError_t set_pass_attributes() {
   cudaError_t e = set_pass_attribute<uint32_t, 256, 8>();
   if (e == cudaSuccess) e = set_pass_attribute<uint32_t, 512, 8>();
   if (e == cudaSuccess) e = set_pass_attribute<uint32_t, 512, 9>();
+  if (e == cudaSuccess) e = set_pass_attribute<uint32_t, 256, 8, true>();
+  if (e == cudaSuccess) e = set_pass_attribute<uint32_t, 512, 8, true>();
   if (e == cudaSuccess) e = set_pass_attribute<uint64_t, 256, 8>();
   if (e == cudaSuccess) e = set_pass_attribute<uint64_t, 512, 8>();
   if (e == cudaSuccess) e = set_pass_attribute<uint64_t, 512, 9>();
@@ -478,10 +484,11 @@ void iota(uint32_t* v, int n, cudaStream_t st) {
 
 ar_status sort_u32(ar_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in,
                    uint32_t* keys_out, uint32_t* vals_out, int n, int begin_bit, int end_bit,
-                   cudaStream_t st, void* ws, size_t ws_bytes, bool external_hist) {
+                   cudaStream_t st, void* ws, size_t ws_bytes, bool external_hist,
+                   bool match_rank) {
   if (n == 0) return AR_OK;
   return sort_impl<uint32_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
-                             st, ws, ws_bytes, external_hist);
+                             st, ws, ws_bytes, external_hist, match_rank);
 }
 
 ar_status sort_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in,
@@ -579,7 +586,7 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
       hist);
   arh::launch_pdl(hist_scan_kernel, dim3(1), dim3(32 * ar_sort::kMaxPasses), 0, st, hist, passes);
   launch_passes<uint32_t>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
-                          status, counters, (int*)d_status, st);
+                          status, counters, (int*)d_status, st, false);
   return arh::check_launch("allocation-free sort");
 }
 

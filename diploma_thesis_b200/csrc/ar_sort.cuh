@@ -52,10 +52,12 @@ void iota(uint32_t* v, int n, cudaStream_t st);
 
 // Sort u32 (key, value) pairs by bits [begin_bit, end_bit) into keys_out/vals_out using the
 // caller's workspace (at least layout(n, 4, passes).total bytes).  vals_in may be null
-// (identity).  Device errors go to ctx->d_err.
+// (identity).  Device errors go to ctx->d_err.  match_rank: rank 8-bit digits with warp
+// match.any (faster when a warp's keys share few digits, as cell keys in particle order do).
 ar_status sort_u32(ar_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in,
                    uint32_t* keys_out, uint32_t* vals_out, int n, int begin_bit, int end_bit,
-                   cudaStream_t st, void* ws, size_t ws_bytes, bool external_hist = false);
+                   cudaStream_t st, void* ws, size_t ws_bytes, bool external_hist = false,
+                   bool match_rank = false);
 
 // The same for u64 keys (histogram computed inside; workspace layout(n, 8, passes)).
 ar_status sort_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in,
