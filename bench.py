@@ -42,6 +42,8 @@ FALLBACK_HBM_GBS = 6650.0
 # in L2 are not counted).  P = sort passes, ppb = particles per body.  A step runs: clear |
 # keys | sort | scatter + cell table | collide | body (sums, integration).
 STAGES = ["clear", "keys", "sort", "scatter", "collide", "body"]
+# Steps each configuration runs (c2 pile: 500; c0 plain scene: 1,000).
+CONFIG_STEPS = {"pile": 500, "plain": 1000}
 BODY_STATE = 16 * 4  # pos, quat, vel, angvel (float4 each)
 
 
@@ -132,12 +134,23 @@ class ClockSampler:
         self.device = device
         self.proc = None
         self.lines: list[str] = []
+        self.first = 0           # index of the first sample at or after mark_start()
+        self.last = None         # one past the last sample before mark_end()
+
+    def mark_start(self):
+        self.first = len(self.lines)
+
+    def mark_end(self):
+        self.last = len(self.lines)
+
+    def samples_since_start(self) -> int:
+        return len(self.lines) - self.first
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
+                 "--format=csv,noheader,nounits", "-lms", "20"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -160,7 +173,7 @@ class ClockSampler:
     def summary(self) -> dict:
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in self.lines[self.first:self.last]:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -232,21 +245,6 @@ def job_rate(world: int, units_per_rank: int, steps: int, ms: float) -> float:
 
 
 # ---- CPU legs (oracle) ---------------------------------------------------------------------
-def reference_sample(scene, bodies: int):
-    """The first `bodies` bodies of the scene as its own scene (bounded CPU sample)."""
-    from diploma_thesis_b200.scenes import Scene
-    off = scene.body_offsets
-    n = int(off[bodies])
-    return Scene(radius=scene.radius, box_min=scene.box_min, box_max=scene.box_max,
-                 body_pos=scene.body_pos[:bodies].copy(), body_quat=scene.body_quat[:bodies].copy(),
-                 body_vel=scene.body_vel[:bodies].copy(), body_angvel=scene.body_angvel[:bodies].copy(),
-                 body_mass=scene.body_mass[:bodies].copy(),
-                 body_inv_inertia=scene.body_inv_inertia[:bodies].copy(),
-                 body_offsets=off[: bodies + 1].copy(), particle_rel=scene.particle_rel[:n].copy(),
-                 gravity=scene.gravity, dt=scene.dt, spring=scene.spring, damping=scene.damping,
-                 shear=scene.shear, grid_log2=scene.grid_log2, cell_size=scene.cell_size)
-
-
 class ReferenceCPUStep:
     """One updateUniformGridDEM step (RigidBodies/UniformGridUpdate.cpp:939-999) made of the
     reference's own kernel bodies run on the host cores: GPUintegratorKernel,
@@ -256,13 +254,12 @@ class ReferenceCPUStep:
     (impulse = force * dt, velocity increment g * dt)."""
 
     def __init__(self, scene, grid):
-        from diploma_thesis_b200.api import sim_params
         from oracle import ref
         self.ref = ref
         self.s = scene
         origin, cell, dims = grid
         dt = scene.dt
-        self.prm = sim_params(scene.radius, origin, cell[0], dims, scene.spring * dt,
+        self.prm = ref.sim_params(scene.radius, origin, cell[0], dims, scene.spring * dt,
                               scene.damping * dt, scene.shear * dt, scene.attraction * dt,
                               gravity=tuple(g * dt for g in scene.gravity), w_damping=1.0)
         self.ncell = int(np.prod(dims))
@@ -318,18 +315,24 @@ class ReferenceCPUStepBVH(ReferenceCPUStep):
             pf, pt, self.st["vel"], self.st["ang"], s.body_mass, s.body_inv_inertia, self.counts)
 
 
-def cpu_reference_rate(scene, grid, target_s: float, steps: int | None = None,
-                       broadphase: str = "grid"):
-    """Particle-steps/s of the reference CPU step on a bounded sample; returns
-    (rate, cores, kind, sample description, steps run, seconds)."""
+REFERENCE_SEMANTICS = ("the reference's own step (REFERENCE semantics: DEM impulses applied as "
+                       "velocity increments, gravity added once per step, world-frame particle "
+                       "offsets re-rotated every step); the GPU arm runs the PHYSICAL step of the "
+                       "same pipeline (same broad phase, contact law and summation order)")
+
+
+def cpu_reference_rate(scene, grid, target_s: float, broadphase: str = "grid",
+                       warmup: int = 1, steps: int | None = None):
+    """Particle-steps/s of the reference CPU step on the whole workload (every body of the
+    scene): `warmup` untimed steps, then steps until `target_s` seconds have passed (or exactly
+    `steps`).  Returns (rate, cores, kind, sample description, steps run, seconds)."""
     from oracle import ref
     if not ref.available():
         return None
-    bodies = min(scene.num_bodies, 4096)
-    sample = reference_sample(scene, bodies)
-    runner = (ReferenceCPUStepBVH if broadphase == "bvh" else ReferenceCPUStep)(sample, grid)
+    runner = (ReferenceCPUStepBVH if broadphase == "bvh" else ReferenceCPUStep)(scene, grid)
     cores = ref.max_threads()
-    runner.step()  # warm caches / page in
+    for _ in range(warmup):
+        runner.step()
     t0 = time.perf_counter()
     k = 0
     while True:
@@ -338,47 +341,45 @@ def cpu_reference_rate(scene, grid, target_s: float, steps: int | None = None,
         el = time.perf_counter() - t0
         if (steps is not None and k >= steps) or (steps is None and el >= target_s):
             break
-    rate = sample.num_particles * k / el
-    where = "BVH" if broadphase == "bvh" else "same grid"
-    desc = (f"first {bodies} bodies ({sample.num_particles} particles) of the workload, "
-            f"{where} path, {k} reference steps in {el:.1f} s")
+    rate = scene.num_particles * k / el
+    where = "BVH" if broadphase == "bvh" else "grid"
+    desc = (f"the whole workload ({scene.num_bodies} bodies, {scene.num_particles} particles), "
+            f"{where} path, {k} timed steps after {warmup} untimed, {el:.1f} s")
     return rate, cores, "reference", desc, k, el
 
 
 # ---- the reference arm -----------------------------------------------------------------------
 def run_reference(args):
+    """The reference's own kernel bodies (oracle/_ref/libref_cpu.so, OpenMP over all host
+    cores) stepping the same scene as our arm.  Imports nothing from diploma_thesis_b200 but
+    the pure-numpy scene generator."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import cpu, ref
     scene, desc = make_scene(args.workload)
+    if args.broadphase == "bvh":
+        desc = desc.replace("grid 256x512x256 wrapped", "BVH").replace("grid 128^3", "BVH")
     grid = cpu.scene_grid(scene)
     if not ref.available():
         print(json.dumps({"impl": "reference", "unavailable":
                           "the reference CPU build (oracle/_ref/libref_cpu.so) is not present"}))
         return 0
-    bodies = min(scene.num_bodies, 2048 if args.workload == "pile" else 4096)
-    sample = reference_sample(scene, bodies)
-    runner = (ReferenceCPUStepBVH if args.broadphase == "bvh" else ReferenceCPUStep)(sample, grid)
-    for _ in range(args.warmup):
-        runner.step()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        runner.step()
-    el = time.perf_counter() - t0
-    rate = sample.num_particles * args.steps / el / 1e6
-    cores = ref.max_threads()
+    r = cpu_reference_rate(scene, grid, 0.0, args.broadphase, warmup=args.warmup,
+                           steps=args.steps)
+    rate, cores, kind, sample, k, el = r
+    rate /= 1e6
     line = {"metric": "Mparticle-steps/s", "value": rate, "unit": "Mparticle-steps/s",
             "impl": "reference", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "ms_per_step": 1e3 * el / k, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": desc, "sample": f"first {bodies} bodies "
-                       f"({sample.num_particles} particles)", "broadphase": args.broadphase},
+            "config": {"workload": desc, "broadphase": args.broadphase,
+                       "particles": scene.num_particles, "bodies": scene.num_bodies,
+                       "parallelism": f"host CPU, {cores} threads",
+                       "semantics": REFERENCE_SEMANTICS},
             "cpu_baseline": {"value": rate, "unit": "Mparticle-steps/s", "cores": cores,
-                             "kind": "reference",
-                             "sample": f"first {bodies} bodies ({sample.num_particles} particles) "
-                                       f"of the workload, {args.steps} steps"},
+                             "kind": kind, "sample": sample},
             "e2e": {"value": rate, "unit": "Mparticle-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -398,8 +399,15 @@ def run_ours(args):
     ctx = api.Context(local)
     gs = api.GpuScene(ctx, scene, broadphase=args.broadphase)
     n, nb = scene.num_particles, scene.num_bodies
+    # the timed window sits in the middle of the configuration's run (contacts build up as the
+    # bodies drift together), unless --start-step says otherwise
+    run_len = CONFIG_STEPS.get(args.workload, args.steps)
+    start_step = (args.start_step if args.start_step is not None
+                  else max(0, (run_len - args.steps) // 2 - args.warmup))
     stream = torch.cuda.Stream()
-    with torch.cuda.stream(stream):
+    with torch.cuda.stream(stream), ClockSampler(local) as clocks:
+        if start_step:
+            gs.step(start_step, use_graph=True, stream=stream)
         gs.step(args.warmup, use_graph=True, stream=stream)
         stream.synchronize()
         ctx.check(stream)
@@ -407,15 +415,27 @@ def run_ours(args):
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier(world)
         torch.cuda.synchronize()
-        with ClockSampler(local) as clocks:
-            start.record(stream)
-            gs.step(args.steps, use_graph=True, stream=stream)
-            end.record(stream)
-            end.synchronize()
+        clocks.mark_start()
+        start.record(stream)
+        gs.step(args.steps, use_graph=True, stream=stream)
+        end.record(stream)
+        end.synchronize()
         torch.cuda.synchronize()
         barrier(world)
         ms = start.elapsed_time(end)
         ctx.check(stream)
+        # a timed region shorter than the sampling period gets no sample of its own: keep the
+        # same step loop running (untimed, on a copy of the scene, so that the measured scene
+        # is not advanced further) until the sampler has seen the GPU under this load
+        if clocks.samples_since_start() < 5:
+            twin = api.GpuScene(ctx, scene, broadphase=args.broadphase)
+            twin.upload_state(gs.download_state(stream=stream), stream=stream)
+            t_end = time.perf_counter() + 2.0
+            while clocks.samples_since_start() < 5 and time.perf_counter() < t_end:
+                twin.step(50, use_graph=True, stream=stream)
+                stream.synchronize()
+            twin.close()
+        clocks.mark_end()
     ms = max_over_ranks(ms, world)
     ms_per_step = ms / args.steps
     value = job_rate(world, n, args.steps, ms)
@@ -472,7 +492,7 @@ def run_ours(args):
         if r is not None:
             rate, cores, kind, sample, k, el = r
             cpu_baseline = {"value": rate / 1e6, "unit": "Mparticle-steps/s", "cores": cores,
-                            "kind": kind, "sample": sample}
+                            "kind": kind, "sample": sample, "semantics": REFERENCE_SEMANTICS}
 
     memsets = 2 if args.broadphase == "bvh" else 1  # memset nodes are not kernels (steady step)
     launches = args.steps * (gs.launches_per_step() - memsets)
@@ -484,6 +504,9 @@ def run_ours(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "broadphase": args.broadphase, "particles": n,
                        "bodies": nb,
+                       "timed_window": f"steps {start_step + args.warmup} to "
+                                       f"{start_step + args.warmup + args.steps} of the "
+                                       f"{run_len}-step run",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "per-step working set > 126 MB L2 (inputs larger than L2)",
                        "timed": "CUDA graph replays, events on the launching stream"},
@@ -836,7 +859,7 @@ def run_served(args):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh", "sis"],
@@ -846,6 +869,10 @@ def main(argv=None):
     ap.add_argument("--broadphase", choices=["grid", "bvh"], default="grid",
                     help="pile / plain: broad phase of the fused step")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--start-step", type=int, default=None,
+                    help="pile / plain: untimed steps run before the warm-up (default: centre "
+                         "the timed window in the configuration's run, 500 steps for the pile, "
+                         "1,000 for the plain scene)")
     ap.add_argument("--tune", action="store_true", help="batched: autotune per size bucket")
     ap.add_argument("--tune-cache", default=str(ROOT / "diploma_thesis_b200" / "autotune_b200.json"))
     ap.add_argument("--rate", type=float, default=2000.0, help="served: requests per second")

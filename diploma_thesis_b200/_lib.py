@@ -90,6 +90,7 @@ SIGNATURES = {
     "ar_ctx_reserve": [P, C.c_size_t],
     "ar_last_error": [],
     "ar_version": [],
+    "ar_test_fail_allocations": [C.c_long],
     "ar_scene_aabb": [P, P, I, P, P, S],
     "ar_morton30": [P, P, I, P, P, P, P, S],
     "ar_morton30_box": [P, P, I, C.POINTER(F), C.POINTER(F), P, P, S],
@@ -97,6 +98,7 @@ SIGNATURES = {
     "ar_radix_sort_pairs_u32": [P, P, P, P, P, I, I, I, S],
     "ar_radix_sort_pairs_u64": [P, P, P, P, P, I, I, I, S],
     "ar_radix_sort_pairs_u32_noalloc": [P, P, P, P, I, I, I, P, S],
+    "ar_radix_sort_pairs_u32_ex": [P, P, P, P, P, I, I, I, C.c_uint32, S],
     "ar_lbvh_build": [P, P, I, P, P, P, P, P, P, S],
     "ar_lbvh_build64": [P, P, I, P, P, P, P, P, P, S],
     "ar_lbvh_leaves": [P, I, P, P, F, P, P, P, P, P, P, S],

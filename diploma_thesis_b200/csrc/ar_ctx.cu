@@ -6,11 +6,49 @@
 #include "ar_internal.cuh"
 #include "ar_sort.cuh"
 
+#include <atomic>
+
 namespace {
 thread_local char g_last_error[512] = "";
+// Allocation fault injection (ar_test_fail_allocations): -1 = off, else the number of
+// allocations that still succeed before every later one fails.
+std::atomic<long> g_alloc_budget{-1};
+
+bool injected_failure() {
+  long b = g_alloc_budget.load();
+  while (b >= 0) {
+    if (b == 0) return true;
+    if (g_alloc_budget.compare_exchange_weak(b, b - 1)) return false;
+  }
+  return false;
 }
+}  // namespace
 
 namespace arh {
+
+cudaError_t dev_malloc(void** p, size_t bytes) {
+  if (injected_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t st) {
+  if (injected_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocAsync(p, bytes, st);
+}
+
+cudaError_t host_malloc(void** p, size_t bytes) {
+  if (injected_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(p, bytes);
+}
 
 void set_error(const char* fmt, ...) {
   va_list ap;
@@ -37,7 +75,7 @@ void* scratch(ar_ctx* ctx, size_t bytes) {
   ctx->scratch = nullptr;
   ctx->scratch_bytes = 0;
   size_t grow = bytes + bytes / 4 + (1u << 20);
-  if (cudaMalloc(&ctx->scratch, grow) != cudaSuccess) {
+  if (dev_malloc(&ctx->scratch, grow) != cudaSuccess) {
     cudaGetLastError();
     set_error("scratch arena: cudaMalloc(%zu) failed", grow);
     return nullptr;
@@ -64,11 +102,16 @@ ar_status ar_ctx_create(int device, ar_ctx** out) {
   ar_ctx* c = new ar_ctx();
   c->device = device;
   cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device);
-  if (cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess ||
-      cudaMallocHost(&c->h_err, sizeof(int)) != cudaSuccess) {
+  auto release = [c]() {  // everything created so far, on any failure below
+    if (c->d_err) cudaFree(c->d_err);
+    if (c->h_err) cudaFreeHost(c->h_err);
+    delete c;
+  };
+  if (arh::dev_malloc((void**)&c->d_err, sizeof(int)) != cudaSuccess ||
+      arh::host_malloc((void**)&c->h_err, sizeof(int)) != cudaSuccess) {
     cudaGetLastError();
     arh::set_error("ar_ctx_create: allocation failed");
-    delete c;
+    release();
     return AR_ERR_OOM;
   }
   cudaMemset(c->d_err, 0, sizeof(int));
@@ -83,10 +126,16 @@ ar_status ar_ctx_create(int device, ar_ctx** out) {
   cudaGetLastError();
   ar_sort::init();
   if (cudaDeviceSynchronize() != cudaSuccess) {
-    arh::set_error("ar_ctx_create: device error");
+    arh::set_error("ar_ctx_create: device error (%s)", cudaGetErrorString(cudaGetLastError()));
+    release();
     return AR_ERR_CUDA;
   }
   *out = c;
+  return AR_OK;
+}
+
+ar_status ar_test_fail_allocations(long after) {
+  g_alloc_budget.store(after < 0 ? -1 : after);
   return AR_OK;
 }
 

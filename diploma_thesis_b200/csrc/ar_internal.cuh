@@ -109,4 +109,9 @@ struct ar_ctx {
 namespace arh {
 // Ensure the context's scratch arena holds at least `bytes`; returns its base or null.
 void* scratch(ar_ctx* ctx, size_t bytes);
+// Every device and pinned-host allocation of the library goes through these, so that a test
+// can make them fail on the host (ar_test_fail_allocations) and check each AR_ERR_OOM path.
+cudaError_t dev_malloc(void** p, size_t bytes);
+cudaError_t dev_malloc_async(void** p, size_t bytes, cudaStream_t st);
+cudaError_t host_malloc(void** p, size_t bytes);
 }  // namespace arh

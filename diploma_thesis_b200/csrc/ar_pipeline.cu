@@ -785,7 +785,7 @@ void drop_graph(ar_batch* B) {
 
 template <class T>
 bool alloc(T** p, size_t count) {
-  if (cudaMalloc((void**)p, count * sizeof(T) + 16) != cudaSuccess) {
+  if (arh::dev_malloc((void**)p, count * sizeof(T) + 16) != cudaSuccess) {
     cudaGetLastError();
     *p = nullptr;
     return false;
@@ -916,7 +916,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
       if (B->h_stage[i]) cudaFreeHost(B->h_stage[i]);
       B->h_stage[i] = nullptr;
       B->h_stage_cap[i] = 0;
-      if (cudaMallocHost((void**)&B->h_stage[i], 2 * need) != cudaSuccess) {
+      if (arh::host_malloc((void**)&B->h_stage[i], 2 * need) != cudaSuccess) {
         cudaGetLastError();
         arh::set_error("batch prepare: pinned staging allocation failed");
         return AR_ERR_OOM;
@@ -1210,7 +1210,7 @@ ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene
                                                  4 * (size_t)(nb + 1), 16 * (size_t)n};
   size_t total = 0;
   for (size_t z : sizes) total += (z + 255) & ~(size_t)255;
-  if (cudaMallocAsync(&s->block, total, st) != cudaSuccess) {
+  if (arh::dev_malloc_async(&s->block, total, st) != cudaSuccess) {
     cudaGetLastError();
     s->block = nullptr;
     ar_scene_destroy(s);
@@ -1441,7 +1441,7 @@ ar_status ar_batch_create(ar_ctx* ctx, ar_batch** out) {
   if (!ctx || !out) return AR_ERR_INVALID_ARG;
   ar_batch* B = new ar_batch();
   B->ctx = ctx;
-  if (cudaMalloc(&B->d_step, sizeof(long long)) != cudaSuccess ||
+  if (arh::dev_malloc((void**)&B->d_step, sizeof(long long)) != cudaSuccess ||
       cudaMemset(B->d_step, 0, sizeof(long long)) != cudaSuccess) {
     cudaGetLastError();
     cudaFree(B->d_step);

@@ -36,6 +36,7 @@ constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagPrefix = 2u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1;
 constexpr long kSpinLimit = 1l << 24;
+constexpr long kTestSpinLimit = 4096;  // AR_SORT_TEST_MUTE_FIRST_TILE: give up quickly
 constexpr int kLookWindow = 8;  // look-back status words read per round trip
 
 template <class K>
@@ -106,7 +107,8 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
     const K* __restrict__ keys_in, const uint32_t* __restrict__ vals_in, K* __restrict__ keys_out,
     uint32_t* __restrict__ vals_out, int n, int shift, int bits,
     const uint32_t* __restrict__ digit_base, uint32_t* __restrict__ status,
-    uint32_t* __restrict__ tile_counter, int* __restrict__ err) {
+    uint32_t* __restrict__ tile_counter, int* __restrict__ err, long spin_limit,
+    int mute_tile0) {
   ar::pdl_wait();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   constexpr int kWarps = kT / 32;
@@ -174,7 +176,8 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
       tile_count += c;
     }
     cuda::atomic_ref<uint32_t, cuda::thread_scope_device> mine(status[(long)tile * kRadix + d]);
-    mine.store((tile == 0 ? kFlagPrefix : kFlagAgg) | tile_count, cuda::memory_order_relaxed);
+    if (!(mute_tile0 && tile == 0))
+      mine.store((tile == 0 ? kFlagPrefix : kFlagAgg) | tile_count, cuda::memory_order_relaxed);
   }
 
   // tile-local exclusive scan over digits (block scan of one value per thread)
@@ -245,7 +248,7 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
         }
         k -= used;
         if (!found && used == 0) {
-          if (++spins > kSpinLimit) {
+          if (++spins > spin_limit) {
             ar::raise_error(err, ar::kErrTimeout);
             break;
           }
@@ -281,13 +284,23 @@ __global__ void __launch_bounds__(kT, (sizeof(K) == 4 ? 1024 : 512) / kT) oneswe
   }
 }
 
+// How the digit passes run: ranking by match.any (8-bit digits), the look-back's spin limit,
+// and the failure-detection hook that keeps tile 0 from publishing its status (every later
+// tile's look-back then runs out of spins, reports kErrTimeout and writes nothing out of
+// range).
+struct PassOpts {
+  bool match_rank = false;
+  long spin_limit = kSpinLimit;
+  int mute_tile0 = 0;
+};
+
 // The digit passes of `plan`, ping-ponging so that the last one lands in keys_out.  `status`
 // holds one [tiles][kRadix] block per pass, tiles = the most tiles any pass uses.
 template <class K>
 void launch_passes(const ar_sort::Plan& plan, int n, const K* keys_in, const uint32_t* vals_in,
                    K* keys_out, uint32_t* vals_out, K* tmp_keys, uint32_t* tmp_vals,
                    const uint32_t* hist, uint32_t* status, uint32_t* counters, int* err,
-                   cudaStream_t st, bool match_rank) {
+                   cudaStream_t st, const PassOpts& o) {
   const long status_tiles = ((long)n + tile_items(n) - 1) / tile_items(n);
   const K* src_k = keys_in;
   const uint32_t* src_v = vals_in;
@@ -303,15 +316,15 @@ void launch_passes(const ar_sort::Plan& plan, int n, const K* keys_in, const uin
     if (bits > 8)
       arh::launch_pdl(onesweep_kernel<K, 512, 9>, dim3(tiles), dim3(512),
           sizeof(PassSmem<K, 512, 9>), st, src_k, src_v, dk, dv, n, shift, bits, base, stat,
-          counters + p, err);
+          counters + p, err, o.spin_limit, o.mute_tile0);
     else if (kt == 512)
-      arh::launch_pdl(match_rank ? onesweep_kernel<K, 512, 8, true> : onesweep_kernel<K, 512, 8>,
+      arh::launch_pdl(o.match_rank ? onesweep_kernel<K, 512, 8, true> : onesweep_kernel<K, 512, 8>,
           dim3(tiles), dim3(512), sizeof(PassSmem<K, 512, 8>), st, src_k, src_v, dk, dv, n, shift,
-          bits, base, stat, counters + p, err);
+          bits, base, stat, counters + p, err, o.spin_limit, o.mute_tile0);
     else
-      arh::launch_pdl(match_rank ? onesweep_kernel<K, 256, 8, true> : onesweep_kernel<K, 256, 8>,
+      arh::launch_pdl(o.match_rank ? onesweep_kernel<K, 256, 8, true> : onesweep_kernel<K, 256, 8>,
           dim3(tiles), dim3(256), sizeof(PassSmem<K, 256, 8>), st, src_k, src_v, dk, dv, n, shift,
-          bits, base, stat, counters + p, err);
+          bits, base, stat, counters + p, err, o.spin_limit, o.mute_tile0);
     src_k = dk;
     src_v = dv;
   }
@@ -324,7 +337,7 @@ template <class K>
 ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* keys_out,
                     uint32_t* vals_out, int n, int begin_bit, int end_bit, cudaStream_t st,
                     void* ws, size_t ws_bytes, bool external_hist = false,
-                    bool match_rank = false) {
+                    const PassOpts& opts = PassOpts()) {
   const ar_sort::Plan plan = ar_sort::make_plan(begin_bit, end_bit);
   const int passes = plan.passes;
   ar_sort::Layout L = ar_sort::layout(n, sizeof(K), passes);
@@ -350,21 +363,42 @@ ar_status sort_impl(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* k
   }
   arh::launch_pdl(hist_scan_kernel, dim3(1), dim3(32 * ar_sort::kMaxPasses), 0, st, hist, passes);
   launch_passes<K>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
-                   status, counters, err, st, match_rank);
+                   status, counters, err, st, opts);
   return arh::check_launch("radix sort");
+}
+
+// True when the byte ranges [a, a + a_bytes) and [b, b + b_bytes) share any byte.
+inline bool overlaps(const void* a, size_t a_bytes, const void* b, size_t b_bytes) {
+  const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b;
+  return x < y + b_bytes && y < x + a_bytes;
+}
+
+// Argument checks shared by every sort entry point (n > 0): an output that overlaps its input
+// anywhere would be overwritten by the first pass while other tiles still read it.
+template <class K>
+ar_status check_sort_args(const K* keys_in, const uint32_t* vals_in, const K* keys_out,
+                          const uint32_t* vals_out, int n, const char* who) {
+  if (!keys_in || !keys_out || !vals_out) return AR_ERR_INVALID_ARG;
+  const size_t kb = (size_t)n * sizeof(K), vb = (size_t)n * 4;
+  if (overlaps(keys_in, kb, keys_out, kb) || overlaps(keys_in, kb, vals_out, vb) ||
+      (vals_in && (overlaps(vals_in, vb, vals_out, vb) || overlaps(vals_in, vb, keys_out, kb))) ||
+      overlaps(keys_out, kb, vals_out, vb)) {
+    arh::set_error("%s: outputs must not overlap the inputs or each other", who);
+    return AR_ERR_INVALID_ARG;
+  }
+  return AR_OK;
 }
 
 template <class K>
 ar_status sort_entry(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* keys_out,
-                     uint32_t* vals_out, int n, int begin_bit, int end_bit, ar_stream_t stream) {
+                     uint32_t* vals_out, int n, int begin_bit, int end_bit, ar_stream_t stream,
+                     const PassOpts& opts = PassOpts()) {
   const int kbits = 8 * (int)sizeof(K);
   if (!ctx || n < 0 || begin_bit < 0 || end_bit > kbits || begin_bit > end_bit)
     return AR_ERR_INVALID_ARG;
-  if (n > 0 && (!keys_in || !keys_out || !vals_out)) return AR_ERR_INVALID_ARG;
-  if (n > 0 && ((const void*)keys_in == (const void*)keys_out ||
-                (vals_in && (const void*)vals_in == (const void*)vals_out))) {
-    arh::set_error("radix sort: outputs must not alias inputs");
-    return AR_ERR_INVALID_ARG;
+  if (n > 0) {
+    const ar_status a = check_sort_args(keys_in, vals_in, keys_out, vals_out, n, "radix sort");
+    if (a != AR_OK) return a;
   }
   if (n >= (1 << 30)) {
     arh::set_error("radix sort: n must be < 2^30");
@@ -385,7 +419,7 @@ ar_status sort_entry(ar_ctx* ctx, const K* keys_in, const uint32_t* vals_in, K* 
   void* ws = arh::scratch(ctx, L.total);
   if (!ws) return AR_ERR_OOM;
   return sort_impl<K>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit, st, ws,
-                      L.total);
+                      L.total, false, opts);
 }
 
 __global__ void iota_kernel(uint32_t* v, int n) {
@@ -487,8 +521,10 @@ ar_status sort_u32(ar_ctx* ctx, const uint32_t* keys_in, const uint32_t* vals_in
                    cudaStream_t st, void* ws, size_t ws_bytes, bool external_hist,
                    bool match_rank) {
   if (n == 0) return AR_OK;
+  PassOpts o;
+  o.match_rank = match_rank;
   return sort_impl<uint32_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
-                             st, ws, ws_bytes, external_hist, match_rank);
+                             st, ws, ws_bytes, external_hist, o);
 }
 
 ar_status sort_u64(ar_ctx* ctx, const uint64_t* keys_in, const uint32_t* vals_in,
@@ -527,6 +563,25 @@ ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in, const ui
                               stream);
 }
 
+ar_status ar_radix_sort_pairs_u32_ex(ar_ctx* ctx, const uint32_t* keys_in,
+                                     const uint32_t* vals_in, uint32_t* keys_out,
+                                     uint32_t* vals_out, int n, int begin_bit, int end_bit,
+                                     uint32_t flags, ar_stream_t stream) {
+  const uint32_t known = AR_SORT_RANK_MATCH | AR_SORT_TEST_MUTE_FIRST_TILE;
+  if (flags & ~known) {
+    arh::set_error("radix sort: unknown flags 0x%x", flags & ~known);
+    return AR_ERR_INVALID_ARG;
+  }
+  PassOpts o;
+  o.match_rank = (flags & AR_SORT_RANK_MATCH) != 0;
+  if (flags & AR_SORT_TEST_MUTE_FIRST_TILE) {
+    o.mute_tile0 = 1;
+    o.spin_limit = kTestSpinLimit;
+  }
+  return sort_entry<uint32_t>(ctx, keys_in, vals_in, keys_out, vals_out, n, begin_bit, end_bit,
+                              stream, o);
+}
+
 // The same sort as ar_radix_sort_pairs_u32, with its workspace in g_noalloc_scratch instead
 // of memory from cudaMalloc.  Shared by every call on a device: calls that overlap on the
 // GPU race; the histogram / look-back head is cleared at the start of each call.
@@ -539,11 +594,10 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
     arh::set_error("allocation-free sort: n = %d exceeds its limit of %d pairs", n, kNoAllocMaxN);
     return AR_ERR_INVALID_ARG;
   }
-  if (n > 0 && (!keys_in || !keys_out || !vals_out)) return AR_ERR_INVALID_ARG;
-  if (n > 0 && ((const void*)keys_in == (const void*)keys_out ||
-                (vals_in && (const void*)vals_in == (const void*)vals_out))) {
-    arh::set_error("allocation-free sort: outputs must not alias inputs");
-    return AR_ERR_INVALID_ARG;
+  if (n > 0) {
+    const ar_status a =
+        check_sort_args(keys_in, vals_in, keys_out, vals_out, n, "allocation-free sort");
+    if (a != AR_OK) return a;
   }
   if (n == 0) return AR_OK;
   cudaStream_t st = arh::stream(stream);
@@ -586,7 +640,7 @@ ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in, const uint32_
       hist);
   arh::launch_pdl(hist_scan_kernel, dim3(1), dim3(32 * ar_sort::kMaxPasses), 0, st, hist, passes);
   launch_passes<uint32_t>(plan, n, keys_in, vals_in, keys_out, vals_out, tmp_keys, tmp_vals, hist,
-                          status, counters, (int*)d_status, st, false);
+                          status, counters, (int*)d_status, st, PassOpts());
   return arh::check_launch("allocation-free sort");
 }
 

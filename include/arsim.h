@@ -86,6 +86,11 @@ AR_API ar_status ar_ctx_status(ar_ctx* ctx, ar_stream_t stream);
 AR_API ar_status ar_ctx_reserve(ar_ctx* ctx, size_t bytes);
 AR_API const char* ar_last_error(void);
 AR_API const char* ar_version(void);
+/* Failure-detection test hook (no counterpart in the reference, whose allocation failures
+ * exit through checkCudaErrors): after `after` more device or pinned-host allocations by this
+ * library succeed, every later one fails on the host as if the memory were exhausted, so each
+ * AR_ERR_OOM path can be exercised; `after` < 0 switches the injection off.  Process-wide. */
+AR_API ar_status ar_test_fail_allocations(long after);
 
 /* ---- (a6) scene bounding box -------------------------------------------------------------
  * findAABBCub (BVHSource/createMortonCodes.cu:65-107): min and max over all four lanes of
@@ -117,7 +122,8 @@ AR_API ar_status ar_morton63(ar_ctx* ctx, const float* pos4, int n, const float*
  * [begin_bit, end_bit) -- the reference always sorts all 32 bits; passing the number of
  * significant bits gives the same order with fewer passes.  Stable: equal keys keep input
  * order.  Inputs are left intact; results go to keys_out/vals_out (vals_in may be NULL to
- * mean the identity 0..n-1).  Onesweep: one histogram pass plus one pass per 8-bit digit
+ * mean the identity 0..n-1); the outputs must not overlap the inputs or each other
+ * (AR_ERR_INVALID_ARG).  Onesweep: one histogram pass plus one pass per 8-bit digit
  * with decoupled look-back. */
 AR_API ar_status ar_radix_sort_pairs_u32(ar_ctx* ctx, const uint32_t* keys_in,
                                          const uint32_t* vals_in, uint32_t* keys_out,
@@ -127,6 +133,22 @@ AR_API ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in,
                                          const uint32_t* vals_in, uint64_t* keys_out,
                                          uint32_t* vals_out, int n, int begin_bit, int end_bit,
                                          ar_stream_t stream);
+/* ar_radix_sort_pairs_u32 with options (the same sort; cub::DeviceRadixSort::SortPairs has no
+ * counterpart of these flags).
+ *   AR_SORT_RANK_MATCH: rank each 8-bit digit with one warp match.any per item instead of a
+ *     ballot per digit bit -- faster when the keys a warp holds share few digits (cell keys of
+ *     particles stored body by body), slower when they share many (Morton codes).  The order
+ *     is the same.
+ *   AR_SORT_TEST_MUTE_FIRST_TILE: failure-detection test hook.  Tile 0 of every digit pass
+ *     never publishes its look-back status, and the spin limit drops to 4,096 polls, so every
+ *     later tile's look-back gives up: the device error word reports AR_ERR_TIMEOUT (read it
+ *     with ar_ctx_status), the outputs are garbage, and nothing is written outside them. */
+#define AR_SORT_RANK_MATCH 1u
+#define AR_SORT_TEST_MUTE_FIRST_TILE 0x80000000u
+AR_API ar_status ar_radix_sort_pairs_u32_ex(ar_ctx* ctx, const uint32_t* keys_in,
+                                            const uint32_t* vals_in, uint32_t* keys_out,
+                                            uint32_t* vals_out, int n, int begin_bit,
+                                            int end_bit, uint32_t flags, ar_stream_t stream);
 
 /* Allocation-free variant of ar_radix_sort_pairs_u32.  No counterpart in the reference.
  * For callers that cannot allocate device memory: a frame loop that must never stall on
@@ -139,7 +161,9 @@ AR_API ar_status ar_radix_sort_pairs_u64(ar_ctx* ctx, const uint64_t* keys_in,
  * a timed-out look-back ORs 1.  The first call on each device sets up (looks up the array's
  * device address with that device current); make that first call before any stream capture.
  * Every call on a device shares the array, so calls that overlap on the GPU race: serialise
- * them (one stream, or events). */
+ * them (one stream, or events).  The set-up is done once per device for the life of the
+ * process and is not redone after cudaDeviceReset: do not call this entry point again in a
+ * process that has reset the device.  Outputs must not overlap the inputs or each other. */
 AR_API ar_status ar_radix_sort_pairs_u32_noalloc(const uint32_t* keys_in,
                                                  const uint32_t* vals_in, uint32_t* keys_out,
                                                  uint32_t* vals_out, int n, int begin_bit,

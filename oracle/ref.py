@@ -16,6 +16,41 @@ _SO = Path(__file__).resolve().parent / "_ref" / "libref_cpu.so"
 _L = None
 
 
+class SimParams(C.Structure):
+    """The reference's `struct SimParams` (Kernels/particleSystem.cuh:27-55), 128 bytes, as the
+    reference build's kernels read it.  Declared here so that nothing on the reference's side
+    (the golden-fixture generator, bench.py's reference arm) loads the product library."""
+    _fields_ = [("collider_pos", C.c_float * 3), ("collider_radius", C.c_float),
+                ("gravity", C.c_float * 3), ("global_damping", C.c_float),
+                ("particle_radius", C.c_float), ("grid_size", C.c_uint32 * 3),
+                ("num_cells", C.c_uint32), ("world_origin", C.c_float * 3),
+                ("cell_size", C.c_float * 3), ("num_bodies", C.c_uint32),
+                ("max_particles_per_cell", C.c_uint32), ("spring", C.c_float),
+                ("damping", C.c_float), ("shear", C.c_float), ("attraction", C.c_float),
+                ("boundary_damping", C.c_float), ("ar_restitution", C.c_float),
+                ("rb_restitution", C.c_float), ("ar_friction", C.c_float),
+                ("rb_friction", C.c_float), ("w_damping", C.c_float), ("v_damping", C.c_float)]
+
+
+def sim_params(radius: float, grid_origin, cell, grid_dims, spring=0.5, damping=0.02,
+               shear=0.1, attraction=0.0, gravity=(0.0, -9.81, 0.0), w_damping=1.0) -> SimParams:
+    """Parameters as the reference's ParticleSystem sets them (Particles/particleSystem.cpp:
+    123-141): global damping 1, boundary damping -0.5, the given grid and DEM constants."""
+    p = SimParams()
+    p.particle_radius = radius
+    for a in range(3):
+        p.world_origin[a] = grid_origin[a]
+        p.cell_size[a] = cell[a] if np.ndim(cell) else cell
+        p.grid_size[a] = int(grid_dims[a])
+        p.gravity[a] = gravity[a]
+    p.num_cells = int(np.prod(grid_dims))
+    p.spring, p.damping, p.shear, p.attraction = spring, damping, shear, attraction
+    p.w_damping = w_damping
+    p.global_damping = 1.0
+    p.boundary_damping = -0.5
+    return p
+
+
 def available() -> bool:
     return _SO.exists()
 

@@ -17,8 +17,8 @@ ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
 
 from diploma_thesis_b200 import scenes  # noqa: E402
-from diploma_thesis_b200._lib import SimParams  # noqa: E402  (struct layout only)
 from oracle import ref  # noqa: E402
+from oracle.ref import SimParams  # noqa: E402  (the reference's struct layout)
 
 OUT = Path(__file__).resolve().parent
 

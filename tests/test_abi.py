@@ -70,3 +70,21 @@ def test_scene_footprint_scales_with_size():
         d.num_bodies *= 10
         assert _lib.lib.ar_scene_footprint(C.byref(d)) > factor * f1 > 0
         assert (_lib.lib.ar_scene_cells(C.byref(d)) > 0) == (bp == 0)
+
+
+def test_sort_rejects_overlapping_outputs_without_a_gpu():
+    """The allocation-free sort checks its arguments before any CUDA call: outputs that
+    overlap an input (or each other) anywhere, not only at the same start address."""
+    from diploma_thesis_b200 import _lib
+    L = _lib.lib
+    f = L.ar_radix_sort_pairs_u32_noalloc
+    a, b, c = 0x100000, 0x200000, 0x300000  # never dereferenced: rejected first
+    n = 1024
+    assert f(C.c_void_p(a), None, C.c_void_p(a + 4), C.c_void_p(b), n, 0, 32, None, None) == 1
+    assert b"overlap" in L.ar_last_error()
+    assert f(C.c_void_p(a), C.c_void_p(b), C.c_void_p(c), C.c_void_p(b + 4 * n - 4), n, 0, 32,
+             None, None) == 1
+    assert f(C.c_void_p(a), None, C.c_void_p(b), C.c_void_p(b + 4 * n - 4), n, 0, 32, None,
+             None) == 1
+    assert f(C.c_void_p(a), None, C.c_void_p(c), C.c_void_p(a), n, 0, 32, None, None) == 1
+    assert L.ar_radix_sort_pairs_u32_ex(None, None, None, None, None, 0, 0, 32, 0, None) == 1
