@@ -287,3 +287,39 @@ def collide_particles(params, rb_idx, rel4, spos4, svel4, gidx, cstart, cend, ve
                                    _p(pt), _p(nv), _p(_f32(spos4)), _p(_f32(svel4)),
                                    _p(_u32(gidx)), _p(_u32(cstart)), _p(_u32(cend)), n)
     return pf, pt, nv
+
+
+def sis_step(params, rb_idx, offsets, cms4, vel4, ang4, inertia9, mass, rel4, contact_distance,
+             contact_body, contact_particle, scene_normals4=None, solve=True):
+    """GatherRigidBodyCollisions (or GatherAugmentedRealityCollisions when scene_normals4 is
+    given) followed by SequentialImpulseSolver -- the reference's own host loops
+    (Particles/updateFunctions.cpp:1431-1874) on a stand-in ParticleSystem.  Returns the
+    contact list (normal, point, body1, body2, bias, the accumulated impulse and the two
+    accumulated frictions after the solve), the bodies' new velocity and angular velocity,
+    and the re-posed particles (rel, pos, particle velocity) of the solver's tail."""
+    n, nb = len(rb_idx), len(cms4)
+    counts = np.diff(_i32(offsets)).astype(np.int32)
+    cms, vel, ang = _f32(cms4).copy(), _f32(vel4).copy(), _f32(ang4).copy()
+    ib, m = _f32(inertia9).copy(), _f32(mass).copy()
+    rel = _f32(rel4).copy()
+    pos, pvel = np.zeros((n, 4), np.float32), np.zeros((n, 4), np.float32)
+    quat = np.tile(np.array([0, 0, 0, 1], np.float32), (nb, 1))
+    cd = _f32(contact_distance).copy()
+    cb = _i32(contact_body if contact_body is not None else np.zeros(n)).copy()
+    cp = _i32(contact_particle).copy()
+    sn = None if scene_normals4 is None else _f32(scene_normals4)
+    cap = n
+    out = {"normal": np.zeros((cap, 4), np.float32), "point": np.zeros((cap, 4), np.float32),
+           "body1": np.zeros(cap, np.int32), "body2": np.zeros(cap, np.int32),
+           "bias": np.zeros(cap, np.float32), "acc": np.zeros((cap, 3), np.float32)}
+    L = lib()
+    L.refcpu_sis_step.restype = C.c_int
+    k = L.refcpu_sis_step(C.byref(params), nb, n, _p(counts), _p(cms), _p(vel), _p(ang), _p(ib),
+                          _p(m), _p(rel), _p(pos), _p(pvel), _p(quat), _p(_i32(rb_idx).copy()),
+                          _p(cd), _p(cb), _p(cp), _p(sn), 0 if sn is None else len(sn),
+                          int(sn is not None), int(solve), cap, _p(out["normal"]),
+                          _p(out["point"]), _p(out["body1"]), _p(out["body2"]), _p(out["bias"]),
+                          _p(out["acc"]))
+    res = {key: v[:k] for key, v in out.items()}
+    res.update({"vel": vel, "ang": ang, "rel": rel, "pos": pos, "pvel": pvel, "count": k})
+    return res

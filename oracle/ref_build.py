@@ -56,6 +56,18 @@ RANGES = [
     ("WallCollisions.cu", 201, 276, "HandleWallCollisionKernelUnmapped"),
 ]
 
+# ParticleSystem member functions of the sequential-impulse path (host C++ with glm): the
+# contact gather and the solver the reference's default update runs on the CPU, plus the
+# contact-point helper they call.  They go to their own file, oracle/_ref/extracted_members.inc,
+# which oracle/ref_cpu_driver.cpp includes after declaring a stand-in ParticleSystem class
+# holding the members these bodies use.
+MEMBER_RANGES = [
+    ("Particles/CPU_Engine.cpp", 461, 473, "void ParticleSystem::findExactContactPoint("),
+    ("Particles/updateFunctions.cpp", 1431, 1509, "void ParticleSystem::GatherRigidBodyCollisions()"),
+    ("Particles/updateFunctions.cpp", 1511, 1578, "void ParticleSystem::GatherAugmentedRealityCollisions()"),
+    ("Particles/updateFunctions.cpp", 1580, 1874, "void ParticleSystem::SequentialImpulseSolver()"),
+]
+
 STUB_HEADERS = {
     "cuda_gl_interop.h": "#pragma once\n",
     "helper_cuda_gl.h": "#pragma once\n",
@@ -68,9 +80,9 @@ def reference_root() -> Path:
     return Path(os.environ.get("AR_REFERENCE_ROOT", "/root/reference"))
 
 
-def extract(ar_sim: Path) -> str:
+def extract(ar_sim: Path, ranges=None) -> str:
     parts = []
-    for rel, first, last, expect in RANGES:
+    for rel, first, last, expect in (RANGES if ranges is None else ranges):
         lines = (ar_sim / rel).read_text(encoding="latin-1").splitlines()
         head = lines[first - 1]
         if expect not in head:
@@ -95,6 +107,7 @@ def build(verbose: bool = False) -> bool:
     for name, text in STUB_HEADERS.items():
         (shim / name).write_text(text)
     (OUT / "extracted.inc").write_text(extract(ar_sim))
+    (OUT / "extracted_members.inc").write_text(extract(ar_sim, MEMBER_RANGES))
     so = OUT / "libref_cpu.so"
     cmd = [
         "g++", "-std=c++14", "-O2", "-fopenmp", "-fPIC", "-shared",

@@ -441,3 +441,122 @@ void refcpu_wall_collisions(const float* particle_pos4, const float* rb_pos4,
 }
 
 }  // extern "C"
+
+// ---- the sequential-impulse host loops (ParticleSystem members) ---------------------------
+// The reference's default update gathers one contact per colliding particle and solves them
+// with a sequential-impulse loop on the host (Particles/updateFunctions.cpp:1431-1874).  Those
+// are member functions of ParticleSystem working on host copies of its device arrays.  The
+// stand-in class below holds exactly the members the extracted bodies use; every array it
+// points to is host memory here, so the device<->host copies become memcpy.  The solver's
+// tail call re-poses the particles with the computeGlobalAttributes kernel body, launched
+// over the grid the reference wrapper uses (Kernels/rigidBodyKernels.cu:423-447).
+#include <cstdlib>
+using std::abs;  // the reference's MSVC build resolves abs(float) to the float overload
+
+namespace {
+cudaError_t host_copy(void* dst, const void* src, size_t bytes) {
+  std::memcpy(dst, src, bytes);
+  return cudaSuccess;
+}
+}  // namespace
+
+void computeGlobalAttributesWrapper(float4* CMs, float4* rigidVel, float4* relativePos,
+                                    float4* globalPos, float4* globalVel, glm::quat* rbQuaternion,
+                                    float4* rbAngularVelocity, int* rigidBodyIndex,
+                                    int numParticles, int numThreads) {
+  launch(numParticles, numThreads, true, [&] {
+    computeGlobalAttributes(CMs, rigidVel, relativePos, globalPos, globalVel, rbQuaternion,
+                            rbAngularVelocity, rigidBodyIndex, numParticles);
+  });
+}
+
+class ParticleSystem {
+ public:
+  SimParams m_params;
+  int numRigidBodies = 0, m_numParticles = 0, numberOfRangeData = 0, numThreads = 128;
+  int* particlesPerObjectThrown = nullptr;
+  float4 *rbPositions = nullptr, *rbVelocities = nullptr, *rbAngularVelocity = nullptr;
+  float4 *relativePos = nullptr, *dPos = nullptr, *m_dVel = nullptr;
+  float4 *staticNorm = nullptr, *contact_normal = nullptr;
+  glm::mat3* rbCurrentInertia = nullptr;
+  float* rbMass = nullptr;
+  glm::quat* rbQuaternion = nullptr;
+  int* rbIndices = nullptr;
+  float* contactDistance = nullptr;
+  int *collidingRigidBodyIndex = nullptr, *collidingParticleIndex = nullptr;
+  std::vector<float4> ContactNormal, ContactPoint;
+  std::vector<int> ContactRigidBody_1, ContactRigidBody_2;
+  std::vector<float> ContactAccumulatedImpulse, ContactAccumulatedFriction,
+      ContactAccumulatedFriction_2, ContactBias;
+  void findExactContactPoint(const float4& p1, const float4& p2, const float& r1,
+                             const float& r2, float4& cp, float4& cn);
+  void GatherRigidBodyCollisions();
+  void GatherAugmentedRealityCollisions();
+  void SequentialImpulseSolver();
+};
+
+#undef checkCudaErrors
+#define checkCudaErrors(val) (val)
+#define cudaMemcpy(dst, src, bytes, kind) host_copy((dst), (src), (bytes))
+#define cudaGetLastError() cudaSuccess
+#define cudaDeviceSynchronize() cudaSuccess
+#include "extracted_members.inc"
+#undef cudaMemcpy
+#undef cudaGetLastError
+#undef cudaDeviceSynchronize
+
+extern "C" {
+
+// One gather (GatherRigidBodyCollisions, or GatherAugmentedRealityCollisions when
+// `static_scene` is set: then contact_body is unused and scene_normals4 gives the normals)
+// followed, when iterations_run > 0, by SequentialImpulseSolver on the gathered contacts.
+// Body state is updated in place (vel4, ang4); pos4 / pvel4 / quat4 receive the re-posed
+// particles.  Writes up to `capacity` contacts (normal, point, body1, body2, bias and the three
+// accumulated impulses after the solve) and returns the number gathered.
+int refcpu_sis_step(const void* sim_params, int num_bodies, int n, const int* particles_per_rb,
+                    float* cms4, float* vel4, float* ang4, float* inertia9, float* mass,
+                    float* rel4, float* pos4, float* pvel4, float* quat4, int* rb_idx,
+                    float* contact_distance, int* contact_body, int* contact_particle,
+                    float* scene_normals4, int num_scene_points, int static_scene,
+                    int solve, int capacity, float* out_normal4, float* out_point4,
+                    int* out_body1, int* out_body2, float* out_bias, float* out_acc) {
+  ParticleSystem ps;
+  std::memcpy(&ps.m_params, sim_params, sizeof(SimParams));
+  ps.numRigidBodies = num_bodies;
+  ps.m_numParticles = n;
+  ps.numberOfRangeData = num_scene_points;
+  ps.particlesPerObjectThrown = const_cast<int*>(particles_per_rb);
+  ps.rbPositions = (float4*)cms4;
+  ps.rbVelocities = (float4*)vel4;
+  ps.rbAngularVelocity = (float4*)ang4;
+  ps.relativePos = (float4*)rel4;
+  ps.dPos = (float4*)pos4;
+  ps.m_dVel = (float4*)pvel4;
+  ps.staticNorm = (float4*)scene_normals4;
+  std::vector<float4> cn_scratch((size_t)n);
+  ps.contact_normal = cn_scratch.data();
+  ps.rbCurrentInertia = (glm::mat3*)inertia9;
+  ps.rbMass = mass;
+  ps.rbQuaternion = (glm::quat*)quat4;
+  ps.rbIndices = rb_idx;
+  ps.contactDistance = contact_distance;
+  ps.collidingRigidBodyIndex = contact_body;
+  ps.collidingParticleIndex = contact_particle;
+  if (static_scene) ps.GatherAugmentedRealityCollisions();
+  else ps.GatherRigidBodyCollisions();
+  if (solve) ps.SequentialImpulseSolver();
+  const int k = (int)ps.ContactNormal.size();
+  for (int c = 0; c < k && c < capacity; ++c) {
+    std::memcpy(out_normal4 + 4 * (size_t)c, &ps.ContactNormal[c], 16);
+    std::memcpy(out_point4 + 4 * (size_t)c, &ps.ContactPoint[c], 16);
+    out_body1[c] = ps.ContactRigidBody_1[c];
+    out_body2[c] = ps.ContactRigidBody_2[c];
+    out_bias[c] = ps.ContactBias[c];
+    out_acc[3 * (size_t)c] = ps.ContactAccumulatedImpulse[c];
+    out_acc[3 * (size_t)c + 1] = ps.ContactAccumulatedFriction[c];
+    out_acc[3 * (size_t)c + 2] = ps.ContactAccumulatedFriction_2[c];
+  }
+  return k;
+}
+
+}  // extern "C"

@@ -244,6 +244,52 @@ def sis_case(seed: int):
                 contact_distance=cd, contact_body=cb, contact_particle=cp)
 
 
+def sis_solve_case(seed: int):
+    """The reference's sequential-impulse host loops (GatherRigidBodyCollisions /
+    GatherAugmentedRealityCollisions, then SequentialImpulseSolver; Particles/
+    updateFunctions.cpp:1431-1874) on seeded body state.  rb_*: the grid contacts of sis_find
+    (body against body); ar_*: one contact per chosen particle against a static point cloud
+    with seeded normals (body against scene, the solver's one-body branch)."""
+    f = sis_case(5)
+    d = dem_case(5)
+    rng = np.random.default_rng(seed)
+    nb = len(d["offsets"]) - 1
+    cms = np.zeros((nb, 4), np.float32)
+    cms[:, :3] = rng.uniform(0.2, 0.8, (nb, 3))
+    vel = rng.normal(0, 1, (nb, 4)).astype(np.float32)
+    ang = rng.normal(0, 1, (nb, 4)).astype(np.float32)
+    vel[:, 3] = ang[:, 3] = 0
+    rel = d["rel"].copy()
+    rel[:, 3] = 0
+    prm = ref.sim_params(float(f["radius"]), (0, 0, 0), float(f["cell"]), f["dims"],
+                         gravity=(0.0, -9.81, 0.0))
+    prm.rb_restitution, prm.rb_friction = 0.5, 0.1
+    prm.ar_restitution, prm.ar_friction = 0.3, 0.3
+    ib, mass = d["body_inv_inertia"].astype(np.float32), d["body_mass"].astype(np.float32)
+    rb = ref.sis_step(prm, f["rb"], d["offsets"], cms, vel, ang, ib, mass, rel,
+                      f["contact_distance"], f["contact_body"], f["contact_particle"])
+    n, m = len(f["rb"]), 500
+    nrm = rng.normal(0, 1, (m, 3))
+    nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    scene_normals = np.concatenate([nrm, np.zeros((m, 1))], 1).astype(np.float32)
+    ar_cd = np.where(rng.random(n) < 0.05, rng.uniform(1e-4, 1e-3, n), 0).astype(np.float32)
+    ar_cp = rng.integers(0, m, n).astype(np.int32)
+    ar = ref.sis_step(prm, f["rb"], d["offsets"], cms, vel, ang, ib, mass, rel, ar_cd, None,
+                      ar_cp, scene_normals4=scene_normals)
+    out = dict(radius=f["radius"], cell=f["cell"], dims=f["dims"], rb_idx=f["rb"],
+               offsets=d["offsets"], cms=cms, vel=vel, ang=ang, inv_inertia=ib, mass=mass,
+               rel=rel, contact_distance=f["contact_distance"], contact_body=f["contact_body"],
+               contact_particle=f["contact_particle"], scene_normals=scene_normals,
+               ar_contact_distance=ar_cd, ar_contact_particle=ar_cp,
+               restitution=np.float32(0.5), rb_friction=np.float32(0.1),
+               ar_restitution=np.float32(0.3), ar_friction=np.float32(0.3),
+               gravity_y=np.float32(-9.81), iterations=np.int32(18))
+    for tag, r in (("rb", rb), ("ar", ar)):
+        for key in ("normal", "point", "body1", "body2", "bias", "acc", "vel", "ang"):
+            out[f"{tag}_{key}"] = r[key]
+    return out
+
+
 CASES = {
     "lbvh_uniform": lambda: lbvh_case(11, 3000, 0.0),
     "lbvh_duplicates": lambda: lbvh_case(12, 3000, 0.2),
@@ -252,6 +298,7 @@ CASES = {
     "reference_extra": lambda: extra_case(21),
     "static_scene": lambda: static_scene_case(31),
     "sis_find": lambda: sis_case(5),
+    "sis_solve": lambda: sis_solve_case(2),
 }
 
 

@@ -227,3 +227,37 @@ def test_sis_steps_match_oracle(ctx):
         for k in ("vel", "ang", "rel", "pos", "pvel"):
             assert np.array_equal(after[k], ref[k]), k
     assert total > 500
+
+
+def test_gather_and_solver_match_the_reference_host_loops(ctx):
+    """ar_gather_contacts and ar_sequential_impulse against tests/golden/sis_solve.npz: the
+    output of the reference's own GatherRigidBodyCollisions / GatherAugmentedRealityCollisions
+    and SequentialImpulseSolver (Particles/updateFunctions.cpp:1431-1874) built for the host.
+    Body-body contacts gathered and solved on the device; the reference's one-body (static
+    scene) contacts solved on the device.  Bit for bit."""
+    z = np.load(GOLDEN / "sis_solve.npz")
+    n = len(z["rb_idx"])
+    prm = api.sim_params(float(z["radius"]), (0, 0, 0), float(z["cell"]), z["dims"])
+    prm.rb_restitution = float(z["restitution"])
+    keys = ("normal", "point", "body1", "body2", "bias")
+    out = {"normal": empty((n, 4)), "point": empty((n, 4)), "body1": empty(n, torch.int32),
+           "body2": empty(n, torch.int32), "bias": empty(n), "acc0": empty(n), "acc1": empty(n),
+           "acc2": empty(n)}
+    cnt = empty(1, torch.int32)
+    call("ar_gather_contacts", ctx.handle, C.byref(prm), n, P(dev(z["rb_idx"])), P(dev(z["cms"])),
+         P(dev(z["vel"])), P(dev(z["ang"])), P(dev(z["rel"])), P(dev(z["contact_distance"])),
+         P(dev(z["contact_body"])), P(dev(z["contact_particle"])), n, P(out["normal"]),
+         P(out["point"]), P(out["body1"]), P(out["body2"]), P(out["bias"]), P(out["acc0"]),
+         P(out["acc1"]), P(out["acc2"]), P(cnt), S())
+    ctx.check()
+    k = int(host(cnt)[0])
+    assert k == len(z["rb_body1"]) > 1000
+    gathered = {key: host(out[key])[:k] for key in keys}
+    for key in keys:
+        assert np.array_equal(gathered[key], z["rb_" + key]), key
+    for tag, contacts in (("rb", gathered), ("ar", {key: z["ar_" + key] for key in keys})):
+        v, w, acc = _solve_gpu(ctx, contacts, z["cms"], z["vel"], z["ang"], z["inv_inertia"],
+                               z["mass"], int(z["iterations"]))
+        assert np.array_equal(v, z[tag + "_vel"]) and np.array_equal(w, z[tag + "_ang"]), tag
+        for i in range(3):
+            assert np.array_equal(acc[i], z[tag + "_acc"][:, i]), (tag, i)
