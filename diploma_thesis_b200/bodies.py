@@ -6,12 +6,15 @@ the file's scale (the shipped files use particle radius 1/64 at scale 1.0, e.g. 
 4 x 4 x 4 lattice at spacing 2/64).
 
 A body built from a file is centred the way the reference centres it
-(RigidBodyAddition.cpp:1598-1630): the mean of the points is subtracted, plus a per-model
-shift of a few particle radii (bunny: (-r, r, -r); banana: (0, 3r, 0); teapot: (0, 2r, 0)).
-Its inertia is the particle sum sum_i (|r_i|^2 E - r_i r_i^T) for unit particle mass
-(RigidBodyAddition.cpp:1631-1650).  With ``reference_inertia=True`` the reference's
-hand-set tensors for some model / scale pairs replace the sum (RigidBodyAddition.cpp:1683-
-1756), and the body mass is 1 as the reference keeps it (rbMass, RigidBodyAddition.cpp:1873).
+(RigidBodyAddition.cpp:1579-1624): the mean of the points (summed in file order in float) is
+subtracted, plus a per-model shift of a few particle radii (bunny: (-r, r, -r); banana:
+(0, 3r, 0); teapot: (0, 2r, 0)).  Its inertia is the particle sum sum_i (|r_i|^2 E - r_i r_i^T)
+for unit particle mass.  With ``reference_inertia=True`` the inverse inertia is the one the
+reference computes (RigidBodyAddition.cpp:1625-1756): the sum accumulated in float onto a
+default-constructed glm::mat3 -- which glm 0.9.7 initialises to the identity, so the tensor is
+E + sum -- then the hand-set tensors for some model / scale pairs, glm::inverse, and hand-set
+inverse tensors for the cube; the body mass is 1 as the reference keeps it (rbMass,
+RigidBodyAddition.cpp:1873).
 """
 from __future__ import annotations
 
@@ -37,6 +40,7 @@ _INERTIA_DIAG = {
 _INVERSE_INERTIA_DIAG = {
     ("cube", 1.0): 6.0 / (0.1 * 0.1),
     ("cube", 2.0): 6.0 / (0.2 * 0.2),
+    ("cube", 1.5): 6.0 / (0.15 * 0.15),
 }
 
 
@@ -68,24 +72,83 @@ def read_points(path: str | Path) -> np.ndarray:
 
 
 def centre(points: np.ndarray, model: str, radius: float) -> np.ndarray:
-    """Body-frame offsets: points minus their mean, minus the model's shift."""
+    """Body-frame offsets: points minus their mean (a float sum in file order, then divided by
+    the count), minus the model's shift."""
     p = np.asarray(points, np.float32)
-    cm = p.sum(0, dtype=np.float32) / np.float32(len(p))
+    cm = np.add.accumulate(p, axis=0, dtype=np.float32)[-1] / np.float32(len(p))
     shift = np.asarray(_CM_SHIFT.get(model, (0.0, 0.0, 0.0)), np.float32) * np.float32(radius)
     return p - (cm + shift)
 
 
+def _glm_inverse3(m):
+    """glm 0.9.7 compute_inverse for tmat3x3<float> (glm/detail/type_mat3x3.inl:37-56), in float;
+    m[c][r] is column c, row r."""
+    f = np.float32
+    det = (f(m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2]))
+           - f(m[1][0] * (m[0][1] * m[2][2] - m[2][1] * m[0][2]))
+           + f(m[2][0] * (m[0][1] * m[1][2] - m[1][1] * m[0][2])))
+    one = f(1) / f(det)
+    inv = [[f(0)] * 3 for _ in range(3)]
+    inv[0][0] = (m[1][1] * m[2][2] - m[2][1] * m[1][2]) * one
+    inv[1][0] = -(m[1][0] * m[2][2] - m[2][0] * m[1][2]) * one
+    inv[2][0] = (m[1][0] * m[2][1] - m[2][0] * m[1][1]) * one
+    inv[0][1] = -(m[0][1] * m[2][2] - m[2][1] * m[0][2]) * one
+    inv[1][1] = (m[0][0] * m[2][2] - m[2][0] * m[0][2]) * one
+    inv[2][1] = -(m[0][0] * m[2][1] - m[2][0] * m[0][1]) * one
+    inv[0][2] = (m[0][1] * m[1][2] - m[1][1] * m[0][2]) * one
+    inv[1][2] = -(m[0][0] * m[1][2] - m[1][0] * m[0][2]) * one
+    inv[2][2] = (m[0][0] * m[1][1] - m[1][0] * m[0][1]) * one
+    return inv
+
+
+def _reference_inverse_inertia(rel: np.ndarray, model: str, scale: float) -> np.ndarray:
+    """The inverse inertia initObject computes (RigidBodyAddition.cpp:1625-1756), operation for
+    operation in float: E + sum over particles, the hand-set tensors, glm::inverse, the cube's
+    hand-set inverse tensors."""
+    f = np.float32
+    t = [[f(1) if c == r else f(0) for r in range(3)] for c in range(3)]
+    for x, y, z in np.asarray(rel, np.float32):
+        t[0][0] = t[0][0] + (y * y + z * z)
+        t[0][1] = t[0][1] - x * y
+        t[0][2] = t[0][2] - x * z
+        t[1][0] = t[1][0] - x * y
+        t[1][1] = t[1][1] + (x * x + z * z)
+        t[1][2] = t[1][2] - y * z
+        t[2][0] = t[2][0] - x * z
+        t[2][1] = t[2][1] - y * z
+        t[2][2] = t[2][2] + (x * x + y * y)
+    sf = f(scale)
+
+    def near_f(v):  # abs(scale - v.f) < 0.0001, the difference taken in float
+        return abs(float(sf - f(v))) < 0.0001
+
+    def diag(d):
+        return [[f(d[c]) if c == r else f(0) for r in range(3)] for c in range(3)]
+
+    for m_, chain in (("banana", (2.0, 1.5, 1.0)), ("bunny", (1.5,)), ("teapot", (2.0, 1.5))):
+        if model == m_:
+            for v in chain:  # an if / else-if chain: the first match wins
+                if near_f(v):
+                    t = diag(_INERTIA_DIAG[(model, v)])
+                    break
+    t = _glm_inverse3(t)
+    if model == "cube":
+        if near_f(1.0):
+            t = diag([_INVERSE_INERTIA_DIAG[("cube", 1.0)]] * 3)
+        elif near_f(2.0):
+            t = diag([_INVERSE_INERTIA_DIAG[("cube", 2.0)]] * 3)
+        if abs(float(sf) - 1.5) < 0.0001:  # this one compares in double
+            t = diag([_INVERSE_INERTIA_DIAG[("cube", 1.5)]] * 3)
+    return np.array([t[c][r] for c in range(3) for r in range(3)], np.float32)
+
+
 def inverse_inertia(rel: np.ndarray, model: str = "", scale: float = 1.0,
                     reference_inertia: bool = False) -> np.ndarray:
-    """Inverse inertia (glm::mat3 layout, 9 floats) of unit-mass particles at offsets `rel`,
-    or the reference's hand-set tensor for this model and scale."""
+    """Inverse inertia (glm::mat3 layout, 9 floats) of unit-mass particles at offsets `rel`
+    (the physical tensor, computed in double), or with ``reference_inertia`` the one the
+    reference computes for this model and scale."""
     if reference_inertia:
-        for (m, s), v in _INVERSE_INERTIA_DIAG.items():
-            if m == model and abs(scale - s) < 1e-4:
-                return np.diag([v, v, v]).astype(np.float32).T.reshape(9)
-        for (m, s), d in _INERTIA_DIAG.items():
-            if m == model and abs(scale - s) < 1e-4:
-                return np.diag(1.0 / np.asarray(d, np.float64)).astype(np.float32).T.reshape(9)
+        return _reference_inverse_inertia(rel, model, scale)
     r = np.asarray(rel, np.float64)
     inertia = (r * r).sum() * np.eye(3) - r.T @ r
     return np.linalg.inv(inertia).astype(np.float32).T.reshape(9)

@@ -323,3 +323,19 @@ def sis_step(params, rb_idx, offsets, cms4, vel4, ang4, inertia9, mass, rel4, co
     res = {key: v[:k] for key, v in out.items()}
     res.update({"vel": vel, "ang": ang, "rel": rel, "pos": pos, "pvel": pvel, "count": k})
     return res
+
+
+def init_object(path, model: str, scale: float, radius: float):
+    """ParticleSystem::initObject's body set-up (RigidBodies/RigidBodyAddition.cpp:1576-1756) on
+    a particle-body file -> (centred offsets [N, 3], inverse inertia [9], glm::mat3 order)."""
+    from pathlib import Path as _P
+    text = _P(path).read_bytes()
+    n = int(text.split(b"\n", 1)[0].split()[0])
+    rel = np.zeros((n, 4), np.float32)
+    inv = np.zeros(9, np.float32)
+    L = lib()
+    L.refcpu_init_object.restype = C.c_int
+    got = L.refcpu_init_object(C.c_char_p(text), C.c_char_p(model.encode()), C.c_float(scale),
+                               C.c_float(radius), _p(rel), _p(inv))
+    assert got == n
+    return rel[:, :3].copy(), inv

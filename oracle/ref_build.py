@@ -68,6 +68,14 @@ MEMBER_RANGES = [
     ("Particles/updateFunctions.cpp", 1580, 1874, "void ParticleSystem::SequentialImpulseSolver()"),
 ]
 
+# The part of ParticleSystem::initObject that turns a particle-body file into a body: centre of
+# mass, per-model shift, the inertia sum (on a default-constructed glm::mat3, i.e. starting
+# from the identity), glm::inverse and the hand-set tensors.  A block of statements, included
+# into a function of oracle/ref_cpu_driver.cpp that supplies the locals it uses.
+INIT_OBJECT_RANGE = [
+    ("RigidBodies/RigidBodyAddition.cpp", 1576, 1756, "float maxDistance = -100000000;"),
+]
+
 STUB_HEADERS = {
     "cuda_gl_interop.h": "#pragma once\n",
     "helper_cuda_gl.h": "#pragma once\n",
@@ -108,6 +116,7 @@ def build(verbose: bool = False) -> bool:
         (shim / name).write_text(text)
     (OUT / "extracted.inc").write_text(extract(ar_sim))
     (OUT / "extracted_members.inc").write_text(extract(ar_sim, MEMBER_RANGES))
+    (OUT / "extracted_init_object.inc").write_text(extract(ar_sim, INIT_OBJECT_RANGE))
     so = OUT / "libref_cpu.so"
     cmd = [
         "g++", "-std=c++14", "-O2", "-fopenmp", "-fPIC", "-shared",

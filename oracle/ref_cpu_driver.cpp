@@ -560,3 +560,36 @@ int refcpu_sis_step(const void* sim_params, int num_bodies, int n, const int* pa
 }
 
 }  // extern "C"
+
+// ---- particle-body files: the body set-up of ParticleSystem::initObject -------------------
+// (RigidBodies/RigidBodyAddition.cpp:1576-1756, extracted into
+// oracle/_ref/extracted_init_object.inc.)  The file's text is given as a string; the
+// statements run with the locals they expect: the particle array m_hPos (4 floats per
+// particle), the stream positioned after the count line, the model name, scale and particle
+// radius, and a particle velocity array it zeroes.  Returns the particle count; writes the
+// centred offsets and the inverse inertia
+// (glm::mat3 memory order).
+#include <sstream>
+#include <string>
+
+extern "C" int refcpu_init_object(const char* text, const char* modelName, float scale,
+                                  float particle_radius, float* rel4, float* inv_inertia9) {
+  std::istringstream myfile{std::string(text)};
+  std::string line;
+  std::getline(myfile, line);
+  const int particles = std::atoi(line.c_str());
+  const int start = 0;
+  std::vector<float> h_pos(4 * (size_t)particles), h_vel(4 * (size_t)particles);
+  float* m_hPos = h_pos.data();
+  float* m_hVel = h_vel.data();
+  struct {
+    float particleRadius;
+  } m_params{particle_radius};
+  const bool initializedNow = true;
+  int m_numParticles = 0;
+#include "extracted_init_object.inc"
+  (void)m_numParticles;
+  std::memcpy(rel4, m_hPos, 4 * sizeof(float) * (size_t)particles);
+  std::memcpy(inv_inertia9, &inertiaTensor[0][0], 9 * sizeof(float));
+  return particles;
+}

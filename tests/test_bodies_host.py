@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from diploma_thesis_b200 import bodies, scenes
-from oracle import cpu
+from oracle import cpu, ref
 
 
 def _write_cube(root: Path, k: int = 4, spacing: float = 2 / 64, suffix: str = "1_0"):
@@ -72,11 +72,42 @@ def test_scene_from_files_steps_on_the_oracle(tmp_path):
     assert (np.abs(out["pforce"]).sum(1) > 0).sum() > 0  # the first two cubes touch
 
 
-@pytest.mark.skipif(not os.environ.get("AR_SIM_DATA"), reason="AR_SIM_DATA not set")
-def test_shipped_models():
-    root = Path(os.environ["AR_SIM_DATA"])
+REF_ROOT = Path(os.environ.get("AR_REFERENCE_ROOT", "/root/reference"))
+DATA = REF_ROOT / "AR_Sim" / "Data" / "OBJparticles"
+
+
+@pytest.mark.skipif(not DATA.is_dir(), reason="the reference checkout's particle-body files are absent")
+def test_shipped_models_read_and_centre():
+    """Every shipped model and scale (the reference's own Data/OBJparticles files) loads, with
+    the counts the files declare, centred offsets whose mean is the model's shift, and a finite
+    physical inverse inertia."""
+    r = 1 / 64
     for model in ("cube", "bunny", "banana", "teapot"):
         for scale in (1.0, 1.5, 2.0, 2.5):
-            rel, inv, m = bodies.load_body(root, model, scale, 1 / 64)
-            assert len(rel) > 0 and np.isfinite(inv).all() and m == len(rel)
-    assert len(bodies.read_points(bodies.body_file(root, "cube", 1.0))) == 64
+            path = bodies.body_file(DATA, model, scale)
+            n = int(path.read_text().split()[0])
+            rel, inv, m = bodies.load_body(DATA, model, scale, r)
+            assert rel.shape == (n, 3) and m == n and np.isfinite(inv).all()
+            shift = np.asarray(bodies._CM_SHIFT.get(model, (0, 0, 0))) * r
+            assert np.allclose(rel.astype(np.float64).mean(0), -shift, atol=1e-5)
+    assert len(bodies.read_points(bodies.body_file(DATA, "cube", 1.0))) == 64
+
+
+@pytest.mark.skipif(not DATA.is_dir() or not ref.available(),
+                    reason="needs the reference checkout and its host build (oracle/_ref)")
+def test_shipped_models_equal_the_reference_init_object():
+    """bodies.load_body(..., reference_inertia=True) against the reference's own initObject body
+    set-up (RigidBodyAddition.cpp:1576-1756, built for the host by oracle/ref_build.py) on every
+    shipped model and scale: the centred offsets and the inverse inertia bit for bit.  That
+    includes the reference's quirks: the inertia sum starts from the identity (a
+    default-constructed glm::mat3), the hand-set tensors (banana, bunny 1.5, teapot) and hand-set
+    inverse tensors (cube 1.0, 1.5, 2.0)."""
+    r = 1 / 64
+    for model in ("cube", "bunny", "banana", "teapot"):
+        for scale in (1.0, 1.5, 2.0, 2.5):
+            rel, inv, m = bodies.load_body(DATA, model, scale, r, reference_inertia=True)
+            want_rel, want_inv = ref.init_object(bodies.body_file(DATA, model, scale), model,
+                                                 scale, r)
+            assert np.array_equal(rel, want_rel), (model, scale)
+            assert np.array_equal(inv, want_inv), (model, scale)
+            assert m == 1.0
