@@ -111,6 +111,11 @@ SIGNATURES = {
     "ar_reorder_cells": [P, P, P, P, P, I, C.c_uint32, P, P, P, P, S],
     "ar_collide_grid_dem": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, I, P, P, S],
     "ar_collide_static_scene_dem": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, I, P, P, P, S],
+    "ar_collide_static_scene_impulse": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, P, P,
+                                        P, I, P, P, P, P, P, S],
+    "ar_find_contacts_static_scene": [P, C.POINTER(SimParams), P, P, P, P, P, P, I, P, P, P, S],
+    "ar_gather_static_contacts": [P, C.POINTER(SimParams), I, P, P, P, P, P, P, P, P, I, P, P, P,
+                                  P, P, P, P, P, P, S],
     "ar_reduce_bodies": [P, P, P, P, I, P, P, S],
     "ar_reduce_impulses": [P, P, P, P, I, P, P, P, P, S],
     "ar_integrate_reference": [P, C.POINTER(SimParams), F, I, P, P, P, P, P, P, P, P, P, S],

@@ -287,6 +287,54 @@ AR_API ar_status ar_collide_static_scene_dem(ar_ctx* ctx, const ar_sim_params* p
                                              float* p_linear4, float* p_angular4,
                                              float* color4, ar_stream_t stream);
 
+/* Impulse variant of the same collision (ARcollisionsUniformGridKernel with
+ * collideARSpheresBaraffExact, Kernels/RB_UniformGridKernels.cu:420-667): per sorted particle,
+ * for each scene point in its cell closer than r + scene_radii[point], an impulse
+ * j = -(1 + ARrestitution) (v . n) / (((I^-1 (r_c x n)) x r_c) . n + 1/m) along n (the unit
+ * vector from the point to the particle), r_c = contact point - body centre; p_force4[orig] and
+ * p_torque4[orig] receive the sums and p_count[orig] the number of impulses (may be NULL).  As
+ * in the reference, each of the 27 neighbour iterations examines the particle's own cell.
+ * inertia9 / mass are the bodies' current inverse inertia and mass, indexed by rb_idx[orig].
+ * A free particle (rb_idx -1) has its force added to new_vel4 instead (zero inverse inertia,
+ * unit mass).  color4 (may be NULL): (0, 1, 0, 0) on any impulse. */
+AR_API ar_status ar_collide_static_scene_impulse(
+    ar_ctx* ctx, const ar_sim_params* params, const int32_t* rb_idx, const float* rel4,
+    const float* inertia9, const float* mass, const float* scene_radii, const float* sorted_pos4,
+    const float* sorted_vel4, const float* scene_sorted_pos4, const uint32_t* grid_idx,
+    const uint32_t* scene_grid_idx, const uint32_t* scene_cell_start,
+    const uint32_t* scene_cell_end, int n, float* p_force4, float* p_torque4, int32_t* p_count,
+    float* new_vel4, float* color4, ar_stream_t stream);
+/* Deepest contact of each particle with the static scene (FindAugmentedRealityCollisionsUniform-
+ * GridKernel, Kernels/RB_UniformGridKernels.cu:879-996): 27 neighbour cells of the scene grid,
+ * a point deepens the contact when 2r - d exceeds the current contact_distance[orig] (the
+ * caller initialises it, 0 = none), which then records 2r - d and the point's cloud index in
+ * contact_point[orig].  color4 (may be NULL): green on any contact, else blue. */
+AR_API ar_status ar_find_contacts_static_scene(ar_ctx* ctx, const ar_sim_params* params,
+                                               const float* sorted_pos4,
+                                               const float* scene_sorted_pos4,
+                                               const uint32_t* grid_idx,
+                                               const uint32_t* scene_grid_idx,
+                                               const uint32_t* scene_cell_start,
+                                               const uint32_t* scene_cell_end, int n,
+                                               float* contact_distance, int32_t* contact_point,
+                                               float* color4, ar_stream_t stream);
+/* GatherAugmentedRealityCollisions (Particles/updateFunctions.cpp:1511-1578) on the device: one
+ * contact per particle with contact_distance > 0, in particle order: normal = scene_normals4 of
+ * the contact point, point = rel + centre of the body, body1 = rb_idx, body2 = -1,
+ * bias = ARrestitution ((v + w x rel) . n), accumulated impulses zero.  Writes the count to
+ * d_count; more than `capacity` contacts raise AR_ERR_OVERFLOW (read with ar_ctx_status).  The
+ * list feeds ar_sequential_impulse. */
+AR_API ar_status ar_gather_static_contacts(ar_ctx* ctx, const ar_sim_params* params, int n,
+                                           const int32_t* rb_idx, const float* cms4,
+                                           const float* vel4, const float* ang4,
+                                           const float* rel4, const float* scene_normals4,
+                                           const float* contact_distance,
+                                           const int32_t* contact_point, int capacity,
+                                           float* normal4, float* point4, int32_t* body1,
+                                           int32_t* body2, float* bias, float* acc_impulse,
+                                           float* acc_friction, float* acc_friction2,
+                                           int32_t* d_count, ar_stream_t stream);
+
 /* ---- (a15) DEM contact forces on the grid ------------------------------------------------------
  * FindAndHandleRigidBodyCollisionsUniformGridKernel (RigidBodies/UniformGridDEM.cu:57-241):
  * per sorted particle, the 27 neighbour cells in z, y, x order (-1..1), occupants in sorted

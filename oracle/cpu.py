@@ -482,3 +482,56 @@ def sis_solve(state: dict, rb_idx, origin, cell, dims, radius, restitution=1.0,
                                             state["rel"])
     return {"vel": vel, "ang": ang, "rel": rel, "pos": ppos, "pvel": ppvel,
             "contacts": len(contacts["body1"]), "acc": a0}
+
+
+# ---- static scene: impulse variant, deepest contacts, contact gather -------------------------
+_L.or_ar_collide_impulse.restype = None
+_L.or_ar_find_contacts.restype = None
+_L.or_gather_static_contacts.restype = C.c_long
+
+
+def ar_collide_impulse(origin, cell, dims, radius, restitution, rb_idx, rel4, inertia9, mass,
+                       scene_radii, spos4, svel4, scene_spos4, gidx, scene_gidx, cstart, cend,
+                       new_vel4=None):
+    """ARcollisionsUniformGridKernel -> (force, torque, count, colour, new_vel4)."""
+    n = len(spos4)
+    g6 = _f32(list(origin) + [cell] * 3)
+    pf, pt, color = (np.zeros((n, 4), np.float32) for _ in range(3))
+    count = np.zeros(n, np.int32)
+    nv = np.zeros((n, 4), np.float32) if new_vel4 is None else _f32(new_vel4).copy()
+    _L.or_ar_collide_impulse(_p(g6), _p(_u32(dims)), C.c_float(radius), C.c_float(restitution),
+                             _p(_i32(rb_idx)), _p(_f32(rel4)), _p(_f32(inertia9)),
+                             _p(_f32(mass)), _p(_f32(scene_radii)), _p(_f32(spos4)),
+                             _p(_f32(svel4)), _p(_f32(scene_spos4)), _p(_u32(gidx)),
+                             _p(_u32(scene_gidx)), _p(_u32(cstart)), _p(_u32(cend)), n, _p(pf),
+                             _p(pt), _p(count), _p(nv), _p(color))
+    return pf, pt, count, color, nv
+
+
+def ar_find_contacts(origin, cell, dims, radius, spos4, scene_spos4, gidx, scene_gidx, cstart,
+                     cend, contact_distance, contact_point):
+    """FindAugmentedRealityCollisionsUniformGridKernel -> (distance, point, colour)."""
+    n = len(spos4)
+    g6 = _f32(list(origin) + [cell] * 3)
+    cd, cp = _f32(contact_distance).copy(), _i32(contact_point).copy()
+    color = np.zeros((n, 4), np.float32)
+    _L.or_ar_find_contacts(_p(g6), _p(_u32(dims)), C.c_float(radius), _p(_f32(spos4)),
+                           _p(_f32(scene_spos4)), _p(_u32(gidx)), _p(_u32(scene_gidx)),
+                           _p(_u32(cstart)), _p(_u32(cend)), n, _p(cd), _p(cp), _p(color))
+    return cd, cp, color
+
+
+def gather_static_contacts(restitution, rb_idx, cms4, vel4, ang4, rel4, scene_normals4,
+                           contact_distance, contact_point) -> dict:
+    """GatherAugmentedRealityCollisions: the contact list in particle order."""
+    n = len(rb_idx)
+    out = {"normal": np.zeros((n, 4), np.float32), "point": np.zeros((n, 4), np.float32),
+           "body1": np.zeros(n, np.int32), "body2": np.zeros(n, np.int32),
+           "bias": np.zeros(n, np.float32)}
+    c = _L.or_gather_static_contacts(C.c_float(restitution), C.c_long(n), _p(_i32(rb_idx)),
+                                     _p(_f32(cms4)), _p(_f32(vel4)), _p(_f32(ang4)),
+                                     _p(_f32(rel4)), _p(_f32(scene_normals4)),
+                                     _p(_f32(contact_distance)), _p(_i32(contact_point)),
+                                     _p(out["normal"]), _p(out["point"]), _p(out["body1"]),
+                                     _p(out["body2"]), _p(out["bias"]))
+    return {k: v[:c] for k, v in out.items()}

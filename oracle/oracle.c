@@ -1107,6 +1107,152 @@ void or_collide_static_scene(const float* grid6, const uint32_t* dims3, float ra
   }
 }
 
+/* ====================================================================================
+ * AR static scene, impulse variant -- ARcollisionsUniformGridKernel / ARCellRigidBody /
+ * collideARSpheresBaraffExact (Kernels/RB_UniformGridKernels.cu:420-678).  Each of the 27
+ * iterations of the neighbour loop examines the particle's own cell (the reference passes
+ * gridPos, :613).  Impulse j = -(1 + e)(v . n) / (((I^-1 (r x n)) x r) . n + 1/m) along
+ * n = (p - q) / |p - q|, r = contact point - (p - rel).  inertia9: glm::mat3 per body.
+ * Particles of a body: force, torque, count at the original index; free particles (body -1):
+ * force added to new_vel4, with a zero inverse inertia and unit mass.
+ * ==================================================================================== */
+void or_ar_collide_impulse(const float* grid6, const uint32_t* dims3, float radius,
+                           float restitution, const int* rb_idx, const float* rel4,
+                           const float* inertia9, const float* mass, const float* scene_radii,
+                           const float* spos4, const float* svel4, const float* scene_spos4,
+                           const uint32_t* gidx, const uint32_t* scene_gidx,
+                           const uint32_t* cstart, const uint32_t* cend, int n, float* pf4,
+                           float* pt4, int* count, float* new_vel4, float* color4) {
+  grid_t G;
+  memcpy(G.o, grid6, 12); memcpy(G.c, grid6 + 3, 12); memcpy(G.g, dims3, 12);
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; ++k) {
+    v3 pos = xyz(spos4 + 4l * k), vel = xyz(svel4 + 4l * k);
+    int gp[3];
+    cell_of(&G, pos, gp);
+    uint32_t orig = gidx[k];
+    int b = rb_idx[orig];
+    float ib[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float m = 1.f;
+    if (b >= 0) {
+      memcpy(ib, inertia9 + 9l * b, 36);
+      m = mass[b];
+    }
+    v3 rel = xyz(rel4 + 4l * orig);
+    v3 force = mk3(0.f, 0.f, 0.f), torque = force;
+    int ncol = 0;
+    uint32_t h = hash3(&G, gp[0], gp[1], gp[2]);
+    for (int it = 0; it < 27; ++it) {
+      v3 lf = mk3(0.f, 0.f, 0.f), lt = lf;
+      if (cstart[h] != 0xffffffffu) {
+        for (uint32_t j = cstart[h]; j < cend[h]; ++j) {
+          uint32_t o2 = scene_gidx[j];
+          v3 q = xyz(scene_spos4 + 4l * j);
+          float ra = radius, rb = scene_radii[o2];
+          v3 rp = sub(pos, q);
+          float dist = sqrtf(dot(rp, rp));
+          if (!(dist < ra + rb)) continue;
+          ++ncol;
+          float t = ra / (ra + rb);
+          v3 d = sub(q, pos);
+          v3 cp = add(pos, mk3(t * d.x, t * d.y, t * d.z));
+          v3 nrm = divs(rp, dist);
+          float rv = dot(vel, nrm);
+          v3 cm = sub(pos, rel);
+          v3 r = mk3(cp.x - cm.x, cp.y - cm.y, cp.z - cm.z);
+          v3 a = glm_cross(glm_mv(ib, glm_cross(r, nrm)), r);
+          float denom = (a.x * nrm.x + a.y * nrm.y + a.z * nrm.z) + 1.f / m;
+          float jj = -(1 + restitution) * rv / denom;
+          v3 f = mk3(nrm.x * jj, nrm.y * jj, nrm.z * jj);
+          lf = add(lf, f);
+          lt = add(lt, cross(r, f));
+        }
+      }
+      force = add(force, lf);
+      torque = add(torque, lt);
+    }
+    if (ncol && color4) st4(color4 + 4l * orig, 0.f, 1.f, 0.f, 0.f);
+    if (b == -1) {
+      if (new_vel4) {
+        float* V = new_vel4 + 4l * orig;
+        st4(V, V[0] + force.x, V[1] + force.y, V[2] + force.z, V[3] + 0.f);
+      }
+    } else {
+      st4(pf4 + 4l * orig, force.x, force.y, force.z, 0.f);
+      st4(pt4 + 4l * orig, torque.x, torque.y, torque.z, 0.f);
+      if (count) count[orig] = ncol;
+    }
+  }
+}
+
+/* Deepest contact with the static scene -- FindAugmentedRealityCollisionsUniformGridCell /
+ * Kernel (Kernels/RB_UniformGridKernels.cu:879-1021): 27 neighbour cells, 2r - d deeper than the
+ * current contact distance updates distance and point; colour green on any update, else blue. */
+void or_ar_find_contacts(const float* grid6, const uint32_t* dims3, float radius,
+                         const float* spos4, const float* scene_spos4, const uint32_t* gidx,
+                         const uint32_t* scene_gidx, const uint32_t* cstart,
+                         const uint32_t* cend, int n, float* contact_distance,
+                         int* contact_point, float* color4) {
+  grid_t G;
+  memcpy(G.o, grid6, 12); memcpy(G.c, grid6 + 3, 12); memcpy(G.g, dims3, 12);
+  const float thr = 2 * radius;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < n; ++k) {
+    v3 pos = xyz(spos4 + 4l * k);
+    int gp[3];
+    cell_of(&G, pos, gp);
+    uint32_t orig = gidx[k];
+    float deepest = contact_distance[orig];
+    int best = contact_point[orig], counter = 0;
+    for (int z = -1; z <= 1; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int x = -1; x <= 1; ++x) {
+          uint32_t h = hash3(&G, gp[0] + x, gp[1] + y, gp[2] + z);
+          if (cstart[h] == 0xffffffffu) continue;
+          for (uint32_t j = cstart[h]; j < cend[h]; ++j) {
+            v3 d = sub(pos, xyz(scene_spos4 + 4l * j));
+            float dist = sqrtf(dot(d, d));
+            if (thr - dist > deepest) {
+              deepest = thr - dist;
+              best = (int)scene_gidx[j];
+              ++counter;
+            }
+          }
+        }
+    contact_distance[orig] = deepest;
+    contact_point[orig] = best;
+    if (color4) {
+      if (counter) st4(color4 + 4l * orig, 0.f, 1.f, 0.f, 0.f);
+      else st4(color4 + 4l * orig, 0.f, 0.f, 1.f, 0.f);
+    }
+  }
+}
+
+/* GatherAugmentedRealityCollisions (Particles/updateFunctions.cpp:1511-1578): one contact per
+ * particle with a positive contact distance, in particle order. */
+long or_gather_static_contacts(float restitution, long n, const int* rb_idx, const float* cms4,
+                               const float* vel4, const float* ang4, const float* rel4,
+                               const float* scene_normals4, const float* contact_distance,
+                               const int* contact_point, float* normal4, float* point4,
+                               int* body1, int* body2, float* bias) {
+  long c = 0;
+  for (long i = 0; i < n; ++i) {
+    if (!(contact_distance[i] > 0)) continue;
+    int b = rb_idx[i];
+    const float* nn = scene_normals4 + 4l * contact_point[i];
+    const float *r4 = rel4 + 4 * i, *cm = cms4 + 4l * b;
+    v3 v = xyz(vel4 + 4l * b), w = xyz(ang4 + 4l * b);
+    float v_rel = dot(add(v, cross(w, xyz(r4))), xyz(nn));
+    memcpy(normal4 + 4 * c, nn, 16);
+    st4(point4 + 4 * c, r4[0] + cm[0], r4[1] + cm[1], r4[2] + cm[2], r4[3] + cm[3]);
+    body1[c] = b;
+    body2[c] = -1;
+    bias[c] = restitution * v_rel;
+    ++c;
+  }
+  return c;
+}
+
 /* ---- FP64 oracle of the same physics (summation order free, all-pairs within cells) ---- */
 static d3 dk3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
 static d3 dadd(d3 a, d3 b) { return dk3(a.x + b.x, a.y + b.y, a.z + b.z); }

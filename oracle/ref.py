@@ -339,3 +339,33 @@ def init_object(path, model: str, scale: float, radius: float):
                                C.c_float(radius), _p(rel), _p(inv))
     assert got == n
     return rel[:, :3].copy(), inv
+
+
+def ar_collide_impulse(params, rb_idx, rel4, inertia9, mass, scene_radii, spos4, svel4,
+                       scene_spos4, scene_normals4, gidx, scene_gidx, cstart, cend, new_vel4):
+    """ARcollisionsUniformGridKernel (Kernels/RB_UniformGridKernels.cu:590-678) -> per-particle
+    force, torque, impulse count, colour, and new_vel4 (free particles)."""
+    n = len(spos4)
+    count = np.zeros(n, np.int32)
+    pf, pt, color = (np.zeros((n, 4), np.float32) for _ in range(3))
+    nv = _f32(new_vel4).copy()
+    lib().refcpu_ar_collide_impulse(C.byref(params), _p(count), _p(pf), _p(_i32(rb_idx)),
+                                    _p(_f32(rel4)), _p(pt), _p(_f32(inertia9)), _p(_f32(mass)),
+                                    _p(color), _p(_f32(scene_radii)), _p(nv), _p(_f32(spos4)),
+                                    _p(_f32(svel4)), _p(_f32(scene_spos4)),
+                                    _p(_f32(scene_normals4)), _p(_u32(gidx)),
+                                    _p(_u32(scene_gidx)), _p(_u32(cstart)), _p(_u32(cend)), n)
+    return pf, pt, count, color, nv
+
+
+def ar_find_contacts(params, spos4, scene_spos4, gidx, scene_gidx, cstart, cend,
+                     contact_distance, contact_point):
+    """FindAugmentedRealityCollisionsUniformGridKernel (:927-1021) -> (distance, point, colour)."""
+    n = len(spos4)
+    cd = _f32(contact_distance).copy()
+    cp = _i32(contact_point).copy()
+    color = np.zeros((n, 4), np.float32)
+    lib().refcpu_ar_find_contacts(C.byref(params), _p(cp), _p(cd), _p(color), _p(_f32(spos4)),
+                                  _p(_f32(scene_spos4)), _p(_u32(gidx)), _p(_u32(scene_gidx)),
+                                  _p(_u32(cstart)), _p(_u32(cend)), n)
+    return cd, cp, color

@@ -50,7 +50,9 @@ RANGES = [
     ("Kernels/RB_BVHKernels.cu", 13, 244, "maxOpF4"),                            # collideStaticSpheresBVH, collideBVHSoARigidBody
     ("Kernels/RB_BVHKernels.cu", 760, 876, "FindRigidBodyCollisionsBVHKernel"),
     ("Kernels/RB_UniformGridKernels.cu", 112, 128, "calcGridPosAuxil"),          # grid pos / hash
+    ("Kernels/RB_UniformGridKernels.cu", 419, 678, "__device__"),                # AR Baraff impulses: sphere pair, cell, kernel
     ("Kernels/RB_UniformGridKernels.cu", 730, 845, "__device__"),                # FindRigidBodyCollisionsUniformGrid cell + kernel
+    ("Kernels/RB_UniformGridKernels.cu", 879, 1021, "__device__"),               # FindAugmentedRealityCollisionsUniformGrid cell + kernel
     ("WallCollisions.cu", 29, 35, "CreateIndexKernel"),
     ("WallCollisions.cu", 46, 129, "DetectWallCollisionKernel"),                 # + FindExactContactPoint, ComputeImpulseMagnitude
     ("WallCollisions.cu", 201, 276, "HandleWallCollisionKernelUnmapped"),

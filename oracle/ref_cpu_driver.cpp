@@ -233,6 +233,45 @@ void refcpu_collide_static_scene(const void* sim_params, float* p_linear4, float
   });
 }
 
+// ---- static scene, impulse variant: ARcollisionsUniformGridKernel (RB_UniformGridKernels.cu:
+// 590-678) and the deepest-contact search FindAugmentedRealityCollisionsUniformGridKernel
+// (:927-1021), over the grid their wrappers launch.
+void refcpu_ar_collide_impulse(const void* sim_params, int* count, float* p_force4,
+                               const int* rb_idx, const float* rel4, float* p_torque4,
+                               const float* inertia9, const float* mass, float* color4,
+                               const float* scene_radii, float* new_vel4,
+                               const float* sorted_pos4, const float* sorted_vel4,
+                               const float* scene_sorted_pos4, const float* scene_normals4,
+                               const uint32_t* grid_idx, const uint32_t* scene_grid_idx,
+                               const uint32_t* cell_start, const uint32_t* cell_end, int n) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  launch(n, 128, true, [&] {
+    ARcollisionsUniformGridKernel(count, (float4*)p_force4, (int*)rb_idx, (float4*)rel4,
+                                  (float4*)p_torque4, (glm::mat3*)inertia9, (float*)mass,
+                                  (float4*)color4, (float*)scene_radii, (float4*)new_vel4,
+                                  (float4*)sorted_pos4, (float4*)sorted_vel4,
+                                  (float4*)scene_sorted_pos4, (float4*)scene_normals4,
+                                  (uint*)grid_idx, (uint*)scene_grid_idx, (uint*)cell_start,
+                                  (uint*)cell_end, (uint)n, p);
+  });
+}
+
+void refcpu_ar_find_contacts(const void* sim_params, int* contact_point, float* contact_distance,
+                             float* color4, const float* sorted_pos4,
+                             const float* scene_sorted_pos4, const uint32_t* grid_idx,
+                             const uint32_t* scene_grid_idx, const uint32_t* cell_start,
+                             const uint32_t* cell_end, int n) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  launch(n, 128, true, [&] {
+    FindAugmentedRealityCollisionsUniformGridKernel(
+        contact_point, contact_distance, nullptr, (float4*)color4, (float4*)sorted_pos4,
+        (float4*)scene_sorted_pos4, (uint*)grid_idx, (uint*)scene_grid_idx, (uint*)cell_start,
+        (uint*)cell_end, (uint)n, p);
+  });
+}
+
 // ---- ReducePerParticleImpulses (UniformGridDEM.cu:462-666) with CombineReducedImpulses ---
 // The two CUB float4 inclusive scans are restated as sequential float scans.
 void refcpu_reduce_impulses(const float* p_force4, const float* p_torque4, float* rb_vel4,

@@ -290,6 +290,57 @@ def sis_solve_case(seed: int):
     return out
 
 
+def static_scene_ar_case(seed: int):
+    """The static-scene inputs of static_scene_case through the reference's impulse variant
+    (ARcollisionsUniformGridKernel), its deepest-contact search
+    (FindAugmentedRealityCollisionsUniformGridKernel), the contact gather and the solver
+    (GatherAugmentedRealityCollisions + SequentialImpulseSolver) -- the reference's augmented-
+    reality sequential-impulse update, stage by stage."""
+    d = static_scene_case(seed)
+    sc = scenes.small_scene(seed, nb_side=4, packed=True)
+    rng = np.random.default_rng(seed + 300)
+    n, nb = sc.num_particles, sc.num_bodies
+    rb = sc.body_index().astype(np.int32)
+    r = float(d["radius"])
+    m = len(d["scene_pos"])
+    scene_radii = (r * rng.uniform(0.8, 1.2, m)).astype(np.float32)
+    inertia = np.zeros((nb, 9), np.float32)
+    inertia[:, [0, 4, 8]] = rng.uniform(5, 50, (nb, 3))
+    inertia[:, [1, 3]] = rng.uniform(-1, 1, (nb, 1))  # symmetric off-diagonal terms
+    mass = rng.uniform(0.5, 2.0, nb).astype(np.float32)
+    prm = ref.sim_params(r, (0, 0, 0), float(d["cell"]), d["dims"], gravity=(0.0, -9.81, 0.0))
+    prm.ar_restitution, prm.ar_friction = 0.4, 0.3
+    pf, pt, count, color, _ = ref.ar_collide_impulse(
+        prm, rb, d["rel"], inertia, mass, scene_radii, d["spos"], d["svel"], d["scene_spos"],
+        d["scene_normals"], d["sidx"], d["scene_sidx"], d["scene_cell_start"],
+        d["scene_cell_end"], np.zeros((n, 4), np.float32))
+    cd0 = np.zeros(n, np.float32)
+    cp0 = np.full(n, -1, np.int32)
+    cd, cp, fcolor = ref.ar_find_contacts(prm, d["spos"], d["scene_spos"], d["sidx"],
+                                          d["scene_sidx"], d["scene_cell_start"],
+                                          d["scene_cell_end"], cd0, cp0)
+    cms = np.zeros((nb, 4), np.float32)
+    cms[:, :3] = sc.body_pos[:, :3]
+    vel = np.zeros((nb, 4), np.float32)
+    vel[:, :3] = rng.normal(0, 0.5, (nb, 3))
+    ang = np.zeros((nb, 4), np.float32)
+    ang[:, :3] = rng.normal(0, 2, (nb, 3))
+    solve = ref.sis_step(prm, rb, sc.body_offsets, cms, vel, ang, inertia, mass, d["rel"], cd,
+                         None, cp, scene_normals4=d["scene_normals"])
+    out = dict(radius=d["radius"], cell=d["cell"], dims=d["dims"], rb_idx=rb, rel=d["rel"],
+               spos=d["spos"], svel=d["svel"], sidx=d["sidx"], scene_normals=d["scene_normals"],
+               scene_spos=d["scene_spos"], scene_sidx=d["scene_sidx"],
+               scene_cell_start=d["scene_cell_start"], scene_cell_end=d["scene_cell_end"],
+               scene_radii=scene_radii, inertia=inertia, mass=mass,
+               ar_restitution=np.float32(0.4), ar_friction=np.float32(0.3),
+               impulse_force=pf, impulse_torque=pt, impulse_count=count, impulse_color=color,
+               contact_distance=cd, contact_point=cp, find_color=fcolor, cms=cms, vel=vel,
+               ang=ang, offsets=sc.body_offsets.astype(np.int32))
+    for key in ("normal", "point", "body1", "body2", "bias", "acc", "vel", "ang"):
+        out["sis_" + key] = solve[key]
+    return out
+
+
 CASES = {
     "lbvh_uniform": lambda: lbvh_case(11, 3000, 0.0),
     "lbvh_duplicates": lambda: lbvh_case(12, 3000, 0.2),
@@ -299,6 +350,7 @@ CASES = {
     "static_scene": lambda: static_scene_case(31),
     "sis_find": lambda: sis_case(5),
     "sis_solve": lambda: sis_solve_case(2),
+    "static_scene_ar": lambda: static_scene_ar_case(31),
 }
 
 
