@@ -114,6 +114,10 @@ SIGNATURES = {
     "ar_collide_static_scene_impulse": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, P, P,
                                         P, I, P, P, P, P, P, S],
     "ar_find_contacts_static_scene": [P, C.POINTER(SimParams), P, P, P, P, P, P, I, P, P, P, S],
+    "ar_collide_bvh_static": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, P, P, I, I, P,
+                              P, P, S],
+    "ar_find_contacts_bvh_static": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, I, I, P,
+                                    P, P, S],
     "ar_gather_static_contacts": [P, C.POINTER(SimParams), I, P, P, P, P, P, P, P, P, I, P, P, P,
                                   P, P, P, P, P, P, S],
     "ar_reduce_bodies": [P, P, P, P, I, P, P, S],

@@ -9,6 +9,8 @@
 // overlapping leaf children are handled left then right, then the walk descends into the
 // left internal child if it overlaps, and on the way back up into the right one.  Handling
 // contacts in the same order keeps the float sums identical to the reference's.
+#include <algorithm>
+
 #include "ar_internal.cuh"
 #include "ar_dem.cuh"
 #include "ar_lbvh.cuh"
@@ -212,6 +214,110 @@ __global__ void __launch_bounds__(128) pairs_bvh_kernel(
 }
 
 
+// ---- static scene through a BVH over its point cloud ----------------------------------------
+// checkOverlap(float4, AABB, radius) (BVHSource/BVHAuxiliary.cuh:159-175): the box point
+// closest to the sphere centre, distance rounded toward zero, strictly below the radius.
+__device__ __forceinline__ bool sphere_box(float4 p, const Box& b, float r) {
+  const float xx = fmaxf(b.lx, fminf(p.x, b.hx));
+  const float yy = fmaxf(b.ly, fminf(p.y, b.hy));
+  const float zz = fmaxf(b.lz, fminf(p.z, b.hz));
+  const float d = __fsqrt_rz((xx - p.x) * (xx - p.x) + (yy - p.y) * (yy - p.y) +
+                             (zz - p.z) * (zz - p.z));
+  return d < r;
+}
+
+// staticCollideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:293-442): particle i (unsorted, radius
+// params.particle_radius) walks the scene's tree (m leaves) in the reference's order; every
+// overlapping leaf adds the DEM force of collideSpheresBVH (BVHAuxiliary.cuh:97-130, the scene
+// point at rest) and rel x force.  The reference adds a body's particles' totals straight into
+// the body's force and torque with plain read-modify-writes from many threads (racy); here each
+// particle's totals go to p_force4 / p_torque4 at its index, for a fixed-order body sum
+// (ar_reduce_bodies).  A free particle (body -1) gets v + force as its velocity.  color4 (may
+// be NULL): green when a leaf is within touching distance.
+__global__ void __launch_bounds__(128) collide_bvh_static_kernel(
+    ar_sim_params prm, const int32_t* __restrict__ rb_idx, const float4* __restrict__ rel,
+    const float4* __restrict__ pos, float4* __restrict__ vel, const uint8_t* __restrict__ is_leaf,
+    const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+    const int32_t* __restrict__ parent, const float4* __restrict__ cms,
+    const float4* __restrict__ bounds, const float* __restrict__ radii, int m, int n,
+    float4* __restrict__ p_force, float4* __restrict__ p_torque, float4* __restrict__ color) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 qpos = __ldg(pos + i);
+    const float3 qvel = ar::xyz(vel[i]);
+    const float qrad = prm.particle_radius;
+    const int qbody = __ldg(rb_idx + i);
+    const float3 r3 = ar::xyz(__ldg(rel + i));
+    float3 force = ar::mk3(0.f, 0.f, 0.f), torque = force;
+    if (m >= 2) {
+      ar_lbvh::walk(m, m, is_leaf, left, right, parent,
+                    [&](int c) { return sphere_box(qpos, load_box(bounds, c), qrad); },
+                    [&](int c, bool) {
+                      const float4 cp = __ldg(cms + c);
+                      const float rc = __ldg(radii + c);
+                      const float3 rp = ar::mk3(cp.x - qpos.x, cp.y - qpos.y, cp.z - qpos.z);
+                      const float dist = sqrtf(ar::dot(rp, rp));
+                      float3 f = ar::mk3(0.f, 0.f, 0.f);
+                      if (dist < qrad + rc)
+                        f = ar_dem::spring_force(rp, dist,
+                                                 ar::mk3(0.f - qvel.x, 0.f - qvel.y, 0.f - qvel.z),
+                                                 qrad + rc, prm.spring, prm.damping, prm.shear,
+                                                 prm.attraction);
+                      force = ar::add(force, f);
+                      torque = ar::add(torque, ar::cross(r3, f));
+                      if (dist < qrad + rc && color) color[i] = make_float4(0.f, 1.f, 0.f, 0.f);
+                    });
+    }
+    if (qbody >= 0) {
+      p_force[i] = make_float4(force.x, force.y, force.z, 0.f);
+      p_torque[i] = make_float4(torque.x, torque.y, torque.z, 0.f);
+    } else {
+      vel[i] = make_float4(qvel.x + force.x, qvel.y + force.y, qvel.z + force.z, 0.f);
+    }
+  }
+}
+
+// FindAugmentedRealityCollisionsBVHKernel (Kernels/RB_BVHKernels.cu:920-1023): deepest contact
+// of particle i with the scene through its tree: an overlapping leaf c (cloud point
+// sorted_idx[c]) deepens the contact when r + radii[point] - |cms[c] - p| (four components, as
+// the reference's length(float4)) exceeds contact_distance[i], which records it with the point.
+// The query radius is params.particle_radius (the reference reads the scene's radius array at
+// the query's index; the two agree when every radius is the particle radius).  color4 (may be
+// NULL): green on a contact, white when none.
+__global__ void __launch_bounds__(128) find_bvh_static_kernel(
+    ar_sim_params prm, const float4* __restrict__ pos, const uint8_t* __restrict__ is_leaf,
+    const int32_t* __restrict__ left, const int32_t* __restrict__ right,
+    const int32_t* __restrict__ parent, const float4* __restrict__ cms,
+    const float4* __restrict__ bounds, const int32_t* __restrict__ sorted_idx,
+    const float* __restrict__ radii, int m, int n, float* __restrict__ contact_distance,
+    int32_t* __restrict__ contact_point, float4* __restrict__ color) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 qpos = __ldg(pos + i);
+    const float qrad = prm.particle_radius;
+    float deepest = contact_distance[i];
+    int best = contact_point[i], ncol = 0;
+    if (m >= 2) {
+      ar_lbvh::walk(m, m, is_leaf, left, right, parent,
+                    [&](int c) { return sphere_box(qpos, load_box(bounds, c), qrad); },
+                    [&](int c, bool) {
+                      const int s = __ldg(sorted_idx + c);
+                      const float4 cp = __ldg(cms + c);
+                      const float4 d = make_float4(cp.x - qpos.x, cp.y - qpos.y, cp.z - qpos.z,
+                                                   cp.w - qpos.w);
+                      const float dist = sqrtf(d.x * d.x + d.y * d.y + d.z * d.z + d.w * d.w);
+                      const float thr = qrad + __ldg(radii + s);
+                      if (thr - dist > deepest) {
+                        ++ncol;
+                        deepest = thr - dist;
+                        best = s;
+                      }
+                    });
+    }
+    contact_distance[i] = deepest;
+    contact_point[i] = best;
+    if (color) color[i] = ncol ? make_float4(0.f, 1.f, 0.f, 0.f) : make_float4(1.f, 1.f, 1.f, 0.f);
+  }
+}
+
 // parent links: the caller's, or derived into scratch when the caller has none
 const int32_t* parents_or_derive(ar_ctx* ctx, int n, const int32_t* left, const int32_t* right,
                                  const int32_t* parent, cudaStream_t st) {
@@ -296,6 +402,54 @@ ar_status ar_collide_bvh_dem(ar_ctx* ctx, const ar_sim_params* params, const int
       (const float4*)cms4, (const float4*)bounds8, sorted_idx, radii, n, (float4*)p_force4,
       (float4*)p_torque4, (float4*)p_positions4);
   return arh::check_launch("ar_collide_bvh_dem");
+}
+
+ar_status ar_collide_bvh_static(ar_ctx* ctx, const ar_sim_params* params, const int32_t* rb_idx,
+                                const float* rel4, const float* pos4, float* vel4,
+                                const uint8_t* is_leaf, const int32_t* left,
+                                const int32_t* right, const int32_t* parent, const float* cms4,
+                                const float* bounds8, const float* radii, int num_scene, int n,
+                                float* p_force4, float* p_torque4, float* color4,
+                                ar_stream_t stream) {
+  if (!ctx || !params || n < 0 || num_scene < 0 ||
+      (n > 0 && (!rb_idx || !rel4 || !pos4 || !vel4 || !p_force4 || !p_torque4)) ||
+      (num_scene >= 2 && (!is_leaf || !left || !right || !cms4 || !bounds8 || !radii)))
+    return AR_ERR_INVALID_ARG;
+  if (n == 0) return AR_OK;
+  cudaStream_t st = arh::stream(stream);
+  parent = parents_or_derive(ctx, num_scene, left, right, parent, st);
+  if (!parent && num_scene >= 2) return AR_ERR_OOM;
+  const unsigned grid = std::min(arh::grid_for(n, 128), (unsigned)ctx->num_sms * 16);
+  collide_bvh_static_kernel<<<grid, 128, 0, st>>>(
+      *params, rb_idx, (const float4*)rel4, (const float4*)pos4, (float4*)vel4, is_leaf, left,
+      right, parent, (const float4*)cms4, (const float4*)bounds8, radii, num_scene, n,
+      (float4*)p_force4, (float4*)p_torque4, (float4*)color4);
+  return arh::check_launch("ar_collide_bvh_static");
+}
+
+ar_status ar_find_contacts_bvh_static(ar_ctx* ctx, const ar_sim_params* params,
+                                      const float* pos4, const uint8_t* is_leaf,
+                                      const int32_t* left, const int32_t* right,
+                                      const int32_t* parent, const float* cms4,
+                                      const float* bounds8, const int32_t* sorted_idx,
+                                      const float* radii, int num_scene, int n,
+                                      float* contact_distance, int32_t* contact_point,
+                                      float* color4, ar_stream_t stream) {
+  if (!ctx || !params || n < 0 || num_scene < 0 ||
+      (n > 0 && (!pos4 || !contact_distance || !contact_point)) ||
+      (num_scene >= 2 && (!is_leaf || !left || !right || !cms4 || !bounds8 || !sorted_idx ||
+                          !radii)))
+    return AR_ERR_INVALID_ARG;
+  if (n == 0) return AR_OK;
+  cudaStream_t st = arh::stream(stream);
+  parent = parents_or_derive(ctx, num_scene, left, right, parent, st);
+  if (!parent && num_scene >= 2) return AR_ERR_OOM;
+  const unsigned grid = std::min(arh::grid_for(n, 128), (unsigned)ctx->num_sms * 16);
+  find_bvh_static_kernel<<<grid, 128, 0, st>>>(
+      *params, (const float4*)pos4, is_leaf, left, right, parent, (const float4*)cms4,
+      (const float4*)bounds8, sorted_idx, radii, num_scene, n, contact_distance, contact_point,
+      (float4*)color4);
+  return arh::check_launch("ar_find_contacts_bvh_static");
 }
 
 ar_status ar_find_contacts_bvh(ar_ctx* ctx, const int32_t* rb_idx, const uint8_t* is_leaf,

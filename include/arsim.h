@@ -335,6 +335,39 @@ AR_API ar_status ar_gather_static_contacts(ar_ctx* ctx, const ar_sim_params* par
                                            float* acc_friction, float* acc_friction2,
                                            int32_t* d_count, ar_stream_t stream);
 
+/* Particles against the static scene through a BVH built over its point cloud (num_scene
+ * leaves, built with ar_morton30 / ar_radix_sort_pairs_u32 / ar_lbvh_build / ar_lbvh_leaves /
+ * ar_lbvh_refit; parent may be NULL), in the reference's visit order, leaves admitted by the
+ * sphere-box test checkOverlap(float4, AABB, r) (BVHSource/BVHAuxiliary.cuh:159-175).
+ * staticCollideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:293-442): particle i (unsorted,
+ * radius params.particle_radius) collects the DEM force of every overlapping leaf (the scene
+ * point at rest, radius radii[leaf]) and rel x force into p_force4[i] / p_torque4[i]; the
+ * reference adds them straight into the body's totals from many threads at once (racy), so
+ * here the body sums are left to ar_reduce_bodies.  A free particle (rb_idx -1) gets v + force
+ * in vel4 instead.  color4 (may be NULL): green when a leaf touches. */
+AR_API ar_status ar_collide_bvh_static(ar_ctx* ctx, const ar_sim_params* params,
+                                       const int32_t* rb_idx, const float* rel4,
+                                       const float* pos4, float* vel4, const uint8_t* is_leaf,
+                                       const int32_t* left, const int32_t* right,
+                                       const int32_t* parent, const float* cms4,
+                                       const float* bounds8, const float* radii, int num_scene,
+                                       int n, float* p_force4, float* p_torque4, float* color4,
+                                       ar_stream_t stream);
+/* FindAugmentedRealityCollisionsBVHKernel (Kernels/RB_BVHKernels.cu:920-1023): deepest
+ * contact of particle i with the scene through its tree: r + radii[point] - |cms[leaf] - p|
+ * deeper than contact_distance[i] records it with the cloud point sorted_idx[leaf] in
+ * contact_point[i].  The query radius is params.particle_radius (the reference reads the
+ * scene's radius array at the query's index; the two agree when every radius is r).
+ * color4 (may be NULL): green on a contact, white when none. */
+AR_API ar_status ar_find_contacts_bvh_static(ar_ctx* ctx, const ar_sim_params* params,
+                                             const float* pos4, const uint8_t* is_leaf,
+                                             const int32_t* left, const int32_t* right,
+                                             const int32_t* parent, const float* cms4,
+                                             const float* bounds8, const int32_t* sorted_idx,
+                                             const float* radii, int num_scene, int n,
+                                             float* contact_distance, int32_t* contact_point,
+                                             float* color4, ar_stream_t stream);
+
 /* ---- (a15) DEM contact forces on the grid ------------------------------------------------------
  * FindAndHandleRigidBodyCollisionsUniformGridKernel (RigidBodies/UniformGridDEM.cu:57-241):
  * per sorted particle, the 27 neighbour cells in z, y, x order (-1..1), occupants in sorted

@@ -535,3 +535,32 @@ def gather_static_contacts(restitution, rb_idx, cms4, vel4, ang4, rel4, scene_no
                                      _p(out["normal"]), _p(out["point"]), _p(out["body1"]),
                                      _p(out["body2"]), _p(out["bias"]))
     return {k: v[:c] for k, v in out.items()}
+
+
+_L.or_collide_bvh_static.restype = None
+_L.or_find_contacts_bvh_static.restype = None
+
+
+def collide_bvh_static(prm4, radius, rb_idx, rel4, pos4, vel4, tree, cms4, bounds8, radii):
+    """staticCollideBVHSoARigidBody -> (force, torque, velocity, colour), per particle."""
+    n, m = len(pos4), len(cms4)
+    pf, pt, color = (np.zeros((n, 4), np.float32) for _ in range(3))
+    vel = _f32(vel4).copy()
+    _L.or_collide_bvh_static(_p(_f32(prm4)), C.c_float(radius), _p(_i32(rb_idx)), _p(_f32(rel4)),
+                             _p(_f32(pos4)), _p(vel), _p(tree["is_leaf"]), _p(_i32(tree["left"])),
+                             _p(_i32(tree["right"])), _p(_f32(cms4)), _p(_f32(bounds8)),
+                             _p(_f32(radii)), m, n, _p(pf), _p(pt), _p(color))
+    return pf, pt, vel, color
+
+
+def find_contacts_bvh_static(radius, pos4, tree, cms4, bounds8, sorted_idx, radii,
+                             contact_distance, contact_point):
+    """FindAugmentedRealityCollisionsBVHKernel -> (distance, point, colour)."""
+    n, m = len(pos4), len(cms4)
+    cd, cp = _f32(contact_distance).copy(), _i32(contact_point).copy()
+    color = np.zeros((n, 4), np.float32)
+    _L.or_find_contacts_bvh_static(C.c_float(radius), _p(_f32(pos4)), _p(tree["is_leaf"]),
+                                   _p(_i32(tree["left"])), _p(_i32(tree["right"])),
+                                   _p(_f32(cms4)), _p(_f32(bounds8)), _p(_i32(sorted_idx)),
+                                   _p(_f32(radii)), m, n, _p(cd), _p(cp), _p(color))
+    return cd, cp, color

@@ -1253,6 +1253,146 @@ long or_gather_static_contacts(float restitution, long n, const int* rb_idx, con
   return c;
 }
 
+/* ====================================================================================
+ * Static scene through a BVH over its point cloud (m leaves; node ids as the Karras build):
+ * staticCollideBVHSoARigidBody and FindAugmentedRealityCollisionsBVHKernel
+ * (Kernels/RB_BVHKernels.cu:293-442, 920-1023).  The sphere-box test is checkOverlap(float4,
+ * AABB, radius) (BVHSource/BVHAuxiliary.cuh:159-175) with a square root rounded toward zero.
+ * ==================================================================================== */
+static float sqrt_rz(float x) {
+  float s = sqrtf(x);
+  if ((double)s * (double)s > (double)x) s = nextafterf(s, 0.0f);
+  return s;
+}
+static int sphere_box8(const float* p, const float* b, float r) {
+  float xx = fmaxf(b[0], fminf(p[0], b[3]));
+  float yy = fmaxf(b[1], fminf(p[1], b[4]));
+  float zz = fmaxf(b[2], fminf(p[2], b[5]));
+  float d = sqrt_rz((xx - p[0]) * (xx - p[0]) + (yy - p[1]) * (yy - p[1]) +
+                    (zz - p[2]) * (zz - p[2]));
+  return d < r;
+}
+
+/* Per particle: force and torque (rel x force) of every overlapping leaf, the DEM law against a
+ * point at rest (collideSpheresBVH, BVHAuxiliary.cuh:97-130), written per particle (a free
+ * particle, body -1, gets v + force as its velocity); colour green on a touching leaf.
+ * prm = {spring, damping, shear, attraction}. */
+void or_collide_bvh_static(const float* prm, float radius, const int* rb_idx, const float* rel4,
+                           const float* pos4, float* vel4, const uint8_t* is_leaf,
+                           const int* left, const int* right, const float* cms4,
+                           const float* bounds8, const float* radii, int m, int n, float* pf4,
+                           float* pt4, float* color4) {
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    const float* qp = pos4 + 4l * i;
+    v3 qvel = xyz(vel4 + 4l * i), r3 = xyz(rel4 + 4l * i);
+    v3 force = mk3(0.f, 0.f, 0.f), torque = force;
+    if (m >= 2) {
+      int cap = 256, top = 0;
+      int* st = (int*)malloc(sizeof(int) * cap);
+      st[top++] = -1;
+      int node = m;
+      do {
+        int lc = left[node], rc = right[node];
+        int ol = sphere_box8(qp, bounds8 + 8l * lc, radius);
+        int orr = sphere_box8(qp, bounds8 + 8l * rc, radius);
+        int ll = is_leaf[lc], rl = is_leaf[rc];
+        for (int side = 0; side < 2; ++side) {
+          int c = side == 0 ? lc : rc;
+          if (!((side == 0 ? ol : orr) && (side == 0 ? ll : rl))) continue;
+          const float* cp = cms4 + 4l * c;
+          float rc_ = radii[c];
+          v3 rp = mk3(cp[0] - qp[0], cp[1] - qp[1], cp[2] - qp[2]);
+          float dist = sqrtf(dot(rp, rp));
+          v3 f = mk3(0.f, 0.f, 0.f);
+          if (dist < radius + rc_)
+            f = spring_force(rp, dist, mk3(0.f - qvel.x, 0.f - qvel.y, 0.f - qvel.z),
+                             radius + rc_, prm);
+          force = add(force, f);
+          torque = add(torque, cross(r3, f));
+          if (dist < radius + rc_ && color4) st4(color4 + 4l * i, 0.f, 1.f, 0.f, 0.f);
+        }
+        int tl = ol && !ll, tr = orr && !rl;
+        if (!tl && !tr) {
+          node = st[--top];
+        } else {
+          node = tl ? lc : rc;
+          if (tl && tr) {
+            if (top == cap) { cap *= 2; st = (int*)realloc(st, sizeof(int) * cap); }
+            st[top++] = rc;
+          }
+        }
+      } while (node != -1);
+      free(st);
+    }
+    if (rb_idx[i] >= 0) {
+      st4(pf4 + 4l * i, force.x, force.y, force.z, 0.f);
+      st4(pt4 + 4l * i, torque.x, torque.y, torque.z, 0.f);
+    } else {
+      st4(vel4 + 4l * i, qvel.x + force.x, qvel.y + force.y, qvel.z + force.z, 0.f);
+    }
+  }
+}
+
+/* Deepest contact through the scene tree: r + radii[point] - |cms[leaf] - p| (four components)
+ * deeper than contact_distance[i] records it with the point sorted_idx[leaf]; colour green on a
+ * contact, white when none. */
+void or_find_contacts_bvh_static(float radius, const float* pos4, const uint8_t* is_leaf,
+                                 const int* left, const int* right, const float* cms4,
+                                 const float* bounds8, const int* sorted_idx,
+                                 const float* radii, int m, int n, float* contact_distance,
+                                 int* contact_point, float* color4) {
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int i = 0; i < n; ++i) {
+    const float* qp = pos4 + 4l * i;
+    float deepest = contact_distance[i];
+    int best = contact_point[i], ncol = 0;
+    if (m >= 2) {
+      int cap = 256, top = 0;
+      int* st = (int*)malloc(sizeof(int) * cap);
+      st[top++] = -1;
+      int node = m;
+      do {
+        int lc = left[node], rc = right[node];
+        int ol = sphere_box8(qp, bounds8 + 8l * lc, radius);
+        int orr = sphere_box8(qp, bounds8 + 8l * rc, radius);
+        int ll = is_leaf[lc], rl = is_leaf[rc];
+        for (int side = 0; side < 2; ++side) {
+          int c = side == 0 ? lc : rc;
+          if (!((side == 0 ? ol : orr) && (side == 0 ? ll : rl))) continue;
+          int s_ = sorted_idx[c];
+          const float* cp = cms4 + 4l * c;
+          float dx = cp[0] - qp[0], dy = cp[1] - qp[1], dz = cp[2] - qp[2], dw = cp[3] - qp[3];
+          float dist = sqrtf(dx * dx + dy * dy + dz * dz + dw * dw);
+          float thr = radius + radii[s_];
+          if (thr - dist > deepest) {
+            ++ncol;
+            deepest = thr - dist;
+            best = s_;
+          }
+        }
+        int tl = ol && !ll, tr = orr && !rl;
+        if (!tl && !tr) {
+          node = st[--top];
+        } else {
+          node = tl ? lc : rc;
+          if (tl && tr) {
+            if (top == cap) { cap *= 2; st = (int*)realloc(st, sizeof(int) * cap); }
+            st[top++] = rc;
+          }
+        }
+      } while (node != -1);
+      free(st);
+    }
+    contact_distance[i] = deepest;
+    contact_point[i] = best;
+    if (color4) {
+      if (ncol) st4(color4 + 4l * i, 0.f, 1.f, 0.f, 0.f);
+      else st4(color4 + 4l * i, 1.f, 1.f, 1.f, 0.f);
+    }
+  }
+}
+
 /* ---- FP64 oracle of the same physics (summation order free, all-pairs within cells) ---- */
 static d3 dk3(double x, double y, double z) { d3 r = {x, y, z}; return r; }
 static d3 dadd(d3 a, d3 b) { return dk3(a.x + b.x, a.y + b.y, a.z + b.z); }

@@ -369,3 +369,35 @@ def ar_find_contacts(params, spos4, scene_spos4, gidx, scene_gidx, cstart, cend,
                                   _p(_f32(scene_spos4)), _p(_u32(gidx)), _p(_u32(scene_gidx)),
                                   _p(_u32(cstart)), _p(_u32(cend)), n)
     return cd, cp, color
+
+
+def collide_bvh_static(params, rb_idx, rel4, pos4, vel4, tree, cms4, bounds8, sorted_idx, radii,
+                       rb_force4, rb_torque4, mass):
+    """staticCollideBVHSoARigidBody (Kernels/RB_BVHKernels.cu:293-442), threads run in order
+    -> (body force, body torque, velocity, colour)."""
+    n, m = len(pos4), len(cms4)
+    f, t = _f32(rb_force4).copy(), _f32(rb_torque4).copy()
+    vel = _f32(vel4).copy()
+    color = np.zeros((n, 4), np.float32)
+    lib().refcpu_collide_bvh_static(C.byref(params), _p(color), _p(_f32(pos4)), _p(_f32(rel4)),
+                                    _p(t), _p(f), _p(_f32(mass)), _p(_i32(rb_idx)), _p(vel),
+                                    _p(tree["is_leaf"]), _p(tree["left"]), _p(tree["right"]),
+                                    _p(tree["min_r"]), _p(tree["max_r"]), _p(_f32(cms4)),
+                                    _p(_f32(bounds8)), _p(_i32(sorted_idx)), _p(_f32(radii)), n, m)
+    return f, t, vel, color
+
+
+def find_contacts_bvh_static(params, pos4, tree, cms4, bounds8, sorted_idx, radii,
+                             contact_distance, contact_point):
+    """FindAugmentedRealityCollisionsBVHKernel (Kernels/RB_BVHKernels.cu:920-1023) ->
+    (distance, point, colour)."""
+    n, m = len(pos4), len(cms4)
+    cd, cp = _f32(contact_distance).copy(), _i32(contact_point).copy()
+    color = np.zeros((n, 4), np.float32)
+    lib().refcpu_find_contacts_bvh_static(C.byref(params), _p(color), _p(_f32(pos4)),
+                                          _p(tree["is_leaf"]), _p(tree["left"]),
+                                          _p(tree["right"]), _p(tree["min_r"]),
+                                          _p(tree["max_r"]), _p(_f32(cms4)), _p(_f32(bounds8)),
+                                          _p(_i32(sorted_idx)), _p(_f32(radii)), n, m, _p(cd),
+                                          _p(cp))
+    return cd, cp, color

@@ -48,7 +48,9 @@ RANGES = [
     ("Kernels/rigidBodyKernels.cu", 382, 421, "/*"),                             # computeGlobalAttributes
     ("Kernels/rigidBodyKernels.cu", 449, 456, "resetQuaternionKernel"),
     ("Kernels/RB_BVHKernels.cu", 13, 244, "maxOpF4"),                            # collideStaticSpheresBVH, collideBVHSoARigidBody
+    ("Kernels/RB_BVHKernels.cu", 293, 442, "__global__"),                         # staticCollideBVHSoARigidBody
     ("Kernels/RB_BVHKernels.cu", 760, 876, "FindRigidBodyCollisionsBVHKernel"),
+    ("Kernels/RB_BVHKernels.cu", 920, 1023, "FindAugmentedRealityCollisionsBVHKernel"),
     ("Kernels/RB_UniformGridKernels.cu", 112, 128, "calcGridPosAuxil"),          # grid pos / hash
     ("Kernels/RB_UniformGridKernels.cu", 419, 678, "__device__"),                # AR Baraff impulses: sphere pair, cell, kernel
     ("Kernels/RB_UniformGridKernels.cu", 730, 845, "__device__"),                # FindRigidBodyCollisionsUniformGrid cell + kernel

@@ -272,6 +272,43 @@ void refcpu_ar_find_contacts(const void* sim_params, int* contact_point, float* 
   });
 }
 
+// ---- static scene through the scene's BVH: staticCollideBVHSoARigidBody
+// (RB_BVHKernels.cu:293-442) and FindAugmentedRealityCollisionsBVHKernel (:920-1023) ---------
+void refcpu_collide_bvh_static(const void* sim_params, float* color4, const float* pos4,
+                               const float* rel4, float* rb_torque4, float* rb_force4,
+                               const float* rb_mass, const int* rb_idx, float* vel4,
+                               const uint8_t* is_leaf, const int* left, const int* right,
+                               const int* min_r, const int* max_r, const float* cms4,
+                               const void* bounds, const int* sorted_idx, const float* radii,
+                               int n, int num_scene) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  launch(n, 128, false, [&] {  // the kernel adds to per-body totals: run the threads in order
+    staticCollideBVHSoARigidBody((float4*)color4, (float4*)pos4, (float4*)rel4,
+                                 (float4*)rb_torque4, (float4*)rb_force4, (float*)rb_mass,
+                                 (int*)rb_idx, nullptr, (float4*)vel4, nullptr, (bool*)is_leaf,
+                                 (int*)left, (int*)right, (int*)min_r, (int*)max_r,
+                                 (float4*)cms4, (AABB*)bounds, (int*)sorted_idx, (float*)radii,
+                                 n, num_scene, p);
+  });
+}
+
+void refcpu_find_contacts_bvh_static(const void* sim_params, float* color4, const float* pos4,
+                                     const uint8_t* is_leaf, const int* left, const int* right,
+                                     const int* min_r, const int* max_r, const float* cms4,
+                                     const void* bounds, const int* sorted_idx,
+                                     const float* radii, int n, int num_scene,
+                                     float* contact_distance, int* contact_point) {
+  SimParams p;
+  std::memcpy(&p, sim_params, sizeof(SimParams));
+  launch(n, 128, true, [&] {
+    FindAugmentedRealityCollisionsBVHKernel(
+        (float4*)color4, (float4*)pos4, (bool*)is_leaf, (int*)left, (int*)right, (int*)min_r,
+        (int*)max_r, (float4*)cms4, (AABB*)bounds, (int*)sorted_idx, (float*)radii, n,
+        num_scene, p, contact_distance, contact_point);
+  });
+}
+
 // ---- ReducePerParticleImpulses (UniformGridDEM.cu:462-666) with CombineReducedImpulses ---
 // The two CUB float4 inclusive scans are restated as sequential float scans.
 void refcpu_reduce_impulses(const float* p_force4, const float* p_torque4, float* rb_vel4,

@@ -341,6 +341,49 @@ def static_scene_ar_case(seed: int):
     return out
 
 
+def static_scene_bvh_case(seed: int):
+    """Particles against a BVH built over the static point cloud of static_scene_case (the
+    reference's own Morton codes, sort, Karras build, leaves and refit), through
+    staticCollideBVHSoARigidBody and FindAugmentedRealityCollisionsBVHKernel.  Each particle is
+    its own body here, so the reference kernel's per-body read-modify-writes do not collide and
+    its body totals are the particles' own; a few particles are free (body -1)."""
+    d = static_scene_case(seed)
+    rng = np.random.default_rng(seed + 400)
+    r = float(d["radius"])
+    pos = d["spos"].copy()
+    n = len(pos)
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0, 0.3, (n, 3))
+    rel = d["rel"].copy()
+    rb = np.arange(n, dtype=np.int32)
+    rb[rng.random(n) < 0.05] = -1
+    cloud = d["scene_pos"]
+    m = len(cloud)
+    mn, mx = ref.aabb(cloud)
+    codes, idx = ref.morton30(cloud, mn, mx)
+    sk, si = ref.sort_pairs_u32(codes, idx.view(np.uint32))
+    tree = ref.radix_tree(sk)
+    cms, _, bounds, radii = ref.leaves_and_refit(tree, si.astype(np.int32), cloud, np.float32(r))
+    prm = params_for(r, (0.0, 0.0, 0.0), d["cell"], tuple(d["dims"]), 0.5, 0.02, 0.1, 0.001)
+    f0 = np.zeros((n, 4), np.float32)
+    mass = np.ones(n, np.float32)
+    bf, bt, bvel, color = ref.collide_bvh_static(prm, rb, rel, pos, vel, tree, cms, bounds,
+                                                 si.astype(np.int32), radii, f0, f0, mass)
+    # the reference reads the query's radius from the scene's radius array at the query's
+    # index (RB_BVHKernels.cu:955): give it an array long enough, every radius r, as the
+    # reference assumes ("currently the same for all particles")
+    padded = np.full(max(n, m), np.float32(r), np.float32)
+    cd, cp, fcolor = ref.find_contacts_bvh_static(prm, pos, tree, cms, bounds,
+                                                  si.astype(np.int32), padded,
+                                                  np.zeros(n, np.float32), np.full(n, -1, np.int32))
+    return dict(radius=np.float32(r), prm=np.array([0.5, 0.02, 0.1, 0.001], np.float32),
+                pos=pos, vel=vel, rel=rel, rb_idx=rb, is_leaf=tree["is_leaf"], left=tree["left"],
+                right=tree["right"], parent=tree["parent"], cms=cms, bounds=bounds,
+                sorted_idx=si.astype(np.int32), radii=radii, body_force=bf, body_torque=bt,
+                vel_out=bvel, color=color, contact_distance=cd, contact_point=cp,
+                find_color=fcolor)
+
+
 CASES = {
     "lbvh_uniform": lambda: lbvh_case(11, 3000, 0.0),
     "lbvh_duplicates": lambda: lbvh_case(12, 3000, 0.2),
@@ -351,6 +394,7 @@ CASES = {
     "sis_find": lambda: sis_case(5),
     "sis_solve": lambda: sis_solve_case(2),
     "static_scene_ar": lambda: static_scene_ar_case(31),
+    "static_scene_bvh": lambda: static_scene_bvh_case(31),
 }
 
 

@@ -96,3 +96,29 @@ def test_gather_overflow_is_reported(ctx):
          *[P(b) for b in bufs], P(cnt), S())
     assert ctx.status() == 7  # AR_ERR_OVERFLOW
     assert int(host(cnt)[0]) == len(z["sis_body1"])
+
+
+def test_bvh_static_variants_match_reference(ctx):
+    z = golden("static_scene_bvh")
+    n, m = len(z["pos"]), len(z["cms"])
+    prm = api.sim_params(float(z["radius"]), (0, 0, 0), 1.0, (4, 4, 4),
+                         *[float(x) for x in z["prm"]])
+    tree = [P(dev(z[k])) for k in ("is_leaf", "left", "right")]
+    scene = [P(dev(z["cms"])), P(dev(z["bounds"]))]
+    pf, pt, color = empty((n, 4)), empty((n, 4)), empty((n, 4))
+    vel = dev(z["vel"])
+    call("ar_collide_bvh_static", ctx.handle, C.byref(prm), P(dev(z["rb_idx"])), P(dev(z["rel"])),
+         P(dev(z["pos"])), P(vel), *tree, None, *scene, P(dev(z["radii"])), m, n, P(pf), P(pt),
+         P(color), S())
+    ctx.check()
+    body = z["rb_idx"] >= 0
+    assert np.array_equal(host(pf)[body], z["body_force"][body])
+    assert np.array_equal(host(pt)[body], z["body_torque"][body])
+    assert np.array_equal(host(vel), z["vel_out"]) and np.array_equal(host(color), z["color"])
+    cd, cp, fc = dev(np.zeros(n, np.float32)), dev(np.full(n, -1, np.int32)), empty((n, 4))
+    call("ar_find_contacts_bvh_static", ctx.handle, C.byref(prm), P(dev(z["pos"])), *tree, None,
+         *scene, P(dev(z["sorted_idx"])), P(dev(z["radii"])), m, n, P(cd), P(cp), P(fc), S())
+    ctx.check()
+    assert np.array_equal(host(cd), z["contact_distance"])
+    assert np.array_equal(host(cp), z["contact_point"])
+    assert np.array_equal(host(fc), z["find_color"])

@@ -44,3 +44,29 @@ def test_find_gather_solve_equal_reference():
                                               rb_friction=0.0, gravity_y=-9.81)
     assert np.array_equal(v, z["sis_vel"]) and np.array_equal(w, z["sis_ang"])
     assert np.array_equal(a0, z["sis_acc"][:, 0]) and np.array_equal(a2, z["sis_acc"][:, 2])
+
+
+def _tree(z):
+    return {k: z[k] for k in ("is_leaf", "left", "right")}
+
+
+def test_bvh_static_variants_equal_reference():
+    """staticCollideBVHSoARigidBody and FindAugmentedRealityCollisionsBVHKernel (golden fixture
+    tests/golden/static_scene_bvh.npz: one particle per body, so the reference's per-body totals
+    are the per-particle values; some free particles)."""
+    z = golden("static_scene_bvh")
+    n = len(z["pos"])
+    pf, pt, vel, color = cpu.collide_bvh_static(z["prm"], float(z["radius"]), z["rb_idx"],
+                                                z["rel"], z["pos"], z["vel"], _tree(z), z["cms"],
+                                                z["bounds"], z["radii"])
+    body = z["rb_idx"] >= 0
+    assert (np.abs(z["body_force"]).sum(1) > 0).sum() > 100 and (~body).sum() > 10
+    assert np.array_equal(pf[body], z["body_force"][body])
+    assert np.array_equal(pt[body], z["body_torque"][body])
+    assert np.array_equal(vel, z["vel_out"]) and np.array_equal(color, z["color"])
+    cd, cp, fc = cpu.find_contacts_bvh_static(float(z["radius"]), z["pos"], _tree(z), z["cms"],
+                                              z["bounds"], z["sorted_idx"], z["radii"],
+                                              np.zeros(n, np.float32), np.full(n, -1, np.int32))
+    assert (cd > 0).sum() > 100
+    assert np.array_equal(cd, z["contact_distance"]) and np.array_equal(cp, z["contact_point"])
+    assert np.array_equal(fc, z["find_color"])
