@@ -84,6 +84,25 @@ struct DeviceInts {
 };
 static DeviceInts g_offsets, g_starts, g_counts;
 
+// Grow-only device scratch (32-bit words) for wrappers that need temporaries.
+struct DeviceWords {
+  uint32_t* ptr = nullptr;
+  size_t cap = 0;
+  uint32_t* reserve(size_t n) {
+    if (n > cap) {
+      if (ptr) cudaFree(ptr);
+      cap = n + n / 4 + 64;
+      if (cudaMalloc(&ptr, cap * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        cap = 0;
+      }
+    }
+    return ptr;
+  }
+};
+static DeviceWords g_spare_keys, g_spare_vals, g_box;
+
 inline std::vector<int32_t> prefix(const int* counts, int n) {
   std::vector<int32_t> off(n + 1, 0);
   for (int i = 0; i < n; ++i) off[i + 1] = off[i] + counts[i];
@@ -168,11 +187,14 @@ void sortParticlesPreallocated(uint** dGridParticleHash, uint** dGridParticleInd
 }
 
 void sortParticles(uint** dGridParticleHash, uint** dGridParticleIndex, uint numParticles) {
-  // sorted in place (through a temporary pair of buffers)
-  uint *k2 = nullptr, *v2 = nullptr;
-  if (cudaMalloc(&k2, sizeof(uint) * numParticles) != cudaSuccess ||
-      cudaMalloc(&v2, sizeof(uint) * numParticles) != cudaSuccess) {
-    arsim_compat_detail::g_handler(AR_ERR_OOM, "sortParticles", "temporary buffers");
+  // sorted in place, through a spare pair of buffers that grows only when a call sorts more
+  // pairs than any call before it (no allocation per call in steady state)
+  using arsim_compat_detail::g_spare_keys;
+  using arsim_compat_detail::g_spare_vals;
+  uint32_t* k2 = g_spare_keys.reserve(numParticles);
+  uint32_t* v2 = g_spare_vals.reserve(numParticles);
+  if (!k2 || !v2) {
+    arsim_compat_detail::g_handler(AR_ERR_OOM, "sortParticles", "spare sort buffers");
     return;
   }
   ARC_CHECK(ar_radix_sort_pairs_u32(ARC_CTX, *dGridParticleHash, *dGridParticleIndex, k2, v2,
@@ -180,8 +202,6 @@ void sortParticles(uint** dGridParticleHash, uint** dGridParticleIndex, uint num
             "sortParticles");
   cudaMemcpy(*dGridParticleHash, k2, sizeof(uint) * numParticles, cudaMemcpyDeviceToDevice);
   cudaMemcpy(*dGridParticleIndex, v2, sizeof(uint) * numParticles, cudaMemcpyDeviceToDevice);
-  cudaFree(k2);
-  cudaFree(v2);
 }
 
 void createMortonCodesPreallocated(float4* positions, unsigned int** mortonCodes, int** indices,
@@ -212,8 +232,9 @@ cudaError_t createMortonCodes(float4* positions, unsigned int** mortonCodes, int
                               unsigned int** sortedMortonCodes, int** sortedIndices,
                               int numberOfPrimitives, int numberOfThreads) {
   (void)numberOfThreads;
-  float4* box = nullptr;
-  if (cudaMalloc(&box, 2 * sizeof(float4)) != cudaSuccess) return cudaErrorMemoryAllocation;
+  // the scene box (min, max) lives in a buffer allocated on the first call only
+  float4* box = reinterpret_cast<float4*>(arsim_compat_detail::g_box.reserve(8));
+  if (!box) return cudaErrorMemoryAllocation;
   ar_status s = ar_scene_aabb(ARC_CTX, (float*)positions, numberOfPrimitives, (float*)box,
                               (float*)(box + 1), nullptr);
   if (s == AR_OK)
@@ -223,7 +244,6 @@ cudaError_t createMortonCodes(float4* positions, unsigned int** mortonCodes, int
     s = ar_radix_sort_pairs_u32(ARC_CTX, *mortonCodes, (uint32_t*)*indices, *sortedMortonCodes,
                                 (uint32_t*)*sortedIndices, numberOfPrimitives, 0, 32, nullptr);
   if (s == AR_OK) s = ar_ctx_status(ARC_CTX, nullptr);
-  cudaFree(box);
   return s == AR_OK ? cudaSuccess : cudaErrorUnknown;
 }
 
