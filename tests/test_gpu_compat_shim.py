@@ -10,8 +10,8 @@ reference's own kernel bodies (tests/golden/make_golden.py):
   bit, and the `**` swap (afterwards *hash and *index point at the sorted data, the sorted
   pointers at the spare buffers, as cub::DoubleBuffer::Current / Alternate);
 * sortParticles: sorted in place, pointers unchanged, no device memory taken by a repeat call;
-* ReducePerParticleImpulses with host-side counts: the oracle's fixed-order sums (the
-  reference's own scan differences drop each body's first particle and are reported beside);
+* ReducePerParticleImpulses with host-side counts: the oracle's fixed-order sums (the shim does
+  not reproduce the reference's prefix-sum differences, which drop each body's first particle);
 * WallCollisionWrapper: the reference's Baraff wall impulses bit for bit.
 """
 import ctypes as C
@@ -44,7 +44,9 @@ def drv(ctx):
 
 
 def _p(t: torch.Tensor) -> C.c_void_p:
-    return C.c_void_p(t.data_ptr())
+    """Device pointer that keeps its tensor alive for as long as the pointer object (temporary
+    tensors passed to a call must not be freed before the call returns)."""
+    return api.ptr(t)
 
 
 def _params(g) -> api.SimParams:
