@@ -70,6 +70,16 @@ __device__ __forceinline__ uint32_t body_tag(int local_body) {
   return (uint32_t)local_body + 1u <= kMaxTag ? (uint32_t)local_body + 1u : 0u;
 }
 
+// The scene of a particle or body.  A batch of one scene passes its descriptor itself as a
+// kernel parameter (kOne): it is read from the constant bank, and no lookup of the scene index
+// and the table entry sits in front of the particle's own loads.
+template <bool kOne>
+__device__ __forceinline__ const SceneDev& scene_at(const SceneDev& one,
+                                                    const SceneDev* __restrict__ table, int s) {
+  if constexpr (kOne) return one;
+  else return table[s];
+}
+
 // Scene index of every particle and body of the batch (run when the member list changes).
 __global__ void __launch_bounds__(256) scene_ids_kernel(const int* __restrict__ poff,
                                                         const int* __restrict__ boff, int ns,
@@ -104,8 +114,10 @@ __global__ void __launch_bounds__(256) step_clear_kernel(uint4* __restrict__ hea
 // and issues the loads of all of them before using any, which keeps several dependent
 // gathers (scene -> offset -> body) in flight per thread.
 constexpr int kKeysBatch = 2;
+template <bool kOne>
 __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table,
+    const int* __restrict__ pscene, int nt,
     uint32_t* __restrict__ keys, uint32_t* __restrict__ ws_hist, ar_sort::Plan plan,
     long long* __restrict__ d_step) {
   ar::pdl_wait();
@@ -121,13 +133,13 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
 #pragma unroll
     for (int u = 0; u < kKeysBatch; ++u) {
       const int g = g0 + u * stride;
-      sc[u] = g < nt ? __ldg(pscene + g) : 0;
+      sc[u] = !kOne && g < nt ? __ldg(pscene + g) : 0;
     }
 #pragma unroll
     for (int u = 0; u < kKeysBatch; ++u) {
       const int g = g0 + u * stride;
       if (g < nt) {
-        const SceneDev& S = table[sc[u]];
+        const SceneDev& S = scene_at<kOne>(one, table, sc[u]);
         r4[u] = __ldg(S.rel + (g - S.poff));
       }
     }
@@ -135,7 +147,7 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
     for (int u = 0; u < kKeysBatch; ++u) {
       const int g = g0 + u * stride;
       if (g < nt) {
-        const SceneDev& S = table[sc[u]];
+        const SceneDev& S = scene_at<kOne>(one, table, sc[u]);
         const int b = __float_as_int(r4[u].w);
         q[u] = __ldg(S.quat + b);
         c[u] = __ldg(S.pos + b);
@@ -145,7 +157,7 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
     for (int u = 0; u < kKeysBatch; ++u) {
       const int g = g0 + u * stride;
       if (g < nt) {
-        const SceneDev& S = table[sc[u]];
+        const SceneDev& S = scene_at<kOne>(one, table, sc[u]);
         const float3 r = ar::quat_rotate(q[u], ar::mk3(r4[u].x, r4[u].y, r4[u].z));
         const float3 p = ar::add(ar::xyz(c[u]), r);
         const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
@@ -168,8 +180,10 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
 // cell's first slot writes the whole entry.
 // kScatterBatch sorted slots per thread and round, loads issued before use (as in K1).
 constexpr int kScatterBatch = 1;
+template <bool kOne>
 __global__ void __launch_bounds__(256) scatter_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int nt,
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table,
+    const int* __restrict__ pscene, int nt,
     const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
     uint2* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
     const long long* __restrict__ d_step) {
@@ -193,18 +207,18 @@ __global__ void __launch_bounds__(256) scatter_kernel(
     }
 #pragma unroll
     for (int u = 0; u < kScatterBatch; ++u)
-      if (k0 + u * stride < nt) sc[u] = __ldg(pscene + g[u]);
+      if (k0 + u * stride < nt) sc[u] = kOne ? 0 : __ldg(pscene + g[u]);
 #pragma unroll
     for (int u = 0; u < kScatterBatch; ++u) {
       if (k0 + u * stride < nt) {
-        const SceneDev& S = table[sc[u]];
+        const SceneDev& S = scene_at<kOne>(one, table, sc[u]);
         r4[u] = __ldg(S.rel + (g[u] - S.poff));
       }
     }
 #pragma unroll
     for (int u = 0; u < kScatterBatch; ++u) {
       if (k0 + u * stride < nt) {
-        const SceneDev& S = table[sc[u]];
+        const SceneDev& S = scene_at<kOne>(one, table, sc[u]);
         const int b = __float_as_int(r4[u].w);
         q[u] = __ldg(S.quat + b);
         c[u] = __ldg(S.pos + b);
@@ -216,7 +230,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(
     for (int u = 0; u < kScatterBatch; ++u) {
       const int k = k0 + u * stride;
       if (k >= nt) continue;
-      const SceneDev& S = table[sc[u]];
+      const SceneDev& S = scene_at<kOne>(one, table, sc[u]);
       const int b = __float_as_int(r4[u].w);
       if (first[u]) {
         // occupants of one cell belong to one scene
@@ -252,8 +266,9 @@ struct RowCells {
   uint2 a, b, c;
 };
 
+template <bool kOne>
 __global__ void __launch_bounds__(256, 4) collide_kernel(
-    const SceneDev* __restrict__ table, int nt, const uint32_t* __restrict__ skeys,
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table, int nt, const uint32_t* __restrict__ skeys,
     const uint32_t* __restrict__ svals, const uint2* __restrict__ cells,
     const float4* __restrict__ spos, const float4* __restrict__ svel,
     float4* __restrict__ pforce, const long long* __restrict__ d_step) {
@@ -263,7 +278,7 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
   const uint32_t epoch = cell_epoch(*d_step);
   const float4 p4 = __ldg(spos + k);
   const float4 v4 = __ldg(svel + k);
-  const SceneDev& S = table[__float_as_int(v4.w)];
+  const SceneDev& S = scene_at<kOne>(one, table, kOne ? 0 : __float_as_int(v4.w));
   const float3 pos = ar::xyz(p4), vel = ar::xyz(v4);
   const int body = __float_as_int(p4.w);
   // the meta word of a cell holding only this body, count bits cleared (an impossible word
@@ -368,16 +383,17 @@ __device__ __forceinline__ uint64_t morton_key(const SceneDev& S, int s, float3 
   return ((uint64_t)s << kMortonBits) | code;
 }
 
-template <class K>
-__global__ void __launch_bounds__(256) morton_key_kernel(const SceneDev* __restrict__ table,
+template <class K, bool kOne>
+__global__ void __launch_bounds__(256) morton_key_kernel(const __grid_constant__ SceneDev one,
+                                                         const SceneDev* __restrict__ table,
                                                          const int* __restrict__ pscene, int ns,
                                                          int nt, K* __restrict__ keys,
                                                          long long* __restrict__ d_step) {
   ar::pdl_wait();
   if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nt; g += gridDim.x * blockDim.x) {
-    const int s = __ldg(pscene + g);
-    const SceneDev& S = table[s];
+    const int s = kOne ? 0 : __ldg(pscene + g);
+    const SceneDev& S = scene_at<kOne>(one, table, s);
     const float4 r4 = __ldg(S.rel + (g - S.poff));
     const int b = __float_as_int(r4.w);
     const float3 r = ar::quat_rotate(__ldg(S.quat + b), ar::mk3(r4.x, r4.y, r4.z));
@@ -456,8 +472,9 @@ __device__ __forceinline__ void refit_from_leaf(int i, int n, const int32_t* __r
 // Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
 // state; the leaf box (position +/- r) goes into its parent's slot, and the thread climbs from
 // there (the refit); leaf flags and ranges.
+template <bool kOne>
 __global__ void __launch_bounds__(256) bvh_leaves_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table, const int* __restrict__ pscene, int ns, int nt,
     const uint32_t* __restrict__ svals, const int32_t* __restrict__ left,
     const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
     WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
@@ -465,8 +482,8 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
   ar::pdl_wait();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const int g = (int)__ldg(svals + k);
-    const int sc = __ldg(pscene + g);
-    const SceneDev& S = table[sc];
+    const int sc = kOne ? 0 : __ldg(pscene + g);
+    const SceneDev& S = scene_at<kOne>(one, table, sc);
     const float4 r4 = __ldg(S.rel + (g - S.poff));
     const int b = __float_as_int(r4.w);
     float3 r, p, v;
@@ -526,8 +543,9 @@ __global__ void bvh_roots_kernel(const int* __restrict__ poff, int ns, int nt,
 // so the stack never holds more than 62 entries.
 constexpr int kBvhStack = 64;
 
+template <bool kOne>
 __global__ void __launch_bounds__(256) bvh_collide_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table, const int* __restrict__ poff, int ns, int nt,
     const uint32_t* __restrict__ svals, const float4* __restrict__ spos,
     const float4* __restrict__ svel, const WideNode* __restrict__ nodes,
     const int32_t* __restrict__ roots, float4* __restrict__ pforce, int* __restrict__ err) {
@@ -536,8 +554,8 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
   if (k >= nt) return;
   const float4 p4 = __ldg(spos + k);
   const float4 v4 = __ldg(svel + k);
-  const int s = __float_as_int(v4.w);
-  const SceneDev& S = table[s];
+  const int s = kOne ? 0 : __float_as_int(v4.w);
+  const SceneDev& S = scene_at<kOne>(one, table, s);
   const float3 pos = ar::xyz(p4), vel = ar::xyz(v4);
   const int body = __float_as_int(p4.w);
   const float rr = S.r;
@@ -597,8 +615,10 @@ __global__ void __launch_bounds__(256) bvh_collide_kernel(
 // kernel, so that the integration runs on every lane instead of lane 0 of each warp).  A scene
 // whose step budget is spent (batch step number > end_step) is frozen: its state and sums are
 // left untouched.
+template <bool kOne>
 __global__ void __launch_bounds__(256) body_step_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table,
+    const int* __restrict__ bscene, int bt,
     const float4* __restrict__ pforce, const long long* __restrict__ d_step,
     int* __restrict__ err) {
   ar::pdl_wait();
@@ -606,7 +626,7 @@ __global__ void __launch_bounds__(256) body_step_kernel(
   const int lane = ar::lane_id();
   const long long step = *d_step;
   for (int gb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; gb < bt; gb += warps) {
-    const SceneDev& S = table[__ldg(bscene + gb)];
+    const SceneDev& S = scene_at<kOne>(one, table, kOne ? 0 : __ldg(bscene + gb));
     if (step > S.end_step) continue;
     const int b = gb - S.boff;
     const int s0 = __ldg(S.offsets + b), s1 = __ldg(S.offsets + b + 1);
@@ -636,13 +656,15 @@ __global__ void __launch_bounds__(256) body_step_kernel(
   }
 }
 
+template <bool kOne>
 __global__ void __launch_bounds__(256) integrate_kernel(
-    const SceneDev* __restrict__ table, const int* __restrict__ bscene, int bt,
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table,
+    const int* __restrict__ bscene, int bt,
     const long long* __restrict__ d_step, int* __restrict__ err) {
   ar::pdl_wait();
   const long long step = *d_step;
   for (int gb = blockIdx.x * blockDim.x + threadIdx.x; gb < bt; gb += gridDim.x * blockDim.x) {
-    const SceneDev& S = table[__ldg(bscene + gb)];
+    const SceneDev& S = scene_at<kOne>(one, table, kOne ? 0 : __ldg(bscene + gb));
     if (step > S.end_step) continue;
     const int b = gb - S.boff;
     float ib[9];
@@ -717,6 +739,7 @@ struct ar_batch {
   uint2* cells = nullptr;  // {first slot, count | epoch | body tag} per cell
   char* sort_ws = nullptr;
   SceneDev* d_table = nullptr;
+  SceneDev one{};  // the scene of a one-scene batch (passed to the kernels as a parameter)
   int *d_poff = nullptr, *d_boff = nullptr;
   int *d_pscene = nullptr, *d_bscene = nullptr;  // scene index per particle / body
   long long* d_step = nullptr;   // number of the step being run (incremented by its first kernel)
@@ -936,6 +959,7 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     scene_ids_kernel<<<std::min(arh::grid_for(m, 256), 4096u), 256, 0, st>>>(
         B->d_poff, B->d_boff, (int)ns, (int)nt, (int)bt, B->d_pscene, B->d_bscene);
   }
+  B->one = tab.empty() ? SceneDev{} : tab[0];
   B->nt = nt;
   B->bt = bt;
   B->total_cells = cells;
@@ -963,18 +987,28 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
   const unsigned gp = std::min(arh::grid_for(nt, 256), (unsigned)ctx->num_sms * 8);
   const unsigned g5 = arh::grid_for((long)bt * 32, 256);
+  // a batch of one scene launches the kernels that take its descriptor as a parameter
+  const bool one = ns == 1;
+#define AR_LAUNCH_ONE(kern, grid, block, ...)                                              \
+  do {                                                                                      \
+    if (one) arh::launch_pdl(kern<true>, grid, block, 0, st, B->one, __VA_ARGS__);          \
+    else arh::launch_pdl(kern<false>, grid, block, 0, st, B->one, __VA_ARGS__);            \
+  } while (0)
   mark(0);
   if (B->broadphase == AR_BROADPHASE_BVH) {
     cudaMemsetAsync(B->counters, 0, (size_t)nt * sizeof(int), st);  // refit arrival counters
     mark(1);
     // keys of at most 32 bits (up to 4 scenes) are sorted as uint32: half the bytes per pass
     const bool k32 = B->bvh_key_bits <= 32;
-    if (k32)
-      arh::launch_pdl(morton_key_kernel<uint32_t>, dim3(gp), dim3(256), 0, st, B->d_table,
-          B->d_pscene, ns, nt, B->keys, B->d_step);
+    if (k32 && one)
+      arh::launch_pdl(morton_key_kernel<uint32_t, true>, dim3(gp), dim3(256), 0, st, B->one,
+          B->d_table, B->d_pscene, ns, nt, B->keys, B->d_step);
+    else if (k32)
+      arh::launch_pdl(morton_key_kernel<uint32_t, false>, dim3(gp), dim3(256), 0, st, B->one,
+          B->d_table, B->d_pscene, ns, nt, B->keys, B->d_step);
     else
-      arh::launch_pdl(morton_key_kernel<uint64_t>, dim3(gp), dim3(256), 0, st, B->d_table,
-          B->d_pscene, ns, nt, B->keys64, B->d_step);
+      arh::launch_pdl(morton_key_kernel<uint64_t, false>, dim3(gp), dim3(256), 0, st, B->one,
+          B->d_table, B->d_pscene, ns, nt, B->keys64, B->d_step);
     mark(2);
     ar_status s = k32 ? ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0,
                                           B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64)
@@ -992,45 +1026,46 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
           ar_lbvh::Lcp64Scene{B->skeys64, nt, B->d_poff, kMortonBits}, nt, B->is_leaf, B->left,
           B->right, B->parent, B->min_r, B->max_r, B->nodes);
     // one thread per leaf: each climbs after storing its leaf
-    arh::launch_pdl(bvh_leaves_kernel, dim3(arh::grid_for(nt, 256)), dim3(256), 0, st, B->d_table,
+    AR_LAUNCH_ONE(bvh_leaves_kernel, dim3(arh::grid_for(nt, 256)), dim3(256), B->d_table,
         B->d_pscene, ns, nt, B->svals, B->left, B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
         B->min_r, B->max_r, B->counters);
     arh::launch_pdl(bvh_roots_kernel, dim3(arh::grid_for(ns, 128)), dim3(128), 0, st, B->d_poff, ns,
         nt, B->parent, B->min_r, B->max_r, B->roots);
     mark(4);
-    arh::launch_pdl(bvh_collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), 0, st, B->d_table,
+    AR_LAUNCH_ONE(bvh_collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), B->d_table,
         B->d_poff, ns, nt, B->svals, B->spos, B->svel, B->nodes, B->roots, B->pforce, ctx->d_err);
     mark(5);
-    arh::launch_pdl(body_step_kernel, dim3(g5), dim3(256), 0, st, B->d_table, B->d_bscene, bt,
+    AR_LAUNCH_ONE(body_step_kernel, dim3(g5), dim3(256), B->d_table, B->d_bscene, bt,
         B->pforce, B->d_step, ctx->d_err);
-    arh::launch_pdl(integrate_kernel, dim3(arh::grid_for(bt, 256)), dim3(256), 0, st, B->d_table,
+    AR_LAUNCH_ONE(integrate_kernel, dim3(arh::grid_for(bt, 256)), dim3(256), B->d_table,
         B->d_bscene, bt, B->d_step, ctx->d_err);
     mark(6);
-    return arh::check_launch("step (BVH)");
+    return arh::check_launch("step (BVH)");  // (AR_LAUNCH_ONE is undefined after the grid path)
   }
   arh::launch_pdl(step_clear_kernel, dim3(ctx->num_sms * 2), dim3(256), 0, st, (uint4*)B->sort_ws,
       (long)(ar_sort::clear_bytes(nt, B->plan.passes) / 16), B->cells, B->cap_cells, B->d_step);
   mark(1);
-  arh::launch_pdl(grid_keys_kernel,
+  AR_LAUNCH_ONE(grid_keys_kernel,
       dim3(std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4)), dim3(kK1Threads),
-      0, st, B->d_table, B->d_pscene, nt, B->keys, (uint32_t*)B->sort_ws, B->plan, B->d_step);
+      B->d_table, B->d_pscene, nt, B->keys, (uint32_t*)B->sort_ws, B->plan, B->d_step);
   mark(2);
   // cell keys in particle order: a warp's keys share few digits, so match.any ranking
   ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
                                   st, B->sort_ws, B->cap_sort, true, true);
   if (s != AR_OK) return s;
   mark(3);
-  arh::launch_pdl(scatter_kernel, dim3(gp), dim3(256), 0, st, B->d_table, B->d_pscene, nt, B->skeys,
+  AR_LAUNCH_ONE(scatter_kernel, dim3(gp), dim3(256), B->d_table, B->d_pscene, nt, B->skeys,
       B->svals, B->cells, B->spos, B->svel, B->d_step);
   mark(4);
-  arh::launch_pdl(collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), 0, st, B->d_table, nt,
+  AR_LAUNCH_ONE(collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), B->d_table, nt,
       B->skeys, B->svals, B->cells, B->spos, B->svel, B->pforce, B->d_step);
   mark(5);
-  arh::launch_pdl(body_step_kernel, dim3(g5), dim3(256), 0, st, B->d_table, B->d_bscene, bt,
+  AR_LAUNCH_ONE(body_step_kernel, dim3(g5), dim3(256), B->d_table, B->d_bscene, bt,
       B->pforce, B->d_step, ctx->d_err);
-  arh::launch_pdl(integrate_kernel, dim3(arh::grid_for(bt, 256)), dim3(256), 0, st, B->d_table,
+  AR_LAUNCH_ONE(integrate_kernel, dim3(arh::grid_for(bt, 256)), dim3(256), B->d_table,
       B->d_bscene, bt, B->d_step, ctx->d_err);
   mark(6);
+#undef AR_LAUNCH_ONE
   return arh::check_launch("step");
 }
 
