@@ -245,88 +245,13 @@ def job_rate(world: int, units_per_rank: int, steps: int, ms: float) -> float:
 
 
 # ---- CPU legs (oracle) ---------------------------------------------------------------------
-class ReferenceCPUStep:
-    """One updateUniformGridDEM step (RigidBodies/UniformGridUpdate.cpp:939-999) made of the
-    reference's own kernel bodies run on the host cores: GPUintegratorKernel,
-    computeGlobalAttributes, calcHashD, the CUB-order stable sort, reorder (with its
-    full-grid clear), FindAndHandleRigidBodyCollisionsUniformGridKernel and
-    ReducePerParticleImpulses.  Physical constants are given the reference's per-step form
-    (impulse = force * dt, velocity increment g * dt)."""
-
-    def __init__(self, scene, grid):
-        from oracle import ref
-        self.ref = ref
-        self.s = scene
-        origin, cell, dims = grid
-        dt = scene.dt
-        self.prm = ref.sim_params(scene.radius, origin, cell[0], dims, scene.spring * dt,
-                              scene.damping * dt, scene.shear * dt, scene.attraction * dt,
-                              gravity=tuple(g * dt for g in scene.gravity), w_damping=1.0)
-        self.ncell = int(np.prod(dims))
-        n, nb = scene.num_particles, scene.num_bodies
-        self.rb = scene.body_index()
-        self.counts = np.diff(scene.body_offsets).astype(np.int32)
-        self.st = {"cms": scene.body_pos.copy(), "vel": scene.body_vel.copy(),
-                   "ang": scene.body_angvel.copy(), "quat": np.tile([0, 0, 0, 1.0], (nb, 1)).astype(np.float32),
-                   "ib": scene.body_inv_inertia.copy(), "cur": np.zeros((nb, 9), np.float32),
-                   "model": np.zeros((nb, 16), np.float32), "cum": scene.body_quat.copy()}
-        # world-frame relative positions, as the reference keeps them
-        from diploma_thesis_b200.scenes import quat_to_matrix
-        R = quat_to_matrix(scene.body_quat.astype(np.float64))[self.rb]
-        self.rel = np.zeros((n, 4), np.float32)
-        self.rel[:, :3] = np.einsum("nij,nj->ni", R, scene.particle_rel[:, :3])
-
-    def step(self):
-        ref, s = self.ref, self.s
-        self.st = ref.gpu_integrator(self.prm, s.dt, self.st)
-        self.rel, pos, vel, q = ref.global_attributes(self.st["cms"], self.st["vel"],
-                                                      self.st["ang"], self.st["quat"], self.rb,
-                                                      self.rel)
-        self.st["quat"] = q
-        h, idx = ref.calc_hash(self.prm, pos)
-        sh, si = ref.sort_pairs_u32(h, idx)
-        cs, ce, sp, sv = ref.reorder(sh, si, pos, vel, self.ncell)
-        pf, pt = ref.collide_grid_dem(self.prm, self.rb, sp, sv, self.rel, si, cs, ce)
-        self.st["vel"], self.st["ang"] = ref.reduce_impulses(
-            pf, pt, self.st["vel"], self.st["ang"], s.body_mass, s.body_inv_inertia, self.counts)
-
-
-class ReferenceCPUStepBVH(ReferenceCPUStep):
-    """The BVH form of the same step, from the reference's own kernel bodies on the host cores:
-    GPUintegratorKernel, computeGlobalAttributes, findAABBCub, generateMortonCodes, the
-    CUB-order stable sort, kernelConstructRadixTreeSoA, kernelConstructLeafNodesSoA,
-    kernelConstructInternalNodesSoA, collideBVHSoARigidBody and ReducePerParticleImpulses."""
-
-    def step(self):
-        ref, s = self.ref, self.s
-        self.st = ref.gpu_integrator(self.prm, s.dt, self.st)
-        self.rel, pos, vel, q = ref.global_attributes(self.st["cms"], self.st["vel"],
-                                                      self.st["ang"], self.st["quat"], self.rb,
-                                                      self.rel)
-        self.st["quat"] = q
-        mn, mx = ref.aabb(pos)
-        codes, idx = ref.morton30(pos, mn, mx)
-        sk, si = ref.sort_pairs_u32(codes, idx)
-        tree = ref.radix_tree(sk)
-        cms, _, bounds, radii = ref.leaves_and_refit(tree, si, pos, s.radius)
-        pf, pt, _ = ref.collide_bvh_rigid(self.prm, self.rb, self.rel, vel, tree, cms, bounds, si,
-                                          radii)
-        self.st["vel"], self.st["ang"] = ref.reduce_impulses(
-            pf, pt, self.st["vel"], self.st["ang"], s.body_mass, s.body_inv_inertia, self.counts)
-
-
-REFERENCE_SEMANTICS = ("the reference's own step (REFERENCE semantics: DEM impulses applied as "
-                       "velocity increments, gravity added once per step, world-frame particle "
-                       "offsets re-rotated every step); the GPU arm runs the PHYSICAL step of the "
-                       "same pipeline (same broad phase, contact law and summation order)")
-
-
 def cpu_reference_rate(scene, grid, target_s: float, broadphase: str = "grid",
                        warmup: int = 1, steps: int | None = None):
     """Particle-steps/s of the reference CPU step on the whole workload (every body of the
     scene): `warmup` untimed steps, then steps until `target_s` seconds have passed (or exactly
     `steps`).  Returns (rate, cores, kind, sample description, steps run, seconds)."""
     from oracle import ref
+    from oracle.ref_step import ReferenceCPUStep, ReferenceCPUStepBVH
     if not ref.available():
         return None
     runner = (ReferenceCPUStepBVH if broadphase == "bvh" else ReferenceCPUStep)(scene, grid)
@@ -358,6 +283,7 @@ def run_reference(args):
     if rank != 0:
         return 0
     from oracle import cpu, ref
+    from oracle.ref_step import REFERENCE_SEMANTICS
     scene, desc = make_scene(args.workload)
     if args.broadphase == "bvh":
         desc = desc.replace("grid 256x512x256 wrapped", "BVH").replace("grid 128^3", "BVH")
@@ -487,6 +413,7 @@ def run_ours(args):
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import cpu
+        from oracle.ref_step import REFERENCE_SEMANTICS
         r = cpu_reference_rate(scene, cpu.scene_grid(scene), target_s=15.0,
                                broadphase=args.broadphase)
         if r is not None:
@@ -494,7 +421,9 @@ def run_ours(args):
             cpu_baseline = {"value": rate / 1e6, "unit": "Mparticle-steps/s", "cores": cores,
                             "kind": kind, "sample": sample, "semantics": REFERENCE_SEMANTICS}
 
-    memsets = 2 if args.broadphase == "bvh" else 1  # memset nodes are not kernels (steady step)
+    # memset nodes are not kernels: the BVH step has two (refit counters, sort head), the grid
+    # step none (its clears are a kernel)
+    memsets = 2 if args.broadphase == "bvh" else 0
     launches = args.steps * (gs.launches_per_step() - memsets)
     if rank == 0:
         line = {
@@ -856,14 +785,81 @@ def run_served(args):
     return 0
 
 
+def run_refgpu(args):
+    """The reference's own GPU step (updateUniformGridDEM: its kernels compiled for sm_100a from
+    the reference's sources, its wrappers with their allocations and synchronisations,
+    oracle/_ref/libref_gpu.so) beside this repository's fused grid step, on the same scene and
+    GPU, stage by stage.  Both start from the scene's initial state; W untimed steps, then K
+    timed steps each (the reference's stages by CUDA events on its legacy stream; ours by the
+    event-bracketed stage profile and by graph replays).  The reference runs REFERENCE
+    semantics (impulses as velocity increments), ours PHYSICAL: same broad phase, contact law
+    and summation order, same particles and cells."""
+    import torch
+    from diploma_thesis_b200 import api
+    from oracle import cpu, ref_gpu
+    if not ref_gpu.available():
+        print(json.dumps({"workload": "refgpu", "unavailable":
+                          "the reference GPU build (oracle/_ref/libref_gpu.so) is not present"}))
+        return 0
+    torch.cuda.set_device(0)
+    scene, desc = make_scene(args.ref_scene)
+    n = scene.num_particles
+    # the reference's step
+    rg = ref_gpu.RefGpuStep(scene, cpu.scene_grid(scene))
+    for _ in range(args.warmup):
+        rg.step()
+    acc = np.zeros(len(ref_gpu.STAGES))
+    host = 0.0
+    for _ in range(args.steps):
+        ms, wall = rg.step()
+        acc += ms
+        host += wall
+    rg.close()
+    ref_stage = acc / args.steps
+    ref_ms = float(ref_stage.sum())
+    # ours, same scene and step window
+    ctx = api.Context(0)
+    gs = api.GpuScene(ctx, scene)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        gs.step(args.warmup, use_graph=True, stream=stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        stream.synchronize()
+        a.record(stream)
+        gs.step(args.steps, use_graph=True, stream=stream)
+        b.record(stream)
+        b.synchronize()
+        ours_ms = a.elapsed_time(b) / args.steps
+        ours_stage = gs.profile(min(args.steps, 50), stream=stream)
+    ctx.check(stream)
+    gs.close()
+    ctx.close()
+    line = {"metric": "ms per step", "workload": "refgpu",
+            "config": {"scene": desc, "particles": n, "steps": args.steps,
+                       "warmup": args.warmup},
+            "reference_gpu": {"ms_per_step": ref_ms, "host_ms_per_step": host / args.steps,
+                              "mparticle_steps_per_s": n / ref_ms / 1e3,
+                              "stages_ms": dict(zip(ref_gpu.STAGES, ref_stage.tolist())),
+                              "build": "the reference's CUDA sources for sm_100a, its wrappers",
+                              "semantics": "REFERENCE"},
+            "ours": {"ms_per_step": ours_ms, "mparticle_steps_per_s": n / ours_ms / 1e3,
+                     "stages_ms": dict(zip(STAGES, [float(x) for x in ours_stage])),
+                     "semantics": "PHYSICAL"},
+            "speedup": ref_ms / ours_ms}
+    print(json.dumps(line))
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh", "sis"],
-                    default="pile")
+    ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh", "sis",
+                                           "refgpu"], default="pile")
+    ap.add_argument("--ref-scene", choices=["pile", "plain"], default="pile",
+                    help="refgpu: the scene both steps run")
     ap.add_argument("--lbvh-sizes", default="", help="lbvh: comma-separated point counts")
     ap.add_argument("--lbvh-reps", type=int, default=10, help="lbvh: timed repetitions")
     ap.add_argument("--broadphase", choices=["grid", "bvh"], default="grid",
@@ -891,6 +887,8 @@ def main(argv=None):
         return run_lbvh(args)
     if args.workload == "sis":
         return run_sis(args)
+    if args.workload == "refgpu":
+        return run_refgpu(args)
     return run_ours(args)
 
 
