@@ -681,8 +681,8 @@ def run_sis(args):
     packed 16^3 block of 4,096 cubes x 27 (110,592 particles, r = 1/256, 128^3 grid), every
     cube in contact with its neighbours; per step the integration, the contact search, the
     gather and 18 sequential-impulse sweeps, all on the device.  The CPU baseline is the
-    oracle's restatement of the same step (the reference's gather and solver are host loops;
-    kind "port"), one thread, one step."""
+    reference's own code for the same step on the host (kind "reference"): its kernel bodies
+    for the contact search, its gather and solver host loops."""
     import torch
     from diploma_thesis_b200 import api, scenes
     from diploma_thesis_b200.sis import SISScene, ITERATIONS
@@ -705,17 +705,33 @@ def run_sis(args):
     n = sc.num_particles
     cpu = None
     if not args.no_cpu:
-        from oracle import cpu as ocpu
-        before = dict(st)
-        before["mass"] = sc.body_mass.astype(np.float32)
-        t0 = time.perf_counter()
-        ocpu.sis_solve(before, sc.body_index(), tuple(sc.box_min), 2 * np.float32(sc.radius),
-                       (128, 128, 128), sc.radius, gravity_y=g.params.gravity[1],
-                       iterations=ITERATIONS)
-        cpu_s = time.perf_counter() - t0
-        cpu = {"value": n / cpu_s / 1e6, "unit": "Mparticle-steps/s", "cores": 1, "kind": "port",
-               "sample": "one step's contact search, gather, sequential-impulse sweeps and "
-                         "particle update of the same scene (oracle restatement, one thread)"}
+        # the second half of the same step (after the integration) by the reference's own code
+        # on the host: its hash / sort / reorder / contact-search kernel bodies (OpenMP), then
+        # GatherRigidBodyCollisions + SequentialImpulseSolver and the re-posing tail, its host
+        # loops (Particles/updateFunctions.cpp:1431-1874, one thread, as in the reference)
+        import ctypes as C
+        from oracle import ref
+        if ref.available():
+            prm = ref.SimParams()
+            C.memmove(C.byref(prm), C.byref(g.params), C.sizeof(prm))
+            rb = sc.body_index().astype(np.int32)
+            t0 = time.perf_counter()
+            h, idx = ref.calc_hash(prm, st["pos"])
+            sh, si = ref.sort_pairs_u32(h, idx)
+            cs, ce, sp, _ = ref.reorder(sh, si, st["pos"], st["pvel"], 128 ** 3)
+            cd, cb, cp = ref.find_rb_collisions_grid(prm, rb, sp, si, cs, ce,
+                                                     np.zeros(n, np.float32))
+            res = ref.sis_step(prm, rb, sc.body_offsets, st["cms"], st["vel"], st["ang"],
+                               st["cur"], sc.body_mass.astype(np.float32), st["rel"], cd, cb,
+                               cp)
+            cpu_s = time.perf_counter() - t0
+            cpu = {"value": n / cpu_s / 1e6, "unit": "Mparticle-steps/s",
+                   "cores": ref.max_threads(), "kind": "reference",
+                   "sample": f"one step's hash, sort, reorder and contact search (the "
+                             f"reference's kernel bodies, OpenMP) and its gather, "
+                             f"{res['count']} contacts' sequential-impulse sweeps and particle "
+                             f"update (the reference's host loops, one thread) on the same "
+                             f"scene state"}
     print(json.dumps({
         "metric": "Mparticle-steps/s (sequential-impulse path)", "value": n / ms / 1e3,
         "unit": "Mparticle-steps/s", "n_gpus": 1, "steps": steps, "warmup": args.warmup,
@@ -749,7 +765,7 @@ def run_served(args):
     stats = server.run(reqs, time_limit=args.duration)
     s = stats.summary()
     # plain: a sample of the same requests, one at a time (create, K steps, download)
-    sample = reqs[: min(len(reqs), 40)]
+    sample = reqs[: min(len(reqs), args.plain_sample)]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     steps = parts = 0
@@ -874,6 +890,8 @@ def main(argv=None):
     ap.add_argument("--rate", type=float, default=2000.0, help="served: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="served: seconds of arrivals")
     ap.add_argument("--pool", type=int, default=64, help="served: distinct scenes drawn from")
+    ap.add_argument("--plain-sample", type=int, default=200,
+                    help="served: requests timed one at a time for the plain form")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     args = ap.parse_args(argv)
     args.warmup = max(args.warmup, 3)
