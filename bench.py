@@ -761,7 +761,8 @@ def run_served(args):
         return sc, int(r.integers(10, 501))
 
     reqs = serve.poisson_requests(args.rate, args.duration, make, seed=2)
-    server = serve.Server(ctx, args.hbm_budget_gb * 1e9, tick_steps=10)
+    # the request loop in C++ (ar_server_run); the pool's scenes become resident templates
+    server = serve.NativeServer(ctx, args.hbm_budget_gb * 1e9, tick_steps=10)
     stats = server.run(reqs, time_limit=args.duration)
     s = stats.summary()
     # plain: a sample of the same requests, one at a time (create, K steps, download)
@@ -784,7 +785,7 @@ def run_served(args):
             "config": {"workload": f"served: Poisson {args.rate}/s for {args.duration} s, "
                                    "scenes 1k-500k particles (cubes/rods 50/50), K in 10..500, "
                                    f"HBM budget {args.hbm_budget_gb} GB",
-                       "scene_pool": args.pool},
+                       "scene_pool": args.pool, "loop": "C++ (ar_server_run)"},
             "p50_latency_s": s["p50_latency_s"], "p99_latency_s": s["p99_latency_s"],
             "completed": s["completed"], "offered_requests": s["offered"],
             "mparticle_steps_per_s": s["mparticle_steps_per_s"],

@@ -54,6 +54,16 @@ class SceneInit(C.Structure):
                 ("body_offsets", C.c_void_p), ("particle_rel4", C.c_void_p)]
 
 
+class ServerStatsC(C.Structure):
+    """ar_server_stats (include/arsim.h)."""
+    _fields_ = [("completed", C.c_int), ("offered", C.c_int), ("peak_resident", C.c_int),
+                ("ticks", C.c_int), ("wall_s", C.c_double), ("scene_steps", C.c_longlong),
+                ("particle_steps", C.c_longlong), ("peak_bytes", C.c_size_t),
+                ("host_admit_s", C.c_double), ("host_set_s", C.c_double),
+                ("host_step_s", C.c_double), ("host_retire_s", C.c_double),
+                ("host_wait_s", C.c_double)]
+
+
 class SceneView(C.Structure):
     _fields_ = [("num_bodies", C.c_int), ("num_particles", C.c_int),
                 ("body_pos4", C.c_void_p), ("body_quat4", C.c_void_p),

@@ -1199,6 +1199,52 @@ uint64_t ar_scene_cells(const ar_scene_desc* d) {
   return (uint64_t)g[0] * g[1] * g[2];
 }
 
+}  // extern "C"
+
+namespace {
+// Bytes of a scene's device block: body centre, orientation, velocity, angular velocity, force
+// and torque sums (float4 each), mass, inverse inertia, body offsets and particle offsets, each
+// array 256-byte aligned.
+size_t scene_block_bytes(int nb, int n, size_t sizes[5]) {
+  const size_t a6 = 16 * (size_t)nb;
+  sizes[0] = 6 * ((a6 + 255) & ~(size_t)255);
+  sizes[1] = 4 * (size_t)nb;
+  sizes[2] = 36 * (size_t)nb;
+  sizes[3] = 4 * (size_t)(nb + 1);
+  sizes[4] = 16 * (size_t)n;
+  size_t total = 0;
+  for (int i = 0; i < 5; ++i) total += (sizes[i] + 255) & ~(size_t)255;
+  return total;
+}
+
+// One allocation from the stream-ordered pool for the scene's arrays, carved in the order of
+// scene_block_bytes.  False (block left null) when the pool has no room.
+bool alloc_scene_block(ar_scene* s, cudaStream_t st) {
+  size_t sizes[5];
+  const size_t total = scene_block_bytes(s->nb, s->n, sizes);
+  if (arh::dev_malloc_async(&s->block, total, st) != cudaSuccess) {
+    cudaGetLastError();
+    s->block = nullptr;
+    return false;
+  }
+  char* b = (char*)s->block;
+  const size_t s6 = sizes[0] / 6;
+  float4** arr6[6] = {&s->pos, &s->quat, &s->vel, &s->ang, &s->bforce, &s->btorque};
+  for (int i = 0; i < 6; ++i) *arr6[i] = (float4*)(b + i * s6);
+  b += (sizes[0] + 255) & ~(size_t)255;
+  s->mass = (float*)b;
+  b += (sizes[1] + 255) & ~(size_t)255;
+  s->inv_inertia = (float*)b;
+  b += (sizes[2] + 255) & ~(size_t)255;
+  s->offsets = (int32_t*)b;
+  b += (sizes[3] + 255) & ~(size_t)255;
+  s->rel = (float4*)b;
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
 ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene_init* init,
                           ar_stream_t stream, ar_scene** out) {
   if (!ctx || !desc || !init || !out) return AR_ERR_INVALID_ARG;
@@ -1240,31 +1286,10 @@ ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene
   cudaStream_t st = arh::stream(stream);
   // one allocation from the stream-ordered pool (no device-wide synchronisation), carved into
   // 256-byte aligned arrays
-  const size_t a6 = 16 * (size_t)nb, sizes[5] = {6 * ((a6 + 255) & ~(size_t)255),
-                                                 4 * (size_t)nb, 36 * (size_t)nb,
-                                                 4 * (size_t)(nb + 1), 16 * (size_t)n};
-  size_t total = 0;
-  for (size_t z : sizes) total += (z + 255) & ~(size_t)255;
-  if (arh::dev_malloc_async(&s->block, total, st) != cudaSuccess) {
-    cudaGetLastError();
-    s->block = nullptr;
+  if (!alloc_scene_block(s, st)) {
     ar_scene_destroy(s);
     arh::set_error("ar_scene_create: out of device memory");
     return AR_ERR_OOM;
-  }
-  {
-    char* b = (char*)s->block;
-    const size_t s6 = (a6 + 255) & ~(size_t)255;
-    float4** arr6[6] = {&s->pos, &s->quat, &s->vel, &s->ang, &s->bforce, &s->btorque};
-    for (int i = 0; i < 6; ++i) *arr6[i] = (float4*)(b + i * s6);
-    b += (sizes[0] + 255) & ~(size_t)255;
-    s->mass = (float*)b;
-    b += (sizes[1] + 255) & ~(size_t)255;
-    s->inv_inertia = (float*)b;
-    b += (sizes[2] + 255) & ~(size_t)255;
-    s->offsets = (int32_t*)b;
-    b += (sizes[3] + 255) & ~(size_t)255;
-    s->rel = (float4*)b;
   }
   // particle rel with the body index in w
   std::vector<float4> rel(n);
@@ -1293,6 +1318,32 @@ ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc, const ar_scene
   }
   *out = s;
   return AR_OK;
+}
+
+ar_status ar_scene_clone_async(const ar_scene* proto, ar_stream_t stream, ar_scene** out) {
+  if (!proto || !out || !proto->block) return AR_ERR_INVALID_ARG;
+  *out = nullptr;
+  ar_scene* s = new ar_scene();
+  s->ctx = proto->ctx;
+  s->desc = proto->desc;
+  s->n = proto->n;
+  s->nb = proto->nb;
+  for (int a = 0; a < 3; ++a) {
+    s->origin[a] = proto->origin[a];
+    s->cell[a] = proto->cell[a];
+    s->gdim[a] = proto->gdim[a];
+  }
+  cudaStream_t st = arh::stream(stream);
+  if (!alloc_scene_block(s, st)) {
+    ar_scene_destroy(s);
+    arh::set_error("ar_scene_clone_async: out of device memory");
+    return AR_ERR_OOM;
+  }
+  size_t sizes[5];
+  cudaMemcpyAsync(s->block, proto->block, scene_block_bytes(s->nb, s->n, sizes),
+                  cudaMemcpyDeviceToDevice, st);
+  *out = s;
+  return arh::check_launch("ar_scene_clone_async");
 }
 
 ar_status ar_scene_destroy(ar_scene* s) {

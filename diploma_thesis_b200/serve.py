@@ -1,5 +1,10 @@
 """Continuous-batching server for scene-step requests.
 
+``NativeServer`` runs the request loop in C++ (``ar_server_run``, csrc/ar_serve.cu): request
+templates stay resident on the device and an admission is a device-side clone.  ``Server`` is
+the same policy written over the Python binding; its scene, batch and stream objects are
+parameters, so its admission and tick logic is tested on the CPU with host-only stand-ins.
+
 A request is a new scene plus a number of steps K.  The server keeps every admitted scene
 resident on the device and runs fixed-size ticks of ``tick_steps`` batch steps:
 
@@ -35,7 +40,7 @@ import numpy as np
 import torch
 
 from . import api
-from ._lib import AR_MAX_BATCH_CELLS, AR_MAX_BATCH_PARTICLES, lib
+from ._lib import AR_MAX_BATCH_CELLS, AR_MAX_BATCH_PARTICLES, ServerStatsC, call, lib
 from .scenes import Scene
 
 
@@ -233,6 +238,84 @@ class Server:
 
     def close(self) -> None:
         self.batch.close()
+
+
+class NativeServer:
+    """The continuous-batching loop in C++ (ar_server_create / ar_server_add_template /
+    ar_server_run): the same policy as ``Server`` -- admission in arrival order by HBM budget
+    and batch limits, ticks of ``tick_steps`` batch steps with a step budget per scene, state
+    copies behind the tick, at most ``max_inflight`` ticks queued ahead -- with no Python in the
+    loop.  Each distinct scene of the requests becomes a resident template once; admitting a
+    request clones its template on the device."""
+
+    def __init__(self, ctx, hbm_budget_bytes: float, tick_steps: int = 10,
+                 max_batch_particles: int | None = None, max_inflight: int = 2,
+                 broadphase: str = "grid"):
+        self.ctx = ctx
+        self.broadphase = api.broadphase_code(broadphase)
+        self.handle = C.c_void_p()
+        call("ar_server_create", ctx.handle, C.c_double(hbm_budget_bytes), int(tick_steps),
+             C.c_longlong(int(max_batch_particles or 0)), int(max_inflight),
+             C.byref(self.handle))
+        self._templates: dict[int, int] = {}  # id(Scene) -> template index
+        self._keep: list = []
+
+    def template(self, scene: Scene) -> int:
+        key = id(scene)
+        if key not in self._templates:
+            desc = api.make_desc(scene, self.broadphase)
+            arrays = [np.ascontiguousarray(a) for a in (
+                scene.body_pos, scene.body_quat, scene.body_vel, scene.body_angvel,
+                scene.body_mass.astype(np.float32), scene.body_inv_inertia.astype(np.float32),
+                scene.body_offsets.astype(np.int32), scene.particle_rel)]
+            init = api.SceneInit(*[C.c_void_p(a.ctypes.data) for a in arrays])
+            tid = C.c_int()
+            call("ar_server_add_template", self.handle, C.byref(desc), C.byref(init),
+                 C.byref(tid))
+            self._templates[key] = tid.value
+            self._keep.append(scene)  # the id stays unique while the scene lives
+        return self._templates[key]
+
+    def run(self, requests: list[Request], time_limit: float | None = None,
+            keep_results: bool = False) -> ServerStats:
+        n = len(requests)
+        tids = np.array([self.template(r.scene) for r in requests], np.int32)
+        steps = np.array([r.steps for r in requests], np.int32)
+        arrival = np.array([r.arrival for r in requests], np.float64)
+        latency = np.full(n, -1.0)
+        results = None
+        pinned = []
+        if keep_results:
+            ptrs = []
+            for r in requests:
+                t = torch.empty((4, r.scene.num_bodies, 4), dtype=torch.float32, pin_memory=True)
+                pinned.append(t)
+                ptrs.append(t.data_ptr())
+            results = (C.c_void_p * max(1, n))(*ptrs)
+        st = ServerStatsC()
+        call("ar_server_run", self.handle, n, C.c_void_p(tids.ctypes.data),
+             C.c_void_p(steps.ctypes.data), C.c_void_p(arrival.ctypes.data),
+             C.c_double(-1.0 if time_limit is None else float(time_limit)), results,
+             C.c_void_p(latency.ctypes.data), C.byref(st))
+        done = []
+        for i, r in enumerate(requests):
+            if latency[i] >= 0:
+                r.done = r.arrival + latency[i]
+                done.append(latency[i])
+                if keep_results:
+                    packed = pinned[i].numpy()  # [4, B, 4]: pos, quat, vel, angvel
+                    r.result = {k: packed[j].copy() for j, k in
+                                enumerate(("pos", "quat", "vel", "angvel"))}
+        host = {"admit": st.host_admit_s, "set_scenes": st.host_set_s, "step": st.host_step_s,
+                "retire": st.host_retire_s, "wait": st.host_wait_s}
+        return ServerStats(st.completed, st.offered, st.wall_s, st.scene_steps,
+                           st.particle_steps, np.array(done), st.peak_resident, st.peak_bytes,
+                           st.ticks, host)
+
+    def close(self) -> None:
+        if self.handle:
+            call("ar_server_destroy", self.handle)
+            self.handle = C.c_void_p()
 
 
 def poisson_requests(rate_per_s: float, duration_s: float, make, seed: int = 0) -> list[Request]:

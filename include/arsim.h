@@ -592,6 +592,13 @@ AR_API ar_status ar_scene_create(ar_ctx* ctx, const ar_scene_desc* desc,
                                  const ar_scene_init* init, ar_stream_t stream,
                                  ar_scene** out);
 AR_API ar_status ar_scene_destroy(ar_scene* scene);
+/* A new scene with `proto`'s description and current state, copied on the device in stream
+ * order (one device-to-device copy of the scene's block, no host synchronisation): the server
+ * keeps request templates resident and admits a request by cloning its template.  `proto`
+ * must not change until the copy has run on `stream`.  No counterpart in the reference (its
+ * bodies are built on the host by ParticleSystem::addRigidBody). */
+AR_API ar_status ar_scene_clone_async(const ar_scene* proto, ar_stream_t stream,
+                                      ar_scene** out);
 /* Release a scene's device memory in stream order (cudaFreeAsync on `stream`), without a
  * host or device-wide synchronisation.  Every use of the scene must be ordered before this
  * point of `stream` (e.g. the scene was removed from its batches before the batch's next step
@@ -733,6 +740,48 @@ AR_API ar_status ar_batch_profile(ar_ctx* ctx, ar_batch* batch, int n_steps,
  * to a 16-byte aligned device buffer -- for a batch in member order, one launch. */
 AR_API ar_status ar_batch_model_matrices(ar_batch* batch, float* d_model16, ar_stream_t stream);
 AR_API ar_status ar_scene_model_matrices(ar_scene* scene, float* d_model16, ar_stream_t stream);
+
+/* ---- continuous-batching server (no counterpart in the reference) ---------------------------
+ * A request loop in C++ over the batch API.  A request names a template scene (uploaded once
+ * with ar_server_add_template and kept resident) and a number of steps K, and arrives at a
+ * given time (seconds from the start of ar_server_run, on the host's steady clock).  The loop
+ * runs fixed ticks of tick_steps batch steps on its own stream:
+ *   1. admission in arrival order while the requests' footprints (ar_scene_footprint) fit the
+ *      HBM budget and the batch stays within AR_MAX_BATCH_* and max_batch_particles; an
+ *      admitted request's scene is a clone of its template (ar_scene_clone_async) on an
+ *      admission stream that the compute stream waits for -- no host synchronisation;
+ *   2. one tick: ar_batch_set_scenes_limited (each scene's remaining K as its step budget, so a
+ *      scene is frozen after exactly K steps) when the members changed, then ar_batch_step;
+ *   3. a finished scene's state is copied to the host behind the tick (into the request's
+ *      pinned buffer h_results[i] when given, in the layout of ar_scene_download_state: 16
+ *      floats per body -- else into a scratch buffer) and the request completes
+ *      when the host sees that copy done; the scene leaves the batch at the next member change
+ *      and is freed in stream order (ar_scene_destroy_async).
+ * The host runs at most max_inflight ticks ahead of the device.  Admission stops at
+ * time_limit_s (< 0: no limit); requests not admitted by then are not completed. */
+typedef struct ar_server ar_server;
+typedef struct ar_server_stats {
+  int completed, offered, peak_resident, ticks;
+  double wall_s;
+  long long scene_steps, particle_steps;
+  size_t peak_bytes;
+  double host_admit_s, host_set_s, host_step_s, host_retire_s, host_wait_s;
+} ar_server_stats;
+AR_API ar_status ar_server_create(ar_ctx* ctx, double hbm_budget_bytes, int tick_steps,
+                                  long long max_batch_particles, int max_inflight,
+                                  ar_server** out);
+/* Uploads a template scene (ar_scene_create on the server's admission stream); *id receives
+ * its index for ar_server_run. */
+AR_API ar_status ar_server_add_template(ar_server* server, const ar_scene_desc* desc,
+                                        const ar_scene_init* init, int* id);
+/* Serves n requests (template_id[i], steps[i], arrival_s[i]; arrival order need not be
+ * sorted).  latency_s[i] receives completion - arrival in seconds, or -1 for a request not
+ * completed; h_results may be NULL, and so may any h_results[i]. */
+AR_API ar_status ar_server_run(ar_server* server, int n, const int* template_id,
+                               const int* steps, const double* arrival_s, double time_limit_s,
+                               float* const* h_results, double* latency_s,
+                               ar_server_stats* stats);
+AR_API ar_status ar_server_destroy(ar_server* server);
 
 /* Number of kernel launches one step of this batch issues (for launch accounting). */
 AR_API int ar_batch_launches_per_step(ar_batch* batch);
