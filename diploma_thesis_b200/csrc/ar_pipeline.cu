@@ -768,7 +768,8 @@ struct ar_batch {
   char* sort64_ws = nullptr;
   int bvh_key_bits = kMortonBits;
   // graph
-  cudaGraphExec_t graph = nullptr;
+  cudaGraphExec_t graph = nullptr;   // one step
+  cudaGraphExec_t graph_k = nullptr; // kGraphSteps steps in one graph
   cudaStream_t cap_stream = nullptr;
 };
 
@@ -803,7 +804,9 @@ void free_batch_buffers(ar_batch* B) {
 
 void drop_graph(ar_batch* B) {
   if (B->graph) cudaGraphExecDestroy(B->graph);
+  if (B->graph_k) cudaGraphExecDestroy(B->graph_k);
   B->graph = nullptr;
+  B->graph_k = nullptr;
 }
 
 template <class T>
@@ -1094,6 +1097,37 @@ ar_status profile_steps(ar_batch* B, int n_steps, float* stage_ms, cudaStream_t 
   return s;
 }
 
+constexpr int kGraphSteps = 8;
+
+// Capture `steps` consecutive steps into *exec (once; kept until the member list changes).
+// Capture records without executing; the graph's launches on the stream it is replayed on are
+// ordered after the work already queued there (table uploads, clears).
+ar_status capture_steps(ar_batch* B, int steps, cudaGraphExec_t* exec) {
+  if (*exec) return AR_OK;
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    arh::set_error("cudaStreamBeginCapture failed");
+    return AR_ERR_CUDA;
+  }
+  ar_status es = AR_OK;
+  for (int i = 0; i < steps && es == AR_OK; ++i) es = enqueue_step(B, B->cap_stream);
+  cudaError_t ce = cudaStreamEndCapture(B->cap_stream, &g);
+  if (es != AR_OK || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    arh::set_error("step capture failed (%s)", cudaGetErrorString(ce));
+    return es != AR_OK ? es : AR_ERR_CUDA;
+  }
+  ce = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  if (ce != cudaSuccess) {
+    *exec = nullptr;
+    arh::set_error("cudaGraphInstantiate failed (%s)", cudaGetErrorString(ce));
+    return AR_ERR_CUDA;
+  }
+  return AR_OK;
+}
+
 ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaStream_t st) {
   ar_status s = prepare(B, st);
   if (s != AR_OK) return s;
@@ -1105,36 +1139,23 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
     }
     return AR_OK;
   }
-  if (!B->graph) {
-    if (!B->cap_stream &&
-        cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
-      arh::set_error("capture stream creation failed");
-      return AR_ERR_CUDA;
-    }
-    // capture records without executing; the graph's launches on `st` are ordered after the
-    // work already queued there (table uploads, clears)
-    cudaGraph_t g = nullptr;
-    if (cudaStreamBeginCapture(B->cap_stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-      arh::set_error("cudaStreamBeginCapture failed");
-      return AR_ERR_CUDA;
-    }
-    ar_status es = enqueue_step(B, B->cap_stream);
-    cudaError_t ce = cudaStreamEndCapture(B->cap_stream, &g);
-    if (es != AR_OK || ce != cudaSuccess) {
-      if (g) cudaGraphDestroy(g);
-      cudaGetLastError();
-      arh::set_error("step capture failed (%s)", cudaGetErrorString(ce));
-      return es != AR_OK ? es : AR_ERR_CUDA;
-    }
-    ce = cudaGraphInstantiate(&B->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (ce != cudaSuccess) {
-      B->graph = nullptr;
-      arh::set_error("cudaGraphInstantiate failed (%s)", cudaGetErrorString(ce));
-      return AR_ERR_CUDA;
-    }
+  if (!B->cap_stream &&
+      cudaStreamCreateWithFlags(&B->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    arh::set_error("capture stream creation failed");
+    return AR_ERR_CUDA;
   }
-  for (int i = 0; i < n_steps; ++i) {
+  // runs of kGraphSteps steps replay one graph holding them all: inside a graph the steps'
+  // launches keep their programmatic dependencies, so each step's first kernel overlaps the
+  // previous step's last one, which a graph boundary would not allow
+  const bool many = n_steps >= kGraphSteps;
+  if ((s = capture_steps(B, 1, &B->graph)) != AR_OK) return s;
+  if (many && (s = capture_steps(B, kGraphSteps, &B->graph_k)) != AR_OK) return s;
+  int left = n_steps;
+  for (; many && left >= kGraphSteps; left -= kGraphSteps) {
+    if (cudaGraphLaunch(B->graph_k, st) != cudaSuccess) return arh::check_launch("graph launch");
+    B->host_step += kGraphSteps;
+  }
+  for (; left > 0; --left) {
     if (cudaGraphLaunch(B->graph, st) != cudaSuccess) return arh::check_launch("graph launch");
     ++B->host_step;
   }
