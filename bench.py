@@ -399,10 +399,8 @@ def run_ours(args):
         barrier(world)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        for _ in range(e2e_steps):
-            gs.upload_state(host, stream=stream)
-            gs.step(1, use_graph=True, stream=stream)
-            gs.download_state(host, stream=stream)
+        for _ in range(e2e_steps):  # upload, one graph step, download: one library call
+            gs.step_io(host, 1, host, stream=stream)
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
         barrier(world)

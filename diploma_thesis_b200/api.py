@@ -159,6 +159,16 @@ class GpuScene:
              _np_ptr(state), stream_handle(stream))
         return state
 
+    def step_io(self, state_in: np.ndarray, n: int, state_out: np.ndarray, stream=None) -> None:
+        """Upload the packed state, step n times (graph), copy the packed state back, in one
+        call (ar_scene_step_io); both arrays are [4, B, 4] float32 pinned host arrays and may be
+        the same."""
+        for a in (state_in, state_out):
+            assert a.dtype == np.float32 and a.size == 16 * self.num_bodies
+            assert a.flags.c_contiguous
+        call("ar_scene_step_io", self.ctx.handle, self.handle, _np_ptr(state_in), int(n),
+             _np_ptr(state_out), stream_handle(stream))
+
     def download_into(self, pos, quat, vel, angvel, stream=None) -> None:
         call("ar_scene_download", self.handle, *[_np_ptr(a) if a is not None else None
                                                  for a in (pos, quat, vel, angvel)],

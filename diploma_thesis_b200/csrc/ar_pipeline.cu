@@ -1501,6 +1501,15 @@ ar_status ar_scene_download_state_async(ar_scene* s, float* h_state16, ar_stream
   return arh::check_launch("ar_scene_download_state_async");
 }
 
+ar_status ar_scene_step_io(ar_ctx* ctx, ar_scene* s, const float* h_state_in16, int n_steps,
+                           float* h_state_out16, ar_stream_t stream) {
+  if (!ctx || !s || !h_state_in16 || !h_state_out16 || n_steps < 0) return AR_ERR_INVALID_ARG;
+  ar_status r = ar_scene_upload_state(s, h_state_in16, stream);
+  if (r == AR_OK) r = ar_step(ctx, s, n_steps, 1, stream);
+  if (r == AR_OK) r = ar_scene_download_state(s, h_state_out16, stream);
+  return r;
+}
+
 ar_status ar_scene_download_state(ar_scene* s, float* h_state16, ar_stream_t stream) {
   ar_status r = ar_scene_download_state_async(s, h_state16, stream);
   if (r != AR_OK) return r;

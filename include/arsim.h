@@ -641,6 +641,13 @@ AR_API ar_status ar_scene_upload_state(ar_scene* scene, const float* h_state16,
 AR_API ar_status ar_scene_download_state(ar_scene* scene, float* h_state16, ar_stream_t stream);
 AR_API ar_status ar_scene_download_state_async(ar_scene* scene, float* h_state16,
                                                ar_stream_t stream);
+/* A host round trip in one call: the packed body state is uploaded from h_state_in16, the
+ * scene advances n_steps (CUDA graph), and its packed state is copied to h_state_out16 (both
+ * pinned host memory; they may be the same array); returns once the state is on the host.
+ * The reference's per-frame pattern -- state to the device, step, state back for the renderer
+ * (Particles/updateFunctions.cpp:2903-2930) -- with one entry instead of three. */
+AR_API ar_status ar_scene_step_io(ar_ctx* ctx, ar_scene* scene, const float* h_state_in16,
+                                  int n_steps, float* h_state_out16, ar_stream_t stream);
 /* Device pointers of the scene's resident arrays (for tests / zero-copy consumers). */
 typedef struct ar_scene_view {
   int num_bodies, num_particles;

@@ -229,3 +229,22 @@ def test_packed_state_transfers(ctx):
         assert np.array_equal(x[k], y[k]), k
     a.close()
     b.close()
+
+
+def test_step_io_round_trip(ctx):
+    """ar_scene_step_io (upload, n graph steps, download in one call) gives what the three
+    separate calls give, into the same pinned array it read from."""
+    sc = scenes.small_scene(13, nb_side=3, packed=True, r=1 / 128)
+    a, b = api.GpuScene(ctx, sc), api.GpuScene(ctx, sc)
+    a.step(4, use_graph=False)
+    state = a.download_state()
+    pinned = torch.empty((4, sc.num_bodies, 4), dtype=torch.float32).pin_memory().numpy()
+    pinned[:] = state
+    for _ in range(3):
+        b.step_io(pinned, 2, pinned)      # b: state in, 2 steps, state back, six steps in all
+        a.step(2, use_graph=True)
+    got = a.download_state()
+    assert np.array_equal(pinned, got)
+    a.close()
+    b.close()
+
