@@ -4,7 +4,8 @@ fused step on this GPU.
 
 Buckets are powers of two of the particle count.  For each bucket a representative scene
 (27-particle cubes, config-0 distributions) is stepped under every candidate and timed with
-CUDA events over CUDA-graph replays; the fastest candidate is kept.  Results are cached in a
+CUDA events over CUDA-graph replays by the library's C++ loop (ar_tune_candidates); the
+fastest candidate is kept.  Results are cached in a
 JSON file keyed by GPU name, so a deployment tunes once.
 
 Candidates: grid with cell = f * 2r for f in CELL_FACTORS and cells per axis wrapped so that
@@ -17,6 +18,7 @@ mixed table is stepped as one batch per broad phase (``group``).
 """
 from __future__ import annotations
 
+import ctypes as C
 import json
 import math
 from dataclasses import asdict, dataclass
@@ -26,6 +28,7 @@ import numpy as np
 import torch
 
 from . import api, scenes
+from ._lib import call
 
 CELL_FACTORS = (1.0, 1.25, 1.5)
 GRID_MULTS = (2, 8, 32)
@@ -71,38 +74,41 @@ def apply(scene: scenes.Scene, choice: Choice) -> dict:
             "block_size": choice.block_size}
 
 
-def _time_steps(ctx: api.Context, scene: scenes.Scene, kw: dict, steps: int) -> float:
-    gs = api.GpuScene(ctx, scene, **kw)
-    s = torch.cuda.Stream()
-    with torch.cuda.stream(s):
-        gs.step(3, use_graph=True, stream=s)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(s)
-        gs.step(steps, use_graph=True, stream=s)
-        b.record(s)
-        b.synchronize()
-    gs.close()
-    return a.elapsed_time(b) / steps
+def _init_of(scene: scenes.Scene):
+    """ar_scene_init of a scene (the arrays kept alive by the returned list)."""
+    keep = [np.ascontiguousarray(a) for a in (
+        scene.body_pos, scene.body_quat, scene.body_vel, scene.body_angvel,
+        scene.body_mass.astype(np.float32), scene.body_inv_inertia.astype(np.float32),
+        scene.body_offsets.astype(np.int32), scene.particle_rel)]
+    return api.SceneInit(*[C.c_void_p(a.ctypes.data) for a in keep]), keep
+
+
+def time_candidates(ctx: api.Context, scene: scenes.Scene, choices: list[Choice],
+                    steps: int = 20, warmup: int = 3) -> list[float]:
+    """Milliseconds per graph-replayed step of the scene under each choice, timed by the
+    library's C++ loop (ar_tune_candidates)."""
+    descs = (api.SceneDesc * len(choices))()
+    for i, c in enumerate(choices):
+        kw = apply(scene, c)
+        descs[i] = api.make_desc(scene, api.broadphase_code(kw.get("broadphase", "grid")),
+                                 kw.get("block_size", 0), kw.get("cell_size"),
+                                 kw.get("grid_log2"))
+    init, _keep = _init_of(scene)
+    ms = np.zeros(len(choices), np.float32)
+    call("ar_tune_candidates", ctx.handle, descs, len(choices), C.byref(init), int(warmup),
+         int(steps), C.c_void_p(ms.ctypes.data))
+    return [float(x) for x in ms]
 
 
 def tune_bucket(ctx: api.Context, bucket: int, steps: int = 20, seed: int = 0) -> Choice:
     n = 1 << bucket
     side = float(np.clip((n / 27 * 0.035 ** 3 * 4) ** (1 / 3), 0.5, 2.0))
     scene = scenes.cube_scene(seed + bucket, n // 27 * 27, side)
-    best = None
-    for f in CELL_FACTORS:
-        for m in GRID_MULTS:
-            for bs in BLOCK_SIZES:
-                c = Choice(f, m, bs, 0.0)
-                c.ms_per_step = _time_steps(ctx, scene, apply(scene, c), steps)
-                if best is None or c.ms_per_step < best.ms_per_step:
-                    best = c
-    for bs in BLOCK_SIZES:
-        c = Choice(1.0, 0, bs, 0.0, "bvh")
-        c.ms_per_step = _time_steps(ctx, scene, apply(scene, c), steps)
-        if c.ms_per_step < best.ms_per_step:
-            best = c
-    return best
+    cands = [Choice(f, m, bs, 0.0) for f in CELL_FACTORS for m in GRID_MULTS for bs in BLOCK_SIZES]
+    cands += [Choice(1.0, 0, bs, 0.0, "bvh") for bs in BLOCK_SIZES]
+    for c, ms in zip(cands, time_candidates(ctx, scene, cands, steps)):
+        c.ms_per_step = ms
+    return min(cands, key=lambda c: c.ms_per_step)  # the first of equal times
 
 
 def group(kwargs: list[dict]) -> dict[str, list[int]]:

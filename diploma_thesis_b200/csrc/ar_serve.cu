@@ -1,5 +1,6 @@
-// Continuous-batching server: the request loop of ar_server_run (include/arsim.h), host code
-// over the batch API.  No counterpart in the reference, which steps one scene per frame.
+// Host loops over the C ABI: the continuous-batching server (ar_server_run) and the
+// autotuner's candidate timing (ar_tune_candidates).  No counterpart in the reference, which
+// steps one scene per frame with fixed settings.
 //
 // Per round of the loop: requests whose arrival time has passed join the waiting queue;
 // waiting requests are admitted in arrival order while they fit (HBM budget by
@@ -97,8 +98,9 @@ ar_status ar_server_create(ar_ctx* ctx, double hbm_budget_bytes, int tick_steps,
                          : AR_MAX_BATCH_PARTICLES;
   s->max_inflight = std::max(1, max_inflight);
   ar_status st = ar_batch_create(ctx, &s->batch);
-  if (st == AR_OK && (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-                      cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking) != cudaSuccess)) {
+  if (st == AR_OK &&
+      (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+       cudaStreamCreateWithFlags(&s->adm, cudaStreamNonBlocking) != cudaSuccess)) {
     cudaGetLastError();
     arh::set_error("ar_server_create: stream creation failed");
     st = AR_ERR_CUDA;
@@ -327,6 +329,50 @@ ar_status ar_server_run(ar_server* s, int n, const int* template_id, const int* 
   if (stats) *stats = out;
   if (status != AR_OK) return status;
   return ar_ctx_status(s->ctx, sth);
+}
+
+ar_status ar_tune_candidates(ar_ctx* ctx, const ar_scene_desc* descs, int n_cand,
+                            const ar_scene_init* init, int warmup, int steps, float* ms_per_step) {
+  if (!ctx || !descs || !init || !ms_per_step || n_cand < 0 || warmup < 0 || steps <= 0)
+    return AR_ERR_INVALID_ARG;
+  cudaStream_t st = nullptr;
+  cudaEvent_t a = nullptr, b = nullptr;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+    cudaGetLastError();
+    if (st) cudaStreamDestroy(st);
+    if (a) cudaEventDestroy(a);
+    arh::set_error("ar_tune_candidates: stream or event creation failed");
+    return AR_ERR_CUDA;
+  }
+  const ar_stream_t sh = reinterpret_cast<ar_stream_t>(st);
+  ar_status status = AR_OK;
+  for (int i = 0; i < n_cand && status == AR_OK; ++i) {
+    ar_scene* g = nullptr;
+    status = ar_scene_create(ctx, &descs[i], init, sh, &g);
+    if (status != AR_OK) break;
+    // the same scene under candidate i: warm-up steps (graph capture included), then the timed
+    // graph replays between two events on the stream
+    status = ar_step(ctx, g, warmup, 1, sh);
+    if (status == AR_OK) {
+      cudaEventRecord(a, st);
+      status = ar_step(ctx, g, steps, 1, sh);
+      cudaEventRecord(b, st);
+    }
+    if (status == AR_OK && cudaEventSynchronize(b) == cudaSuccess) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, a, b);
+      ms_per_step[i] = ms / (float)steps;
+      status = ar_ctx_status(ctx, sh);
+    } else if (status == AR_OK) {
+      status = arh::check_launch("ar_tune_candidates");
+    }
+    ar_scene_destroy(g);
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaStreamDestroy(st);
+  return status;
 }
 
 ar_status ar_server_destroy(ar_server* s) {

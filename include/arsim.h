@@ -790,6 +790,15 @@ AR_API ar_status ar_server_run(ar_server* server, int n, const int* template_id,
                                ar_server_stats* stats);
 AR_API ar_status ar_server_destroy(ar_server* server);
 
+/* Autotuner timing loop (no counterpart in the reference): the scene `init` is created under
+ * each of the n_cand descriptions (candidate broad phase, cell size, wrapped grid and collision
+ * block size), stepped `warmup` times (CUDA graph), then `steps` graph-replayed steps are timed
+ * with CUDA events on a stream of its own; ms_per_step[i] receives candidate i's time.  The
+ * caller picks the fastest; every candidate gives the same contacts. */
+AR_API ar_status ar_tune_candidates(ar_ctx* ctx, const ar_scene_desc* descs, int n_cand,
+                                    const ar_scene_init* init, int warmup, int steps,
+                                    float* ms_per_step);
+
 /* Number of kernel launches one step of this batch issues (for launch accounting). */
 AR_API int ar_batch_launches_per_step(ar_batch* batch);
 AR_API int ar_scene_launches_per_step(ar_scene* scene);
