@@ -800,81 +800,14 @@ def run_served(args):
     return 0
 
 
-def run_refgpu(args):
-    """The reference's own GPU step (updateUniformGridDEM: its kernels compiled for sm_100a from
-    the reference's sources, its wrappers with their allocations and synchronisations,
-    oracle/_ref/libref_gpu.so) beside this repository's fused grid step, on the same scene and
-    GPU, stage by stage.  Both start from the scene's initial state; W untimed steps, then K
-    timed steps each (the reference's stages by CUDA events on its legacy stream; ours by the
-    event-bracketed stage profile and by graph replays).  The reference runs REFERENCE
-    semantics (impulses as velocity increments), ours PHYSICAL: same broad phase, contact law
-    and summation order, same particles and cells."""
-    import torch
-    from diploma_thesis_b200 import api
-    from oracle import cpu, ref_gpu
-    if not ref_gpu.available():
-        print(json.dumps({"workload": "refgpu", "unavailable":
-                          "the reference GPU build (oracle/_ref/libref_gpu.so) is not present"}))
-        return 0
-    torch.cuda.set_device(0)
-    scene, desc = make_scene(args.ref_scene)
-    n = scene.num_particles
-    # the reference's step
-    rg = ref_gpu.RefGpuStep(scene, cpu.scene_grid(scene))
-    for _ in range(args.warmup):
-        rg.step()
-    acc = np.zeros(len(ref_gpu.STAGES))
-    host = 0.0
-    for _ in range(args.steps):
-        ms, wall = rg.step()
-        acc += ms
-        host += wall
-    rg.close()
-    ref_stage = acc / args.steps
-    ref_ms = float(ref_stage.sum())
-    # ours, same scene and step window
-    ctx = api.Context(0)
-    gs = api.GpuScene(ctx, scene)
-    stream = torch.cuda.Stream()
-    with torch.cuda.stream(stream):
-        gs.step(args.warmup, use_graph=True, stream=stream)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        stream.synchronize()
-        a.record(stream)
-        gs.step(args.steps, use_graph=True, stream=stream)
-        b.record(stream)
-        b.synchronize()
-        ours_ms = a.elapsed_time(b) / args.steps
-        ours_stage = gs.profile(min(args.steps, 50), stream=stream)
-    ctx.check(stream)
-    gs.close()
-    ctx.close()
-    line = {"metric": "ms per step", "workload": "refgpu",
-            "config": {"scene": desc, "particles": n, "steps": args.steps,
-                       "warmup": args.warmup},
-            "reference_gpu": {"ms_per_step": ref_ms, "host_ms_per_step": host / args.steps,
-                              "mparticle_steps_per_s": n / ref_ms / 1e3,
-                              "stages_ms": dict(zip(ref_gpu.STAGES, ref_stage.tolist())),
-                              "build": "the reference's CUDA sources for sm_100a, its wrappers",
-                              "semantics": "REFERENCE"},
-            "ours": {"ms_per_step": ours_ms, "mparticle_steps_per_s": n / ours_ms / 1e3,
-                     "stages_ms": dict(zip(STAGES, [float(x) for x in ours_stage])),
-                     "semantics": "PHYSICAL"},
-            "speedup": ref_ms / ours_ms}
-    print(json.dumps(line))
-    return 0
-
-
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh", "sis",
-                                           "refgpu"], default="pile")
-    ap.add_argument("--ref-scene", choices=["pile", "plain"], default="pile",
-                    help="refgpu: the scene both steps run")
+    ap.add_argument("--workload", choices=["pile", "plain", "batched", "served", "lbvh", "sis"],
+                    default="pile")
     ap.add_argument("--lbvh-sizes", default="", help="lbvh: comma-separated point counts")
     ap.add_argument("--lbvh-reps", type=int, default=10, help="lbvh: timed repetitions")
     ap.add_argument("--broadphase", choices=["grid", "bvh"], default="grid",
@@ -904,8 +837,6 @@ def main(argv=None):
         return run_lbvh(args)
     if args.workload == "sis":
         return run_sis(args)
-    if args.workload == "refgpu":
-        return run_refgpu(args)
     return run_ours(args)
 
 

@@ -1,6 +1,6 @@
 """The reference's own GPU step (oracle/_ref/libref_gpu.so, built from the reference's CUDA
 sources), checked against the reference's CPU build on the same scene, so that the timings
-bench.py reports for it (``--workload refgpu``) are timings of the reference's real step.
+oracle/ref_gpu_bench.py reports for it are timings of the reference's real step.
 
 Both run REFERENCE semantics from the same state for three steps on a packed scene with
 contacts.  The GPU build sorts with CUB and sums the per-body impulses as prefix-sum
