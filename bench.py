@@ -60,17 +60,21 @@ def sort_passes(bits: int) -> int:
 
 def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int,
                 cells: int = 0) -> dict[str, float]:
-    tiles = (n + 8191) // 8192
+    """Algorithmic bytes of one grid step that re-sorts from the previous order (every step
+    but the first after a change of the member list).  The movers' own bytes (about 1 % of the
+    particles, 8-16 bytes each per kernel) are left out."""
+    tiles = (n + 2047) // 2048
     return {
-        # sort histogram / look-back head; one 255th of the 8-byte cell table
-        "clear": 4 * 512 * 8 + passes * 4 * 512 * tiles + 8 * cells // 255,
+        # re-sort counters and bucket counts; one 255th of the 8-byte cell table
+        "clear": 4 * (4 + 2 * 4096) + 8 * cells // 255,
         # rel in, key out; body pose (32) per body
         "keys": n * (16 + 4) + nb * 32,
-        # first pass reads the key only; every pass writes key + index; later passes read both
-        "sort": n * (4 + 8) + (passes - 1) * n * 16 + passes * 4 * 512 * tiles,
-        # sorted key + index and rel in, sorted position + velocity out; body state per body;
-        # one 8-byte cell entry per occupied cell
-        "scatter": n * (8 + 16 + 32) + nb * BODY_STATE + occupied_cells * 8,
+        # movers: previous keys + indices in, new key gathered, mover bits out; placement:
+        # previous keys + indices and mover bits in, keys + indices out; tile counts/headers
+        "sort": n * (8 + 4 + 0.125) + n * (8 + 0.125 + 8) + tiles * 40,
+        # sorted key + index and rel in, sorted position + velocity and the order kept for the
+        # next step out; body state per body; one 8-byte cell entry per occupied cell
+        "scatter": n * (8 + 16 + 32 + 8) + nb * BODY_STATE + occupied_cells * 8,
         # own key, index, position, velocity in; force out
         "collide": n * (4 + 4 + 32 + 16),
         # force + rel in; body state

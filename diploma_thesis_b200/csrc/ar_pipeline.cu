@@ -1,14 +1,17 @@
 // Fused PHYSICAL-mode step over a table of resident scenes.
 //
 // Per step (one launch per stage, whatever the number of scenes):
-//   K0       clear the sort's histogram / look-back head and one 255th of the cell table
-//            (see cell_epoch)
+//   K0       clear the sort's counters and one 255th of the cell table (see cell_epoch)
 //   K1       re-pose + hash: key = scene cell base + wrapped cell of the particle's world
-//            position; the sort histogram is accumulated on the fly
-//   sort     onesweep passes over the global keys (values = global particle index)
+//            position
+//   sort     the order by (key, global particle index): re-sorted from the last step's order
+//            (ar_resort.cuh: particles whose key changed found, bucketed and sorted, every
+//            particle placed); the first
+//            step after a change of the member list radix-sorts instead (onesweep passes,
+//            histogram accumulated in K1)
 //   K3       scatter + cell table: sorted position (w = global body id) and velocity,
 //            recomputed from the body state; first slot, count, step epoch and body tag of
-//            every occupied cell
+//            every occupied cell; the order kept for the next step
 //   K4       DEM gather over the 27 neighbour cells + box walls -> per-particle force at the
 //            particle's original index (no atomics)
 //   K5       one warp per body: fixed-order sum of F and r x F, then integration
@@ -31,6 +34,7 @@
 #include "ar_dem.cuh"
 #include "ar_lbvh.cuh"
 #include "ar_pipeline.cuh"
+#include "ar_resort.cuh"
 #include "ar_sort.cuh"
 
 using ar_pipe::SceneDev;
@@ -93,8 +97,9 @@ __global__ void __launch_bounds__(256) scene_ids_kernel(const int* __restrict__ 
 }
 
 // ---- K0: clears ------------------------------------------------------------------------------
-// Zeroes the sort's histogram / look-back head and the cell-table slice of the step about to
-// run (its number is *d_step + 1; K1 increments the counter).
+// Zeroes the head of the sort about to run (the radix sort's histogram / look-back counters, or
+// the re-sort's counters) and the cell-table slice of the step about to run (its number is
+// *d_step + 1; K1 increments the counter).
 __global__ void __launch_bounds__(256) step_clear_kernel(uint4* __restrict__ head, long head16,
                                                          uint2* __restrict__ cells,
                                                          unsigned long long num_cells,
@@ -109,12 +114,13 @@ __global__ void __launch_bounds__(256) step_clear_kernel(uint4* __restrict__ hea
   for (unsigned long long i = lo + t; i < hi; i += stride) cells[i] = make_uint2(0u, 0u);
 }
 
-// ---- K1: re-pose + cell keys + sort histogram ---------------------------------------------
+// ---- K1: re-pose + cell keys (+ sort histogram) ---------------------------------------------
 // Each thread takes kKeysBatch particles per round (stride apart, so each load is coalesced)
 // and issues the loads of all of them before using any, which keeps several dependent
-// gathers (scene -> offset -> body) in flight per thread.
+// gathers (scene -> offset -> body) in flight per thread.  kHist: the radix sort's histogram
+// is accumulated (a step that re-sorts needs none).
 constexpr int kKeysBatch = 2;
-template <bool kOne>
+template <bool kOne, bool kHist>
 __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
     const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table,
     const int* __restrict__ pscene, int nt,
@@ -123,9 +129,11 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
   ar::pdl_wait();
   __shared__ uint32_t s_hist[ar_sort::kMaxPasses][ar_sort::kMaxRadix];
   if (blockIdx.x == 0 && threadIdx.x == 0) *d_step += 1;  // this step's number
-  for (int i = threadIdx.x; i < plan.passes * ar_sort::kMaxRadix; i += blockDim.x)
-    (&s_hist[0][0])[i] = 0;
-  __syncthreads();
+  if (kHist) {
+    for (int i = threadIdx.x; i < plan.passes * ar_sort::kMaxRadix; i += blockDim.x)
+      (&s_hist[0][0])[i] = 0;
+    __syncthreads();
+  }
   const int stride = gridDim.x * blockDim.x;
   for (int g0 = blockIdx.x * blockDim.x + threadIdx.x; g0 < nt; g0 += stride * kKeysBatch) {
     int sc[kKeysBatch];
@@ -162,12 +170,14 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
         const float3 p = ar::add(ar::xyz(c[u]), r);
         const uint32_t key = ar_pipe::cell_key(S, ar_pipe::cell_of(S, p));
         keys[g] = key;
-        ar_sort::hist_count_warp(s_hist, key, plan);
+        if (kHist) ar_sort::hist_count_warp(s_hist, key, plan);
       }
     }
   }
-  __syncthreads();
-  ar_sort::hist_flush(s_hist, ws_hist, plan.passes);
+  if (kHist) {
+    __syncthreads();
+    ar_sort::hist_flush(s_hist, ws_hist, plan.passes);
+  }
 }
 
 // ---- K3: scatter + cell table -------------------------------------------------------------
@@ -177,7 +187,8 @@ __global__ void __launch_bounds__(kK1Threads) grid_keys_kernel(
 // the gathers.)  Cell entry = {first sorted slot, count | epoch | body tag}; the tag names the
 // body when every occupant belongs to one body, so that a particle skips a neighbour cell of
 // its own body without loading its occupants (they could only be rejected).  The thread at a
-// cell's first slot writes the whole entry.
+// cell's first slot writes the whole entry.  The sorted keys and indices are also copied to
+// prev_keys / prev_vals: the order the next step's re-sort starts from.
 // kScatterBatch sorted slots per thread and round, loads issued before use (as in K1).
 constexpr int kScatterBatch = 1;
 template <bool kOne>
@@ -186,6 +197,7 @@ __global__ void __launch_bounds__(256) scatter_kernel(
     const int* __restrict__ pscene, int nt,
     const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
     uint2* __restrict__ cells, float4* __restrict__ spos, float4* __restrict__ svel,
+    uint32_t* __restrict__ prev_keys, uint32_t* __restrict__ prev_vals,
     const long long* __restrict__ d_step) {
   ar::pdl_wait();
   const uint32_t epoch = cell_epoch(*d_step) << kEpochShift;
@@ -203,6 +215,8 @@ __global__ void __launch_bounds__(256) scatter_kernel(
         key[u] = __ldg(skeys + k);
         g[u] = (int)__ldg(svals + k);
         first[u] = k == 0 || key[u] != __ldg(skeys + k - 1);
+        prev_keys[k] = key[u];
+        prev_vals[k] = (uint32_t)g[u];
       }
     }
 #pragma unroll
@@ -738,6 +752,12 @@ struct ar_batch {
   float4 *spos = nullptr, *svel = nullptr, *pforce = nullptr;
   uint2* cells = nullptr;  // {first slot, count | epoch | body tag} per cell
   char* sort_ws = nullptr;
+  // re-sort from the previous step's order (grid broad phase): that order, and the workspace
+  uint32_t *pkeys = nullptr, *pvals = nullptr;
+  uint32_t *rs_head = nullptr, *rs_bstart = nullptr;
+  uint2 *rs_movers = nullptr, *rs_grouped = nullptr;
+  uint4* rs_thead = nullptr;
+  bool order_valid = false;  // pkeys / pvals hold the last step's order of this particle set
   SceneDev* d_table = nullptr;
   SceneDev one{};  // the scene of a one-scene batch (passed to the kernels as a parameter)
   int *d_poff = nullptr, *d_boff = nullptr;
@@ -779,6 +799,12 @@ void free_batch_buffers(ar_batch* B) {
   cudaFree(B->keys); cudaFree(B->skeys); cudaFree(B->svals);
   cudaFree(B->spos); cudaFree(B->svel); cudaFree(B->pforce);
   cudaFree(B->cells); cudaFree(B->sort_ws);
+  cudaFree(B->pkeys); cudaFree(B->pvals); cudaFree(B->rs_head);
+  cudaFree(B->rs_bstart); cudaFree(B->rs_movers); cudaFree(B->rs_grouped); cudaFree(B->rs_thead);
+  B->pkeys = B->pvals = B->rs_head = B->rs_bstart = nullptr;
+  B->rs_movers = B->rs_grouped = nullptr;
+  B->rs_thead = nullptr;
+  B->order_valid = false;
   cudaFree(B->d_table); cudaFree(B->d_poff); cudaFree(B->d_boff);
   cudaFree(B->d_pscene); cudaFree(B->d_bscene);
   B->d_pscene = B->d_bscene = nullptr;
@@ -827,6 +853,7 @@ uint64_t scene_cells(const ar_scene* s) {
 ar_status prepare(ar_batch* B, cudaStream_t st) {
   if (!B->table_dirty) return AR_OK;
   drop_graph(B);
+  B->order_valid = false;  // the particle set may differ: the next step sorts from scratch
   long nt = 0, bt = 0;
   uint64_t cells = 0;
   std::vector<SceneDev> tab;
@@ -892,7 +919,12 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
               alloc(&B->spos, cn) && alloc(&B->svel, cn) && alloc(&B->pforce, cn) &&
               alloc(&B->cells, cc) && alloc(&B->sort_ws, csort) && alloc(&B->d_table, cs) &&
               alloc(&B->d_poff, cs + 1) && alloc(&B->d_boff, cs + 1) &&
-              alloc(&B->d_pscene, cn) && alloc(&B->d_bscene, cb);
+              alloc(&B->d_pscene, cn) && alloc(&B->d_bscene, cb) && alloc(&B->pkeys, cn) &&
+              alloc(&B->pvals, cn) &&
+              alloc(&B->rs_head, ar_resort::region_words(cn)) &&
+              alloc(&B->rs_thead, 2 * ar_resort::tiles_for(cn) + 2) &&
+              alloc(&B->rs_bstart, (1 << ar_resort::kBucketLog2) + 1) &&
+              alloc(&B->rs_movers, cn) && alloc(&B->rs_grouped, cn);
     if (!ok) {
       free_batch_buffers(B);
       arh::set_error("batch workspace allocation failed (%ld particles, %llu cells)", nt,
@@ -961,6 +993,17 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
     const long m = std::max(nt, bt);
     scene_ids_kernel<<<std::min(arh::grid_for(m, 256), 4096u), 256, 0, st>>>(
         B->d_poff, B->d_boff, (int)ns, (int)nt, (int)bt, B->d_pscene, B->d_bscene);
+  }
+  {
+    // the re-sort's tile kernels keep their tiles in shared memory: ask for the full carveout
+    // so that eight blocks fit on an SM
+    static bool carveout_set = false;
+    if (!carveout_set) {
+      cudaFuncSetAttribute(ar_resort::place_kernel,
+          cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+      cudaGetLastError();
+      carveout_set = true;
+    }
   }
   B->one = tab.empty() ? SceneDev{} : tab[0];
   B->nt = nt;
@@ -1045,20 +1088,59 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     mark(6);
     return arh::check_launch("step (BVH)");  // (AR_LAUNCH_ONE is undefined after the grid path)
   }
-  arh::launch_pdl(step_clear_kernel, dim3(ctx->num_sms * 2), dim3(256), 0, st, (uint4*)B->sort_ws,
-      (long)(ar_sort::clear_bytes(nt, B->plan.passes) / 16), B->cells, B->cap_cells, B->d_step);
+  // With the last step's order of this particle set at hand, the keys are re-sorted from it
+  // (ar_resort); otherwise (first step after a change of the member list) they are radix-sorted
+  // from scratch, with the histogram accumulated in K1.
+  const bool resort = B->order_valid;
+  ar_resort::Work rw{};
+  if (resort) {
+    rw.head = B->rs_head;
+    rw.tcount = B->rs_head + ar_resort::tcount_offset();
+    rw.bits = B->rs_head + ar_resort::bits_offset(B->cap_n);
+    rw.thead = B->rs_thead;
+    rw.bstart = B->rs_bstart;
+    rw.local = B->rs_movers;   // the tiles' movers are dead once grouped by bucket,
+    rw.movers = B->rs_movers;  // before the sorted movers are written
+    rw.grouped = B->rs_grouped;
+    const int nb_log2 = std::min(ar_resort::kBucketLog2, B->key_bits);
+    rw.nb = 1 << nb_log2;
+    rw.bshift = B->key_bits - nb_log2;
+  }
+  const long head16 = resort ? (long)(ar_resort::cleared_words() / 4)
+                             : (long)(ar_sort::clear_bytes(nt, B->plan.passes) / 16);
+  arh::launch_pdl(step_clear_kernel, dim3(ctx->num_sms * 2), dim3(256), 0, st,
+      resort ? (uint4*)B->rs_head : (uint4*)B->sort_ws, head16, B->cells, B->cap_cells, B->d_step);
   mark(1);
-  AR_LAUNCH_ONE(grid_keys_kernel,
-      dim3(std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4)), dim3(kK1Threads),
-      B->d_table, B->d_pscene, nt, B->keys, (uint32_t*)B->sort_ws, B->plan, B->d_step);
+  {
+    const dim3 gk(std::min(arh::grid_for(nt, kK1Threads), (unsigned)ctx->num_sms * 4));
+    auto* k1 = one ? (resort ? grid_keys_kernel<true, false> : grid_keys_kernel<true, true>)
+                   : (resort ? grid_keys_kernel<false, false> : grid_keys_kernel<false, true>);
+    arh::launch_pdl(k1, gk, dim3(kK1Threads), 0, st, B->one, B->d_table, B->d_pscene, nt, B->keys,
+        (uint32_t*)B->sort_ws, B->plan, B->d_step);
+  }
   mark(2);
-  // cell keys in particle order: a warp's keys share few digits, so match.any ranking
-  ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0, B->key_bits,
-                                  st, B->sort_ws, B->cap_sort, true, true);
-  if (s != AR_OK) return s;
+  if (resort) {
+    const unsigned tiles = (unsigned)ar_resort::tiles_for(nt);
+    const unsigned wpb = ar_resort::kWarps;  // warps per block: one per tile / bucket
+    arh::launch_pdl(ar_resort::leavers_kernel, dim3(tiles), dim3(ar_resort::kThreads), 0, st,
+        (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals, (const uint32_t*)B->keys, nt, rw);
+    arh::launch_pdl(ar_resort::bucket_kernel, dim3((tiles + wpb - 1) / wpb),
+        dim3(ar_resort::kThreads), 0, st, (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals,
+        nt, (int)tiles, rw);
+    arh::launch_pdl(ar_resort::bucket_sort_kernel, dim3((rw.nb + wpb - 1) / wpb),
+        dim3(ar_resort::kThreads), 0, st, rw);
+    arh::launch_pdl(ar_resort::place_kernel, dim3(tiles), dim3(ar_resort::kThreads), 0, st,
+        (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals, nt, rw, B->skeys, B->svals,
+        ctx->d_err);
+  } else {
+    // cell keys in particle order: a warp's keys share few digits, so match.any ranking
+    ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0,
+                                    B->key_bits, st, B->sort_ws, B->cap_sort, true, true);
+    if (s != AR_OK) return s;
+  }
   mark(3);
   AR_LAUNCH_ONE(scatter_kernel, dim3(gp), dim3(256), B->d_table, B->d_pscene, nt, B->skeys,
-      B->svals, B->cells, B->spos, B->svel, B->d_step);
+      B->svals, B->cells, B->spos, B->svel, B->pkeys, B->pvals, B->d_step);
   mark(4);
   AR_LAUNCH_ONE(collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), B->d_table, nt,
       B->skeys, B->svals, B->cells, B->spos, B->svel, B->pforce, B->d_step);
@@ -1069,6 +1151,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
       B->d_bscene, bt, B->d_step, ctx->d_err);
   mark(6);
 #undef AR_LAUNCH_ONE
+  B->order_valid = true;  // the scatter leaves this step's order in pkeys / pvals
   return arh::check_launch("step");
 }
 
@@ -1132,6 +1215,13 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
   ar_status s = prepare(B, st);
   if (s != AR_OK) return s;
   if (B->nt == 0 || n_steps <= 0) return AR_OK;
+  if (B->broadphase == AR_BROADPHASE_GRID && !B->order_valid) {
+    // the first step after a change of the member list sorts from scratch, outside the graphs
+    // (which hold re-sorting steps)
+    if ((s = enqueue_step(B, st)) != AR_OK) return s;
+    ++B->host_step;
+    if (--n_steps == 0) return AR_OK;
+  }
   if (!use_graph) {
     for (int i = 0; i < n_steps; ++i) {
       if ((s = enqueue_step(B, st)) != AR_OK) return s;
@@ -1642,8 +1732,11 @@ int ar_batch_launches_per_step(ar_batch* B) {
   // memset, keys, sort, 4 tree kernels, collide, body sums, integration
   if (B->broadphase == AR_BROADPHASE_BVH)
     return 1 + 1 + ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 1 + 2;
-  return 1 /*memset*/ + 1 /*keys*/ + ar_sort::launches(0, B->key_bits, true) + 1 /*scatter*/ +
-         1 /*collide*/ + 2 /*body sums, integration*/;
+  // a step that re-sorts from the previous order (every step but the first after a change of
+  // the member list): clear, keys, four re-sort kernels, scatter, collide, body sums,
+  // integration
+  return 1 /*clear*/ + 1 /*keys*/ + 4 /*re-sort*/ + 1 /*scatter*/ + 1 /*collide*/ +
+         2 /*body sums, integration*/;
 }
 
 int ar_scene_launches_per_step(ar_scene* s) {
