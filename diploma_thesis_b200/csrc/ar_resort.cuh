@@ -218,6 +218,8 @@ __global__ void __launch_bounds__(kThreads, 7) leavers_kernel(
 // ---- movers into their buckets, tile headers -----------------------------------------------
 // One warp per tile.  Every block scans the bucket counts into shared memory and sums the tile
 // counts before its tiles (and all of them, m); block 0 also stores the bucket starts and m.
+// The loads that do not need the scans (the tile's first 32 movers, its first and last old
+// keys, the last stayer before it) are issued before them.
 __global__ void __launch_bounds__(kThreads) bucket_kernel(const uint32_t* __restrict__ pk,
                                                           const uint32_t* __restrict__ pv,
                                                           int n, int tiles, Work w) {
@@ -227,11 +229,41 @@ __global__ void __launch_bounds__(kThreads) bucket_kernel(const uint32_t* __rest
   __shared__ uint32_t s_tc[kWarps];  // movers of the block's tiles
   const int lane = ar::lane_id(), warp = threadIdx.x >> 5;
   const int t0 = blockIdx.x * kWarps;
+  const int t = t0 + warp;
+  const bool live = t < tiles;
+  const long base = (long)t * kTile, end = min((long)n, base + kTile);
+  const uint2* __restrict__ src = w.local + (size_t)t * kTile;
+  // issued early: the first 32 movers of the tile (slots of the tile, always in bounds), the
+  // tile's first and last old keys, the last stayer before it
+  uint2 e0 = make_uint2(0u, 0u);
+  uint32_t kfirst = 0, klast = 0;
+  uint2 prev = make_uint2(0u, 0u);
+  bool has_prev = false;
+  if (live) {
+    e0 = src[lane];
+    if (lane == 0) {
+      kfirst = __ldg(pk + base);
+      klast = __ldg(pk + end - 1);
+    } else if (lane == 1 && t > 0) {
+      long q = t - 1;
+      while (q > 0 && __ldcg(w.tcount + q) == (uint32_t)kTile) --q;  // tiles of movers only
+      for (long wi = (q + 1) * (kTile / 32) - 1; wi >= q * (kTile / 32); --wi) {
+        const uint32_t stay = ~__ldcg(w.bits + wi);  // earlier tiles are full
+        if (stay) {
+          const long j = wi * 32 + 31 - __clz(stay);
+          prev = make_uint2(__ldg(pk + j), __ldg(pv + j));
+          has_prev = true;
+          break;
+        }
+      }
+    }
+  }
   uint32_t before = 0, total = 0;
   for (int i = threadIdx.x; i < tiles; i += kThreads) {
     const uint32_t c = __ldcg(w.tcount + i);
     total += c;
     before += i < t0 ? c : 0u;
+    if (i >= t0 && i < t0 + kWarps) s_tc[i - t0] = c;
   }
   block_scan(w.bcount(), s_bstart, w.nb);
 #pragma unroll
@@ -255,40 +287,25 @@ __global__ void __launch_bounds__(kThreads) bucket_kernel(const uint32_t* __rest
     for (int i = threadIdx.x; i <= w.nb; i += kThreads) w.bstart[i] = s_bstart[i];
     if (threadIdx.x == 0) w.ctr()[3] = m;
   }
-  const int t = t0 + warp;
-  const uint32_t cnt = t < tiles ? __ldcg(w.tcount + t) : 0u;
-  if (lane == 0) s_tc[warp] = cnt;
-  __syncthreads();
-  if (t >= tiles) return;
+  if (!live) return;
+  const uint32_t cnt = s_tc[warp];
   uint32_t lead = before;  // movers before tile t
   for (int q = 0; q < warp; ++q) lead += s_tc[q];
-  const uint2* __restrict__ src = w.local + (size_t)t * kTile;
   for (uint32_t i = lane; i < cnt; i += 32) {
-    const uint2 e = src[i];
+    const uint2 e = i < 32 ? e0 : src[i];
     const uint32_t b = e.x >> w.bshift;
     const uint32_t slot = atomicAdd(w.bfill() + b, 1u);
     w.grouped[s_bstart[b] + slot] = e;
   }
+  has_prev = __shfl_sync(0xffffffffu, has_prev, 1);
+  prev.x = __shfl_sync(0xffffffffu, prev.x, 1);
+  prev.y = __shfl_sync(0xffffffffu, prev.y, 1);
   if (lane == 0) {
-    const long base = (long)t * kTile, end = min((long)n, base + kTile);
     const uint32_t len = (uint32_t)(end - base);
-    const uint32_t w0 = s_bstart[__ldg(pk + base) >> w.bshift];
-    const uint32_t w1 = s_bstart[(__ldg(pk + end - 1) >> w.bshift) + 1];
+    const uint32_t w0 = s_bstart[kfirst >> w.bshift];
+    const uint32_t w1 = s_bstart[(klast >> w.bshift) + 1];
     uint32_t flags = 0;
-    uint2 prev = make_uint2(0u, 0u);
-    if ((uint32_t)base > lead) {  // some stayer lies before this tile: find the last one
-      long q = t - 1;
-      while (q > 0 && __ldcg(w.tcount + q) == (uint32_t)kTile) --q;  // tiles of movers only
-      for (long wi = (q + 1) * (kTile / 32) - 1; wi >= q * (kTile / 32); --wi) {
-        const uint32_t stay = ~__ldcg(w.bits + wi);  // earlier tiles are full
-        if (stay) {
-          const long j = wi * 32 + 31 - __clz(stay);
-          prev = make_uint2(__ldg(pk + j), __ldg(pv + j));
-          flags |= kHasPrev;
-          break;
-        }
-      }
-    }
+    if ((uint32_t)base > lead && has_prev) flags |= kHasPrev;  // some stayer lies before
     const uint32_t stay_here = len - cnt;
     const uint32_t stay_after = (uint32_t)(n - end) - (m - (lead + cnt));
     if (stay_after == 0 && stay_here > 0) flags |= kTailOwner;
@@ -299,9 +316,11 @@ __global__ void __launch_bounds__(kThreads) bucket_kernel(const uint32_t* __rest
 }
 
 // ---- each bucket sorted by (key, index) into w.movers --------------------------------------
-// One warp per bucket; rank = number of the bucket's movers with a smaller (key, index) (they
-// are distinct).  Up to 32 movers: one per lane, compared through shuffles; up to kWarpStage:
-// staged in the warp's shared memory and compared there; beyond: compared in global memory.
+// One warp per bucket; a mover's rank is the number of the bucket's movers with a smaller (key,
+// index) (they are distinct).  Up to 32 movers: one per lane, compared through shuffles; up to
+// kWarpStage: staged in the warp's shared memory and compared there; beyond: compared in
+// global memory.  (Sorting chunks of 32 and merging them by binary searches was measured
+// slower for the buckets of the 2M-particle pile, at most ~130 movers.)
 constexpr int kWarpStage = 256;
 __global__ void __launch_bounds__(kThreads) bucket_sort_kernel(Work w) {
   ar::pdl_wait();
@@ -381,7 +400,6 @@ __global__ void __launch_bounds__(kThreads, 7) place_kernel(
   auto mover = [&](uint32_t i) {
     return i - w0 < wn ? s_win[i - w0] : composite(w.movers[i]);
   };
-  auto is_mover = [&](int off) { return (s_bits[off >> 5] >> (off & 31)) & 1u; };
   for (uint32_t i = w0 + threadIdx.x; i < w1; i += kThreads) {
     const unsigned long long c = mover(i);
     int lo = 0, hi = len;  // first position whose old entry is above the mover
@@ -389,22 +407,31 @@ __global__ void __launch_bounds__(kThreads, 7) place_kernel(
       const int mid = (lo + hi) >> 1;
       if (composite(s_k[mid], s_v[mid]) < c) lo = mid + 1; else hi = mid;
     }
-    while (lo < len && is_mover(lo)) ++lo;  // on to a stayer
+    // on to the first stayer at or after lo: a clear bit of the tile's mover bits (a body
+    // whose particles are consecutive in the old order moves as one run of up to 64)
+    if (lo < len) {
+      int wi = lo >> 5;
+      uint32_t stay = ~s_bits[wi] & (0xffffffffu << (lo & 31));
+      while (!stay && ++wi < kTile / 32) stay = ~s_bits[wi];
+      lo = stay ? (wi << 5) + __ffs(stay) - 1 : len;
+    }
     if (lo < len) atomicAdd(s_cnt + lo, 1u);
   }
   __syncthreads();
-  // per (row, warp): mover count and the in-warp inclusive sum of the counts (kept in s_cnt's
-  // place as count | inclusive sum << 16 would overflow; the count is re-derived instead)
+  // per (row, warp): mover count, and the in-warp inclusive sum of the counts in s_cnt's place
+  // (the count itself is re-derived from the neighbour's sum)
 #pragma unroll
   for (int u = 0; u < kRows; ++u) {
     const int off = u * kThreads + threadIdx.x;
     uint32_t x = s_cnt[off];
+    if (__any_sync(0xffffffffu, x != 0u)) {  // most rows have no mover counted
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      s_cnt[off] = x;  // in-warp inclusive sum
     }
-    s_cnt[off] = x;  // in-warp inclusive sum
     if (lane == 31) {
       s_lv[u * kWarps + warp] = __popc(s_bits[off >> 5]);
       s_cs[u * kWarps + warp] = x;
