@@ -492,10 +492,15 @@ __global__ void __launch_bounds__(256) bvh_leaves_kernel(
     const uint32_t* __restrict__ svals, const int32_t* __restrict__ left,
     const int32_t* __restrict__ parent, float4* __restrict__ spos, float4* __restrict__ svel,
     WideNode* __restrict__ nodes, uint8_t* __restrict__ is_leaf, int32_t* __restrict__ min_r,
-    int32_t* __restrict__ max_r, int* __restrict__ counters) {
+    int32_t* __restrict__ max_r, int* __restrict__ counters, const uint32_t* __restrict__ skeys32,
+    uint32_t* __restrict__ prev_keys, uint32_t* __restrict__ prev_vals) {
   ar::pdl_wait();
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nt; k += gridDim.x * blockDim.x) {
     const int g = (int)__ldg(svals + k);
+    if (prev_keys) {  // 32-bit keys: the order the next step's re-sort starts from
+      prev_keys[k] = __ldg(skeys32 + k);
+      prev_vals[k] = (uint32_t)g;
+    }
     const int sc = kOne ? 0 : __ldg(pscene + g);
     const SceneDev& S = scene_at<kOne>(one, table, sc);
     const float4 r4 = __ldg(S.rel + (g - S.poff));
@@ -1015,6 +1020,41 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
   return arh::check_launch("batch prepare");
 }
 
+// The re-sort's workspace for keys of key_bits bits (buckets = the key's top bits).
+ar_resort::Work resort_work(ar_batch* B, int key_bits) {
+  ar_resort::Work rw{};
+  rw.head = B->rs_head;
+  rw.tcount = B->rs_head + ar_resort::tcount_offset();
+  rw.bits = B->rs_head + ar_resort::bits_offset(B->cap_n);
+  rw.thead = B->rs_thead;
+  rw.bstart = B->rs_bstart;
+  rw.local = B->rs_movers;   // the tiles' movers are dead once grouped by bucket,
+  rw.movers = B->rs_movers;  // before the sorted movers are written
+  rw.grouped = B->rs_grouped;
+  const int nb_log2 = std::min(ar_resort::kBucketLog2, key_bits);
+  rw.nb = 1 << nb_log2;
+  rw.bshift = key_bits - nb_log2;
+  return rw;
+}
+
+// The four re-sort kernels: B->keys (this step's keys in particle order) from the previous
+// order (pkeys, pvals) into skeys / svals.
+void launch_resort(ar_ctx* ctx, ar_batch* B, const ar_resort::Work& rw, cudaStream_t st) {
+  const int nt = (int)B->nt;
+  const unsigned tiles = (unsigned)ar_resort::tiles_for(nt);
+  const unsigned wpb = ar_resort::kWarps;  // warps per block: one per tile / bucket
+  arh::launch_pdl(ar_resort::leavers_kernel, dim3(tiles), dim3(ar_resort::kThreads), 0, st,
+      (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals, (const uint32_t*)B->keys, nt, rw);
+  arh::launch_pdl(ar_resort::bucket_kernel, dim3((tiles + wpb - 1) / wpb),
+      dim3(ar_resort::kThreads), 0, st, (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals,
+      nt, (int)tiles, rw);
+  arh::launch_pdl(ar_resort::bucket_sort_kernel, dim3((rw.nb + wpb - 1) / wpb),
+      dim3(ar_resort::kThreads), 0, st, rw);
+  arh::launch_pdl(ar_resort::place_kernel, dim3(tiles), dim3(ar_resort::kThreads), 0, st,
+      (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals, nt, rw, B->skeys, B->svals,
+      ctx->d_err);
+}
+
 // Stage boundaries for ar_step_profile: events[0] before the step, events[i] after stage i.
 // Grid: clear (sort histogram head, cell-table slice) | cell keys + histogram | sort |
 // scatter + cell table | collide | body sums + integration.  BVH: clear (refit counters) | Morton keys
@@ -1056,11 +1096,20 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
       arh::launch_pdl(morton_key_kernel<uint64_t, false>, dim3(gp), dim3(256), 0, st, B->one,
           B->d_table, B->d_pscene, ns, nt, B->keys64, B->d_step);
     mark(2);
-    ar_status s = k32 ? ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0,
-                                          B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64)
-                      : ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
-                                          B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
-    if (s != AR_OK) return s;
+    // 32-bit keys are re-sorted from the last step's order once there is one (as in the grid
+    // step; ar_resort.cuh), 64-bit keys radix-sorted every step
+    const bool resort32 = k32 && B->order_valid;
+    if (resort32) {
+      const ar_resort::Work rw = resort_work(B, B->bvh_key_bits);
+      cudaMemsetAsync(rw.head, 0, ar_resort::cleared_words() * 4, st);
+      launch_resort(ctx, B, rw, st);
+    } else {
+      ar_status s = k32 ? ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0,
+                                            B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64)
+                        : ar_sort::sort_u64(ctx, B->keys64, nullptr, B->skeys64, B->svals, nt, 0,
+                                            B->bvh_key_bits, st, B->sort64_ws, B->cap_sort64);
+      if (s != AR_OK) return s;
+    }
     mark(3);
     const dim3 gb(arh::grid_for(std::max(nt - 1, 1), 256));
     if (k32)
@@ -1074,7 +1123,8 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     // one thread per leaf: each climbs after storing its leaf
     AR_LAUNCH_ONE(bvh_leaves_kernel, dim3(arh::grid_for(nt, 256)), dim3(256), B->d_table,
         B->d_pscene, ns, nt, B->svals, B->left, B->parent, B->spos, B->svel, B->nodes, B->is_leaf,
-        B->min_r, B->max_r, B->counters);
+        B->min_r, B->max_r, B->counters, (const uint32_t*)B->skeys, k32 ? B->pkeys : nullptr,
+        k32 ? B->pvals : nullptr);
     arh::launch_pdl(bvh_roots_kernel, dim3(arh::grid_for(ns, 128)), dim3(128), 0, st, B->d_poff, ns,
         nt, B->parent, B->min_r, B->max_r, B->roots);
     mark(4);
@@ -1086,26 +1136,14 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
     AR_LAUNCH_ONE(integrate_kernel, dim3(arh::grid_for(bt, 256)), dim3(256), B->d_table,
         B->d_bscene, bt, B->d_step, ctx->d_err);
     mark(6);
+    B->order_valid = k32;  // the leaves kernel left this step's order in pkeys / pvals
     return arh::check_launch("step (BVH)");  // (AR_LAUNCH_ONE is undefined after the grid path)
   }
   // With the last step's order of this particle set at hand, the keys are re-sorted from it
   // (ar_resort); otherwise (first step after a change of the member list) they are radix-sorted
   // from scratch, with the histogram accumulated in K1.
   const bool resort = B->order_valid;
-  ar_resort::Work rw{};
-  if (resort) {
-    rw.head = B->rs_head;
-    rw.tcount = B->rs_head + ar_resort::tcount_offset();
-    rw.bits = B->rs_head + ar_resort::bits_offset(B->cap_n);
-    rw.thead = B->rs_thead;
-    rw.bstart = B->rs_bstart;
-    rw.local = B->rs_movers;   // the tiles' movers are dead once grouped by bucket,
-    rw.movers = B->rs_movers;  // before the sorted movers are written
-    rw.grouped = B->rs_grouped;
-    const int nb_log2 = std::min(ar_resort::kBucketLog2, B->key_bits);
-    rw.nb = 1 << nb_log2;
-    rw.bshift = B->key_bits - nb_log2;
-  }
+  const ar_resort::Work rw = resort ? resort_work(B, B->key_bits) : ar_resort::Work{};
   const long head16 = resort ? (long)(ar_resort::cleared_words() / 4)
                              : (long)(ar_sort::clear_bytes(nt, B->plan.passes) / 16);
   arh::launch_pdl(step_clear_kernel, dim3(ctx->num_sms * 2), dim3(256), 0, st,
@@ -1120,18 +1158,7 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   }
   mark(2);
   if (resort) {
-    const unsigned tiles = (unsigned)ar_resort::tiles_for(nt);
-    const unsigned wpb = ar_resort::kWarps;  // warps per block: one per tile / bucket
-    arh::launch_pdl(ar_resort::leavers_kernel, dim3(tiles), dim3(ar_resort::kThreads), 0, st,
-        (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals, (const uint32_t*)B->keys, nt, rw);
-    arh::launch_pdl(ar_resort::bucket_kernel, dim3((tiles + wpb - 1) / wpb),
-        dim3(ar_resort::kThreads), 0, st, (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals,
-        nt, (int)tiles, rw);
-    arh::launch_pdl(ar_resort::bucket_sort_kernel, dim3((rw.nb + wpb - 1) / wpb),
-        dim3(ar_resort::kThreads), 0, st, rw);
-    arh::launch_pdl(ar_resort::place_kernel, dim3(tiles), dim3(ar_resort::kThreads), 0, st,
-        (const uint32_t*)B->pkeys, (const uint32_t*)B->pvals, nt, rw, B->skeys, B->svals,
-        ctx->d_err);
+    launch_resort(ctx, B, rw, st);
   } else {
     // cell keys in particle order: a warp's keys share few digits, so match.any ranking
     ar_status s = ar_sort::sort_u32(ctx, B->keys, nullptr, B->skeys, B->svals, nt, 0,
@@ -1215,7 +1242,8 @@ ar_status batch_step(ar_ctx* ctx, ar_batch* B, int n_steps, int use_graph, cudaS
   ar_status s = prepare(B, st);
   if (s != AR_OK) return s;
   if (B->nt == 0 || n_steps <= 0) return AR_OK;
-  if (B->broadphase == AR_BROADPHASE_GRID && !B->order_valid) {
+  const bool resorts = B->broadphase == AR_BROADPHASE_GRID || B->bvh_key_bits <= 32;
+  if (resorts && !B->order_valid) {
     // the first step after a change of the member list sorts from scratch, outside the graphs
     // (which hold re-sorting steps)
     if ((s = enqueue_step(B, st)) != AR_OK) return s;
@@ -1730,8 +1758,11 @@ ar_status ar_scene_model_matrices(ar_scene* s, float* d_model16, ar_stream_t str
 int ar_batch_launches_per_step(ar_batch* B) {
   if (!B) return 0;
   // memset, keys, sort, 4 tree kernels, collide, body sums, integration
+  // BVH: memset, keys, the sort (32-bit keys: memset + four re-sort kernels after the first
+  // step; 64-bit keys: the radix sort), four tree kernels, collide, body sums, integration
   if (B->broadphase == AR_BROADPHASE_BVH)
-    return 1 + 1 + ar_sort::launches(0, B->bvh_key_bits, false) + 4 + 1 + 2;
+    return 1 + 1 + (B->bvh_key_bits <= 32 ? 1 + 4 : ar_sort::launches(0, B->bvh_key_bits, false)) +
+           4 + 1 + 2;
   // a step that re-sorts from the previous order (every step but the first after a change of
   // the member list): clear, keys, four re-sort kernels, scatter, collide, body sums,
   // integration

@@ -61,7 +61,7 @@ def test_resort_equals_radix_sort_small_scenes(ctx):
 
 
 def test_resort_equals_radix_sort_pile_2m(ctx):
-    # the 2,097,152-particle pile: 1,024 tiles, 2^14 buckets over 25-bit keys
+    # the 2,097,152-particle pile: 1,024 tiles, 2^12 buckets over 25-bit keys
     _compare_next_step(ctx, scenes.config2(0), 12)
 
 
@@ -106,3 +106,34 @@ def test_resort_in_batches_equals_solo(ctx):
     batch.close()
     for g in solo + mem:
         g.close()
+
+
+def _compare_next_step_bvh(ctx, sc, warm_steps, perturb=None):
+    a = api.GpuScene(ctx, sc, broadphase="bvh")
+    a.step(warm_steps, use_graph=True)
+    state = a.download_state()
+    if perturb is not None:
+        state = np.ascontiguousarray(perturb(state))
+        a.upload_state(state)
+    b = api.GpuScene(ctx, sc, broadphase="bvh")
+    b.upload_state(state)
+    a.step(1, use_graph=True)
+    b.step(1, use_graph=True)
+    ctx.check()
+    ka, ia, fa = _sorted(a)
+    kb, ib, fb = _sorted(b)
+    assert np.array_equal(ka, kb) and np.array_equal(ia, ib)
+    assert np.array_equal(fa, fb)
+    assert np.array_equal(a.download_state(), b.download_state())
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("perturb", [None, _scatter_bodies(7)], ids=["steps", "bodies_swapped"])
+def test_bvh_resort_equals_radix_sort(ctx, perturb):
+    # the BVH step's 30-bit Morton keys (one scene) are re-sorted the same way
+    _compare_next_step_bvh(ctx, scenes.config0(0), 9, perturb)
+
+
+def test_bvh_resort_pile_2m(ctx):
+    _compare_next_step_bvh(ctx, scenes.config2(0), 12)
