@@ -85,21 +85,26 @@ def stage_bytes(n: int, nb: int, passes: int, occupied_cells: int,
 BVH_STAGES = ["clear", "keys", "sort", "tree", "collide", "body"]
 
 
-def stage_bytes_bvh(n: int, nb: int, passes: int) -> dict[str, float]:
-    """The same accounting for the BVH broad phase (64-bit keys, 64-byte wide nodes)."""
+def stage_bytes_bvh(n: int, nb: int, passes: int, key_bits: int = 64) -> dict[str, float]:
+    """The same accounting for the BVH broad phase (64-byte wide nodes).  Keys of up to 32 bits
+    (up to four scenes) are re-sorted from the previous step's order after the first step
+    (movers' own bytes left out); wider keys are radix-sorted as 64-bit keys."""
     tiles = (n + 8191) // 8192
+    k32 = key_bits <= 32
     return {
-        "clear": 4 * n,  # refit arrival counters
-        # rel in, 64-bit key out; body pose per body
-        "keys": n * (16 + 8) + nb * 32,
-        # histogram pass reads the keys; first pass reads keys, every pass writes key + index,
-        # later passes read both
-        "sort": n * 8 + n * (8 + 12) + (passes - 1) * n * 24 + passes * 4 * 512 * tiles,
+        "clear": 4 * n + (4 * (4 + 2 * 4096) if k32 else 0),  # refit arrival counters
+        # rel in, key out; body pose per body
+        "keys": n * (16 + (4 if k32 else 8)) + nb * 32,
+        # re-sort: previous keys + indices in, new key gathered, mover bits; placement: previous
+        # keys + indices and bits in, keys + indices out.  Radix: histogram pass reads the keys;
+        # first pass reads keys, every pass writes key + index, later passes read both
+        "sort": (n * (8 + 4 + 0.125) + n * (8 + 0.125 + 8) + (n // 2048) * 40) if k32 else
+                n * 8 + n * (8 + 12) + (passes - 1) * n * 24 + passes * 4 * 512 * tiles,
         # nodes: keys in, flags, children, parent, ranges and wide-node ids out; leaves: index,
-        # rel in, sorted pos + vel and the leaf box out, body state per body; refit: links and
-        # the node's two child boxes in, its box out
-        "tree": n * (8 + 21 + 8 + 8) + n * (4 + 16 + 32 + 24 + 9) + nb * BODY_STATE +
-                n * (8 + 64 + 24),
+        # rel in, sorted pos + vel and the leaf box out (and the order kept, 32-bit keys), body
+        # state per body; refit: links and the node's two child boxes in, its box out
+        "tree": n * ((4 if k32 else 8) + 21 + 8 + 8) + n * (4 + 16 + 32 + 24 + 9) +
+                (n * 8 if k32 else 0) + nb * BODY_STATE + n * (8 + 64 + 24),
         # own index, position + velocity in; force out
         "collide": n * (4 + 32 + 16),
         "body": n * (16 + 16) + _body_bytes(nb),
@@ -378,7 +383,7 @@ def run_ours(args):
     passes = sort_passes(sv.key_bits)
     if args.broadphase == "bvh":
         names = BVH_STAGES
-        sbytes = stage_bytes_bvh(n, nb, passes)
+        sbytes = stage_bytes_bvh(n, nb, passes, int(sv.key_bits))
     else:
         names = STAGES
         keys = api.device_view(sv.sorted_keys, n, torch.int32)
