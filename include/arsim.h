@@ -541,8 +541,10 @@ AR_API ar_status ar_sequential_impulse(ar_ctx* ctx, const ar_sim_params* params,
 
 /* ==== fused step: scenes and batches ================================================================
  * A scene is one independent rigid-body world resident on the device.  ar_step advances it
- * with the fused pipeline (re-pose + hash, onesweep sort, scatter + cell ranges, DEM
- * gather + walls, fixed-order body reduction + integration), PHYSICAL semantics:
+ * with the fused pipeline (re-pose + hash, the order by (key, particle index) -- re-sorted
+ * from the previous step's order, or radix-sorted in the first step after a change of the
+ * member list -- scatter + cell ranges, DEM gather + walls, fixed-order body reduction +
+ * integration), PHYSICAL semantics:
  *   v += (g + F/m) dt,  omega += I_w^-1 tau dt,  x += v dt,
  *   q += dt/2 (omega, 0) q, normalised;  I_w^-1 = R I_b^-1 R^T,
  * with box walls as DEM springs (the wall is a static sphere surface at the plane).
