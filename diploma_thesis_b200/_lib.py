@@ -120,6 +120,8 @@ SIGNATURES = {
     "ar_calc_hash": [P, C.POINTER(SimParams), P, I, P, P, S],
     "ar_reorder_cells": [P, P, P, P, P, I, C.c_uint32, P, P, P, P, S],
     "ar_collide_grid_dem": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, I, P, P, S],
+    "ar_range_image_cloud": [P, P, I, I, P, F, P, P, P, S],
+    "ar_range_image_normals": [P, P, I, I, P, S],
     "ar_collide_static_scene_dem": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, I, P, P, P, S],
     "ar_collide_static_scene_impulse": [P, C.POINTER(SimParams), P, P, P, P, P, P, P, P, P, P, P,
                                         P, I, P, P, P, P, P, S],

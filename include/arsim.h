@@ -267,6 +267,27 @@ AR_API ar_status ar_reorder_cells(ar_ctx* ctx, const uint32_t* sorted_hash,
                                   uint32_t* cell_start, uint32_t* cell_end, float* sorted_pos4,
                                   float* sorted_vel4, ar_stream_t stream);
 
+/* ---- depth-camera ingestion: the static scene's point cloud from a range image --------------
+ * RGBDloader (Kernels/customRangeImageLoader.cu:14-113): per pixel (x, y) of a width x height
+ * image of 16-bit depths (device memory; pixels whose index y * width + x exceeds
+ * (width - 1) * (height - 1) are skipped, as in the reference): z = depth / 5000 (z < 0.01 ->
+ * -1000), x' = z (x - 318.6) / 517.3, y' = z (y - 255.3) / 516.5, the point (x', y', z, 0) through
+ * the transposed camera matrix (camera16: host, 16 floats, column-major glm::mat4) and the
+ * reference's fixed gravity rotation, then (x, -y, -z) -> static_pos4 (w = 0), static_radii =
+ * particle_radius, and vao5 (may be NULL) = x, y, z, x / width, y / height (the vertex records
+ * the reference writes into its GL buffer).  Covers every pixel (the reference's launch only
+ * whole 16 x 32 blocks). */
+AR_API ar_status ar_range_image_cloud(ar_ctx* ctx, const uint16_t* depth, int width, int height,
+                                      const float* camera16, float particle_radius,
+                                      float* static_pos4, float* static_radii, float* vao5,
+                                      ar_stream_t stream);
+
+/* computeNormals (Kernels/customRangeImageLoader.cu:122-177): for every pixel not on the image
+ * border, normal = normalize(cross(p(x, y+1) - p(x, y-1), p(x+1, y) - p(x-1, y))) with the
+ * inverse length 1 / sqrtf (the reference's device build: rsqrtf); border pixels untouched. */
+AR_API ar_status ar_range_image_normals(ar_ctx* ctx, const float* static_pos4, int width,
+                                        int height, float* static_norm4, ar_stream_t stream);
+
 /* ---- AR static scene (point cloud with normals) against the particles ---------------------
  * FindAndHandleAugmentedRealityCollisionsUniformGridKernel (RigidBodies/UniformGridDEM.cu:
  * 243-377): the scene's particles are hashed, sorted and given cell ranges with the same grid

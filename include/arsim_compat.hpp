@@ -496,6 +496,25 @@ void FindRigidBodyCollisionsBVHWrapper(float4* color, int* rigidBodyIndex, bool*
             "FindRigidBodyCollisionsBVHWrapper");
 }
 
+/* ---- depth-camera ingestion: declared in Particles/loadRangeDataFromFile.cpp:13-22, defined in
+ * Kernels/customRangeImageLoader.cu:179-221 (VAOdata: the mapped GL buffer there, any device
+ * buffer of 5 floats per pixel here) ------------------------------------------------------- */
+cudaError_t loadRangeImage(unsigned short* image, float** VAOdata, float** staticPos,
+                           float** staticNorm, glm::mat4& cameraTransformation,
+                           float* staticRadii, float particleRadius, int imageWidth,
+                           int imageHeight) {
+  float cam[16];
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) cam[4 * c + r] = cameraTransformation[c][r];
+  ARC_CHECK(ar_range_image_cloud(ARC_CTX, image, imageWidth, imageHeight, cam, particleRadius,
+                                 *staticPos, staticRadii, *VAOdata, nullptr),
+            "loadRangeImage");
+  ARC_CHECK(ar_range_image_normals(ARC_CTX, *staticPos, imageWidth, imageHeight, *staticNorm,
+                                   nullptr),
+            "loadRangeImage");
+  return cudaDeviceSynchronize();
+}
+
 #undef ARC_CTX
 #undef ARC_CHECK
 #endif /* ARSIM_COMPAT_IMPLEMENTATION */

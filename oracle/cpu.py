@@ -564,3 +564,24 @@ def find_contacts_bvh_static(radius, pos4, tree, cms4, bounds8, sorted_idx, radi
                                    _p(_f32(cms4)), _p(_f32(bounds8)), _p(_i32(sorted_idx)),
                                    _p(_f32(radii)), m, n, _p(cd), _p(cp), _p(color))
     return cd, cp, color
+
+
+def range_image_cloud(depth: np.ndarray, camera16, radius: float, with_vao: bool = True):
+    """RGBDloader (Kernels/customRangeImageLoader.cu:14-113): depth [h, w] uint16 -> pos4 [h*w, 4],
+    radii [h*w], vao5 [h*w, 5]; pixels past the reference's bound stay NaN."""
+    d = np.ascontiguousarray(depth, dtype=np.uint16)
+    h, w = d.shape
+    pos4 = np.full((h * w, 4), np.nan, np.float32)
+    radii = np.full(h * w, np.nan, np.float32)
+    vao5 = np.full((h * w, 5), np.nan, np.float32) if with_vao else None
+    cam = _f32(np.asarray(camera16, np.float32).reshape(16))
+    _L.or_range_cloud(_p(d), C.c_int(w), C.c_int(h), _p(cam), C.c_float(radius), _p(pos4),
+                      _p(radii), _p(vao5) if with_vao else None)
+    return {"pos4": pos4, "radii": radii, "vao5": vao5}
+
+
+def range_image_normals(pos4: np.ndarray, w: int, h: int, init: float = np.nan):
+    """computeNormals (Kernels/customRangeImageLoader.cu:122-177); border pixels keep `init`."""
+    norm4 = np.full((h * w, 4), init, np.float32)
+    _L.or_range_normals(_p(_f32(pos4)), C.c_int(w), C.c_int(h), _p(norm4))
+    return norm4

@@ -1865,3 +1865,75 @@ void or_sequential_impulse(long count, const float* normal4, const float* point4
       st4(ang4 + 4 * i2, w2.x, w2.y, w2.z, 0.f);
     }
 }
+
+/* ---- depth-camera ingestion (Kernels/customRangeImageLoader.cu) ----------------------------
+ * RGBDloader (:14-113) and computeNormals (:122-177), per pixel in the reference's arithmetic
+ * order; glm 0.9.7 mat4 * vec4 pairs (m0 v0 + m1 v1) + (m2 v2 + m3 v3); normalize takes
+ * 1 / sqrtf (helper_math's host rsqrtf, glm's inversesqrt). */
+static void or_mat4_mul_(const float m[16], const float v[4], float out[4]) {
+  for (int i = 0; i < 4; ++i) {
+    const float a0 = m[0 * 4 + i] * v[0] + m[1 * 4 + i] * v[1];
+    const float a1 = m[2 * 4 + i] * v[2] + m[3 * 4 + i] * v[3];
+    out[i] = a0 + a1;
+  }
+}
+
+void or_range_cloud(const uint16_t* depth, int w, int h, const float* cam16, float radius,
+                    float* pos4, float* radii, float* vao5) {
+  float t[16];  /* transpose (column-major in, column-major out) */
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) t[4 * c + r] = cam16[4 * r + c];
+  const float fx = (float)517.3, fy = (float)516.5, cx = (float)318.6, cy = (float)255.3;
+  const float gx0 = (float)0.478957, gy0 = (float)-8.010560, gz0 = (float)4.166928;
+  const float inv = 1.0f / sqrtf(gx0 * gx0 + gy0 * gy0 + gz0 * gz0);
+  const float gx = gx0 * inv, gy = gy0 * inv, gz = gz0 * inv;
+  const float grav[16] = {1.f, 0.f, 0.f, 0.f, -gx, -gy, -gz, 0.f,
+                          0.f, gz, -gy, 0.f, 0.f, 0.f, 0.f, 1.f};
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      const long index = (long)y * w + x;
+      if (index > (long)(w - 1) * (h - 1)) continue;
+      float pz = (float)depth[index];
+      pz /= 5000.f;
+      radii[index] = radius;
+      if ((double)pz < 0.01) pz = -1000.f;
+      const float px = pz * ((float)x - cx) / fx;
+      const float py = pz * ((float)y - cy) / fy;
+      const float v[4] = {px, py, pz, 0.f};
+      float a[4], b[4];
+      or_mat4_mul_(t, v, a);
+      or_mat4_mul_(grav, a, b);
+      const float ox = b[0], oy = -b[1], oz = -b[2];
+      if (vao5) {
+        vao5[5 * index] = ox;
+        vao5[5 * index + 1] = oy;
+        vao5[5 * index + 2] = oz;
+        vao5[5 * index + 3] = (float)x / (float)w;
+        vao5[5 * index + 4] = (float)y / (float)h;
+      }
+      pos4[4 * index] = ox;
+      pos4[4 * index + 1] = oy;
+      pos4[4 * index + 2] = oz;
+      pos4[4 * index + 3] = 0.f;
+    }
+}
+
+void or_range_normals(const float* pos4, int w, int h, float* norm4) {
+  for (int y = 1; y < h - 1; ++y)
+    for (int x = 1; x < w - 1; ++x) {
+      const float* up = pos4 + 4 * ((long)(y - 1) * w + x);
+      const float* right = pos4 + 4 * ((long)y * w + x + 1);
+      const float* down = pos4 + 4 * ((long)(y + 1) * w + x);
+      const float* left = pos4 + 4 * ((long)y * w + x - 1);
+      const float dx[3] = {right[0] - left[0], right[1] - left[1], right[2] - left[2]};
+      const float dy[3] = {down[0] - up[0], down[1] - up[1], down[2] - up[2]};
+      const float c[3] = {dy[1] * dx[2] - dy[2] * dx[1], dy[2] * dx[0] - dy[0] * dx[2],
+                          dy[0] * dx[1] - dy[1] * dx[0]};
+      const float inv = 1.0f / sqrtf(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+      float* o = norm4 + 4 * ((long)y * w + x);
+      o[0] = c[0] * inv;
+      o[1] = c[1] * inv;
+      o[2] = c[2] * inv;
+      o[3] = 0.f;
+    }
+}

@@ -401,3 +401,20 @@ def find_contacts_bvh_static(params, pos4, tree, cms4, bounds8, sorted_idx, radi
                                           _p(_i32(sorted_idx)), _p(_f32(radii)), n, m, _p(cd),
                                           _p(cp))
     return cd, cp, color
+
+
+def range_image(depth, camera16, radius):
+    """RGBDloader and computeNormals (Kernels/customRangeImageLoader.cu:14-177) over the grid
+    loadRangeImage launches (whole 16 x 32 blocks) -> pos4, radii, vao5, norm4; pixels the
+    reference does not write stay NaN."""
+    d = np.ascontiguousarray(depth, dtype=np.uint16)
+    h, w = d.shape
+    pos4 = np.full((h * w, 4), np.nan, np.float32)
+    radii = np.full(h * w, np.nan, np.float32)
+    vao5 = np.full((h * w, 5), np.nan, np.float32)
+    norm4 = np.full((h * w, 4), np.nan, np.float32)
+    cam = _f32(np.asarray(camera16, np.float32).reshape(16))
+    lib().refcpu_range_cloud(_p(d), C.c_int(w), C.c_int(h), _p(cam), C.c_float(radius),
+                             _p(pos4), _p(radii), _p(vao5))
+    lib().refcpu_range_normals(_p(pos4), C.c_int(w), C.c_int(h), _p(norm4))
+    return {"pos4": pos4, "radii": radii, "vao5": vao5, "norm4": norm4}

@@ -58,6 +58,8 @@ RANGES = [
     ("WallCollisions.cu", 29, 35, "CreateIndexKernel"),
     ("WallCollisions.cu", 46, 129, "DetectWallCollisionKernel"),                 # + FindExactContactPoint, ComputeImpulseMagnitude
     ("WallCollisions.cu", 201, 276, "HandleWallCollisionKernelUnmapped"),
+    ("Kernels/customRangeImageLoader.cu", 14, 113, "__global__ void RGBDloader("),
+    ("Kernels/customRangeImageLoader.cu", 122, 177, "__global__ void computeNormals("),
 ]
 
 # ParticleSystem member functions of the sequential-impulse path (host C++ with glm): the

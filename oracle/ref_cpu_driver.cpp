@@ -669,3 +669,40 @@ extern "C" int refcpu_init_object(const char* text, const char* modelName, float
   std::memcpy(inv_inertia9, &inertiaTensor[0][0], 9 * sizeof(float));
   return particles;
 }
+
+// ---- depth-camera ingestion: RGBDloader and computeNormals (Kernels/customRangeImageLoader.cu
+// :14-177) over the grid loadRangeImage launches (:179-221): 16 x 32 blocks, width / 16 x
+// height / 32 of them.  vao5 must hold 5 floats per pixel (the kernel writes it always).
+namespace {
+template <class F>
+void launch_image(int w, int h, F&& body) {
+  const int bx = 16, by = 32, gx = w / bx, gy = h / by;
+  for (int yb = 0; yb < gy; ++yb)
+    for (int xb = 0; xb < gx; ++xb)
+      for (int ty = 0; ty < by; ++ty)
+        for (int tx = 0; tx < bx; ++tx) {
+          blockIdx = make_uint3((unsigned)xb, (unsigned)yb, 0);
+          threadIdx = make_uint3((unsigned)tx, (unsigned)ty, 0);
+          blockDim = dim3(bx, by, 1);
+          gridDim = dim3(gx, gy, 1);
+          body();
+        }
+}
+}  // namespace
+
+extern "C" void refcpu_range_cloud(const unsigned short* depth, int w, int h, const float* cam16,
+                                   float radius, float* pos4, float* radii, float* vao5) {
+  glm::mat4 cam;
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) cam[c][r] = cam16[4 * c + r];
+  launch_image(w, h, [&] {
+    RGBDloader(const_cast<unsigned short*>(depth), vao5, pos4, cam, radii, radius, w, h);
+  });
+}
+
+extern "C" void refcpu_range_normals(const float* pos4, int w, int h, float* norm4) {
+  launch_image(w, h, [&] {
+    computeNormals(reinterpret_cast<float4*>(const_cast<float*>(pos4)),
+                   reinterpret_cast<float4*>(norm4), w, h);
+  });
+}

@@ -112,4 +112,13 @@ void drv_walls(const void* params, float* ppos, float* bpos, const float* mn, co
                        counts_host, nb, n, 128, params_of(params));
 }
 
+// loadRangeImage with the camera as a glm::mat4 (column-major 16 floats in).
+int drv_range_image(unsigned short* depth, float* vao5, float* pos4, float* norm4, float* radii,
+                    const float* cam16, float radius, int w, int h) {
+  glm::mat4 cam;
+  for (int c = 0; c < 4; ++c)
+    for (int r = 0; r < 4; ++r) cam[c][r] = cam16[4 * c + r];
+  return (int)loadRangeImage(depth, &vao5, &pos4, &norm4, cam, radii, radius, w, h);
+}
+
 }  // extern "C"

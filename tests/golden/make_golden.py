@@ -395,7 +395,29 @@ CASES = {
     "sis_solve": lambda: sis_solve_case(2),
     "static_scene_ar": lambda: static_scene_ar_case(31),
     "static_scene_bvh": lambda: static_scene_bvh_case(31),
+    "range_image": lambda: range_image_case(41),
 }
+
+
+def range_image_case(seed: int):
+    """A 96 x 64 depth image (whole 16 x 32 blocks, as loadRangeImage launches): a tilted plane
+    with a sphere cap, holes of zero depth and noise, in the TUM depth scale (5000 per metre);
+    a rotated and shifted camera."""
+    rng = np.random.default_rng(seed)
+    h, w = 64, 96
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float64)
+    z = 1.2 + 0.004 * xx + 0.002 * yy
+    cap = 0.25 - ((xx - 40) ** 2 + (yy - 30) ** 2) / 400.0
+    z = z - np.clip(cap, 0, None)
+    z = z + rng.normal(0, 0.002, z.shape)
+    depth = np.clip(np.round(z * 5000.0), 0, 65535).astype(np.uint16)
+    depth[rng.random(depth.shape) < 0.03] = 0
+    ang = 0.3
+    cam = np.eye(4, dtype=np.float32)  # glm::mat4, column-major: cam[column][row]
+    cam[0, 0], cam[0, 2], cam[2, 0], cam[2, 2] = np.cos(ang), -np.sin(ang), np.sin(ang), np.cos(ang)
+    cam[3, :3] = (0.1, -0.2, 0.3)
+    out = ref.range_image(depth, cam.reshape(16), 1.0 / 128)
+    return {"depth": depth, "camera16": cam.reshape(16), "radius": np.float32(1.0 / 128), **out}
 
 
 def main() -> None:

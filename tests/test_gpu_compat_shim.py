@@ -12,7 +12,8 @@ reference's own kernel bodies (tests/golden/make_golden.py):
 * sortParticles: sorted in place, pointers unchanged, no device memory taken by a repeat call;
 * ReducePerParticleImpulses with host-side counts: the oracle's fixed-order sums (the shim does
   not reproduce the reference's prefix-sum differences, which drop each body's first particle);
-* WallCollisionWrapper: the reference's Baraff wall impulses bit for bit.
+* WallCollisionWrapper: the reference's Baraff wall impulses bit for bit;
+* loadRangeImage: the depth image's point cloud, vertex records and normals bit for bit.
 """
 import ctypes as C
 
@@ -140,3 +141,24 @@ def test_walls_through_the_shim(drv):
     assert drv.drv_take_status() == 0
     assert np.array_equal(host(vel), g["wall_vel_out"])
     assert np.array_equal(host(ang), g["wall_ang_out"])
+
+
+def test_load_range_image_through_the_shim(drv):
+    # loadRangeImage(image, &VAOdata, &staticPos, &staticNorm, camera, radii, r, w, h): the
+    # reference's cloud, vertex records and normals bit for bit
+    z = golden("range_image")
+    h, w = z["depth"].shape
+    depth = torch.from_numpy(z["depth"].view(np.int16).copy()).cuda()
+    bufs = {k: torch.full(shape, float("nan"), device="cuda") for k, shape in
+            (("vao5", (h * w, 5)), ("pos4", (h * w, 4)), ("norm4", (h * w, 4)),
+             ("radii", (h * w,)))}
+    cam = np.ascontiguousarray(z["camera16"].astype(np.float32))
+    rc = drv.drv_range_image(_p(depth), _p(bufs["vao5"]), _p(bufs["pos4"]), _p(bufs["norm4"]),
+                             _p(bufs["radii"]), cam.ctypes.data_as(C.c_void_p),
+                             C.c_float(float(z["radius"])), w, h)
+    assert rc == 0 and drv.drv_take_status() == 0
+    for k, t in bufs.items():
+        got, want = host(t), z[k]
+        written = ~np.isnan(want)
+        assert np.array_equal(~np.isnan(got), written)
+        assert np.array_equal(got[written].view(np.uint32), want[written].view(np.uint32)), k
