@@ -233,14 +233,14 @@ __global__ void __launch_bounds__(kThreads) bucket_kernel(const uint32_t* __rest
   const bool live = t < tiles;
   const long base = (long)t * kTile, end = min((long)n, base + kTile);
   const uint2* __restrict__ src = w.local + (size_t)t * kTile;
-  // issued early: the first 32 movers of the tile (slots of the tile, always in bounds), the
-  // tile's first and last old keys, the last stayer before it
+  // issued early: the tile's first 32 mover slots (only those below the tile's length, so
+  // within the particle count), its first and last old keys, the last stayer before it
   uint2 e0 = make_uint2(0u, 0u);
   uint32_t kfirst = 0, klast = 0;
   uint2 prev = make_uint2(0u, 0u);
   bool has_prev = false;
   if (live) {
-    e0 = src[lane];
+    if (lane < end - base) e0 = src[lane];
     if (lane == 0) {
       kfirst = __ldg(pk + base);
       klast = __ldg(pk + end - 1);
