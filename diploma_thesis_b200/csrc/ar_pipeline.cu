@@ -464,23 +464,38 @@ __global__ void __launch_bounds__(256) bvh_build_kernel(Lcp lcp, int n,
 __device__ __forceinline__ void refit_from_leaf(int i, int n, const int32_t* __restrict__ left,
                                                 const int32_t* __restrict__ parent,
                                                 WideNode* nodes, int* __restrict__ counters) {
-  auto children = [&](int node, ar_lbvh::Box6* a, ar_lbvh::Box6* b) {
+  // The climb of ar_lbvh::refit_climb with the wide nodes: the second child to arrive at a node
+  // merges the node's two child records (boxes, and body tags in their w) and writes the result
+  // into the node's slot in its parent.  The parent and the side of the slot depend only on
+  // the tree, so they are loaded before the arrival: each level costs the arrival and the
+  // children's records, two round trips.
+  int node = __ldg(parent + i);
+  if (node < n || node >= 2 * n - 1) return;  // malformed parent link
+  int pn = node != n ? __ldg(parent + node) : n;
+  int side = node != n ? (__ldg(left + pn) == node ? 0 : 1) : 0;
+  for (int depth = 0; depth < n; ++depth) {  // a valid tree is at most n - 1 deep
+    // the next level's parent and side, loaded while the arrival is in flight (wasted when this
+    // thread arrives first)
+    const int next = pn;
+    const bool next_ok = next != n && next >= n && next < 2 * n - 1;
+    const int npn = next_ok ? __ldg(parent + next) : n;
+    if (ar_lbvh::arrive(counters + (node - n)) == 0) return;
     const float4* c = nodes[node - n].c;
     const float4 a0 = __ldcg(c), a1 = __ldcg(c + 1), b0 = __ldcg(c + 2), b1 = __ldcg(c + 3);
-    *a = ar_lbvh::Box6{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y};
-    *b = ar_lbvh::Box6{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y};
-  };
-  auto store = [&](int node, const ar_lbvh::Box6& m) {
     if (node == n) return;  // the root's box is not stored anywhere
-    const int pn = __ldg(parent + node);
-    // both children have arrived, so their tags are visible like their boxes
-    const int* w = node_ints(nodes, node - n);
-    const int tl = __ldcg(w + 7), tr = __ldcg(w + 15);
-    put_child(nodes, pn - n, __ldg(left + pn) == node ? 0 : 1,
-              make_float4(m.lx, m.ly, m.lz, m.hx), make_float2(m.hy, m.hz), node,
-              tl == tr ? tl : -1);
-  };
-  ar_lbvh::refit_climb(i, n, parent, counters, children, store);
+    if (next != n && !next_ok) return;  // malformed parent link
+    const int nside = next_ok && npn >= n && npn < 2 * n - 1 && __ldg(left + npn) != next ? 1 : 0;
+    const ar_lbvh::Box6 m = ar_lbvh::merge_boxes(ar_lbvh::Box6{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y},
+                                                 ar_lbvh::Box6{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y});
+    // both children have arrived, so their tags (the records' last words) are visible like
+    // their boxes
+    const int tl = __float_as_int(a1.w), tr = __float_as_int(b1.w);
+    put_child(nodes, pn - n, side, make_float4(m.lx, m.ly, m.lz, m.hx), make_float2(m.hy, m.hz),
+              node, tl == tr ? tl : -1);
+    node = next;
+    pn = npn;
+    side = nside;
+  }
 }
 
 // Leaves in sorted order: position (w = global body id) and velocity recomputed from the body
