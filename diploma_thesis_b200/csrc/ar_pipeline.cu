@@ -1356,12 +1356,12 @@ uint64_t ar_scene_cells(const ar_scene_desc* d) {
 }  // extern "C"
 
 namespace {
-// Bytes of a scene's device block: body centre, orientation, velocity, angular velocity, force
-// and torque sums (float4 each), mass, inverse inertia, body offsets and particle offsets, each
-// array 256-byte aligned.
+// Bytes of a scene's device block: body centre, orientation, velocity, angular velocity (float4
+// each, adjacent, so that the four move in one copy), force and torque sums, mass, inverse
+// inertia, body offsets and particle offsets; the groups 256-byte aligned.
 size_t scene_block_bytes(int nb, int n, size_t sizes[5]) {
-  const size_t a6 = 16 * (size_t)nb;
-  sizes[0] = 6 * ((a6 + 255) & ~(size_t)255);
+  const size_t a4 = 64 * (size_t)nb, a1 = 16 * (size_t)nb;
+  sizes[0] = ((a4 + 255) & ~(size_t)255) + 2 * ((a1 + 255) & ~(size_t)255);
   sizes[1] = 4 * (size_t)nb;
   sizes[2] = 36 * (size_t)nb;
   sizes[3] = 4 * (size_t)(nb + 1);
@@ -1382,9 +1382,11 @@ bool alloc_scene_block(ar_scene* s, cudaStream_t st) {
     return false;
   }
   char* b = (char*)s->block;
-  const size_t s6 = sizes[0] / 6;
-  float4** arr6[6] = {&s->pos, &s->quat, &s->vel, &s->ang, &s->bforce, &s->btorque};
-  for (int i = 0; i < 6; ++i) *arr6[i] = (float4*)(b + i * s6);
+  const size_t a1 = 16 * (size_t)s->nb, a4 = (4 * a1 + 255) & ~(size_t)255;
+  float4** state[4] = {&s->pos, &s->quat, &s->vel, &s->ang};
+  for (int i = 0; i < 4; ++i) *state[i] = (float4*)(b + i * a1);
+  s->bforce = (float4*)(b + a4);
+  s->btorque = (float4*)(b + a4 + ((a1 + 255) & ~(size_t)255));
   b += (sizes[0] + 255) & ~(size_t)255;
   s->mass = (float*)b;
   b += (sizes[1] + 255) & ~(size_t)255;
@@ -1610,27 +1612,24 @@ ar_status ar_scene_upload(ar_scene* s, const float* h_pos4, const float* h_quat4
   return arh::check_launch("ar_scene_upload");
 }
 
-// The four body-state arrays sit at a fixed pitch in the scene's block (pos, quat, vel, ang),
-// so one 2D copy moves all of them.
-static size_t state_pitch(const ar_scene* s) {
-  return (size_t)((char*)s->quat - (char*)s->pos);
-}
+// The four body-state arrays are adjacent in the scene's block (pos, quat, vel, ang; carved
+// 16 * nb bytes apart by alloc_scene_block), so one contiguous copy moves all of them.  A 2D
+// copy of the same four rows ran at about 5 GB/s (256 KB each way: 95 us against 12 us).
+static_assert(sizeof(float4) == 16, "state rows are 16 * nb bytes");
 
 ar_status ar_scene_upload_state(ar_scene* s, const float* h_state16, ar_stream_t stream) {
   if (!s || !h_state16) return AR_ERR_INVALID_ARG;
   if (s->nb == 0) return AR_OK;
-  const size_t row = 16 * (size_t)s->nb;
-  cudaMemcpy2DAsync(s->pos, state_pitch(s), h_state16, row, row, 4, cudaMemcpyHostToDevice,
-                    arh::stream(stream));
+  cudaMemcpyAsync(s->pos, h_state16, 64 * (size_t)s->nb, cudaMemcpyHostToDevice,
+                  arh::stream(stream));
   return arh::check_launch("ar_scene_upload_state");
 }
 
 ar_status ar_scene_download_state_async(ar_scene* s, float* h_state16, ar_stream_t stream) {
   if (!s || !h_state16) return AR_ERR_INVALID_ARG;
   if (s->nb == 0) return AR_OK;
-  const size_t row = 16 * (size_t)s->nb;
-  cudaMemcpy2DAsync(h_state16, row, s->pos, state_pitch(s), row, 4, cudaMemcpyDeviceToHost,
-                    arh::stream(stream));
+  cudaMemcpyAsync(h_state16, s->pos, 64 * (size_t)s->nb, cudaMemcpyDeviceToHost,
+                  arh::stream(stream));
   return arh::check_launch("ar_scene_download_state_async");
 }
 

@@ -654,7 +654,7 @@ AR_API ar_status ar_scene_upload(ar_scene* scene, const float* h_body_pos4,
                                  const float* h_body_quat4, const float* h_body_vel4,
                                  const float* h_body_angvel4, ar_stream_t stream);
 /* Packed body state: h_state16 holds pos[nb], quat[nb], vel[nb], angvel[nb] back to back
- * (16 floats per body in all), moved with one strided copy each way instead of four.
+ * (16 floats per body in all), moved with one contiguous copy each way instead of four.
  * ar_scene_upload_state is asynchronous (pinned memory for overlap);
  * ar_scene_download_state returns once the state is on the host, and
  * ar_scene_download_state_async once the copy is queued on `stream`.  Same role as
