@@ -14,16 +14,19 @@
 //            every occupied cell; the order kept for the next step
 //   K4       DEM gather over the 27 neighbour cells + box walls -> per-particle force at the
 //            particle's original index (no atomics)
-//   K5       one warp per body: fixed-order sum of F and r x F, then integration
+//   K5       one warp per body: fixed-order sum of F and r x F; then one thread per body
+//            integrates (a separate kernel)
 // A scene's keys live in its own cell range, so sorting all scenes together orders them by
 // scene and within a scene exactly as a solo sort would: batched and solo steps are
 // bit-identical.  The sequence is captured once into a CUDA graph and replayed.
 //
-// Batches of BVH scenes replace K1-K4 by: 64-bit keys (scene index above the particle's 30-bit
-// Morton code), a 64-bit onesweep sort, leaves in sorted order, Karras nodes over all scenes
-// (equal codes tie-broken by the index within the scene), each scene's subtree root, fenced
-// refit, and a stackless walk of the scene's subtree per particle in the reference's visit
-// order.  K5 is shared.
+// Batches of BVH scenes replace K0-K4 by: a memset of the refit's arrival counters; Morton keys
+// (scene index above the particle's 30-bit code: 32-bit keys for up to 4 scenes, else 64-bit);
+// the sort (32-bit keys re-sorted from the last step's order as above, 64-bit keys radix-sorted
+// every step); Karras nodes over all scenes (equal codes tie-broken by the index within the
+// scene); leaves in sorted order, each leaf's thread then climbing the refit (acquire-release
+// arrival counters); each scene's subtree root; and per particle a walk of its scene's subtree
+// in the reference's visit order with a 64-entry stack.  K5 is shared.
 #include <algorithm>
 #include <climits>
 #include <cmath>

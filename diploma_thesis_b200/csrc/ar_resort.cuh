@@ -15,7 +15,8 @@
 //                   buckets' ranges, and the tile's header for place_kernel; every block scans
 //                   the bucket counts and the tile counts it needs itself.
 //   bucket_sort_kernel  each bucket sorted by (key, index): one warp per bucket, ranks by
-//                   comparison (buckets hold a few movers each).
+//                   comparison (in registers up to 32 movers, in shared memory up to 256, in
+//                   global memory beyond; buckets usually hold a few movers).
 //   place_kernel    over the previous order.  A stayer (a particle that kept its key) at old
 //                   position j has r = j - (movers before j) stayers before it in the new
 //                   order too (their keys did not change and the old order is sorted), and A =
