@@ -150,6 +150,7 @@ SIGNATURES = {
     "ar_scene_footprint": [C.POINTER(SceneDesc)],
     "ar_scene_cells": [C.POINTER(SceneDesc)],
     "ar_scene_destroy_async": [P, S],
+    "ar_scene_set_static_cloud": [P, P, P, P, I, S],
     "ar_batch_set_scenes_limited": [P, C.POINTER(P), I, P],
     "ar_batch_model_matrices": [P, P, S],
     "ar_scene_model_matrices": [P, P, S],

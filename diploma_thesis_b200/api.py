@@ -159,6 +159,22 @@ class GpuScene:
              _np_ptr(state), stream_handle(stream))
         return state
 
+    def set_static_cloud(self, pos4: torch.Tensor | None, norm4: torch.Tensor | None,
+                         stream=None) -> None:
+        """Attach a static point cloud (device float32 [M, 4] positions and normals) whose
+        points push the particles within 2r from the next step on (ar_scene_set_static_cloud);
+        None detaches it."""
+        if pos4 is None:
+            call("ar_scene_set_static_cloud", self.ctx.handle, self.handle, None, None, 0,
+                 stream_handle(stream))
+            return
+        for t in (pos4, norm4):
+            assert t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()
+            assert t.dim() == 2 and t.shape[1] == 4
+        assert pos4.shape == norm4.shape
+        call("ar_scene_set_static_cloud", self.ctx.handle, self.handle, ptr(pos4), ptr(norm4),
+             int(pos4.shape[0]), stream_handle(stream))
+
     def step_io(self, state_in: np.ndarray, n: int, state_out: np.ndarray, stream=None) -> None:
         """Upload the packed state, step n times (graph), copy the packed state back, in one
         call (ar_scene_step_io); both arrays are [4, B, 4] float32 pinned host arrays and may be

@@ -29,6 +29,24 @@ __host__ __device__ __forceinline__ float3 spring_force(float3 rp, float dist, f
   return f;
 }
 
+// Impulse on a particle at velocity v from a static scene point (the depth camera's point
+// cloud), FindAndHandleAugmentedRealityCollisionsUniformGridCell (RigidBodies/
+// UniformGridDEM.cu:275-296): along the negated normal nn of the scene point, the scene at
+// rest (rv = 0 - v), rp = scene point - particle, d = |rp| < contact tested by the caller.
+__host__ __device__ __forceinline__ float3 scene_force(float3 rp, float dist, float3 vel,
+                                                       float3 nn, float contact, float spring,
+                                                       float damping, float shear,
+                                                       float attraction) {
+  const float3 nrm = ar::mk3(-nn.x, -nn.y, -nn.z);
+  const float3 rv = ar::mk3(0.f - vel.x, 0.f - vel.y, 0.f - vel.z);
+  const float3 tv = ar::sub(rv, ar::scl(ar::dot(rv, nrm), nrm));
+  float3 f = ar::scl(-spring * (contact - dist), nrm);
+  f = ar::add(f, ar::scl(damping, rv));
+  f = ar::add(f, ar::scl(shear, tv));
+  f = ar::add(f, ar::scl(attraction, rp));
+  return f;
+}
+
 // collideStaticSpheresBVH (Kernels/RB_BVHKernels.cu:24-98): force on A from B plus the
 // position correction it writes when the spheres overlap.
 __device__ __forceinline__ float3 static_pair(float4 pa, float4 pb, float4 cm, float3 va,

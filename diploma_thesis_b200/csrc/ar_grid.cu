@@ -131,14 +131,9 @@ __global__ void __launch_bounds__(128) collide_static_kernel(
             const float3 rp = ar::sub(ar::xyz(__ldg(scene_spos + j)), pos);
             const float dist = sqrtf(ar::dot(rp, rp));
             if (!(dist < thr)) continue;
-            const float3 nn = ar::xyz(__ldg(scene_normals + o2));
-            const float3 nrm = ar::mk3(-nn.x, -nn.y, -nn.z);
-            const float3 rv = ar::mk3(0.f - vel.x, 0.f - vel.y, 0.f - vel.z);
-            const float3 tv = ar::sub(rv, ar::scl(ar::dot(rv, nrm), nrm));
-            float3 f = ar::scl(-prm.spring * (thr - dist), nrm);
-            f = ar::add(f, ar::scl(prm.damping, rv));
-            f = ar::add(f, ar::scl(prm.shear, tv));
-            f = ar::add(f, ar::scl(prm.attraction, rp));
+            const float3 f = ar_dem::scene_force(rp, dist, vel, ar::xyz(__ldg(scene_normals + o2)),
+                                                 thr, prm.spring, prm.damping, prm.shear,
+                                                 prm.attraction);
             cell_f = make_float4(cell_f.x + f.x, cell_f.y + f.y, cell_f.z + f.z, cell_f.w + 0.f);
             ++contacts;
           }

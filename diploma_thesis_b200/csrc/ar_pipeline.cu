@@ -373,6 +373,81 @@ __global__ void __launch_bounds__(256, 4) collide_kernel(
   pforce[__ldg(svals + k)] = make_float4(lin.x, lin.y, lin.z, 0.f);
 }
 
+// ---- K4b: the static point cloud of the scene ---------------------------------------------
+// updateUniformGridDEM's simulateAR branch (RigidBodies/UniformGridUpdate.cpp:967-969,
+// Find_And_Handle_Augmented_Reality_Collisions_Uniform_Grid_DEM :881-936): after the particle
+// contacts and the walls, each particle of a scene with a point cloud takes the impulses of the
+// cloud's points within 2r -- the 27 neighbour cells of its own grid in z, y, x order, the
+// points of a cell in the cloud's sorted order, per-cell partial sums added to the cloud total
+// (FindAndHandleAugmentedRealityCollisionsUniformGridKernel, RigidBodies/UniformGridDEM.cu:
+// 301-377) -- and the cloud total is added to its force, as the reference adds it to
+// pLinearImpulse.  Launched only when a scene of the batch has a cloud.
+template <bool kOne>
+__global__ void __launch_bounds__(128) cloud_collide_kernel(
+    const __grid_constant__ SceneDev one, const SceneDev* __restrict__ table, int nt,
+    const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ svals,
+    const float4* __restrict__ spos, const float4* __restrict__ svel,
+    float4* __restrict__ pforce) {
+  ar::pdl_wait();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  const float4 v4 = __ldg(svel + k);
+  const SceneDev& S = scene_at<kOne>(one, table, kOne ? 0 : __float_as_int(v4.w));
+  const uint2* __restrict__ cc = S.cloud_cells;
+  if (!cc) return;
+  const float4* __restrict__ cp = S.cloud_pos;
+  const float4* __restrict__ cn = S.cloud_norm;
+  const float3 pos = ar::xyz(__ldg(spos + k)), vel = ar::xyz(v4);
+  const float thr = 2.0f * S.r;
+  const uint32_t lx = S.lx, ly = S.ly, mx = S.gx - 1, my = S.gy - 1, mz = S.gz - 1;
+  const uint32_t local = __ldg(skeys + k) - S.cell_base;
+  const uint32_t x = local & mx, y = (local >> lx) & my, z = local >> (lx + ly);
+  float3 total = ar::mk3(0.f, 0.f, 0.f);
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy) {
+      const uint32_t zz = (z + (uint32_t)dz) & mz, yy = (y + (uint32_t)dy) & my;
+      const uint32_t row = (zz << (lx + ly)) + (yy << lx);
+      for (int dx = -1; dx <= 1; ++dx) {
+        const uint2 c = __ldg(cc + row + ((x + (uint32_t)dx) & mx));
+        float3 cf = ar::mk3(0.f, 0.f, 0.f);
+        for (uint32_t j = c.x; j < c.y; ++j) {
+          const float3 rp = ar::sub(ar::xyz(__ldg(cp + j)), pos);
+          const float dist = sqrtf(ar::dot(rp, rp));
+          if (!(dist < thr)) continue;
+          cf = ar::add(cf, ar_dem::scene_force(rp, dist, vel, ar::xyz(__ldg(cn + j)), thr, S.k,
+                                               S.damping, S.shear, S.attraction));
+        }
+        total = ar::add(total, cf);
+      }
+    }
+  float4* f = pforce + __ldg(svals + k);
+  const float4 f0 = *f;
+  *f = make_float4(f0.x + total.x, f0.y + total.y, f0.z + total.z, f0.w);
+}
+
+// Cell key of each cloud point in its scene's grid (cell_base 0).
+__global__ void cloud_keys_kernel(SceneDev d, const float4* __restrict__ pos, int m,
+                                  uint32_t* __restrict__ keys) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) keys[i] = ar_pipe::cell_key(d, ar_pipe::cell_of(d, ar::xyz(__ldg(pos + i))));
+}
+
+// Cloud points and normals in sorted order, and each occupied cell's {first, end}.
+__global__ void cloud_place_kernel(const float4* __restrict__ pos, const float4* __restrict__ nrm,
+                                   const uint32_t* __restrict__ skeys,
+                                   const uint32_t* __restrict__ sidx, int m,
+                                   float4* __restrict__ out_pos, float4* __restrict__ out_nrm,
+                                   uint2* __restrict__ cells) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const uint32_t i = __ldg(sidx + k), key = __ldg(skeys + k);
+  out_pos[k] = __ldg(pos + i);
+  out_nrm[k] = __ldg(nrm + i);
+  uint32_t* c = reinterpret_cast<uint32_t*>(cells + key);
+  if (k == 0 || __ldg(skeys + k - 1) != key) c[0] = (uint32_t)k;
+  if (k == m - 1 || __ldg(skeys + k + 1) != key) c[1] = (uint32_t)k + 1;
+}
+
 // ---- BVH broad phase ---------------------------------------------------------------------------
 // Key = scene index above a 30-bit Morton code of the particle's world position normalised to
 // its scene's box (generateMortonCodes, BVHSource/BVHkernels.cu:646-716).  Sorting all scenes
@@ -760,12 +835,21 @@ struct ar_scene {
   float origin[3], cell[3];
   uint32_t gdim[3];
   ar_batch* solo = nullptr;
+  // static point cloud (ar_scene_set_static_cloud): sorted points, normals, cell table
+  int cloud_n = 0;
+  float4 *cloud_pos = nullptr, *cloud_norm = nullptr;
+  uint2* cloud_cells = nullptr;
+  // bumped by every change that the batches' scene tables hold (the cloud), so that a batch
+  // holding the scene rebuilds its table before its next step
+  uint64_t version = 0;
 };
 
 struct ar_batch {
   ar_ctx* ctx = nullptr;
   std::vector<ar_scene*> scenes;
   bool table_dirty = true;
+  std::vector<uint64_t> seen_version;  // scenes' versions when the table was built
+  bool has_cloud = false;              // some scene has a static point cloud
   // capacities
   long cap_n = 0, cap_b = 0, cap_s = 0;
   uint64_t cap_cells = 0;
@@ -872,15 +956,43 @@ uint64_t scene_cells(const ar_scene* s) {
   return (uint64_t)s->gdim[0] * s->gdim[1] * s->gdim[2];
 }
 
+// Grid of a scene as the kernels see it (cell_base 0).
+void scene_dev_grid(const ar_scene* s, SceneDev* d) {
+  for (int a = 0; a < 3; ++a) {
+    d->origin[a] = s->origin[a];
+    d->cell[a] = s->cell[a];
+    d->inv_cell[a] = 1.0f / s->cell[a];
+  }
+  d->cell_pow2 = 1;
+  for (int a = 0; a < 3; ++a) {
+    int e = 0;
+    if (!(std::frexp(s->cell[a], &e) == 0.5f) || !std::isnormal(s->cell[a]) ||
+        !std::isnormal(d->inv_cell[a]))
+      d->cell_pow2 = 0;
+  }
+  d->gx = s->gdim[0]; d->gy = s->gdim[1]; d->gz = s->gdim[2];
+  d->lx = (uint32_t)ceil_log2(d->gx);
+  d->ly = (uint32_t)ceil_log2(d->gy);
+  d->cell_base = 0;
+}
+
 // (Re)build the scene table and make sure every buffer is large enough.
 ar_status prepare(ar_batch* B, cudaStream_t st) {
-  if (!B->table_dirty) return AR_OK;
+  if (!B->table_dirty) {
+    bool same = B->seen_version.size() == B->scenes.size();
+    for (size_t i = 0; same && i < B->scenes.size(); ++i)
+      same = B->scenes[i]->version == B->seen_version[i];
+    if (same) return AR_OK;
+    B->table_dirty = true;
+  }
   drop_graph(B);
   B->order_valid = false;  // the particle set may differ: the next step sorts from scratch
   long nt = 0, bt = 0;
   uint64_t cells = 0;
   std::vector<SceneDev> tab;
   std::vector<int> poff, boff;
+  B->seen_version.clear();
+  B->has_cloud = false;
   for (ar_scene* s : B->scenes) {
     SceneDev d{};
     const ar_scene_desc& D = s->desc;
@@ -888,28 +1000,23 @@ ar_status prepare(ar_batch* B, cudaStream_t st) {
       d.bmin[a] = D.box_min[a];
       d.bmax[a] = D.box_max[a];
       d.g[a] = D.gravity[a];
-      d.origin[a] = s->origin[a];
-      d.cell[a] = s->cell[a];
-      d.inv_cell[a] = 1.0f / s->cell[a];
     }
-    d.cell_pow2 = 1;
-    for (int a = 0; a < 3; ++a) {
-      int e = 0;
-      if (!(std::frexp(s->cell[a], &e) == 0.5f) || !std::isnormal(s->cell[a]) ||
-          !std::isnormal(d.inv_cell[a]))
-        d.cell_pow2 = 0;
-    }
+    scene_dev_grid(s, &d);
     d.r = D.radius; d.dt = D.dt; d.k = D.spring; d.damping = D.damping; d.shear = D.shear;
     d.attraction = D.attraction;
-    d.gx = s->gdim[0]; d.gy = s->gdim[1]; d.gz = s->gdim[2];
-    d.lx = (uint32_t)ceil_log2(d.gx);
-    d.ly = (uint32_t)ceil_log2(d.gy);
     d.cell_base = (uint32_t)cells;
     d.poff = (int)nt; d.boff = (int)bt; d.n = s->n; d.nb = s->nb;
     d.pos = s->pos; d.quat = s->quat; d.vel = s->vel; d.ang = s->ang;
     d.mass = s->mass; d.inv_inertia = s->inv_inertia; d.offsets = s->offsets; d.rel = s->rel;
     d.bforce = s->bforce; d.btorque = s->btorque;
     d.end_step = B->end_steps.empty() ? LLONG_MAX : B->end_steps[tab.size()];
+    if (s->cloud_n > 0) {
+      d.cloud_cells = s->cloud_cells;
+      d.cloud_pos = s->cloud_pos;
+      d.cloud_norm = s->cloud_norm;
+      B->has_cloud = true;
+    }
+    B->seen_version.push_back(s->version);
     tab.push_back(d);
     poff.push_back((int)nt);
     boff.push_back((int)bt);
@@ -1189,6 +1296,9 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   mark(4);
   AR_LAUNCH_ONE(collide_kernel, dim3(arh::grid_for(nt, bs)), dim3(bs), B->d_table, nt,
       B->skeys, B->svals, B->cells, B->spos, B->svel, B->pforce, B->d_step);
+  if (B->has_cloud)
+    AR_LAUNCH_ONE(cloud_collide_kernel, dim3(arh::grid_for(nt, 128)), dim3(128), B->d_table, nt,
+        B->skeys, B->svals, B->spos, B->svel, B->pforce);
   mark(5);
   AR_LAUNCH_ONE(body_step_kernel, dim3(g5), dim3(256), B->d_table, B->d_bscene, bt,
       B->pforce, B->d_step, ctx->d_err);
@@ -1505,10 +1615,20 @@ ar_status ar_scene_clone_async(const ar_scene* proto, ar_stream_t stream, ar_sce
   return arh::check_launch("ar_scene_clone_async");
 }
 
+static void free_cloud(ar_scene* s) {
+  cudaFree(s->cloud_pos);
+  cudaFree(s->cloud_norm);
+  cudaFree(s->cloud_cells);
+  s->cloud_pos = s->cloud_norm = nullptr;
+  s->cloud_cells = nullptr;
+  s->cloud_n = 0;
+}
+
 ar_status ar_scene_destroy(ar_scene* s) {
   if (!s) return AR_ERR_INVALID_ARG;
   if (s->solo) ar_batch_destroy(s->solo);
   if (s->block) cudaFree(s->block);  // waits for the device, like any cudaFree
+  free_cloud(s);
   delete s;
   return AR_OK;
 }
@@ -1516,11 +1636,77 @@ ar_status ar_scene_destroy(ar_scene* s) {
 ar_status ar_scene_destroy_async(ar_scene* s, ar_stream_t stream) {
   if (!s) return AR_ERR_INVALID_ARG;
   if (s->solo) ar_batch_destroy(s->solo);
+  if (s->cloud_n > 0) {  // the cloud is freed synchronously (it is not stream-ordered memory)
+    cudaStreamSynchronize(arh::stream(stream));
+    free_cloud(s);
+  }
   if (s->block && cudaFreeAsync(s->block, arh::stream(stream)) != cudaSuccess) {
     delete s;
     return arh::check_launch("ar_scene_destroy_async");
   }
   delete s;
+  return AR_OK;
+}
+
+ar_status ar_scene_set_static_cloud(ar_ctx* ctx, ar_scene* s, const float* cloud_pos4,
+                                    const float* cloud_norm4, int num_points,
+                                    ar_stream_t stream) {
+  if (!ctx || !s || num_points < 0 || (num_points > 0 && (!cloud_pos4 || !cloud_norm4)))
+    return AR_ERR_INVALID_ARG;
+  if (s->desc.broadphase != AR_BROADPHASE_GRID) {
+    arh::set_error("ar_scene_set_static_cloud: a static cloud needs the grid broad phase");
+    return AR_ERR_INVALID_ARG;
+  }
+  if (num_points > 0 && (((uintptr_t)cloud_pos4 | (uintptr_t)cloud_norm4) & 15u) != 0) {
+    arh::set_error("ar_scene_set_static_cloud: pointers must be 16-byte aligned");
+    return AR_ERR_INVALID_ARG;
+  }
+  // steps in flight, on any stream, may still read the old cloud
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    arh::set_error("ar_scene_set_static_cloud: %s", cudaGetErrorString(e));
+    return AR_ERR_CUDA;
+  }
+  free_cloud(s);
+  ++s->version;  // every batch holding the scene rebuilds its table (and graphs)
+  if (num_points == 0) return AR_OK;
+  cudaStream_t st = arh::stream(stream);
+  const int m = num_points;
+  SceneDev d{};
+  scene_dev_grid(s, &d);
+  const uint64_t cells = scene_cells(s);
+  const int key_bits = std::max(1, ceil_log2(cells));
+  const size_t ws_bytes = ar_sort::layout(m, 4, ar_sort::make_plan(0, key_bits).passes).total;
+  uint32_t *keys = nullptr, *skeys = nullptr, *sidx = nullptr;
+  char* ws = nullptr;
+  ar_status r = AR_OK;
+  if (!(alloc(&keys, m) && alloc(&skeys, m) && alloc(&sidx, m) && alloc(&ws, ws_bytes) &&
+        alloc(&s->cloud_pos, m) && alloc(&s->cloud_norm, m) && alloc(&s->cloud_cells, cells))) {
+    arh::set_error("ar_scene_set_static_cloud: out of device memory (%d points, %llu cells)", m,
+                   (unsigned long long)cells);
+    r = AR_ERR_OOM;
+  } else {
+    cudaMemsetAsync(s->cloud_cells, 0, cells * sizeof(uint2), st);  // every cell empty
+    cloud_keys_kernel<<<arh::grid_for(m, 256), 256, 0, st>>>(d, (const float4*)cloud_pos4, m,
+                                                             keys);
+    r = ar_sort::sort_u32(ctx, keys, nullptr, skeys, sidx, m, 0, key_bits, st, ws, ws_bytes);
+    if (r == AR_OK) {
+      cloud_place_kernel<<<arh::grid_for(m, 256), 256, 0, st>>>(
+          (const float4*)cloud_pos4, (const float4*)cloud_norm4, skeys, sidx, m, s->cloud_pos,
+          s->cloud_norm, s->cloud_cells);
+      r = arh::check_launch("ar_scene_set_static_cloud");
+    }
+    if (r == AR_OK && (e = cudaStreamSynchronize(st)) != cudaSuccess) {
+      arh::set_error("ar_scene_set_static_cloud: %s", cudaGetErrorString(e));
+      r = AR_ERR_CUDA;
+    }
+  }
+  cudaFree(keys); cudaFree(skeys); cudaFree(sidx); cudaFree(ws);
+  if (r != AR_OK) {
+    free_cloud(s);
+    return r;
+  }
+  s->cloud_n = m;
   return AR_OK;
 }
 
@@ -1774,17 +1960,17 @@ ar_status ar_scene_model_matrices(ar_scene* s, float* d_model16, ar_stream_t str
 
 int ar_batch_launches_per_step(ar_batch* B) {
   if (!B) return 0;
-  // memset, keys, sort, 4 tree kernels, collide, body sums, integration
   // BVH: memset, keys, the sort (32-bit keys: memset + four re-sort kernels after the first
-  // step; 64-bit keys: the radix sort), four tree kernels, collide, body sums, integration
+  // step; 64-bit keys: the radix sort), three tree kernels (build, leaves + refit, roots),
+  // collide, body sums, integration
   if (B->broadphase == AR_BROADPHASE_BVH)
     return 1 + 1 + (B->bvh_key_bits <= 32 ? 1 + 4 : ar_sort::launches(0, B->bvh_key_bits, false)) +
-           4 + 1 + 2;
+           3 + 1 + 2;
   // a step that re-sorts from the previous order (every step but the first after a change of
-  // the member list): clear, keys, four re-sort kernels, scatter, collide, body sums,
-  // integration
+  // the member list): clear, keys, four re-sort kernels, scatter, collide (and the static
+  // clouds' impulses when a scene has one), body sums, integration
   return 1 /*clear*/ + 1 /*keys*/ + 4 /*re-sort*/ + 1 /*scatter*/ + 1 /*collide*/ +
-         2 /*body sums, integration*/;
+         (B->has_cloud ? 1 : 0) + 2 /*body sums, integration*/;
 }
 
 int ar_scene_launches_per_step(ar_scene* s) {

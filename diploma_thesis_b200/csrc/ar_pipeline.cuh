@@ -31,6 +31,11 @@ struct SceneDev {
   const float4* rel;         // body-frame offset, w = local body index (int bits)
   float4* bforce;            // last step's per-body totals
   float4* btorque;
+  // static point cloud of the scene (null: none): its points sorted by cell of this scene's
+  // grid, with their normals, and {first, end} of every cell's points by local cell key
+  const uint2* cloud_cells;
+  const float4* cloud_pos;
+  const float4* cloud_norm;
 };
 
 __host__ __device__ __forceinline__ int3 cell_of(const SceneDev& s, float3 p) {

@@ -628,6 +628,23 @@ AR_API ar_status ar_scene_clone_async(const ar_scene* proto, ar_stream_t stream,
  * on that stream).  Scene memory comes from the device's stream-ordered pool, so a server can
  * admit and retire scenes while steps run. */
 AR_API ar_status ar_scene_destroy_async(ar_scene* scene, ar_stream_t stream);
+/* Attach a static point cloud to a grid scene (the augmented-reality scene from
+ * ar_range_image_cloud / ar_range_image_normals): cloud_pos4 and cloud_norm4 are device arrays
+ * of num_points float4 (w ignored), copied into the library, sorted by cell of the scene's grid
+ * and given their own cell table (8 bytes per cell of the scene's grid).  From the next step
+ * on, every particle also takes the impulses of the cloud points within 2r, in the reference's
+ * law (FindAndHandleAugmentedRealityCollisionsUniformGridKernel, RigidBodies/UniformGridDEM.cu:
+ * 243-377: along the point's negated normal, the scene at rest), summed over the 27
+ * neighbour cells in z, y, x order and added to the particle's force after its particle
+ * contacts and walls -- the simulateAR branch of updateUniformGridDEM
+ * (RigidBodies/UniformGridUpdate.cpp:967-969), which re-sorts the cloud every step; here it
+ * is sorted once.  num_points = 0 detaches the cloud.  Synchronises the device (steps in
+ * flight may read the old cloud); every batch holding the scene rebuilds its table before
+ * its next step.  A clone (ar_scene_clone_async) starts without a cloud.  BVH scenes:
+ * AR_ERR_INVALID_ARG. */
+AR_API ar_status ar_scene_set_static_cloud(ar_ctx* ctx, ar_scene* scene, const float* cloud_pos4,
+                                           const float* cloud_norm4, int num_points,
+                                           ar_stream_t stream);
 /* Device bytes a scene with this description keeps resident (state + its share of the
  * step workspace); used for HBM-budget admission. */
 AR_API size_t ar_scene_footprint(const ar_scene_desc* desc);

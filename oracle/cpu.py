@@ -44,6 +44,7 @@ for _name in ["or_aabb", "or_morton30", "or_morton63", "or_sort_pairs_u32", "or_
     getattr(_L, _name).restype = None
 _L.or_pairs_brute.restype = C.c_long
 _L.or_step.restype = C.c_int
+_L.or_step_ex.restype = C.c_int
 _L.or_step_f64.restype = C.c_int
 for _name in ["or_aabb", "or_morton30", "or_morton63", "or_sort_pairs_u32", "or_sort_pairs_u64",
               "or_calc_hash", "or_reorder", "or_collide_grid_dem", "or_pairs_brute"]:
@@ -269,11 +270,14 @@ def _scene_arrays(scene):
 
 
 def step(scene, steps: int = 1, grid=None, state: dict | None = None,
-         broadphase: str = "grid") -> dict:
+         broadphase: str = "grid", cloud=None) -> dict:
     """Float32 restatement of ar_step (operation for operation).  Returns the new body state
     and, for the last step, the sorted keys / indices, per-particle forces and body sums.
-    broadphase 'bvh' restates the BVH step (sorted keys are then the 30-bit Morton codes)."""
+    broadphase 'bvh' restates the BVH step (sorted keys are then the 30-bit Morton codes).
+    cloud = (positions [M, 4], normals [M, 4]): a static point cloud attached to the scene
+    (ar_scene_set_static_cloud; grid broad phase)."""
     if broadphase == "bvh":
+        assert cloud is None, "a static cloud needs the grid broad phase"
         return _step_bvh(scene, steps, state)
     origin, cell, dims = grid if grid is not None else scene_grid(scene)
     rel, s15 = _scene_arrays(scene)
@@ -285,11 +289,17 @@ def step(scene, steps: int = 1, grid=None, state: dict | None = None,
            "pforce": np.zeros((n, 4), np.float32), "bforce": np.zeros((nb, 4), np.float32),
            "btorque": np.zeros((nb, 4), np.float32)}
     g6 = _f32(list(origin) + list(cell))
-    ok = _L.or_step(_p(s15), _p(g6), _p(_u32(dims)), nb, n, _p(st["pos"]), _p(st["quat"]),
-                    _p(st["vel"]), _p(st["angvel"]), _p(_f32(scene.body_mass)),
-                    _p(_f32(scene.body_inv_inertia)), _p(_i32(scene.body_offsets)), _p(rel),
-                    steps, _p(out["skeys"]), _p(out["sidx"]), _p(out["pforce"]),
-                    _p(out["bforce"]), _p(out["btorque"]))
+    cp = cn = None
+    cm = 0
+    if cloud is not None:
+        cp, cn = _f32(cloud[0]).reshape(-1, 4), _f32(cloud[1]).reshape(-1, 4)
+        assert cp.shape == cn.shape
+        cm = cp.shape[0]
+    ok = _L.or_step_ex(_p(s15), _p(g6), _p(_u32(dims)), nb, n, _p(st["pos"]), _p(st["quat"]),
+                       _p(st["vel"]), _p(st["angvel"]), _p(_f32(scene.body_mass)),
+                       _p(_f32(scene.body_inv_inertia)), _p(_i32(scene.body_offsets)), _p(rel),
+                       steps, _p(out["skeys"]), _p(out["sidx"]), _p(out["pforce"]),
+                       _p(out["bforce"]), _p(out["btorque"]), _p(cp), _p(cn), cm)
     st.update(out)
     st["finite"] = bool(ok)
     return st

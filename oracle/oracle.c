@@ -307,6 +307,22 @@ static v3 spring_force(v3 rp, float dist, v3 rv, float contact, const float* prm
   f = add(f, scl(prm[3], rp));
   return f;
 }
+
+/* Impulse on a particle at velocity vel from a static scene point with normal nn,
+ * FindAndHandleAugmentedRealityCollisionsUniformGridCell (RigidBodies/UniformGridDEM.cu:275-296):
+ * along -nn, the scene at rest (rv = 0 - vel), rp = point - particle, dist = |rp| < contact
+ * tested by the caller.  prm = {spring, damping, shear, attraction}. */
+static v3 scene_force(v3 rp, float dist, v3 vel, v3 nn, float contact, const float* prm) {
+  v3 nrm = mk3(-nn.x, -nn.y, -nn.z);
+  v3 rv = mk3(0.f - vel.x, 0.f - vel.y, 0.f - vel.z);
+  v3 tv = sub(rv, scl(dot(rv, nrm), nrm));
+  v3 f = scl(-prm[0] * (contact - dist), nrm);
+  f = add(f, scl(prm[1], rv));
+  f = add(f, scl(prm[2], tv));
+  f = add(f, scl(prm[3], rp));
+  return f;
+}
+
 static v3 static_pair(v4 pa, v4 pb, v4 cm, v3 va, v3 vb, float ra, float rb, const float* prm,
                       v4* corr) {
   v3 rp = mk3(pb.x - pa.x, pb.y - pa.y, pb.z - pa.z);
@@ -753,8 +769,9 @@ void or_walls_reference(float radius, const float* ppos4, const float* rbpos4,
 
 /* ====================================================================================
  * Fused PHYSICAL step (the product's ar_step), float32, operation for operation:
- *   re-pose + hash -> stable sort -> cell ranges -> DEM gather + walls -> fixed-order body
- *   sums of F and r x F -> semi-implicit Euler.
+ *   re-pose + hash -> stable sort -> cell ranges -> DEM gather + walls (+ the static point
+ *   cloud's impulses, or_step_ex) -> fixed-order body sums of F and r x F -> semi-implicit
+ *   Euler.
  * scene12 = {bmin[3], bmax[3], g[3], r, dt, k}, scene3 = {damping, shear, attraction},
  * grid: origin[3], cell[3], dims[3].  rel4.w holds the body index (int bits).
  * Outputs (optional): sorted keys and indices, per-particle force, per-body sums.
@@ -850,13 +867,41 @@ static int bodies_step(const scene_t* S, int nb, const float* pf, float* bpos4, 
   return ok;
 }
 
-int or_step(const float* s15, const float* grid6, const uint32_t* dims3, int nb, int n,
-            float* bpos4, float* bquat4, float* bvel4, float* bang4, const float* mass,
-            const float* ib9, const int* off, const float* rel4, int steps, uint32_t* skeys_out,
-            uint32_t* sidx_out, float* pforce4_out, float* bforce4_out, float* btorque4_out) {
+/* or_step with a static point cloud of cm points (cloud_pos4, cloud_norm4; cm = 0: none): the
+ * cloud is sorted by (cell key, index) in the same grid once; after a particle's contacts and
+ * walls, the cloud points in its 27 neighbour cells (z, y, x order, a cell's points in sorted
+ * order, per-cell partial sums) with |rp| < 2r add scene_force, and the cloud total is added
+ * to the particle's force (the simulateAR branch of updateUniformGridDEM,
+ * RigidBodies/UniformGridUpdate.cpp:967-969, with the kernel of
+ * RigidBodies/UniformGridDEM.cu:301-377). */
+int or_step_ex(const float* s15, const float* grid6, const uint32_t* dims3, int nb, int n,
+               float* bpos4, float* bquat4, float* bvel4, float* bang4, const float* mass,
+               const float* ib9, const int* off, const float* rel4, int steps,
+               uint32_t* skeys_out, uint32_t* sidx_out, float* pforce4_out, float* bforce4_out,
+               float* btorque4_out, const float* cloud_pos4, const float* cloud_norm4, int cm) {
   scene_t S;
   scene_from(s15, grid6, dims3, &S);
   const int key_bits = 32;
+  uint32_t* ck = NULL;  /* the cloud's sorted keys and points, normals in the same order */
+  float *cp = NULL, *cn = NULL;
+  if (cm > 0) {
+    uint32_t* k0 = (uint32_t*)malloc(4l * cm);
+    uint32_t* ci = (uint32_t*)malloc(4l * cm);
+    ck = (uint32_t*)malloc(4l * cm);
+    cp = (float*)malloc(16l * cm);
+    cn = (float*)malloc(16l * cm);
+    for (int i = 0; i < cm; ++i) {
+      int c[3];
+      cell_of(&S.G, xyz(cloud_pos4 + 4l * i), c);
+      k0[i] = hash3(&S.G, c[0], c[1], c[2]);
+    }
+    or_sort_pairs_u32(k0, NULL, ck, ci, cm, 0, key_bits);
+    for (int j = 0; j < cm; ++j) {
+      memcpy(cp + 4l * j, cloud_pos4 + 4l * ci[j], 16);
+      memcpy(cn + 4l * j, cloud_norm4 + 4l * ci[j], 16);
+    }
+    free(k0); free(ci);
+  }
   uint32_t* keys = (uint32_t*)malloc(4l * n);
   uint32_t* sk = (uint32_t*)malloc(4l * n);
   uint32_t* sv = (uint32_t*)malloc(4l * n);
@@ -909,6 +954,22 @@ int or_step(const float* s15, const float* grid6, const uint32_t* dims3, int nb,
             lin = add(lin, cf);
           }
       lin = add(lin, wall_force(&S, pos, vel));
+      if (cm > 0) {
+        v3 tot = mk3(0.f, 0.f, 0.f);
+        for (int z = -1; z <= 1; ++z)
+          for (int y = -1; y <= 1; ++y)
+            for (int x = -1; x <= 1; ++x) {
+              v3 cf = mk3(0.f, 0.f, 0.f);
+              uint32_t h = hash3(&S.G, gp[0] + x, gp[1] + y, gp[2] + z);
+              for (long j = lower_bound_u32(ck, cm, h); j < cm && ck[j] == h; ++j) {
+                v3 rp = sub(xyz(cp + 4l * j), pos);
+                float dist = sqrtf(dot(rp, rp));
+                if (dist < thr) cf = add(cf, scene_force(rp, dist, vel, xyz(cn + 4l * j), thr, prm));
+              }
+              tot = add(tot, cf);
+            }
+        lin = add(lin, tot);
+      }
       st4(pf + 4l * sv[k], lin.x, lin.y, lin.z, 0.f);
     }
     if (!bodies_step(&S, nb, pf, bpos4, bquat4, bvel4, bang4, mass, ib9, off, rel4, bforce4_out,
@@ -919,7 +980,17 @@ int or_step(const float* s15, const float* grid6, const uint32_t* dims3, int nb,
   if (sidx_out) memcpy(sidx_out, sv, 4l * n);
   if (pforce4_out) memcpy(pforce4_out, pf, 16l * n);
   free(keys); free(sk); free(sv); free(sp); free(svl); free(pf);
+  free(ck); free(cp); free(cn);
   return ok;
+}
+
+int or_step(const float* s15, const float* grid6, const uint32_t* dims3, int nb, int n,
+            float* bpos4, float* bquat4, float* bvel4, float* bang4, const float* mass,
+            const float* ib9, const int* off, const float* rel4, int steps, uint32_t* skeys_out,
+            uint32_t* sidx_out, float* pforce4_out, float* bforce4_out, float* btorque4_out) {
+  return or_step_ex(s15, grid6, dims3, nb, n, bpos4, bquat4, bvel4, bang4, mass, ib9, off, rel4,
+                    steps, skeys_out, sidx_out, pforce4_out, bforce4_out, btorque4_out, NULL,
+                    NULL, 0);
 }
 
 /* ====================================================================================
@@ -1084,14 +1155,7 @@ void or_collide_static_scene(const float* grid6, const uint32_t* dims3, float ra
               v3 rp = sub(xyz(scene_spos4 + 4l * j), pos);
               float dist = sqrtf(dot(rp, rp));
               if (!(dist < thr)) continue;
-              v3 nn = xyz(scene_normals4 + 4l * o2);
-              v3 nrm = mk3(-nn.x, -nn.y, -nn.z);
-              v3 rv = mk3(0.f - vel.x, 0.f - vel.y, 0.f - vel.z);
-              v3 tv = sub(rv, scl(dot(rv, nrm), nrm));
-              v3 f = scl(-prm[0] * (thr - dist), nrm);
-              f = add(f, scl(prm[1], rv));
-              f = add(f, scl(prm[2], tv));
-              f = add(f, scl(prm[3], rp));
+              v3 f = scene_force(rp, dist, vel, xyz(scene_normals4 + 4l * o2), thr, prm);
               cf[0] = cf[0] + f.x; cf[1] = cf[1] + f.y; cf[2] = cf[2] + f.z; cf[3] = cf[3] + 0.f;
               ++contacts;
             }
