@@ -1194,7 +1194,9 @@ ar_status enqueue_step(ar_batch* B, cudaStream_t st, cudaEvent_t* ev = nullptr) 
   auto mark = [&](int i) {
     if (ev) cudaEventRecord(ev[i], st);
   };
-  int bs = 128;
+  // collision block size: the BVH walk runs 64-thread blocks (2M pile: 340 -> 336 us against
+  // 128), the grid gather 128 (32 to 128 measured within 1 us of one another)
+  int bs = B->broadphase == AR_BROADPHASE_BVH ? 64 : 128;
   if (ns > 0 && B->scenes[0]->desc.block_size > 0) bs = B->scenes[0]->desc.block_size;
   const unsigned gp = std::min(arh::grid_for(nt, 256), (unsigned)ctx->num_sms * 8);
   const unsigned g5 = arh::grid_for((long)bt * 32, 256);

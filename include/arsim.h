@@ -590,8 +590,8 @@ typedef struct ar_scene_desc {
   int broadphase;        /* AR_BROADPHASE_GRID or AR_BROADPHASE_BVH */
   float cell_size;       /* grid cell edge; 0 -> 2r */
   int grid_log2[3];      /* log2 grid cells per axis (wrapped); 0 -> derived from the box */
-  int block_size;        /* threads per CTA for the collision kernel: 0 -> 128, else a
-                            multiple of 32 in [32, 256] */
+  int block_size;        /* threads per CTA for the collision kernel: 0 -> 128 (grid) or 64
+                            (BVH), else a multiple of 32 in [32, 256] */
 } ar_scene_desc;
 
 typedef struct ar_scene ar_scene;
