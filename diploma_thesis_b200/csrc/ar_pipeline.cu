@@ -744,14 +744,21 @@ __global__ void __launch_bounds__(256) body_step_kernel(
     const int s0 = __ldg(S.offsets + b), s1 = __ldg(S.offsets + b + 1);
     const float4 q = S.quat[b];
     float fx = 0.f, fy = 0.f, fz = 0.f, tx = 0.f, ty = 0.f, tz = 0.f;
-    for (int i = s0 + lane; i < s1; i += 32) {
-      const float4 f4 = __ldcs(pforce + S.poff + i);
-      const float4 r4 = __ldg(S.rel + i);
+    auto add = [&](const float4& f4, const float4& r4) {
       const float3 f = ar::xyz(f4);
       const float3 t = ar::cross(ar::quat_rotate(q, ar::mk3(r4.x, r4.y, r4.z)), f);
       fx += f.x; fy += f.y; fz += f.z;
       tx += t.x; ty += t.y; tz += t.z;
+    };
+    // two of a lane's particles in flight together, added in the lane's order
+    int i = s0 + lane;
+    for (; i + 32 < s1; i += 64) {
+      const float4 f4a = __ldcs(pforce + S.poff + i), f4b = __ldcs(pforce + S.poff + i + 32);
+      const float4 r4a = __ldg(S.rel + i), r4b = __ldg(S.rel + i + 32);
+      add(f4a, r4a);
+      add(f4b, r4b);
     }
+    if (i < s1) add(__ldcs(pforce + S.poff + i), __ldg(S.rel + i));
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       fx += __shfl_xor_sync(0xffffffffu, fx, o);
